@@ -1,0 +1,237 @@
+/*
+ * Oracle (test infrastructure only): on-site energies, hoppings and Peierls
+ * phases of the models on the recursion hot path.  Restates the reference's
+ * arithmetic in the same operation order (see oracle.h for the rules).
+ */
+#include "oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define ORC_PI 3.14159265358979323846264338327950288
+
+/* diago, ham.F90:4696-4716:
+ * 2 C Re[(e^{-i G dy} + 2 e^{i G dy/2} cos(sqrt3 G dx/2)) e^{i phi}] */
+static double diago(double dx, double dy, double C, double phi, double aG)
+{
+    const double G1 = 4.0 * ORC_PI / sqrt(3.0) / aG;
+    const double e1r = cos(G1 * dy), e1i = -sin(G1 * dy);
+    const double hh = G1 * dy / 2.0;
+    const double k = cos(sqrt(3.0) * G1 * dx / 2.0);
+    const double e2r = 2.0 * cos(hh) * k, e2i = 2.0 * sin(hh) * k;
+    const double sr = e1r + e2r, si = e1i + e2i;
+    const double pr = cos(phi), pi_ = sin(phi);
+    return 2.0 * C * (sr * pr - si * pi_);
+}
+
+/* offdiago, ham.F90:4752-4776 */
+static void offdiago(double dx, double dy, double C, double phi, double aG, double* re, double* im)
+{
+    const double G1 = 4.0 * ORC_PI / sqrt(3.0) / aG;
+    const double ax = sqrt(3.0) * G1 * dx / 2.0;
+    const double p = cos(G1 * dy / 2.0 - phi);
+    const double q = sin(G1 * dy / 2.0 - phi - ORC_PI / 6.0);
+    *re = 2.0 * C * cos(ax) * (p + q) + 2.0 * C * sin(G1 * dy + phi - ORC_PI / 6.0);
+    *im = 2.0 * C * sin(ax) * (p - q);
+}
+
+/* del(1..3) of one atom or bond: ham.F90:12666-12678, :4862-4868 */
+static void bond_deltas(int spec, double re, double im, double del[3])
+{
+    del[0] = 2.0 * re / 3.0;
+    if (spec == 1) {
+        del[1] = -(re + sqrt(3.0) * im) / 3.0;
+        del[2] = (-re + sqrt(3.0) * im) / 3.0;
+    } else {
+        del[1] = (-re + sqrt(3.0) * im) / 3.0;
+        del[2] = -(re + sqrt(3.0) * im) / 3.0;
+    }
+}
+
+/* moire displacement map d = ((1+eps) R(theta) - 1) r (ham.F90:12610-12617, :3452-3458) */
+static void moire_disp(const orc_model* m, double x, double y, int integer_one, double* dx, double* dy)
+{
+    (void)integer_one;
+    if (m->moire_twisted) {
+        const double t = m->twist_rad;
+        *dx = x * ((1.0 + m->eps) * cos(t) - 1.0) - y * (1.0 + m->eps) * sin(t);
+        *dy = y * ((1.0 + m->eps) * cos(t) - 1.0) + x * (1.0 + m->eps) * sin(t);
+    } else {
+        *dx = x * m->eps;
+        *dy = y * m->eps;
+    }
+}
+
+void orc_onsite(const orc_model* m, int64_t n, const double* Rat, const int32_t* species,
+                const int32_t* layer, double* H0)
+{
+    /* ham.F90:846-850 and HamOnSiteSpeciesEnergies :3703-4014 (carbon) */
+    for (int64_t i = 0; i < n; ++i) H0[i] = m->e0_c;
+    /* HamOnSiteMoireEffective, ham.F90:3437-3544 */
+    if (m->moire_onsite != ORC_ONSITE_NONE) {
+        for (int64_t i = 0; i < n; ++i) {
+            double dx, dy;
+            moire_disp(m, Rat[3 * i], Rat[3 * i + 1], 1, &dx, &dy);
+            dy = dy + m->shift1;
+            if ((layer[i] == 1 && m->sign1 < 0.0) || (layer[i] == 2 && m->sign2 < 0.0)) {
+                dx = -dx;
+                dy = -dy;
+            }
+            double Hz = 0.0, Hd = 0.0;
+            switch (m->moire_onsite) {
+            case ORC_ONSITE_ONLY_H0: Hz = 0.0; Hd = diago(dx, dy, m->C0, m->Phi0, m->aG); break;
+            case ORC_ONSITE_ONLY_HZ: Hz = diago(dx, dy, m->Cz, m->Phiz, m->aG); Hd = 0.0; break;
+            case ORC_ONSITE_NO_H0_AND_HZ: Hz = 0.0; Hd = 0.0; break;
+            case ORC_ONSITE_H0_AND_HZ:
+                Hz = diago(dx, dy, m->Cz, m->Phiz, m->aG);
+                Hd = diago(dx, dy, m->C0, m->Phi0, m->aG);
+                break;
+            }
+            const double sgn = (species[i] % 2 == 1) ? -1.0 : 1.0; /* (-1)**Species */
+            if (layer[i] == 1) H0[i] = H0[i] + (sgn * Hz * m->sign1 + Hd);
+            else if (layer[i] == 2) H0[i] = H0[i] + (sgn * Hz * m->sign2 + Hd);
+        }
+    }
+    /* Anderson disorder, ham.F90:1237-1248, seeded by RandSeedFromInput (random.F90:31-52) */
+    if (m->anderson) {
+        orc_rng r;
+        orc_rng_put(&r, m->seed);
+        for (int64_t i = 0; i < n; ++i) {
+            const double rnd = orc_rng_r8(&r);
+            H0[i] = H0[i] + (rnd - 0.5) * m->anderson_w;
+        }
+    }
+}
+
+/* MoireBondDeltaMidpoint, ham.F90:4822-4883 (first moire: no post shift, no flips of Im) */
+static double moire_mid_delta(const orc_model* m, const double* ri, const double* bond, int spec, int flip)
+{
+    if (spec != 1 && spec != 2) return 0.0;
+    const double rm0 = ri[0] + 0.5 * bond[0], rm1 = ri[1] + 0.5 * bond[1];
+    const double th = m->moire_twisted ? m->twist_rad : 0.0;
+    double ddx = rm0 * ((1.0 + m->eps) * cos(th) - 1.0) - rm1 * (1.0 + m->eps) * sin(th);
+    double ddy = rm1 * ((1.0 + m->eps) * cos(th) - 1.0) + rm0 * (1.0 + m->eps) * sin(th);
+    ddy = ddy + m->shift1;
+    if (flip) {
+        ddx = -ddx;
+        ddy = -ddy;
+    }
+    ddx = ddx + 0.0;
+    ddy = ddy + 0.0;
+    double re, im, del[3];
+    offdiago(ddx, ddy, m->Cab, m->Phiab, m->aG, &re, &im);
+    bond_deltas(spec, re, im, del);
+    if (fabs(bond[0]) < m->aG / 4.0) return del[0];
+    if (bond[0] < 0.0) return del[2];
+    return del[1];
+}
+
+/* F2G2 single-layer shell terms of HamHopIntralayerGraphene, ham.F90:10660-10925 (twoLayers/oneLayer). */
+static double f2g2_shell(const orc_model* m, double dist)
+{
+    const double aG = m->aG, aCC = m->aCC;
+    if (dist > aCC * 0.9 && dist < aCC * 1.1) return 0.0;
+    if (dist > aG * 0.9 && dist < aG * 1.1) return m->tksl[2];
+    if (dist > 2.0 * aCC * 0.9 && dist < aCC * 2.0 * 1.1) return m->tksl[3];
+    if (dist > 2.0 * aCC * 1.1 && dist < 4.0) return m->tksl[4];
+    if (dist > (aCC * 3.0) * 0.9 && dist < (aCC * 3.0) * 1.1) return m->tksl[5];
+    if (dist > 2.0 * aG * 0.97 && dist < 2.0 * aG * 1.03) return m->tksl[6];
+    const double r7 = sqrt((2.0 * aG) * (2.0 * aG) + aCC * aCC);
+    if (dist > r7 * 0.9 && dist < r7 * 1.1) return m->tksl[7];
+    return 0.0; /* shell 8 is zero in every configuration used here */
+}
+
+/* HamHopping bond loop, ham.F90:6517-6846, for carbon layers (Species 1, 2):
+ * intralayer HamHopIntralayerDefault (:10177-10194) or HamHopIntralayerGraphene
+ * (:10616-10931); interlayer HamHopInterlayerTwoCenter (:9620-9838) with
+ * interlayerTwoCenter (:4094-4110), or the gIntLay term (:6837-6840). */
+void orc_hopping(const orc_model* m, int64_t n, const double* Rat, const int32_t* species,
+                 const int32_t* layer, int32_t maxNeigh, const int32_t* Nneigh, const int32_t* NList,
+                 const double* NeighD, double* hopp)
+{
+    memset(hopp, 0, sizeof(double) * 2 * (size_t)n * maxNeigh);
+    for (int64_t i = 0; i < n; ++i) {
+        double delta = 0.0;
+        double del[3] = {0.0, 0.0, 0.0};
+        if (m->moire_offdiag) { /* HamHopBondTermsMoire, ham.F90:12542-12680 (single-layer branch) */
+            double dx, dy, re, im;
+            moire_disp(m, Rat[3 * i], Rat[3 * i + 1], 0, &dx, &dy);
+            dy = dy + m->shift1;
+            if ((layer[i] == 1 && m->sign1 < 0.0) || (layer[i] == 2 && m->sign2 < 0.0)) {
+                dx = -dx;
+                dy = -dy;
+            }
+            offdiago(dx, dy, m->Cab, m->Phiab, m->aG, &re, &im);
+            if (species[i] == 1 || species[i] == 2) bond_deltas(species[i], re, im, del);
+        }
+        const int flip = (layer[i] == 1 && m->sign1 < 0.0) || (layer[i] == 2 && m->sign2 < 0.0);
+        for (int32_t j = 0; j < Nneigh[i]; ++j) {
+            const size_t e = (size_t)i * maxNeigh + j;
+            const int64_t jj = NList[e] - 1;
+            const double* D = NeighD + 3 * e;
+            double* h = hopp + 2 * e;
+            if (layer[i] == layer[jj]) {
+                const double d = sqrt(D[0] * D[0] + D[1] * D[1]);
+                for (int lv = 0; lv < m->tbnn; ++lv) {
+                    if (d < m->nradii[lv]) {
+                        if (d < 1.7) {
+                            if (fabs(D[0]) < m->aG / 4.0) delta = del[0];
+                            else if (D[0] < -m->aG / 4.0) delta = del[2];
+                            else if (D[0] > m->aG / 4.0) delta = del[1];
+                            if (m->moire_mid) delta = moire_mid_delta(m, Rat + 3 * i, D, species[i], flip);
+                        }
+                        if (m->intralayer == ORC_INTRA_F2G2_SL) {
+                            const double dist = sqrt(D[0] * D[0] + D[1] * D[1]);
+                            h[0] = h[0] + f2g2_shell(m, dist);
+                        }
+                        if (d > 1.5) delta = 0.0;
+                        h[0] = h[0] + (m->gn_cc[lv] - 1.0 * delta);
+                        break;
+                    }
+                }
+            } else if (layer[i] == layer[jj] + 1 || layer[i] == layer[jj] - 1) {
+                if (m->interlayer == ORC_INTER_TWO_CENTRE) {
+                    const double dist = sqrt(D[0] * D[0] + D[1] * D[1] + D[2] * D[2]);
+                    const double vsig = m->vppsigma0 * exp(-(dist - m->d_interlayer) / m->bl_delta) * 1.0;
+                    const double vpi = m->vpppi0 * exp(-(dist - m->aCC) / m->bl_delta) * 1.0;
+                    const double q = D[2] / dist;
+                    h[0] = h[0] + (vpi * (1.0 - q * q) + vsig * (q * q));
+                } else {
+                    const double d = sqrt(D[0] * D[0] + D[1] * D[1]);
+                    h[0] = h[0] + m->g_intlay * exp(-d / m->d_interlayer);
+                }
+            }
+        }
+    }
+}
+
+/* HamPeierlsPeriodicGauge, ham.F90:12834-12882 (with the corner term). */
+void orc_peierls(int64_t n, const double* Rat, const double* ucell, int32_t maxNeigh,
+                 const int32_t* Nneigh, const int32_t* NList, const int32_t* neighCell,
+                 double flux, double* hopp)
+{
+    const double cellArea = fabs(ucell[0] * ucell[4] - ucell[1] * ucell[3]);
+    const double fluxQuanta = flux * cellArea / (ORC_PI * 1.0e20);
+    const double mq = (double)lround(fluxQuanta);
+    for (int64_t i = 0; i < n; ++i) {
+        const double* ri = Rat + 3 * i;
+        for (int32_t j = 0; j < Nneigh[i]; ++j) {
+            const size_t e = (size_t)i * maxNeigh + j;
+            const double* rj = Rat + 3 * (size_t)(NList[e] - 1);
+            const int n1 = neighCell[3 * e], n2 = neighCell[3 * e + 1];
+            double v1[3] = {ri[0] + rj[0], ri[1] + rj[1], ri[2] + rj[2]};
+            double v2[3];
+            for (int k = 0; k < 3; ++k) v2[k] = (double)n1 * ucell[k] + (double)n2 * ucell[3 + k];
+            const double c3 = v1[0] * v2[1] - v1[1] * v2[0];             /* (v1 x v2)_z */
+            const double r3 = ri[0] * rj[1] - ri[1] * rj[0];             /* (ri x rj)_z */
+            double phase = flux * (r3 + c3) / 1.0e20;
+            if (n1 != 0 && n2 != 0) phase = phase + ORC_PI * mq * (double)n1 * (double)n2;
+            const double c = cos(phase), s = sin(phase);
+            double* h = hopp + 2 * e;
+            const double hr = h[0], hi = h[1];
+            h[0] = hr * c - hi * s;
+            h[1] = hr * s + hi * c;
+        }
+    }
+}
