@@ -1,0 +1,263 @@
+"""grabnes_b200 -- B200 (sm_100a) implementation of the GRABNES large-cell recursion hot path.
+
+The work is done by libgrabnes_gpu.so (CUDA kernels behind the C ABI of include/grabnes_gpu.h);
+this module is a thin ctypes binding that mirrors that ABI for Python callers and tests.  There is
+no CPU fallback: importing works without a GPU, but every call that needs the library raises if the
+shared object is missing or no CUDA device is present.
+"""
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libgrabnes_gpu.so")
+
+GBN_FP64, GBN_MIXED = 0, 1
+ERRORS = {-1: "argument", -2: "cuda", -3: "state", -4: "numeric", -5: "alloc", -6: "timeout"}
+
+
+class GbnError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"grabnes_gpu error {code} ({ERRORS.get(code, '?')}): {msg}")
+        self.code = code
+
+
+class Model(C.Structure):
+    """gbn_model of include/grabnes_gpu.h"""
+    _fields_ = [
+        ("aG", C.c_double), ("tbnn", C.c_int32), ("gn_cc", C.c_double * 8), ("nradii", C.c_double * 8),
+        ("intralayer", C.c_int32), ("tksl", C.c_double * 8),
+        ("moire_offdiag", C.c_int32), ("moire_mid", C.c_int32), ("moire_twisted", C.c_int32),
+        ("moire_onsite", C.c_int32), ("eps", C.c_double), ("twist_rad", C.c_double), ("shift1", C.c_double),
+        ("sign1", C.c_double), ("sign2", C.c_double), ("C0", C.c_double), ("Cz", C.c_double), ("Cab", C.c_double),
+        ("Phi0", C.c_double), ("Phiz", C.c_double), ("Phiab", C.c_double),
+        ("interlayer", C.c_int32), ("vpppi0", C.c_double), ("vppsigma0", C.c_double), ("bl_delta", C.c_double),
+        ("d_interlayer", C.c_double), ("aCC", C.c_double), ("g_intlay", C.c_double),
+        ("anderson", C.c_int32), ("anderson_w", C.c_double), ("e0_c", C.c_double),
+    ]
+
+
+_lib = None
+
+
+def lib():
+    """Load libgrabnes_gpu.so; raise (never fall back) if it is missing."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m grabnes_b200.build`")
+        _lib = C.CDLL(LIB_PATH)
+        _declare(_lib)
+    return _lib
+
+
+def _p(dtype):
+    return np.ctypeslib.ndpointer(dtype=dtype, flags="C_CONTIGUOUS")
+
+
+def _opt(dtype):
+    """pointer argument that also accepts None"""
+    base = _p(dtype)
+
+    class Opt(base):
+        @classmethod
+        def from_param(cls, obj):
+            return None if obj is None else base.from_param(obj)
+    return Opt
+
+
+EXPORTS = ["gbn_create", "gbn_destroy", "gbn_last_error", "gbn_version", "gbn_set_stream", "gbn_launch_count",
+           "gbn_last_timing", "gbn_set_geometry", "gbn_neighbours", "gbn_get_neighbours", "gbn_assemble",
+           "gbn_peierls", "gbn_get_hamiltonian", "gbn_load_hamiltonian", "gbn_lanczos", "gbn_lanczos_phases",
+           "gbn_stage_phases", "gbn_run_staged", "gbn_cf_dos", "gbn_cheb_evolve", "gbn_kubo_evol", "gbn_set_neighd"]
+
+
+def _declare(L):
+    d, i32, i64, vp = C.c_double, C.c_int32, C.c_int64, C.c_void_p
+    L.gbn_create.argtypes = [C.POINTER(vp), i32]
+    L.gbn_destroy.argtypes = [vp]
+    L.gbn_last_error.argtypes = [vp]
+    L.gbn_last_error.restype = C.c_char_p
+    L.gbn_version.restype = C.c_char_p
+    L.gbn_set_stream.argtypes = [vp, vp]
+    L.gbn_launch_count.argtypes = [vp]
+    L.gbn_launch_count.restype = i64
+    L.gbn_last_timing.argtypes = [vp, C.POINTER(d), C.POINTER(i64)]
+    L.gbn_set_geometry.argtypes = [vp, i64, _p(np.float64), _p(np.int32), _p(np.int32), _p(np.float64)]
+    L.gbn_neighbours.argtypes = [vp, d, d, i32, C.POINTER(i32), C.POINTER(i64)]
+    L.gbn_get_neighbours.argtypes = [vp, _opt(np.int32), _opt(np.int32), _opt(np.float64), _opt(np.int32)]
+    L.gbn_assemble.argtypes = [vp, C.POINTER(Model), _opt(np.float64), _opt(np.float64), _opt(np.float64)]
+    L.gbn_peierls.argtypes = [vp, d]
+    L.gbn_get_hamiltonian.argtypes = [vp, _opt(np.float64), _opt(np.complex128)]
+    L.gbn_load_hamiltonian.argtypes = [vp, i64, i32, _p(np.int32), _p(np.int32), _p(np.complex128), _p(np.float64)]
+    L.gbn_lanczos.argtypes = [vp, i32, i32, _p(np.complex128), _opt(np.int32), i32, _p(np.float64), _p(np.float64)]
+    L.gbn_lanczos_phases.argtypes = [vp, i32, i32, _p(np.float64), _opt(np.int32), i32, _p(np.float64),
+                                     _p(np.float64)]
+    L.gbn_stage_phases.argtypes = [vp, i32, i32, _p(np.float64)]
+    L.gbn_run_staged.argtypes = [vp, i32, _opt(np.float64), _opt(np.float64)]
+    L.gbn_cf_dos.argtypes = [vp, i32, _p(np.float64), _p(np.float64), _opt(np.int32), i32, d, i32, d, d,
+                             _opt(np.float64), _opt(np.float64), _p(np.float64)]
+    L.gbn_cheb_evolve.argtypes = [vp, i32, _p(np.complex128), i32, d, d, _p(np.complex128)]
+    L.gbn_kubo_evol.argtypes = [vp, i32, _p(np.complex128), i32, d, d, i32, _p(np.complex128), _p(np.complex128)]
+    L.gbn_set_neighd.argtypes = [vp, _p(np.float64)]
+
+
+def _c(a, dtype):
+    return np.ascontiguousarray(a, dtype=dtype).reshape(-1)
+
+
+class Context:
+    """One library context on one CUDA device (owns device memory and a stream)."""
+
+    def __init__(self, device=0):
+        self._L = lib()
+        h = C.c_void_p()
+        rc = self._L.gbn_create(C.byref(h), device)
+        if rc != 0:
+            raise GbnError(rc, "gbn_create failed (no CUDA device?)")
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.gbn_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _ck(self, rc):
+        if rc != 0:
+            raise GbnError(rc, self._L.gbn_last_error(self._h).decode())
+
+    # ---------------------------------------------------------------- plumbing
+    def set_stream(self, stream_handle):
+        self._ck(self._L.gbn_set_stream(self._h, C.c_void_p(stream_handle)))
+
+    @property
+    def launches(self):
+        return self._L.gbn_launch_count(self._h)
+
+    def last_timing(self):
+        ms, n = C.c_double(), C.c_int64()
+        self._ck(self._L.gbn_last_timing(self._h, C.byref(ms), C.byref(n)))
+        return ms.value, n.value
+
+    # ---------------------------------------------------------------- geometry / search
+    def set_geometry(self, rat, species, layer, ucell):
+        n = len(species)
+        self._ck(self._L.gbn_set_geometry(self._h, n, _c(rat, np.float64), _c(species, np.int32),
+                                          _c(layer, np.int32), _c(ucell, np.float64)))
+        self.n = n
+
+    def neighbours(self, cut2intra, cut2inter, second_layer=False, tables=True):
+        mx, tot = C.c_int32(), C.c_int64()
+        self._ck(self._L.gbn_neighbours(self._h, cut2intra, cut2inter, int(second_layer), C.byref(mx), C.byref(tot)))
+        self.max_neigh = mx.value
+        if not tables:
+            return dict(max_neigh=mx.value, total=tot.value)
+        n = self.n
+        nn = np.zeros(n, np.int32)
+        nl = np.zeros(n * mx.value, np.int32)
+        nd = np.zeros(n * mx.value * 3, np.float64)
+        nc = np.zeros(n * mx.value * 3, np.int32)
+        self._ck(self._L.gbn_get_neighbours(self._h, nn, nl, nd, nc))
+        return dict(max_neigh=mx.value, total=tot.value, nneigh=nn, nlist=nl.reshape(n, -1),
+                    neighd=nd.reshape(n, -1, 3), ncell=nc.reshape(n, -1, 3))
+
+    # ---------------------------------------------------------------- Hamiltonian
+    def assemble(self, model, rat_onsite=None, rat_hop=None, uniform=None):
+        self._ck(self._L.gbn_assemble(self._h, C.byref(model),
+                                      None if rat_onsite is None else _c(rat_onsite, np.float64),
+                                      None if rat_hop is None else _c(rat_hop, np.float64),
+                                      None if uniform is None else _c(uniform, np.float64)))
+
+    def peierls(self, flux):
+        self._ck(self._L.gbn_peierls(self._h, flux))
+
+    def hamiltonian(self):
+        h0 = np.zeros(self.n, np.float64)
+        hop = np.zeros(self.n * self.max_neigh, np.complex128)
+        self._ck(self._L.gbn_get_hamiltonian(self._h, h0, hop))
+        return h0, hop.reshape(self.n, -1)
+
+    def load_hamiltonian(self, nneigh, nlist, hopp, h0):
+        n = len(h0)
+        mx = np.asarray(nlist).reshape(n, -1).shape[1]
+        self._ck(self._L.gbn_load_hamiltonian(self._h, n, mx, _c(nneigh, np.int32), _c(nlist, np.int32),
+                                              _c(hopp, np.complex128), _c(h0, np.float64)))
+        self.n, self.max_neigh = n, mx
+
+    def set_neighd(self, neighd):
+        self._ck(self._L.gbn_set_neighd(self._h, _c(neighd, np.float64)))
+
+    # ---------------------------------------------------------------- recursion
+    def lanczos(self, psi0, nsteps, precision=GBN_FP64):
+        """psi0: complex [nrhs, N] start vectors; nsteps: int or [nrhs]; returns a, b [nrhs, nmax]."""
+        psi = np.ascontiguousarray(np.atleast_2d(psi0), np.complex128)
+        nrhs = psi.shape[0]
+        ns = np.broadcast_to(np.asarray(nsteps, np.int32), (nrhs,)).copy()
+        nmax = int(ns.max())
+        a = np.zeros((nrhs, nmax))
+        b = np.zeros((nrhs, nmax))
+        self._ck(self._L.gbn_lanczos(self._h, precision, nrhs, psi.reshape(-1), ns, nmax, a.reshape(-1), b.reshape(-1)))
+        return a, b
+
+    def lanczos_phases(self, u, nsteps, precision=GBN_FP64):
+        """u: uniform draws [nrhs, N]: start vectors exp(2 pi i u)/sqrt(N)."""
+        uu = np.ascontiguousarray(np.atleast_2d(u), np.float64)
+        nrhs = uu.shape[0]
+        ns = np.broadcast_to(np.asarray(nsteps, np.int32), (nrhs,)).copy()
+        nmax = int(ns.max())
+        a = np.zeros((nrhs, nmax))
+        b = np.zeros((nrhs, nmax))
+        self._ck(self._L.gbn_lanczos_phases(self._h, precision, nrhs, uu.reshape(-1), ns, nmax, a.reshape(-1),
+                                            b.reshape(-1)))
+        return a, b
+
+    def stage_phases(self, u, precision=GBN_MIXED):
+        uu = np.ascontiguousarray(np.atleast_2d(u), np.float64)
+        self._staged = uu.shape[0]
+        self._ck(self._L.gbn_stage_phases(self._h, precision, uu.shape[0], uu.reshape(-1)))
+
+    def run_staged(self, nmax, a=None, b=None):
+        self._ck(self._L.gbn_run_staged(self._h, nmax, None if a is None else a.reshape(-1),
+                                        None if b is None else b.reshape(-1)))
+
+    def cf_dos(self, a, b, eta, n_en, emin, emax, nsteps=None, norm=None):
+        a = np.ascontiguousarray(np.atleast_2d(a), np.float64)
+        b = np.ascontiguousarray(np.atleast_2d(b), np.float64)
+        nrhs, nmax = a.shape
+        ns = None if nsteps is None else np.broadcast_to(np.asarray(nsteps, np.int32), (nrhs,)).copy()
+        nm = None if norm is None else np.broadcast_to(np.asarray(norm, np.float64), (nrhs,)).copy()
+        e = np.zeros(n_en + 1)
+        dos = np.zeros((nrhs, n_en + 1))
+        self._ck(self._L.gbn_cf_dos(self._h, nrhs, a.reshape(-1), b.reshape(-1), ns, nmax, eta, n_en, emin, emax, nm,
+                                    e, dos.reshape(-1)))
+        return e, dos
+
+    # ---------------------------------------------------------------- Chebyshev
+    def cheb_evolve(self, c, ac, bc, z):
+        zz = np.ascontiguousarray(np.atleast_2d(z), np.complex128).copy()
+        cc = _c(c, np.complex128)
+        self._ck(self._L.gbn_cheb_evolve(self._h, zz.shape[0], cc, len(cc), ac, bc, zz.reshape(-1)))
+        return zz
+
+    def kubo_evol(self, c, ac, bc, psi, zupsi, direction=1):
+        p = np.ascontiguousarray(np.atleast_2d(psi), np.complex128).copy()
+        z = np.ascontiguousarray(np.atleast_2d(zupsi), np.complex128).copy()
+        cc = _c(c, np.complex128)
+        self._ck(self._L.gbn_kubo_evol(self._h, p.shape[0], cc, len(cc), ac, bc, direction, p.reshape(-1),
+                                       z.reshape(-1)))
+        return p, z
+
+
+def version():
+    return lib().gbn_version().decode()

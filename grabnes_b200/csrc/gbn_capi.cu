@@ -1,0 +1,455 @@
+// C ABI of libgrabnes_gpu (declared in include/grabnes_gpu.h): context management, argument
+// checking, host<->device copies, tiling of many right-hand sides.  No function aborts; every error is
+// returned as a GBN_ERR_* code with its text in gbn_last_error().
+#include <cuda_runtime.h>
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "gbn_internal.cuh"
+
+namespace gbn {
+
+int fail(gbn_ctx* c, int code, const std::string& msg)
+{
+    if (c) c->err = msg;
+    return code;
+}
+
+int cuda_fail(gbn_ctx* c, cudaError_t e, const char* what)
+{
+    if (c) c->err = std::string("CUDA error in ") + what + ": " + cudaGetErrorString(e);
+    return (e == cudaErrorMemoryAllocation) ? GBN_ERR_ALLOC : GBN_ERR_CUDA;
+}
+
+static int tile_width(int nrhs)
+{
+    int t = 1;
+    while (t < nrhs && t < 32) t <<= 1;
+    return t;
+}
+
+// Runs the recursion for all right-hand sides in tiles of at most 32; inputs are either complex start
+// vectors (psi) or uniform draws (phases), [nrhs][n] on the host.
+static int run_tiled(gbn_ctx* c, int prec, int nrhs, const double* host_in, bool phases, const int32_t* nsteps,
+                     int32_t nmax, double* a, double* b)
+{
+    const int T = tile_width(nrhs);
+    int rc = lanczos_prepare(c, prec, T);
+    if (rc) return rc;
+    const size_t per = (size_t)c->n * (phases ? 1 : 2);
+    GBN_CK(c, c->upload.ensure(sizeof(double) * per * T));
+    double step_ms = 0.0;
+    int64_t launches = 0;
+    std::vector<double> hab;
+    for (int r0 = 0; r0 < nrhs; r0 += T) {
+        const int cnt = std::min(T, nrhs - r0);
+        int32_t nt = 0;
+        for (int r = r0; r < r0 + cnt; ++r) nt = std::max(nt, nsteps ? nsteps[r] : nmax);
+        GBN_CK(c, cudaMemcpyAsync(c->upload.p, host_in + per * r0, sizeof(double) * per * cnt, cudaMemcpyHostToDevice,
+                                  c->stream));
+        rc = phases ? lanczos_start_from_phases(c, c->upload.as<double>(), cnt)
+                    : lanczos_start_from_psi(c, c->upload.as<double>(), cnt);
+        if (rc) return rc;
+        rc = lanczos_run(c, nt);
+        if (rc) return rc;
+        step_ms += c->timing.step_ms;
+        launches += c->timing.step_launches;
+        hab.resize((size_t)2 * T * nt);
+        GBN_CK(c, cudaMemcpyAsync(hab.data(), c->ab.p, sizeof(double) * hab.size(), cudaMemcpyDeviceToHost, c->stream));
+        GBN_CK(c, cudaStreamSynchronize(c->stream));
+        for (int r = 0; r < cnt; ++r) {
+            memcpy(a + (size_t)(r0 + r) * nmax, hab.data() + (size_t)r * nt, sizeof(double) * nt);
+            memcpy(b + (size_t)(r0 + r) * nmax, hab.data() + (size_t)T * nt + (size_t)r * nt, sizeof(double) * nt);
+        }
+    }
+    c->timing.step_ms = step_ms;
+    c->timing.step_launches = launches;
+    return GBN_OK;
+}
+
+static int check_solver_args(gbn_ctx* c, int32_t precision, int32_t nrhs, const void* in, const int32_t* nsteps,
+                             int32_t nmax, const double* a, const double* b)
+{
+    if (!c->have_ham) return fail(c, GBN_ERR_STATE, "no Hamiltonian: call gbn_load_hamiltonian or gbn_assemble first");
+    if (precision != GBN_FP64 && precision != GBN_MIXED) return fail(c, GBN_ERR_ARG, "precision must be GBN_FP64 or GBN_MIXED");
+    if (nrhs < 1) return fail(c, GBN_ERR_ARG, "nrhs must be at least 1");
+    if (nmax < 1) return fail(c, GBN_ERR_ARG, "nmax must be at least 1");
+    if (!in || !a || !b) return fail(c, GBN_ERR_ARG, "NULL input or output array");
+    if (nsteps)
+        for (int r = 0; r < nrhs; ++r)
+            if (nsteps[r] < 1 || nsteps[r] > nmax) return fail(c, GBN_ERR_ARG, "nsteps[r] must be in 1..nmax");
+    return GBN_OK;
+}
+
+}  // namespace gbn
+
+using namespace gbn;
+
+extern "C" {
+
+const char* gbn_version(void) { return "grabnes_b200 0.1 (sm_100a)"; }
+
+int gbn_create(gbn_ctx** out, int32_t device)
+{
+    if (!out) return GBN_ERR_ARG;
+    *out = nullptr;
+    gbn_ctx* c = new (std::nothrow) gbn_ctx();
+    if (!c) return GBN_ERR_ALLOC;
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0) {
+        delete c;
+        return GBN_ERR_CUDA;
+    }
+    if (device < 0 || device >= ndev) {
+        delete c;
+        return GBN_ERR_ARG;
+    }
+    c->device = device;
+    if (cudaSetDevice(device) != cudaSuccess ||
+        cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete c;
+        return GBN_ERR_CUDA;
+    }
+    c->own_stream = true;
+    *out = c;
+    return GBN_OK;
+}
+
+int gbn_destroy(gbn_ctx* c)
+{
+    if (!c) return GBN_OK;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    DevBuf* bufs[] = {&c->rat, &c->species, &c->layer, &c->nneigh, &c->nlist, &c->neighd, &c->ncell, &c->h0,
+                      &c->hopp, &c->rat_hop, &c->perm, &c->iperm, &c->ell.slice_ptr, &c->ell.col, &c->ell.val,
+                      &c->ell.h0, &c->partials, &c->scal, &c->counter, &c->ab, &c->upload};
+    for (DevBuf* b : bufs) b->release();
+    for (auto& v : c->vec) v.release();
+    for (auto& v : c->cheb) v.release();
+    if (c->ev0) cudaEventDestroy(c->ev0);
+    if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return GBN_OK;
+}
+
+const char* gbn_last_error(const gbn_ctx* c) { return c ? c->err.c_str() : "no context"; }
+
+int gbn_set_stream(gbn_ctx* c, void* s)
+{
+    if (!c) return GBN_ERR_ARG;
+    cudaSetDevice(c->device);
+    if (c->own_stream && c->stream) cudaStreamSynchronize(c->stream);
+    if (s) {
+        if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+        c->stream = static_cast<cudaStream_t>(s);
+        c->own_stream = false;
+    } else if (!c->own_stream) {
+        GBN_CK(c, cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+        c->own_stream = true;
+    }
+    return GBN_OK;
+}
+
+int64_t gbn_launch_count(const gbn_ctx* c) { return c ? c->launches : 0; }
+
+int gbn_last_timing(const gbn_ctx* c, double* ms, int64_t* launches)
+{
+    if (!c) return GBN_ERR_ARG;
+    if (ms) *ms = c->timing.step_ms;
+    if (launches) *launches = c->timing.step_launches;
+    return GBN_OK;
+}
+
+int gbn_set_geometry(gbn_ctx* c, int64_t n, const double* rat, const int32_t* species, const int32_t* layer,
+                     const double* ucell)
+{
+    if (!c) return GBN_ERR_ARG;
+    if (n < 1 || n >= (int64_t)1 << 31) return fail(c, GBN_ERR_ARG, "number of atoms must be in 1..2^31-1");
+    if (!rat || !species || !layer || !ucell) return fail(c, GBN_ERR_ARG, "NULL geometry array");
+    cudaSetDevice(c->device);
+    GBN_CK(c, c->rat.ensure(sizeof(double) * 3 * n));
+    GBN_CK(c, c->species.ensure(sizeof(int32_t) * n));
+    GBN_CK(c, c->layer.ensure(sizeof(int32_t) * n));
+    GBN_CK(c, cudaMemcpyAsync(c->rat.p, rat, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, c->stream));
+    GBN_CK(c, cudaMemcpyAsync(c->species.p, species, sizeof(int32_t) * n, cudaMemcpyHostToDevice, c->stream));
+    GBN_CK(c, cudaMemcpyAsync(c->layer.p, layer, sizeof(int32_t) * n, cudaMemcpyHostToDevice, c->stream));
+    GBN_CK(c, cudaStreamSynchronize(c->stream));
+    memcpy(c->ucell, ucell, sizeof(c->ucell));
+    c->n = n;
+    c->have_geometry = true;
+    c->have_neigh = c->have_neighd = c->have_ham = false;
+    c->ell.valid = false;
+    return build_spatial_perm(c);
+}
+
+int gbn_neighbours(gbn_ctx* c, double cut2intra, double cut2inter, int32_t second_layer, int32_t* max_neigh,
+                   int64_t* total)
+{
+    if (!c) return GBN_ERR_ARG;
+    if (!c->have_geometry) return fail(c, GBN_ERR_STATE, "no geometry: call gbn_set_geometry first");
+    if (!(cut2intra > 0.0) || !(cut2inter > 0.0)) return fail(c, GBN_ERR_ARG, "search radii must be positive");
+    cudaSetDevice(c->device);
+    const int rc = neigh_search(c, cut2intra, cut2inter, second_layer);
+    if (rc) return rc;
+    if (max_neigh) *max_neigh = c->max_neigh;
+    if (total) *total = c->total;
+    return GBN_OK;
+}
+
+int gbn_get_neighbours(gbn_ctx* c, int32_t* nneigh, int32_t* nlist, double* neighd, int32_t* ncell)
+{
+    if (!c) return GBN_ERR_ARG;
+    if (!c->have_neigh) return fail(c, GBN_ERR_STATE, "no neighbour tables");
+    cudaSetDevice(c->device);
+    const size_t e = (size_t)c->n * c->max_neigh;
+    if (nneigh) GBN_CK(c, cudaMemcpyAsync(nneigh, c->nneigh.p, sizeof(int32_t) * c->n, cudaMemcpyDeviceToHost, c->stream));
+    if (nlist) GBN_CK(c, cudaMemcpyAsync(nlist, c->nlist.p, sizeof(int32_t) * e, cudaMemcpyDeviceToHost, c->stream));
+    if (neighd) {
+        if (!c->have_neighd) return fail(c, GBN_ERR_STATE, "no NeighD table");
+        GBN_CK(c, cudaMemcpyAsync(neighd, c->neighd.p, sizeof(double) * 3 * e, cudaMemcpyDeviceToHost, c->stream));
+    }
+    if (ncell) {
+        if (!c->ncell.p) return fail(c, GBN_ERR_STATE, "no neighCell table");
+        GBN_CK(c, cudaMemcpyAsync(ncell, c->ncell.p, sizeof(int32_t) * 3 * e, cudaMemcpyDeviceToHost, c->stream));
+    }
+    GBN_CK(c, cudaStreamSynchronize(c->stream));
+    return GBN_OK;
+}
+
+int gbn_assemble(gbn_ctx* c, const gbn_model* m, const double* rat_on, const double* rat_hop, const double* uniform)
+{
+    if (!c || !m) return GBN_ERR_ARG;
+    if (!c->have_neigh || !c->have_neighd) return fail(c, GBN_ERR_STATE, "no neighbour tables: call gbn_neighbours first");
+    if (m->tbnn < 1 || m->tbnn > 8) return fail(c, GBN_ERR_ARG, "tbnn must be in 1..8");
+    if (m->anderson && !uniform) return fail(c, GBN_ERR_ARG, "Anderson disorder needs the uniform draws");
+    cudaSetDevice(c->device);
+    DevBuf ron, uni;
+    const double* d_on = c->rat.as<double>();
+    const double* d_hop = c->rat.as<double>();
+    if (rat_on) {
+        GBN_CK(c, ron.ensure(sizeof(double) * 3 * c->n));
+        GBN_CK(c, cudaMemcpyAsync(ron.p, rat_on, sizeof(double) * 3 * c->n, cudaMemcpyHostToDevice, c->stream));
+        d_on = ron.as<double>();
+    }
+    GBN_CK(c, c->rat_hop.ensure(sizeof(double) * 3 * c->n));
+    if (rat_hop)
+        GBN_CK(c, cudaMemcpyAsync(c->rat_hop.p, rat_hop, sizeof(double) * 3 * c->n, cudaMemcpyHostToDevice, c->stream));
+    else
+        GBN_CK(c, cudaMemcpyAsync(c->rat_hop.p, c->rat.p, sizeof(double) * 3 * c->n, cudaMemcpyDeviceToDevice, c->stream));
+    d_hop = c->rat_hop.as<double>();
+    const double* d_uni = nullptr;
+    if (m->anderson) {
+        GBN_CK(c, uni.ensure(sizeof(double) * c->n));
+        GBN_CK(c, cudaMemcpyAsync(uni.p, uniform, sizeof(double) * c->n, cudaMemcpyHostToDevice, c->stream));
+        d_uni = uni.as<double>();
+    }
+    const int rc = assemble(c, m, d_on, d_hop, d_uni);
+    GBN_CK(c, cudaStreamSynchronize(c->stream));
+    return rc;
+}
+
+int gbn_peierls(gbn_ctx* c, double flux)
+{
+    if (!c) return GBN_ERR_ARG;
+    if (!c->have_ham || !c->ncell.p || !c->rat_hop.p)
+        return fail(c, GBN_ERR_STATE, "Peierls phases need an assembled Hamiltonian (gbn_assemble)");
+    cudaSetDevice(c->device);
+    return peierls(c, flux);
+}
+
+int gbn_get_hamiltonian(gbn_ctx* c, double* h0, double* hopp)
+{
+    if (!c) return GBN_ERR_ARG;
+    if (!c->have_ham) return fail(c, GBN_ERR_STATE, "no Hamiltonian");
+    cudaSetDevice(c->device);
+    if (h0) GBN_CK(c, cudaMemcpyAsync(h0, c->h0.p, sizeof(double) * c->n, cudaMemcpyDeviceToHost, c->stream));
+    if (hopp)
+        GBN_CK(c, cudaMemcpyAsync(hopp, c->hopp.p, sizeof(double2) * (size_t)c->n * c->max_neigh, cudaMemcpyDeviceToHost,
+                                  c->stream));
+    GBN_CK(c, cudaStreamSynchronize(c->stream));
+    return GBN_OK;
+}
+
+int gbn_load_hamiltonian(gbn_ctx* c, int64_t n, int32_t max_neigh, const int32_t* nneigh, const int32_t* nlist,
+                         const double* hopp, const double* h0)
+{
+    if (!c) return GBN_ERR_ARG;
+    if (n < 1 || n >= (int64_t)1 << 31) return fail(c, GBN_ERR_ARG, "number of atoms must be in 1..2^31-1");
+    if (max_neigh < 1) return fail(c, GBN_ERR_ARG, "max_neigh must be at least 1");
+    if (!nneigh || !nlist || !hopp || !h0) return fail(c, GBN_ERR_ARG, "NULL Hamiltonian array");
+    for (int64_t i = 0; i < n; ++i) {
+        if (nneigh[i] < 0 || nneigh[i] > max_neigh) return fail(c, GBN_ERR_ARG, "Nneigh(i) outside 0..maxNeigh");
+        for (int32_t j = 0; j < nneigh[i]; ++j) {
+            const int32_t m = nlist[i * max_neigh + j];
+            if (m < 1 || m > n) return fail(c, GBN_ERR_ARG, "NList entry outside 1..N");
+        }
+    }
+    bool cplx = false;
+    const size_t e = (size_t)n * max_neigh;
+    for (size_t k = 0; k < e && !cplx; ++k) cplx = hopp[2 * k + 1] != 0.0;
+    cudaSetDevice(c->device);
+    const bool same_atoms = c->have_geometry && c->n == n;
+    GBN_CK(c, c->nneigh.ensure(sizeof(int32_t) * n));
+    GBN_CK(c, c->nlist.ensure(sizeof(int32_t) * e));
+    GBN_CK(c, c->hopp.ensure(sizeof(double2) * e));
+    GBN_CK(c, c->h0.ensure(sizeof(double) * n));
+    GBN_CK(c, cudaMemcpyAsync(c->nneigh.p, nneigh, sizeof(int32_t) * n, cudaMemcpyHostToDevice, c->stream));
+    GBN_CK(c, cudaMemcpyAsync(c->nlist.p, nlist, sizeof(int32_t) * e, cudaMemcpyHostToDevice, c->stream));
+    GBN_CK(c, cudaMemcpyAsync(c->hopp.p, hopp, sizeof(double2) * e, cudaMemcpyHostToDevice, c->stream));
+    GBN_CK(c, cudaMemcpyAsync(c->h0.p, h0, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
+    GBN_CK(c, cudaStreamSynchronize(c->stream));
+    if (!same_atoms) {
+        c->have_geometry = false;
+        c->n = n;
+        const int rc = build_identity_perm(c);
+        if (rc) return rc;
+    }
+    c->max_neigh = max_neigh;
+    c->have_neigh = true;
+    c->have_neighd = same_atoms && c->have_neighd;
+    c->have_ham = true;
+    c->ham_complex = cplx;
+    c->ell.valid = false;
+    return GBN_OK;
+}
+
+int gbn_set_neighd(gbn_ctx* c, const double* neighd)
+{
+    if (!c || !neighd) return GBN_ERR_ARG;
+    if (!c->have_neigh) return fail(c, GBN_ERR_STATE, "load the neighbour list first");
+    cudaSetDevice(c->device);
+    const size_t e = (size_t)c->n * c->max_neigh;
+    GBN_CK(c, c->neighd.ensure(sizeof(double) * 3 * e));
+    GBN_CK(c, cudaMemcpyAsync(c->neighd.p, neighd, sizeof(double) * 3 * e, cudaMemcpyHostToDevice, c->stream));
+    GBN_CK(c, cudaStreamSynchronize(c->stream));
+    c->have_neighd = true;
+    return GBN_OK;
+}
+
+int gbn_lanczos(gbn_ctx* c, int32_t precision, int32_t nrhs, const double* psi0, const int32_t* nsteps, int32_t nmax,
+                double* a, double* b)
+{
+    if (!c) return GBN_ERR_ARG;
+    int rc = check_solver_args(c, precision, nrhs, psi0, nsteps, nmax, a, b);
+    if (rc) return rc;
+    cudaSetDevice(c->device);
+    return run_tiled(c, precision, nrhs, psi0, false, nsteps, nmax, a, b);
+}
+
+int gbn_lanczos_phases(gbn_ctx* c, int32_t precision, int32_t nrhs, const double* u, const int32_t* nsteps,
+                       int32_t nmax, double* a, double* b)
+{
+    if (!c) return GBN_ERR_ARG;
+    int rc = check_solver_args(c, precision, nrhs, u, nsteps, nmax, a, b);
+    if (rc) return rc;
+    cudaSetDevice(c->device);
+    return run_tiled(c, precision, nrhs, u, true, nsteps, nmax, a, b);
+}
+
+int gbn_stage_phases(gbn_ctx* c, int32_t precision, int32_t nrhs, const double* u)
+{
+    if (!c) return GBN_ERR_ARG;
+    if (!c->have_ham) return fail(c, GBN_ERR_STATE, "no Hamiltonian");
+    if (!u) return fail(c, GBN_ERR_ARG, "NULL draws");
+    if (precision != GBN_FP64 && precision != GBN_MIXED) return fail(c, GBN_ERR_ARG, "bad precision");
+    if (nrhs != 1 && nrhs != 2 && nrhs != 4 && nrhs != 8 && nrhs != 16 && nrhs != 32)
+        return fail(c, GBN_ERR_ARG, "staged runs take 1, 2, 4, 8, 16 or 32 vectors");
+    cudaSetDevice(c->device);
+    int rc = lanczos_prepare(c, precision, nrhs);
+    if (rc) return rc;
+    GBN_CK(c, c->upload.ensure(sizeof(double) * (size_t)c->n * nrhs));
+    GBN_CK(c, cudaMemcpyAsync(c->upload.p, u, sizeof(double) * (size_t)c->n * nrhs, cudaMemcpyHostToDevice, c->stream));
+    rc = lanczos_start_from_phases(c, c->upload.as<double>(), nrhs);
+    if (rc) return rc;
+    GBN_CK(c, cudaStreamSynchronize(c->stream));
+    c->staged = true;
+    return GBN_OK;
+}
+
+int gbn_run_staged(gbn_ctx* c, int32_t nmax, double* a, double* b)
+{
+    if (!c) return GBN_ERR_ARG;
+    if (!c->staged) return fail(c, GBN_ERR_STATE, "nothing staged: call gbn_stage_phases first");
+    if (nmax < 1) return fail(c, GBN_ERR_ARG, "nmax must be at least 1");
+    cudaSetDevice(c->device);
+    // the start vectors are rebuilt from the staged draws so that every run starts from them
+    int rc = lanczos_start_from_phases(c, c->upload.as<double>(), c->nrhs);
+    if (rc) return rc;
+    rc = lanczos_run(c, nmax);
+    if (rc) return rc;
+    if (a && b) {
+        GBN_CK(c, cudaMemcpyAsync(a, c->ab.p, sizeof(double) * (size_t)c->nrhs * nmax, cudaMemcpyDeviceToHost, c->stream));
+        GBN_CK(c, cudaMemcpyAsync(b, c->ab.as<double>() + (size_t)c->nrhs * nmax, sizeof(double) * (size_t)c->nrhs * nmax,
+                                  cudaMemcpyDeviceToHost, c->stream));
+        GBN_CK(c, cudaStreamSynchronize(c->stream));
+    }
+    return GBN_OK;
+}
+
+int gbn_cf_dos(gbn_ctx* c, int32_t nrhs, const double* a, const double* b, const int32_t* nsteps, int32_t nmax,
+               double eta, int32_t n_en, double emin, double emax, const double* norm, double* energy, double* dos)
+{
+    if (!c) return GBN_ERR_ARG;
+    if (nrhs < 1 || nmax < 1 || n_en < 1 || !a || !b || !dos) return fail(c, GBN_ERR_ARG, "bad continued-fraction arguments");
+    if (!(eta > 0.0)) return fail(c, GBN_ERR_ARG, "eta must be positive");
+    if (nsteps)
+        for (int r = 0; r < nrhs; ++r)
+            if (nsteps[r] < 1 || nsteps[r] > nmax) return fail(c, GBN_ERR_ARG, "nsteps[r] must be in 1..nmax");
+    cudaSetDevice(c->device);
+    const size_t nab = (size_t)nrhs * nmax, nd = (size_t)nrhs * (n_en + 1);
+    DevBuf da, db, dn, dno, dd;
+    GBN_CK(c, da.ensure(sizeof(double) * nab));
+    GBN_CK(c, db.ensure(sizeof(double) * nab));
+    GBN_CK(c, dd.ensure(sizeof(double) * nd));
+    GBN_CK(c, cudaMemcpyAsync(da.p, a, sizeof(double) * nab, cudaMemcpyHostToDevice, c->stream));
+    GBN_CK(c, cudaMemcpyAsync(db.p, b, sizeof(double) * nab, cudaMemcpyHostToDevice, c->stream));
+    if (nsteps) {
+        GBN_CK(c, dn.ensure(sizeof(int32_t) * nrhs));
+        GBN_CK(c, cudaMemcpyAsync(dn.p, nsteps, sizeof(int32_t) * nrhs, cudaMemcpyHostToDevice, c->stream));
+    }
+    if (norm) {
+        GBN_CK(c, dno.ensure(sizeof(double) * nrhs));
+        GBN_CK(c, cudaMemcpyAsync(dno.p, norm, sizeof(double) * nrhs, cudaMemcpyHostToDevice, c->stream));
+    }
+    int rc = cf_dos(c, nrhs, da.as<double>(), db.as<double>(), nsteps ? dn.as<int32_t>() : nullptr, nmax, eta, n_en, emin,
+                    emax, norm ? dno.as<double>() : nullptr, dd.as<double>());
+    if (rc) return rc;
+    GBN_CK(c, cudaMemcpyAsync(dos, dd.p, sizeof(double) * nd, cudaMemcpyDeviceToHost, c->stream));
+    GBN_CK(c, cudaStreamSynchronize(c->stream));
+    if (energy) {
+        const double de = (emax - emin) / n_en;
+        for (int k = 0; k <= n_en; ++k) energy[k] = emin + (double)k * de;
+    }
+    return GBN_OK;
+}
+
+int gbn_cheb_evolve(gbn_ctx* c, int32_t nrhs, const double* coef, int32_t npol, double ac, double bc, double* z)
+{
+    if (!c) return GBN_ERR_ARG;
+    if (!c->have_ham) return fail(c, GBN_ERR_STATE, "no Hamiltonian");
+    if (nrhs < 1 || npol < 1 || !coef || !z || !(bc > 0.0)) return fail(c, GBN_ERR_ARG, "bad Chebyshev arguments");
+    cudaSetDevice(c->device);
+    return cheb_evolve(c, nrhs, coef, npol, ac, bc, z);
+}
+
+int gbn_kubo_evol(gbn_ctx* c, int32_t nrhs, const double* coef, int32_t npol, double ac, double bc, int32_t dir,
+                  double* psi, double* zupsi)
+{
+    if (!c) return GBN_ERR_ARG;
+    if (!c->have_ham) return fail(c, GBN_ERR_STATE, "no Hamiltonian");
+    if (!c->have_neighd) return fail(c, GBN_ERR_STATE, "KuboEvol needs NeighD (gbn_neighbours or gbn_set_neighd)");
+    if (dir != 1 && dir != 2) return fail(c, GBN_ERR_ARG, "dir must be 1 (x) or 2 (y)");
+    if (nrhs < 1 || npol < 1 || !coef || !psi || !zupsi || !(bc > 0.0)) return fail(c, GBN_ERR_ARG, "bad KuboEvol arguments");
+    cudaSetDevice(c->device);
+    return kubo_evol(c, nrhs, coef, npol, ac, bc, dir, psi, zupsi);
+}
+
+}  // extern "C"

@@ -1,0 +1,156 @@
+// Internal declarations of libgrabnes_gpu: context, device buffers, error plumbing.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/grabnes_gpu.h"
+
+namespace gbn {
+
+// Device allocation that grows on demand and is freed with the context.
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    cudaError_t ensure(size_t need) {
+        if (need <= bytes && p) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+        cudaError_t e = cudaMalloc(&p, need ? need : 16);
+        if (e == cudaSuccess) bytes = need ? need : 16;
+        return e;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    template <typename T> T* as() const { return static_cast<T*>(p); }
+};
+
+// Sliced ELL matrix of the permuted Hamiltonian: slices of `sh` rows, entries of a slice stored
+// column by column (entry k of row r of slice s at slice_ptr[s] + k*sh + r).  Padding entries point
+// at their own row with a zero value, padded rows have no entries that matter.
+struct Ell {
+    int sh = 0;              // rows per slice (= rows a warp processes at once)
+    int prec = -1;           // GBN_FP64 / GBN_MIXED
+    bool cplx = false;       // complex values stored
+    int64_t nslices = 0;
+    int64_t npad = 0;        // nslices * sh
+    int64_t nnz_stored = 0;  // entries including padding
+    DevBuf slice_ptr;        // int64 [nslices + 1]
+    DevBuf col;              // int32 [nnz_stored]
+    DevBuf val;              // float | double | float2 | double2
+    DevBuf h0;               // float | double [npad]
+    bool valid = false;
+};
+
+struct Timing {
+    double step_ms = 0.0;
+    int64_t step_launches = 0;
+};
+
+}  // namespace gbn
+
+struct gbn_ctx {
+    int device = 0;
+    int num_sms = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    std::string err;
+    int64_t launches = 0;
+
+    // geometry (reference order)
+    int64_t n = 0;
+    double ucell[9] = {0};
+    gbn::DevBuf rat, species, layer;  // double[3n], int32[n], int32[n]
+    bool have_geometry = false;
+
+    // neighbour tables (reference layout)
+    int32_t max_neigh = 0;
+    int64_t total = 0;
+    gbn::DevBuf nneigh, nlist, neighd, ncell;
+    bool have_neigh = false;
+    bool have_neighd = false;
+
+    // Hamiltonian (reference layout, FP64)
+    gbn::DevBuf h0, hopp;  // double[n], double2[n*max_neigh]
+    gbn::DevBuf rat_hop;   // positions used for the Peierls phases
+    bool have_ham = false;
+    bool ham_complex = false;
+
+    // row permutation used by the solver: perm[new] = reference index, iperm[reference] = new
+    gbn::DevBuf perm, iperm;
+    bool perm_spatial = false;
+
+    gbn::Ell ell;
+
+    // recursion state
+    int prec = -1;
+    int nrhs = 0;
+    gbn::DevBuf vec[4];      // (v, x) pairs, ping-pong
+    gbn::DevBuf partials;    // double [blocks][R][4]
+    gbn::DevBuf scal;        // double [R][2]: a_{k-1}, b_{k-1}
+    gbn::DevBuf counter;     // uint32 block counter + int32 step index + int32 flag
+    gbn::DevBuf ab;          // double [2][R][nmax]
+    gbn::DevBuf upload;      // staging of host inputs
+    int32_t staged_nmax = 0;
+    bool staged = false;
+    gbn::Timing timing;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+
+    // Chebyshev work vectors
+    gbn::DevBuf cheb[8];
+};
+
+namespace gbn {
+
+int fail(gbn_ctx* c, int code, const std::string& msg);
+int cuda_fail(gbn_ctx* c, cudaError_t e, const char* what);
+
+#define GBN_CK(ctx, call)                                                   \
+    do {                                                                    \
+        cudaError_t e__ = (call);                                           \
+        if (e__ != cudaSuccess) return gbn::cuda_fail((ctx), e__, #call);  \
+    } while (0)
+
+#define GBN_CK_LAUNCH(ctx)                                                          \
+    do {                                                                            \
+        (ctx)->launches++;                                                          \
+        cudaError_t e__ = cudaGetLastError();                                       \
+        if (e__ != cudaSuccess) return gbn::cuda_fail((ctx), e__, "kernel launch"); \
+    } while (0)
+
+// layout / permutation (gbn_layout.cu)
+int build_identity_perm(gbn_ctx* c);
+int build_spatial_perm(gbn_ctx* c);
+int build_ell(gbn_ctx* c, int prec, int sh);
+
+// recursion (gbn_lanczos.cu)
+int lanczos_prepare(gbn_ctx* c, int prec, int nrhs);
+int lanczos_start_from_phases(gbn_ctx* c, const double* d_u, int nrhs_real);
+int lanczos_start_from_psi(gbn_ctx* c, const double* d_psi, int nrhs_real);
+int lanczos_run(gbn_ctx* c, int32_t nmax);
+int rows_per_slice(int prec, int nrhs);
+
+// continued fraction (gbn_cf.cu)
+int cf_dos(gbn_ctx* c, int32_t nrhs, const double* d_a, const double* d_b, const int32_t* d_nsteps, int32_t nmax,
+           double eta, int32_t n_en, double emin, double emax, const double* d_norm, double* d_dos);
+
+// neighbour search and assembly (gbn_neigh.cu, gbn_model.cu)
+int neigh_search(gbn_ctx* c, double cut2intra, double cut2inter, int32_t second_layer);
+int assemble(gbn_ctx* c, const gbn_model* m, const double* d_rat_on, const double* d_rat_hop, const double* d_uniform);
+int peierls(gbn_ctx* c, double flux);
+
+// Chebyshev (gbn_cheb.cu)
+int cheb_evolve(gbn_ctx* c, int32_t nrhs, const double* c_host, int32_t npol, double ac, double bc, double* z_host);
+int kubo_evol(gbn_ctx* c, int32_t nrhs, const double* c_host, int32_t npol, double ac, double bc, int32_t dir,
+              double* psi_host, double* zupsi_host);
+
+inline int grid_for(gbn_ctx* c, int blocks_per_sm) { return c->num_sms * blocks_per_sm; }
+
+}  // namespace gbn

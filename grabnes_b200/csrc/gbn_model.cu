@@ -1,0 +1,250 @@
+// Hamiltonian assembly on the device: on-site energies (HamOnSite), hoppings of the bond loop
+// (HamHopping) and Peierls phases (HamPeierlsPeriodicGauge) for the models on the recursion path:
+//   - carbon shells with gn(C,C,shell) and, for the Koshino/HTC bilayers, the single-layer F2G2
+//     shell terms (ham.F90:10177-10194, 10616-10931);
+//   - the effective moire model of Jung et al. (PRB 89, 205414): on-site H0/Hz harmonics
+//     (ham.F90:3437-3544, diago :4696-4716) and the bond term del(1..3) per atom (:12542-12680) or at
+//     the bond midpoint (:4822-4883, offdiago :4752-4776), with or without twist;
+//   - the two-centre interlayer hopping Vpp_pi/Vpp_sigma (ham.F90:9620-9838, :4094-4110);
+//   - Anderson disorder (ham.F90:1237-1248) from host-drawn uniform numbers.
+// One thread per atom, FP64; results are in the reference layout hopp(maxNeigh,N).
+#include <cuda_runtime.h>
+#include <math.h>
+
+#include "gbn_internal.cuh"
+
+namespace gbn {
+
+#define GBN_PI 3.14159265358979323846
+
+__device__ double d_diago(double dx, double dy, double C, double phi, double aG)
+{
+    const double G1 = 4.0 * GBN_PI / sqrt(3.0) / aG;
+    const double e1r = cos(G1 * dy), e1i = -sin(G1 * dy);
+    const double hh = G1 * dy / 2.0;
+    const double k = cos(sqrt(3.0) * G1 * dx / 2.0);
+    double sh, ch;
+    sincos(hh, &sh, &ch);
+    const double sr = e1r + 2.0 * ch * k, si = e1i + 2.0 * sh * k;
+    double sp, cp;
+    sincos(phi, &sp, &cp);
+    return 2.0 * C * (sr * cp - si * sp);
+}
+
+__device__ void d_offdiago(double dx, double dy, double C, double phi, double aG, double* re, double* im)
+{
+    const double G1 = 4.0 * GBN_PI / sqrt(3.0) / aG;
+    const double ax = sqrt(3.0) * G1 * dx / 2.0;
+    const double p = cos(G1 * dy / 2.0 - phi);
+    const double q = sin(G1 * dy / 2.0 - phi - GBN_PI / 6.0);
+    double sa, ca;
+    sincos(ax, &sa, &ca);
+    *re = 2.0 * C * ca * (p + q) + 2.0 * C * sin(G1 * dy + phi - GBN_PI / 6.0);
+    *im = 2.0 * C * sa * (p - q);
+}
+
+__device__ void d_bond_deltas(int spec, double re, double im, double del[3])
+{
+    del[0] = 2.0 * re / 3.0;
+    const double u = -(re + sqrt(3.0) * im) / 3.0, w = (-re + sqrt(3.0) * im) / 3.0;
+    if (spec == 1) { del[1] = u; del[2] = w; }
+    else { del[1] = w; del[2] = u; }
+}
+
+__device__ void d_moire_disp(const gbn_model& m, double x, double y, double* dx, double* dy)
+{
+    if (m.moire_twisted) {
+        double st, ct;
+        sincos(m.twist_rad, &st, &ct);
+        *dx = x * ((1.0 + m.eps) * ct - 1.0) - y * (1.0 + m.eps) * st;
+        *dy = y * ((1.0 + m.eps) * ct - 1.0) + x * (1.0 + m.eps) * st;
+    } else {
+        *dx = x * m.eps;
+        *dy = y * m.eps;
+    }
+}
+
+__global__ void k_onsite(gbn_model m, int64_t n, const double* rat, const int32_t* species, const int32_t* layer,
+                         const double* uniform, double* h0)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double h = m.e0_c;
+    if (m.moire_onsite != 0) {
+        double dx, dy;
+        d_moire_disp(m, rat[3 * i], rat[3 * i + 1], &dx, &dy);
+        dy = dy + m.shift1;
+        const int L = layer[i];
+        if ((L == 1 && m.sign1 < 0.0) || (L == 2 && m.sign2 < 0.0)) { dx = -dx; dy = -dy; }
+        double hz = 0.0, hd = 0.0;
+        if (m.moire_onsite == 2) hd = d_diago(dx, dy, m.C0, m.Phi0, m.aG);
+        else if (m.moire_onsite == 3) hz = d_diago(dx, dy, m.Cz, m.Phiz, m.aG);
+        else if (m.moire_onsite == 1) {
+            hz = d_diago(dx, dy, m.Cz, m.Phiz, m.aG);
+            hd = d_diago(dx, dy, m.C0, m.Phi0, m.aG);
+        }
+        const double sgn = (species[i] % 2 == 1) ? -1.0 : 1.0;
+        if (L == 1) h = h + (sgn * hz * m.sign1 + hd);
+        else if (L == 2) h = h + (sgn * hz * m.sign2 + hd);
+    }
+    if (m.anderson) h = h + (uniform[i] - 0.5) * m.anderson_w;
+    h0[i] = h;
+}
+
+__device__ double d_moire_mid_delta(const gbn_model& m, double rix, double riy, double bx, double by, int spec, bool flip)
+{
+    if (spec != 1 && spec != 2) return 0.0;
+    const double rm0 = rix + 0.5 * bx, rm1 = riy + 0.5 * by;
+    const double th = m.moire_twisted ? m.twist_rad : 0.0;
+    double st, ct;
+    sincos(th, &st, &ct);
+    double ddx = rm0 * ((1.0 + m.eps) * ct - 1.0) - rm1 * (1.0 + m.eps) * st;
+    double ddy = rm1 * ((1.0 + m.eps) * ct - 1.0) + rm0 * (1.0 + m.eps) * st;
+    ddy = ddy + m.shift1;
+    if (flip) { ddx = -ddx; ddy = -ddy; }
+    double re, im, del[3];
+    d_offdiago(ddx, ddy, m.Cab, m.Phiab, m.aG, &re, &im);
+    d_bond_deltas(spec, re, im, del);
+    if (fabs(bx) < m.aG / 4.0) return del[0];
+    if (bx < 0.0) return del[2];
+    return del[1];
+}
+
+__device__ double d_f2g2_shell(const gbn_model& m, double dist)
+{
+    const double aG = m.aG, aCC = m.aCC;
+    if (dist > aCC * 0.9 && dist < aCC * 1.1) return 0.0;
+    if (dist > aG * 0.9 && dist < aG * 1.1) return m.tksl[2];
+    if (dist > 2.0 * aCC * 0.9 && dist < aCC * 2.0 * 1.1) return m.tksl[3];
+    if (dist > 2.0 * aCC * 1.1 && dist < 4.0) return m.tksl[4];
+    if (dist > (aCC * 3.0) * 0.9 && dist < (aCC * 3.0) * 1.1) return m.tksl[5];
+    if (dist > 2.0 * aG * 0.97 && dist < 2.0 * aG * 1.03) return m.tksl[6];
+    const double r7 = sqrt((2.0 * aG) * (2.0 * aG) + aCC * aCC);
+    if (dist > r7 * 0.9 && dist < r7 * 1.1) return m.tksl[7];
+    return 0.0;
+}
+
+__global__ void k_hopping(gbn_model m, int64_t n, const double* rat, const int32_t* species, const int32_t* layer,
+                          int32_t max_neigh, const int32_t* nneigh, const int32_t* nlist, const double* neighd,
+                          double2* hopp)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double delta = 0.0;
+    double del[3] = {0.0, 0.0, 0.0};
+    const int Li = layer[i], si = species[i];
+    const bool flip = (Li == 1 && m.sign1 < 0.0) || (Li == 2 && m.sign2 < 0.0);
+    const double rix = rat[3 * i], riy = rat[3 * i + 1];
+    if (m.moire_offdiag) {
+        double dx, dy, re, im;
+        d_moire_disp(m, rix, riy, &dx, &dy);
+        dy = dy + m.shift1;
+        if (flip) { dx = -dx; dy = -dy; }
+        d_offdiago(dx, dy, m.Cab, m.Phiab, m.aG, &re, &im);
+        if (si == 1 || si == 2) d_bond_deltas(si, re, im, del);
+    }
+    const int k = nneigh[i];
+    for (int j = 0; j < max_neigh; ++j) {
+        const int64_t e = i * max_neigh + j;
+        double hr = 0.0;
+        if (j < k) {
+            const int64_t jj = nlist[e] - 1;
+            const double Dx = neighd[3 * e], Dy = neighd[3 * e + 1], Dz = neighd[3 * e + 2];
+            const int Lj = layer[jj];
+            if (Li == Lj) {
+                const double d = sqrt(Dx * Dx + Dy * Dy);
+                for (int lv = 0; lv < m.tbnn; ++lv) {
+                    if (d < m.nradii[lv]) {
+                        if (d < 1.7) {
+                            if (fabs(Dx) < m.aG / 4.0) delta = del[0];
+                            else if (Dx < -m.aG / 4.0) delta = del[2];
+                            else if (Dx > m.aG / 4.0) delta = del[1];
+                            if (m.moire_mid) delta = d_moire_mid_delta(m, rix, riy, Dx, Dy, si, flip);
+                        }
+                        if (m.intralayer == 1) hr = hr + d_f2g2_shell(m, d);
+                        if (d > 1.5) delta = 0.0;
+                        hr = hr + (m.gn_cc[lv] - delta);
+                        break;
+                    }
+                }
+            } else if (Li == Lj + 1 || Li == Lj - 1) {
+                if (m.interlayer == 1) {
+                    const double dist = sqrt(Dx * Dx + Dy * Dy + Dz * Dz);
+                    const double vsig = m.vppsigma0 * exp(-(dist - m.d_interlayer) / m.bl_delta);
+                    const double vpi = m.vpppi0 * exp(-(dist - m.aCC) / m.bl_delta);
+                    const double q = Dz / dist;
+                    hr = hr + (vpi * (1.0 - q * q) + vsig * (q * q));
+                } else {
+                    const double d = sqrt(Dx * Dx + Dy * Dy);
+                    hr = hr + m.g_intlay * exp(-d / m.d_interlayer);
+                }
+            }
+        }
+        hopp[e] = make_double2(hr, 0.0);
+    }
+}
+
+__global__ void k_peierls(int64_t n, const double* rat, double u0, double u1, double u3, double u4, int32_t max_neigh,
+                          const int32_t* nneigh, const int32_t* nlist, const int32_t* ncell, double flux, double mq,
+                          double2* hopp)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double rix = rat[3 * i], riy = rat[3 * i + 1];
+    for (int j = 0; j < nneigh[i]; ++j) {
+        const int64_t e = i * max_neigh + j;
+        const int64_t jj = nlist[e] - 1;
+        const double rjx = rat[3 * jj], rjy = rat[3 * jj + 1];
+        const int n1 = ncell[3 * e], n2 = ncell[3 * e + 1];
+        const double v1x = rix + rjx, v1y = riy + rjy;
+        const double v2x = (double)n1 * u0 + (double)n2 * u3, v2y = (double)n1 * u1 + (double)n2 * u4;
+        const double c3 = v1x * v2y - v1y * v2x;
+        const double r3 = rix * rjy - riy * rjx;
+        double ph = flux * (r3 + c3) / 1.0e20;
+        if (n1 != 0 && n2 != 0) ph = ph + GBN_PI * mq * (double)n1 * (double)n2;
+        double s, co;
+        sincos(ph, &s, &co);
+        const double2 h = hopp[e];
+        hopp[e] = make_double2(h.x * co - h.y * s, h.x * s + h.y * co);
+    }
+}
+
+int assemble(gbn_ctx* c, const gbn_model* m, const double* d_rat_on, const double* d_rat_hop, const double* d_uniform)
+{
+    const int64_t n = c->n;
+    GBN_CK(c, c->h0.ensure(sizeof(double) * n));
+    GBN_CK(c, c->hopp.ensure(sizeof(double2) * (size_t)n * c->max_neigh));
+    const unsigned grd = (unsigned)((n + 127) / 128);
+    k_onsite<<<grd, 128, 0, c->stream>>>(*m, n, d_rat_on, c->species.as<int32_t>(), c->layer.as<int32_t>(), d_uniform,
+                                         c->h0.as<double>());
+    GBN_CK_LAUNCH(c);
+    k_hopping<<<grd, 128, 0, c->stream>>>(*m, n, d_rat_hop, c->species.as<int32_t>(), c->layer.as<int32_t>(),
+                                          c->max_neigh, c->nneigh.as<int32_t>(), c->nlist.as<int32_t>(),
+                                          c->neighd.as<double>(), c->hopp.as<double2>());
+    GBN_CK_LAUNCH(c);
+    c->have_ham = true;
+    c->ham_complex = false;
+    c->ell.valid = false;
+    return GBN_OK;
+}
+
+int peierls(gbn_ctx* c, double flux)
+{
+    const double* u = c->ucell;
+    const double area = fabs(u[0] * u[4] - u[1] * u[3]);
+    const double fq = flux * area / (GBN_PI * 1.0e20);
+    const double mq = (double)llround(fq);
+    if (fabs(fq - mq) > 1.0e-6)
+        return fail(c, GBN_ERR_NUMERIC, "the number of flux quanta through the cell is not an integer");
+    const unsigned grd = (unsigned)((c->n + 127) / 128);
+    k_peierls<<<grd, 128, 0, c->stream>>>(c->n, c->rat_hop.as<double>(), u[0], u[1], u[3], u[4], c->max_neigh,
+                                          c->nneigh.as<int32_t>(), c->nlist.as<int32_t>(), c->ncell.as<int32_t>(), flux,
+                                          mq, c->hopp.as<double2>());
+    GBN_CK_LAUNCH(c);
+    GBN_CK(c, cudaStreamSynchronize(c->stream));
+    c->ham_complex = true;
+    c->ell.valid = false;
+    return GBN_OK;
+}
+
+}  // namespace gbn

@@ -1,0 +1,147 @@
+/*
+ * grabnes_gpu.h -- C ABI of the B200 (sm_100a) library for the large-cell
+ * recursion hot path of GRABNES: neighbour search, Hamiltonian assembly,
+ * Lanczos recursion, continued-fraction DOS and Chebyshev time evolution.
+ *
+ * Conventions of the reference solver (gjung-group/grabnes, Fortran) are kept
+ * at this boundary so that a Fortran host can bind every entry point with
+ * iso_c_binding and pass its module arrays unchanged:
+ *   - arrays are the Fortran arrays in memory order: Rat(3,N) -> rat[3*i+k],
+ *     NList(maxNeigh,N) -> nlist[maxNeigh*i+j] (1-based atom numbers),
+ *     NeighD(3,maxNeigh,N), neighCell(3,maxNeigh,N), hopp(maxNeigh,N) complex
+ *     (interleaved re, im), H0(N); energies in units of g0 (TB.Hopping);
+ *   - hopp stores MINUS the hopping: (H x)_i = H0_i x_i - sum_j hopp(j,i) x(NList(j,i)).
+ * Every function returns GBN_OK (0) or a negative GBN_ERR_* code; the text of
+ * the last error is gbn_last_error().  Nothing in the library aborts, traps or
+ * exits.  A context owns device memory and one CUDA stream; calls on one
+ * context must not overlap (one context per host thread).  Host buffers are
+ * owned by the caller; the library copies them in and writes results into
+ * caller buffers.
+ */
+#ifndef GRABNES_GPU_H
+#define GRABNES_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GBN_OK 0
+#define GBN_ERR_ARG (-1)     /* invalid argument (the message names it)            */
+#define GBN_ERR_CUDA (-2)    /* CUDA runtime error                                  */
+#define GBN_ERR_STATE (-3)   /* call out of order (e.g. no Hamiltonian loaded)      */
+#define GBN_ERR_NUMERIC (-4) /* non-finite or non-positive b_n, non-integer flux ... */
+#define GBN_ERR_ALLOC (-5)   /* device or host allocation failed                    */
+#define GBN_ERR_TIMEOUT (-6) /* a bounded device wait ran out                       */
+
+#define GBN_FP64 0  /* complex128 vectors and hoppings, FP64 everything              */
+#define GBN_MIXED 1 /* complex64 vectors, FP32 hoppings, FP64 a_n/b_n reductions      */
+
+typedef struct gbn_ctx gbn_ctx;
+
+/* Model of the hot path (units: g0 unless stated; see grabnes_b200/model.py for
+ * the mapping from Gendata.in keys).  Mirrors the variables the reference's
+ * HamOnSite / HamHopping read (lanczosKuboCode/Src/ham.F90:756-4016, 5373-12829). */
+typedef struct gbn_model {
+    double  aG;            /* Structure.LatticeParameter [Ang]                        */
+    int32_t tbnn;          /* TB.NeighLevels (1..8)                                   */
+    double  gn_cc[8];      /* gn(C,C,shell)/g0                                        */
+    double  nradii[8];     /* Nradii(shell,1) [Ang]                                   */
+    int32_t intralayer;    /* 0 HamHopIntralayerDefault, 1 F2G2 single layer          */
+    double  tksl[8];       /* F2G2 shell terms t2..t7 at index 2..7 (/g0)             */
+    int32_t moire_offdiag; /* Moire.OffDiag                                           */
+    int32_t moire_mid;     /* Moire.OffDiagMidpoint                                   */
+    int32_t moire_twisted; /* Moire.Twisted                                           */
+    int32_t moire_onsite;  /* 0 none, 1 H0AndHZ, 2 OnlyH0, 3 OnlyHZ, 4 NoH0AndHZ       */
+    double  eps, twist_rad, shift1, sign1, sign2;
+    double  C0, Cz, Cab, Phi0, Phiz, Phiab;
+    int32_t interlayer;    /* 0 gIntLay*exp(-d/dIntLay), 1 two-centre (Koshino/HTC)   */
+    double  vpppi0, vppsigma0, bl_delta, d_interlayer, aCC, g_intlay;
+    int32_t anderson;      /* Disorder.Anderson: add (u_i - 0.5) * anderson_w         */
+    double  anderson_w;
+    double  e0_c;          /* TB.OnSiteC/g0                                           */
+} gbn_model;
+
+/* ---- context ------------------------------------------------------------------------ */
+/* No counterpart in the reference (module state); device = CUDA ordinal. */
+int         gbn_create(gbn_ctx** out, int32_t device);
+int         gbn_destroy(gbn_ctx* ctx);
+const char* gbn_last_error(const gbn_ctx* ctx);
+const char* gbn_version(void);
+/* Use the caller's CUDA stream (a cudaStream_t) for all work of the context; NULL = own stream. */
+int         gbn_set_stream(gbn_ctx* ctx, void* cuda_stream);
+/* Kernels launched by this context since creation (for launch accounting). */
+int64_t     gbn_launch_count(const gbn_ctx* ctx);
+/* Device time of the recursion-step kernels of the last gbn_lanczos* call. */
+int         gbn_last_timing(const gbn_ctx* ctx, double* step_ms_total, int64_t* step_launches);
+
+/* ---- geometry and neighbour search ---------------------------------------------------- */
+/* Atoms of the cell: Rat(3,N) Cartesian [Ang], Species(N), layerIndex(N), ucell(3,3).
+ * Replaces the module arrays of lanczosKuboCode/Src/atoms.F90 and cell.F90 (AtomsPos, CellGet). */
+int gbn_set_geometry(gbn_ctx* ctx, int64_t n, const double* rat, const int32_t* species,
+                     const int32_t* layer, const double* ucell);
+/* NeighSearchLayered (lanczosKuboCode/Src/neigh.F90:117-316, periodicZ = .false.) on the device:
+ * same entries, same order within each atom, NeighD bit-identical. */
+int gbn_neighbours(gbn_ctx* ctx, double cut2intra, double cut2inter, int32_t second_layer,
+                   int32_t* max_neigh, int64_t* total);
+/* Copy Nneigh(N), NList(maxNeigh,N), NeighD(3,maxNeigh,N), neighCell(3,maxNeigh,N) out (any may be NULL). */
+int gbn_get_neighbours(gbn_ctx* ctx, int32_t* nneigh, int32_t* nlist, double* neighd, int32_t* neigh_cell);
+
+/* ---- Hamiltonian ----------------------------------------------------------------------- */
+/* HamOnSite + HamHopping bond loop (ham.F90:846-1248, 6517-6846) on the device.  rat_onsite and
+ * rat_hop are the positions HamOnSite and HamHopping see (they may differ in the last bit after
+ * the reference's fractional/Cartesian round trips); uniform holds the N Anderson draws (or NULL). */
+int gbn_assemble(gbn_ctx* ctx, const gbn_model* model, const double* rat_onsite,
+                 const double* rat_hop, const double* uniform);
+/* HamPeierlsPeriodicGauge (ham.F90:12834-12882): multiply the assembled hoppings by the phases of
+ * flux (= B pi / Phi0, in 1/Ang^2 * 1e20) including the corner term; positions from gbn_assemble. */
+int gbn_peierls(gbn_ctx* ctx, double flux);
+/* Copy H0(N) and hopp(maxNeigh,N) (complex) of the current Hamiltonian out (either may be NULL). */
+int gbn_get_hamiltonian(gbn_ctx* ctx, double* h0, double* hopp);
+/* Minimal drop-in for a Fortran host: the arrays KuboRecursion receives
+ * (lanczosKuboCode/Src/kubosubs.F90:26-43: H0, hopp, NList2 and the module's Nneigh, nAt). */
+int gbn_load_hamiltonian(gbn_ctx* ctx, int64_t n, int32_t max_neigh, const int32_t* nneigh,
+                         const int32_t* nlist, const double* hopp, const double* h0);
+
+/* ---- recursion ------------------------------------------------------------------------- */
+/* KuboRecursion (kubosubs.F90:26-138) for nrhs start vectors at once.  psi0: complex [nrhs][N]
+ * (reference atom order, normalised by the caller); nsteps[r] <= nmax recursion steps of vector r;
+ * a, b: [nrhs][nmax] (entries beyond nsteps[r] are left as computed for nmax).  precision:
+ * GBN_FP64 or GBN_MIXED.  Host buffers; copies in and out are part of the call. */
+int gbn_lanczos(gbn_ctx* ctx, int32_t precision, int32_t nrhs, const double* psi0,
+                const int32_t* nsteps, int32_t nmax, double* a, double* b);
+/* Same with random-phase start vectors built on the device from host uniform draws
+ * u[nrhs][N]: psi_i = exp(2 pi i u_i)/sqrt(N) (KuboInitWF, kubo.F90:61-64). */
+int gbn_lanczos_phases(gbn_ctx* ctx, int32_t precision, int32_t nrhs, const double* u,
+                       const int32_t* nsteps, int32_t nmax, double* a, double* b);
+/* Split form used for timing with device-resident inputs: gbn_stage_phases uploads and builds the
+ * start vectors; gbn_run_staged runs nmax steps and leaves a, b on the device unless a, b are
+ * non-NULL (then they are copied out). */
+int gbn_stage_phases(gbn_ctx* ctx, int32_t precision, int32_t nrhs, const double* u);
+int gbn_run_staged(gbn_ctx* ctx, int32_t nmax, double* a, double* b);
+
+/* ---- continued fraction ------------------------------------------------------------------ */
+/* KuboFrac (kubosubs.F90:222-288) for nrhs coefficient sets a, b [nrhs][nmax] of lengths
+ * nsteps[r]; energies E_k = emin + k (emax - emin)/n_en, k = 0..n_en; dos [nrhs][n_en+1] =
+ * -Im g(E + i eta)/pi * norm[r] (norm may be NULL: 1). energy [n_en+1] may be NULL. */
+int gbn_cf_dos(gbn_ctx* ctx, int32_t nrhs, const double* a, const double* b, const int32_t* nsteps,
+               int32_t nmax, double eta, int32_t n_en, double emin, double emax, const double* norm,
+               double* energy, double* dos);
+
+/* ---- Chebyshev time evolution --------------------------------------------------------------- */
+/* KuboChebyshevEvolve (kubosubs.F90:557-619): z <- sum_n c_n T_n((H-ac)/bc) z for nrhs complex
+ * vectors z [nrhs][N] (host, in place), c complex [npol]. */
+int gbn_cheb_evolve(gbn_ctx* ctx, int32_t nrhs, const double* c, int32_t npol, double ac, double bc,
+                    double* z);
+/* KuboEvol (kubosubs.F90:438-553): psi <- U psi and zupsi <- U zupsi + [U, X] psi, X along
+ * dir (1 = x, 2 = y) from NeighD; needs gbn_neighbours or NeighD through gbn_set_neighd. */
+int gbn_kubo_evol(gbn_ctx* ctx, int32_t nrhs, const double* c, int32_t npol, double ac, double bc,
+                  int32_t dir, double* psi, double* zupsi);
+/* NeighD(3,maxNeigh,N) for gbn_kubo_evol after gbn_load_hamiltonian. */
+int gbn_set_neighd(gbn_ctx* ctx, const double* neighd);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -144,8 +144,26 @@ def build(keys):
         bmag = mb * FLUXQ / (area * 1.0e-20)
         flux = bmag * math.pi / FLUXQ
         hop = orc.peierls(rat_hop, geo["ucell"], nb, flux, hop)
-    return dict(geo=geo, nb=nb, h0=h0, hop=hop, g0=g0, model=m, area=area, rat_hop=rat_hop,
-                cut2intra=cut2intra, cut2inter=cut2inter)
+    flux = 0.0
+    if mb != 0:
+        flux = mb * FLUXQ / (area * 1.0e-20) * math.pi / FLUXQ
+    return dict(geo=geo, nb=nb, h0=h0, hop=hop, g0=g0, model=m, area=area, rat_on=rat_on, rat_hop=rat_hop,
+                cut2intra=cut2intra, cut2inter=cut2inter, flux=flux, second_layer=g("AddSecondLayerInteractions", False))
+
+
+def gpu_model(m):
+    """The same model as the library's gbn_model structure."""
+    import grabnes_b200 as G
+    out = G.Model()
+    for name, _ in G.Model._fields_:
+        v = getattr(m, name)
+        if hasattr(v, "__len__"):
+            arr = getattr(out, name)
+            for i in range(len(arr)):
+                arr[i] = v[i]
+        else:
+            setattr(out, name, v)
+    return out
 
 
 # F2G2 single-layer graphene intralayer terms [eV] of HamHopF2G2sParameters (ham.F90:8253-8395)

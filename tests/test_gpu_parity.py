@@ -1,0 +1,170 @@
+"""Parity of the CUDA library (through its C ABI) with the oracle, on a B200.
+
+Bars (from the task's contract): neighbour and index arrays bit-exact; NeighD bitwise; FP64 Lanczos
+a_n, b_n within 1e-10 relative for the first 200 steps; hoppings and on-site energies to 1e-13 g0
+(the device's sin/cos/exp differ from glibc's in the last bit); continued fraction to 1e-12.
+"""
+import math
+
+import numpy as np
+import pytest
+
+import refcases as R
+from oracle import oracle as orc
+
+pytestmark = pytest.mark.gpu
+
+G = pytest.importorskip("grabnes_b200")
+
+MOIRE = dict(MoirePotential=True, MoireJeil=True, MoireH0AndHZ=True, MoireOffDiag=True, MoireOffDiagMidpoint=True)
+# Sizes are chosen so that 200 Lanczos steps stay below the onset of the recursion's sensitivity to
+# rounding: in small, highly symmetric cells the spectrum is degenerate and two FP64 runs that differ
+# only in summation order part ways after 120-150 steps (measured with the oracle, 1 vs 8 threads).
+CASES = {
+    # pristine graphene, nearest neighbours (config 1 model)
+    "graphene": dict(TypeOfSystem="Graphene", CellSize=100, Hopping=2.7, LatticeParameter=2.4595),
+    # graphene/hBN effective moire model with a field (config 3 model, example 06 at small size)
+    "moire_field": dict(TypeOfSystem="Graphene", CellSize=11, SuperCell=4, LatticePercent=-1.0 / 11.0,
+                        MagFieldInteger=2, **MOIRE),
+    # twisted moire model (example 07 model at small size)
+    "moire_twist": dict(TypeOfSystem="Graphene", CellSize=27, SuperCell=2, LatticePercent=-0.017989,
+                        MoireTwisted=True, MoireTwistAngle=1.872, **MOIRE),
+    # twisted bilayer, two-centre interlayer, 5 A in-plane interlayer radius (config 2 model)
+    "tbg": dict(TypeOfSystem="TwistedBilayerBasedOnMoireCell", MoireCellParameters=(31, 30, 30, 31), SuperCell=1,
+                TypeOfBL="Koshino", Hopping=2.7, LatticeParameter=2.4595, Vpppi0=2.7, Vppsigma0=0.48,
+                BLdelta=0.319, InterlayerDistance=3.35, LayerNeighbors=100, LayerDistFactor=3.2005),
+    # Anderson disorder (config 5 model) on graphene
+    "anderson": dict(TypeOfSystem="Graphene", CellSize=30, Anderson=True, AndersonAmp=1.0, SeedValue=5),
+}
+
+_built = {}
+
+
+def built(name):
+    if name not in _built:
+        _built[name] = R.build(CASES[name])
+    return _built[name]
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    with G.Context(0) as c:
+        yield c
+
+
+def gpu_pipeline(ctx, r):
+    geo = r["geo"]
+    ctx.set_geometry(geo["rat"], geo["species"], geo["layer"], geo["ucell"])
+    nb = ctx.neighbours(r["cut2intra"], r["cut2inter"], r["second_layer"])
+    m = r["model"]
+    uni = orc.rng_draws(m.seed, geo["n"]) if m.anderson else None
+    ctx.assemble(R.gpu_model(m), r["rat_on"], r["rat_hop"], uni)
+    if r["flux"] != 0.0:
+        ctx.peierls(r["flux"])
+    return nb
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_neighbour_tables_bit_exact(ctx, name):
+    r = built(name)
+    nb = gpu_pipeline(ctx, r)
+    ref = r["nb"]
+    assert nb["max_neigh"] == ref["max_neigh"]
+    assert np.array_equal(nb["nneigh"], ref["nneigh"])
+    assert np.array_equal(nb["nlist"], ref["nlist"])
+    assert np.array_equal(nb["ncell"], ref["ncell"])
+    assert np.array_equal(nb["neighd"].view(np.int64), ref["neighd"].view(np.int64))  # bitwise
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_hamiltonian_assembly(ctx, name):
+    r = built(name)
+    gpu_pipeline(ctx, r)
+    h0, hop = ctx.hamiltonian()
+    assert np.abs(h0 - r["h0"]).max() <= 1e-13
+    assert np.abs(hop - r["hop"]).max() <= 1e-13
+
+
+def _rel(x, y):
+    return np.abs(x - y).max() / np.abs(y).max()
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_lanczos_fp64_dropin(ctx, name):
+    """gbn_load_hamiltonian with the oracle's arrays (the Fortran-host drop-in), FP64 recursion."""
+    r = built(name)
+    n = r["geo"]["n"]
+    psi = orc.init_wf(n, 123456)
+    a0, b0 = orc.recursion(r["nb"], r["hop"], r["h0"], psi, 200, 0)
+    ctx.load_hamiltonian(r["nb"]["nneigh"], r["nb"]["nlist"], r["hop"], r["h0"])
+    a, b = ctx.lanczos(psi, 200, G.GBN_FP64)
+    assert _rel(a[0], a0) <= 1e-10 and _rel(b[0], b0) <= 1e-10
+
+
+@pytest.mark.parametrize("name", ["graphene", "tbg", "moire_field"])
+def test_lanczos_full_pipeline_phases(ctx, name):
+    """Search + assembly + Peierls + random-phase start vector, all on the device."""
+    r = built(name)
+    n = r["geo"]["n"]
+    psi = orc.init_wf(n, 123456)
+    a0, b0 = orc.recursion(r["nb"], r["hop"], r["h0"], psi, 200, 0)
+    gpu_pipeline(ctx, r)
+    u = orc.rng_draws(123456, n)
+    a, b = ctx.lanczos_phases(u, 200, G.GBN_FP64)
+    assert _rel(a[0], a0) <= 1e-10 and _rel(b[0], b0) <= 1e-10
+
+
+def test_lanczos_batched_matches_single(ctx):
+    r = built("tbg")
+    n = r["geo"]["n"]
+    ctx.load_hamiltonian(r["nb"]["nneigh"], r["nb"]["nlist"], r["hop"], r["h0"])
+    u = np.stack([orc.rng_draws(7 + k, n) for k in range(16)])
+    a16, b16 = ctx.lanczos_phases(u, 150, G.GBN_FP64)
+    for k in (0, 5, 15):
+        a1, b1 = ctx.lanczos_phases(u[k], 150, G.GBN_FP64)
+        assert _rel(a16[k], a1[0]) <= 1e-10 and _rel(b16[k], b1[0]) <= 1e-10
+
+
+def test_lanczos_uneven_lengths_and_odd_batch(ctx):
+    r = built("graphene")
+    n = r["geo"]["n"]
+    ctx.load_hamiltonian(r["nb"]["nneigh"], r["nb"]["nlist"], r["hop"], r["h0"])
+    u = np.stack([orc.rng_draws(11 + k, n) for k in range(5)])
+    steps = np.array([40, 120, 80, 200, 10], np.int32)
+    a, b = ctx.lanczos_phases(u, steps, G.GBN_FP64)
+    for k in range(5):
+        psi = orc.init_wf(n, 11 + k)
+        a0, b0 = orc.recursion(r["nb"], r["hop"], r["h0"], psi, int(steps[k]), 0)
+        assert _rel(a[k, :steps[k]], a0) <= 1e-10 and _rel(b[k, :steps[k]], b0) <= 1e-10
+
+
+def test_continued_fraction(ctx):
+    r = built("graphene")
+    n = r["geo"]["n"]
+    psi = orc.init_wf(n, 1)
+    a0, b0 = orc.recursion(r["nb"], r["hop"], r["h0"], psi, 300, 0)
+    g0 = r["g0"]
+    e_ref, d_ref = orc.frac(a0, b0, 0.01 / g0, 4000, -9.0 / g0, 9.0 / g0)
+    e, d = ctx.cf_dos(a0, b0, 0.01 / g0, 4000, -9.0 / g0, 9.0 / g0)
+    assert np.abs(e - e_ref).max() == 0.0
+    assert np.abs(d[0] - d_ref).max() <= 1e-12 * np.abs(d_ref).max()
+
+
+def test_mixed_precision_dos(ctx):
+    """Complex FP32 vectors and hoppings with FP64 a_n/b_n: broadened DOS against the FP64 oracle.
+
+    44 656-atom twisted bilayer, 300 steps, eta = 10 meV.  (In a cell ten times smaller the DOS after
+    300 steps resolves single levels and even two FP64 runs that differ only in summation order
+    disagree at 1e-3; at this size FP32 storage costs about 1e-8.)"""
+    r = R.build(dict(CASES["tbg"], SuperCell=2))
+    n = r["geo"]["n"]
+    psi = orc.init_wf(n, 3)
+    g0 = r["g0"]
+    a0, b0 = orc.recursion(r["nb"], r["hop"], r["h0"], psi, 300, 0)
+    e, d_ref = orc.frac(a0, b0, 0.01 / g0, 1000, -9.0 / g0, 9.0 / g0)
+    ctx.load_hamiltonian(r["nb"]["nneigh"], r["nb"]["nlist"], r["hop"], r["h0"])
+    a, b = ctx.lanczos(psi, 300, G.GBN_MIXED)
+    _, d = ctx.cf_dos(a, b, 0.01 / g0, 1000, -9.0 / g0, 9.0 / g0)
+    l1 = np.abs(d[0] - d_ref).sum() / np.abs(d_ref).sum()
+    print("mixed-precision DOS error (normalised L1):", l1)
+    assert l1 <= 1e-6, l1
