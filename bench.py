@@ -1,0 +1,357 @@
+#!/usr/bin/env python
+"""Throughput of the batched Lanczos-recursion DOS on a B200.
+
+Workload (one bench step = one complete recursion job): twisted-bilayer graphene at 1.08 degrees
+(commensurate moire cell 31 30 30 31, 11 164 atoms) tiled 20 x 20 = 4 465 600 atoms, rigid,
+intralayer nearest-neighbour t = -2.7 eV, two-centre interlayer hopping (Vpp_pi0 = 2.7, Vpp_sigma0 =
+0.48 eV, decay 0.319 Ang, d = 3.35 Ang) to 5 Ang in-plane; 16 random-phase vectors (GNU Fortran
+RNG, seed 7, vector r = draws r*N .. (r+1)*N-1); 2000 recursion steps each; complex FP32 vectors and
+hoppings with FP64 a_n/b_n ("mixed").  Synthetic input of the reference's own model (no dataset).
+
+Reported: value = atom-steps/s with the start vectors resident on the device (whole job, all
+ranks); e2e = the same through gbn_lanczos_phases with host buffers (H2D of the draws, D2H of a, b);
+roofline of the recursion-step kernel against measured HBM bandwidth; the plain FP64 paths (batched
+and single vector) and the DOS error of the mixed path against the FP64 path; the oracle port timed
+on the host cores as CPU baseline.  --impl reference times that CPU port alone (the reference is
+Fortran + MPI and cannot be built in this image).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = {
+    "Run.TypeOfSystem": "TwistedBilayerBasedOnMoireCell", "Structure.MoireCellParameters": (31, 30, 30, 31),
+    "Structure.SuperCell": 20, "Structure.LatticeParameter": 2.4595, "Structure.InterlayerDistance": 3.35,
+    "TB.Hopping": 2.7, "TB.NeighLevels": 1, "Interlayer.TypeOfBL": "Koshino", "Interlayer.Vpppi0": 2.7,
+    "Interlayer.Vppsigma0": 0.48, "Interlayer.BLdelta": 0.319, "Neigh.LayerNeighbors": 100,
+    "Neigh.LayerDistFactor": 3.2005,
+}
+NRHS, SEED, NSTEPS = 16, 7, 2000
+METRIC = "Lanczos atom-steps/s & HBM GB/s: batched FP32 vs plain FP64 at DOS err<1e-6"
+WORKLOAD_NAME = "tbg_1.08deg_20x20_4465600atoms_16vec_2000steps"
+ETA_EV, NE, EMIN_EV, EMAX_EV = 0.01, 4000, -9.0, 9.0
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi samples every 200 ms during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                       "-i", str(self.index), "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        rows = [l.split(",") for l in open(self.f.name).read().splitlines() if l.strip()]
+        os.unlink(self.f.name)
+        sm = [float(r[1]) for r in rows if len(r) >= 9 and r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if len(r) >= 9 and r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows if len(r) >= 9 for k in range(4) if r[5 + k].strip() == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def cpu_count():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def dist_init():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    return ws, rank, local
+
+
+def dist_max(x, ws):
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def traffic_from_profile():
+    """DRAM bytes per recursion-step launch from the committed ncu summary (scaled to this workload)."""
+    path = os.path.join(ROOT, "profiles", "lanczos_step_tbg.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["dram_bytes_per_launch_full_workload"])
+    except Exception:
+        return None
+
+
+# ------------------------------------------------------------------------------------------- ours
+def run_ours(args, ws, rank, local):
+    import torch
+
+    import grabnes_b200 as G
+    from grabnes_b200 import model as M
+
+    torch.cuda.set_device(local)
+    stream = torch.cuda.Stream()
+    ctx = G.Context(local)
+    ctx.set_stream(stream.cuda_stream)
+    job = M.job_from_keys(dict(WORKLOAD, **{"Structure.SuperCell": args.supercell}))
+    nsteps = args.nsteps
+    t0 = time.time()
+    cell = M.setup(ctx, job)
+    setup_s = time.time() - t0
+    n = cell["n"]
+    nnz = ctx.neighbours_total
+    g0 = job["g0"]
+    seed = SEED + 1000 * rank   # every rank runs its own replica of the workload (weak scaling)
+    u = G.rng_uniform(seed, NRHS * n).reshape(NRHS, n)
+
+    # ---- autotuning of the recursion kernels on this Hamiltonian, then device-resident inputs: the start
+    # vectors are staged once and every job rebuilds them on the device
+    from grabnes_b200.tune import autotune
+    if args.tuning:
+        rpt, bps, st = (int(x) for x in args.tuning.split(","))
+        ctx.set_tuning(rpt, bps, st)
+        best, tuning = dict(rhs_per_thread=rpt, blocks_per_sm=bps, staged=st, fixed=True), []
+    else:
+        best, tuning = autotune(ctx, u, G.GBN_MIXED)
+    ctx.stage_phases(u, G.GBN_MIXED)
+    for _ in range(args.warmup):
+        ctx.run_staged(nsteps)
+    torch.cuda.synchronize()
+    barrier(ws)
+    clocks = Clocks(int(os.environ.get("GBN_SMI_INDEX", local)))
+    clocks.start()
+    launches0 = ctx.launches
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    kern_ms = 0.0
+    kern_launches = 0
+    for _ in range(args.steps):
+        ctx.run_staged(nsteps)
+        ms, nl = ctx.last_timing()
+        kern_ms += ms
+        kern_launches += nl
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    launches = ctx.launches - launches0
+    barrier(ws)
+    clk = clocks.stop()
+    ms_total = dist_max(ev0.elapsed_time(ev1), ws)
+    atom_steps = float(n) * NRHS * nsteps
+    value = ws * atom_steps * args.steps / (ms_total / 1e3)
+    spmm_ms, update_ms = ctx.kernel_timing()
+    if args.value_only:   # short runs for profiling: the timed loop only
+        if rank == 0:
+            print(json.dumps({"value": value, "unit": "atom-steps/s", "step_ms": kern_ms / kern_launches,
+                              "spmm_ms": spmm_ms, "update_ms": update_ms, "atoms": n, "entries": nnz,
+                              "tuning": best, "candidates": tuning}), flush=True)
+        ctx.close()
+        return
+
+    # ---- roofline of the sparse-product kernel (the dominant one): algorithmic bytes of one recursion
+    # step = matrix (int32 column + FP32 hopping per entry) + on-site FP32 + 3 vector streams
+    b_alg = nnz * (4 + 4) + n * 4 + NRHS * n * 3 * 8
+    avg_launch_s = spmm_ms / 1e3
+    achieved = b_alg / avg_launch_s / 1e9
+    peak, peak_kind = peaks()
+    traffic = traffic_from_profile()
+
+    # ---- end to end through the C ABI with host buffers (pinned)
+    u_pin = torch.from_numpy(u.copy()).pin_memory()
+    u_np = u_pin.numpy()
+    e2e_ms = []
+    for it in range(max(1, min(args.steps, 2)) + 1):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        a_mix, b_mix = ctx.lanczos_phases(u_np, nsteps, G.GBN_MIXED)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if it > 0:   # the first call also rebuilds the device layout
+            e2e_ms.append(e0.elapsed_time(e1))
+    e2e_ms = dist_max(statistics.median(e2e_ms), ws)
+    e2e_value = ws * atom_steps / (e2e_ms / 1e3)
+
+    # ---- plain FP64 paths and the DOS error of the mixed path
+    torch.cuda.synchronize()
+    f0 = time.perf_counter()
+    a64, b64 = ctx.lanczos_phases(u_np, nsteps, G.GBN_FP64)
+    fp64_batched_s = time.perf_counter() - f0
+    fp64_batched_kernel_ms, nl64 = ctx.last_timing()
+    f0 = time.perf_counter()
+    ctx.lanczos_phases(u_np[:1], nsteps, G.GBN_FP64)
+    fp64_single_s = time.perf_counter() - f0
+    fp64_single_kernel_ms, _ = ctx.last_timing()
+    e, d_mix = ctx.cf_dos(a_mix, b_mix, ETA_EV / g0, NE, EMIN_EV / g0, EMAX_EV / g0)
+    _, d_64 = ctx.cf_dos(a64, b64, ETA_EV / g0, NE, EMIN_EV / g0, EMAX_EV / g0)
+    dm, d6 = d_mix.mean(axis=0), d_64.mean(axis=0)
+    dos_err = float(np.abs(dm - d6).sum() / np.abs(d6).sum())
+    dos_err_per_vector = float(max(np.abs(d_mix[r] - d_64[r]).sum() / np.abs(d_64[r]).sum() for r in range(NRHS)))
+
+    # ---- CPU baseline: the oracle's OpenMP port of KuboRecursion on the host cores (rank 0, N=1)
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        cpu = cpu_baseline(ctx, n, u[0], args.cpu_steps)
+
+    out = {
+        "metric": METRIC, "value": value, "unit": "atom-steps/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_total / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "c64 vectors/f32 hoppings, f64 a_n b_n", "data": "synthetic (reference model)",
+        "config": {"workload": WORKLOAD_NAME, "atoms": n, "entries": nnz, "vectors": NRHS, "recursion_steps": nsteps,
+                   "precision": "mixed", "parallelism": f"replicas x{ws}",
+                   "l2_policy": "inputs larger than L2 (vectors 572 MB, matrix 1.2 GB per step)"},
+        "e2e": {"value": e2e_value, "unit": "atom-steps/s", "h2d_bytes_per_step": int(u.nbytes),
+                "d2h_bytes_per_step": int(a_mix.nbytes + b_mix.nbytes)},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_source": peak_kind, "traffic": traffic, "algorithmic_bytes_per_launch": b_alg,
+                     "kernel": "k_spmm_step<float,real>", "avg_launch_ms": spmm_ms,
+                     "update_kernel_ms": update_ms, "step_ms": kern_ms / kern_launches},
+        "tuning": best,
+        "fp64": {"batched_atom_steps_per_s": atom_steps / (fp64_batched_kernel_ms / 1e3),
+                 "single_vector_atom_steps_per_s": float(n) * nsteps / (fp64_single_kernel_ms / 1e3),
+                 "batched_wall_s": fp64_batched_s, "single_wall_s": fp64_single_s},
+        "dos_error_vs_fp64": {"l1_mean_dos": dos_err, "l1_worst_vector": dos_err_per_vector,
+                              "eta_ev": ETA_EV, "energies": NE + 1},
+        "cpu_baseline": cpu, "clocks": clk, "gpu_launches": launches, "setup_s": setup_s,
+    }
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    ctx.close()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def cpu_baseline(ctx, n, u0, steps):
+    """The oracle port of KuboRecursion (reference data layout, complex128, three passes per step)."""
+    from oracle import oracle as orc
+    tabs = ctx.tables()
+    h0, hop = ctx.hamiltonian()
+    psi = np.exp(2j * np.pi * u0) / np.sqrt(n)
+    cores = cpu_count()
+    orc.recursion(tabs, hop, h0, psi, 1, cores)   # first touch
+    t0 = time.perf_counter()
+    orc.recursion(tabs, hop, h0, psi, steps, cores)
+    dt = time.perf_counter() - t0
+    return {"value": n * steps / dt, "unit": "atom-steps/s", "cores": cores, "kind": "port",
+            "sample": f"1 vector x {steps} recursion steps on the full {n}-atom Hamiltonian (complex128, "
+                      f"reference layout), {dt:.2f} s"}
+
+
+# ------------------------------------------------------------------------------------- reference
+def run_reference(args, ws, rank):
+    """The reference's CPU algorithm (oracle port: Fortran + MPI are not available) on the host cores."""
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from oracle import oracle as orc
+    import refcases as R
+    cores = cpu_count()
+    keys = {k.split(".")[-1]: v for k, v in WORKLOAD.items()}
+    keys["Hopping"] = WORKLOAD["TB.Hopping"]
+    keys["NeighLevels"] = 1
+    t0 = time.time()
+    r = R.build(keys)
+    setup_s = time.time() - t0
+    n = r["geo"]["n"]
+    psi = orc.init_wf(n, SEED)
+    steps = args.cpu_steps
+    for _ in range(args.warmup):
+        orc.recursion(r["nb"], r["hop"], r["h0"], psi, steps, cores)
+    ts = []
+    for _ in range(args.steps):
+        t = time.perf_counter()
+        orc.recursion(r["nb"], r["hop"], r["h0"], psi, steps, cores)
+        ts.append(time.perf_counter() - t)
+    per = statistics.median(ts)
+    value = n * steps / per
+    out = {"metric": METRIC, "value": value, "unit": "atom-steps/s", "n_gpus": ws, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": per * 1e3, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "c128", "data": "synthetic (reference model)", "impl": "reference",
+           "config": {"workload": WORKLOAD_NAME, "atoms": n, "sample_steps": steps, "vectors": 1},
+           "cpu_baseline": {"value": value, "unit": "atom-steps/s", "cores": cores, "kind": "port",
+                            "sample": f"1 vector x {steps} steps per bench step (setup {setup_s:.0f} s untimed)"},
+           "e2e": {"value": value, "unit": "atom-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--cpu-steps", type=int, default=300, help="recursion steps of the CPU sample")
+    p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--supercell", type=int, default=20, help="moire cells per side (20 = the workload)")
+    p.add_argument("--nsteps", type=int, default=NSTEPS, help="recursion steps per job (2000 = the workload)")
+    p.add_argument("--value-only", action="store_true", help="time the device-resident jobs only (profiling)")
+    p.add_argument("--tuning", default="", help="fixed kernel tuning 'rhs_per_thread,blocks_per_sm,staged' "
+                                                "instead of the autotuner")
+    args = p.parse_args()
+    ws, rank, local = dist_init() if args.impl == "ours" else (int(os.environ.get("WORLD_SIZE", "1")),
+                                                                 int(os.environ.get("RANK", "0")), 0)
+    if args.impl == "reference":
+        run_reference(args, ws, rank)
+    else:
+        run_ours(args, ws, rank, local)
+
+
+if __name__ == "__main__":
+    main()

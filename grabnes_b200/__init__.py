@@ -39,6 +39,14 @@ class Model(C.Structure):
     ]
 
 
+class Cell(C.Structure):
+    """gbn_cell of include/grabnes_gpu.h"""
+    _fields_ = [("kind", C.c_int32), ("cell_size", C.c_int32), ("super_cell", C.c_int32), ("m", C.c_int32 * 4),
+                ("aG", C.c_double), ("height", C.c_double), ("d_interlayer", C.c_double)]
+
+
+CELL_GRAPHENE, CELL_TBG_MOIRE = 0, 1
+
 _lib = None
 
 
@@ -68,23 +76,30 @@ def _opt(dtype):
     return Opt
 
 
-EXPORTS = ["gbn_create", "gbn_destroy", "gbn_last_error", "gbn_version", "gbn_set_stream", "gbn_launch_count",
-           "gbn_last_timing", "gbn_set_geometry", "gbn_neighbours", "gbn_get_neighbours", "gbn_assemble",
+EXPORTS = ["gbn_cell_atoms", "gbn_build_cell", "gbn_cart_roundtrip", "gbn_rng_uniform", "gbn_create", "gbn_destroy", "gbn_last_error", "gbn_version", "gbn_set_stream", "gbn_set_tuning", "gbn_launch_count",
+           "gbn_last_timing", "gbn_last_kernel_timing", "gbn_set_geometry", "gbn_neighbours", "gbn_get_neighbours", "gbn_assemble",
            "gbn_peierls", "gbn_get_hamiltonian", "gbn_load_hamiltonian", "gbn_lanczos", "gbn_lanczos_phases",
            "gbn_stage_phases", "gbn_run_staged", "gbn_cf_dos", "gbn_cheb_evolve", "gbn_kubo_evol", "gbn_set_neighd"]
 
 
 def _declare(L):
     d, i32, i64, vp = C.c_double, C.c_int32, C.c_int64, C.c_void_p
+    L.gbn_cell_atoms.argtypes = [C.POINTER(Cell), C.POINTER(i64)]
+    L.gbn_build_cell.argtypes = [C.POINTER(Cell), _p(np.float64), _p(np.float64), _p(np.int32), _p(np.int32),
+                                 C.POINTER(d)]
+    L.gbn_cart_roundtrip.argtypes = [i64, _p(np.float64), _p(np.float64)]
+    L.gbn_rng_uniform.argtypes = [i32, i64, _p(np.float64)]
     L.gbn_create.argtypes = [C.POINTER(vp), i32]
     L.gbn_destroy.argtypes = [vp]
     L.gbn_last_error.argtypes = [vp]
     L.gbn_last_error.restype = C.c_char_p
     L.gbn_version.restype = C.c_char_p
     L.gbn_set_stream.argtypes = [vp, vp]
+    L.gbn_set_tuning.argtypes = [vp, i32, i32, i32]
     L.gbn_launch_count.argtypes = [vp]
     L.gbn_launch_count.restype = i64
     L.gbn_last_timing.argtypes = [vp, C.POINTER(d), C.POINTER(i64)]
+    L.gbn_last_kernel_timing.argtypes = [vp, C.POINTER(d), C.POINTER(d)]
     L.gbn_set_geometry.argtypes = [vp, i64, _p(np.float64), _p(np.int32), _p(np.int32), _p(np.float64)]
     L.gbn_neighbours.argtypes = [vp, d, d, i32, C.POINTER(i32), C.POINTER(i64)]
     L.gbn_get_neighbours.argtypes = [vp, _opt(np.int32), _opt(np.int32), _opt(np.float64), _opt(np.int32)]
@@ -141,6 +156,9 @@ class Context:
     def set_stream(self, stream_handle):
         self._ck(self._L.gbn_set_stream(self._h, C.c_void_p(stream_handle)))
 
+    def set_tuning(self, rhs_per_thread=0, blocks_per_sm=0, staged=-1):
+        self._ck(self._L.gbn_set_tuning(self._h, rhs_per_thread, blocks_per_sm, staged))
+
     @property
     def launches(self):
         return self._L.gbn_launch_count(self._h)
@@ -149,6 +167,12 @@ class Context:
         ms, n = C.c_double(), C.c_int64()
         self._ck(self._L.gbn_last_timing(self._h, C.byref(ms), C.byref(n)))
         return ms.value, n.value
+
+    def kernel_timing(self):
+        """(sparse-product ms, update ms) per launch, averaged over the first steps of the last call."""
+        a, b = C.c_double(), C.c_double()
+        self._ck(self._L.gbn_last_kernel_timing(self._h, C.byref(a), C.byref(b)))
+        return a.value, b.value
 
     # ---------------------------------------------------------------- geometry / search
     def set_geometry(self, rat, species, layer, ucell):
@@ -161,6 +185,7 @@ class Context:
         mx, tot = C.c_int32(), C.c_int64()
         self._ck(self._L.gbn_neighbours(self._h, cut2intra, cut2inter, int(second_layer), C.byref(mx), C.byref(tot)))
         self.max_neigh = mx.value
+        self.neighbours_total = tot.value
         if not tables:
             return dict(max_neigh=mx.value, total=tot.value)
         n = self.n
@@ -171,6 +196,13 @@ class Context:
         self._ck(self._L.gbn_get_neighbours(self._h, nn, nl, nd, nc))
         return dict(max_neigh=mx.value, total=tot.value, nneigh=nn, nlist=nl.reshape(n, -1),
                     neighd=nd.reshape(n, -1, 3), ncell=nc.reshape(n, -1, 3))
+
+    def tables(self):
+        """Nneigh(N) and NList(maxNeigh,N) of the current neighbour list (reference layout)."""
+        nn = np.zeros(self.n, np.int32)
+        nl = np.zeros(self.n * self.max_neigh, np.int32)
+        self._ck(self._L.gbn_get_neighbours(self._h, nn, nl, None, None))
+        return dict(max_neigh=self.max_neigh, nneigh=nn, nlist=nl.reshape(self.n, -1))
 
     # ---------------------------------------------------------------- Hamiltonian
     def assemble(self, model, rat_onsite=None, rat_hop=None, uniform=None):
@@ -257,6 +289,42 @@ class Context:
         self._ck(self._L.gbn_kubo_evol(self._h, p.shape[0], cc, len(cc), ac, bc, direction, p.reshape(-1),
                                        z.reshape(-1)))
         return p, z
+
+
+def build_cell(kind, aG=2.46, cell_size=50, super_cell=1, m=(0, 0, 0, 0), height=40.0, d_interlayer=3.35):
+    """Atoms of a Graphene or TwistedBilayerBasedOnMoireCell cell, in the reference's order."""
+    p = Cell(kind, cell_size, super_cell, (C.c_int32 * 4)(*m), aG, height, d_interlayer)
+    n = C.c_int64()
+    rc = lib().gbn_cell_atoms(C.byref(p), C.byref(n))
+    if rc:
+        raise GbnError(rc, "invalid cell")
+    n = n.value
+    ucell = np.zeros(9)
+    rat = np.zeros(3 * n)
+    species = np.zeros(n, np.int32)
+    layer = np.zeros(n, np.int32)
+    tw = C.c_double()
+    rc = lib().gbn_build_cell(C.byref(p), ucell, rat, species, layer, C.byref(tw))
+    if rc:
+        raise GbnError(rc, "invalid cell")
+    return dict(n=n, ucell=ucell, rat=rat.reshape(n, 3), species=species, layer=layer, twist=tw.value)
+
+
+def cart_roundtrip(rat, ucell):
+    r = np.ascontiguousarray(rat, np.float64).reshape(-1).copy()
+    rc = lib().gbn_cart_roundtrip(len(r) // 3, np.ascontiguousarray(ucell, np.float64), r)
+    if rc:
+        raise GbnError(rc, "bad arguments")
+    return r.reshape(-1, 3)
+
+
+def rng_uniform(seed, n):
+    """GNU Fortran random_number draws after random_seed(PUT=[seed]*8)."""
+    out = np.zeros(n)
+    rc = lib().gbn_rng_uniform(seed, n, out)
+    if rc:
+        raise GbnError(rc, "bad arguments")
+    return out
 
 
 def version():

@@ -43,8 +43,9 @@ static int run_tiled(gbn_ctx* c, int prec, int nrhs, const double* host_in, bool
     if (rc) return rc;
     const size_t per = (size_t)c->n * (phases ? 1 : 2);
     GBN_CK(c, c->upload.ensure(sizeof(double) * per * T));
-    double step_ms = 0.0;
+    double step_ms = 0.0, spmm_sum = 0.0, upd_sum = 0.0;
     int64_t launches = 0;
+    int tiles = 0;
     std::vector<double> hab;
     for (int r0 = 0; r0 < nrhs; r0 += T) {
         const int cnt = std::min(T, nrhs - r0);
@@ -59,6 +60,9 @@ static int run_tiled(gbn_ctx* c, int prec, int nrhs, const double* host_in, bool
         if (rc) return rc;
         step_ms += c->timing.step_ms;
         launches += c->timing.step_launches;
+        spmm_sum += c->timing.spmm_ms_avg;
+        upd_sum += c->timing.update_ms_avg;
+        ++tiles;
         hab.resize((size_t)2 * T * nt);
         GBN_CK(c, cudaMemcpyAsync(hab.data(), c->ab.p, sizeof(double) * hab.size(), cudaMemcpyDeviceToHost, c->stream));
         GBN_CK(c, cudaStreamSynchronize(c->stream));
@@ -69,6 +73,8 @@ static int run_tiled(gbn_ctx* c, int prec, int nrhs, const double* host_in, bool
     }
     c->timing.step_ms = step_ms;
     c->timing.step_launches = launches;
+    c->timing.spmm_ms_avg = tiles ? spmm_sum / tiles : 0.0;
+    c->timing.update_ms_avg = tiles ? upd_sum / tiles : 0.0;
     return GBN_OK;
 }
 
@@ -135,6 +141,8 @@ int gbn_destroy(gbn_ctx* c)
     for (auto& v : c->cheb) v.release();
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
+    for (auto& e : c->kev)
+        if (e) cudaEventDestroy(e);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return GBN_OK;
@@ -165,6 +173,26 @@ int gbn_last_timing(const gbn_ctx* c, double* ms, int64_t* launches)
     if (!c) return GBN_ERR_ARG;
     if (ms) *ms = c->timing.step_ms;
     if (launches) *launches = c->timing.step_launches;
+    return GBN_OK;
+}
+
+int gbn_set_tuning(gbn_ctx* c, int32_t rhs_per_thread, int32_t blocks_per_sm, int32_t staged)
+{
+    if (!c) return GBN_ERR_ARG;
+    if (rhs_per_thread < 0 || rhs_per_thread > 4 || blocks_per_sm < 0 || blocks_per_sm > 32 || staged < -1 || staged > 1)
+        return fail(c, GBN_ERR_ARG, "tuning values out of range");
+    c->tune_rpt = rhs_per_thread;
+    c->tune_blocks_per_sm = blocks_per_sm;
+    c->tune_staged = staged;
+    c->ell.valid = false;
+    return GBN_OK;
+}
+
+int gbn_last_kernel_timing(const gbn_ctx* c, double* spmm_ms, double* update_ms)
+{
+    if (!c) return GBN_ERR_ARG;
+    if (spmm_ms) *spmm_ms = c->timing.spmm_ms_avg;
+    if (update_ms) *update_ms = c->timing.update_ms_avg;
     return GBN_OK;
 }
 

@@ -46,13 +46,22 @@ struct Ell {
     DevBuf col;              // int32 [nnz_stored]
     DevBuf val;              // float | double | float2 | double2
     DevBuf h0;               // float | double [npad]
+    int64_t max_chunk_entries = 0;  // largest chunk of kChunkSlices consecutive slices
+    int val_size = 0;               // bytes per stored value
     bool valid = false;
 };
 
+// slices per chunk of the staged sparse-product kernel (one slice per warp of a 256-thread block)
+constexpr int kChunkSlices = 8;
+
 struct Timing {
-    double step_ms = 0.0;
-    int64_t step_launches = 0;
+    double step_ms = 0.0;        // whole recursion loop of the last call
+    int64_t step_launches = 0;   // recursion steps of the last call
+    double update_ms_avg = 0.0;  // per-launch duration of the update kernel (first steps)
+    double spmm_ms_avg = 0.0;    // per-launch duration of the sparse-product kernel (first steps)
 };
+
+constexpr int kTimedSteps = 64;
 
 }  // namespace gbn
 
@@ -92,7 +101,7 @@ struct gbn_ctx {
     // recursion state
     int prec = -1;
     int nrhs = 0;
-    gbn::DevBuf vec[4];      // (v, x) pairs, ping-pong
+    gbn::DevBuf vec[4];      // v, x_prev, x_cur (ping-pong of the x pair)
     gbn::DevBuf partials;    // double [blocks][R][4]
     gbn::DevBuf scal;        // double [R][2]: a_{k-1}, b_{k-1}
     gbn::DevBuf counter;     // uint32 block counter + int32 step index + int32 flag
@@ -102,6 +111,13 @@ struct gbn_ctx {
     bool staged = false;
     gbn::Timing timing;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t kev[3 * gbn::kTimedSteps] = {};
+
+    // tuning of the recursion kernels (0 = automatic)
+    int tune_rpt = 0;            // right-hand sides per thread
+    int tune_blocks_per_sm = 0;  // cap on resident blocks per SM
+    int tune_staged = -1;        // sparse product with the matrix staged in shared memory (-1 auto, 0 no, 1 yes)
+    bool last_staged = false;    // the last recursion used the staged kernel
 
     // Chebyshev work vectors
     gbn::DevBuf cheb[8];
@@ -135,7 +151,7 @@ int lanczos_prepare(gbn_ctx* c, int prec, int nrhs);
 int lanczos_start_from_phases(gbn_ctx* c, const double* d_u, int nrhs_real);
 int lanczos_start_from_psi(gbn_ctx* c, const double* d_psi, int nrhs_real);
 int lanczos_run(gbn_ctx* c, int32_t nmax);
-int rows_per_slice(int prec, int nrhs);
+int rows_per_slice(int prec, int nrhs, int want_rpt);
 
 // continued fraction (gbn_cf.cu)
 int cf_dos(gbn_ctx* c, int32_t nrhs, const double* d_a, const double* d_b, const int32_t* d_nsteps, int32_t nmax,

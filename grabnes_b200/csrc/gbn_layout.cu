@@ -12,6 +12,9 @@
 #include <thrust/sequence.h>
 #include <thrust/sort.h>
 
+#include <algorithm>
+#include <vector>
+
 #include "gbn_internal.cuh"
 
 namespace gbn {
@@ -101,6 +104,8 @@ int build_spatial_perm(gbn_ctx* c)
     return GBN_OK;
 }
 
+// entries of every slice: sh rows times the longest row, the width rounded up so that a slice holds a
+// multiple of 4 entries (every slice then starts on a 16-byte boundary for the bulk copies)
 __global__ void k_slice_width(const int32_t* nneigh, const int32_t* perm, int64_t n, int sh, int64_t nslices,
                               int64_t* width_x_sh)
 {
@@ -114,6 +119,8 @@ __global__ void k_slice_width(const int32_t* nneigh, const int32_t* perm, int64_
             w = k > w ? k : w;
         }
     }
+    const int unit = sh >= 4 ? 1 : 4 / sh;
+    w = (w + unit - 1) / unit * unit;
     width_x_sh[s] = (int64_t)w * sh;
 }
 
@@ -215,7 +222,16 @@ int build_ell(gbn_ctx* c, int prec, int sh)
                                                                    E.h0.as<double>());
     }
     GBN_CK_LAUNCH(c);
+    // largest chunk of kChunkSlices consecutive slices (the unit the staged kernel copies to shared memory)
+    std::vector<int64_t> hsp((size_t)E.nslices + 1);
+    GBN_CK(c, cudaMemcpyAsync(hsp.data(), sp, sizeof(int64_t) * hsp.size(), cudaMemcpyDeviceToHost, c->stream));
     GBN_CK(c, cudaStreamSynchronize(c->stream));
+    E.max_chunk_entries = 0;
+    for (int64_t a = 0; a < E.nslices; a += kChunkSlices) {
+        const int64_t b = a + kChunkSlices < E.nslices ? a + kChunkSlices : E.nslices;
+        E.max_chunk_entries = std::max(E.max_chunk_entries, hsp[b] - hsp[a]);
+    }
+    E.val_size = (int)vsz;
     E.valid = true;
     return GBN_OK;
 }

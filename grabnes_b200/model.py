@@ -1,0 +1,178 @@
+"""Gendata.in keys -> inputs of the C ABI (cell, search radii, gbn_model, fields, Kubo parameters).
+
+Defaults and unit conversions follow the readers of the reference (gjung-group/grabnes):
+  cell / atoms      lanczosKuboCode/Src/cell.F90:16-140, 207-240; atoms.F90:124-230, 330-380
+  TB parameters     tbpar.f90:20-130 (g0 = TB.Hopping, default -3.72 aG + 12.14 eV)
+  search radii      ham.F90:542-606 (NeighShellCutoff2, Neigh.LayerDistFactor), neigh.F90:27-31, 348-381
+  hopping keys      ham.F90:5720-5941 (Moire.PotCab, Interlayer.Vpppi0/Vppsigma0/BLdelta, ...)
+  on-site keys      ham.F90:2099-2140, 2646-2690 (Moire.*), 1237-1248 and 13260-13283 (Anderson, eV)
+  fields            magf.F90:20-146 (B = m Phi0 / A), ham.F90:5657 (flux = B pi / Phi0)
+  Kubo              calc.F90:161-188 (energies and broadening in eV, divided by g0)
+Keys are given here in their short (former) form without section, matching case-insensitively
+with '_' and '-' ignored, as the reference's input library does.
+"""
+
+import math
+
+from . import CELL_GRAPHENE, CELL_TBG_MOIRE, Model
+
+SHELL_RADIUS = [1.0, 1.7320508075688772, 2.0, 2.6457513110645906, 3.0,
+                3.4641016151377544, 3.6055512754639891, 4.0, 4.3588989435406740]
+FLUXQ = 6.62606896e-34 / 1.602176565e-19   # h/e of constants.f90
+F2G2_SINGLE_LAYER = {2: -0.2354, 3: 0.1877, 4: 0.0, 5: -0.0633, 6: 0.0, 7: 0.0}   # ham.F90:8331-8350 [eV]
+
+
+# former (section-less) names of the keys read here: lanczosKuboCode/Src/MIO/input_aliases.inc
+FORMER = {
+    "Run.TypeOfSystem": "TypeOfSystem", "Structure.LatticeParameter": "LatticeParameter",
+    "Structure.CellSize": "CellSize", "Structure.SuperCell": "SuperCell",
+    "Structure.MoireCellParameters": "MoireCellParameters", "Structure.CellHeight": "CellHeight",
+    "Structure.InterlayerDistance": "InterlayerDistance", "Interlayer.TypeOfBL": "TypeOfBL",
+    "Interlayer.Vpppi0": "vpppi0", "Interlayer.Vppsigma0": "vppsigma0", "Interlayer.BLdelta": "BLdelta",
+    "Interlayer.AddSecondLayerInteractions": "addSecondLayerInteractions",
+    "Intralayer.KoshinoIntralayer": "KoshinoIntralayer", "Moire.Potential": "MoirePotential",
+    "Moire.Jeil": "MoireJeil", "Moire.OnlyH0": "MoireOnlyH0", "Moire.OnlyHZ": "MoireOnlyHZ",
+    "Moire.NoH0AndHZ": "MoireNoH0AndHZ", "Moire.H0AndHZ": "MoireH0AndHZ", "Moire.PreFactor": "MoirePreFactor",
+    "Moire.PotC0": "MoirePotC0", "Moire.PotCz": "MoirePotCz", "Moire.PotCab": "MoirePotCab",
+    "Moire.PotPhi0": "MoirePotPhi0", "Moire.PotPhiz": "MoirePotPhiz", "Moire.PotPhiab": "MoirePotPhiab",
+    "Moire.LatticePercent": "Latticepercent", "Moire.Twisted": "MoireTwisted", "Moire.TwistAngle": "MoireTwistAngle",
+    "Moire.OffDiag": "MoireOffDiag", "Moire.OffDiagMidpoint": "MoireOffDiagMidpoint",
+    "Moire.LayerShift1": "MoireLayerShift1", "Moire.FirstMoireMassFactor": "MoireFirstMoireMassFactor",
+    "Moire.SecondMoireMassFactor": "MoireSecondMoireMassFactor", "Disorder.Anderson": "Anderson",
+    "Disorder.AndersonAmp": "AndersonAmp", "Kubo.RecursionNumber": "RecursionNumber", "Kubo.Epsilon": "Epsilon",
+    "Kubo.NumberofEnergyPoints": "NumberofEnergyPoints", "Kubo.EnergyMin": "EnergyMin",
+    "Kubo.EnergyMax": "EnergyMax", "Kubo.SeedValue": "seedValue", "Kubo.SetSeed": "setSeed",
+    "Kubo.NumberofPolynomials": "NumberofPolynomials", "Kubo.TimeStep": "TimeStep",
+    "Kubo.NumberofTimeSteps": "NumberofTimeSteps", "Kubo.WriteNumberofSteps": "WriteNumberofSteps",
+    "Run.Prefix": "Prefix",
+}
+
+
+def _norm(k):
+    return k.lower().replace("_", "").replace("-", "")
+
+
+class Keys:
+    """Input keys; a key is found by its present Section.Name or by its former name."""
+
+    def __init__(self, keys):
+        self._k = {}
+        for k, v in keys.items():
+            self._k.setdefault(_norm(k), v)   # the first occurrence wins
+
+    def has(self, name):
+        return _norm(name) in self._k or _norm(FORMER.get(name, "\0")) in self._k
+
+    def get(self, name, default):
+        for cand in (name, FORMER.get(name)):
+            if cand is not None and _norm(cand) in self._k:
+                return self._k[_norm(cand)]
+        return default
+
+
+def job_from_keys(keys):
+    k = Keys(keys)
+    g = k.get
+    aG = g("Structure.LatticeParameter", 2.46)
+    system = g("Run.TypeOfSystem", "Graphene")
+    kind = {"graphene": CELL_GRAPHENE, "twistedbilayerbasedonmoirecell": CELL_TBG_MOIRE}.get(system.lower())
+    if kind is None:
+        raise ValueError(f"Run.TypeOfSystem {system} is not on the recursion path of this library")
+    cell = dict(kind=kind, aG=aG, cell_size=g("Structure.CellSize", 50), super_cell=g("Structure.SuperCell", 1),
+                m=tuple(g("Structure.MoireCellParameters", (0, 0, 0, 0))), height=g("Structure.CellHeight", 40.0),
+                d_interlayer=g("Structure.InterlayerDistance", 3.35))
+    g0 = g("TB.Hopping", -3.72 * aG + 12.14)
+    tbnn = g("TB.NeighLevels", 1)
+    if not 1 <= tbnn <= 8:
+        raise ValueError("TB.NeighLevels must be between 1 and 8")
+    acc = aG / math.sqrt(3.0)
+    r = 0.5 * (SHELL_RADIUS[tbnn - 1] + SHELL_RADIUS[tbnn]) * acc
+    cut2intra = r * r
+    if g("Neigh.LayerNeighbors", 0) != 0:
+        x = aG / math.sqrt(3.0) * 1.1 * g("Neigh.LayerDistFactor", 1.0)
+        cut2inter = x * x
+    else:
+        cut2inter = 1.0
+    m = Model()
+    m.aG = aG
+    m.tbnn = tbnn
+    for i in range(tbnn):
+        m.nradii[i] = SHELL_RADIUS[i] * aG / math.sqrt(3.0) * 1.1
+        m.gn_cc[i] = (g0 / g0) if i == 0 else 0.0
+    bl = g("Interlayer.TypeOfBL", "None")
+    koshino_intra = g("Intralayer.KoshinoIntralayer", False)
+    if bl in ("Koshino", "Mayou", "HTC") and not koshino_intra:
+        m.intralayer = 1
+        for i, v in F2G2_SINGLE_LAYER.items():
+            m.tksl[i] = v / g0
+    moire = bool(g("Moire.Potential", False) and g("Moire.Jeil", False))
+    if moire:
+        sel = [("Moire.OnlyH0", 2), ("Moire.OnlyHZ", 3), ("Moire.NoH0AndHZ", 4), ("Moire.H0AndHZ", 1)]
+        chosen = [v for key, v in sel if g(key, False)]
+        if not chosen:
+            raise ValueError("the moire potential needs one of MoireH0AndHZ, MoireOnlyH0, MoireOnlyHZ, MoireNoH0AndHZ")
+        m.moire_onsite = chosen[0]
+    pref = g("Moire.PreFactor", 1.0)
+    m.C0 = g("Moire.PotC0", -0.01013) / g0 * pref
+    m.Cz = g("Moire.PotCz", -0.00901) / g0 * pref
+    m.Phi0 = g("Moire.PotPhi0", 1.510233401750693)
+    m.Phiz = g("Moire.PotPhiz", 0.147131255943122)
+    m.Cab = g("Moire.PotCab", 0.01134) / g0
+    m.Phiab = g("Moire.PotPhiab", 0.342084533390889)
+    m.eps = g("Moire.LatticePercent", -0.018181818181818)
+    m.moire_twisted = int(bool(g("Moire.Twisted", False)))
+    m.twist_rad = g("Moire.TwistAngle", 0.0) * math.pi / 180.0
+    m.moire_offdiag = int(bool(g("Moire.OffDiag", False)))
+    m.moire_mid = int(bool(g("Moire.OffDiagMidpoint", False)) and m.moire_offdiag)
+    m.shift1 = g("Moire.LayerShift1", 0.0)
+    m.sign1 = g("Moire.FirstMoireMassFactor", 1.0)
+    m.sign2 = g("Moire.SecondMoireMassFactor", 1.0)
+    if bl in ("Koshino", "HTC"):
+        m.interlayer = 1
+    m.vpppi0 = g("Interlayer.Vpppi0", 2.7 if koshino_intra else 3.5) / g0
+    m.vppsigma0 = -g("Interlayer.Vppsigma0", 0.48) / g0
+    m.bl_delta = g("Interlayer.BLdelta", 0.184 * aG)
+    m.d_interlayer = g("Structure.InterlayerDistance", 3.35)
+    m.aCC = acc
+    m.g_intlay = g("TB.InterLayerHopping", 0.39) / g0
+    m.anderson = int(bool(g("Disorder.Anderson", False)))
+    amp = g("Disorder.AndersonAmp", None)
+    m.anderson_w = 1.0 if amp is None else amp / g0
+    m.e0_c = g("TB.OnSiteC", 0.0) / g0
+    seed = g("Kubo.SeedValue", 123456)
+    kubo = dict(nrecurs=g("Kubo.RecursionNumber", 700), eta=g("Kubo.Epsilon", 0.01) / g0, n_en=g("Kubo.NumberofEnergyPoints", 1000),
+                emin=g("Kubo.EnergyMin", -4.0) / g0, emax=g("Kubo.EnergyMax", 4.0) / g0, seed=seed,
+                npol=g("Kubo.NumberofPolynomials", 100), dt=g("Kubo.TimeStep", 5.0), nt=g("Kubo.NumberofTimeSteps", 500),
+                nwr=g("Kubo.WriteNumberofSteps", 10))
+    return dict(cell=cell, g0=g0, cut2intra=cut2intra, cut2inter=cut2inter,
+                second_layer=bool(g("Interlayer.AddSecondLayerInteractions", False)), model=m, moire=moire, kubo=kubo)
+
+
+def flux_of(m_quanta, area):
+    """Peierls flux parameter of HamHopping for m flux quanta through a cell of area [Ang^2]."""
+    bmag = m_quanta * FLUXQ / (area * 1.0e-20)
+    return bmag * math.pi / FLUXQ
+
+
+def cell_area(ucell):
+    u = ucell
+    v1 = u[1] * u[5] - u[2] * u[4]
+    v2 = u[2] * u[3] - u[0] * u[5]
+    v3 = u[0] * u[4] - u[1] * u[3]
+    return math.sqrt(v1 * v1 + v2 * v2 + v3 * v3)
+
+
+def setup(ctx, job):
+    """Cell, device neighbour search and device assembly for a job; returns the cell dict."""
+    from . import build_cell, cart_roundtrip, rng_uniform
+    cell = build_cell(**job["cell"])
+    ctx.set_geometry(cell["rat"], cell["species"], cell["layer"], cell["ucell"])
+    ctx.neighbours(job["cut2intra"], job["cut2inter"], job["second_layer"], tables=False)
+    rat_on = rat_hop = None
+    if job["moire"]:
+        rat_on = cart_roundtrip(cell["rat"], cell["ucell"])
+        rat_hop = cart_roundtrip(rat_on, cell["ucell"])
+    m = job["model"]
+    uniform = rng_uniform(job["kubo"]["seed"], cell["n"]) if m.anderson else None
+    ctx.assemble(m, rat_on, rat_hop, uniform)
+    return cell

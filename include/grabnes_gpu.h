@@ -63,6 +63,30 @@ typedef struct gbn_model {
     double  e0_c;          /* TB.OnSiteC/g0                                           */
 } gbn_model;
 
+/* ---- host-side cell construction and random numbers (no context, no GPU needed) ------ */
+#define GBN_CELL_GRAPHENE 0  /* Run.TypeOfSystem Graphene                       */
+#define GBN_CELL_TBG_MOIRE 1 /* Run.TypeOfSystem TwistedBilayerBasedOnMoireCell */
+typedef struct gbn_cell {
+    int32_t kind;         /* GBN_CELL_*                                   */
+    int32_t cell_size;    /* Structure.CellSize (graphene)                */
+    int32_t super_cell;   /* Structure.SuperCell                          */
+    int32_t m[4];         /* Structure.MoireCellParameters (bilayer)      */
+    double  aG;           /* Structure.LatticeParameter [Ang]             */
+    double  height;       /* Structure.CellHeight [Ang]                   */
+    double  d_interlayer; /* Structure.InterlayerDistance [Ang]           */
+} gbn_cell;
+/* Number of atoms of the cell (CellGet/AtomsPos, lanczosKuboCode/Src/cell.F90:108-140, 207-240). */
+int gbn_cell_atoms(const gbn_cell* cell, int64_t* n);
+/* ucell(3,3), Rat(3,N) Cartesian, Species(N), layerIndex(N) and the twist [rad] in the reference's
+ * atom order and rounding (atoms.F90:124-230, 330-380, 1506-1607, 1768-1794). */
+int gbn_build_cell(const gbn_cell* cell, double* ucell, double* rat, int32_t* species, int32_t* layer, double* twist);
+/* AtomsSetFrac followed by AtomsSetCart (atoms.F90:1768-1830), in place: the positions the reference's
+ * moire on-site and hopping routines see after their own conversions. */
+int gbn_cart_roundtrip(int64_t n, const double* ucell, double* rat);
+/* n draws of GNU Fortran's random_number(real(8)) after random_seed(PUT=[seed]*n_seed)
+ * (the start vectors of KuboInitWF, kubo.F90:46-64, and Anderson disorder, ham.F90:1237-1248). */
+int gbn_rng_uniform(int32_t seed, int64_t n, double* out);
+
 /* ---- context ------------------------------------------------------------------------ */
 /* No counterpart in the reference (module state); device = CUDA ordinal. */
 int         gbn_create(gbn_ctx** out, int32_t device);
@@ -71,10 +95,19 @@ const char* gbn_last_error(const gbn_ctx* ctx);
 const char* gbn_version(void);
 /* Use the caller's CUDA stream (a cudaStream_t) for all work of the context; NULL = own stream. */
 int         gbn_set_stream(gbn_ctx* ctx, void* cuda_stream);
+/* Tuning of the recursion kernels: right-hand sides per thread (1, 2, 4; 0 = widest load), a cap on
+ * resident blocks per SM (0 = occupancy limit) and the sparse-product variant (1 = matrix chunks staged
+ * in shared memory by bulk asynchronous copies, 0 = matrix read from global memory, -1 = automatic).
+ * Used by the autotuner (grabnes_b200/tune.py). */
+int         gbn_set_tuning(gbn_ctx* ctx, int32_t rhs_per_thread, int32_t blocks_per_sm, int32_t staged);
 /* Kernels launched by this context since creation (for launch accounting). */
 int64_t     gbn_launch_count(const gbn_ctx* ctx);
-/* Device time of the recursion-step kernels of the last gbn_lanczos* call. */
+/* Device time of the recursion loop of the last gbn_lanczos* / gbn_run_staged call and its number of
+ * recursion steps (each step launches one update and one sparse-product kernel). */
 int         gbn_last_timing(const gbn_ctx* ctx, double* step_ms_total, int64_t* step_launches);
+/* Average per-launch device time of the sparse-product and the update kernels over the first (up to 64)
+ * steps of the last call, measured with CUDA events on the context's stream. */
+int         gbn_last_kernel_timing(const gbn_ctx* ctx, double* spmm_ms, double* update_ms);
 
 /* ---- geometry and neighbour search ---------------------------------------------------- */
 /* Atoms of the cell: Rat(3,N) Cartesian [Ang], Species(N), layerIndex(N), ucell(3,3).

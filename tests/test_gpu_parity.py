@@ -168,3 +168,20 @@ def test_mixed_precision_dos(ctx):
     l1 = np.abs(d[0] - d_ref).sum() / np.abs(d_ref).sum()
     print("mixed-precision DOS error (normalised L1):", l1)
     assert l1 <= 1e-6, l1
+
+
+@pytest.mark.parametrize("rpt", [1, 2, 4])
+def test_kernel_variants_agree(ctx, rpt):
+    """Matrix staged in shared memory (bulk copies) or read from global memory, for every split of the
+    right-hand sides over threads: the same per-row arithmetic; only the partition of the rows over
+    blocks (and so the order of the FP64 partial sums) differs."""
+    r = built("tbg")
+    n = r["geo"]["n"]
+    ctx.load_hamiltonian(r["nb"]["nneigh"], r["nb"]["nlist"], r["hop"], r["h0"])
+    u = np.stack([orc.rng_draws(21 + k, n) for k in range(16)])
+    out = []
+    for staged in (0, 1):
+        ctx.set_tuning(rpt, 0, staged)
+        out.append(ctx.lanczos_phases(u, 60, G.GBN_MIXED))
+    ctx.set_tuning(0, 0, -1)
+    assert _rel(out[0][0], out[1][0]) <= 1e-9 and _rel(out[0][1], out[1][1]) <= 1e-9
