@@ -15,7 +15,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libgrabnes_gpu.so")
 
 GBN_FP64, GBN_MIXED = 0, 1
-ERRORS = {-1: "argument", -2: "cuda", -3: "state", -4: "numeric", -5: "alloc", -6: "timeout"}
+ERRORS = {-1: "argument", -2: "cuda", -3: "state", -4: "numeric", -5: "alloc", -6: "timeout", -7: "limit"}
+GBN_ERR_LIMIT = -7
+NOALLOC_MAX_ATOMS = 1048576   # GBN_NOALLOC_MAX_ATOMS
 
 
 class GbnError(RuntimeError):
@@ -79,7 +81,7 @@ def _opt(dtype):
 EXPORTS = ["gbn_cell_atoms", "gbn_build_cell", "gbn_cart_roundtrip", "gbn_rng_uniform", "gbn_create", "gbn_destroy", "gbn_last_error", "gbn_version", "gbn_set_stream", "gbn_set_tuning", "gbn_launch_count",
            "gbn_last_timing", "gbn_last_kernel_timing", "gbn_set_geometry", "gbn_neighbours", "gbn_get_neighbours", "gbn_assemble",
            "gbn_peierls", "gbn_get_hamiltonian", "gbn_load_hamiltonian", "gbn_lanczos", "gbn_lanczos_phases",
-           "gbn_stage_phases", "gbn_run_staged", "gbn_cf_dos", "gbn_cheb_evolve", "gbn_kubo_evol", "gbn_set_neighd"]
+           "gbn_stage_phases", "gbn_run_staged", "gbn_cf_dos", "gbn_cheb_evolve", "gbn_kubo_evol", "gbn_set_neighd", "gbn_lanczos_noalloc"]
 
 
 def _declare(L):
@@ -117,6 +119,8 @@ def _declare(L):
     L.gbn_cheb_evolve.argtypes = [vp, i32, _p(np.complex128), i32, d, d, _p(np.complex128)]
     L.gbn_kubo_evol.argtypes = [vp, i32, _p(np.complex128), i32, d, d, i32, _p(np.complex128), _p(np.complex128)]
     L.gbn_set_neighd.argtypes = [vp, _p(np.float64)]
+    # device pointers (ints from tensor.data_ptr()), no context
+    L.gbn_lanczos_noalloc.argtypes = [i64, i32, vp, vp, vp, vp, vp, i32, vp, vp, vp]
 
 
 def _c(a, dtype):

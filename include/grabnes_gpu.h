@@ -174,6 +174,34 @@ int gbn_kubo_evol(gbn_ctx* ctx, int32_t nrhs, const double* c, int32_t npol, dou
 /* NeighD(3,maxNeigh,N) for gbn_kubo_evol after gbn_load_hamiltonian. */
 int gbn_set_neighd(gbn_ctx* ctx, const double* neighd);
 
+/* ---- recursion without device allocation ------------------------------------------------------ */
+/* No counterpart in the reference: an addition for hosts that cannot allocate device memory.
+ *
+ * A host that gives all of a GPU's memory to its own pool allocator, or that must not call cudaMalloc
+ * and cudaFree because they synchronise the whole device while the host has other work in flight
+ * there, cannot create a gbn_ctx (a context allocates per-context device buffers).  This call needs
+ * no context and allocates nothing: its three recursion vectors, reduction partials and counter sit
+ * in one fixed array inside the library, sized for GBN_NOALLOC_MAX_ATOMS atoms (about 48 MiB), which
+ * every GPU that loads the library holds until the process exits.
+ *
+ * It runs the KuboRecursion of one start vector in FP64 on the CURRENT device, on `stream` (NULL:
+ * the default stream), and returns when the stream has finished it.  All pointers are device memory
+ * of the current device, in the layouts of gbn_load_hamiltonian: nneigh(N), nlist(maxNeigh,N)
+ * (1-based), hopp(maxNeigh,N) complex, h0(N), psi(N) complex (normalised by the caller; hopp and psi
+ * 16-byte aligned); a, b: nrecurs doubles each, written by the call.
+ * The first call on a device looks up the array's device address (cudaGetSymbolAddress); make that
+ * first call before any stream capture on that device.  All calls on a device share the array, so
+ * calls that overlap on the GPU (other host threads, other streams) race: serialise them.
+ * Returns GBN_ERR_LIMIT when n > GBN_NOALLOC_MAX_ATOMS, GBN_ERR_ARG for other bad arguments
+ * (including Nneigh/NList entries out of range, found on the device), GBN_ERR_NUMERIC for a b_n that
+ * is not finite or not positive, GBN_ERR_CUDA for a failed launch or copy.  gbn_last_error() does not
+ * apply (there is no context). */
+#define GBN_NOALLOC_MAX_ATOMS 1048576
+#define GBN_ERR_LIMIT (-7) /* a size beyond the stated maximum of the call */
+int gbn_lanczos_noalloc(int64_t n, int32_t max_neigh, const int32_t* nneigh, const int32_t* nlist,
+                        const double* hopp, const double* h0, const double* psi, int32_t nrecurs,
+                        double* a, double* b, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
