@@ -164,9 +164,10 @@ def run_ours(args, ws, rank, local):
     # vectors are staged once and every job rebuilds them on the device
     from grabnes_b200.tune import autotune
     if args.tuning:
-        rpt, bps, st = (int(x) for x in args.tuning.split(","))
-        ctx.set_tuning(rpt, bps, st)
-        best, tuning = dict(rhs_per_thread=rpt, blocks_per_sm=bps, staged=st, fixed=True), []
+        rpt, bps, grp, st, pf = (int(x) for x in args.tuning.split(","))
+        ctx.set_tuning(rpt, bps, grp, st, pf)
+        best = dict(rhs_per_thread=rpt, blocks_per_sm=bps, rows_per_group=grp, staged=st, prefetch=pf, fixed=True)
+        tuning = []
     else:
         best, tuning = autotune(ctx, u, G.GBN_MIXED)
     ctx.stage_phases(u, G.GBN_MIXED)
@@ -342,7 +343,7 @@ def main():
     p.add_argument("--supercell", type=int, default=20, help="moire cells per side (20 = the workload)")
     p.add_argument("--nsteps", type=int, default=NSTEPS, help="recursion steps per job (2000 = the workload)")
     p.add_argument("--value-only", action="store_true", help="time the device-resident jobs only (profiling)")
-    p.add_argument("--tuning", default="", help="fixed kernel tuning 'rhs_per_thread,blocks_per_sm,staged' "
+    p.add_argument("--tuning", default="", help="fixed kernel tuning 'rhs_per_thread,blocks_per_sm,rows_per_group,staged,prefetch' "
                                                 "instead of the autotuner")
     args = p.parse_args()
     ws, rank, local = dist_init() if args.impl == "ours" else (int(os.environ.get("WORLD_SIZE", "1")),

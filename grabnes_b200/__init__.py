@@ -97,7 +97,7 @@ def _declare(L):
     L.gbn_last_error.restype = C.c_char_p
     L.gbn_version.restype = C.c_char_p
     L.gbn_set_stream.argtypes = [vp, vp]
-    L.gbn_set_tuning.argtypes = [vp, i32, i32, i32]
+    L.gbn_set_tuning.argtypes = [vp, i32, i32, i32, i32, i32]
     L.gbn_launch_count.argtypes = [vp]
     L.gbn_launch_count.restype = i64
     L.gbn_last_timing.argtypes = [vp, C.POINTER(d), C.POINTER(i64)]
@@ -160,8 +160,8 @@ class Context:
     def set_stream(self, stream_handle):
         self._ck(self._L.gbn_set_stream(self._h, C.c_void_p(stream_handle)))
 
-    def set_tuning(self, rhs_per_thread=0, blocks_per_sm=0, staged=-1):
-        self._ck(self._L.gbn_set_tuning(self._h, rhs_per_thread, blocks_per_sm, staged))
+    def set_tuning(self, rhs_per_thread=0, blocks_per_sm=0, rows_per_group=0, staged=-1, prefetch=0):
+        self._ck(self._L.gbn_set_tuning(self._h, rhs_per_thread, blocks_per_sm, rows_per_group, staged, prefetch))
 
     @property
     def launches(self):

@@ -134,8 +134,8 @@ int gbn_destroy(gbn_ctx* c)
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     DevBuf* bufs[] = {&c->rat, &c->species, &c->layer, &c->nneigh, &c->nlist, &c->neighd, &c->ncell, &c->h0,
-                      &c->hopp, &c->rat_hop, &c->perm, &c->iperm, &c->ell.slice_ptr, &c->ell.col, &c->ell.val,
-                      &c->ell.h0, &c->partials, &c->scal, &c->counter, &c->ab, &c->upload};
+                      &c->hopp, &c->rat_hop, &c->perm, &c->iperm, &c->ell.slice_ptr, &c->ell.mat,
+                      &c->ell.h0, &c->ell.rperm, &c->ell.riperm, &c->partials, &c->scal, &c->counter, &c->ab, &c->upload};
     for (DevBuf* b : bufs) b->release();
     for (auto& v : c->vec) v.release();
     for (auto& v : c->cheb) v.release();
@@ -176,14 +176,19 @@ int gbn_last_timing(const gbn_ctx* c, double* ms, int64_t* launches)
     return GBN_OK;
 }
 
-int gbn_set_tuning(gbn_ctx* c, int32_t rhs_per_thread, int32_t blocks_per_sm, int32_t staged)
+int gbn_set_tuning(gbn_ctx* c, int32_t rhs_per_thread, int32_t blocks_per_sm, int32_t rows_per_group, int32_t staged,
+                   int32_t prefetch)
 {
     if (!c) return GBN_ERR_ARG;
-    if (rhs_per_thread < 0 || rhs_per_thread > 4 || blocks_per_sm < 0 || blocks_per_sm > 32 || staged < -1 || staged > 1)
+    if (rhs_per_thread < 0 || rhs_per_thread > 4 || blocks_per_sm < 0 || blocks_per_sm > 32 ||
+        (rows_per_group != 0 && rows_per_group != 1 && rows_per_group != 2 && rows_per_group != 4) || staged < -1 ||
+        staged > 1 || prefetch < 0 || prefetch > 2)
         return fail(c, GBN_ERR_ARG, "tuning values out of range");
     c->tune_rpt = rhs_per_thread;
     c->tune_blocks_per_sm = blocks_per_sm;
+    c->tune_group = rows_per_group;
     c->tune_staged = staged;
+    c->tune_prefetch = prefetch;
     c->ell.valid = false;
     return GBN_OK;
 }
@@ -313,8 +318,10 @@ int gbn_load_hamiltonian(gbn_ctx* c, int64_t n, int32_t max_neigh, const int32_t
     if (n < 1 || n >= (int64_t)1 << 31) return fail(c, GBN_ERR_ARG, "number of atoms must be in 1..2^31-1");
     if (max_neigh < 1) return fail(c, GBN_ERR_ARG, "max_neigh must be at least 1");
     if (!nneigh || !nlist || !hopp || !h0) return fail(c, GBN_ERR_ARG, "NULL Hamiltonian array");
+    int64_t total = 0;
     for (int64_t i = 0; i < n; ++i) {
         if (nneigh[i] < 0 || nneigh[i] > max_neigh) return fail(c, GBN_ERR_ARG, "Nneigh(i) outside 0..maxNeigh");
+        total += nneigh[i];
         for (int32_t j = 0; j < nneigh[i]; ++j) {
             const int32_t m = nlist[i * max_neigh + j];
             if (m < 1 || m > n) return fail(c, GBN_ERR_ARG, "NList entry outside 1..N");
@@ -341,6 +348,7 @@ int gbn_load_hamiltonian(gbn_ctx* c, int64_t n, int32_t max_neigh, const int32_t
         if (rc) return rc;
     }
     c->max_neigh = max_neigh;
+    c->total = total;
     c->have_neigh = true;
     c->have_neighd = same_atoms && c->have_neighd;
     c->have_ham = true;
@@ -408,8 +416,13 @@ int gbn_run_staged(gbn_ctx* c, int32_t nmax, double* a, double* b)
     if (!c->staged) return fail(c, GBN_ERR_STATE, "nothing staged: call gbn_stage_phases first");
     if (nmax < 1) return fail(c, GBN_ERR_ARG, "nmax must be at least 1");
     cudaSetDevice(c->device);
+    int rc = GBN_OK;
+    if (!c->ell.valid) {   // the layout was invalidated (new tuning or Hamiltonian) since staging
+        rc = lanczos_prepare(c, c->prec, c->nrhs);
+        if (rc) return rc;
+    }
     // the start vectors are rebuilt from the staged draws so that every run starts from them
-    int rc = lanczos_start_from_phases(c, c->upload.as<double>(), c->nrhs);
+    rc = lanczos_start_from_phases(c, c->upload.as<double>(), c->nrhs);
     if (rc) return rc;
     rc = lanczos_run(c, nmax);
     if (rc) return rc;

@@ -11,10 +11,14 @@
 
 namespace gbn {
 
-// Device allocation that grows on demand and is freed with the context.
+// Device allocation that grows on demand; freed by release() or when it goes out of scope.
 struct DevBuf {
     void* p = nullptr;
     size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() { release(); }
     cudaError_t ensure(size_t need) {
         if (need <= bytes && p) return cudaSuccess;
         if (p) cudaFree(p);
@@ -32,27 +36,38 @@ struct DevBuf {
     template <typename T> T* as() const { return static_cast<T*>(p); }
 };
 
-// Sliced ELL matrix of the permuted Hamiltonian: slices of `sh` rows, entries of a slice stored
-// column by column (entry k of row r of slice s at slice_ptr[s] + k*sh + r).  Padding entries point
-// at their own row with a zero value, padded rows have no entries that matter.
+// Grouped sliced ELL of the permuted Hamiltonian.  Rows are taken in groups of G consecutive rows
+// (neighbouring atoms in the solver's row order); a group stores the union of its rows' neighbour
+// columns once, with G values per union column (zero where a row has no such neighbour), so a
+// gathered vector row serves all G rows.  gpw groups form a slice (the groups one warp processes
+// together).  A slice is one contiguous record in `mat`, starting at byte slice_ptr[s] * entry_bytes
+// (entry_bytes = 4 + G * val_size; slice_ptr counts union entries, w * gpw per slice):
+//     int32 col[w][gpw]   then   value val[w][gpw][G]
+// Slice widths w are multiples of 4 (records are multiples of 16 bytes and start on 16-byte
+// boundaries); padding columns point at the group's first row with zero values.  Values are stored
+// NEGATED (-hopp = +t/g0), so that (H x)_i = h0_i x_i + sum val * x.  G = 1 is the plain sliced ELL.
 struct Ell {
-    int sh = 0;              // rows per slice (= rows a warp processes at once)
+    int G = 0;               // rows per group
+    int gpw = 0;             // groups per slice
     int prec = -1;           // GBN_FP64 / GBN_MIXED
     bool cplx = false;       // complex values stored
+    int64_t ngroups = 0;
     int64_t nslices = 0;
-    int64_t npad = 0;        // nslices * sh
-    int64_t nnz_stored = 0;  // entries including padding
+    int64_t npad = 0;        // nslices * gpw * G rows (vectors are allocated for npad rows)
+    int64_t nnz_stored = 0;  // union entries including padding
     DevBuf slice_ptr;        // int64 [nslices + 1]
-    DevBuf col;              // int32 [nnz_stored]
-    DevBuf val;              // float | double | float2 | double2
+    DevBuf mat;              // slice records
     DevBuf h0;               // float | double [npad]
-    int64_t max_chunk_entries = 0;  // largest chunk of kChunkSlices consecutive slices
-    int val_size = 0;               // bytes per stored value
+    DevBuf rperm, riperm;    // solver row order: rperm[row] = reference atom (row < n), riperm inverse
+    int val_size = 0;        // bytes per stored value
+    int entry_bytes = 0;     // 4 + G * val_size
+    int64_t max_record = 0;  // bytes of the largest slice record
+    int64_t cap_record = 0;  // staging buffer size: 99.5 % of the records fit (larger ones are read in place)
     bool valid = false;
 };
 
-// slices per chunk of the staged sparse-product kernel (one slice per warp of a 256-thread block)
-constexpr int kChunkSlices = 8;
+// unroll of the union-column loop (slice widths are multiples of it)
+constexpr int kColUnroll = 4;
 
 struct Timing {
     double step_ms = 0.0;        // whole recursion loop of the last call
@@ -116,7 +131,9 @@ struct gbn_ctx {
     // tuning of the recursion kernels (0 = automatic)
     int tune_rpt = 0;            // right-hand sides per thread
     int tune_blocks_per_sm = 0;  // cap on resident blocks per SM
-    int tune_staged = -1;        // sparse product with the matrix staged in shared memory (-1 auto, 0 no, 1 yes)
+    int tune_group = 0;          // rows per group of the matrix layout (1, 2, 4)
+    int tune_staged = -1;        // matrix records staged in shared memory by bulk copies (-1 auto, 0 no, 1 yes)
+    int tune_prefetch = 0;       // staged kernel: prefetch the gather rows of a slice (0 no, 1 to L2, 2 to L1)
     bool last_staged = false;    // the last recursion used the staged kernel
 
     // Chebyshev work vectors
@@ -144,14 +161,14 @@ int cuda_fail(gbn_ctx* c, cudaError_t e, const char* what);
 // layout / permutation (gbn_layout.cu)
 int build_identity_perm(gbn_ctx* c);
 int build_spatial_perm(gbn_ctx* c);
-int build_ell(gbn_ctx* c, int prec, int sh);
+int build_ell(gbn_ctx* c, int prec, int G, int gpw);
+int auto_group(const gbn_ctx* c);
 
 // recursion (gbn_lanczos.cu)
 int lanczos_prepare(gbn_ctx* c, int prec, int nrhs);
 int lanczos_start_from_phases(gbn_ctx* c, const double* d_u, int nrhs_real);
 int lanczos_start_from_psi(gbn_ctx* c, const double* d_psi, int nrhs_real);
 int lanczos_run(gbn_ctx* c, int32_t nmax);
-int rows_per_slice(int prec, int nrhs, int want_rpt);
 
 // continued fraction (gbn_cf.cu)
 int cf_dos(gbn_ctx* c, int32_t nrhs, const double* d_a, const double* d_b, const int32_t* d_nsteps, int32_t nmax,

@@ -6,20 +6,22 @@
 //     v_k = H x_{k-1} - b_{k-2} x_{k-2}      and     x_{k-1},
 // and a step is
 //   k_update    x_k = (v_k - a_{k-1} x_{k-1}) / b_{k-1}             stream: read v, x_{k-1}; write x_k
-//   k_spmm_step y = H x_k (one gather of x_k per matrix entry), v_{k+1} = y - b_{k-1} x_{k-1}, and
-//               four FP64 dot products per vector
+//   k_spmm_*    y = H x_k (one gather of x_k per union column of a row group), v_{k+1} = y - b_{k-1} x_{k-1},
+//               and four FP64 dot products per vector
 //                  S1 = Re<x_k, y>, S2 = |v_{k+1}|^2, S3 = Re<x_k, v_{k+1}>, S4 = |x_k|^2,
 //               from which a_k = S1 and b_k^2 = |v_{k+1} - a_k x_k|^2 = S2 - 2 a_k S3 + a_k^2 S4.
 // The partial sums of the blocks are reduced in a fixed order by the last block to finish (so the
 // result does not depend on scheduling), which also writes a_k, b_k and the scalars of the next step.
-// Each matrix entry is gathered once per step: for many right-hand sides the gathers, not the
-// DRAM stream, bound the product (a row of R vectors is read once per neighbour that references it).
 //
-// Vectors of R right-hand sides are interleaved per row ([row][R] complex): TPR threads share a row,
-// each holding RPT right-hand sides (16-32 bytes per gather); a warp processes a slice of
-// SH = 32/TPR rows of the sliced-ELL matrix.
+// Vectors of R right-hand sides are interleaved per row ([row][R] complex): TPR threads share a row
+// group, each holding RPT right-hand sides (8-32 bytes per gather).  With 16 vectors a gathered row is
+// one 128-byte line.  The product is bound by the latency of the chain column index -> gather: the
+// grouped layout (struct Ell) gathers a column once for the G rows of a group, and the staged kernel
+// brings each warp's next slice record (column indices and values) into shared memory with one bulk
+// asynchronous copy, so that only the gathers themselves wait on memory.
 #include <cuda_runtime.h>
 #include <math.h>
+#include <string.h>
 
 #include "gbn_internal.cuh"
 
@@ -31,8 +33,10 @@ template <> struct V2<double> { using t = double2; };
 
 struct StepParams {
     const int64_t* slice_ptr;
-    const int32_t* col;
-    const void* val;
+    const unsigned char* mat;  // slice records (column indices, then G values per union column)
+    int64_t entry_bytes;       // 4 + G * value bytes
+    int64_t cap_record;        // bytes of a staging buffer (larger records are read in place)
+    int32_t prefetch;          // staged kernel: prefetch the gather rows of a slice (1 L2, 2 L1)
     const void* h0;
     const void* x_cur;   // x_k   [npad][R] (gathered)
     const void* x_prev;  // x_{k-1}
@@ -43,7 +47,6 @@ struct StepParams {
     double* a_out;       // [R][nmax]
     double* b_out;
     int64_t nslices;
-    int64_t max_chunk;   // entries of the largest chunk (staged kernel)
     int32_t nmax;
 };
 
@@ -83,125 +86,89 @@ template <> struct VecIO<double, 1> {
     static __device__ __forceinline__ void store(double2* p, const double2 o[1]) { p[0] = o[0]; }
 };
 
-// hopping value types: real VT or complex V2<VT>
+// hopping value types: real VT or complex V2<VT>; values are stored negated, so products are added
 template <typename VT, bool CPLX> struct Hop;
-template <typename VT> struct Hop<VT, false> {
-    using t = VT;
-    static __device__ __forceinline__ void msub(typename V2<VT>::t& acc, VT h, typename V2<VT>::t x) {
-        acc.x = fma(-h, x.x, acc.x);
-        acc.y = fma(-h, x.y, acc.y);
+template <> struct Hop<float, false> {
+    using t = float;
+    // packed FP32 (one FFMA2 for the real and imaginary parts)
+    static __device__ __forceinline__ void madd(float2& acc, float h, float2 x) {
+        acc = __ffma2_rn(make_float2(h, h), x, acc);
     }
-    static __device__ __forceinline__ VT load(const VT* p) { return __ldcs(p); }
+};
+template <> struct Hop<double, false> {
+    using t = double;
+    static __device__ __forceinline__ void madd(double2& acc, double h, double2 x) {
+        acc.x = fma(h, x.x, acc.x);
+        acc.y = fma(h, x.y, acc.y);
+    }
 };
 template <typename VT> struct Hop<VT, true> {
     using t = typename V2<VT>::t;
-    static __device__ __forceinline__ void msub(typename V2<VT>::t& acc, t h, typename V2<VT>::t x) {
-        acc.x = fma(-h.x, x.x, acc.x);
-        acc.x = fma(h.y, x.y, acc.x);
-        acc.y = fma(-h.x, x.y, acc.y);
-        acc.y = fma(-h.y, x.x, acc.y);
+    static __device__ __forceinline__ void madd(typename V2<VT>::t& acc, t h, typename V2<VT>::t x) {
+        acc.x = fma(h.x, x.x, acc.x);
+        acc.x = fma(-h.y, x.y, acc.x);
+        acc.y = fma(h.x, x.y, acc.y);
+        acc.y = fma(h.y, x.x, acc.y);
     }
-    static __device__ __forceinline__ t load(const t* p) { return __ldcs(p); }
 };
 
+// G consecutive values of one union column (G * sizeof(HT) = 4..64 bytes, naturally aligned), read
+// with the widest loads: from global memory once and evicted first (the matrix is streamed every
+// step), or from shared memory
+template <typename HT, int G, bool SMEM>
+__device__ __forceinline__ void load_group_vals(const HT* p, HT (&h)[G])
+{
+    constexpr int B = G * (int)sizeof(HT);
+    if constexpr (B % 16 == 0) {
+        uint4 t[B / 16];
+#pragma unroll
+        for (int i = 0; i < B / 16; ++i) {
+            if constexpr (SMEM) t[i] = reinterpret_cast<const uint4*>(p)[i];
+            else t[i] = __ldcs(reinterpret_cast<const uint4*>(p) + i);
+        }
+        memcpy(h, t, B);
+    } else if constexpr (B == 8) {
+        uint2 t;
+        if constexpr (SMEM) t = *reinterpret_cast<const uint2*>(p);
+        else t = __ldcs(reinterpret_cast<const uint2*>(p));
+        memcpy(h, &t, B);
+    } else {
+        static_assert(B == 4, "value group of 4, 8 or a multiple of 16 bytes");
+        unsigned int t;
+        if constexpr (SMEM) t = *reinterpret_cast<const unsigned int*>(p);
+        else t = __ldcs(reinterpret_cast<const unsigned int*>(p));
+        memcpy(h, &t, B);
+    }
+}
+
 // ---------------------------------------------------------------------------- update kernel
-// x_k = (v_k - a x_{k-1}) * (1/b) for all rows and right-hand sides (streaming, 16 B per thread).
+// x_k = (v_k - a x_{k-1}) * (1/b) for all rows and right-hand sides (streaming).  The grid stride and
+// the block size are multiples of R, so every thread keeps one right-hand side and its 1/b.
 template <typename VT>
 __global__ void __launch_bounds__(256) k_update(const typename V2<VT>::t* __restrict__ v,
                                                 const typename V2<VT>::t* __restrict__ xp,
                                                 typename V2<VT>::t* __restrict__ xc, const double* __restrict__ scal,
                                                 int64_t total, int R)
 {
+    const int r = (int)(threadIdx.x & (unsigned)(R - 1));
+    const double a = scal[2 * r], ib = 1.0 / scal[2 * r + 1];
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += stride) {
-        const int r = (int)(e % R);
-        const double a = scal[2 * r], b = scal[2 * r + 1];
         const typename V2<VT>::t vv = __ldcs(v + e), xx = __ldcs(xp + e);
         typename V2<VT>::t o;   // FP64 arithmetic, one rounding to the storage type
-        o.x = (VT)(((double)vv.x - a * (double)xx.x) / b);
-        o.y = (VT)(((double)vv.y - a * (double)xx.y) / b);
+        o.x = (VT)(((double)vv.x - a * (double)xx.x) * ib);
+        o.y = (VT)(((double)vv.y - a * (double)xx.y) * ib);
         xc[e] = o;
     }
 }
 
-// ---------------------------------------------------------------------------- SpMM kernels
-// matrix entries are read either from global memory (streamed, evict-first) or from shared memory
-struct FromGlobal {
-    template <typename T> static __device__ __forceinline__ T ld(const T* p) { return __ldcs(p); }
-};
-struct FromShared {
-    template <typename T> static __device__ __forceinline__ T ld(const T* p) { return *p; }
-};
-
+// ---------------------------------------------------------------------------- sparse product
 struct SliceSums {
     double s1, s2, s3, s4;
 };
 
-// One slice of SH rows: y = H x_k for the thread's row and right-hand sides, v_{k+1} = y - b x_{k-1},
-// and the four dot-product terms of the row.
-template <typename VT, bool CPLX, int RPT, int TPR, typename SRC>
-__device__ __forceinline__ void spmm_slice(const StepParams& p, int64_t s, int w, const int32_t* __restrict__ cp,
-                                           const typename Hop<VT, CPLX>::t* __restrict__ hp, const double* cb,
-                                           SliceSums* acc_s)
-{
-    using C2 = typename V2<VT>::t;
-    using HT = typename Hop<VT, CPLX>::t;
-    constexpr int SH = 32 / TPR;
-    constexpr int R = RPT * TPR;
-    const int lane = threadIdx.x & 31;
-    const int sub = lane / TPR;
-    const int q = lane % TPR;
-    const C2* __restrict__ xc = static_cast<const C2*>(p.x_cur);
-    const C2* __restrict__ xp = static_cast<const C2*>(p.x_prev);
-    C2* __restrict__ vout = static_cast<C2*>(p.v_out);
-    const VT* __restrict__ h0 = static_cast<const VT*>(p.h0);
-    const int64_t row = s * SH + sub;
-    C2 xo[RPT], acc[RPT];
-    VecIO<VT, RPT>::load(xc + row * R + q * RPT, xo);
-    const VT d = h0[row];
-#pragma unroll
-    for (int t = 0; t < RPT; ++t) { acc[t].x = d * xo[t].x; acc[t].y = d * xo[t].y; }
-    // batches of KB entries: all column indices first, then all gathers, then the products, so that KB
-    // independent gathers are in flight per thread
-    constexpr int KB = (RPT * sizeof(VT) >= 16) ? 8 : 16;
-    for (int k0 = 0; k0 < w; k0 += KB) {
-        int32_t c[KB];
-        HT h[KB];
-#pragma unroll
-        for (int j = 0; j < KB; ++j) {
-            if (k0 + j < w) {
-                c[j] = SRC::ld(cp + (int64_t)(k0 + j) * SH);
-                h[j] = SRC::ld(hp + (int64_t)(k0 + j) * SH);
-            } else {
-                c[j] = (int32_t)row;
-                h[j] = HT{};
-            }
-        }
-        C2 xg[KB][RPT];
-#pragma unroll
-        for (int j = 0; j < KB; ++j) VecIO<VT, RPT>::load(xc + (int64_t)c[j] * R + q * RPT, xg[j]);
-#pragma unroll
-        for (int j = 0; j < KB; ++j)
-#pragma unroll
-            for (int t = 0; t < RPT; ++t) Hop<VT, CPLX>::msub(acc[t], h[j], xg[j][t]);
-    }
-    C2 xm[RPT], vn[RPT];
-    VecIO<VT, RPT>::load(xp + row * R + q * RPT, xm);
-#pragma unroll
-    for (int t = 0; t < RPT; ++t) {
-        // epilogue in FP64: v_{k+1} = y - b_{k-1} x_{k-1}, rounded once to the storage type
-        vn[t].x = (VT)((double)acc[t].x - cb[t] * (double)xm[t].x);
-        vn[t].y = (VT)((double)acc[t].y - cb[t] * (double)xm[t].y);
-        const double xr = xo[t].x, xi = xo[t].y, yr = acc[t].x, yi = acc[t].y, vr = vn[t].x, vi = vn[t].y;
-        acc_s[t].s1 += xr * yr + xi * yi;
-        acc_s[t].s2 += vr * vr + vi * vi;
-        acc_s[t].s3 += xr * vr + xi * vi;
-        acc_s[t].s4 += xr * xr + xi * xi;
-    }
-    VecIO<VT, RPT>::store(vout + row * R + q * RPT, vn);
-}
-
 // Reduction of the four sums over the block, then by the last block over all blocks; writes a_k, b_k.
+// Needs at least 4 R threads per block.
 template <int RPT, int TPR>
 __device__ __forceinline__ void reduce_and_finalize(const StepParams& p, SliceSums* acc_s)
 {
@@ -273,13 +240,89 @@ __device__ __forceinline__ void reduce_and_finalize(const StepParams& p, SliceSu
     }
 }
 
-// Matrix read from global memory.  Every block owns a contiguous range of slices (a compact region of
-// the Morton order); its warps take neighbouring slices, so the rows they gather overlap in L1.
-template <typename VT, bool CPLX, int RPT, int TPR>
+// One slice of the grouped sliced ELL: GPW = 32/TPR groups; the TPR threads of a group each hold RPT
+// right-hand sides of all G rows of the group.  Per union column a thread reads the column index and
+// the G values (same address for the group's threads) and gathers RPT vector elements of that column
+// once for all G rows.  The epilogue per row adds the on-site term and is FP64 from there:
+// v_{k+1} = y - b_{k-1} x_{k-1} rounded once, and the four dot-product terms.  cp/vp point at the
+// thread's group in the slice record, in global memory (streamed) or in shared memory (SMEM).
+template <typename VT, bool CPLX, int G, int RPT, int TPR, bool SMEM>
+__device__ __forceinline__ void group_slice(const StepParams& p, int64_t s, int w, const int32_t* __restrict__ cp,
+                                            const typename Hop<VT, CPLX>::t* __restrict__ vp, const double* cb,
+                                            SliceSums* acc_s)
+{
+    using C2 = typename V2<VT>::t;
+    using HT = typename Hop<VT, CPLX>::t;
+    constexpr int GPW = 32 / TPR;
+    constexpr int R = RPT * TPR;
+    constexpr int U = kColUnroll;
+    const int lane = threadIdx.x & 31;
+    const int sub = lane / TPR;
+    const int q = lane % TPR;
+    const C2* __restrict__ xc = static_cast<const C2*>(p.x_cur);
+    const C2* __restrict__ xp = static_cast<const C2*>(p.x_prev);
+    C2* __restrict__ vout = static_cast<C2*>(p.v_out);
+    const VT* __restrict__ h0 = static_cast<const VT*>(p.h0);
+    const C2* __restrict__ xq = xc + q * RPT;
+    const int64_t row0 = (s * GPW + sub) * G;
+    C2 acc[G][RPT];
+#pragma unroll
+    for (int g = 0; g < G; ++g)
+#pragma unroll
+        for (int t = 0; t < RPT; ++t) { acc[g][t].x = 0; acc[g][t].y = 0; }
+    for (int k = 0; k < w; k += U) {
+        int32_t c[U];
+        HT h[U][G];
+        C2 xg[U][RPT];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            if constexpr (SMEM) c[u] = cp[u * GPW];
+            else c[u] = __ldcs(cp + u * GPW);
+            load_group_vals<HT, G, SMEM>(vp + u * GPW * G, h[u]);
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) VecIO<VT, RPT>::load(xq + (size_t)(uint32_t)c[u] * R, xg[u]);
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+#pragma unroll
+            for (int g = 0; g < G; ++g)
+#pragma unroll
+                for (int t = 0; t < RPT; ++t) Hop<VT, CPLX>::madd(acc[g][t], h[u][g], xg[u][t]);
+        cp += U * GPW;
+        vp += U * GPW * G;
+    }
+    // epilogue per row: the on-site term (own x_k row, loaded here so that it holds no registers during
+    // the column loop), then v_{k+1} and the dot-product terms in FP64
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+        C2 xo[RPT], xm[RPT], vn[RPT];
+        VecIO<VT, RPT>::load(xc + (row0 + g) * R + q * RPT, xo);
+        VecIO<VT, RPT>::load(xp + (row0 + g) * R + q * RPT, xm);
+        const VT d = h0[row0 + g];
+#pragma unroll
+        for (int t = 0; t < RPT; ++t) {
+            acc[g][t].x = fma(d, xo[t].x, acc[g][t].x);
+            acc[g][t].y = fma(d, xo[t].y, acc[g][t].y);
+            vn[t].x = (VT)((double)acc[g][t].x - cb[t] * (double)xm[t].x);
+            vn[t].y = (VT)((double)acc[g][t].y - cb[t] * (double)xm[t].y);
+            const double xr = xo[t].x, xi = xo[t].y, yr = acc[g][t].x, yi = acc[g][t].y;
+            const double vr = vn[t].x, vi = vn[t].y;
+            acc_s[t].s1 += xr * yr + xi * yi;
+            acc_s[t].s2 += vr * vr + vi * vi;
+            acc_s[t].s3 += xr * vr + xi * vi;
+            acc_s[t].s4 += xr * xr + xi * xi;
+        }
+        VecIO<VT, RPT>::store(vout + (row0 + g) * R + q * RPT, vn);
+    }
+}
+
+// Matrix records read from global memory.  Every block owns a contiguous range of slices (a compact
+// region of the row order); its warps take neighbouring slices, so the rows they gather overlap in L1.
+template <typename VT, bool CPLX, int G, int RPT, int TPR>
 __global__ void __launch_bounds__(256) k_spmm_step(StepParams p)
 {
     using HT = typename Hop<VT, CPLX>::t;
-    constexpr int SH = 32 / TPR;
+    constexpr int GPW = 32 / TPR;
     const int q = (threadIdx.x & 31) % TPR;
     const int sub = (threadIdx.x & 31) / TPR;
     double cb[RPT];
@@ -289,20 +332,22 @@ __global__ void __launch_bounds__(256) k_spmm_step(StepParams p)
         cb[t] = p.scal[2 * (q * RPT + t) + 1];
         acc_s[t] = SliceSums{0.0, 0.0, 0.0, 0.0};
     }
-    const HT* __restrict__ val = static_cast<const HT*>(p.val);
     const int nwb = (int)(blockDim.x >> 5);
     const int64_t per = (p.nslices + gridDim.x - 1) / gridDim.x;
     const int64_t s0 = (int64_t)blockIdx.x * per;
     const int64_t s1e = (s0 + per < p.nslices) ? s0 + per : p.nslices;
     for (int64_t s = s0 + (threadIdx.x >> 5); s < s1e; s += nwb) {
         const int64_t base = p.slice_ptr[s];
-        const int w = (int)((p.slice_ptr[s + 1] - base) / SH);
-        spmm_slice<VT, CPLX, RPT, TPR, FromGlobal>(p, s, w, p.col + base + sub, val + base + sub, cb, acc_s);
+        const int w = (int)((p.slice_ptr[s + 1] - base) / GPW);
+        const unsigned char* rec = p.mat + base * p.entry_bytes;
+        group_slice<VT, CPLX, G, RPT, TPR, false>(p, s, w, reinterpret_cast<const int32_t*>(rec) + sub,
+                                                  reinterpret_cast<const HT*>(rec + (size_t)w * GPW * 4) + sub * G,
+                                                  cb, acc_s);
     }
     reduce_and_finalize<RPT, TPR>(p, acc_s);
 }
 
-// ---- bulk asynchronous copies (TMA, cp.async.bulk) into shared memory with mbarrier completion
+// ---- bulk asynchronous copies (cp.async.bulk, the TMA engine) into shared memory, mbarrier completion
 __device__ __forceinline__ uint32_t smem_u32(const void* ptr) { return (uint32_t)__cvta_generic_to_shared(ptr); }
 
 __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
@@ -318,6 +363,7 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes)
     (void)state;
 }
 
+// global -> shared copy of `bytes` (multiple of 16, both addresses 16-byte aligned), no multicast
 __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
 {
     asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
@@ -349,30 +395,45 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
     return true;
 }
 
-// Matrix staged in shared memory: the block's slices are processed in chunks of kChunkSlices
-// consecutive slices (one per warp); thread 0 copies chunk i+2 while the warps work on chunk i
-// (double buffering, completion by mbarrier transaction counts).  Chunks start on 16-byte boundaries
-// and hold a multiple of 16 bytes (slices hold a multiple of 4 entries).
-template <typename VT, bool CPLX, int RPT, int TPR>
+// Prefetch of the vector rows that the columns of a staged record will gather (x_k rows of R
+// complex values, 128-byte lines), spread over the warp's lanes.  Prefetches do not block and hold
+// no registers.
+template <typename VT, int R>
+__device__ __forceinline__ void prefetch_rows(const StepParams& p, const int32_t* cols, int ncols)
+{
+    constexpr int ROWB = R * (int)sizeof(typename V2<VT>::t);
+    const char* x = static_cast<const char*>(p.x_cur);
+    const int lane = threadIdx.x & 31;
+    for (int i = lane; i < ncols; i += 32) {
+        const char* a = x + (size_t)(uint32_t)cols[i] * ROWB;
+#pragma unroll
+        for (int off = 0; off < ROWB; off += 128) {
+            if (p.prefetch == 2) asm volatile("prefetch.global.L1 [%0];" ::"l"(a + off));
+            else asm volatile("prefetch.global.L2 [%0];" ::"l"(a + off));
+        }
+    }
+}
+
+// Matrix records staged in shared memory.  Each warp owns two record buffers and an mbarrier per
+// buffer; its lane 0 copies the record of the warp's next-but-one slice with one bulk copy while the
+// warp works on the current one, so the column indices that the gathers depend on come from shared
+// memory instead of a DRAM round trip per unrolled column batch.  Optionally the warp first
+// prefetches all the vector rows a slice will gather.  Records larger than a buffer (the largest
+// 0.5 %) are read in place.  No block-wide synchronisation in the loop; every wait is bounded (flag
+// bit 2, GBN_ERR_TIMEOUT).
+template <typename VT, bool CPLX, int G, int RPT, int TPR>
 __global__ void __launch_bounds__(256) k_spmm_staged(StepParams p)
 {
     using HT = typename Hop<VT, CPLX>::t;
-    constexpr int SH = 32 / TPR;
+    constexpr int GPW = 32 / TPR;
+    constexpr int R = RPT * TPR;
     extern __shared__ __align__(128) unsigned char dyn[];
-    uint64_t* bar = reinterpret_cast<uint64_t*>(dyn);               // 2 barriers
-    int32_t* scol[2];
-    HT* sval[2];
-    {
-        unsigned char* b = dyn + 128;
-        const size_t ccol = (size_t)p.max_chunk * sizeof(int32_t), cval = (size_t)p.max_chunk * sizeof(HT);
-        scol[0] = reinterpret_cast<int32_t*>(b);
-        sval[0] = reinterpret_cast<HT*>(b + ccol);
-        scol[1] = reinterpret_cast<int32_t*>(b + ccol + cval);
-        sval[1] = reinterpret_cast<HT*>(b + 2 * ccol + cval);
-    }
-    const int q = (threadIdx.x & 31) % TPR;
-    const int sub = (threadIdx.x & 31) / TPR;
+    const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
+    const int q = lane % TPR;
+    const int sub = lane / TPR;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(dyn) + 2 * wib;
+    unsigned char* buf = dyn + 128 + (size_t)wib * 2 * p.cap_record;
     double cb[RPT];
     SliceSums acc_s[RPT];
 #pragma unroll
@@ -380,70 +441,78 @@ __global__ void __launch_bounds__(256) k_spmm_staged(StepParams p)
         cb[t] = p.scal[2 * (q * RPT + t) + 1];
         acc_s[t] = SliceSums{0.0, 0.0, 0.0, 0.0};
     }
-    const int32_t* __restrict__ gcol = p.col;
-    const HT* __restrict__ gval = static_cast<const HT*>(p.val);
-    const int64_t nchunks = (p.nslices + kChunkSlices - 1) / kChunkSlices;
-    const int64_t per = (nchunks + gridDim.x - 1) / gridDim.x;
-    const int64_t c0 = (int64_t)blockIdx.x * per;
-    const int64_t c1 = (c0 + per < nchunks) ? c0 + per : nchunks;
+    const int nwb = (int)(blockDim.x >> 5);
+    const int64_t per = (p.nslices + gridDim.x - 1) / gridDim.x;
+    const int64_t s0 = (int64_t)blockIdx.x * per;
+    const int64_t s1e = (s0 + per < p.nslices) ? s0 + per : p.nslices;
+    const int64_t eb = p.entry_bytes;
 
-    auto issue = [&](int64_t ci, int buf) {
-        const int64_t sa = ci * kChunkSlices;
-        const int64_t sb = (sa + kChunkSlices < p.nslices) ? sa + kChunkSlices : p.nslices;
-        const int64_t e0 = p.slice_ptr[sa], e1 = p.slice_ptr[sb];
-        const uint32_t ne = (uint32_t)(e1 - e0);
-        const uint32_t bc = ne * (uint32_t)sizeof(int32_t), bv = ne * (uint32_t)sizeof(HT);
+    auto rec_bytes = [&](int64_t s) { return (p.slice_ptr[s + 1] - p.slice_ptr[s]) * eb; };
+    auto issue = [&](int64_t s, int st) {   // lane 0 only; records above the cap are not copied
+        const int64_t bytes = rec_bytes(s);
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        mbar_expect_tx(&bar[buf], bc + bv);
-        if (ne) {
-            bulk_g2s(scol[buf], gcol + e0, bc, &bar[buf]);
-            bulk_g2s(sval[buf], gval + e0, bv, &bar[buf]);
-        }
+        const bool copy = bytes > 0 && bytes <= p.cap_record;
+        mbar_expect_tx(&bar[st], copy ? (uint32_t)bytes : 0u);
+        if (copy) bulk_g2s(buf + st * p.cap_record, p.mat + p.slice_ptr[s] * eb, (uint32_t)bytes, &bar[st]);
     };
 
-    if (threadIdx.x == 0) {
+    if (lane == 0) {
         mbar_init(&bar[0], 1);
         mbar_init(&bar[1], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        if (c0 < c1) issue(c0, 0);
-        if (c0 + 1 < c1) issue(c0 + 1, 1);
+    __syncwarp();
+    int64_t s = s0 + wib;
+    uint32_t pending = (s < s1e ? 1u : 0u) | (s + nwb < s1e ? 2u : 0u);   // bit st: a copy into buffer st
+    if (lane == 0) {
+        if (pending & 1u) issue(s, 0);
+        if (pending & 2u) issue(s + nwb, 1);
     }
-    uint32_t phase[2] = {0u, 0u};
+    uint32_t phase = 0u;   // bit st: parity of buffer st's next phase
     bool ok = true;
-    for (int64_t ci = c0; ci < c1; ++ci) {
-        const int buf = (int)((ci - c0) & 1);
-        const bool got = mbar_wait_bounded(&bar[buf], phase[buf]);
-        phase[buf] ^= 1u;
-        if (!__syncthreads_and(got)) {   // uniform exit of the block if a copy never completed
+    for (int it = 0; s < s1e; s += nwb, ++it) {
+        const int st = it & 1;
+        // the record of this slice (copied while the previous one was processed)
+        const bool got = mbar_wait_bounded(&bar[st], (phase >> st) & 1u);
+        if (!__all_sync(0xffffffffu, got)) {   // uniform exit of the warp if a copy never completed
             ok = false;
             break;
         }
-        const int64_t s = ci * kChunkSlices + wib;
-        if (s < p.nslices && wib < kChunkSlices) {
-            const int64_t ebase = p.slice_ptr[ci * kChunkSlices];
-            const int64_t base = p.slice_ptr[s];
-            const int w = (int)((p.slice_ptr[s + 1] - base) / SH);
-            spmm_slice<VT, CPLX, RPT, TPR, FromShared>(p, s, w, scol[buf] + (base - ebase) + sub,
-                                                       sval[buf] + (base - ebase) + sub, cb, acc_s);
+        phase ^= 1u << st;
+        pending &= ~(1u << st);
+        const int64_t base = p.slice_ptr[s];
+        const int w = (int)((p.slice_ptr[s + 1] - base) / GPW);
+        const int64_t bytes = rec_bytes(s);
+        if (bytes <= p.cap_record) {
+            const unsigned char* rec = buf + st * p.cap_record;
+            if (p.prefetch) prefetch_rows<VT, R>(p, reinterpret_cast<const int32_t*>(rec), w * GPW);
+            group_slice<VT, CPLX, G, RPT, TPR, true>(p, s, w, reinterpret_cast<const int32_t*>(rec) + sub,
+                                                     reinterpret_cast<const HT*>(rec + (size_t)w * GPW * 4) + sub * G,
+                                                     cb, acc_s);
+        } else {
+            const unsigned char* rec = p.mat + base * eb;
+            group_slice<VT, CPLX, G, RPT, TPR, false>(p, s, w, reinterpret_cast<const int32_t*>(rec) + sub,
+                                                      reinterpret_cast<const HT*>(rec + (size_t)w * GPW * 4) + sub * G,
+                                                      cb, acc_s);
         }
-        __syncthreads();
-        if (threadIdx.x == 0 && ci + 2 < c1) issue(ci + 2, buf);
+        __syncwarp();   // every lane is done with this buffer before it is refilled
+        if (s + 2 * nwb < s1e) {
+            pending |= 1u << st;
+            if (lane == 0) issue(s + 2 * nwb, st);
+        }
     }
     if (!ok) {
-        if (threadIdx.x == 0) atomicOr(&p.counter[2], 2u);
+        if (lane == 0) atomicOr(&p.counter[2], 2u);
         // let copies still in flight land before the block's shared memory is released
-        mbar_wait_bounded(&bar[0], phase[0]);
-        mbar_wait_bounded(&bar[1], phase[1]);
-        __syncthreads();
+        for (int st = 0; st < 2; ++st)
+            if ((pending >> st) & 1u) mbar_wait_bounded(&bar[st], (phase >> st) & 1u);
+        __syncwarp();
     }
     reduce_and_finalize<RPT, TPR>(p, acc_s);
 }
 
 // ---------------------------------------------------------------------------- start vectors
-// v <- psi (permuted rows), x_prev <- 0; then the first update gives x_1 = psi (a_0 = 0, b_0 = 1).
+// v <- psi (rows in the solver order), x_prev <- 0; then the first update gives x_1 = psi (a_0 = 0, b_0 = 1).
 template <typename VT>
 __global__ void k_start_from_phases(typename V2<VT>::t* v, typename V2<VT>::t* x, const double* u,
                                     const int32_t* perm, int64_t n, int64_t npad, int R, int nrhs_real,
@@ -517,20 +586,13 @@ static void split_rhs(int prec, int R, int want, int* rpt, int* tpr)
     *tpr = R / r;
 }
 
-int rows_per_slice(int prec, int nrhs, int want_rpt)
-{
-    int rpt, tpr;
-    split_rhs(prec, nrhs, want_rpt, &rpt, &tpr);
-    return 32 / tpr;
-}
-
 using StepFn = void (*)(StepParams);
 
-template <typename VT, bool CPLX>
-static StepFn pick(int rpt, int tpr, bool staged)
+template <typename VT, bool CPLX, int G>
+static StepFn pick_g(int rpt, int tpr, bool staged)
 {
 #define GBN_CASE(RP, TP) \
-    if (rpt == RP && tpr == TP) return staged ? k_spmm_staged<VT, CPLX, RP, TP> : k_spmm_step<VT, CPLX, RP, TP>;
+    if (rpt == RP && tpr == TP) return staged ? k_spmm_staged<VT, CPLX, G, RP, TP> : k_spmm_step<VT, CPLX, G, RP, TP>;
     GBN_CASE(1, 1) GBN_CASE(1, 2) GBN_CASE(1, 4) GBN_CASE(1, 8) GBN_CASE(1, 16) GBN_CASE(1, 32)
     GBN_CASE(2, 1) GBN_CASE(2, 2) GBN_CASE(2, 4) GBN_CASE(2, 8) GBN_CASE(2, 16)
     if constexpr (sizeof(VT) == 4) {
@@ -540,42 +602,70 @@ static StepFn pick(int rpt, int tpr, bool staged)
     return nullptr;
 }
 
-static StepFn step_kernel(int prec, bool cplx, int R, int want_rpt, bool staged)
+template <typename VT, bool CPLX>
+static StepFn pick(int G, int rpt, int tpr, bool staged)
+{
+    if (G == 1) return pick_g<VT, CPLX, 1>(rpt, tpr, staged);
+    if (G == 2) return pick_g<VT, CPLX, 2>(rpt, tpr, staged);
+    if (G == 4) return pick_g<VT, CPLX, 4>(rpt, tpr, staged);
+    return nullptr;
+}
+
+static StepFn step_kernel(int prec, bool cplx, int G, int R, int want_rpt, bool staged)
 {
     int rpt, tpr;
     split_rhs(prec, R, want_rpt, &rpt, &tpr);
-    if (prec == GBN_MIXED) return cplx ? pick<float, true>(rpt, tpr, staged) : pick<float, false>(rpt, tpr, staged);
-    return cplx ? pick<double, true>(rpt, tpr, staged) : pick<double, false>(rpt, tpr, staged);
+    if (prec == GBN_MIXED) return cplx ? pick<float, true>(G, rpt, tpr, staged) : pick<float, false>(G, rpt, tpr, staged);
+    return cplx ? pick<double, true>(G, rpt, tpr, staged) : pick<double, false>(G, rpt, tpr, staged);
 }
 
-// dynamic shared memory of the staged kernel: two chunk buffers of column indices and values
-static size_t staged_smem(const gbn_ctx* c)
-{
-    return 128 + 2 * (size_t)c->ell.max_chunk_entries * (sizeof(int32_t) + (size_t)c->ell.val_size);
-}
+// Launch shape of the sparse product.  Staged: warps per block such that two record buffers per warp
+// fit the shared-memory budget (the plain kernel when the block reduction's 4 R threads do not fit).
+struct StepLaunch {
+    StepFn fn = nullptr;
+    int grid = 0, block = 256;
+    size_t smem = 0;
+    bool staged = false;
+};
 
-static bool use_staged(const gbn_ctx* c)
-{
-    if (c->tune_staged == 0) return false;
-    return staged_smem(c) <= 160 * 1024;
-}
+constexpr size_t kStagedSmemBudget = 200 * 1024;
 
-static int step_grid(gbn_ctx* c, StepFn fn, size_t smem)
+static int step_launch(gbn_ctx* c, int R, StepLaunch* L)
 {
+    const Ell& E = c->ell;
+    const size_t per_warp = 2 * (size_t)E.cap_record;
+    const size_t min_warps = (size_t)((4 * R + 31) / 32);
+    const bool staged = c->tune_staged != 0 && per_warp > 0 && 128 + min_warps * per_warp <= kStagedSmemBudget;
+    L->staged = staged;
+    L->fn = step_kernel(c->prec, E.cplx, E.G, R, c->tune_rpt, staged);
+    if (!L->fn) return fail(c, GBN_ERR_ARG, "no recursion kernel for this tile width");
+    L->block = 256;
+    L->smem = 0;
+    if (staged) {
+        size_t nw = (kStagedSmemBudget - 128) / per_warp;
+        nw = nw > 8 ? 8 : nw;   // >= min_warps by the test above
+        L->block = (int)(32 * nw);
+        L->smem = 128 + nw * per_warp;
+        GBN_CK(c, cudaFuncSetAttribute(L->fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L->smem));
+    }
     int per_sm = 0;
-    if (smem > 0) cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 256, smem) != cudaSuccess || per_sm < 1) per_sm = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, L->fn, L->block, L->smem) != cudaSuccess || per_sm < 1)
+        per_sm = 1;
     if (c->tune_blocks_per_sm > 0 && c->tune_blocks_per_sm < per_sm) per_sm = c->tune_blocks_per_sm;
-    return c->num_sms * per_sm;
+    L->grid = c->num_sms * per_sm;
+    return GBN_OK;
 }
 
 int lanczos_prepare(gbn_ctx* c, int prec, int nrhs)
 {
     if (nrhs != 1 && nrhs != 2 && nrhs != 4 && nrhs != 8 && nrhs != 16 && nrhs != 32)
         return fail(c, GBN_ERR_ARG, "internal: tile width must be 1, 2, 4, 8, 16 or 32");
-    const int sh = rows_per_slice(prec, nrhs, c->tune_rpt);
-    if (!c->ell.valid || c->ell.prec != prec || c->ell.sh != sh) {
-        const int rc = build_ell(c, prec, sh);
+    int rpt, tpr;
+    split_rhs(prec, nrhs, c->tune_rpt, &rpt, &tpr);
+    const int gpw = 32 / tpr;
+    const int G = c->tune_group > 0 ? c->tune_group : auto_group(c);
+    if (!c->ell.valid || c->ell.prec != prec || c->ell.gpw != gpw || c->ell.G != G) {
+        const int rc = build_ell(c, prec, G, gpw);
         if (rc) return rc;
     }
     c->prec = prec;
@@ -583,11 +673,10 @@ int lanczos_prepare(gbn_ctx* c, int prec, int nrhs)
     const size_t esz = (prec == GBN_MIXED) ? sizeof(float2) : sizeof(double2);
     const size_t vbytes = (size_t)c->ell.npad * nrhs * esz;
     for (int i = 0; i < 3; ++i) GBN_CK(c, c->vec[i].ensure(vbytes));
-    const bool staged = use_staged(c);
-    StepFn fn = step_kernel(prec, c->ell.cplx, nrhs, c->tune_rpt, staged);
-    if (!fn) return fail(c, GBN_ERR_ARG, "no recursion kernel for this tile width");
-    const int grid = step_grid(c, fn, staged ? staged_smem(c) : 0);
-    GBN_CK(c, c->partials.ensure(sizeof(double) * (size_t)grid * nrhs * 4));
+    StepLaunch L;
+    const int rc = step_launch(c, nrhs, &L);
+    if (rc) return rc;
+    GBN_CK(c, c->partials.ensure(sizeof(double) * (size_t)L.grid * nrhs * 4));
     GBN_CK(c, c->scal.ensure(sizeof(double) * 2 * nrhs));
     GBN_CK(c, c->counter.ensure(sizeof(unsigned int) * 4));
     return GBN_OK;
@@ -601,11 +690,11 @@ int lanczos_start_from_phases(gbn_ctx* c, const double* d_u, int nrhs_real)
     const double isn = 1.0 / sqrt((double)c->n);
     if (c->prec == GBN_MIXED)
         k_start_from_phases<float><<<grd, blk, 0, c->stream>>>(c->vec[0].as<float2>(), c->vec[1].as<float2>(), d_u,
-                                                               c->perm.as<int32_t>(), c->n, c->ell.npad, c->nrhs,
+                                                               c->ell.rperm.as<int32_t>(), c->n, c->ell.npad, c->nrhs,
                                                                nrhs_real, isn);
     else
         k_start_from_phases<double><<<grd, blk, 0, c->stream>>>(c->vec[0].as<double2>(), c->vec[1].as<double2>(),
-                                                                d_u, c->perm.as<int32_t>(), c->n, c->ell.npad,
+                                                                d_u, c->ell.rperm.as<int32_t>(), c->n, c->ell.npad,
                                                                 c->nrhs, nrhs_real, isn);
     GBN_CK_LAUNCH(c);
     return GBN_OK;
@@ -619,11 +708,12 @@ int lanczos_start_from_psi(gbn_ctx* c, const double* d_psi, int nrhs_real)
     if (c->prec == GBN_MIXED)
         k_start_from_psi<float><<<grd, blk, 0, c->stream>>>(c->vec[0].as<float2>(), c->vec[1].as<float2>(),
                                                             reinterpret_cast<const double2*>(d_psi),
-                                                            c->perm.as<int32_t>(), c->n, c->ell.npad, c->nrhs, nrhs_real);
+                                                            c->ell.rperm.as<int32_t>(), c->n, c->ell.npad, c->nrhs,
+                                                            nrhs_real);
     else
         k_start_from_psi<double><<<grd, blk, 0, c->stream>>>(c->vec[0].as<double2>(), c->vec[1].as<double2>(),
                                                              reinterpret_cast<const double2*>(d_psi),
-                                                             c->perm.as<int32_t>(), c->n, c->ell.npad, c->nrhs,
+                                                             c->ell.rperm.as<int32_t>(), c->n, c->ell.npad, c->nrhs,
                                                              nrhs_real);
     GBN_CK_LAUNCH(c);
     return GBN_OK;
@@ -635,16 +725,16 @@ int lanczos_run(gbn_ctx* c, int32_t nmax)
     GBN_CK(c, c->ab.ensure(sizeof(double) * 2 * (size_t)R * nmax));
     k_init_scalars<<<1, 64, 0, c->stream>>>(c->scal.as<double>(), c->counter.as<unsigned int>(), R);
     GBN_CK_LAUNCH(c);
-    const bool staged = use_staged(c);
-    const size_t smem = staged ? staged_smem(c) : 0;
-    StepFn fn = step_kernel(c->prec, c->ell.cplx, R, c->tune_rpt, staged);
-    if (!fn) return fail(c, GBN_ERR_ARG, "no recursion kernel for this tile width");
-    const int grid = step_grid(c, fn, smem);
-    c->last_staged = staged;
+    StepLaunch L;
+    const int rc = step_launch(c, R, &L);
+    if (rc) return rc;
+    c->last_staged = L.staged;
     StepParams p;
     p.slice_ptr = c->ell.slice_ptr.as<int64_t>();
-    p.col = c->ell.col.as<int32_t>();
-    p.val = c->ell.val.p;
+    p.mat = c->ell.mat.as<unsigned char>();
+    p.entry_bytes = c->ell.entry_bytes;
+    p.cap_record = c->ell.cap_record;
+    p.prefetch = c->tune_prefetch;
     p.h0 = c->ell.h0.p;
     p.v_out = c->vec[0].p;
     p.scal = c->scal.as<double>();
@@ -653,10 +743,9 @@ int lanczos_run(gbn_ctx* c, int32_t nmax)
     p.a_out = c->ab.as<double>();
     p.b_out = c->ab.as<double>() + (size_t)R * nmax;
     p.nslices = c->ell.nslices;
-    p.max_chunk = c->ell.max_chunk_entries;
     p.nmax = nmax;
     const int64_t total = c->ell.npad * R;
-    const int ublk = 256;
+    const int ublk = 256;   // a multiple of R (k_update keeps one right-hand side per thread)
     const int ugrid = c->num_sms * 8;
     if (!c->ev0) {
         GBN_CK(c, cudaEventCreate(&c->ev0));
@@ -683,7 +772,7 @@ int lanczos_run(gbn_ctx* c, int32_t nmax)
         if (k < nsample) GBN_CK(c, cudaEventRecord(c->kev[3 * k + 1], c->stream));
         p.x_cur = xcur;
         p.x_prev = xprev;
-        fn<<<grid, 256, smem, c->stream>>>(p);
+        L.fn<<<L.grid, L.block, L.smem, c->stream>>>(p);
         GBN_CK_LAUNCH(c);
         if (k < nsample) GBN_CK(c, cudaEventRecord(c->kev[3 * k + 2], c->stream));
     }

@@ -1,16 +1,18 @@
-// Row order and sliced-ELL layout of the Hamiltonian for the recursion kernels.
+// Row order and grouped sliced-ELL layout of the Hamiltonian for the recursion kernels.
 //
 // Rows are renumbered along a Morton (Z-order) curve over the fractional coordinates of the atoms
 // (cells of about 4 Angstrom), both layers of a bilayer falling into the same cells.  Consecutive
-// slices then touch a compact region of the vectors, so the gathers of neighbouring rows hit L2.
+// slices then touch a compact region of the vectors, so the gathers of neighbouring rows hit L1/L2.
 // The reference's own atom order (kept for all exchanged arrays) is restored at the boundary by the
-// permutation perm[new] = reference index.
+// permutation perm[new] = reference index.  Groups of G consecutive rows then share one list of
+// union columns (the layout is described with struct Ell).
 #include <cuda_runtime.h>
 #include <thrust/device_ptr.h>
 #include <thrust/execution_policy.h>
 #include <thrust/scan.h>
 #include <thrust/sequence.h>
 #include <thrust/sort.h>
+#include <thrust/unique.h>
 
 #include <algorithm>
 #include <vector>
@@ -104,132 +106,298 @@ int build_spatial_perm(gbn_ctx* c)
     return GBN_OK;
 }
 
-// entries of every slice: sh rows times the longest row, the width rounded up so that a slice holds a
-// multiple of 4 entries (every slice then starts on a 16-byte boundary for the bulk copies)
-__global__ void k_slice_width(const int32_t* nneigh, const int32_t* perm, int64_t n, int sh, int64_t nslices,
-                              int64_t* width_x_sh)
+// ---- grouped sliced ELL -------------------------------------------------------------------------
+
+// entry offsets of the rows in the base order (exclusive scan follows)
+__global__ void k_row_counts(const int32_t* nneigh, const int32_t* perm, int64_t n, int64_t* cnt)
+{
+    const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r < n) cnt[r] = nneigh[perm[r]];
+}
+
+// key of every entry: (group of its row in the base order, reference column)
+__global__ void k_group_keys(const int32_t* nneigh, const int32_t* nlist, const int32_t* perm, int64_t n,
+                             int32_t max_neigh, int G, const int64_t* off, uint64_t* keys)
+{
+    const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    const int64_t p = perm[r];
+    const uint64_t g = (uint64_t)(r / G);
+    const int k = nneigh[p];
+    const int64_t o = off[r];
+    for (int j = 0; j < k; ++j) keys[o + j] = (g << 32) | (uint32_t)(nlist[p * max_neigh + j] - 1);
+}
+
+// union columns per group: the sorted keys are unique after thrust::unique; count them per group
+__global__ void k_union_counts(const uint64_t* ukeys, int64_t nu, int32_t* ucount)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < nu) atomicAdd(&ucount[ukeys[i] >> 32], 1);
+}
+
+// Groups are reordered inside windows of kSortWindow full groups by decreasing union size, so that
+// the groups of a slice have similar widths (less padding) while staying spatially close.
+constexpr int kSortWindow = 16;
+
+__global__ void k_group_order(const int32_t* ucount, int64_t ngroups, int64_t nfull, int32_t* gorder)
+{
+    const int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t g0 = w * kSortWindow;
+    if (g0 >= ngroups) return;
+    const int64_t g1 = g0 + kSortWindow <= ngroups ? g0 + kSortWindow : ngroups;
+    int32_t idx[kSortWindow];
+    const int m = (int)(g1 - g0);
+    for (int i = 0; i < m; ++i) idx[i] = (int32_t)(g0 + i);
+    if (g1 <= nfull) {   // only windows of full groups are reordered (stable insertion sort, largest first)
+        for (int i = 1; i < m; ++i) {
+            const int32_t v = idx[i];
+            int j = i - 1;
+            while (j >= 0 && ucount[idx[j]] < ucount[v]) {
+                idx[j + 1] = idx[j];
+                --j;
+            }
+            idx[j + 1] = v;
+        }
+    }
+    for (int i = 0; i < m; ++i) gorder[g0 + i] = idx[i];
+}
+
+__global__ void k_solver_perm(const int32_t* perm, const int32_t* gorder, int64_t n, int G, int32_t* rperm,
+                              int32_t* riperm)
+{
+    const int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (row >= n) return;
+    const int64_t src = (int64_t)gorder[row / G] * G + row % G;   // a row < n of a full group, or the tail
+    const int32_t p = perm[src];
+    rperm[row] = p;
+    riperm[p] = (int32_t)row;
+}
+
+// widths of the slices: the largest union of their groups, rounded up to the column unroll
+__global__ void k_slice_width(const int32_t* ucount, const int32_t* gorder, int64_t ngroups, int gpw, int64_t nslices,
+                              int64_t* entries)
 {
     const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= nslices) return;
     int w = 0;
-    for (int r = 0; r < sh; ++r) {
-        const int64_t row = s * sh + r;
-        if (row < n) {
-            const int k = nneigh[perm[row]];
-            w = k > w ? k : w;
+    for (int j = 0; j < gpw; ++j) {
+        const int64_t g = s * gpw + j;
+        if (g < ngroups) {
+            const int u = ucount[gorder[g]];
+            w = u > w ? u : w;
         }
     }
-    const int unit = sh >= 4 ? 1 : 4 / sh;
-    w = (w + unit - 1) / unit * unit;
-    width_x_sh[s] = (int64_t)w * sh;
+    w = (w + kColUnroll - 1) / kColUnroll * kColUnroll;
+    entries[s] = (int64_t)w * gpw;
 }
 
 template <typename HV>
-__device__ __forceinline__ HV conv_hop(double2 h);
-template <> __device__ __forceinline__ float conv_hop<float>(double2 h) { return (float)h.x; }
-template <> __device__ __forceinline__ double conv_hop<double>(double2 h) { return h.x; }
-template <> __device__ __forceinline__ float2 conv_hop<float2>(double2 h) { return make_float2((float)h.x, (float)h.y); }
-template <> __device__ __forceinline__ double2 conv_hop<double2>(double2 h) { return h; }
-template <typename HV> __device__ __forceinline__ HV zero_hop();
-template <> __device__ __forceinline__ float zero_hop<float>() { return 0.f; }
-template <> __device__ __forceinline__ double zero_hop<double>() { return 0.0; }
-template <> __device__ __forceinline__ float2 zero_hop<float2>() { return make_float2(0.f, 0.f); }
-template <> __device__ __forceinline__ double2 zero_hop<double2>() { return make_double2(0.0, 0.0); }
+__device__ __forceinline__ HV neg_hop(double2 h);
+template <> __device__ __forceinline__ float neg_hop<float>(double2 h) { return (float)(-h.x); }
+template <> __device__ __forceinline__ double neg_hop<double>(double2 h) { return -h.x; }
+template <> __device__ __forceinline__ float2 neg_hop<float2>(double2 h) { return make_float2((float)(-h.x), (float)(-h.y)); }
+template <> __device__ __forceinline__ double2 neg_hop<double2>(double2 h) { return make_double2(-h.x, -h.y); }
+__device__ __forceinline__ void add_to(float& a, float b) { a += b; }
+__device__ __forceinline__ void add_to(double& a, double b) { a += b; }
+__device__ __forceinline__ void add_to(float2& a, float2 b) { a.x += b.x; a.y += b.y; }
+__device__ __forceinline__ void add_to(double2& a, double2 b) { a.x += b.x; a.y += b.y; }
 
+// One thread per group (solver order): union columns, padding columns, values (the records must be
+// zeroed), on-site terms.  An entry that repeats a column of its row (two periodic images of one atom)
+// is added to the same value.
 template <typename HV, typename DV>
-__global__ void k_fill_ell(const int32_t* nneigh, const int32_t* nlist, const double2* hopp, const double* h0,
-                           const int32_t* perm, const int32_t* iperm, int64_t n, int32_t max_neigh, int sh,
-                           int64_t npad, const int64_t* slice_ptr, int32_t* col, HV* val, DV* h0p)
+__global__ void k_fill_groups(const int32_t* nneigh, const int32_t* nlist, const double2* hopp, const double* h0,
+                              const int32_t* rperm, const int32_t* riperm, const int32_t* gorder, const int32_t* ucount,
+                              const int64_t* ustart, const uint64_t* ukeys, int64_t n, int32_t max_neigh, int G,
+                              int gpw, int64_t ngroups, int64_t nslices, const int64_t* slice_ptr, unsigned char* mat,
+                              DV* h0p)
 {
-    const int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (row >= npad) return;
-    const int64_t s = row / sh;
-    const int r = (int)(row % sh);
+    const int64_t ng = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (ng >= nslices * gpw) return;
+    const int64_t s = ng / gpw;
+    const int j = (int)(ng % gpw);
     const int64_t base = slice_ptr[s];
-    const int w = (int)((slice_ptr[s + 1] - base) / sh);
-    int k = 0;
-    if (row < n) {
-        const int64_t p = perm[row];
-        k = nneigh[p];
-        for (int j = 0; j < k; ++j) {
-            const int64_t e = p * max_neigh + j;
-            col[base + (int64_t)j * sh + r] = iperm[nlist[e] - 1];
-            val[base + (int64_t)j * sh + r] = conv_hop<HV>(hopp[e]);
-        }
-        h0p[row] = (DV)h0[p];
-    } else {
-        h0p[row] = (DV)0;
+    const int w = (int)((slice_ptr[s + 1] - base) / gpw);
+    unsigned char* rec = mat + base * (int64_t)(sizeof(int32_t) + G * sizeof(HV));
+    int32_t* col = reinterpret_cast<int32_t*>(rec);
+    HV* val = reinterpret_cast<HV*>(rec + (size_t)w * gpw * sizeof(int32_t));
+    const int64_t row0 = ng * G;
+    int u = 0;
+    const uint64_t* ul = nullptr;
+    if (ng < ngroups) {
+        const int32_t og = gorder[ng];
+        u = ucount[og];
+        ul = ukeys + ustart[og];
     }
-    for (int j = k; j < w; ++j) {
-        col[base + (int64_t)j * sh + r] = (int32_t)row;
-        val[base + (int64_t)j * sh + r] = zero_hop<HV>();
+    for (int k = 0; k < u; ++k) col[k * gpw + j] = riperm[(uint32_t)ul[k]];
+    for (int k = u; k < w; ++k) col[k * gpw + j] = (int32_t)row0;
+    for (int rr = 0; rr < G; ++rr) {
+        const int64_t row = row0 + rr;
+        if (row >= n) {
+            h0p[row] = (DV)0;
+            continue;
+        }
+        const int64_t p = rperm[row];
+        h0p[row] = (DV)h0[p];
+        const int kk = nneigh[p];
+        for (int e = 0; e < kk; ++e) {
+            const uint32_t rc = (uint32_t)(nlist[p * max_neigh + e] - 1);
+            int lo = 0, hi = u;   // lower bound of rc among the group's sorted union columns
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if ((uint32_t)ul[mid] < rc) lo = mid + 1;
+                else hi = mid;
+            }
+            add_to(val[(lo * gpw + j) * G + rr], neg_hop<HV>(hopp[p * max_neigh + e]));
+        }
     }
 }
 
-int build_ell(gbn_ctx* c, int prec, int sh)
+// bytes of the largest slice record
+__global__ void k_max_record(const int64_t* slice_ptr, int64_t nslices, int64_t entry_bytes,
+                             unsigned long long* out)
+{
+    const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < nslices) atomicMax(out, (unsigned long long)((slice_ptr[s + 1] - slice_ptr[s]) * entry_bytes));
+}
+
+// Mean entries per row decide the default group size: the union of a group's columns pays off when
+// neighbouring rows share many columns (bilayers with tens of interlayer neighbours).
+int auto_group(const gbn_ctx* c)
+{
+    const double per_row = c->n > 0 ? (double)c->total / (double)c->n : 0.0;
+    return per_row >= 8.0 ? 2 : 1;
+}
+
+int build_ell(gbn_ctx* c, int prec, int G, int gpw)
 {
     if (!c->have_ham) return fail(c, GBN_ERR_STATE, "no Hamiltonian loaded");
+    if (G != 1 && G != 2 && G != 4) return fail(c, GBN_ERR_ARG, "rows per group must be 1, 2 or 4");
     if (!c->perm.p) {
         const int rc = build_identity_perm(c);
         if (rc) return rc;
     }
     Ell& E = c->ell;
     E.valid = false;
-    E.sh = sh;
+    E.G = G;
+    E.gpw = gpw;
     E.prec = prec;
     E.cplx = c->ham_complex;
-    E.nslices = (c->n + sh - 1) / sh;
-    E.npad = E.nslices * sh;
-    GBN_CK(c, E.slice_ptr.ensure(sizeof(int64_t) * (E.nslices + 1)));
+    const int64_t n = c->n;
+    E.ngroups = (n + G - 1) / G;
+    E.nslices = (E.ngroups + gpw - 1) / gpw;
+    E.npad = E.nslices * gpw * G;
+    const unsigned grn = (unsigned)((n + 255) / 256);
+    const int32_t* nn = c->nneigh.as<int32_t>();
+    const int32_t* nl = c->nlist.as<int32_t>();
+    auto pol = thrust::cuda::par.on(c->stream);
+
+    // entry keys (group, reference column), sorted and made unique: the union of every group
+    DevBuf off, keys, ucount, ustart, gorder, maxbuf;
+    GBN_CK(c, off.ensure(sizeof(int64_t) * (n + 1)));
+    GBN_CK(c, cudaMemsetAsync(off.as<int64_t>() + n, 0, sizeof(int64_t), c->stream));
+    k_row_counts<<<grn, 256, 0, c->stream>>>(nn, c->perm.as<int32_t>(), n, off.as<int64_t>());
+    GBN_CK_LAUNCH(c);
+    thrust::device_ptr<int64_t> op(off.as<int64_t>());
+    thrust::exclusive_scan(pol, op, op + n + 1, op);
+    int64_t nnz = 0;
+    GBN_CK(c, cudaMemcpyAsync(&nnz, off.as<int64_t>() + n, sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream));
+    GBN_CK(c, cudaStreamSynchronize(c->stream));
+    GBN_CK(c, keys.ensure(sizeof(uint64_t) * (size_t)(nnz > 0 ? nnz : 1)));
+    k_group_keys<<<grn, 256, 0, c->stream>>>(nn, nl, c->perm.as<int32_t>(), n, c->max_neigh, G, off.as<int64_t>(),
+                                             keys.as<uint64_t>());
+    GBN_CK_LAUNCH(c);
+    thrust::device_ptr<uint64_t> kp(keys.as<uint64_t>());
+    thrust::sort(pol, kp, kp + nnz);
+    const int64_t nu = thrust::unique(pol, kp, kp + nnz) - kp;
+    c->launches += 8;  // scan, sort and unique passes issued by thrust (setup only)
+    off.release();
+    GBN_CK(c, ucount.ensure(sizeof(int32_t) * (size_t)E.ngroups));
+    GBN_CK(c, cudaMemsetAsync(ucount.p, 0, sizeof(int32_t) * (size_t)E.ngroups, c->stream));
+    if (nu > 0) {
+        k_union_counts<<<(unsigned)((nu + 255) / 256), 256, 0, c->stream>>>(keys.as<uint64_t>(), nu, ucount.as<int32_t>());
+        GBN_CK_LAUNCH(c);
+    }
+    GBN_CK(c, ustart.ensure(sizeof(int64_t) * (size_t)(E.ngroups + 1)));
+    {
+        thrust::device_ptr<int32_t> up(ucount.as<int32_t>());
+        thrust::device_ptr<int64_t> usp(ustart.as<int64_t>());
+        GBN_CK(c, cudaMemsetAsync(ustart.as<int64_t>() + E.ngroups, 0, sizeof(int64_t), c->stream));
+        thrust::exclusive_scan(pol, up, up + E.ngroups, usp, (int64_t)0);
+    }
+
+    // solver row order: groups reordered by union size inside small windows
+    GBN_CK(c, gorder.ensure(sizeof(int32_t) * (size_t)E.ngroups));
+    const int64_t nwin = (E.ngroups + kSortWindow - 1) / kSortWindow;
+    k_group_order<<<(unsigned)((nwin + 127) / 128), 128, 0, c->stream>>>(ucount.as<int32_t>(), E.ngroups, n / G,
+                                                                         gorder.as<int32_t>());
+    GBN_CK_LAUNCH(c);
+    GBN_CK(c, E.rperm.ensure(sizeof(int32_t) * n));
+    GBN_CK(c, E.riperm.ensure(sizeof(int32_t) * n));
+    k_solver_perm<<<grn, 256, 0, c->stream>>>(c->perm.as<int32_t>(), gorder.as<int32_t>(), n, G, E.rperm.as<int32_t>(),
+                                              E.riperm.as<int32_t>());
+    GBN_CK_LAUNCH(c);
+
+    // slices
+    GBN_CK(c, E.slice_ptr.ensure(sizeof(int64_t) * (size_t)(E.nslices + 1)));
     int64_t* sp = E.slice_ptr.as<int64_t>();
     GBN_CK(c, cudaMemsetAsync(sp + E.nslices, 0, sizeof(int64_t), c->stream));
-    k_slice_width<<<(unsigned)((E.nslices + 255) / 256), 256, 0, c->stream>>>(
-        c->nneigh.as<int32_t>(), c->perm.as<int32_t>(), c->n, sh, E.nslices, sp);
+    k_slice_width<<<(unsigned)((E.nslices + 255) / 256), 256, 0, c->stream>>>(ucount.as<int32_t>(), gorder.as<int32_t>(),
+                                                                            E.ngroups, gpw, E.nslices, sp);
     GBN_CK_LAUNCH(c);
     thrust::device_ptr<int64_t> tp(sp);
-    thrust::exclusive_scan(thrust::cuda::par.on(c->stream), tp, tp + E.nslices + 1, tp);
-    c->launches += 2;
+    thrust::exclusive_scan(pol, tp, tp + E.nslices + 1, tp);
     GBN_CK(c, cudaMemcpyAsync(&E.nnz_stored, sp + E.nslices, sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream));
     GBN_CK(c, cudaStreamSynchronize(c->stream));
+
     size_t vsz;
     if (prec == GBN_MIXED) vsz = E.cplx ? sizeof(float2) : sizeof(float);
     else vsz = E.cplx ? sizeof(double2) : sizeof(double);
-    GBN_CK(c, E.col.ensure(sizeof(int32_t) * (size_t)(E.nnz_stored > 0 ? E.nnz_stored : 1)));
-    GBN_CK(c, E.val.ensure(vsz * (size_t)(E.nnz_stored > 0 ? E.nnz_stored : 1)));
+    const size_t eb = sizeof(int32_t) + vsz * G;
+    const size_t ne = (size_t)(E.nnz_stored > 0 ? E.nnz_stored : 1);
+    GBN_CK(c, E.mat.ensure(eb * ne));
+    GBN_CK(c, cudaMemsetAsync(E.mat.p, 0, eb * ne, c->stream));
     GBN_CK(c, E.h0.ensure((prec == GBN_MIXED ? sizeof(float) : sizeof(double)) * (size_t)E.npad));
-    const unsigned grd = (unsigned)((E.npad + 255) / 256);
-    const int32_t* nn = c->nneigh.as<int32_t>();
-    const int32_t* nl = c->nlist.as<int32_t>();
+    const unsigned grg = (unsigned)((E.nslices * gpw + 127) / 128);
     const double2* hp = c->hopp.as<double2>();
     const double* h0 = c->h0.as<double>();
-    const int32_t* pm = c->perm.as<int32_t>();
-    const int32_t* ip = c->iperm.as<int32_t>();
+#define GBN_FILL(HV, DV)                                                                                          \
+    k_fill_groups<HV, DV><<<grg, 128, 0, c->stream>>>(nn, nl, hp, h0, E.rperm.as<int32_t>(), E.riperm.as<int32_t>(), \
+                                                      gorder.as<int32_t>(), ucount.as<int32_t>(), ustart.as<int64_t>(), \
+                                                      keys.as<uint64_t>(), n, c->max_neigh, G, gpw, E.ngroups,         \
+                                                      E.nslices, sp, E.mat.as<unsigned char>(), E.h0.as<DV>())
     if (prec == GBN_MIXED) {
-        if (E.cplx)
-            k_fill_ell<float2, float><<<grd, 256, 0, c->stream>>>(nn, nl, hp, h0, pm, ip, c->n, c->max_neigh, sh, E.npad, sp,
-                                                                  E.col.as<int32_t>(), E.val.as<float2>(), E.h0.as<float>());
-        else
-            k_fill_ell<float, float><<<grd, 256, 0, c->stream>>>(nn, nl, hp, h0, pm, ip, c->n, c->max_neigh, sh, E.npad, sp,
-                                                                 E.col.as<int32_t>(), E.val.as<float>(), E.h0.as<float>());
+        if (E.cplx) GBN_FILL(float2, float);
+        else GBN_FILL(float, float);
     } else {
-        if (E.cplx)
-            k_fill_ell<double2, double><<<grd, 256, 0, c->stream>>>(nn, nl, hp, h0, pm, ip, c->n, c->max_neigh, sh, E.npad,
-                                                                    sp, E.col.as<int32_t>(), E.val.as<double2>(),
-                                                                    E.h0.as<double>());
-        else
-            k_fill_ell<double, double><<<grd, 256, 0, c->stream>>>(nn, nl, hp, h0, pm, ip, c->n, c->max_neigh, sh, E.npad,
-                                                                   sp, E.col.as<int32_t>(), E.val.as<double>(),
-                                                                   E.h0.as<double>());
+        if (E.cplx) GBN_FILL(double2, double);
+        else GBN_FILL(double, double);
     }
+#undef GBN_FILL
     GBN_CK_LAUNCH(c);
-    // largest chunk of kChunkSlices consecutive slices (the unit the staged kernel copies to shared memory)
-    std::vector<int64_t> hsp((size_t)E.nslices + 1);
-    GBN_CK(c, cudaMemcpyAsync(hsp.data(), sp, sizeof(int64_t) * hsp.size(), cudaMemcpyDeviceToHost, c->stream));
+    GBN_CK(c, maxbuf.ensure(sizeof(unsigned long long)));
+    unsigned long long* dmax = maxbuf.as<unsigned long long>();
+    GBN_CK(c, cudaMemsetAsync(dmax, 0, sizeof(unsigned long long), c->stream));
+    k_max_record<<<(unsigned)((E.nslices + 255) / 256), 256, 0, c->stream>>>(sp, E.nslices, (int64_t)eb, dmax);
+    GBN_CK_LAUNCH(c);
+    unsigned long long mr = 0;
+    GBN_CK(c, cudaMemcpyAsync(&mr, dmax, sizeof(mr), cudaMemcpyDeviceToHost, c->stream));
     GBN_CK(c, cudaStreamSynchronize(c->stream));
-    E.max_chunk_entries = 0;
-    for (int64_t a = 0; a < E.nslices; a += kChunkSlices) {
-        const int64_t b = a + kChunkSlices < E.nslices ? a + kChunkSlices : E.nslices;
-        E.max_chunk_entries = std::max(E.max_chunk_entries, hsp[b] - hsp[a]);
+    E.max_record = (int64_t)mr;
+    E.entry_bytes = (int)eb;
+    {   // staging buffer size: the 99.5th percentile of the record sizes
+        std::vector<int64_t> hsp((size_t)E.nslices + 1);
+        GBN_CK(c, cudaMemcpyAsync(hsp.data(), sp, sizeof(int64_t) * hsp.size(), cudaMemcpyDeviceToHost, c->stream));
+        GBN_CK(c, cudaStreamSynchronize(c->stream));
+        std::vector<int64_t> rec((size_t)E.nslices);
+        for (int64_t i = 0; i < E.nslices; ++i) rec[(size_t)i] = (hsp[(size_t)i + 1] - hsp[(size_t)i]) * (int64_t)eb;
+        if (!rec.empty()) {
+            const size_t k = std::min(rec.size() - 1, (size_t)((double)rec.size() * 0.995));
+            std::nth_element(rec.begin(), rec.begin() + (ptrdiff_t)k, rec.end());
+            E.cap_record = (rec[k] + 15) / 16 * 16;
+        } else {
+            E.cap_record = 0;
+        }
     }
     E.val_size = (int)vsz;
     E.valid = true;

@@ -96,10 +96,15 @@ const char* gbn_version(void);
 /* Use the caller's CUDA stream (a cudaStream_t) for all work of the context; NULL = own stream. */
 int         gbn_set_stream(gbn_ctx* ctx, void* cuda_stream);
 /* Tuning of the recursion kernels: right-hand sides per thread (1, 2, 4; 0 = widest load), a cap on
- * resident blocks per SM (0 = occupancy limit) and the sparse-product variant (1 = matrix chunks staged
- * in shared memory by bulk asynchronous copies, 0 = matrix read from global memory, -1 = automatic).
- * Used by the autotuner (grabnes_b200/tune.py). */
-int         gbn_set_tuning(gbn_ctx* ctx, int32_t rhs_per_thread, int32_t blocks_per_sm, int32_t staged);
+ * resident blocks per SM (0 = occupancy limit), the rows per group of the matrix layout (1 = plain
+ * sliced ELL; 2, 4 = neighbouring rows share one gather per union column; 0 = chosen from the mean
+ * entries per row), the matrix path of the sparse product (1 = each warp stages its next slice
+ * records in shared memory with bulk asynchronous copies, 0 = records read from global memory,
+ * -1 = staged when two records per warp fit in shared memory) and, for the staged path, a prefetch of
+ * the vector rows each slice gathers (0 = none, 1 = into L2, 2 = into L1).  Used by the autotuner
+ * (grabnes_b200/tune.py). */
+int         gbn_set_tuning(gbn_ctx* ctx, int32_t rhs_per_thread, int32_t blocks_per_sm, int32_t rows_per_group,
+                           int32_t staged, int32_t prefetch);
 /* Kernels launched by this context since creation (for launch accounting). */
 int64_t     gbn_launch_count(const gbn_ctx* ctx);
 /* Device time of the recursion loop of the last gbn_lanczos* / gbn_run_staged call and its number of

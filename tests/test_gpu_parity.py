@@ -171,17 +171,42 @@ def test_mixed_precision_dos(ctx):
 
 
 @pytest.mark.parametrize("rpt", [1, 2, 4])
-def test_kernel_variants_agree(ctx, rpt):
-    """Matrix staged in shared memory (bulk copies) or read from global memory, for every split of the
-    right-hand sides over threads: the same per-row arithmetic; only the partition of the rows over
-    blocks (and so the order of the FP64 partial sums) differs."""
+def test_layout_variants_agree(ctx, rpt):
+    """Rows per group 1, 2 and 4 of the matrix layout, records staged in shared memory (with and without
+    the gather-row prefetch) or read from global memory, for every split of the right-hand sides over
+    threads: the same products summed in another order (union columns of a group instead of a row's own
+    columns), so mixed-precision a_n, b_n agree to FP32 rounding over 60 steps."""
     r = built("tbg")
     n = r["geo"]["n"]
     ctx.load_hamiltonian(r["nb"]["nneigh"], r["nb"]["nlist"], r["hop"], r["h0"])
     u = np.stack([orc.rng_draws(21 + k, n) for k in range(16)])
     out = []
-    for staged in (0, 1):
-        ctx.set_tuning(rpt, 0, staged)
-        out.append(ctx.lanczos_phases(u, 60, G.GBN_MIXED))
-    ctx.set_tuning(0, 0, -1)
-    assert _rel(out[0][0], out[1][0]) <= 1e-9 and _rel(out[0][1], out[1][1]) <= 1e-9
+    try:
+        for grp in (1, 2, 4):
+            for staged, pf in ((0, 0), (1, 0), (1, 1), (1, 2)):
+                ctx.set_tuning(rpt, 0, grp, staged, pf)
+                out.append(ctx.lanczos_phases(u, 60, G.GBN_MIXED))
+    finally:
+        ctx.set_tuning()
+    for k in range(1, len(out)):
+        assert _rel(out[0][0], out[k][0]) <= 1e-6 and _rel(out[0][1], out[k][1]) <= 1e-6
+
+
+@pytest.mark.parametrize("grp", [1, 2, 4])
+def test_fp64_every_layout(ctx, grp):
+    """FP64 recursion through each matrix layout and matrix path against the oracle (1e-10 relative,
+    200 steps)."""
+    r = built("tbg")
+    n = r["geo"]["n"]
+    psi = orc.init_wf(n, 5)
+    a0, b0 = orc.recursion(r["nb"], r["hop"], r["h0"], psi, 200, 0)
+    ctx.load_hamiltonian(r["nb"]["nneigh"], r["nb"]["nlist"], r["hop"], r["h0"])
+    out = []
+    try:
+        for staged in (0, 1):
+            ctx.set_tuning(0, 0, grp, staged)
+            out.append(ctx.lanczos(psi, 200, G.GBN_FP64))
+    finally:
+        ctx.set_tuning()
+    for a, b in out:
+        assert _rel(a[0], a0) <= 1e-10 and _rel(b[0], b0) <= 1e-10
