@@ -128,13 +128,18 @@ def barrier(ws):
         dist.barrier()
 
 
+PROFILE = os.path.join(ROOT, "profiles", "k_spmm_staged_tbg.md")
+
+
 def traffic_from_profile():
-    """DRAM bytes per recursion-step launch from the committed ncu summary (scaled to this workload)."""
-    path = os.path.join(ROOT, "profiles", "lanczos_step_tbg.json")
+    """DRAM bytes per sparse-product launch at the bench workload, from the committed ncu summary (a
+    capture of the same kernel on the 10 x 10 tiling, scaled by the rows processed)."""
+    import re
     try:
-        with open(path) as f:
-            return float(json.load(f)["dram_bytes_per_launch_full_workload"])
-    except Exception:
+        with open(PROFILE) as f:
+            m = re.search(r"dram_bytes_per_launch_bench_workload\s*=\s*([0-9.eE+]+)", f.read())
+        return float(m.group(1)) if m else None
+    except OSError:
         return None
 
 
@@ -205,13 +210,16 @@ def run_ours(args, ws, rank, local):
         ctx.close()
         return
 
-    # ---- roofline of the sparse-product kernel (the dominant one): algorithmic bytes of one recursion
-    # step = matrix (int32 column + FP32 hopping per entry) + on-site FP32 + 3 vector streams
+    # ---- roofline of the sparse-product kernel (the dominant one).  Its algorithmic bytes are those of a
+    # recursion step: matrix (int32 column + FP32 hopping per entry), on-site FP32 and the three vector
+    # streams (gather of x_k counted once, x_{k-1} read, v_{k+1} written); the update kernel's own stream
+    # is extra traffic of the two-kernel design and is reported with the step time.
     b_alg = nnz * (4 + 4) + n * 4 + NRHS * n * 3 * 8
-    avg_launch_s = spmm_ms / 1e3
-    achieved = b_alg / avg_launch_s / 1e9
+    achieved = b_alg / (spmm_ms / 1e3) / 1e9
     peak, peak_kind = peaks()
     traffic = traffic_from_profile()
+    kname = "k_spmm_{}<float, real, G={}>".format("staged" if best.get("staged", -1) != 0 else "step",
+                                                  best.get("rows_per_group", 0))
 
     # ---- end to end through the C ABI with host buffers (pinned)
     u_pin = torch.from_numpy(u.copy()).pin_memory()
@@ -261,8 +269,9 @@ def run_ours(args, ws, rank, local):
                 "d2h_bytes_per_step": int(a_mix.nbytes + b_mix.nbytes)},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_source": peak_kind, "traffic": traffic, "algorithmic_bytes_per_launch": b_alg,
-                     "kernel": "k_spmm_step<float,real>", "avg_launch_ms": spmm_ms,
-                     "update_kernel_ms": update_ms, "step_ms": kern_ms / kern_launches},
+                     "kernel": kname, "avg_launch_ms": spmm_ms, "update_kernel_ms": update_ms,
+                     "step_ms": kern_ms / kern_launches,
+                     "step_achieved": b_alg / (kern_ms / kern_launches / 1e3) / 1e9},
         "tuning": best,
         "fp64": {"batched_atom_steps_per_s": atom_steps / (fp64_batched_kernel_ms / 1e3),
                  "single_vector_atom_steps_per_s": float(n) * nsteps / (fp64_single_kernel_ms / 1e3),

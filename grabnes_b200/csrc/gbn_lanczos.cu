@@ -52,12 +52,14 @@ struct StepParams {
 
 // ---------------------------------------------------------------------------- vector loads
 template <typename VT, int RPT> struct VecIO;
+// 32-byte loads are single 256-bit instructions (ld.global.v8 / v4.f64, sm_100): the TPR threads of a
+// row group then read a whole 128-byte row in one instruction, one L1 wavefront per row
 template <> struct VecIO<float, 4> {
     static __device__ __forceinline__ void load(const float2* p, float2 o[4]) {
-        const float4 a = __ldg(reinterpret_cast<const float4*>(p));
-        const float4 b = __ldg(reinterpret_cast<const float4*>(p) + 1);
-        o[0] = make_float2(a.x, a.y); o[1] = make_float2(a.z, a.w);
-        o[2] = make_float2(b.x, b.y); o[3] = make_float2(b.z, b.w);
+        asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+            : "=f"(o[0].x), "=f"(o[0].y), "=f"(o[1].x), "=f"(o[1].y), "=f"(o[2].x), "=f"(o[2].y), "=f"(o[3].x),
+              "=f"(o[3].y)
+            : "l"(p));
     }
     static __device__ __forceinline__ void store(float2* p, const float2 o[4]) {
         reinterpret_cast<float4*>(p)[0] = make_float4(o[0].x, o[0].y, o[1].x, o[1].y);
@@ -78,7 +80,11 @@ template <> struct VecIO<float, 1> {
     static __device__ __forceinline__ void store(float2* p, const float2 o[1]) { p[0] = o[0]; }
 };
 template <> struct VecIO<double, 2> {
-    static __device__ __forceinline__ void load(const double2* p, double2 o[2]) { o[0] = __ldg(p); o[1] = __ldg(p + 1); }
+    static __device__ __forceinline__ void load(const double2* p, double2 o[2]) {
+        asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];"
+            : "=d"(o[0].x), "=d"(o[0].y), "=d"(o[1].x), "=d"(o[1].y)
+            : "l"(p));
+    }
     static __device__ __forceinline__ void store(double2* p, const double2 o[2]) { p[0] = o[0]; p[1] = o[1]; }
 };
 template <> struct VecIO<double, 1> {
