@@ -116,7 +116,7 @@ def _declare(L):
     L.gbn_run_staged.argtypes = [vp, i32, _opt(np.float64), _opt(np.float64)]
     L.gbn_cf_dos.argtypes = [vp, i32, _p(np.float64), _p(np.float64), _opt(np.int32), i32, d, i32, d, d,
                              _opt(np.float64), _opt(np.float64), _p(np.float64)]
-    L.gbn_cheb_evolve.argtypes = [vp, i32, _p(np.complex128), i32, d, d, _p(np.complex128)]
+    L.gbn_cheb_evolve.argtypes = [vp, i32, i32, _p(np.complex128), i32, d, d, _p(np.complex128)]
     L.gbn_kubo_evol.argtypes = [vp, i32, _p(np.complex128), i32, d, d, i32, _p(np.complex128), _p(np.complex128)]
     L.gbn_set_neighd.argtypes = [vp, _p(np.float64)]
     # device pointers (ints from tensor.data_ptr()), no context
@@ -280,10 +280,10 @@ class Context:
         return e, dos
 
     # ---------------------------------------------------------------- Chebyshev
-    def cheb_evolve(self, c, ac, bc, z):
+    def cheb_evolve(self, c, ac, bc, z, precision=GBN_FP64):
         zz = np.ascontiguousarray(np.atleast_2d(z), np.complex128).copy()
         cc = _c(c, np.complex128)
-        self._ck(self._L.gbn_cheb_evolve(self._h, zz.shape[0], cc, len(cc), ac, bc, zz.reshape(-1)))
+        self._ck(self._L.gbn_cheb_evolve(self._h, precision, zz.shape[0], cc, len(cc), ac, bc, zz.reshape(-1)))
         return zz
 
     def kubo_evol(self, c, ac, bc, psi, zupsi, direction=1):

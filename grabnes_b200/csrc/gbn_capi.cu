@@ -472,13 +472,12 @@ int gbn_cf_dos(gbn_ctx* c, int32_t nrhs, const double* a, const double* b, const
     return GBN_OK;
 }
 
-int gbn_cheb_evolve(gbn_ctx* c, int32_t nrhs, const double* coef, int32_t npol, double ac, double bc, double* z)
+int gbn_cheb_evolve(gbn_ctx* c, int32_t precision, int32_t nrhs, const double* coef, int32_t npol, double ac, double bc,
+                    double* z)
 {
     if (!c) return GBN_ERR_ARG;
-    if (!c->have_ham) return fail(c, GBN_ERR_STATE, "no Hamiltonian");
-    if (nrhs < 1 || npol < 1 || !coef || !z || !(bc > 0.0)) return fail(c, GBN_ERR_ARG, "bad Chebyshev arguments");
     cudaSetDevice(c->device);
-    return cheb_evolve(c, nrhs, coef, npol, ac, bc, z);
+    return cheb_evolve(c, precision, nrhs, coef, npol, ac, bc, z);
 }
 
 int gbn_kubo_evol(gbn_ctx* c, int32_t nrhs, const double* coef, int32_t npol, double ac, double bc, int32_t dir,

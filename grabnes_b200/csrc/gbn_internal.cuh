@@ -169,6 +169,8 @@ int lanczos_prepare(gbn_ctx* c, int prec, int nrhs);
 int lanczos_start_from_phases(gbn_ctx* c, const double* d_u, int nrhs_real);
 int lanczos_start_from_psi(gbn_ctx* c, const double* d_psi, int nrhs_real);
 int lanczos_run(gbn_ctx* c, int32_t nmax);
+// right-hand sides per thread and threads per row group for a tile of R vectors
+void split_rhs(int prec, int R, int want, int* rpt, int* tpr);
 
 // continued fraction (gbn_cf.cu)
 int cf_dos(gbn_ctx* c, int32_t nrhs, const double* d_a, const double* d_b, const int32_t* d_nsteps, int32_t nmax,
@@ -180,7 +182,8 @@ int assemble(gbn_ctx* c, const gbn_model* m, const double* d_rat_on, const doubl
 int peierls(gbn_ctx* c, double flux);
 
 // Chebyshev (gbn_cheb.cu)
-int cheb_evolve(gbn_ctx* c, int32_t nrhs, const double* c_host, int32_t npol, double ac, double bc, double* z_host);
+int cheb_evolve(gbn_ctx* c, int32_t prec, int32_t nrhs, const double* c_host, int32_t npol, double ac, double bc,
+                double* z_host);
 int kubo_evol(gbn_ctx* c, int32_t nrhs, const double* c_host, int32_t npol, double ac, double bc, int32_t dir,
               double* psi_host, double* zupsi_host);
 

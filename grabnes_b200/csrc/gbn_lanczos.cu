@@ -23,13 +23,9 @@
 #include <math.h>
 #include <string.h>
 
-#include "gbn_internal.cuh"
+#include "gbn_spmm.cuh"
 
 namespace gbn {
-
-template <typename VT> struct V2;
-template <> struct V2<float> { using t = float2; };
-template <> struct V2<double> { using t = double2; };
 
 struct StepParams {
     const int64_t* slice_ptr;
@@ -49,103 +45,6 @@ struct StepParams {
     int64_t nslices;
     int32_t nmax;
 };
-
-// ---------------------------------------------------------------------------- vector loads
-template <typename VT, int RPT> struct VecIO;
-// 32-byte loads are single 256-bit instructions (ld.global.v8 / v4.f64, sm_100): the TPR threads of a
-// row group then read a whole 128-byte row in one instruction, one L1 wavefront per row
-template <> struct VecIO<float, 4> {
-    static __device__ __forceinline__ void load(const float2* p, float2 o[4]) {
-        asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-            : "=f"(o[0].x), "=f"(o[0].y), "=f"(o[1].x), "=f"(o[1].y), "=f"(o[2].x), "=f"(o[2].y), "=f"(o[3].x),
-              "=f"(o[3].y)
-            : "l"(p));
-    }
-    static __device__ __forceinline__ void store(float2* p, const float2 o[4]) {
-        reinterpret_cast<float4*>(p)[0] = make_float4(o[0].x, o[0].y, o[1].x, o[1].y);
-        reinterpret_cast<float4*>(p)[1] = make_float4(o[2].x, o[2].y, o[3].x, o[3].y);
-    }
-};
-template <> struct VecIO<float, 2> {
-    static __device__ __forceinline__ void load(const float2* p, float2 o[2]) {
-        const float4 a = __ldg(reinterpret_cast<const float4*>(p));
-        o[0] = make_float2(a.x, a.y); o[1] = make_float2(a.z, a.w);
-    }
-    static __device__ __forceinline__ void store(float2* p, const float2 o[2]) {
-        reinterpret_cast<float4*>(p)[0] = make_float4(o[0].x, o[0].y, o[1].x, o[1].y);
-    }
-};
-template <> struct VecIO<float, 1> {
-    static __device__ __forceinline__ void load(const float2* p, float2 o[1]) { o[0] = __ldg(p); }
-    static __device__ __forceinline__ void store(float2* p, const float2 o[1]) { p[0] = o[0]; }
-};
-template <> struct VecIO<double, 2> {
-    static __device__ __forceinline__ void load(const double2* p, double2 o[2]) {
-        asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];"
-            : "=d"(o[0].x), "=d"(o[0].y), "=d"(o[1].x), "=d"(o[1].y)
-            : "l"(p));
-    }
-    static __device__ __forceinline__ void store(double2* p, const double2 o[2]) { p[0] = o[0]; p[1] = o[1]; }
-};
-template <> struct VecIO<double, 1> {
-    static __device__ __forceinline__ void load(const double2* p, double2 o[1]) { o[0] = __ldg(p); }
-    static __device__ __forceinline__ void store(double2* p, const double2 o[1]) { p[0] = o[0]; }
-};
-
-// hopping value types: real VT or complex V2<VT>; values are stored negated, so products are added
-template <typename VT, bool CPLX> struct Hop;
-template <> struct Hop<float, false> {
-    using t = float;
-    // packed FP32 (one FFMA2 for the real and imaginary parts)
-    static __device__ __forceinline__ void madd(float2& acc, float h, float2 x) {
-        acc = __ffma2_rn(make_float2(h, h), x, acc);
-    }
-};
-template <> struct Hop<double, false> {
-    using t = double;
-    static __device__ __forceinline__ void madd(double2& acc, double h, double2 x) {
-        acc.x = fma(h, x.x, acc.x);
-        acc.y = fma(h, x.y, acc.y);
-    }
-};
-template <typename VT> struct Hop<VT, true> {
-    using t = typename V2<VT>::t;
-    static __device__ __forceinline__ void madd(typename V2<VT>::t& acc, t h, typename V2<VT>::t x) {
-        acc.x = fma(h.x, x.x, acc.x);
-        acc.x = fma(-h.y, x.y, acc.x);
-        acc.y = fma(h.x, x.y, acc.y);
-        acc.y = fma(h.y, x.x, acc.y);
-    }
-};
-
-// G consecutive values of one union column (G * sizeof(HT) = 4..64 bytes, naturally aligned), read
-// with the widest loads: from global memory once and evicted first (the matrix is streamed every
-// step), or from shared memory
-template <typename HT, int G, bool SMEM>
-__device__ __forceinline__ void load_group_vals(const HT* p, HT (&h)[G])
-{
-    constexpr int B = G * (int)sizeof(HT);
-    if constexpr (B % 16 == 0) {
-        uint4 t[B / 16];
-#pragma unroll
-        for (int i = 0; i < B / 16; ++i) {
-            if constexpr (SMEM) t[i] = reinterpret_cast<const uint4*>(p)[i];
-            else t[i] = __ldcs(reinterpret_cast<const uint4*>(p) + i);
-        }
-        memcpy(h, t, B);
-    } else if constexpr (B == 8) {
-        uint2 t;
-        if constexpr (SMEM) t = *reinterpret_cast<const uint2*>(p);
-        else t = __ldcs(reinterpret_cast<const uint2*>(p));
-        memcpy(h, &t, B);
-    } else {
-        static_assert(B == 4, "value group of 4, 8 or a multiple of 16 bytes");
-        unsigned int t;
-        if constexpr (SMEM) t = *reinterpret_cast<const unsigned int*>(p);
-        else t = __ldcs(reinterpret_cast<const unsigned int*>(p));
-        memcpy(h, &t, B);
-    }
-}
 
 // ---------------------------------------------------------------------------- update kernel
 // x_k = (v_k - a x_{k-1}) * (1/b) for all rows and right-hand sides (streaming).  The grid stride and
@@ -258,10 +157,8 @@ __device__ __forceinline__ void group_slice(const StepParams& p, int64_t s, int 
                                             SliceSums* acc_s)
 {
     using C2 = typename V2<VT>::t;
-    using HT = typename Hop<VT, CPLX>::t;
     constexpr int GPW = 32 / TPR;
     constexpr int R = RPT * TPR;
-    constexpr int U = kColUnroll;
     const int lane = threadIdx.x & 31;
     const int sub = lane / TPR;
     const int q = lane % TPR;
@@ -269,34 +166,9 @@ __device__ __forceinline__ void group_slice(const StepParams& p, int64_t s, int 
     const C2* __restrict__ xp = static_cast<const C2*>(p.x_prev);
     C2* __restrict__ vout = static_cast<C2*>(p.v_out);
     const VT* __restrict__ h0 = static_cast<const VT*>(p.h0);
-    const C2* __restrict__ xq = xc + q * RPT;
     const int64_t row0 = (s * GPW + sub) * G;
     C2 acc[G][RPT];
-#pragma unroll
-    for (int g = 0; g < G; ++g)
-#pragma unroll
-        for (int t = 0; t < RPT; ++t) { acc[g][t].x = 0; acc[g][t].y = 0; }
-    for (int k = 0; k < w; k += U) {
-        int32_t c[U];
-        HT h[U][G];
-        C2 xg[U][RPT];
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-            if constexpr (SMEM) c[u] = cp[u * GPW];
-            else c[u] = __ldcs(cp + u * GPW);
-            load_group_vals<HT, G, SMEM>(vp + u * GPW * G, h[u]);
-        }
-#pragma unroll
-        for (int u = 0; u < U; ++u) VecIO<VT, RPT>::load(xq + (size_t)(uint32_t)c[u] * R, xg[u]);
-#pragma unroll
-        for (int u = 0; u < U; ++u)
-#pragma unroll
-            for (int g = 0; g < G; ++g)
-#pragma unroll
-                for (int t = 0; t < RPT; ++t) Hop<VT, CPLX>::madd(acc[g][t], h[u][g], xg[u][t]);
-        cp += U * GPW;
-        vp += U * GPW * G;
-    }
+    group_columns<VT, CPLX, G, RPT, TPR, SMEM>(xc, w, cp, vp, acc);
     // epilogue per row: the on-site term (own x_k row, loaded here so that it holds no registers during
     // the column loop), then v_{k+1} and the dot-product terms in FP64
 #pragma unroll
@@ -582,7 +454,7 @@ __global__ void k_init_scalars(double* scal, unsigned int* counter, int R)
 
 // ---------------------------------------------------------------------------- host side
 // right-hand sides per thread: the widest vector load (32 bytes) unless the tuning asks for fewer
-static void split_rhs(int prec, int R, int want, int* rpt, int* tpr)
+void split_rhs(int prec, int R, int want, int* rpt, int* tpr)
 {
     const int maxr = (prec == GBN_MIXED) ? 4 : 2;
     int r = R < maxr ? R : maxr;

@@ -1,0 +1,160 @@
+// Device building blocks shared by the recursion and the Chebyshev kernels: vector loads, the product
+// of a stored hopping with a gathered vector element, and the union-column loop of the grouped sliced
+// ELL (struct Ell): y[g][t] = sum over the group's union columns of val[g] * x[col][t].
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string.h>
+
+#include "gbn_internal.cuh"
+
+namespace gbn {
+
+template <typename VT> struct V2;
+template <> struct V2<float> { using t = float2; };
+template <> struct V2<double> { using t = double2; };
+
+// ---------------------------------------------------------------------------- vector loads
+template <typename VT, int RPT> struct VecIO;
+// 32-byte loads are single 256-bit instructions (ld.global.v8 / v4.f64, sm_100): the TPR threads of a
+// row group then read a whole 128-byte row in one instruction, one L1 wavefront per row
+template <> struct VecIO<float, 4> {
+    static __device__ __forceinline__ void load(const float2* p, float2 o[4]) {
+        asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+            : "=f"(o[0].x), "=f"(o[0].y), "=f"(o[1].x), "=f"(o[1].y), "=f"(o[2].x), "=f"(o[2].y), "=f"(o[3].x),
+              "=f"(o[3].y)
+            : "l"(p));
+    }
+    static __device__ __forceinline__ void store(float2* p, const float2 o[4]) {
+        reinterpret_cast<float4*>(p)[0] = make_float4(o[0].x, o[0].y, o[1].x, o[1].y);
+        reinterpret_cast<float4*>(p)[1] = make_float4(o[2].x, o[2].y, o[3].x, o[3].y);
+    }
+};
+template <> struct VecIO<float, 2> {
+    static __device__ __forceinline__ void load(const float2* p, float2 o[2]) {
+        const float4 a = __ldg(reinterpret_cast<const float4*>(p));
+        o[0] = make_float2(a.x, a.y); o[1] = make_float2(a.z, a.w);
+    }
+    static __device__ __forceinline__ void store(float2* p, const float2 o[2]) {
+        reinterpret_cast<float4*>(p)[0] = make_float4(o[0].x, o[0].y, o[1].x, o[1].y);
+    }
+};
+template <> struct VecIO<float, 1> {
+    static __device__ __forceinline__ void load(const float2* p, float2 o[1]) { o[0] = __ldg(p); }
+    static __device__ __forceinline__ void store(float2* p, const float2 o[1]) { p[0] = o[0]; }
+};
+template <> struct VecIO<double, 2> {
+    static __device__ __forceinline__ void load(const double2* p, double2 o[2]) {
+        asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];"
+            : "=d"(o[0].x), "=d"(o[0].y), "=d"(o[1].x), "=d"(o[1].y)
+            : "l"(p));
+    }
+    static __device__ __forceinline__ void store(double2* p, const double2 o[2]) { p[0] = o[0]; p[1] = o[1]; }
+};
+template <> struct VecIO<double, 1> {
+    static __device__ __forceinline__ void load(const double2* p, double2 o[1]) { o[0] = __ldg(p); }
+    static __device__ __forceinline__ void store(double2* p, const double2 o[1]) { p[0] = o[0]; }
+};
+
+// hopping value types: real VT or complex V2<VT>; values are stored negated, so products are added
+template <typename VT, bool CPLX> struct Hop;
+template <> struct Hop<float, false> {
+    using t = float;
+    // packed FP32 (one FFMA2 for the real and imaginary parts)
+    static __device__ __forceinline__ void madd(float2& acc, float h, float2 x) {
+        acc = __ffma2_rn(make_float2(h, h), x, acc);
+    }
+};
+template <> struct Hop<double, false> {
+    using t = double;
+    static __device__ __forceinline__ void madd(double2& acc, double h, double2 x) {
+        acc.x = fma(h, x.x, acc.x);
+        acc.y = fma(h, x.y, acc.y);
+    }
+};
+template <typename VT> struct Hop<VT, true> {
+    using t = typename V2<VT>::t;
+    static __device__ __forceinline__ void madd(typename V2<VT>::t& acc, t h, typename V2<VT>::t x) {
+        acc.x = fma(h.x, x.x, acc.x);
+        acc.x = fma(-h.y, x.y, acc.x);
+        acc.y = fma(h.x, x.y, acc.y);
+        acc.y = fma(h.y, x.x, acc.y);
+    }
+};
+
+// G consecutive values of one union column (G * sizeof(HT) = 4..64 bytes, naturally aligned), read
+// with the widest loads: from global memory once and evicted first (the matrix is streamed every
+// step), or from shared memory
+template <typename HT, int G, bool SMEM>
+__device__ __forceinline__ void load_group_vals(const HT* p, HT (&h)[G])
+{
+    constexpr int B = G * (int)sizeof(HT);
+    if constexpr (B % 16 == 0) {
+        uint4 t[B / 16];
+#pragma unroll
+        for (int i = 0; i < B / 16; ++i) {
+            if constexpr (SMEM) t[i] = reinterpret_cast<const uint4*>(p)[i];
+            else t[i] = __ldcs(reinterpret_cast<const uint4*>(p) + i);
+        }
+        memcpy(h, t, B);
+    } else if constexpr (B == 8) {
+        uint2 t;
+        if constexpr (SMEM) t = *reinterpret_cast<const uint2*>(p);
+        else t = __ldcs(reinterpret_cast<const uint2*>(p));
+        memcpy(h, &t, B);
+    } else {
+        static_assert(B == 4, "value group of 4, 8 or a multiple of 16 bytes");
+        unsigned int t;
+        if constexpr (SMEM) t = *reinterpret_cast<const unsigned int*>(p);
+        else t = __ldcs(reinterpret_cast<const unsigned int*>(p));
+        memcpy(h, &t, B);
+    }
+}
+
+// The union-column loop of one group: GPW = 32/TPR groups per slice; the TPR threads of a group each
+// hold RPT right-hand sides of all G rows of the group.  Per union column a thread reads the column
+// index and the G values (same address for the group's threads) and gathers RPT vector elements of that
+// column once for all G rows.  cp/vp point at the thread's group in the slice record, in global memory
+// (streamed, evict-first) or in shared memory (SMEM); w is the slice width (a multiple of 4).
+template <typename VT, bool CPLX, int G, int RPT, int TPR, bool SMEM>
+__device__ __forceinline__ void group_columns(const typename V2<VT>::t* __restrict__ x, int w,
+                                              const int32_t* __restrict__ cp,
+                                              const typename Hop<VT, CPLX>::t* __restrict__ vp,
+                                              typename V2<VT>::t (&acc)[G][RPT])
+{
+    using C2 = typename V2<VT>::t;
+    using HT = typename Hop<VT, CPLX>::t;
+    constexpr int GPW = 32 / TPR;
+    constexpr int R = RPT * TPR;
+    constexpr int U = kColUnroll;
+    const int q = (threadIdx.x & 31) % TPR;
+    const C2* __restrict__ xq = x + q * RPT;
+#pragma unroll
+    for (int g = 0; g < G; ++g)
+#pragma unroll
+        for (int t = 0; t < RPT; ++t) { acc[g][t].x = 0; acc[g][t].y = 0; }
+    for (int k = 0; k < w; k += U) {
+        int32_t c[U];
+        HT h[U][G];
+        C2 xg[U][RPT];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            if constexpr (SMEM) c[u] = cp[u * GPW];
+            else c[u] = __ldcs(cp + u * GPW);
+            load_group_vals<HT, G, SMEM>(vp + u * GPW * G, h[u]);
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) VecIO<VT, RPT>::load(xq + (size_t)(uint32_t)c[u] * R, xg[u]);
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+#pragma unroll
+            for (int g = 0; g < G; ++g)
+#pragma unroll
+                for (int t = 0; t < RPT; ++t) Hop<VT, CPLX>::madd(acc[g][t], h[u][g], xg[u][t]);
+        cp += U * GPW;
+        vp += U * GPW * G;
+    }
+}
+
+}  // namespace gbn

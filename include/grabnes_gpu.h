@@ -168,10 +168,13 @@ int gbn_cf_dos(gbn_ctx* ctx, int32_t nrhs, const double* a, const double* b, con
                double* energy, double* dos);
 
 /* ---- Chebyshev time evolution --------------------------------------------------------------- */
-/* KuboChebyshevEvolve (kubosubs.F90:557-619): z <- sum_n c_n T_n((H-ac)/bc) z for nrhs complex
- * vectors z [nrhs][N] (host, in place), c complex [npol]. */
-int gbn_cheb_evolve(gbn_ctx* ctx, int32_t nrhs, const double* c, int32_t npol, double ac, double bc,
-                    double* z);
+/* KuboChebyshevEvolve (kubosubs.F90:557-619) for nrhs complex vectors z [nrhs][N] (host, reference atom
+ * order, in place): with x = (H - ac)/(2 bc), psi_0 = sqrt(2) z, psi_1 = x psi_0,
+ * psi_{n+1} = 2 x psi_n - psi_{n-1}, z <- c_0 z + sum_{n=1}^{npol-1} c_n psi_n; c complex [npol] (the
+ * coefficients of KuboCn).  precision: GBN_FP64, or GBN_MIXED (complex FP32 psi_n, FP64 step
+ * arithmetic and FP64 accumulation of z). */
+int gbn_cheb_evolve(gbn_ctx* ctx, int32_t precision, int32_t nrhs, const double* c, int32_t npol, double ac,
+                    double bc, double* z);
 /* KuboEvol (kubosubs.F90:438-553): psi <- U psi and zupsi <- U zupsi + [U, X] psi, X along
  * dir (1 = x, 2 = y) from NeighD; needs gbn_neighbours or NeighD through gbn_set_neighd. */
 int gbn_kubo_evol(gbn_ctx* ctx, int32_t nrhs, const double* c, int32_t npol, double ac, double bc,
