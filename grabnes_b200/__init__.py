@@ -117,7 +117,8 @@ def _declare(L):
     L.gbn_cf_dos.argtypes = [vp, i32, _p(np.float64), _p(np.float64), _opt(np.int32), i32, d, i32, d, d,
                              _opt(np.float64), _opt(np.float64), _p(np.float64)]
     L.gbn_cheb_evolve.argtypes = [vp, i32, i32, _p(np.complex128), i32, d, d, _p(np.complex128)]
-    L.gbn_kubo_evol.argtypes = [vp, i32, _p(np.complex128), i32, d, d, i32, _p(np.complex128), _p(np.complex128)]
+    L.gbn_kubo_evol.argtypes = [vp, i32, i32, _p(np.complex128), i32, d, d, i32, _p(np.complex128),
+                                _p(np.complex128)]
     L.gbn_set_neighd.argtypes = [vp, _p(np.float64)]
     # device pointers (ints from tensor.data_ptr()), no context
     L.gbn_lanczos_noalloc.argtypes = [i64, i32, vp, vp, vp, vp, vp, i32, vp, vp, vp]
@@ -286,11 +287,11 @@ class Context:
         self._ck(self._L.gbn_cheb_evolve(self._h, precision, zz.shape[0], cc, len(cc), ac, bc, zz.reshape(-1)))
         return zz
 
-    def kubo_evol(self, c, ac, bc, psi, zupsi, direction=1):
+    def kubo_evol(self, c, ac, bc, psi, zupsi, direction=1, precision=GBN_FP64):
         p = np.ascontiguousarray(np.atleast_2d(psi), np.complex128).copy()
         z = np.ascontiguousarray(np.atleast_2d(zupsi), np.complex128).copy()
         cc = _c(c, np.complex128)
-        self._ck(self._L.gbn_kubo_evol(self._h, p.shape[0], cc, len(cc), ac, bc, direction, p.reshape(-1),
+        self._ck(self._L.gbn_kubo_evol(self._h, precision, p.shape[0], cc, len(cc), ac, bc, direction, p.reshape(-1),
                                        z.reshape(-1)))
         return p, z
 

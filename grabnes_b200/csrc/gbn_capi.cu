@@ -135,7 +135,7 @@ int gbn_destroy(gbn_ctx* c)
     if (c->stream) cudaStreamSynchronize(c->stream);
     DevBuf* bufs[] = {&c->rat, &c->species, &c->layer, &c->nneigh, &c->nlist, &c->neighd, &c->ncell, &c->h0,
                       &c->hopp, &c->rat_hop, &c->perm, &c->iperm, &c->ell.slice_ptr, &c->ell.mat,
-                      &c->ell.h0, &c->ell.rperm, &c->ell.riperm, &c->partials, &c->scal, &c->counter, &c->ab, &c->upload};
+                      &c->ell.h0, &c->ell.rperm, &c->ell.riperm, &c->ell.dval, &c->partials, &c->scal, &c->counter, &c->ab, &c->upload};
     for (DevBuf* b : bufs) b->release();
     for (auto& v : c->vec) v.release();
     for (auto& v : c->cheb) v.release();
@@ -480,8 +480,8 @@ int gbn_cheb_evolve(gbn_ctx* c, int32_t precision, int32_t nrhs, const double* c
     return cheb_evolve(c, precision, nrhs, coef, npol, ac, bc, z);
 }
 
-int gbn_kubo_evol(gbn_ctx* c, int32_t nrhs, const double* coef, int32_t npol, double ac, double bc, int32_t dir,
-                  double* psi, double* zupsi)
+int gbn_kubo_evol(gbn_ctx* c, int32_t precision, int32_t nrhs, const double* coef, int32_t npol, double ac, double bc,
+                  int32_t dir, double* psi, double* zupsi)
 {
     if (!c) return GBN_ERR_ARG;
     if (!c->have_ham) return fail(c, GBN_ERR_STATE, "no Hamiltonian");
@@ -489,7 +489,7 @@ int gbn_kubo_evol(gbn_ctx* c, int32_t nrhs, const double* coef, int32_t npol, do
     if (dir != 1 && dir != 2) return fail(c, GBN_ERR_ARG, "dir must be 1 (x) or 2 (y)");
     if (nrhs < 1 || npol < 1 || !coef || !psi || !zupsi || !(bc > 0.0)) return fail(c, GBN_ERR_ARG, "bad KuboEvol arguments");
     cudaSetDevice(c->device);
-    return kubo_evol(c, nrhs, coef, npol, ac, bc, dir, psi, zupsi);
+    return kubo_evol(c, precision, nrhs, coef, npol, ac, bc, dir, psi, zupsi);
 }
 
 }  // extern "C"

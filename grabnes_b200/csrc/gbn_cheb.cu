@@ -236,9 +236,348 @@ int cheb_evolve(gbn_ctx* c, int32_t prec, int32_t nrhs, const double* c_host, in
     return GBN_OK;
 }
 
-int kubo_evol(gbn_ctx* c, int32_t, const double*, int32_t, double, double, int32_t, double*, double*)
+// ---------------------------------------------------------------------------- KuboEvol
+// KuboEvol (kubosubs.F90:438-553): psi <- U psi and zupsi <- U zupsi + [U, X] psi, U the Chebyshev
+// propagator above and X the position along dir.  The commutator term runs a second recurrence beside
+// psi_n:
+//     X_0 = 0,  X_{n+1} = ((H - ac) X_n + D psi_n) * alpha - beta X_{n-1},   D = d (*) H off-diagonal,
+// d the NeighD component (the neighbour's displacement) of each entry; zupsi accumulates c_n X_n.
+// D is stored as a second value array with the indexing of the layout's values (built once per
+// direction), so a union column's d * val sits beside its val.
+
+template <typename HV>
+__device__ __forceinline__ HV scaled_neg_hop(double2 h, double d);
+template <> __device__ __forceinline__ float scaled_neg_hop<float>(double2 h, double d) { return (float)(-d * h.x); }
+template <> __device__ __forceinline__ double scaled_neg_hop<double>(double2 h, double d) { return -d * h.x; }
+template <> __device__ __forceinline__ float2 scaled_neg_hop<float2>(double2 h, double d)
 {
-    return fail(c, GBN_ERR_STATE, "Kubo time evolution is not built yet");
+    return make_float2((float)(-d * h.x), (float)(-d * h.y));
+}
+template <> __device__ __forceinline__ double2 scaled_neg_hop<double2>(double2 h, double d)
+{
+    return make_double2(-d * h.x, -d * h.y);
+}
+__device__ __forceinline__ void acc_into(float& a, float b) { a += b; }
+__device__ __forceinline__ void acc_into(double& a, double b) { a += b; }
+__device__ __forceinline__ void acc_into(float2& a, float2 b) { a.x += b.x; a.y += b.y; }
+__device__ __forceinline__ void acc_into(double2& a, double2 b) { a.x += b.x; a.y += b.y; }
+
+// One thread per group: every entry of the group's rows finds its union column in the slice record
+// (first match among the stored columns) and adds -d * hopp there.  dval must be zeroed.
+template <typename HV>
+__global__ void k_fill_dvals(const int32_t* nneigh, const int32_t* nlist, const double2* hopp, const double* neighd,
+                             int comp, const int32_t* rperm, const int32_t* riperm, int64_t n, int32_t max_neigh,
+                             int G, int gpw, int64_t nslices, const int64_t* slice_ptr, const unsigned char* mat,
+                             int64_t entry_bytes, HV* dval)
+{
+    const int64_t ng = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (ng >= nslices * gpw) return;
+    const int64_t s = ng / gpw;
+    const int j = (int)(ng % gpw);
+    const int64_t base = slice_ptr[s];
+    const int w = (int)((slice_ptr[s + 1] - base) / gpw);
+    const int32_t* col = reinterpret_cast<const int32_t*>(mat + base * entry_bytes);
+    for (int rr = 0; rr < G; ++rr) {
+        const int64_t row = ng * G + rr;
+        if (row >= n) break;
+        const int64_t p = rperm[row];
+        for (int e = 0; e < nneigh[p]; ++e) {
+            const int64_t ent = p * max_neigh + e;
+            const int32_t target = riperm[nlist[ent] - 1];
+            int k = 0;
+            while (k < w && col[k * gpw + j] != target) ++k;
+            if (k == w) continue;   // cannot happen: every entry's column is in its group's union
+            acc_into(dval[((base + (int64_t)k * gpw + j) * G) + rr], scaled_neg_hop<HV>(hopp[ent], neighd[3 * ent + comp]));
+        }
+    }
+}
+
+struct DualParams {
+    const int64_t* slice_ptr;
+    const unsigned char* mat;
+    const void* dval;
+    int64_t entry_bytes;
+    const void* h0;
+    const void* psi_n;   // gathered
+    const void* x_n;     // gathered
+    void* psi_out;       // psi_{n-1} in, psi_{n+1} out
+    void* x_out;         // X_{n-1} in, X_{n+1} out
+    double2* pacc;       // psi accumulator (FP64)
+    double2* zacc;       // zupsi accumulator (FP64)
+    double cr, ci, ac, alpha, beta;
+    int64_t nslices;
+};
+
+template <typename VT, bool CPLX, int G, int RPT, int TPR>
+__global__ void __launch_bounds__(256) k_dual_step(DualParams p)
+{
+    using C2 = typename V2<VT>::t;
+    using HT = typename Hop<VT, CPLX>::t;
+    constexpr int GPW = 32 / TPR;
+    constexpr int R = RPT * TPR;
+    constexpr int U = kColUnroll;
+    const int lane = threadIdx.x & 31;
+    const int sub = lane / TPR;
+    const int q = lane % TPR;
+    const C2* __restrict__ pn = static_cast<const C2*>(p.psi_n);
+    const C2* __restrict__ xn = static_cast<const C2*>(p.x_n);
+    C2* __restrict__ po = static_cast<C2*>(p.psi_out);
+    C2* __restrict__ xo = static_cast<C2*>(p.x_out);
+    const VT* __restrict__ h0 = static_cast<const VT*>(p.h0);
+    const HT* __restrict__ dv = static_cast<const HT*>(p.dval);
+    const int nwb = (int)(blockDim.x >> 5);
+    const int64_t per = (p.nslices + gridDim.x - 1) / gridDim.x;
+    const int64_t s0 = (int64_t)blockIdx.x * per;
+    const int64_t s1e = (s0 + per < p.nslices) ? s0 + per : p.nslices;
+    for (int64_t s = s0 + (threadIdx.x >> 5); s < s1e; s += nwb) {
+        const int64_t base = p.slice_ptr[s];
+        const int w = (int)((p.slice_ptr[s + 1] - base) / GPW);
+        const unsigned char* rec = p.mat + base * p.entry_bytes;
+        const int32_t* __restrict__ cp = reinterpret_cast<const int32_t*>(rec) + sub;
+        const HT* __restrict__ vp = reinterpret_cast<const HT*>(rec + (size_t)w * GPW * 4) + sub * G;
+        const HT* __restrict__ dp = dv + (base + sub) * G;
+        C2 ap[G][RPT], ax[G][RPT];
+#pragma unroll
+        for (int g = 0; g < G; ++g)
+#pragma unroll
+            for (int t = 0; t < RPT; ++t) {
+                ap[g][t].x = 0; ap[g][t].y = 0;
+                ax[g][t].x = 0; ax[g][t].y = 0;
+            }
+        for (int k = 0; k < w; k += U) {
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int32_t c = __ldcs(cp + u * GPW);
+                HT h[G], hd[G];
+                load_group_vals<HT, G, false>(vp + u * GPW * G, h);
+                load_group_vals<HT, G, false>(dp + u * GPW * G, hd);
+                C2 gp[RPT], gx[RPT];
+                VecIO<VT, RPT>::load(pn + (size_t)(uint32_t)c * R + q * RPT, gp);
+                VecIO<VT, RPT>::load(xn + (size_t)(uint32_t)c * R + q * RPT, gx);
+#pragma unroll
+                for (int g = 0; g < G; ++g)
+#pragma unroll
+                    for (int t = 0; t < RPT; ++t) {
+                        Hop<VT, CPLX>::madd(ap[g][t], h[g], gp[t]);
+                        Hop<VT, CPLX>::madd(ax[g][t], h[g], gx[t]);
+                        Hop<VT, CPLX>::madd(ax[g][t], hd[g], gp[t]);
+                    }
+            }
+            cp += U * GPW;
+            vp += U * GPW * G;
+            dp += U * GPW * G;
+        }
+        const int64_t row0 = (s * GPW + sub) * G;
+#pragma unroll
+        for (int g = 0; g < G; ++g) {
+            const int64_t e0 = (row0 + g) * R + q * RPT;
+            C2 ownp[RPT], ownx[RPT], prevp[RPT], prevx[RPT], np[RPT], nx[RPT];
+            VecIO<VT, RPT>::load(pn + e0, ownp);
+            VecIO<VT, RPT>::load(xn + e0, ownx);
+#pragma unroll
+            for (int t = 0; t < RPT; ++t) {   // read before the in-place writes below
+                prevp[t] = po[e0 + t];
+                prevx[t] = xo[e0 + t];
+            }
+            const VT d = h0[row0 + g];
+#pragma unroll
+            for (int t = 0; t < RPT; ++t) {
+                C2 yp = ap[g][t], yx = ax[g][t];
+                yp.x = fma(d, ownp[t].x, yp.x);
+                yp.y = fma(d, ownp[t].y, yp.y);
+                yx.x = fma(d, ownx[t].x, yx.x);
+                yx.y = fma(d, ownx[t].y, yx.y);
+                np[t].x = (VT)(((double)yp.x - p.ac * (double)ownp[t].x) * p.alpha - p.beta * (double)prevp[t].x);
+                np[t].y = (VT)(((double)yp.y - p.ac * (double)ownp[t].y) * p.alpha - p.beta * (double)prevp[t].y);
+                nx[t].x = (VT)(((double)yx.x - p.ac * (double)ownx[t].x) * p.alpha - p.beta * (double)prevx[t].x);
+                nx[t].y = (VT)(((double)yx.y - p.ac * (double)ownx[t].y) * p.alpha - p.beta * (double)prevx[t].y);
+                double2 a1 = p.pacc[e0 + t], a2 = p.zacc[e0 + t];
+                const double pr = (double)np[t].x, pi = (double)np[t].y, xr = (double)nx[t].x, xi = (double)nx[t].y;
+                a1.x += p.cr * pr - p.ci * pi;
+                a1.y += p.cr * pi + p.ci * pr;
+                a2.x += p.cr * xr - p.ci * xi;
+                a2.y += p.cr * xi + p.ci * xr;
+                p.pacc[e0 + t] = a1;
+                p.zacc[e0 + t] = a2;
+            }
+            VecIO<VT, RPT>::store(po + e0, np);
+            VecIO<VT, RPT>::store(xo + e0, nx);
+        }
+    }
+}
+
+// psi_0 = sqrt(2) psi, psi_{-1} = X_0 = X_{-1} = 0, pacc = c_0 psi, zacc = zupsi (already U zupsi)
+template <typename VT>
+__global__ void k_dual_start(typename V2<VT>::t* p0, typename V2<VT>::t* pm1, typename V2<VT>::t* x0,
+                             typename V2<VT>::t* xm1, double2* pacc, double2* zacc, const double2* psi_in,
+                             const double2* zu_in, const int32_t* rperm, int64_t n, int64_t npad, int R, int nrhs_real,
+                             double c0r, double c0i)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= npad * R) return;
+    const int64_t row = i / R;
+    const int r = (int)(i % R);
+    double2 v = make_double2(0.0, 0.0), zu = make_double2(0.0, 0.0);
+    if (row < n && r < nrhs_real) {
+        v = psi_in[(int64_t)r * n + rperm[row]];
+        zu = zu_in[(int64_t)r * n + rperm[row]];
+    }
+    typename V2<VT>::t a, zero;
+    a.x = (VT)(1.4142135623730951 * v.x);
+    a.y = (VT)(1.4142135623730951 * v.y);
+    zero.x = 0;
+    zero.y = 0;
+    p0[i] = a;
+    pm1[i] = zero;
+    x0[i] = zero;
+    xm1[i] = zero;
+    pacc[i] = make_double2(c0r * v.x - c0i * v.y, c0r * v.y + c0i * v.x);
+    zacc[i] = zu;
+}
+
+using DualFn = void (*)(DualParams);
+
+template <typename VT, bool CPLX, int G>
+static DualFn pick_dual_g(int rpt, int tpr)
+{
+#define GBN_CASE(RP, TP) \
+    if (rpt == RP && tpr == TP) return k_dual_step<VT, CPLX, G, RP, TP>;
+    GBN_CASE(1, 1) GBN_CASE(1, 2) GBN_CASE(1, 4) GBN_CASE(1, 8) GBN_CASE(1, 16) GBN_CASE(1, 32)
+    GBN_CASE(2, 1) GBN_CASE(2, 2) GBN_CASE(2, 4) GBN_CASE(2, 8) GBN_CASE(2, 16)
+    if constexpr (sizeof(VT) == 4) {
+        GBN_CASE(4, 1) GBN_CASE(4, 2) GBN_CASE(4, 4) GBN_CASE(4, 8)
+    }
+#undef GBN_CASE
+    return nullptr;
+}
+
+template <typename VT, bool CPLX>
+static DualFn pick_dual(int G, int rpt, int tpr)
+{
+    if (G == 1) return pick_dual_g<VT, CPLX, 1>(rpt, tpr);
+    if (G == 2) return pick_dual_g<VT, CPLX, 2>(rpt, tpr);
+    if (G == 4) return pick_dual_g<VT, CPLX, 4>(rpt, tpr);
+    return nullptr;
+}
+
+static int build_dvals(gbn_ctx* c, int dir)
+{
+    Ell& E = c->ell;
+    if (E.dval_dir == dir) return GBN_OK;
+    const size_t bytes = (size_t)E.val_size * E.G * (size_t)(E.nnz_stored > 0 ? E.nnz_stored : 1);
+    GBN_CK(c, E.dval.ensure(bytes));
+    GBN_CK(c, cudaMemsetAsync(E.dval.p, 0, bytes, c->stream));
+    const unsigned grd = (unsigned)((E.nslices * E.gpw + 127) / 128);
+#define GBN_DV(HV)                                                                                                  \
+    k_fill_dvals<HV><<<grd, 128, 0, c->stream>>>(c->nneigh.as<int32_t>(), c->nlist.as<int32_t>(), c->hopp.as<double2>(), \
+                                                 c->neighd.as<double>(), dir - 1, E.rperm.as<int32_t>(),                 \
+                                                 E.riperm.as<int32_t>(), c->n, c->max_neigh, E.G, E.gpw, E.nslices,        \
+                                                 E.slice_ptr.as<int64_t>(), E.mat.as<unsigned char>(), E.entry_bytes,     \
+                                                 E.dval.as<HV>())
+    if (E.prec == GBN_MIXED) {
+        if (E.cplx) GBN_DV(float2);
+        else GBN_DV(float);
+    } else {
+        if (E.cplx) GBN_DV(double2);
+        else GBN_DV(double);
+    }
+#undef GBN_DV
+    GBN_CK_LAUNCH(c);
+    E.dval_dir = dir;
+    return GBN_OK;
+}
+
+int kubo_evol(gbn_ctx* c, int32_t prec, int32_t nrhs, const double* c_host, int32_t npol, double ac, double bc,
+              int32_t dir, double* psi_host, double* zupsi_host)
+{
+    if (!c->have_neighd) return fail(c, GBN_ERR_STATE, "KuboEvol needs NeighD (gbn_neighbours or gbn_set_neighd)");
+    if (dir != 1 && dir != 2) return fail(c, GBN_ERR_ARG, "dir must be 1 (x) or 2 (y)");
+    // zupsi <- U zupsi (the reference's first call of KuboChebyshevEvolve)
+    int rc = cheb_evolve(c, prec, nrhs, c_host, npol, ac, bc, zupsi_host);
+    if (rc) return rc;
+    const int T = tile_width(nrhs);   // the layout cheb_evolve prepared
+    int rpt, tpr;
+    split_rhs(prec, T, c->tune_rpt, &rpt, &tpr);
+    rc = build_dvals(c, dir);
+    if (rc) return rc;
+    DualFn fn;
+    if (prec == GBN_MIXED) fn = c->ell.cplx ? pick_dual<float, true>(c->ell.G, rpt, tpr)
+                                            : pick_dual<float, false>(c->ell.G, rpt, tpr);
+    else fn = c->ell.cplx ? pick_dual<double, true>(c->ell.G, rpt, tpr) : pick_dual<double, false>(c->ell.G, rpt, tpr);
+    if (!fn) return fail(c, GBN_ERR_ARG, "no KuboEvol kernel for this tile width");
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 256, 0) != cudaSuccess || per_sm < 1) per_sm = 1;
+    const int grid = c->num_sms * per_sm;
+    const int64_t n = c->n, npad = c->ell.npad;
+    const size_t esz = (prec == GBN_MIXED) ? sizeof(float2) : sizeof(double2);
+    GBN_CK(c, c->cheb[0].ensure(sizeof(double2) * (size_t)npad * T));   // psi accumulator
+    GBN_CK(c, c->cheb[2].ensure(sizeof(double2) * (size_t)npad * T));   // zupsi accumulator
+    GBN_CK(c, c->cheb[3].ensure(esz * (size_t)npad * T));              // X_n
+    GBN_CK(c, c->cheb[4].ensure(esz * (size_t)npad * T));              // X_{n-1}
+    GBN_CK(c, c->cheb[1].ensure(sizeof(double2) * (size_t)n * T));     // psi in / out
+    GBN_CK(c, c->cheb[5].ensure(sizeof(double2) * (size_t)n * T));     // zupsi in / out
+    double2* pacc = c->cheb[0].as<double2>();
+    double2* zacc = c->cheb[2].as<double2>();
+    double2* pin = c->cheb[1].as<double2>();
+    double2* zin = c->cheb[5].as<double2>();
+    const int32_t* rp = c->ell.rperm.as<int32_t>();
+    const int blk = 256;
+    const unsigned sgrid = (unsigned)((npad * T + blk - 1) / blk);
+    const unsigned fgrid = (unsigned)((n * T + blk - 1) / blk);
+    for (int r0 = 0; r0 < nrhs; r0 += T) {
+        const int cnt = std::min(T, nrhs - r0);
+        GBN_CK(c, cudaMemcpyAsync(pin, psi_host + (size_t)2 * n * r0, sizeof(double2) * (size_t)n * cnt,
+                                  cudaMemcpyHostToDevice, c->stream));
+        GBN_CK(c, cudaMemcpyAsync(zin, zupsi_host + (size_t)2 * n * r0, sizeof(double2) * (size_t)n * cnt,
+                                  cudaMemcpyHostToDevice, c->stream));
+        void* pA = c->vec[1].p;
+        void* pB = c->vec[2].p;
+        void* xA = c->cheb[3].p;
+        void* xB = c->cheb[4].p;
+        if (prec == GBN_MIXED)
+            k_dual_start<float><<<sgrid, blk, 0, c->stream>>>(static_cast<float2*>(pA), static_cast<float2*>(pB),
+                                                               static_cast<float2*>(xA), static_cast<float2*>(xB), pacc,
+                                                               zacc, pin, zin, rp, n, npad, T, cnt, c_host[0], c_host[1]);
+        else
+            k_dual_start<double><<<sgrid, blk, 0, c->stream>>>(static_cast<double2*>(pA), static_cast<double2*>(pB),
+                                                                static_cast<double2*>(xA), static_cast<double2*>(xB), pacc,
+                                                                zacc, pin, zin, rp, n, npad, T, cnt, c_host[0], c_host[1]);
+        GBN_CK_LAUNCH(c);
+        DualParams p;
+        p.slice_ptr = c->ell.slice_ptr.as<int64_t>();
+        p.mat = c->ell.mat.as<unsigned char>();
+        p.dval = c->ell.dval.p;
+        p.entry_bytes = c->ell.entry_bytes;
+        p.h0 = c->ell.h0.p;
+        p.pacc = pacc;
+        p.zacc = zacc;
+        p.ac = ac;
+        p.nslices = c->ell.nslices;
+        for (int k = 1; k < npol; ++k) {
+            p.psi_n = pA;
+            p.x_n = xA;
+            p.psi_out = pB;
+            p.x_out = xB;
+            p.cr = c_host[2 * k];
+            p.ci = c_host[2 * k + 1];
+            p.alpha = (k == 1) ? 1.0 / (2.0 * bc) : 1.0 / bc;
+            p.beta = (k == 1) ? 0.0 : 1.0;
+            fn<<<grid, 256, 0, c->stream>>>(p);
+            GBN_CK_LAUNCH(c);
+            std::swap(pA, pB);
+            std::swap(xA, xB);
+        }
+        k_cheb_finish<<<fgrid, blk, 0, c->stream>>>(pacc, pin, rp, n, T, cnt);
+        GBN_CK_LAUNCH(c);
+        k_cheb_finish<<<fgrid, blk, 0, c->stream>>>(zacc, zin, rp, n, T, cnt);
+        GBN_CK_LAUNCH(c);
+        GBN_CK(c, cudaMemcpyAsync(psi_host + (size_t)2 * n * r0, pin, sizeof(double2) * (size_t)n * cnt,
+                                  cudaMemcpyDeviceToHost, c->stream));
+        GBN_CK(c, cudaMemcpyAsync(zupsi_host + (size_t)2 * n * r0, zin, sizeof(double2) * (size_t)n * cnt,
+                                  cudaMemcpyDeviceToHost, c->stream));
+        GBN_CK(c, cudaStreamSynchronize(c->stream));
+    }
+    return GBN_OK;
 }
 
 }  // namespace gbn

@@ -61,6 +61,8 @@ struct Ell {
     DevBuf rperm, riperm;    // solver row order: rperm[row] = reference atom (row < n), riperm inverse
     int val_size = 0;        // bytes per stored value
     int entry_bytes = 0;     // 4 + G * val_size
+    DevBuf dval;             // d * val per stored value (KuboEvol's commutator), same indexing as the values
+    int dval_dir = 0;        // NeighD component of dval (1 = x, 2 = y; 0 = not built)
     int64_t max_record = 0;  // bytes of the largest slice record
     int64_t cap_record = 0;  // staging buffer size: 99.5 % of the records fit (larger ones are read in place)
     bool valid = false;
@@ -184,8 +186,8 @@ int peierls(gbn_ctx* c, double flux);
 // Chebyshev (gbn_cheb.cu)
 int cheb_evolve(gbn_ctx* c, int32_t prec, int32_t nrhs, const double* c_host, int32_t npol, double ac, double bc,
                 double* z_host);
-int kubo_evol(gbn_ctx* c, int32_t nrhs, const double* c_host, int32_t npol, double ac, double bc, int32_t dir,
-              double* psi_host, double* zupsi_host);
+int kubo_evol(gbn_ctx* c, int32_t prec, int32_t nrhs, const double* c_host, int32_t npol, double ac, double bc,
+              int32_t dir, double* psi_host, double* zupsi_host);
 
 inline int grid_for(gbn_ctx* c, int blocks_per_sm) { return c->num_sms * blocks_per_sm; }
 

@@ -279,6 +279,7 @@ int build_ell(gbn_ctx* c, int prec, int G, int gpw)
     }
     Ell& E = c->ell;
     E.valid = false;
+    E.dval_dir = 0;
     E.G = G;
     E.gpw = gpw;
     E.prec = prec;

@@ -175,10 +175,13 @@ int gbn_cf_dos(gbn_ctx* ctx, int32_t nrhs, const double* a, const double* b, con
  * arithmetic and FP64 accumulation of z). */
 int gbn_cheb_evolve(gbn_ctx* ctx, int32_t precision, int32_t nrhs, const double* c, int32_t npol, double ac,
                     double bc, double* z);
-/* KuboEvol (kubosubs.F90:438-553): psi <- U psi and zupsi <- U zupsi + [U, X] psi, X along
- * dir (1 = x, 2 = y) from NeighD; needs gbn_neighbours or NeighD through gbn_set_neighd. */
-int gbn_kubo_evol(gbn_ctx* ctx, int32_t nrhs, const double* c, int32_t npol, double ac, double bc,
-                  int32_t dir, double* psi, double* zupsi);
+/* KuboEvol (kubosubs.F90:438-553): psi <- U psi and zupsi <- U zupsi + [U, X] psi for nrhs vectors
+ * psi, zupsi [nrhs][N] (host, in place), U the propagator of gbn_cheb_evolve (same c, ac, bc) and X
+ * the position along dir (1 = x, 2 = y) through NeighD: the commutator recurrence
+ * X_0 = 0, X_{n+1} = 2 x X_n + D psi_n / bc - X_{n-1} with D = NeighD(dir) * (-hopp).  Needs
+ * gbn_neighbours or NeighD through gbn_set_neighd.  precision as for gbn_cheb_evolve. */
+int gbn_kubo_evol(gbn_ctx* ctx, int32_t precision, int32_t nrhs, const double* c, int32_t npol, double ac,
+                  double bc, int32_t dir, double* psi, double* zupsi);
 /* NeighD(3,maxNeigh,N) for gbn_kubo_evol after gbn_load_hamiltonian. */
 int gbn_set_neighd(gbn_ctx* ctx, const double* neighd);
 

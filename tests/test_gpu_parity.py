@@ -268,3 +268,38 @@ def test_chebyshev_mixed_precision(ctx):
     for k in (0, 7, 15):
         ref = orc.cheb_evolve(r["nb"], r["hop"], r["h0"], c, ac, bc, z0[k])
         assert np.linalg.norm(z[k] - ref) <= 2e-6 * np.linalg.norm(ref)
+
+
+@pytest.mark.parametrize("name,direction,zero_zu", [("moire_field", 1, False), ("tbg", 2, False), ("graphene", 1, True)])
+def test_kubo_evol_fp64(ctx, name, direction, zero_zu):
+    """KuboEvol: psi <- U psi and zupsi <- U zupsi + [U, X] psi within 1e-9 in norm of the oracle, along x
+    and y, with complex (field) and real hoppings; zupsi = 0 isolates the commutator term."""
+    r = built(name)
+    n = r["geo"]["n"]
+    ac, bc, c = _cheb_setup(r)
+    psi = _zstart(n, 2)
+    zu = np.zeros_like(psi) if zero_zu else np.stack([orc.init_wf(n, 70 + j) for j in range(2)])
+    ctx.load_hamiltonian(r["nb"]["nneigh"], r["nb"]["nlist"], r["hop"], r["h0"])
+    ctx.set_neighd(r["nb"]["neighd"])
+    p, z = ctx.kubo_evol(c, ac, bc, psi, zu, direction, G.GBN_FP64)
+    for k in range(2):
+        pr, zr = orc.evol(r["nb"], r["hop"], r["h0"], c, ac, bc, psi[k], zu[k], direction)
+        assert np.linalg.norm(p[k] - pr) <= 1e-9 * np.linalg.norm(pr)
+        assert np.linalg.norm(z[k] - zr) <= 1e-9 * np.linalg.norm(zr)
+
+
+def test_kubo_evol_mixed_precision(ctx):
+    """The dual recurrence with complex FP32 vectors (FP64 step arithmetic and accumulations), 8 vectors
+    of the bilayer: within 1e-5 in norm of the FP64 oracle."""
+    r = built("tbg")
+    n = r["geo"]["n"]
+    ac, bc, c = _cheb_setup(r)
+    psi = _zstart(n, 8)
+    zu = np.zeros_like(psi)
+    ctx.load_hamiltonian(r["nb"]["nneigh"], r["nb"]["nlist"], r["hop"], r["h0"])
+    ctx.set_neighd(r["nb"]["neighd"])
+    p, z = ctx.kubo_evol(c, ac, bc, psi, zu, 1, G.GBN_MIXED)
+    for k in (0, 7):
+        pr, zr = orc.evol(r["nb"], r["hop"], r["h0"], c, ac, bc, psi[k], zu[k], 1)
+        assert np.linalg.norm(p[k] - pr) <= 1e-5 * np.linalg.norm(pr)
+        assert np.linalg.norm(z[k] - zr) <= 1e-5 * np.linalg.norm(zr)
