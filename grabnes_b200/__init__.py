@@ -81,7 +81,8 @@ def _opt(dtype):
 EXPORTS = ["gbn_cell_atoms", "gbn_build_cell", "gbn_cart_roundtrip", "gbn_rng_uniform", "gbn_create", "gbn_destroy", "gbn_last_error", "gbn_version", "gbn_set_stream", "gbn_set_tuning", "gbn_launch_count",
            "gbn_last_timing", "gbn_last_kernel_timing", "gbn_set_geometry", "gbn_neighbours", "gbn_get_neighbours", "gbn_assemble",
            "gbn_peierls", "gbn_get_hamiltonian", "gbn_load_hamiltonian", "gbn_lanczos", "gbn_lanczos_phases",
-           "gbn_stage_phases", "gbn_run_staged", "gbn_cf_dos", "gbn_cheb_evolve", "gbn_kubo_evol", "gbn_set_neighd", "gbn_lanczos_noalloc"]
+           "gbn_stage_phases", "gbn_run_staged", "gbn_cf_dos", "gbn_cheb_evolve", "gbn_kubo_evol", "gbn_set_neighd", "gbn_lanczos_noalloc",
+           "gbn_cheb_interval", "gbn_cheb_coef"]
 
 
 def _declare(L):
@@ -120,6 +121,8 @@ def _declare(L):
     L.gbn_kubo_evol.argtypes = [vp, i32, i32, _p(np.complex128), i32, d, d, i32, _p(np.complex128),
                                 _p(np.complex128)]
     L.gbn_set_neighd.argtypes = [vp, _p(np.float64)]
+    L.gbn_cheb_interval.argtypes = [_p(np.float64), _p(np.float64), i32, C.POINTER(d), C.POINTER(d)]
+    L.gbn_cheb_coef.argtypes = [d, d, d, i32, _p(np.complex128)]
     # device pointers (ints from tensor.data_ptr()), no context
     L.gbn_lanczos_noalloc.argtypes = [i64, i32, vp, vp, vp, vp, vp, i32, vp, vp, vp]
 
@@ -294,6 +297,26 @@ class Context:
         self._ck(self._L.gbn_kubo_evol(self._h, precision, p.shape[0], cc, len(cc), ac, bc, direction, p.reshape(-1),
                                        z.reshape(-1)))
         return p, z
+
+
+def cheb_interval(a, b):
+    """KuboInterval: spectral centre ac and scale bc from recursion coefficients a, b (host)."""
+    a = _c(a, np.float64)
+    b = _c(b, np.float64)
+    ac, bc = C.c_double(), C.c_double()
+    rc = lib().gbn_cheb_interval(a, b, len(a), C.byref(ac), C.byref(bc))
+    if rc != 0:
+        raise GbnError(rc, "gbn_cheb_interval failed")
+    return ac.value, bc.value
+
+
+def cheb_coef(dt, ac, bc, npol):
+    """KuboCn: the npol complex propagator coefficients for the time step dt (host)."""
+    c = np.zeros(npol, np.complex128)
+    rc = lib().gbn_cheb_coef(dt, ac, bc, npol, c)
+    if rc != 0:
+        raise GbnError(rc, "gbn_cheb_coef failed")
+    return c
 
 
 def build_cell(kind, aG=2.46, cell_size=50, super_cell=1, m=(0, 0, 0, 0), height=40.0, d_interlayer=3.35):

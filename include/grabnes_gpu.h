@@ -168,6 +168,15 @@ int gbn_cf_dos(gbn_ctx* ctx, int32_t nrhs, const double* a, const double* b, con
                double* energy, double* dos);
 
 /* ---- Chebyshev time evolution --------------------------------------------------------------- */
+/* KuboInterval (kubosubs.F90:290-350) on the host: from the recursion coefficients a, b [nrecurs]
+ * (b[i] couples levels i and i+1), ac = (emax + emin)/2 and bc = 1.2 (emax - emin)/4 of the extreme
+ * eigenvalues of the tridiagonal matrix.  No context, no GPU. */
+int gbn_cheb_interval(const double* a, const double* b, int32_t nrecurs, double* ac, double* bc);
+/* KuboCn (kubosubs.F90:352-433) on the host: the npol complex coefficients c [npol] of the propagator
+ * exp(-i H dt) in the scaled Chebyshev basis of gbn_cheb_evolve, c_0 = exp(-i ac dt) J_0(2 bc dt),
+ * c_n = sqrt(2) (-i)^n exp(-i ac dt) J_n(2 bc dt) (the reference's Jacobi-matrix quadrature gives the
+ * same values).  No context, no GPU. */
+int gbn_cheb_coef(double dt, double ac, double bc, int32_t npol, double* c);
 /* KuboChebyshevEvolve (kubosubs.F90:557-619) for nrhs complex vectors z [nrhs][N] (host, reference atom
  * order, in place): with x = (H - ac)/(2 bc), psi_0 = sqrt(2) z, psi_1 = x psi_0,
  * psi_{n+1} = 2 x psi_n - psi_{n-1}, z <- c_0 z + sum_{n=1}^{npol-1} c_n psi_n; c complex [npol] (the
