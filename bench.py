@@ -98,34 +98,18 @@ def cpu_count():
 
 
 def dist_init():
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if ws > 1:
-        import datetime
-
-        import torch
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
-    return ws, rank, local
+    from grabnes_b200 import replicas
+    return replicas.init("nccl")
 
 
 def dist_max(x, ws):
-    if ws == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    from grabnes_b200 import replicas
+    return replicas.max_over_ranks(x, ws)
 
 
 def barrier(ws):
-    if ws > 1:
-        import torch.distributed as dist
-        dist.barrier()
+    from grabnes_b200 import replicas
+    replicas.barrier(ws)
 
 
 PROFILE = os.path.join(ROOT, "profiles", "k_spmm_staged_tbg.md")
@@ -149,6 +133,7 @@ def run_ours(args, ws, rank, local):
 
     import grabnes_b200 as G
     from grabnes_b200 import model as M
+    from grabnes_b200 import replicas
 
     torch.cuda.set_device(local)
     stream = torch.cuda.Stream()
@@ -162,7 +147,7 @@ def run_ours(args, ws, rank, local):
     n = cell["n"]
     nnz = ctx.neighbours_total
     g0 = job["g0"]
-    seed = SEED + 1000 * rank   # every rank runs its own replica of the workload (weak scaling)
+    seed = replicas.seed_of(SEED, rank)   # every rank runs its own replica of the workload (weak scaling)
     u = G.rng_uniform(seed, NRHS * n).reshape(NRHS, n)
 
     # ---- autotuning of the recursion kernels on this Hamiltonian, then device-resident inputs: the start
@@ -208,6 +193,7 @@ def run_ours(args, ws, rank, local):
                               "spmm_ms": spmm_ms, "update_ms": update_ms, "atoms": n, "entries": nnz,
                               "tuning": best, "candidates": tuning}), flush=True)
         ctx.close()
+        replicas.finish(ws)
         return
 
     # ---- roofline of the sparse-product kernel (the dominant one).  Its algorithmic bytes are those of a
@@ -283,9 +269,7 @@ def run_ours(args, ws, rank, local):
     if rank == 0:
         print(json.dumps(out), flush=True)
     ctx.close()
-    if ws > 1:
-        import torch.distributed as dist
-        dist.destroy_process_group()
+    replicas.finish(ws)
 
 
 def cpu_baseline(ctx, n, u0, steps):
