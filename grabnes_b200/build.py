@@ -15,6 +15,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libgrabnes_gpu.so")
 OBJ = os.path.join(HERE, "_build")
+DRIVER_DIR = os.path.join(HERE, "driver")
+DRIVER = os.path.join(HERE, "grabnes")
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -59,7 +61,23 @@ def build(verbose=False, jobs=8):
     if not os.path.exists(LIB) or any(os.path.getmtime(o) > os.path.getmtime(LIB) for o in objs):
         cmd = [nvcc(), "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", LIB] + objs + ["-lcudart"]
         subprocess.run(cmd, check=True)
+    build_driver(verbose)
     return LIB
+
+
+def build_driver(verbose=False):
+    """The `grabnes Gendata.in` executable (host C++ over the C ABI), next to the library."""
+    src = os.path.join(DRIVER_DIR, "grabnes.cpp")
+    deps = [src, LIB] + glob.glob(os.path.join(HERE, "..", "include", "*.h"))
+    if os.path.exists(DRIVER) and os.path.getmtime(DRIVER) >= max(os.path.getmtime(d) for d in deps):
+        return DRIVER
+    cxx = shutil.which("g++") or "g++"
+    cmd = [cxx, "-O2", "-std=c++17", "-Wall", src, "-o", DRIVER, "-L" + HERE, "-lgrabnes_gpu",
+           "-Wl,-rpath,$ORIGIN"]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+    return DRIVER
 
 
 if __name__ == "__main__":

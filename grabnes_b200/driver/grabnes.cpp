@@ -1,0 +1,565 @@
+// grabnes -- the recursion path of GRABNES's `grabnes Gendata.in` on the B200 library.
+//
+//     grabnes [Gendata.in]            run the job, write the reference's output files
+//     grabnes --print-job [file]      print the job the input describes (JSON) and exit (no GPU)
+//
+// Mirrors the reference's driver for the recursion DOS (lanczosKuboCode/Src/grabnes.f90, CalcSelect and
+// CalcKubo in calc.F90:13-566, KuboDOS in kubo.F90:276-319): the input keys are read as MIO reads them
+// (Src/MIO/input.F90, parser.f90: `Section.Name value` lines, '#' comments, keys matched without case,
+// '_' and '-', former names through the alias table, numbers as arithmetic expressions), the cell,
+// neighbour search, Hamiltonian and Peierls phases are built on the device, and for every field of the
+// sweep (magf.F90:20-146) the recursion and the continued fraction write
+//     <prefix>.a0.dat, <prefix>.b0.dat   a_n and b_n, one per line        (kubosubs.F90:140-176)
+//     <prefix>.DOS                       E and DOS in units of g0          (kubosubs.F90:247-276)
+//     <prefix>.AB                        the norm, then a_n b_n per line
+// inside m<m:05>_B<B:.4f>/ when the sweep has more than one field.  Everything on the device goes
+// through the C ABI of include/grabnes_gpu.h.
+#include <errno.h>
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <sys/stat.h>
+
+#include <cctype>
+#include <map>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/grabnes_gpu.h"
+
+namespace {
+
+const double kPi = 3.14159265358979323846;
+const double kFluxQuantum = 6.62606896e-34 / 1.602176565e-19;   // h/e (constants.f90)
+const double kShellRadius[9] = {1.0, 1.7320508075688772, 2.0, 2.6457513110645906, 3.0,
+                                3.4641016151377544, 3.6055512754639891, 4.0, 4.3588989435406740};
+
+[[noreturn]] void die(const std::string& msg)
+{
+    fprintf(stderr, "ERROR: %s\n*** PROGRAM ABORTED\n", msg.c_str());
+    exit(1);
+}
+
+std::string norm_key(const std::string& k)
+{
+    std::string o;
+    for (char ch : k)
+        if (ch != '_' && ch != '-') o += (char)tolower((unsigned char)ch);
+    return o;
+}
+
+// former (section-less) names of the keys read here (lanczosKuboCode/Src/MIO/input_aliases.inc)
+const char* kAliases[][2] = {
+    {"Run.TypeOfSystem", "TypeOfSystem"}, {"Run.Prefix", "Prefix"},
+    {"Structure.LatticeParameter", "LatticeParameter"}, {"Structure.CellSize", "CellSize"},
+    {"Structure.SuperCell", "SuperCell"}, {"Structure.MoireCellParameters", "MoireCellParameters"},
+    {"Structure.CellHeight", "CellHeight"}, {"Structure.InterlayerDistance", "InterlayerDistance"},
+    {"Interlayer.TypeOfBL", "TypeOfBL"}, {"Interlayer.Vpppi0", "vpppi0"}, {"Interlayer.Vppsigma0", "vppsigma0"},
+    {"Interlayer.BLdelta", "BLdelta"}, {"Interlayer.AddSecondLayerInteractions", "addSecondLayerInteractions"},
+    {"Intralayer.KoshinoIntralayer", "KoshinoIntralayer"}, {"Moire.Potential", "MoirePotential"},
+    {"Moire.Jeil", "MoireJeil"}, {"Moire.OnlyH0", "MoireOnlyH0"}, {"Moire.OnlyHZ", "MoireOnlyHZ"},
+    {"Moire.NoH0AndHZ", "MoireNoH0AndHZ"}, {"Moire.H0AndHZ", "MoireH0AndHZ"}, {"Moire.PreFactor", "MoirePreFactor"},
+    {"Moire.PotC0", "MoirePotC0"}, {"Moire.PotCz", "MoirePotCz"}, {"Moire.PotCab", "MoirePotCab"},
+    {"Moire.PotPhi0", "MoirePotPhi0"}, {"Moire.PotPhiz", "MoirePotPhiz"}, {"Moire.PotPhiab", "MoirePotPhiab"},
+    {"Moire.LatticePercent", "Latticepercent"}, {"Moire.Twisted", "MoireTwisted"},
+    {"Moire.TwistAngle", "MoireTwistAngle"}, {"Moire.OffDiag", "MoireOffDiag"},
+    {"Moire.OffDiagMidpoint", "MoireOffDiagMidpoint"}, {"Moire.LayerShift1", "MoireLayerShift1"},
+    {"Moire.FirstMoireMassFactor", "MoireFirstMoireMassFactor"},
+    {"Moire.SecondMoireMassFactor", "MoireSecondMoireMassFactor"}, {"Disorder.Anderson", "Anderson"},
+    {"Disorder.AndersonAmp", "AndersonAmp"}, {"Kubo.RecursionNumber", "RecursionNumber"},
+    {"Kubo.Epsilon", "Epsilon"}, {"Kubo.NumberofEnergyPoints", "NumberofEnergyPoints"},
+    {"Kubo.EnergyMin", "EnergyMin"}, {"Kubo.EnergyMax", "EnergyMax"}, {"Kubo.SeedValue", "seedValue"},
+    {"Kubo.SetSeed", "setSeed"}, {"Kubo.NumberofPolynomials", "NumberofPolynomials"},
+    {"Kubo.TimeStep", "TimeStep"}, {"Kubo.NumberofTimeSteps", "NumberofTimeSteps"},
+    {"Kubo.WriteNumberofSteps", "WriteNumberofSteps"}, {"MagField.Value", "MagField"},
+};
+
+// ---------------------------------------------------------------------------- values
+// A number as the reference's parser reads it: an arithmetic expression with + - * / ** and
+// parentheses, Fortran exponents (1.0d-3), and the functions acos asin atan cos sin tan sqrt exp.
+class Expr {
+public:
+    explicit Expr(const std::string& s) : s_(s), i_(0) {}
+    double eval()
+    {
+        const double v = sum();
+        skip();
+        if (i_ != s_.size()) throw std::runtime_error("unexpected '" + s_.substr(i_) + "'");
+        return v;
+    }
+
+private:
+    std::string s_;
+    size_t i_;
+    void skip()
+    {
+        while (i_ < s_.size() && isspace((unsigned char)s_[i_])) ++i_;
+    }
+    bool eat(const char* tok)
+    {
+        skip();
+        const size_t n = strlen(tok);
+        if (s_.compare(i_, n, tok) == 0) {
+            i_ += n;
+            return true;
+        }
+        return false;
+    }
+    double sum()
+    {
+        double v = product();
+        for (;;) {
+            if (eat("+")) v += product();
+            else if (eat("-")) v -= product();
+            else return v;
+        }
+    }
+    double product()
+    {
+        double v = power();
+        for (;;) {
+            skip();
+            if (s_.compare(i_, 2, "**") == 0) return v;   // handled by power()
+            if (eat("*")) v *= power();
+            else if (eat("/")) v /= power();
+            else return v;
+        }
+    }
+    double power()
+    {
+        const double b = unary();
+        if (eat("**")) return pow(b, power());   // right-associative
+        return b;
+    }
+    double unary()
+    {
+        if (eat("-")) return -unary();
+        if (eat("+")) return unary();
+        return primary();
+    }
+    double primary()
+    {
+        skip();
+        if (eat("(")) {
+            const double v = sum();
+            if (!eat(")")) throw std::runtime_error("missing ')'");
+            return v;
+        }
+        static const char* fn[] = {"acos", "asin", "atan", "cos", "sin", "tan", "sqrt", "exp"};
+        for (int k = 0; k < 8; ++k) {
+            const size_t n = strlen(fn[k]);
+            if (s_.compare(i_, n, fn[k]) == 0 && i_ + n < s_.size() && s_[i_ + n] == '(') {
+                i_ += n + 1;
+                const double x = sum();
+                if (!eat(")")) throw std::runtime_error("missing ')'");
+                switch (k) {
+                    case 0: return acos(x);
+                    case 1: return asin(x);
+                    case 2: return atan(x);
+                    case 3: return cos(x);
+                    case 4: return sin(x);
+                    case 5: return tan(x);
+                    case 6: return sqrt(x);
+                    default: return exp(x);
+                }
+            }
+        }
+        // number: digits, optional point, optional exponent e/E/d/D
+        std::string num;
+        while (i_ < s_.size() && (isdigit((unsigned char)s_[i_]) || s_[i_] == '.')) num += s_[i_++];
+        if (num.empty()) throw std::runtime_error("number expected at '" + s_.substr(i_) + "'");
+        if (i_ < s_.size() && strchr("eEdD", s_[i_])) {
+            size_t j = i_ + 1;
+            std::string ex = "e";
+            if (j < s_.size() && (s_[j] == '+' || s_[j] == '-')) ex += s_[j++];
+            if (j < s_.size() && isdigit((unsigned char)s_[j])) {
+                while (j < s_.size() && isdigit((unsigned char)s_[j])) ex += s_[j++];
+                num += ex;
+                i_ = j;
+            }
+        }
+        return strtod(num.c_str(), nullptr);
+    }
+};
+
+std::vector<std::string> split_ws(const std::string& s)
+{
+    std::vector<std::string> out;
+    size_t i = 0;
+    while (i < s.size()) {
+        while (i < s.size() && isspace((unsigned char)s[i])) ++i;
+        size_t j = i;
+        while (j < s.size() && !isspace((unsigned char)s[j])) ++j;
+        if (j > i) out.push_back(s.substr(i, j - i));
+        i = j;
+    }
+    return out;
+}
+
+class Input {
+public:
+    void load(const std::string& path)
+    {
+        FILE* f = fopen(path.c_str(), "r");
+        if (!f) die("cannot open input file " + path + ": " + strerror(errno));
+        char buf[4096];
+        bool in_block = false;
+        while (fgets(buf, sizeof buf, f)) {
+            std::string line(buf);
+            const size_t hash = line.find('#');
+            if (hash != std::string::npos) line.resize(hash);
+            std::vector<std::string> w = split_ws(line);
+            if (w.empty()) continue;
+            const std::string k0 = norm_key(w[0]);
+            if (k0 == "%block") { in_block = true; continue; }
+            if (k0 == "%endblock") { in_block = false; continue; }
+            if (in_block) continue;
+            std::string val;
+            for (size_t i = 1; i < w.size(); ++i) val += (i > 1 ? " " : "") + w[i];
+            kv_.emplace(k0, val);   // the first occurrence of a key wins
+        }
+        fclose(f);
+    }
+    bool find(const std::string& name, std::string* val) const
+    {
+        auto it = kv_.find(norm_key(name));
+        if (it == kv_.end())
+            for (auto& a : kAliases)
+                if (norm_key(a[0]) == norm_key(name)) it = kv_.find(norm_key(a[1]));
+        if (it == kv_.end()) return false;
+        if (val) *val = it->second;
+        return true;
+    }
+    bool has(const std::string& name) const { return find(name, nullptr); }
+    double d(const std::string& name, double def, int elem = 0) const
+    {
+        std::string v;
+        if (!find(name, &v)) return def;
+        std::vector<std::string> w = split_ws(v);
+        if ((int)w.size() <= elem) die("input key " + name + " has too few values");
+        try {
+            return Expr(w[elem]).eval();
+        } catch (const std::exception& e) {
+            die("input key " + name + ": " + e.what());
+        }
+    }
+    long i(const std::string& name, long def, int elem = 0) const
+    {
+        const double v = d(name, (double)def, elem);
+        if (v != floor(v)) die("input key " + name + " must be an integer");
+        return (long)v;
+    }
+    bool l(const std::string& name, bool def) const
+    {
+        std::string v;
+        if (!find(name, &v)) return def;
+        std::string t;
+        for (char ch : split_ws(v).empty() ? std::string() : split_ws(v)[0]) t += (char)tolower((unsigned char)ch);
+        if (t == ".true." || t == "true" || t == "t" || t == "yes" || t == ".t.") return true;
+        if (t == ".false." || t == "false" || t == "f" || t == "no" || t == ".f.") return false;
+        die("input key " + name + " must be a logical, not '" + v + "'");
+    }
+    std::string s(const std::string& name, const std::string& def) const
+    {
+        std::string v;
+        if (!find(name, &v)) return def;
+        std::vector<std::string> w = split_ws(v);
+        return w.empty() ? def : w[0];
+    }
+
+private:
+    std::map<std::string, std::string> kv_;
+};
+
+std::string lower(std::string s)
+{
+    for (auto& ch : s) ch = (char)tolower((unsigned char)ch);
+    return s;
+}
+
+// ---------------------------------------------------------------------------- the job
+struct Job {
+    gbn_cell cell{};
+    gbn_model model{};
+    double g0 = 0, cut2intra = 0, cut2inter = 0;
+    bool second_layer = false, moire = false;
+    int nrecurs = 0, n_en = 0, seed = 0;
+    double eta = 0, emin = 0, emax = 0;   // units of g0
+    long mbi = 0, mbf = 0, mstep = 1;
+    bool field_by_value = false, field_steps_by_value = false;
+    double b_value = 0, b_init = 0, b_final = 0, b_step = 0;
+    std::string prefix;
+};
+
+Job job_from_input(const Input& in)
+{
+    Job j;
+    const double aG = in.d("Structure.LatticeParameter", 2.46);
+    const std::string system = in.s("Run.TypeOfSystem", "Graphene");
+    if (lower(system) == "graphene") j.cell.kind = GBN_CELL_GRAPHENE;
+    else if (lower(system) == "twistedbilayerbasedonmoirecell") j.cell.kind = GBN_CELL_TBG_MOIRE;
+    else die("Run.TypeOfSystem " + system + " is not on the recursion path of this program");
+    if (!in.l("Kubo.Calc", true)) die("this program runs the recursion (Kubo.Calc .true.) only");
+    if (in.l("Diag.Calc", false)) die("exact diagonalisation (Diag.Calc) is not part of this program");
+    if (!in.l("Calculate.OnlyDOS", true)) die("time evolution (Calculate.OnlyDOS .false.) is run through the library API");
+    j.cell.aG = aG;
+    j.cell.cell_size = (int32_t)in.i("Structure.CellSize", 50);
+    j.cell.super_cell = (int32_t)in.i("Structure.SuperCell", 1);
+    for (int k = 0; k < 4; ++k) j.cell.m[k] = in.has("Structure.MoireCellParameters")
+                                               ? (int32_t)in.i("Structure.MoireCellParameters", 0, k) : 0;
+    j.cell.height = in.d("Structure.CellHeight", 40.0);
+    j.cell.d_interlayer = in.d("Structure.InterlayerDistance", 3.35);
+    j.g0 = in.d("TB.Hopping", -3.72 * aG + 12.14);
+    const long tbnn = in.i("TB.NeighLevels", 1);
+    if (tbnn < 1 || tbnn > 8) die("TB.NeighLevels must be between 1 and 8");
+    const double acc = aG / sqrt(3.0);
+    const double r = 0.5 * (kShellRadius[tbnn - 1] + kShellRadius[tbnn]) * acc;
+    j.cut2intra = r * r;
+    if (in.i("Neigh.LayerNeighbors", 0) != 0) {
+        const double x = aG / sqrt(3.0) * 1.1 * in.d("Neigh.LayerDistFactor", 1.0);
+        j.cut2inter = x * x;
+    } else {
+        j.cut2inter = 1.0;
+    }
+    gbn_model& m = j.model;
+    const double g0 = j.g0;
+    m.aG = aG;
+    m.tbnn = (int32_t)tbnn;
+    for (int k = 0; k < tbnn; ++k) {
+        m.nradii[k] = kShellRadius[k] * aG / sqrt(3.0) * 1.1;
+        m.gn_cc[k] = (k == 0) ? g0 / g0 : 0.0;
+    }
+    const std::string bl = in.s("Interlayer.TypeOfBL", "None");
+    const bool koshino_intra = in.l("Intralayer.KoshinoIntralayer", false);
+    if ((bl == "Koshino" || bl == "Mayou" || bl == "HTC") && !koshino_intra) {
+        static const double f2g2[8] = {0, 0, -0.2354, 0.1877, 0.0, -0.0633, 0.0, 0.0};   // ham.F90:8331-8350 [eV]
+        m.intralayer = 1;
+        for (int k = 2; k < 8; ++k) m.tksl[k] = f2g2[k] / g0;
+    }
+    j.moire = in.l("Moire.Potential", false) && in.l("Moire.Jeil", false);
+    if (j.moire) {
+        if (in.l("Moire.OnlyH0", false)) m.moire_onsite = 2;
+        else if (in.l("Moire.OnlyHZ", false)) m.moire_onsite = 3;
+        else if (in.l("Moire.NoH0AndHZ", false)) m.moire_onsite = 4;
+        else if (in.l("Moire.H0AndHZ", false)) m.moire_onsite = 1;
+        else die("the moire potential needs one of MoireH0AndHZ, MoireOnlyH0, MoireOnlyHZ, MoireNoH0AndHZ");
+    }
+    const double pref = in.d("Moire.PreFactor", 1.0);
+    m.C0 = in.d("Moire.PotC0", -0.01013) / g0 * pref;
+    m.Cz = in.d("Moire.PotCz", -0.00901) / g0 * pref;
+    m.Phi0 = in.d("Moire.PotPhi0", 1.510233401750693);
+    m.Phiz = in.d("Moire.PotPhiz", 0.147131255943122);
+    m.Cab = in.d("Moire.PotCab", 0.01134) / g0;
+    m.Phiab = in.d("Moire.PotPhiab", 0.342084533390889);
+    m.eps = in.d("Moire.LatticePercent", -0.018181818181818);
+    m.moire_twisted = in.l("Moire.Twisted", false) ? 1 : 0;
+    m.twist_rad = in.d("Moire.TwistAngle", 0.0) * kPi / 180.0;
+    m.moire_offdiag = in.l("Moire.OffDiag", false) ? 1 : 0;
+    m.moire_mid = (in.l("Moire.OffDiagMidpoint", false) && m.moire_offdiag) ? 1 : 0;
+    m.shift1 = in.d("Moire.LayerShift1", 0.0);
+    m.sign1 = in.d("Moire.FirstMoireMassFactor", 1.0);
+    m.sign2 = in.d("Moire.SecondMoireMassFactor", 1.0);
+    if (bl == "Koshino" || bl == "HTC") m.interlayer = 1;
+    m.vpppi0 = in.d("Interlayer.Vpppi0", koshino_intra ? 2.7 : 3.5) / g0;
+    m.vppsigma0 = -in.d("Interlayer.Vppsigma0", 0.48) / g0;
+    m.bl_delta = in.d("Interlayer.BLdelta", 0.184 * aG);
+    m.d_interlayer = in.d("Structure.InterlayerDistance", 3.35);
+    m.aCC = acc;
+    m.g_intlay = in.d("TB.InterLayerHopping", 0.39) / g0;
+    m.anderson = in.l("Disorder.Anderson", false) ? 1 : 0;
+    m.anderson_w = in.has("Disorder.AndersonAmp") ? in.d("Disorder.AndersonAmp", 0.0) / g0 : 1.0;
+    m.e0_c = in.d("TB.OnSiteC", 0.0) / g0;
+    j.second_layer = in.l("Interlayer.AddSecondLayerInteractions", false);
+    j.nrecurs = (int)in.i("Kubo.RecursionNumber", 700);
+    j.eta = in.d("Kubo.Epsilon", 0.01) / g0;
+    j.n_en = (int)in.i("Kubo.NumberofEnergyPoints", 1000);
+    j.emin = in.d("Kubo.EnergyMin", -4.0) / g0;
+    j.emax = in.d("Kubo.EnergyMax", 4.0) / g0;
+    j.seed = (int)in.i("Kubo.SeedValue", 123456);
+    if (j.nrecurs < 1 || j.n_en < 1) die("Kubo.RecursionNumber and Kubo.NumberofEnergyPoints must be positive");
+    // field sweep (MagfInit, magf.F90:20-98); values in tesla are converted once the cell area is known
+    if (in.has("MagField.Value")) {
+        j.field_by_value = true;
+        j.b_value = in.d("MagField.Value", 0.0);
+    } else if (in.has("MagField.Integer")) {
+        j.mbi = j.mbf = in.i("MagField.Integer", 0);
+    } else if (in.has("MagField.InitialB")) {
+        j.field_steps_by_value = true;
+        j.b_init = in.d("MagField.InitialB", 0.0);
+        j.b_final = in.d("MagField.FinalB", 0.0);
+    } else if (in.has("MagField.InitialInteger")) {
+        j.mbi = in.i("MagField.InitialInteger", 0);
+        j.mbf = in.i("MagField.FinalInteger", 0);
+        if (j.mbi > j.mbf) die("MagField.InitialInteger is above MagField.FinalInteger");
+    }
+    j.b_step = in.has("MagField.Step") ? in.d("MagField.Step", 1.0) : 0.0;
+    j.mstep = in.i("MagField.IntegerStep", 1);
+    j.prefix = in.s("Run.Prefix", "grabnes");
+    return j;
+}
+
+double cell_area(const double* u)
+{
+    const double v1 = u[1] * u[5] - u[2] * u[4], v2 = u[2] * u[3] - u[0] * u[5], v3 = u[0] * u[4] - u[1] * u[3];
+    return sqrt(v1 * v1 + v2 * v2 + v3 * v3);
+}
+
+// field sweep in flux quanta through the cell, once the area is known
+void resolve_fields(Job& j, double area)
+{
+    auto quanta = [&](double bmag) { return lround(area * 1.0e-20 * bmag / kFluxQuantum); };
+    if (j.field_by_value) j.mbi = j.mbf = quanta(j.b_value);
+    if (j.field_steps_by_value) {
+        j.mbi = quanta(j.b_init);
+        j.mbf = quanta(j.b_final);
+        if (j.mbi > j.mbf) die("MagField.InitialB is above MagField.FinalB");
+    }
+    if (j.b_step > 0.0) j.mstep = quanta(j.b_step);
+    if (j.mstep <= 0) j.mstep = 1;
+}
+
+// a double as gfortran's list-directed output writes it: 17 significant digits in a 25-wide field, fixed
+// notation for 0.1 <= |x| < 1e16, otherwise a mantissa and a three-digit exponent.  The decimal exponent
+// is taken from the correctly rounded 17-digit form, so the text always reads back to the same double.
+std::string fortran_ld(double x)
+{
+    char sci[64], buf[80];
+    snprintf(sci, sizeof sci, "%.16e", x);
+    const char* ep = strchr(sci, 'e');
+    const int e = ep ? atoi(ep + 1) : 0;
+    if (x == 0.0) {
+        snprintf(buf, sizeof buf, "   0.0000000000000000     ");
+    } else if (e >= -1 && e < 16) {
+        snprintf(buf, sizeof buf, "   %.*f     ", 16 - e, x);
+    } else {
+        const std::string mant(sci, ep ? (size_t)(ep - sci) : strlen(sci));
+        snprintf(buf, sizeof buf, "   %sE%c%03d", mant.c_str(), e < 0 ? '-' : '+', abs(e));
+    }
+    return buf;
+}
+
+void write_column(const std::string& path, const std::vector<double>& v)
+{
+    FILE* f = fopen(path.c_str(), "w");
+    if (!f) die("cannot write " + path);
+    for (double x : v) fprintf(f, "%s\n", fortran_ld(x).c_str());
+    fclose(f);
+}
+
+void ck(int rc, gbn_ctx* ctx, const char* what)
+{
+    if (rc != GBN_OK) die(std::string(what) + ": " + (ctx ? gbn_last_error(ctx) : "error " + std::to_string(rc)));
+}
+
+void print_job(const Job& j)
+{
+    const gbn_model& m = j.model;
+    printf("{\"kind\": %d, \"aG\": %.17g, \"cell_size\": %d, \"super_cell\": %d, \"m\": [%d, %d, %d, %d], "
+           "\"height\": %.17g, \"d_interlayer\": %.17g, \"g0\": %.17g, \"cut2intra\": %.17g, \"cut2inter\": %.17g, "
+           "\"second_layer\": %d, \"moire\": %d, \"nrecurs\": %d, \"eta\": %.17g, \"n_en\": %d, \"emin\": %.17g, "
+           "\"emax\": %.17g, \"seed\": %d, \"prefix\": \"%s\", \"model\": {\"tbnn\": %d, \"intralayer\": %d, "
+           "\"moire_onsite\": %d, \"moire_offdiag\": %d, \"moire_mid\": %d, \"moire_twisted\": %d, \"eps\": %.17g, "
+           "\"twist_rad\": %.17g, \"C0\": %.17g, \"Cz\": %.17g, \"Cab\": %.17g, \"interlayer\": %d, "
+           "\"vpppi0\": %.17g, \"vppsigma0\": %.17g, \"bl_delta\": %.17g, \"anderson\": %d, \"anderson_w\": %.17g, "
+           "\"tksl2\": %.17g}}\n",
+           j.cell.kind, j.cell.aG, j.cell.cell_size, j.cell.super_cell, j.cell.m[0], j.cell.m[1], j.cell.m[2], j.cell.m[3],
+           j.cell.height, j.cell.d_interlayer, j.g0, j.cut2intra, j.cut2inter, (int)j.second_layer, (int)j.moire,
+           j.nrecurs, j.eta, j.n_en, j.emin, j.emax, j.seed, j.prefix.c_str(), m.tbnn, m.intralayer, m.moire_onsite,
+           m.moire_offdiag, m.moire_mid, m.moire_twisted, m.eps, m.twist_rad, m.C0, m.Cz, m.Cab, m.interlayer,
+           m.vpppi0, m.vppsigma0, m.bl_delta, m.anderson, m.anderson_w, m.tksl[2]);
+}
+
+int run(const Job& j0)
+{
+    Job j = j0;
+    int64_t n = 0;
+    ck(gbn_cell_atoms(&j.cell, &n), nullptr, "gbn_cell_atoms");
+    std::vector<double> ucell(9), rat((size_t)3 * n);
+    std::vector<int32_t> species((size_t)n), layer((size_t)n);
+    double twist = 0.0;
+    ck(gbn_build_cell(&j.cell, ucell.data(), rat.data(), species.data(), layer.data(), &twist), nullptr,
+       "gbn_build_cell");
+    const double area = cell_area(ucell.data());
+    resolve_fields(j, area);
+    printf("grabnes: %lld atoms, cell area %.6f Ang^2, g0 = %.6f eV\n", (long long)n, area, j.g0);
+    gbn_ctx* ctx = nullptr;
+    const char* dev = getenv("GRABNES_DEVICE");
+    ck(gbn_create(&ctx, dev ? atoi(dev) : 0), nullptr, "gbn_create (no CUDA device?)");
+    ck(gbn_set_geometry(ctx, n, rat.data(), species.data(), layer.data(), ucell.data()), ctx, "gbn_set_geometry");
+    int32_t maxn = 0;
+    int64_t total = 0;
+    ck(gbn_neighbours(ctx, j.cut2intra, j.cut2inter, j.second_layer ? 1 : 0, &maxn, &total), ctx, "gbn_neighbours");
+    printf("grabnes: %lld neighbour entries (at most %d per atom)\n", (long long)total, maxn);
+    std::vector<double> rat_on, rat_hop;
+    if (j.moire) {   // the positions the reference's moire routines see after their own conversions
+        rat_on = rat;
+        ck(gbn_cart_roundtrip(n, ucell.data(), rat_on.data()), nullptr, "gbn_cart_roundtrip");
+        rat_hop = rat_on;
+        ck(gbn_cart_roundtrip(n, ucell.data(), rat_hop.data()), nullptr, "gbn_cart_roundtrip");
+    }
+    // Anderson disorder and the start vector draw the same stream (random_seed(PUT=SeedValue) in both)
+    std::vector<double> u((size_t)n);
+    ck(gbn_rng_uniform(j.seed, n, u.data()), nullptr, "gbn_rng_uniform");
+    const bool magfield = !(j.mbi == 0 && j.mbf == 0);
+    std::vector<double> a((size_t)j.nrecurs), b((size_t)j.nrecurs), energy((size_t)j.n_en + 1), dos((size_t)j.n_en + 1);
+    for (long mb = j.mbi; mb <= j.mbf; mb += (magfield ? j.mstep : 1)) {
+        std::string prefix = j.prefix;
+        if (magfield && j.mbi != j.mbf) {
+            const double bmag = mb * kFluxQuantum / (area * 1.0e-20);
+            char folder[64];
+            snprintf(folder, sizeof folder, "m%05ld_B%.4f", mb, bmag);
+            if (mkdir(folder, 0755) != 0 && errno != EEXIST) die(std::string("cannot create folder ") + folder);
+            prefix = std::string("./") + folder + "/" + j.prefix;
+            printf("grabnes: field %ld of %ld..%ld, %.5f T, files in %s\n", mb, j.mbi, j.mbf, bmag, folder);
+        }
+        ck(gbn_assemble(ctx, &j.model, j.moire ? rat_on.data() : nullptr, j.moire ? rat_hop.data() : nullptr,
+                        j.model.anderson ? u.data() : nullptr),
+           ctx, "gbn_assemble");
+        if (magfield) {
+            const double bmag = mb * kFluxQuantum / (area * 1.0e-20);
+            ck(gbn_peierls(ctx, bmag * kPi / kFluxQuantum), ctx, "gbn_peierls");
+        }
+        ck(gbn_lanczos_phases(ctx, GBN_FP64, 1, u.data(), nullptr, j.nrecurs, a.data(), b.data()), ctx,
+           "gbn_lanczos_phases");
+        write_column(prefix + ".b0.dat", b);
+        write_column(prefix + ".a0.dat", a);
+        ck(gbn_cf_dos(ctx, 1, a.data(), b.data(), nullptr, j.nrecurs, j.eta, j.n_en, j.emin, j.emax, nullptr,
+                      energy.data(), dos.data()),
+           ctx, "gbn_cf_dos");
+        FILE* f = fopen((prefix + ".DOS").c_str(), "w");
+        if (!f) die("cannot write " + prefix + ".DOS");
+        for (int k = 0; k <= j.n_en; ++k) fprintf(f, "%s%s\n", fortran_ld(energy[k]).c_str(), fortran_ld(dos[k]).c_str());
+        fclose(f);
+        f = fopen((prefix + ".AB").c_str(), "w");
+        if (!f) die("cannot write " + prefix + ".AB");
+        fprintf(f, "%s\n", fortran_ld(1.0).c_str());
+        for (int k = 0; k < j.nrecurs; ++k) fprintf(f, "%s%s\n", fortran_ld(a[k]).c_str(), fortran_ld(b[k]).c_str());
+        fclose(f);
+        printf("grabnes: DOS written to %s.DOS and %s.AB\n", prefix.c_str(), prefix.c_str());
+        if (!magfield) break;
+    }
+    gbn_destroy(ctx);
+    return 0;
+}
+
+}  // namespace
+
+int main(int argc, char** argv)
+{
+    bool print = false;
+    std::string path = "Gendata.in";
+    for (int k = 1; k < argc; ++k) {
+        if (strcmp(argv[k], "--print-job") == 0) print = true;
+        else path = argv[k];
+    }
+    Input in;
+    in.load(path);
+    const Job j = job_from_input(in);
+    if (print) {
+        print_job(j);
+        return 0;
+    }
+    return run(j);
+}

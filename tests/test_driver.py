@@ -1,0 +1,123 @@
+"""The `grabnes Gendata.in` driver: its reading of the input against the package's key mapping (CPU),
+and its output files against the oracle for a field sweep (GPU)."""
+import json
+import math
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import refcases as R
+from oracle import oracle as orc
+
+G = pytest.importorskip("grabnes_b200")
+from grabnes_b200 import model as M  # noqa: E402
+
+DRIVER = os.path.join(os.path.dirname(G.__file__), "grabnes")
+
+INPUTS = {
+    "moire_sweep": {
+        "Run.Prefix": "generate", "Run.TypeOfSystem": "Graphene", "Structure.CellSize": 11, "Structure.SuperCell": 4,
+        "Moire.LatticePercent": -1.0 / 11.0, "Moire.Potential": True, "Moire.Jeil": True, "Moire.H0AndHZ": True,
+        "Moire.OffDiag": True, "Moire.OffDiagMidpoint": True, "Kubo.RecursionNumber": 120,
+        "Kubo.Epsilon": 0.004, "Kubo.EnergyMin": -0.3, "Kubo.EnergyMax": 0.3, "Kubo.SeedValue": 123456,
+    },
+    "tbg_former_names": {
+        "TypeOfSystem": "TwistedBilayerBasedOnMoireCell", "MoireCellParameters": (31, 30, 30, 31),
+        "TypeOfBL": "Koshino", "vpppi0": 2.7, "vppsigma0": 0.48, "BLdelta": 0.319, "InterlayerDistance": 3.35,
+        "Neigh.LayerNeighbors": 100, "Neigh.LayerDistFactor": 3.2005, "TB.Hopping": 2.7, "RecursionNumber": 150,
+    },
+    "anderson": {"Run.TypeOfSystem": "Graphene", "Structure.CellSize": 30, "Disorder.Anderson": True,
+                 "Disorder.AndersonAmp": 1.0, "Kubo.SeedValue": 5, "TB.NeighLevels": 2},
+}
+
+
+def _fmt(v):
+    if isinstance(v, bool):
+        return ".true." if v else ".false."
+    if isinstance(v, tuple):
+        return " ".join(str(x) for x in v)
+    if isinstance(v, float) and v < 0:
+        return f"0-{-v!r}"   # the reference's way of writing a negative number
+    return repr(v) if isinstance(v, float) else str(v)
+
+
+def _write(path, keys, extra=""):
+    with open(path, "w") as f:
+        f.write("# written by the test\n")
+        for k, v in keys.items():
+            f.write(f"{k} {_fmt(v)}   # a comment\n")
+        f.write(extra)
+
+
+def _print_job(path):
+    out = subprocess.run([DRIVER, "--print-job", path], check=True, capture_output=True, text=True).stdout
+    return json.loads(out)
+
+
+pytestmark_cpu = pytest.mark.skipif(not os.path.exists(DRIVER), reason="driver not built")
+
+
+@pytestmark_cpu
+@pytest.mark.parametrize("name", sorted(INPUTS))
+def test_driver_reads_input_like_the_package(tmp_path, name):
+    keys = INPUTS[name]
+    path = str(tmp_path / "Gendata.in")
+    _write(path, keys)
+    got = _print_job(path)
+    job = M.job_from_keys(keys)
+    assert got["g0"] == job["g0"]
+    assert got["cut2intra"] == job["cut2intra"] and got["cut2inter"] == job["cut2inter"]
+    assert got["moire"] == int(job["moire"])
+    assert got["nrecurs"] == job["kubo"]["nrecurs"] and got["seed"] == job["kubo"]["seed"]
+    assert math.isclose(got["eta"], job["kubo"]["eta"], rel_tol=1e-15)
+    assert math.isclose(got["emin"], job["kubo"]["emin"], rel_tol=1e-15)
+    m = job["model"]
+    for f in ("tbnn", "intralayer", "moire_onsite", "moire_offdiag", "moire_mid", "moire_twisted", "interlayer",
+              "anderson"):
+        assert got["model"][f] == getattr(m, f), f
+    for f in ("eps", "C0", "Cz", "Cab", "vpppi0", "vppsigma0", "bl_delta", "anderson_w"):
+        assert math.isclose(got["model"][f], getattr(m, f), rel_tol=1e-15, abs_tol=1e-300), f
+    assert got["cell_size"] == job["cell"]["cell_size"] and got["super_cell"] == job["cell"]["super_cell"]
+    assert tuple(got["m"]) == tuple(job["cell"]["m"])
+
+
+@pytestmark_cpu
+def test_driver_expressions(tmp_path):
+    path = str(tmp_path / "Gendata.in")
+    _write(path, {"TB.Hopping": "2*1.35", "Kubo.Epsilon": "1.0d-2", "Kubo.EnergyMin": "-(1+2)*sqrt(4)",
+                  "Kubo.EnergyMax": "2**3", "Kubo.RecursionNumber": "10*10"})
+    got = _print_job(path)
+    assert got["g0"] == 2.7 and got["nrecurs"] == 100
+    assert math.isclose(got["eta"] * 2.7, 0.01, rel_tol=1e-15)
+    assert math.isclose(got["emin"] * 2.7, -6.0, rel_tol=1e-15) and math.isclose(got["emax"] * 2.7, 8.0, rel_tol=1e-15)
+
+
+@pytest.mark.gpu
+def test_driver_field_sweep_against_oracle(tmp_path):
+    """A three-field sweep of the moire model: one folder per field with the reference's files; a_n, b_n
+    and the DOS of every field against the oracle's recursion and continued fraction.  120 steps: this
+    3872-atom cell is small and symmetric, and beyond about 150 steps two FP64 recursions that differ
+    only in summation order part ways (the recursion's own parity is tested on larger cells)."""
+    keys = dict(INPUTS["moire_sweep"])
+    path = str(tmp_path / "Gendata.in")
+    _write(path, keys, "MagField.InitialInteger 0\nMagField.FinalInteger 4\nMagField.IntegerStep 2\n")
+    subprocess.run([DRIVER, path], check=True, cwd=str(tmp_path), capture_output=True, text=True)
+    folders = sorted(d for d in os.listdir(tmp_path) if d.startswith("m0"))
+    assert [f[:6] for f in folders] == ["m00000", "m00002", "m00004"]
+    base = dict(TypeOfSystem="Graphene", CellSize=11, SuperCell=4, LatticePercent=-1.0 / 11.0, MoirePotential=True,
+                MoireJeil=True, MoireH0AndHZ=True, MoireOffDiag=True, MoireOffDiagMidpoint=True)
+    for folder, mb in zip(folders, (0, 2, 4)):
+        r = R.build(dict(base, MagFieldInteger=mb))
+        n, g0 = r["geo"]["n"], r["g0"]
+        a0, b0 = orc.recursion(r["nb"], r["hop"], r["h0"], orc.init_wf(n, 123456), 120, 0)
+        a = np.loadtxt(tmp_path / folder / "generate.a0.dat")
+        b = np.loadtxt(tmp_path / folder / "generate.b0.dat")
+        assert np.abs(a - a0).max() <= 1e-10 * np.abs(a0).max() and np.abs(b - b0).max() <= 1e-10 * np.abs(b0).max()
+        e0, d0 = orc.frac(a0, b0, 0.004 / g0, 1000, -0.3 / g0, 0.3 / g0)
+        dos = np.loadtxt(tmp_path / folder / "generate.DOS")
+        assert np.abs(dos[:, 0] - e0).max() == 0.0
+        assert np.abs(dos[:, 1] - d0).sum() <= 1e-6 * np.abs(d0).sum()   # normalised L1, the DOS bar
+        ab = np.loadtxt(tmp_path / folder / "generate.AB", skiprows=1)
+        assert np.array_equal(ab[:, 0], a) and np.array_equal(ab[:, 1], b)
