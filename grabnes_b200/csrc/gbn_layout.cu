@@ -1,7 +1,7 @@
 // Row order and grouped sliced-ELL layout of the Hamiltonian for the recursion kernels.
 //
-// Rows are renumbered along a Morton (Z-order) curve over the fractional coordinates of the atoms
-// (cells of about 4 Angstrom), both layers of a bilayer falling into the same cells.  Consecutive
+// Rows are renumbered along a Hilbert curve over the fractional coordinates of the atoms (cells of about
+// 4 Angstrom), both layers of a bilayer falling into the same cells.  Consecutive
 // slices then touch a compact region of the vectors, so the gathers of neighbouring rows hit L1/L2.
 // The reference's own atom order (kept for all exchanged arrays) is restored at the boundary by the
 // permutation perm[new] = reference index.  Groups of G consecutive rows then share one list of
@@ -30,19 +30,32 @@ __global__ void k_identity(int32_t* perm, int32_t* iperm, int64_t n)
     }
 }
 
-__device__ __forceinline__ uint64_t spread_bits(uint32_t v)
+// Position of cell (x, y) along a Hilbert curve filling the 2^order x 2^order grid (the classic
+// quadrant-rotation construction: at each level take the quadrant's two bits, then rotate / reflect the
+// coordinates into that quadrant's frame).  Unlike the Z-order curve it never jumps between distant
+// cells, so atoms close in the row order are close in space.
+__device__ __forceinline__ uint64_t hilbert_index(uint32_t x, uint32_t y, int order)
 {
-    uint64_t x = v & 0x1fffffu;
-    x = (x | (x << 32)) & 0x1f00000000ffffULL;
-    x = (x | (x << 16)) & 0x1f0000ff0000ffULL;
-    x = (x | (x << 8)) & 0x100f00f00f00f00fULL;
-    x = (x | (x << 4)) & 0x10c30c30c30c30c3ULL;
-    x = (x | (x << 2)) & 0x1249249249249249ULL;
-    return x;
+    uint64_t d = 0;
+    for (uint32_t s = 1u << (order - 1); s > 0; s >>= 1) {
+        const uint32_t rx = (x & s) ? 1u : 0u;
+        const uint32_t ry = (y & s) ? 1u : 0u;
+        d += (uint64_t)s * s * ((3u * rx) ^ ry);
+        if (ry == 0) {   // rotate the quadrant
+            if (rx == 1) {
+                x = s - 1 - (x & (s - 1)) + (x & ~(s - 1));
+                y = s - 1 - (y & (s - 1)) + (y & ~(s - 1));
+            }
+            const uint32_t t = x;
+            x = y;
+            y = t;
+        }
+    }
+    return d;
 }
 
-__global__ void k_morton_keys(const double* rat, int64_t n, double a1x, double a1y, double a2x, double a2y,
-                              int32_t g1, int32_t g2, uint64_t* keys, int32_t* idx)
+__global__ void k_curve_keys(const double* rat, int64_t n, double a1x, double a1y, double a2x, double a2y,
+                              int32_t g1, int32_t g2, int order, uint64_t* keys, int32_t* idx)
 {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -55,7 +68,7 @@ __global__ void k_morton_keys(const double* rat, int64_t n, double a1x, double a
     int32_t ix = (int32_t)(s1 * g1), iy = (int32_t)(s2 * g2);
     ix = ix < 0 ? 0 : (ix >= g1 ? g1 - 1 : ix);
     iy = iy < 0 ? 0 : (iy >= g2 ? g2 - 1 : iy);
-    keys[i] = spread_bits((uint32_t)ix) | (spread_bits((uint32_t)iy) << 1);
+    keys[i] = hilbert_index((uint32_t)ix, (uint32_t)iy, order);
     idx[i] = (int32_t)i;
 }
 
@@ -90,7 +103,9 @@ int build_spatial_perm(gbn_ctx* c)
     GBN_CK(c, c->perm.ensure(sizeof(int32_t) * c->n));
     GBN_CK(c, c->iperm.ensure(sizeof(int32_t) * c->n));
     const unsigned grd = (unsigned)((c->n + 255) / 256);
-    k_morton_keys<<<grd, 256, 0, c->stream>>>(c->rat.as<double>(), c->n, a1x, a1y, a2x, a2y, g1, g2,
+    int order = 1;   // Hilbert curve over the smallest 2^order grid that holds the cells
+    while ((1 << order) < g1 || (1 << order) < g2) ++order;
+    k_curve_keys<<<grd, 256, 0, c->stream>>>(c->rat.as<double>(), c->n, a1x, a1y, a2x, a2y, g1, g2, order,
                                               keys.as<uint64_t>(), c->perm.as<int32_t>());
     GBN_CK_LAUNCH(c);
     thrust::device_ptr<uint64_t> kp(keys.as<uint64_t>());
