@@ -492,4 +492,13 @@ int gbn_kubo_evol(gbn_ctx* c, int32_t precision, int32_t nrhs, const double* coe
     return kubo_evol(c, precision, nrhs, coef, npol, ac, bc, dir, psi, zupsi);
 }
 
+int gbn_dos_gradient(gbn_ctx* c, const gbn_model* model, double g0, const double* u, int32_t nrecurs, int32_t checkpoint,
+                     double eta, int32_t n_en, double emin, double emax, const double* target, double* loss, double* grad,
+                     double* dos, double* a, double* b)
+{
+    if (!c) return GBN_ERR_ARG;
+    cudaSetDevice(c->device);
+    return dos_gradient(c, model, g0, u, nrecurs, checkpoint, eta, n_en, emin, emax, target, loss, grad, dos, a, b);
+}
+
 }  // extern "C"

@@ -183,6 +183,11 @@ int neigh_search(gbn_ctx* c, double cut2intra, double cut2inter, int32_t second_
 int assemble(gbn_ctx* c, const gbn_model* m, const double* d_rat_on, const double* d_rat_hop, const double* d_uniform);
 int peierls(gbn_ctx* c, double flux);
 
+// gradient of a DOS loss (gbn_adjoint.cu)
+int dos_gradient(gbn_ctx* c, const gbn_model* m, double g0, const double* u_host, int32_t K, int32_t C, double eta,
+                 int32_t n_en, double emin, double emax, const double* target, double* loss_out, double* grad,
+                 double* dos, double* a_out, double* b_out);
+
 // Chebyshev (gbn_cheb.cu)
 int cheb_evolve(gbn_ctx* c, int32_t prec, int32_t nrhs, const double* c_host, int32_t npol, double ac, double bc,
                 double* z_host);

@@ -124,6 +124,16 @@ __device__ double d_f2g2_shell(const gbn_model& m, double dist)
     return 0.0;
 }
 
+// smooth interlayer cutoff factor (1 when the model has none)
+__device__ __forceinline__ double smooth_cut(const gbn_model& m, double rho)
+{
+    if (!(m.inter_smooth_w > 0.0)) return 1.0;
+    const double w = m.inter_smooth_w, r0 = m.inter_cut_rho - w;
+    if (rho <= r0) return 1.0;
+    if (rho >= m.inter_cut_rho) return 0.0;
+    return 0.5 * (1.0 + cospi((rho - r0) / w));
+}
+
 __global__ void k_hopping(gbn_model m, int64_t n, const double* rat, const int32_t* species, const int32_t* layer,
                           int32_t max_neigh, const int32_t* nneigh, const int32_t* nlist, const double* neighd,
                           double2* hopp)
@@ -173,7 +183,7 @@ __global__ void k_hopping(gbn_model m, int64_t n, const double* rat, const int32
                     const double vsig = m.vppsigma0 * exp(-(dist - m.d_interlayer) / m.bl_delta);
                     const double vpi = m.vpppi0 * exp(-(dist - m.aCC) / m.bl_delta);
                     const double q = Dz / dist;
-                    hr = hr + (vpi * (1.0 - q * q) + vsig * (q * q));
+                    hr = hr + (vpi * (1.0 - q * q) + vsig * (q * q)) * smooth_cut(m, sqrt(Dx * Dx + Dy * Dy));
                 } else {
                     const double d = sqrt(Dx * Dx + Dy * Dy);
                     hr = hr + m.g_intlay * exp(-d / m.d_interlayer);

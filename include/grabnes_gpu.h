@@ -61,6 +61,12 @@ typedef struct gbn_model {
     int32_t anderson;      /* Disorder.Anderson: add (u_i - 0.5) * anderson_w         */
     double  anderson_w;
     double  e0_c;          /* TB.OnSiteC/g0                                           */
+    /* Smooth interlayer cutoff (no counterpart in the reference, whose cutoff is the hard edge of the
+     * neighbour table): with inter_smooth_w > 0 the interlayer hoppings are multiplied by
+     * s(rho) = 1 for rho <= rho_c - w, (1 + cos(pi (rho - rho_c + w) / w)) / 2 up to rho_c, 0 beyond,
+     * rho the in-plane distance [Ang] and rho_c = inter_cut_rho.  0 = the reference's hard cutoff. */
+    double  inter_cut_rho;
+    double  inter_smooth_w;
 } gbn_model;
 
 /* ---- host-side cell construction and random numbers (no context, no GPU needed) ------ */
@@ -193,6 +199,20 @@ int gbn_kubo_evol(gbn_ctx* ctx, int32_t precision, int32_t nrhs, const double* c
                   double bc, int32_t dir, double* psi, double* zupsi);
 /* NeighD(3,maxNeigh,N) for gbn_kubo_evol after gbn_load_hamiltonian. */
 int gbn_set_neighd(gbn_ctx* ctx, const double* neighd);
+
+/* ---- gradient of a DOS loss ------------------------------------------------------------------ */
+/* No counterpart in the reference.  Loss L = sum_E (DOS(E) - target(E))^2, DOS from one start vector
+ * (phases from the uniform draws u [N]) by an FP64 recursion of nrecurs steps and the continued
+ * fraction (eta, n_en, emin, emax as for gbn_cf_dos, units of g0; target [n_en+1]).  grad [4] =
+ * dL/d(t, Vpp_sigma0, delta, w): the intralayer nearest-neighbour hopping [eV], the sigma two-centre
+ * amplitude [eV], the two-centre decay length [Ang] and the width of the smooth interlayer cutoff
+ * [Ang], for the Hamiltonian last assembled with `model` (gbn_assemble; real hoppings, geometry and
+ * NeighD on the context; g0 [eV] the energy unit).  Reverse sweep through the same sparse product
+ * (the adjoint of the three-term recurrence), with the recursion vectors checkpointed every
+ * `checkpoint` steps and recomputed in between.  dos [n_en+1], a, b [nrecurs] may be NULL. */
+int gbn_dos_gradient(gbn_ctx* ctx, const gbn_model* model, double g0, const double* u, int32_t nrecurs,
+                     int32_t checkpoint, double eta, int32_t n_en, double emin, double emax, const double* target,
+                     double* loss, double* grad, double* dos, double* a, double* b);
 
 /* ---- recursion without device allocation ------------------------------------------------------ */
 /* No counterpart in the reference: an addition for hosts that cannot allocate device memory.
