@@ -152,10 +152,13 @@ def build(keys):
 
 
 def gpu_model(m):
-    """The same model as the library's gbn_model structure."""
+    """The same model as the library's gbn_model structure.  Fields the oracle does not have (the smooth
+    interlayer cutoff, which the reference lacks) stay 0: the reference's hard cutoff."""
     import grabnes_b200 as G
     out = G.Model()
     for name, _ in G.Model._fields_:
+        if not hasattr(m, name):
+            continue
         v = getattr(m, name)
         if hasattr(v, "__len__"):
             arr = getattr(out, name)
