@@ -305,9 +305,13 @@ def run_reference(args, ws, rank):
     setup_s = time.time() - t0
     n = r["geo"]["n"]
     psi = orc.init_wf(n, SEED)
-    steps = args.cpu_steps
-    for _ in range(args.warmup):
-        orc.recursion(r["nb"], r["hop"], r["h0"], psi, steps, cores)
+    # one short first-touch run, which also sizes the samples to about 15 s of CPU work each (at most
+    # --cpu-steps); the CPU needs no further warm-up, so W only bounds it
+    t = time.perf_counter()
+    probe = 20
+    orc.recursion(r["nb"], r["hop"], r["h0"], psi, probe, cores)
+    rate = probe / (time.perf_counter() - t)
+    steps = int(max(20, min(args.cpu_steps, 15.0 * rate)))
     ts = []
     for _ in range(args.steps):
         t = time.perf_counter()
@@ -320,7 +324,8 @@ def run_reference(args, ws, rank):
            "vs_baseline": None, "dtype": "c128", "data": "synthetic (reference model)", "impl": "reference",
            "config": {"workload": WORKLOAD_NAME, "atoms": n, "sample_steps": steps, "vectors": 1},
            "cpu_baseline": {"value": value, "unit": "atom-steps/s", "cores": cores, "kind": "port",
-                            "sample": f"1 vector x {steps} steps per bench step (setup {setup_s:.0f} s untimed)"},
+                            "sample": f"1 vector x {steps} recursion steps of the full {n}-atom Hamiltonian per bench "
+                                      f"step (complex128, reference layout; setup {setup_s:.0f} s untimed)"},
            "e2e": {"value": value, "unit": "atom-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
 
