@@ -13,7 +13,8 @@
 //     <prefix>.DOS                       E and DOS in units of g0          (kubosubs.F90:247-276)
 //     <prefix>.AB                        the norm, then a_n b_n per line
 // inside m<m:05>_B<B:.4f>/ when the sweep has more than one field.  Everything on the device goes
-// through the C ABI of include/grabnes_gpu.h.
+// through the C ABI of include/grabnes_gpu.h.  Without Calculate.OnlyDOS the Kubo time evolution follows
+// (KuboInterval, KuboCn -> <prefix>.cn.dat; KuboTEvol -> <prefix>.Z2_<step>.dat, <prefix>.AB_<step>.dat).
 #include <errno.h>
 #include <math.h>
 #include <stdio.h>
@@ -287,6 +288,9 @@ struct Job {
     bool second_layer = false, moire = false;
     int nrecurs = 0, n_en = 0, seed = 0;
     double eta = 0, emin = 0, emax = 0;   // units of g0
+    bool only_dos = false, polynomials = false;
+    int npol = 100, nt = 500, nwr = 10;
+    double dt = 5.0;   // units of hbar / g0
     long mbi = 0, mbf = 0, mstep = 1;
     bool field_by_value = false, field_steps_by_value = false;
     double b_value = 0, b_init = 0, b_final = 0, b_step = 0;
@@ -303,7 +307,6 @@ Job job_from_input(const Input& in)
     else die("Run.TypeOfSystem " + system + " is not on the recursion path of this program");
     if (!in.l("Kubo.Calc", true)) die("this program runs the recursion (Kubo.Calc .true.) only");
     if (in.l("Diag.Calc", false)) die("exact diagonalisation (Diag.Calc) is not part of this program");
-    if (!in.l("Calculate.OnlyDOS", true)) die("time evolution (Calculate.OnlyDOS .false.) is run through the library API");
     j.cell.aG = aG;
     j.cell.cell_size = (int32_t)in.i("Structure.CellSize", 50);
     j.cell.super_cell = (int32_t)in.i("Structure.SuperCell", 1);
@@ -379,6 +382,14 @@ Job job_from_input(const Input& in)
     j.emax = in.d("Kubo.EnergyMax", 4.0) / g0;
     j.seed = (int)in.i("Kubo.SeedValue", 123456);
     if (j.nrecurs < 1 || j.n_en < 1) die("Kubo.RecursionNumber and Kubo.NumberofEnergyPoints must be positive");
+    // time evolution (CalcKubo, calc.F90:164-170, 545-556): it follows the DOS unless Calculate.OnlyDOS
+    j.only_dos = in.l("Calculate.OnlyDOS", false);
+    j.polynomials = in.l("Calculate.Polynomials", false);
+    j.npol = (int)in.i("Kubo.NumberofPolynomials", 100);
+    j.nt = (int)in.i("Kubo.NumberofTimeSteps", 500);
+    j.nwr = (int)in.i("Kubo.WriteNumberofSteps", 10);
+    j.dt = in.d("Kubo.TimeStep", 5.0);
+    if (j.npol < 1 || j.nt < 0 || j.nwr < 1) die("Kubo.NumberofPolynomials and Kubo.WriteNumberofSteps must be positive");
     // field sweep (MagfInit, magf.F90:20-98); values in tesla are converted once the cell area is known
     if (in.has("MagField.Value")) {
         j.field_by_value = true;
@@ -459,16 +470,73 @@ void print_job(const Job& j)
     printf("{\"kind\": %d, \"aG\": %.17g, \"cell_size\": %d, \"super_cell\": %d, \"m\": [%d, %d, %d, %d], "
            "\"height\": %.17g, \"d_interlayer\": %.17g, \"g0\": %.17g, \"cut2intra\": %.17g, \"cut2inter\": %.17g, "
            "\"second_layer\": %d, \"moire\": %d, \"nrecurs\": %d, \"eta\": %.17g, \"n_en\": %d, \"emin\": %.17g, "
-           "\"emax\": %.17g, \"seed\": %d, \"prefix\": \"%s\", \"model\": {\"tbnn\": %d, \"intralayer\": %d, "
+           "\"emax\": %.17g, \"seed\": %d, \"prefix\": \"%s\", \"only_dos\": %d, \"npol\": %d, \"nt\": %d, "
+           "\"nwr\": %d, \"dt\": %.17g, \"model\": {\"tbnn\": %d, \"intralayer\": %d, "
            "\"moire_onsite\": %d, \"moire_offdiag\": %d, \"moire_mid\": %d, \"moire_twisted\": %d, \"eps\": %.17g, "
            "\"twist_rad\": %.17g, \"C0\": %.17g, \"Cz\": %.17g, \"Cab\": %.17g, \"interlayer\": %d, "
            "\"vpppi0\": %.17g, \"vppsigma0\": %.17g, \"bl_delta\": %.17g, \"anderson\": %d, \"anderson_w\": %.17g, "
            "\"tksl2\": %.17g}}\n",
            j.cell.kind, j.cell.aG, j.cell.cell_size, j.cell.super_cell, j.cell.m[0], j.cell.m[1], j.cell.m[2], j.cell.m[3],
            j.cell.height, j.cell.d_interlayer, j.g0, j.cut2intra, j.cut2inter, (int)j.second_layer, (int)j.moire,
-           j.nrecurs, j.eta, j.n_en, j.emin, j.emax, j.seed, j.prefix.c_str(), m.tbnn, m.intralayer, m.moire_onsite,
+           j.nrecurs, j.eta, j.n_en, j.emin, j.emax, j.seed, j.prefix.c_str(), (int)j.only_dos, j.npol, j.nt, j.nwr,
+           j.dt, m.tbnn, m.intralayer, m.moire_onsite,
            m.moire_offdiag, m.moire_mid, m.moire_twisted, m.eps, m.twist_rad, m.C0, m.Cz, m.Cab, m.interlayer,
            m.vpppi0, m.vppsigma0, m.bl_delta, m.anderson, m.anderson_w, m.tksl[2]);
+}
+
+void write_pairs(const std::string& path, const std::vector<double>& x, const std::vector<double>& y, double head,
+                 bool with_head)
+{
+    FILE* f = fopen(path.c_str(), "w");
+    if (!f) die("cannot write " + path);
+    if (with_head) fprintf(f, "%s\n", fortran_ld(head).c_str());
+    for (size_t k = 0; k < x.size(); ++k) fprintf(f, "%s%s\n", fortran_ld(x[k]).c_str(), fortran_ld(y[k]).c_str());
+    fclose(f);
+}
+
+// KuboInterval + KuboCn (<prefix>.cn.dat: Re c_n and |c_n|), then, without Calculate.OnlyDOS, KuboTEvol
+// (kubo.F90:321-397): nT steps of KuboEvol along x from the start vector psi with zupsi = 0; every nWr
+// steps the recursion of zupsi / |zupsi| and the continued fraction weighted by |zupsi|^2 are written
+// to <prefix>.Z2_<step>.dat and <prefix>.AB_<step>.dat.
+void time_evolution(gbn_ctx* ctx, const Job& j, const std::vector<double>& u, const std::vector<double>& a,
+                    const std::vector<double>& b, const std::string& prefix, int64_t n)
+{
+    double ac = 0.0, bc = 0.0;
+    ck(gbn_cheb_interval(a.data(), b.data(), j.nrecurs, &ac, &bc), nullptr, "gbn_cheb_interval");
+    std::vector<double> c((size_t)2 * j.npol);
+    ck(gbn_cheb_coef(j.dt, ac, bc, j.npol, c.data()), nullptr, "gbn_cheb_coef");
+    std::vector<double> re((size_t)j.npol), ab((size_t)j.npol);
+    for (int k = 0; k < j.npol; ++k) {
+        re[(size_t)k] = c[(size_t)2 * k];
+        ab[(size_t)k] = hypot(c[(size_t)2 * k], c[(size_t)2 * k + 1]);
+    }
+    write_pairs(prefix + ".cn.dat", re, ab, 0.0, false);
+    if (j.only_dos) return;
+    std::vector<double> psi((size_t)2 * n), zu((size_t)2 * n, 0.0), zn((size_t)2 * n);
+    const double isn = 1.0 / sqrt((double)n);
+    for (int64_t i = 0; i < n; ++i) {
+        psi[(size_t)2 * i] = cos(2.0 * kPi * u[(size_t)i]) * isn;
+        psi[(size_t)2 * i + 1] = sin(2.0 * kPi * u[(size_t)i]) * isn;
+    }
+    std::vector<double> az((size_t)j.nrecurs), bz((size_t)j.nrecurs), energy((size_t)j.n_en + 1), dos((size_t)j.n_en + 1);
+    for (int it = 1; it <= j.nt; ++it) {
+        ck(gbn_kubo_evol(ctx, GBN_FP64, 1, c.data(), j.npol, ac, bc, 1, psi.data(), zu.data()), ctx, "gbn_kubo_evol");
+        if (it % j.nwr != 0) continue;
+        double norm = 0.0;
+        for (int64_t i = 0; i < 2 * n; ++i) norm += zu[(size_t)i] * zu[(size_t)i];
+        if (!(norm > 0.0)) continue;
+        const double s = 1.0 / sqrt(norm);
+        for (int64_t i = 0; i < 2 * n; ++i) zn[(size_t)i] = zu[(size_t)i] * s;
+        ck(gbn_lanczos(ctx, GBN_FP64, 1, zn.data(), nullptr, j.nrecurs, az.data(), bz.data()), ctx, "gbn_lanczos");
+        ck(gbn_cf_dos(ctx, 1, az.data(), bz.data(), nullptr, j.nrecurs, j.eta, j.n_en, j.emin, j.emax, &norm,
+                      energy.data(), dos.data()),
+           ctx, "gbn_cf_dos");
+        char tag[32];
+        snprintf(tag, sizeof tag, "%04d", it);
+        write_pairs(prefix + ".Z2_" + tag + ".dat", energy, dos, 0.0, false);
+        write_pairs(prefix + ".AB_" + tag + ".dat", az, bz, norm, true);
+        printf("grabnes: time step %d of %d, |ZUPsi|^2 = %.10g\n", it, j.nt, norm);
+    }
 }
 
 int run(const Job& j0)
@@ -538,6 +606,7 @@ int run(const Job& j0)
         for (int k = 0; k < j.nrecurs; ++k) fprintf(f, "%s%s\n", fortran_ld(a[k]).c_str(), fortran_ld(b[k]).c_str());
         fclose(f);
         printf("grabnes: DOS written to %s.DOS and %s.AB\n", prefix.c_str(), prefix.c_str());
+        if (j.polynomials || !j.only_dos) time_evolution(ctx, j, u, a, b, prefix, n);
         if (!magfield) break;
     }
     gbn_destroy(ctx);

@@ -22,6 +22,7 @@ INPUTS = {
         "Moire.LatticePercent": -1.0 / 11.0, "Moire.Potential": True, "Moire.Jeil": True, "Moire.H0AndHZ": True,
         "Moire.OffDiag": True, "Moire.OffDiagMidpoint": True, "Kubo.RecursionNumber": 120,
         "Kubo.Epsilon": 0.004, "Kubo.EnergyMin": -0.3, "Kubo.EnergyMax": 0.3, "Kubo.SeedValue": 123456,
+        "Calculate.OnlyDOS": True,
     },
     "tbg_former_names": {
         "TypeOfSystem": "TwistedBilayerBasedOnMoireCell", "MoireCellParameters": (31, 30, 30, 31),
@@ -121,3 +122,42 @@ def test_driver_field_sweep_against_oracle(tmp_path):
         assert np.abs(dos[:, 1] - d0).sum() <= 1e-6 * np.abs(d0).sum()   # normalised L1, the DOS bar
         ab = np.loadtxt(tmp_path / folder / "generate.AB", skiprows=1)
         assert np.array_equal(ab[:, 0], a) and np.array_equal(ab[:, 1], b)
+
+
+@pytest.mark.gpu
+def test_driver_time_evolution_against_oracle(tmp_path):
+    """Without Calculate.OnlyDOS: KuboInterval and KuboCn (<prefix>.cn.dat), then four steps of KuboEvol in
+    a field, writing the recursion of the commutator term every two steps (.AB_0002/.Z2_0002, ...),
+    against the oracle's KuboEvol loop."""
+    keys = {"Run.Prefix": "tev", "Run.TypeOfSystem": "Graphene", "Structure.CellSize": 60, "TB.Hopping": 2.7,
+            "MagField.Integer": 3, "Kubo.RecursionNumber": 80, "Kubo.NumberofEnergyPoints": 200,
+            "Kubo.Epsilon": 0.05, "Kubo.EnergyMin": -8.0, "Kubo.EnergyMax": 8.0, "Kubo.SeedValue": 11,
+            "Kubo.NumberofPolynomials": 40, "Kubo.TimeStep": 2.0, "Kubo.NumberofTimeSteps": 4,
+            "Kubo.WriteNumberofSteps": 2}
+    path = str(tmp_path / "Gendata.in")
+    _write(path, keys)
+    subprocess.run([DRIVER, path], check=True, cwd=str(tmp_path), capture_output=True, text=True)
+    r = R.build(dict(TypeOfSystem="Graphene", CellSize=60, Hopping=2.7, MagFieldInteger=3))
+    n, g0 = r["geo"]["n"], r["g0"]
+    psi = orc.init_wf(n, 11)
+    a, b = orc.recursion(r["nb"], r["hop"], r["h0"], psi, 80, 0)
+    ac, bc = orc.interval(a, b)
+    c = orc.cheb_coef(2.0, ac, bc, 40)
+    cn = np.loadtxt(tmp_path / "tev.cn.dat")
+    assert np.abs(cn[:, 0] - c.real).max() <= 1e-11 and np.abs(cn[:, 1] - np.abs(c)).max() <= 1e-11
+    zu = np.zeros(n, np.complex128)
+    for it in range(1, 5):
+        psi, zu = orc.evol(r["nb"], r["hop"], r["h0"], c, ac, bc, psi, zu, 1)
+        if it % 2:
+            continue
+        norm = float(np.vdot(zu, zu).real)
+        az, bz = orc.recursion(r["nb"], r["hop"], r["h0"], zu / np.sqrt(norm), 80, 0)
+        tag = f"{it:04d}"
+        ab = np.loadtxt(tmp_path / f"tev.AB_{tag}.dat", skiprows=1)
+        with open(tmp_path / f"tev.AB_{tag}.dat") as f:
+            assert abs(float(f.readline()) - norm) <= 1e-9 * norm
+        assert np.abs(ab[:, 0] - az).max() <= 1e-9 * np.abs(az).max()
+        assert np.abs(ab[:, 1] - bz).max() <= 1e-9 * np.abs(bz).max()
+        e0, d0 = orc.frac(az, bz, 0.05 / g0, 200, -8.0 / g0, 8.0 / g0, norm)
+        z2 = np.loadtxt(tmp_path / f"tev.Z2_{tag}.dat")
+        assert np.abs(z2[:, 1] - d0).sum() <= 1e-6 * np.abs(d0).sum()
