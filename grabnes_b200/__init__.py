@@ -50,6 +50,21 @@ class Cell(C.Structure):
 
 CELL_GRAPHENE, CELL_TBG_MOIRE = 0, 1
 
+
+class Pdos(C.Structure):
+    """gbn_pdos of include/grabnes_gpu.h: a Kubo.PDOS selection"""
+    _fields_ = [("mode", C.c_int32), ("xmin", C.c_double), ("xmax", C.c_double), ("ymin", C.c_double),
+                ("ymax", C.c_double), ("min_value", C.c_int32), ("super_cell", C.c_int32), ("cell_size", C.c_int32),
+                ("supermoire_length", C.c_double), ("aG", C.c_double), ("ignore_layers_1_4", C.c_int32),
+                ("atom_list", C.c_int32 * 6), ("atom_number", C.c_int32), ("pnp_delta", C.c_double),
+                ("number_of_layers", C.c_int32), ("stack", C.c_int32), ("n_bn1", C.c_int32), ("n_bn2", C.c_int32),
+                ("n_c", C.c_int32)]
+
+
+(PDOS_LAYER, PDOS_LAYER_SPECIES, PDOS_DIST, PDOS_MOIRE_SC1, PDOS_SUPERMOIRE, PDOS_SUPERMOIRE2, PDOS_SUPERMOIRE3,
+ PDOS_ATOM_LIST, PDOS_BY_NUMBER, PDOS_PNP) = range(1, 11)
+STACK_NONE, STACK_ENCAPSULATED_FOUR, STACK_T3BG = 0, 1, 2
+
 _lib = None
 
 
@@ -83,7 +98,8 @@ EXPORTS = ["gbn_cell_atoms", "gbn_build_cell", "gbn_cart_roundtrip", "gbn_rng_un
            "gbn_last_timing", "gbn_last_kernel_timing", "gbn_set_geometry", "gbn_neighbours", "gbn_get_neighbours", "gbn_assemble",
            "gbn_peierls", "gbn_get_hamiltonian", "gbn_load_hamiltonian", "gbn_lanczos", "gbn_lanczos_phases",
            "gbn_stage_phases", "gbn_run_staged", "gbn_cf_dos", "gbn_cheb_evolve", "gbn_kubo_evol", "gbn_set_neighd", "gbn_lanczos_noalloc",
-           "gbn_cheb_interval", "gbn_cheb_coef", "gbn_dos_gradient"]
+           "gbn_cheb_interval", "gbn_cheb_coef", "gbn_dos_gradient", "gbn_lanczos_sites", "gbn_lanczos_sets",
+           "gbn_pdos_atoms", "gbn_pdos_sets"]
 
 
 def _declare(L):
@@ -114,6 +130,13 @@ def _declare(L):
     L.gbn_lanczos.argtypes = [vp, i32, i32, _p(np.complex128), _opt(np.int32), i32, _p(np.float64), _p(np.float64)]
     L.gbn_lanczos_phases.argtypes = [vp, i32, i32, _p(np.float64), _opt(np.int32), i32, _p(np.float64),
                                      _p(np.float64)]
+    L.gbn_lanczos_sites.argtypes = [vp, i32, i32, _p(np.int64), _opt(np.int32), i32, _p(np.float64), _p(np.float64)]
+    L.gbn_lanczos_sets.argtypes = [vp, i32, i32, _p(np.int32), _p(np.float64), _p(np.float64), _opt(np.int32), i32,
+                                   _p(np.float64), _p(np.float64)]
+    L.gbn_pdos_atoms.argtypes = [C.POINTER(Pdos), i64, _p(np.float64), _p(np.int32), _p(np.int32), _p(np.float64), i64,
+                                 C.POINTER(i64), _opt(np.int64), _opt(np.float64)]
+    L.gbn_pdos_sets.argtypes = [C.POINTER(Pdos), i64, _p(np.int32), _p(np.int32), i32, C.POINTER(i32), _p(np.int32),
+                                _p(np.int32), _p(np.int32), _p(np.float64)]
     L.gbn_stage_phases.argtypes = [vp, i32, i32, _p(np.float64)]
     L.gbn_run_staged.argtypes = [vp, i32, _opt(np.float64), _opt(np.float64)]
     L.gbn_cf_dos.argtypes = [vp, i32, _p(np.float64), _p(np.float64), _opt(np.int32), i32, d, i32, d, d,
@@ -265,6 +288,28 @@ class Context:
                                             b.reshape(-1)))
         return a, b
 
+    def lanczos_sites(self, sites, nsteps, precision=GBN_FP64):
+        """Local DOS recursion of single atoms: unit start vectors on sites (1-based), one per vector."""
+        st = np.ascontiguousarray(np.atleast_1d(sites), np.int64)
+        ns = np.broadcast_to(np.asarray(nsteps, np.int32), (len(st),)).copy()
+        nmax = int(ns.max())
+        a = np.zeros((len(st), nmax))
+        b = np.zeros((len(st), nmax))
+        self._ck(self._L.gbn_lanczos_sites(self._h, precision, len(st), st, ns, nmax, a.reshape(-1), b.reshape(-1)))
+        return a, b
+
+    def lanczos_sets(self, set_of_atom, u, assumed, nsteps, precision=GBN_FP64):
+        """Layer / layer-and-species DOS recursion: random phases on each set of atoms (gbn_lanczos_sets)."""
+        so = _c(set_of_atom, np.int32)
+        asm = np.ascontiguousarray(np.atleast_1d(assumed), np.float64)
+        ns = np.broadcast_to(np.asarray(nsteps, np.int32), (len(asm),)).copy()
+        nmax = int(ns.max())
+        a = np.zeros((len(asm), nmax))
+        b = np.zeros((len(asm), nmax))
+        self._ck(self._L.gbn_lanczos_sets(self._h, precision, len(asm), so, _c(u, np.float64), asm, ns, nmax,
+                                          a.reshape(-1), b.reshape(-1)))
+        return a, b
+
     def stage_phases(self, u, precision=GBN_MIXED):
         uu = np.ascontiguousarray(np.atleast_2d(u), np.float64)
         self._staged = uu.shape[0]
@@ -332,6 +377,36 @@ def cheb_coef(dt, ac, bc, npol):
     if rc != 0:
         raise GbnError(rc, "gbn_cheb_coef failed")
     return c
+
+
+def pdos_atoms(p, rat, species, layer, ucell):
+    """Atoms (1-based) of a single-atom Kubo.PDOS selection and the positions written to their coords files."""
+    r = _c(rat, np.float64).reshape(-1)
+    n = len(r) // 3
+    sp, ly, uc = _c(species, np.int32), _c(layer, np.int32), _c(ucell, np.float64)
+    cnt = C.c_int64()
+    rc = lib().gbn_pdos_atoms(C.byref(p), n, r, sp, ly, uc, 0, C.byref(cnt), None, None)
+    if rc:
+        raise GbnError(rc, "bad PDOS selection")
+    atoms = np.zeros(max(cnt.value, 1), np.int64)
+    coords = np.zeros(3 * max(cnt.value, 1))
+    rc = lib().gbn_pdos_atoms(C.byref(p), n, r, sp, ly, uc, cnt.value, C.byref(cnt), atoms, coords)
+    if rc:
+        raise GbnError(rc, "bad PDOS selection")
+    return atoms[:cnt.value], coords.reshape(-1, 3)[:cnt.value]
+
+
+def pdos_sets(p, species, layer, cap=4096):
+    """Sets of a layer Kubo.PDOS selection: (set_of_atom, layers, species, assumed counts)."""
+    sp, ly = _c(species, np.int32), _c(layer, np.int32)
+    so = np.zeros(len(sp), np.int32)
+    sl, ss, asm = np.zeros(cap, np.int32), np.zeros(cap, np.int32), np.zeros(cap)
+    ns = C.c_int32()
+    rc = lib().gbn_pdos_sets(C.byref(p), len(sp), sp, ly, cap, C.byref(ns), so, sl, ss, asm)
+    if rc:
+        raise GbnError(rc, "bad PDOS selection")
+    k = ns.value
+    return so, sl[:k], ss[:k], asm[:k]
 
 
 def build_cell(kind, aG=2.46, cell_size=50, super_cell=1, m=(0, 0, 0, 0), height=40.0, d_interlayer=3.35):

@@ -33,16 +33,15 @@ static int tile_width(int nrhs)
     return t;
 }
 
-// Runs the recursion for all right-hand sides in tiles of at most 32; inputs are either complex start
-// vectors (psi) or uniform draws (phases), [nrhs][n] on the host.
-static int run_tiled(gbn_ctx* c, int prec, int nrhs, const double* host_in, bool phases, const int32_t* nsteps,
-                     int32_t nmax, double* a, double* b)
+// Runs the recursion for all right-hand sides in tiles of at most 32; start(r0, cnt) writes the start
+// vectors of right-hand sides r0 .. r0 + cnt - 1 into the tile (after lanczos_prepare).
+template <typename Start>
+static int run_tiles(gbn_ctx* c, int prec, int nrhs, Start&& start, const int32_t* nsteps, int32_t nmax, double* a,
+                     double* b)
 {
     const int T = tile_width(nrhs);
     int rc = lanczos_prepare(c, prec, T);
     if (rc) return rc;
-    const size_t per = (size_t)c->n * (phases ? 1 : 2);
-    GBN_CK(c, c->upload.ensure(sizeof(double) * per * T));
     double step_ms = 0.0, spmm_sum = 0.0, upd_sum = 0.0;
     int64_t launches = 0;
     int tiles = 0;
@@ -51,10 +50,7 @@ static int run_tiled(gbn_ctx* c, int prec, int nrhs, const double* host_in, bool
         const int cnt = std::min(T, nrhs - r0);
         int32_t nt = 0;
         for (int r = r0; r < r0 + cnt; ++r) nt = std::max(nt, nsteps ? nsteps[r] : nmax);
-        GBN_CK(c, cudaMemcpyAsync(c->upload.p, host_in + per * r0, sizeof(double) * per * cnt, cudaMemcpyHostToDevice,
-                                  c->stream));
-        rc = phases ? lanczos_start_from_phases(c, c->upload.as<double>(), cnt)
-                    : lanczos_start_from_psi(c, c->upload.as<double>(), cnt);
+        rc = start(r0, cnt);
         if (rc) return rc;
         rc = lanczos_run(c, nt);
         if (rc) return rc;
@@ -76,6 +72,23 @@ static int run_tiled(gbn_ctx* c, int prec, int nrhs, const double* host_in, bool
     c->timing.spmm_ms_avg = tiles ? spmm_sum / tiles : 0.0;
     c->timing.update_ms_avg = tiles ? upd_sum / tiles : 0.0;
     return GBN_OK;
+}
+
+// Inputs are either complex start vectors (psi) or uniform draws (phases), [nrhs][n] on the host.
+static int run_tiled(gbn_ctx* c, int prec, int nrhs, const double* host_in, bool phases, const int32_t* nsteps,
+                     int32_t nmax, double* a, double* b)
+{
+    const size_t per = (size_t)c->n * (phases ? 1 : 2);
+    GBN_CK(c, c->upload.ensure(sizeof(double) * per * tile_width(nrhs)));
+    return run_tiles(
+        c, prec, nrhs,
+        [&](int r0, int cnt) -> int {
+            GBN_CK(c, cudaMemcpyAsync(c->upload.p, host_in + per * r0, sizeof(double) * per * cnt,
+                                      cudaMemcpyHostToDevice, c->stream));
+            return phases ? lanczos_start_from_phases(c, c->upload.as<double>(), cnt)
+                          : lanczos_start_from_psi(c, c->upload.as<double>(), cnt);
+        },
+        nsteps, nmax, a, b);
 }
 
 static int check_solver_args(gbn_ctx* c, int32_t precision, int32_t nrhs, const void* in, const int32_t* nsteps,
@@ -388,6 +401,96 @@ int gbn_lanczos_phases(gbn_ctx* c, int32_t precision, int32_t nrhs, const double
     if (rc) return rc;
     cudaSetDevice(c->device);
     return run_tiled(c, precision, nrhs, u, true, nsteps, nmax, a, b);
+}
+
+int gbn_lanczos_sites(gbn_ctx* c, int32_t precision, int32_t nsites, const int64_t* sites, const int32_t* nsteps,
+                      int32_t nmax, double* a, double* b)
+{
+    if (!c) return GBN_ERR_ARG;
+    int rc = check_solver_args(c, precision, nsites, sites, nsteps, nmax, a, b);
+    if (rc) return rc;
+    std::vector<int64_t> s0((size_t)nsites);
+    for (int r = 0; r < nsites; ++r) {
+        if (sites[r] < 1 || sites[r] > c->n) return fail(c, GBN_ERR_ARG, "site index out of 1..N");
+        s0[(size_t)r] = sites[r] - 1;
+    }
+    cudaSetDevice(c->device);
+    DevBuf d_site;
+    GBN_CK(c, d_site.ensure(sizeof(int64_t) * (size_t)nsites));
+    GBN_CK(c, cudaMemcpyAsync(d_site.p, s0.data(), sizeof(int64_t) * (size_t)nsites, cudaMemcpyHostToDevice,
+                              c->stream));
+    rc = run_tiles(
+        c, precision, nsites,
+        [&](int r0, int cnt) -> int { return lanczos_start_from_sites(c, d_site.as<int64_t>() + r0, cnt); }, nsteps,
+        nmax, a, b);
+    cudaStreamSynchronize(c->stream);
+    return rc;
+}
+
+int gbn_lanczos_sets(gbn_ctx* c, int32_t precision, int32_t nsets, const int32_t* set_of_atom, const double* u,
+                     const double* assumed, const int32_t* nsteps, int32_t nmax, double* a, double* b)
+{
+    if (!c) return GBN_ERR_ARG;
+    int rc = check_solver_args(c, precision, nsets, set_of_atom, nsteps, nmax, a, b);
+    if (rc) return rc;
+    if (!u || !assumed) return fail(c, GBN_ERR_ARG, "NULL draws or assumed counts");
+    const int64_t n = c->n;
+    // draw of each atom: the k-th member of a set takes u[k] (each set reseeds the same stream)
+    std::vector<int64_t> members((size_t)nsets, 0);
+    std::vector<double> draw((size_t)n, 0.0);
+    for (int64_t i = 0; i < n; ++i) {
+        const int32_t s = set_of_atom[i];
+        if (s < -1 || s >= nsets) return fail(c, GBN_ERR_ARG, "set_of_atom entries must be in -1..nsets-1");
+        if (s >= 0) draw[(size_t)i] = u[members[(size_t)s]++];
+    }
+    for (int s = 0; s < nsets; ++s)
+        if (!(assumed[s] > 0.0)) return fail(c, GBN_ERR_ARG, "assumed counts must be positive");
+    // A set without atoms has a zero start vector and no DOS (the reference divides by its zero norm):
+    // its a, b are NaN and the others run as a compact batch.
+    std::vector<int32_t> slot((size_t)nsets, -1), owner;
+    for (int s = 0; s < nsets; ++s)
+        if (members[(size_t)s] > 0) {
+            slot[(size_t)s] = (int32_t)owner.size();
+            owner.push_back(s);
+        }
+    const int ne = (int)owner.size();
+    for (int s = 0; s < nsets; ++s)
+        if (slot[(size_t)s] < 0)
+            for (int k = 0; k < nmax; ++k) a[(size_t)s * nmax + k] = b[(size_t)s * nmax + k] = NAN;
+    if (ne == 0) return GBN_OK;
+    std::vector<int32_t> so((size_t)n), ns;
+    for (int64_t i = 0; i < n; ++i) so[(size_t)i] = set_of_atom[i] >= 0 ? slot[(size_t)set_of_atom[i]] : -1;
+    // psi = e^(i th)/sqrt(M); the reference normalises when |<psi|psi> - 1| > 1e-6, <psi|psi> = count/M
+    std::vector<double> den((size_t)2 * ne);
+    for (int e = 0; e < ne; ++e) {
+        const int s = owner[(size_t)e];
+        const double nrm = (double)members[(size_t)s] / assumed[s];
+        den[(size_t)2 * e] = sqrt(assumed[s]);
+        den[(size_t)2 * e + 1] = fabs(nrm - 1.0) > 1.0e-6 ? sqrt(nrm) : 1.0;
+        if (nsteps) ns.push_back(nsteps[s]);
+    }
+    cudaSetDevice(c->device);
+    DevBuf d_set, d_draw, d_den;
+    GBN_CK(c, d_set.ensure(sizeof(int32_t) * (size_t)n));
+    GBN_CK(c, d_draw.ensure(sizeof(double) * (size_t)n));
+    GBN_CK(c, d_den.ensure(sizeof(double) * den.size()));
+    GBN_CK(c, cudaMemcpyAsync(d_set.p, so.data(), sizeof(int32_t) * (size_t)n, cudaMemcpyHostToDevice, c->stream));
+    GBN_CK(c, cudaMemcpyAsync(d_draw.p, draw.data(), sizeof(double) * (size_t)n, cudaMemcpyHostToDevice, c->stream));
+    GBN_CK(c, cudaMemcpyAsync(d_den.p, den.data(), sizeof(double) * den.size(), cudaMemcpyHostToDevice, c->stream));
+    std::vector<double> ae((size_t)ne * nmax), be((size_t)ne * nmax);
+    rc = run_tiles(
+        c, precision, ne,
+        [&](int r0, int cnt) -> int {
+            return lanczos_start_from_sets(c, d_set.as<int32_t>(), d_draw.as<double>(), d_den.as<double>(), r0, cnt);
+        },
+        nsteps ? ns.data() : nullptr, nmax, ae.data(), be.data());
+    cudaStreamSynchronize(c->stream);   // the host vectors above must outlive the copies
+    if (rc) return rc;
+    for (int e = 0; e < ne; ++e) {
+        memcpy(a + (size_t)owner[(size_t)e] * nmax, ae.data() + (size_t)e * nmax, sizeof(double) * nmax);
+        memcpy(b + (size_t)owner[(size_t)e] * nmax, be.data() + (size_t)e * nmax, sizeof(double) * nmax);
+    }
+    return GBN_OK;
 }
 
 int gbn_stage_phases(gbn_ctx* c, int32_t precision, int32_t nrhs, const double* u)

@@ -146,6 +146,33 @@ void cart_to_frac(int64_t n, const double* u, double* r)
     }
 }
 
+
+// One Cartesian -> fractional -> Cartesian conversion of a single position (AtomsSetFrac followed by
+// AtomsSetCart, atoms.F90:1768-1830).
+void roundtrip1(const double* u, double* p)
+{
+    cart_to_frac(1, u, p);
+    frac_to_cart(1, u, p);
+}
+
+// The position of one atom after k roundtrips.  The map reaches a fixed point (or, rarely, a 2-cycle)
+// within a few applications, so k is cut short once it does.
+void roundtrip_k(const double* u, const double* c0, int64_t k, double* p)
+{
+    p[0] = c0[0]; p[1] = c0[1]; p[2] = c0[2];
+    double prev[3] = {p[0], p[1], p[2]};
+    for (int64_t it = 0; it < k; ++it) {
+        const double before[3] = {p[0], p[1], p[2]};
+        roundtrip1(u, p);
+        if (p[0] == before[0] && p[1] == before[1] && p[2] == before[2]) return;   // fixed point
+        if (it >= 1 && p[0] == prev[0] && p[1] == prev[1] && p[2] == prev[2]) {  // 2-cycle: parity decides
+            if (((k - 1 - it) & 1) != 0) { p[0] = before[0]; p[1] = before[1]; p[2] = before[2]; }
+            return;
+        }
+        prev[0] = before[0]; prev[1] = before[1]; prev[2] = before[2];
+    }
+}
+
 }  // namespace
 
 extern "C" {
@@ -230,6 +257,148 @@ int gbn_rng_uniform(int32_t seed, int64_t n, double* out)
     Xoshiro x;
     x.put(seed);
     for (int64_t i = 0; i < n; ++i) out[i] = x.r8();
+    return GBN_OK;
+}
+
+// Kubo.PDOS atom selections of CalcKubo (lanczosKuboCode/Src/calc.F90:362-541).  The reference's loops
+// switch the module positions between fractional and Cartesian coordinates: the moire selections
+// convert to fractional before testing an atom and back to Cartesian after each selected atom, so an
+// atom is tested at F(R^k(r0)) with k the atoms selected before it (R = Cartesian->fractional->Cartesian)
+// and its coords line holds R^(k+1)(r0).  The positions enter in Cartesian form.
+int gbn_pdos_atoms(const gbn_pdos* p, int64_t n, const double* rat, const int32_t* species, const int32_t* layer,
+                   const double* ucell, int64_t cap, int64_t* count, int64_t* atoms, double* coords)
+{
+    if (!p || n < 0 || !rat || !species || !layer || !ucell || !count || cap < 0 || (cap > 0 && (!atoms || !coords)))
+        return GBN_ERR_ARG;
+    int64_t cnt = 0;
+    auto take = [&](int64_t i, const double* pos) {
+        if (cnt < cap) {
+            atoms[cnt] = i + 1;
+            coords[3 * cnt] = pos[0]; coords[3 * cnt + 1] = pos[1]; coords[3 * cnt + 2] = pos[2];
+        }
+        ++cnt;
+    };
+    switch (p->mode) {
+    case GBN_PDOS_DIST:   // calc.F90:362-380, Cartesian positions, open bounds
+        for (int64_t i = 0; i < n; ++i) {
+            const double* r = rat + 3 * i;
+            if (r[0] > p->xmin && r[0] < p->xmax && r[1] > p->ymin && r[1] < p->ymax && i + 1 >= p->min_value)
+                take(i, r);
+        }
+        break;
+    case GBN_PDOS_MOIRE_SC1:
+    case GBN_PDOS_SUPERMOIRE:
+    case GBN_PDOS_SUPERMOIRE2:
+    case GBN_PDOS_SUPERMOIRE3: {   // calc.F90:381-467
+        const double len = p->supermoire_length / p->aG;
+        const double sc = (double)p->super_cell, cs = (double)p->cell_size;
+        const double t1 = 1.0 / sc / cs * len, t2 = 2.0 / sc / cs * len, t3 = 3.0 / sc / cs * len;
+        const double sc1 = 1.0 / sc;
+        int64_t k = 0;
+        double pos[3], f[3];
+        for (int64_t i = 0; i < n; ++i) {
+            roundtrip_k(ucell, rat + 3 * i, k, pos);
+            f[0] = pos[0]; f[1] = pos[1]; f[2] = pos[2];
+            cart_to_frac(1, ucell, f);
+            bool sel = false;
+            if (p->mode == GBN_PDOS_MOIRE_SC1) {
+                sel = f[0] < sc1 && f[1] < sc1 && i + 1 >= p->min_value;
+                if (sel && p->ignore_layers_1_4 && (layer[i] == 1 || layer[i] == 4)) sel = false;
+            } else {
+                const double lo = p->mode == GBN_PDOS_SUPERMOIRE ? -INFINITY : (p->mode == GBN_PDOS_SUPERMOIRE2 ? t1 : t2);
+                const double hi = p->mode == GBN_PDOS_SUPERMOIRE ? t1 : (p->mode == GBN_PDOS_SUPERMOIRE2 ? t2 : t3);
+                sel = f[0] >= lo && f[1] >= lo && f[0] < hi && f[1] < hi && species[i] == 1 && i + 1 >= p->min_value;
+            }
+            if (!sel) continue;
+            frac_to_cart(1, ucell, f);
+            take(i, f);
+            ++k;
+        }
+        break;
+    }
+    case GBN_PDOS_ATOM_LIST:   // calc.F90:471-487
+        for (int j = 0; j < 6; ++j) {
+            const int64_t i = (int64_t)p->atom_list[j] - 1;
+            if (i < 0 || i >= n) return GBN_ERR_ARG;
+            take(i, rat + 3 * i);
+        }
+        break;
+    case GBN_PDOS_BY_NUMBER: {   // calc.F90:489-493
+        const int64_t i = (int64_t)p->atom_number - 1;
+        if (i < 0 || i >= n) return GBN_ERR_ARG;
+        take(i, rat + 3 * i);
+        break;
+    }
+    case GBN_PDOS_PNP: {   // calc.F90:494-541: the first atom past L/4 and the first past L/4 + 2 delta
+        const double acc = p->aG / sqrt(3.0);
+        const double limit1 = ((double)(p->cell_size * p->super_cell) * p->aG) * 1.0 / 4.0;
+        const double lo2 = limit1 + p->pnp_delta * 2.0;
+        bool f1 = false, f2 = false;
+        for (int64_t i = 0; i < n; ++i) {
+            const double* r = rat + 3 * i;
+            if (r[0] > limit1 && r[0] < limit1 + acc && !f1) { f1 = true; take(i, r); }
+            if (r[0] > lo2 && r[0] < lo2 + acc && !f2) { f2 = true; take(i, r); }
+        }
+        break;
+    }
+    default:
+        return GBN_ERR_ARG;
+    }
+    *count = cnt;
+    return GBN_OK;
+}
+
+// The sets of Kubo.PDOSLayer and Kubo.PDOSLayerAndSpecies (calc.F90:300-361) with the atom counts the
+// reference assumes when it scales their start vectors.
+int gbn_pdos_sets(const gbn_pdos* p, int64_t n, const int32_t* species, const int32_t* layer, int32_t cap,
+                  int32_t* nsets, int32_t* set_of_atom, int32_t* set_layer, int32_t* set_species, double* assumed)
+{
+    if (!p || n < 0 || !species || !layer || !nsets || !set_of_atom || cap < 0 ||
+        (cap > 0 && (!set_layer || !set_species || !assumed)))
+        return GBN_ERR_ARG;
+    const int32_t L = p->number_of_layers;
+    if (L < 1) return GBN_ERR_ARG;
+    const int64_t s2 = (int64_t)p->super_cell * p->super_cell;
+    int32_t ns = 0;
+    for (int64_t i = 0; i < n; ++i) set_of_atom[i] = -1;
+    if (p->mode == GBN_PDOS_LAYER) {
+        if (L > cap) return GBN_ERR_ARG;
+        for (int32_t l = 1; l <= L; ++l) {
+            int64_t m;
+            const bool t3 = p->stack == GBN_STACK_T3BG, e4 = p->stack == GBN_STACK_ENCAPSULATED_FOUR;
+            if (t3 && l >= 1 && l <= 6) m = (int64_t)p->n_c * s2;
+            else if (e4 && l == 1) m = (int64_t)p->n_bn1 * s2;
+            else if (e4 && l == 4) m = (int64_t)p->n_bn2 * s2;
+            else if (e4 && (l == 2 || l == 3)) m = (int64_t)p->n_c * s2;
+            else m = n / L;
+            set_layer[l - 1] = l;
+            set_species[l - 1] = 0;
+            assumed[l - 1] = (double)m;
+        }
+        for (int64_t i = 0; i < n; ++i)
+            if (layer[i] >= 1 && layer[i] <= L) set_of_atom[i] = layer[i] - 1;
+        ns = L;
+    } else if (p->mode == GBN_PDOS_LAYER_SPECIES) {
+        int32_t maxs = 1;
+        for (int64_t i = 0; i < n; ++i) maxs = species[i] > maxs ? species[i] : maxs;
+        for (int32_t l = 1; l <= L; ++l)
+            for (int32_t s = 1; s <= maxs; ++s) {
+                int64_t m = 0;
+                for (int64_t i = 0; i < n; ++i)
+                    if (layer[i] == l && species[i] == s) ++m;
+                if (m == 0) continue;   // combinations without atoms are skipped
+                if (ns >= cap) return GBN_ERR_ARG;
+                for (int64_t i = 0; i < n; ++i)
+                    if (layer[i] == l && species[i] == s) set_of_atom[i] = ns;
+                set_layer[ns] = l;
+                set_species[ns] = s;
+                assumed[ns] = (double)m;
+                ++ns;
+            }
+    } else {
+        return GBN_ERR_ARG;
+    }
+    *nsets = ns;
     return GBN_OK;
 }
 

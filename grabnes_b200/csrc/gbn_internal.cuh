@@ -170,6 +170,9 @@ int auto_group(const gbn_ctx* c);
 int lanczos_prepare(gbn_ctx* c, int prec, int nrhs);
 int lanczos_start_from_phases(gbn_ctx* c, const double* d_u, int nrhs_real);
 int lanczos_start_from_psi(gbn_ctx* c, const double* d_psi, int nrhs_real);
+int lanczos_start_from_sites(gbn_ctx* c, const int64_t* d_site, int nrhs_real);
+int lanczos_start_from_sets(gbn_ctx* c, const int32_t* d_set, const double* d_draw, const double* d_den, int set0,
+                            int nrhs_real);
 int lanczos_run(gbn_ctx* c, int32_t nmax);
 // right-hand sides per thread and threads per row group for a tile of R vectors
 void split_rhs(int prec, int R, int want, int* rpt, int* tpr);

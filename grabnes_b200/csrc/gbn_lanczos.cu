@@ -438,6 +438,55 @@ __global__ void k_start_from_psi(typename V2<VT>::t* v, typename V2<VT>::t* x, c
     x[i] = zero;
 }
 
+// Unit vectors on single atoms (KuboInitWFPDOS): vector r of the tile is 1 on atom site[r] (0-based).
+template <typename VT>
+__global__ void k_start_from_sites(typename V2<VT>::t* v, typename V2<VT>::t* x, const int64_t* site,
+                                   const int32_t* perm, int64_t n, int64_t npad, int R, int nrhs_real)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= npad * R) return;
+    const int64_t row = i / R;
+    const int r = (int)(i % R);
+    typename V2<VT>::t z;
+    z.x = 0; z.y = 0;
+    if (row < n && perm[row] == site[r < nrhs_real ? r : 0]) z.x = (VT)1;
+    v[i] = z;
+    typename V2<VT>::t zero;
+    zero.x = 0; zero.y = 0;
+    x[i] = zero;
+}
+
+// Random phases on one set of atoms per vector (KuboInitWFLayerDOS): atom a of set s = set0 + r takes
+// exp(2 pi i draw[a]) / den[s].x / den[s].y (den.x = sqrt of the assumed count, den.y = the norm
+// correction, 1 when none is made).
+template <typename VT>
+__global__ void k_start_from_sets(typename V2<VT>::t* v, typename V2<VT>::t* x, const int32_t* set_of_atom,
+                                  const double* draw, const double2* den, const int32_t* perm, int64_t n,
+                                  int64_t npad, int R, int set0, int nrhs_real)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= npad * R) return;
+    const int64_t row = i / R;
+    const int r = (int)(i % R);
+    typename V2<VT>::t z;
+    z.x = 0; z.y = 0;
+    if (row < n) {
+        const int32_t a = perm[row];
+        const int s = set0 + (r < nrhs_real ? r : 0);
+        if (set_of_atom[a] == s) {
+            double sn, cs;
+            sincos(6.283185307179586 * draw[a], &sn, &cs);
+            const double2 d = den[s];
+            z.x = (VT)(cs / d.x / d.y);
+            z.y = (VT)(sn / d.x / d.y);
+        }
+    }
+    v[i] = z;
+    typename V2<VT>::t zero;
+    zero.x = 0; zero.y = 0;
+    x[i] = zero;
+}
+
 __global__ void k_init_scalars(double* scal, unsigned int* counter, int R)
 {
     const int r = threadIdx.x;
@@ -593,6 +642,42 @@ int lanczos_start_from_psi(gbn_ctx* c, const double* d_psi, int nrhs_real)
                                                              reinterpret_cast<const double2*>(d_psi),
                                                              c->ell.rperm.as<int32_t>(), c->n, c->ell.npad, c->nrhs,
                                                              nrhs_real);
+    GBN_CK_LAUNCH(c);
+    return GBN_OK;
+}
+
+int lanczos_start_from_sites(gbn_ctx* c, const int64_t* d_site, int nrhs_real)
+{
+    const int64_t tot = c->ell.npad * c->nrhs;
+    const int blk = 256;
+    const int64_t grd = (tot + blk - 1) / blk;
+    if (c->prec == GBN_MIXED)
+        k_start_from_sites<float><<<grd, blk, 0, c->stream>>>(c->vec[0].as<float2>(), c->vec[1].as<float2>(), d_site,
+                                                              c->ell.rperm.as<int32_t>(), c->n, c->ell.npad, c->nrhs,
+                                                              nrhs_real);
+    else
+        k_start_from_sites<double><<<grd, blk, 0, c->stream>>>(c->vec[0].as<double2>(), c->vec[1].as<double2>(),
+                                                               d_site, c->ell.rperm.as<int32_t>(), c->n, c->ell.npad,
+                                                               c->nrhs, nrhs_real);
+    GBN_CK_LAUNCH(c);
+    return GBN_OK;
+}
+
+int lanczos_start_from_sets(gbn_ctx* c, const int32_t* d_set, const double* d_draw, const double* d_den, int set0,
+                            int nrhs_real)
+{
+    const int64_t tot = c->ell.npad * c->nrhs;
+    const int blk = 256;
+    const int64_t grd = (tot + blk - 1) / blk;
+    const double2* den = reinterpret_cast<const double2*>(d_den);
+    if (c->prec == GBN_MIXED)
+        k_start_from_sets<float><<<grd, blk, 0, c->stream>>>(c->vec[0].as<float2>(), c->vec[1].as<float2>(), d_set,
+                                                             d_draw, den, c->ell.rperm.as<int32_t>(), c->n,
+                                                             c->ell.npad, c->nrhs, set0, nrhs_real);
+    else
+        k_start_from_sets<double><<<grd, blk, 0, c->stream>>>(c->vec[0].as<double2>(), c->vec[1].as<double2>(),
+                                                              d_set, d_draw, den, c->ell.rperm.as<int32_t>(), c->n,
+                                                              c->ell.npad, c->nrhs, set0, nrhs_real);
     GBN_CK_LAUNCH(c);
     return GBN_OK;
 }

@@ -23,6 +23,7 @@
 #include <sys/stat.h>
 
 #include <cctype>
+#include <cmath>
 #include <map>
 #include <stdexcept>
 #include <string>
@@ -295,6 +296,8 @@ struct Job {
     bool field_by_value = false, field_steps_by_value = false;
     double b_value = 0, b_init = 0, b_final = 0, b_step = 0;
     std::string prefix;
+    gbn_pdos pdos{};        // Kubo.PDOS selection (mode 0: the DOS of the whole cell)
+    int seed_set = 1235;    // Kubo.SeedSet: the stream of the layer start vectors
 };
 
 Job job_from_input(const Input& in)
@@ -390,6 +393,39 @@ Job job_from_input(const Input& in)
     j.nwr = (int)in.i("Kubo.WriteNumberofSteps", 10);
     j.dt = in.d("Kubo.TimeStep", 5.0);
     if (j.npol < 1 || j.nt < 0 || j.nwr < 1) die("Kubo.NumberofPolynomials and Kubo.WriteNumberofSteps must be positive");
+    // local DOS selections (CalcKubo, calc.F90:214-300): the first flag that is set picks the mode
+    if (in.l("Kubo.PDOS", false)) {
+        gbn_pdos& p = j.pdos;
+        const char* flags[10][2] = {{"Kubo.PDOSLayer", "f"}, {"Kubo.PDOSLayerAndSpecies", "f"}, {"Kubo.PDOSDist", "f"},
+                                    {"Kubo.PDOSMoireSC1", "f"}, {"Kubo.PDOSMoireSuperMoire", "t"},
+                                    {"Kubo.PDOSMoireSuperMoire2", "t"}, {"Kubo.PDOSMoireSuperMoire3", "t"},
+                                    {"Kubo.PDOSAtomList", "f"}, {"Kubo.PDOSByNumber", "f"}, {"Kubo.PDOSPNP", "f"}};
+        const int modes[10] = {GBN_PDOS_LAYER, GBN_PDOS_LAYER_SPECIES, GBN_PDOS_DIST, GBN_PDOS_MOIRE_SC1,
+                               GBN_PDOS_SUPERMOIRE, GBN_PDOS_SUPERMOIRE2, GBN_PDOS_SUPERMOIRE3, GBN_PDOS_ATOM_LIST,
+                               GBN_PDOS_BY_NUMBER, GBN_PDOS_PNP};
+        for (int k = 0; k < 10 && p.mode == 0; ++k)
+            if (in.l(flags[k][0], flags[k][1][0] == 't')) p.mode = modes[k];
+        p.xmin = in.d("Kubo.PDOSxmin", 0.0);
+        p.xmax = in.d("Kubo.PDOSxmax", 5.0);
+        p.ymin = in.d("Kubo.PDOSymin", 0.0);
+        p.ymax = in.d("Kubo.PDOSymax", 5.0);
+        p.min_value = (int32_t)in.i("Kubo.PDOSMinValue", 0);
+        p.super_cell = j.cell.super_cell;
+        p.cell_size = j.cell.cell_size;
+        p.supermoire_length = in.d("Kubo.PDOSMoireSuperMoireLength", 135.0);
+        p.aG = aG;
+        p.ignore_layers_1_4 = in.l("Kubo.PDOSIgnoreLayer1and4", false) ? 1 : 0;
+        for (int k = 0; k < 6; ++k) p.atom_list[k] = (int32_t)(in.has("Kubo.PDOSList") ? in.i("Kubo.PDOSList", 0, k) : k + 1);
+        p.atom_number = (int32_t)in.i("Kubo.PDOSNumber", 1);
+        p.pnp_delta = in.d("Potential.PNPDelta", 10.0);
+        p.number_of_layers = (int32_t)in.i("Kubo.NumberOfLayers", 2);
+        p.n_bn1 = (int32_t)in.i("Kubo.NumberOfBNAtoms1", 5832);
+        p.n_bn2 = (int32_t)in.i("Kubo.NumberOfBNAtoms2", 5832);
+        p.n_c = (int32_t)in.i("Kubo.NumberOfCAtoms", 6050);
+        p.stack = in.l("Stack.EncapsulatedFourLayers", false) ? GBN_STACK_ENCAPSULATED_FOUR
+                                                              : (in.l("Stack.T3BG", false) ? GBN_STACK_T3BG : GBN_STACK_NONE);
+        j.seed_set = (int)in.i("Kubo.SeedSet", 1235);
+    }
     // field sweep (MagfInit, magf.F90:20-98); values in tesla are converted once the cell area is known
     if (in.has("MagField.Value")) {
         j.field_by_value = true;
@@ -440,7 +476,9 @@ std::string fortran_ld(double x)
     snprintf(sci, sizeof sci, "%.16e", x);
     const char* ep = strchr(sci, 'e');
     const int e = ep ? atoi(ep + 1) : 0;
-    if (x == 0.0) {
+    if (!std::isfinite(x)) {   // gfortran's list-directed NaN / Infinity
+        snprintf(buf, sizeof buf, "%26s", std::isnan(x) ? "NaN" : (x > 0 ? "Infinity" : "-Infinity"));
+    } else if (x == 0.0) {
         snprintf(buf, sizeof buf, "   0.0000000000000000     ");
     } else if (e >= -1 && e < 16) {
         snprintf(buf, sizeof buf, "   %.*f     ", 16 - e, x);
@@ -471,7 +509,7 @@ void print_job(const Job& j)
            "\"height\": %.17g, \"d_interlayer\": %.17g, \"g0\": %.17g, \"cut2intra\": %.17g, \"cut2inter\": %.17g, "
            "\"second_layer\": %d, \"moire\": %d, \"nrecurs\": %d, \"eta\": %.17g, \"n_en\": %d, \"emin\": %.17g, "
            "\"emax\": %.17g, \"seed\": %d, \"prefix\": \"%s\", \"only_dos\": %d, \"npol\": %d, \"nt\": %d, "
-           "\"nwr\": %d, \"dt\": %.17g, \"model\": {\"tbnn\": %d, \"intralayer\": %d, "
+           "\"nwr\": %d, \"dt\": %.17g, \"pdos_mode\": %d, \"seed_set\": %d, \"model\": {\"tbnn\": %d, \"intralayer\": %d, "
            "\"moire_onsite\": %d, \"moire_offdiag\": %d, \"moire_mid\": %d, \"moire_twisted\": %d, \"eps\": %.17g, "
            "\"twist_rad\": %.17g, \"C0\": %.17g, \"Cz\": %.17g, \"Cab\": %.17g, \"interlayer\": %d, "
            "\"vpppi0\": %.17g, \"vppsigma0\": %.17g, \"bl_delta\": %.17g, \"anderson\": %d, \"anderson_w\": %.17g, "
@@ -479,7 +517,7 @@ void print_job(const Job& j)
            j.cell.kind, j.cell.aG, j.cell.cell_size, j.cell.super_cell, j.cell.m[0], j.cell.m[1], j.cell.m[2], j.cell.m[3],
            j.cell.height, j.cell.d_interlayer, j.g0, j.cut2intra, j.cut2inter, (int)j.second_layer, (int)j.moire,
            j.nrecurs, j.eta, j.n_en, j.emin, j.emax, j.seed, j.prefix.c_str(), (int)j.only_dos, j.npol, j.nt, j.nwr,
-           j.dt, m.tbnn, m.intralayer, m.moire_onsite,
+           j.dt, j.pdos.mode, j.seed_set, m.tbnn, m.intralayer, m.moire_onsite,
            m.moire_offdiag, m.moire_mid, m.moire_twisted, m.eps, m.twist_rad, m.C0, m.Cz, m.Cab, m.interlayer,
            m.vpppi0, m.vppsigma0, m.bl_delta, m.anderson, m.anderson_w, m.tksl[2]);
 }
@@ -498,7 +536,7 @@ void write_pairs(const std::string& path, const std::vector<double>& x, const st
 // (kubo.F90:321-397): nT steps of KuboEvol along x from the start vector psi with zupsi = 0; every nWr
 // steps the recursion of zupsi / |zupsi| and the continued fraction weighted by |zupsi|^2 are written
 // to <prefix>.Z2_<step>.dat and <prefix>.AB_<step>.dat.
-void time_evolution(gbn_ctx* ctx, const Job& j, const std::vector<double>& u, const std::vector<double>& a,
+void time_evolution(gbn_ctx* ctx, const Job& j, std::vector<double> psi, const std::vector<double>& a,
                     const std::vector<double>& b, const std::string& prefix, int64_t n)
 {
     double ac = 0.0, bc = 0.0;
@@ -512,12 +550,7 @@ void time_evolution(gbn_ctx* ctx, const Job& j, const std::vector<double>& u, co
     }
     write_pairs(prefix + ".cn.dat", re, ab, 0.0, false);
     if (j.only_dos) return;
-    std::vector<double> psi((size_t)2 * n), zu((size_t)2 * n, 0.0), zn((size_t)2 * n);
-    const double isn = 1.0 / sqrt((double)n);
-    for (int64_t i = 0; i < n; ++i) {
-        psi[(size_t)2 * i] = cos(2.0 * kPi * u[(size_t)i]) * isn;
-        psi[(size_t)2 * i + 1] = sin(2.0 * kPi * u[(size_t)i]) * isn;
-    }
+    std::vector<double> zu((size_t)2 * n, 0.0), zn((size_t)2 * n);
     std::vector<double> az((size_t)j.nrecurs), bz((size_t)j.nrecurs), energy((size_t)j.n_en + 1), dos((size_t)j.n_en + 1);
     for (int it = 1; it <= j.nt; ++it) {
         ck(gbn_kubo_evol(ctx, GBN_FP64, 1, c.data(), j.npol, ac, bc, 1, psi.data(), zu.data()), ctx, "gbn_kubo_evol");
@@ -537,6 +570,127 @@ void time_evolution(gbn_ctx* ctx, const Job& j, const std::vector<double>& u, co
         write_pairs(prefix + ".AB_" + tag + ".dat", az, bz, norm, true);
         printf("grabnes: time step %d of %d, |ZUPsi|^2 = %.10g\n", it, j.nt, norm);
     }
+}
+
+// KuboDOS (kubo.F90:276-319) after the recursion: <prefix>.b0.dat, .a0.dat (KuboRecursion's files), the
+// continued fraction <prefix>.DOS and the coefficients <prefix>.AB.
+void kubo_dos_files(gbn_ctx* ctx, const Job& j, const std::string& prefix, const double* a, const double* b)
+{
+    std::vector<double> av(a, a + j.nrecurs), bv(b, b + j.nrecurs), energy((size_t)j.n_en + 1), dos((size_t)j.n_en + 1);
+    write_column(prefix + ".b0.dat", bv);
+    write_column(prefix + ".a0.dat", av);
+    ck(gbn_cf_dos(ctx, 1, a, b, nullptr, j.nrecurs, j.eta, j.n_en, j.emin, j.emax, nullptr, energy.data(), dos.data()),
+       ctx, "gbn_cf_dos");
+    write_pairs(prefix + ".DOS", energy, dos, 0.0, false);
+    write_pairs(prefix + ".AB", av, bv, 1.0, true);
+    printf("grabnes: DOS written to %s.DOS and %s.AB\n", prefix.c_str(), prefix.c_str());
+}
+
+std::string make_folder(const std::string& name, const std::string& sysname)
+{
+    if (mkdir(name.c_str(), 0755) != 0 && errno != EEXIST) die("cannot create folder " + name);
+    printf("grabnes: writing files in folder '%s'\n", name.c_str());
+    return "./" + name + "/" + sysname;
+}
+
+// One Kubo.PDOS pass (CalcKubo, calc.F90:300-541).  All start vectors of the selection run as one batch
+// of right-hand sides; the files of each go to its PDOS_* folder as the reference writes them.  On return
+// psi, a, b and prefix are those of the last start vector, which the time evolution continues from.
+void pdos_pass(gbn_ctx* ctx, const Job& j, int64_t n, const std::vector<double>& rat_now,
+               const std::vector<int32_t>& species, const std::vector<int32_t>& layer, const std::vector<double>& ucell,
+               std::vector<double>& psi, std::vector<double>& a, std::vector<double>& b, std::string& prefix, bool& any)
+{
+    const gbn_pdos& p = j.pdos;
+    any = false;
+    if (p.mode == GBN_PDOS_LAYER || p.mode == GBN_PDOS_LAYER_SPECIES) {
+        int32_t maxl = 0;
+        for (int32_t l : layer) maxl = l > maxl ? l : maxl;
+        if (p.mode == GBN_PDOS_LAYER && p.number_of_layers < maxl)
+            printf("grabnes: warning: Kubo.NumberOfLayers is %d but the structure has %d layers: the layer DOS of "
+                   "layers above %d is not written\n", p.number_of_layers, maxl, p.number_of_layers);
+        const int32_t cap = 4096;
+        std::vector<int32_t> set_of_atom((size_t)n), sl(cap), ss(cap);
+        std::vector<double> assumed(cap);
+        int32_t ns = 0;
+        ck(gbn_pdos_sets(&p, n, species.data(), layer.data(), cap, &ns, set_of_atom.data(), sl.data(), ss.data(),
+                         assumed.data()),
+           nullptr, "gbn_pdos_sets");
+        if (ns == 0) return;
+        std::vector<double> u((size_t)n);
+        ck(gbn_rng_uniform(j.seed_set, n, u.data()), nullptr, "gbn_rng_uniform");
+        std::vector<int64_t> count((size_t)ns, 0);
+        for (int64_t i = 0; i < n; ++i)
+            if (set_of_atom[(size_t)i] >= 0) ++count[(size_t)set_of_atom[(size_t)i]];
+        for (int s = 0; s < ns; ++s)
+            if (count[(size_t)s] == 0)
+                printf("grabnes: warning: layer %d has no atoms: its DOS is undefined\n", sl[(size_t)s]);
+        std::vector<double> aa((size_t)ns * j.nrecurs), bb((size_t)ns * j.nrecurs);
+        ck(gbn_lanczos_sets(ctx, GBN_FP64, ns, set_of_atom.data(), u.data(), assumed.data(), nullptr, j.nrecurs,
+                            aa.data(), bb.data()),
+           ctx, "gbn_lanczos_sets");
+        for (int s = 0; s < ns; ++s) {
+            char folder[64];
+            if (p.mode == GBN_PDOS_LAYER) snprintf(folder, sizeof folder, "PDOS_layer%02d", sl[(size_t)s]);
+            else snprintf(folder, sizeof folder, "PDOS_layer%02d_sub%02d", sl[(size_t)s], ss[(size_t)s]);
+            prefix = make_folder(folder, j.prefix);
+            kubo_dos_files(ctx, j, prefix, aa.data() + (size_t)s * j.nrecurs, bb.data() + (size_t)s * j.nrecurs);
+        }
+        // the last set's start vector (KuboInitWFLayerDOS)
+        const int last = ns - 1;
+        const double nrm = (double)count[(size_t)last] / assumed[(size_t)last];
+        const double den = sqrt(assumed[(size_t)last]), fix = (nrm > 0.0 && fabs(nrm - 1.0) > 1.0e-6) ? sqrt(nrm) : 1.0;
+        psi.assign((size_t)2 * n, 0.0);
+        int64_t k = 0;
+        for (int64_t i = 0; i < n; ++i)
+            if (set_of_atom[(size_t)i] == last) {
+                psi[(size_t)2 * i] = cos(2.0 * kPi * u[(size_t)k]) / den / fix;
+                psi[(size_t)2 * i + 1] = sin(2.0 * kPi * u[(size_t)k]) / den / fix;
+                ++k;
+            }
+        a.assign(aa.end() - j.nrecurs, aa.end());
+        b.assign(bb.end() - j.nrecurs, bb.end());
+        any = true;
+        return;
+    }
+    int64_t cnt = 0;
+    ck(gbn_pdos_atoms(&p, n, rat_now.data(), species.data(), layer.data(), ucell.data(), 0, &cnt, nullptr, nullptr),
+       nullptr, "gbn_pdos_atoms (atom index out of range?)");
+    if (cnt == 0) return;
+    std::vector<int64_t> atoms((size_t)cnt);
+    std::vector<double> coords((size_t)3 * cnt);
+    ck(gbn_pdos_atoms(&p, n, rat_now.data(), species.data(), layer.data(), ucell.data(), cnt, &cnt, atoms.data(),
+                      coords.data()),
+       nullptr, "gbn_pdos_atoms");
+    std::vector<double> aa((size_t)cnt * j.nrecurs), bb((size_t)cnt * j.nrecurs);
+    ck(gbn_lanczos_sites(ctx, GBN_FP64, (int32_t)cnt, atoms.data(), nullptr, j.nrecurs, aa.data(), bb.data()), ctx,
+       "gbn_lanczos_sites");
+    for (int64_t k = 0; k < cnt; ++k) {
+        const int64_t i = atoms[(size_t)k];
+        if (p.mode != GBN_PDOS_BY_NUMBER) {   // PDOSByNumber writes to the run's own prefix
+            char folder[64];
+            snprintf(folder, sizeof folder, "PDOS_atom%08lld", (long long)i);
+            prefix = make_folder(folder, j.prefix);
+            const std::string cpath = "./" + std::string(folder) + "/coords";
+            FILE* f = fopen(cpath.c_str(), "w");
+            if (!f) die("cannot write " + cpath);
+            const double* r = coords.data() + 3 * k;
+            if (p.mode == GBN_PDOS_MOIRE_SC1)
+                fprintf(f, "%12lld%s%s%12d%12d\n", (long long)i, fortran_ld(r[0]).c_str(), fortran_ld(r[1]).c_str(),
+                        species[(size_t)(i - 1)], layer[(size_t)(i - 1)]);
+            else
+                fprintf(f, "%12lld%s%s%s\n", (long long)i, fortran_ld(r[0]).c_str(), fortran_ld(r[1]).c_str(),
+                        fortran_ld(r[2]).c_str());
+            fclose(f);
+        } else {
+            prefix = j.prefix;
+        }
+        kubo_dos_files(ctx, j, prefix, aa.data() + (size_t)k * j.nrecurs, bb.data() + (size_t)k * j.nrecurs);
+    }
+    psi.assign((size_t)2 * n, 0.0);
+    psi[(size_t)2 * (atoms.back() - 1)] = 1.0;   // KuboInitWFPDOS of the last atom
+    a.assign(aa.end() - j.nrecurs, aa.end());
+    b.assign(bb.end() - j.nrecurs, bb.end());
+    any = true;
 }
 
 int run(const Job& j0)
@@ -567,11 +721,12 @@ int run(const Job& j0)
         rat_hop = rat_on;
         ck(gbn_cart_roundtrip(n, ucell.data(), rat_hop.data()), nullptr, "gbn_cart_roundtrip");
     }
+    const std::vector<double>& rat_now = j.moire ? rat_hop : rat;   // the module positions CalcKubo sees
     // Anderson disorder and the start vector draw the same stream (random_seed(PUT=SeedValue) in both)
     std::vector<double> u((size_t)n);
     ck(gbn_rng_uniform(j.seed, n, u.data()), nullptr, "gbn_rng_uniform");
     const bool magfield = !(j.mbi == 0 && j.mbf == 0);
-    std::vector<double> a((size_t)j.nrecurs), b((size_t)j.nrecurs), energy((size_t)j.n_en + 1), dos((size_t)j.n_en + 1);
+    std::vector<double> a((size_t)j.nrecurs), b((size_t)j.nrecurs), psi;
     for (long mb = j.mbi; mb <= j.mbf; mb += (magfield ? j.mstep : 1)) {
         std::string prefix = j.prefix;
         if (magfield && j.mbi != j.mbf) {
@@ -589,24 +744,24 @@ int run(const Job& j0)
             const double bmag = mb * kFluxQuantum / (area * 1.0e-20);
             ck(gbn_peierls(ctx, bmag * kPi / kFluxQuantum), ctx, "gbn_peierls");
         }
-        ck(gbn_lanczos_phases(ctx, GBN_FP64, 1, u.data(), nullptr, j.nrecurs, a.data(), b.data()), ctx,
-           "gbn_lanczos_phases");
-        write_column(prefix + ".b0.dat", b);
-        write_column(prefix + ".a0.dat", a);
-        ck(gbn_cf_dos(ctx, 1, a.data(), b.data(), nullptr, j.nrecurs, j.eta, j.n_en, j.emin, j.emax, nullptr,
-                      energy.data(), dos.data()),
-           ctx, "gbn_cf_dos");
-        FILE* f = fopen((prefix + ".DOS").c_str(), "w");
-        if (!f) die("cannot write " + prefix + ".DOS");
-        for (int k = 0; k <= j.n_en; ++k) fprintf(f, "%s%s\n", fortran_ld(energy[k]).c_str(), fortran_ld(dos[k]).c_str());
-        fclose(f);
-        f = fopen((prefix + ".AB").c_str(), "w");
-        if (!f) die("cannot write " + prefix + ".AB");
-        fprintf(f, "%s\n", fortran_ld(1.0).c_str());
-        for (int k = 0; k < j.nrecurs; ++k) fprintf(f, "%s%s\n", fortran_ld(a[k]).c_str(), fortran_ld(b[k]).c_str());
-        fclose(f);
-        printf("grabnes: DOS written to %s.DOS and %s.AB\n", prefix.c_str(), prefix.c_str());
-        if (j.polynomials || !j.only_dos) time_evolution(ctx, j, u, a, b, prefix, n);
+        bool any = true;
+        if (j.pdos.mode == 0) {   // KuboInitWF + KuboDOS
+            ck(gbn_lanczos_phases(ctx, GBN_FP64, 1, u.data(), nullptr, j.nrecurs, a.data(), b.data()), ctx,
+               "gbn_lanczos_phases");
+            kubo_dos_files(ctx, j, prefix, a.data(), b.data());
+            psi.assign((size_t)2 * n, 0.0);
+            const double isn = 1.0 / sqrt((double)n);
+            for (int64_t i = 0; i < n; ++i) {
+                psi[(size_t)2 * i] = cos(2.0 * kPi * u[(size_t)i]) * isn;
+                psi[(size_t)2 * i + 1] = sin(2.0 * kPi * u[(size_t)i]) * isn;
+            }
+        } else {
+            pdos_pass(ctx, j, n, rat_now, species, layer, ucell, psi, a, b, prefix, any);
+        }
+        if (j.polynomials || !j.only_dos) {
+            if (any) time_evolution(ctx, j, psi, a, b, prefix, n);
+            else printf("grabnes: the PDOS selection is empty: no time evolution\n");
+        }
         if (!magfield) break;
     }
     gbn_destroy(ctx);

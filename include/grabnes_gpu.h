@@ -159,6 +159,61 @@ int gbn_lanczos(gbn_ctx* ctx, int32_t precision, int32_t nrhs, const double* psi
  * u[nrhs][N]: psi_i = exp(2 pi i u_i)/sqrt(N) (KuboInitWF, kubo.F90:61-64). */
 int gbn_lanczos_phases(gbn_ctx* ctx, int32_t precision, int32_t nrhs, const double* u,
                        const int32_t* nsteps, int32_t nmax, double* a, double* b);
+/* Local DOS of single atoms (KuboInitWFPDOS, kubo.F90:87-138): start vector r is the unit vector
+ * on atom sites[r] (1-based), built on the device; all sites run as one batch of right-hand sides. */
+int gbn_lanczos_sites(gbn_ctx* ctx, int32_t precision, int32_t nsites, const int64_t* sites,
+                      const int32_t* nsteps, int32_t nmax, double* a, double* b);
+/* Layer (and species) DOS (KuboInitWFLayerDOS / KuboInitWFLayerAndSpeciesDOS, kubo.F90:140-274):
+ * set_of_atom[N] gives each atom's set (0..nsets-1, or -1); the k-th atom of a set, in atom order,
+ * takes psi = exp(2 pi i u[k])/sqrt(assumed[set]), and a set whose norm then differs from 1 by more
+ * than 1e-6 is normalised.  All sets run as one batch of right-hand sides; a set without atoms has a
+ * zero start vector and no DOS, and its a, b are NaN (the reference divides by the zero norm). */
+int gbn_lanczos_sets(gbn_ctx* ctx, int32_t precision, int32_t nsets, const int32_t* set_of_atom,
+                     const double* u, const double* assumed, const int32_t* nsteps, int32_t nmax,
+                     double* a, double* b);
+
+/* ---- Kubo.PDOS selections (CalcKubo, calc.F90:214-541) ------------------------------------ */
+enum {
+    GBN_PDOS_LAYER = 1,           /* Kubo.PDOSLayer */
+    GBN_PDOS_LAYER_SPECIES = 2,   /* Kubo.PDOSLayerAndSpecies */
+    GBN_PDOS_DIST = 3,            /* Kubo.PDOSDist */
+    GBN_PDOS_MOIRE_SC1 = 4,       /* Kubo.PDOSMoireSC1 */
+    GBN_PDOS_SUPERMOIRE = 5,      /* Kubo.PDOSMoireSuperMoire */
+    GBN_PDOS_SUPERMOIRE2 = 6,     /* Kubo.PDOSMoireSuperMoire2 */
+    GBN_PDOS_SUPERMOIRE3 = 7,     /* Kubo.PDOSMoireSuperMoire3 */
+    GBN_PDOS_ATOM_LIST = 8,       /* Kubo.PDOSAtomList */
+    GBN_PDOS_BY_NUMBER = 9,       /* Kubo.PDOSByNumber */
+    GBN_PDOS_PNP = 10             /* Kubo.PDOSPNP */
+};
+enum { GBN_STACK_NONE = 0, GBN_STACK_ENCAPSULATED_FOUR = 1, GBN_STACK_T3BG = 2 };
+typedef struct gbn_pdos {
+    int32_t mode;                 /* GBN_PDOS_*: the first selection flag that is set */
+    double xmin, xmax, ymin, ymax;   /* Kubo.PDOSxmin.. [Ang] */
+    int32_t min_value;            /* Kubo.PDOSMinValue */
+    int32_t super_cell;           /* Structure.SuperCell */
+    int32_t cell_size;            /* Structure.CellSize */
+    double supermoire_length;     /* Kubo.PDOSMoireSuperMoireLength [Ang] */
+    double aG;                    /* lattice parameter [Ang] */
+    int32_t ignore_layers_1_4;    /* Kubo.PDOSIgnoreLayer1and4 */
+    int32_t atom_list[6];         /* Kubo.PDOSList */
+    int32_t atom_number;          /* Kubo.PDOSNumber */
+    double pnp_delta;             /* Potential.PNPDelta [Ang] */
+    int32_t number_of_layers;     /* Kubo.NumberOfLayers */
+    int32_t stack;                /* GBN_STACK_*: Stack.EncapsulatedFourLayers / Stack.T3BG */
+    int32_t n_bn1, n_bn2, n_c;    /* Kubo.NumberOfBNAtoms1/2, Kubo.NumberOfCAtoms */
+} gbn_pdos;
+/* The atoms of the single-atom modes (3..10), in the order the reference visits them: atoms[k]
+ * (1-based) and coords[k][3], the position the reference writes to the folder's coords file (after
+ * the fractional/Cartesian conversions the selection loop makes).  rat: Cartesian positions as the
+ * Hamiltonian left them.  At most cap atoms are written; *count is the full count. */
+int gbn_pdos_atoms(const gbn_pdos* p, int64_t n, const double* rat, const int32_t* species,
+                   const int32_t* layer, const double* ucell, int64_t cap, int64_t* count,
+                   int64_t* atoms, double* coords);
+/* The sets of the layer modes (1, 2): set_of_atom[N] for gbn_lanczos_sets, and per set (at most cap)
+ * its layer, species (0 for GBN_PDOS_LAYER) and the reference's assumed atom count. */
+int gbn_pdos_sets(const gbn_pdos* p, int64_t n, const int32_t* species, const int32_t* layer,
+                  int32_t cap, int32_t* nsets, int32_t* set_of_atom, int32_t* set_layer,
+                  int32_t* set_species, double* assumed);
 /* Split form used for timing with device-resident inputs: gbn_stage_phases uploads and builds the
  * start vectors; gbn_run_staged runs nmax steps and leaves a, b on the device unless a, b are
  * non-NULL (then they are copied out). */

@@ -161,3 +161,79 @@ def test_driver_time_evolution_against_oracle(tmp_path):
         e0, d0 = orc.frac(az, bz, 0.05 / g0, 200, -8.0 / g0, 8.0 / g0, norm)
         z2 = np.loadtxt(tmp_path / f"tev.Z2_{tag}.dat")
         assert np.abs(z2[:, 1] - d0).sum() <= 1e-6 * np.abs(d0).sum()
+
+
+@pytest.mark.gpu
+def test_driver_layer_pdos_against_oracle(tmp_path):
+    """Kubo.PDOSLayer: one folder per layer with the reference's files, from random phases on the layer's
+    atoms (Kubo.SeedSet stream), against the oracle's recursion and continued fraction."""
+    from oracle import pdos as OP
+    keys = dict(INPUTS["tbg_former_names"], **{"Run.Prefix": "tbg", "Kubo.PDOS": True, "Kubo.PDOSLayer": True,
+                                                "Kubo.SeedSet": 77, "Kubo.EnergyMin": -1.0, "Kubo.EnergyMax": 1.0,
+                                                "Kubo.Epsilon": 0.01, "Calculate.OnlyDOS": True})
+    path = str(tmp_path / "Gendata.in")
+    _write(path, keys)
+    subprocess.run([DRIVER, path], check=True, cwd=str(tmp_path), capture_output=True, text=True)
+    r = R.build(dict(TypeOfSystem="TwistedBilayerBasedOnMoireCell", MoireCellParameters=(31, 30, 30, 31),
+                     TypeOfBL="Koshino", Vpppi0=2.7, Vppsigma0=0.48, BLdelta=0.319, InterlayerDistance=3.35,
+                     LayerNeighbors=100, LayerDistFactor=3.2005, Hopping=2.7))
+    geo, g0 = r["geo"], r["g0"]
+    n = geo["n"]
+    u = orc.rng_draws(77, n)
+    for lay, _, m, mask in OP.layer_sets(OP.LAYER, geo["species"], geo["layer"], number_of_layers=2):
+        psi = OP.layer_start_vector(mask, m, u)
+        a0, b0 = orc.recursion(r["nb"], r["hop"], r["h0"], psi, 150, 0)
+        folder = tmp_path / f"PDOS_layer{lay:02d}"
+        a = np.loadtxt(folder / "tbg.a0.dat")
+        b = np.loadtxt(folder / "tbg.b0.dat")
+        assert np.abs(a - a0).max() <= 1e-10 * np.abs(a0).max() and np.abs(b - b0).max() <= 1e-10 * np.abs(b0).max()
+        _, d0 = orc.frac(a0, b0, 0.01 / g0, 1000, -1.0 / g0, 1.0 / g0)
+        dos = np.loadtxt(folder / "tbg.DOS")
+        assert np.abs(dos[:, 1] - d0).sum() <= 1e-6 * np.abs(d0).sum()
+
+
+@pytest.mark.gpu
+def test_driver_atom_pdos_and_time_evolution(tmp_path):
+    """Kubo.PDOSDist: one folder per atom in the window (coords file and DOS files), then the time
+    evolution continuing from the last atom's start vector, as the reference's CalcKubo does."""
+    from oracle import pdos as OP
+    keys = {"Run.Prefix": "gr", "Run.TypeOfSystem": "Graphene", "Structure.CellSize": 60, "TB.Hopping": 2.7,
+            "MagField.Integer": 2, "Kubo.RecursionNumber": 120, "Kubo.NumberofEnergyPoints": 300,
+            "Kubo.Epsilon": 0.05, "Kubo.EnergyMin": -8.0, "Kubo.EnergyMax": 8.0, "Kubo.PDOS": True,
+            "Kubo.PDOSDist": True, "Kubo.PDOSxmin": 10.0, "Kubo.PDOSxmax": 14.0, "Kubo.PDOSymin": 5.0,
+            "Kubo.PDOSymax": 9.0, "Kubo.NumberofPolynomials": 30, "Kubo.TimeStep": 1.5,
+            "Kubo.NumberofTimeSteps": 2, "Kubo.WriteNumberofSteps": 2}
+    path = str(tmp_path / "Gendata.in")
+    _write(path, keys)
+    subprocess.run([DRIVER, path], check=True, cwd=str(tmp_path), capture_output=True, text=True)
+    r = R.build(dict(TypeOfSystem="Graphene", CellSize=60, Hopping=2.7, MagFieldInteger=2))
+    geo, g0 = r["geo"], r["g0"]
+    n = geo["n"]
+    sel = OP.select_atoms(OP.DIST, geo["rat"], geo["species"], geo["layer"], geo["ucell"], xmin=10.0, xmax=14.0,
+                          ymin=5.0, ymax=9.0)
+    assert len(sel) >= 2
+    folders = sorted(d for d in os.listdir(tmp_path) if d.startswith("PDOS_atom"))
+    assert folders == [f"PDOS_atom{i:08d}" for i, _ in sel]
+    for i, xyz in sel:
+        folder = tmp_path / f"PDOS_atom{i:08d}"
+        line = np.loadtxt(folder / "coords")
+        assert int(line[0]) == i and np.abs(line[1:] - np.asarray(xyz)).max() <= 1e-15 * 200
+        a0, b0 = orc.recursion(r["nb"], r["hop"], r["h0"], OP.site_start_vector(n, i), 120, 0)
+        a = np.loadtxt(folder / "gr.a0.dat")
+        b = np.loadtxt(folder / "gr.b0.dat")
+        assert np.abs(a - a0).max() <= 1e-10 * np.abs(a0).max() and np.abs(b - b0).max() <= 1e-10 * np.abs(b0).max()
+    # KuboTEvol from the last atom's start vector, files under the last atom's prefix
+    last = sel[-1][0]
+    psi = OP.site_start_vector(n, last)
+    a0, b0 = orc.recursion(r["nb"], r["hop"], r["h0"], psi, 120, 0)
+    ac, bc = orc.interval(a0, b0)
+    c = orc.cheb_coef(1.5, ac, bc, 30)
+    zu = np.zeros(n, np.complex128)
+    for _ in range(2):
+        psi, zu = orc.evol(r["nb"], r["hop"], r["h0"], c, ac, bc, psi, zu, 1)
+    norm = float(np.vdot(zu, zu).real)
+    az, bz = orc.recursion(r["nb"], r["hop"], r["h0"], zu / np.sqrt(norm), 120, 0)
+    folder = tmp_path / f"PDOS_atom{last:08d}"
+    ab = np.loadtxt(folder / "gr.AB_0002.dat", skiprows=1)
+    assert np.abs(ab[:, 0] - az).max() <= 1e-9 * np.abs(az).max()
+    assert np.abs(ab[:, 1] - bz).max() <= 1e-9 * np.abs(bz).max()
