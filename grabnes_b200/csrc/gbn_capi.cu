@@ -156,6 +156,7 @@ int gbn_destroy(gbn_ctx* c)
     if (c->ev1) cudaEventDestroy(c->ev1);
     for (auto& e : c->kev)
         if (e) cudaEventDestroy(e);
+    if (c->step_graph) cudaGraphExecDestroy(c->step_graph);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return GBN_OK;

@@ -79,6 +79,8 @@ struct Timing {
 };
 
 constexpr int kTimedSteps = 64;
+// steps per CUDA-graph replay of the recursion loop (even: the two x buffers alternate with the step)
+constexpr int kGraphSteps = 32;
 
 }  // namespace gbn
 
@@ -140,6 +142,11 @@ struct gbn_ctx {
 
     // Chebyshev work vectors
     gbn::DevBuf cheb[8];
+
+    // the recursion loop's CUDA graph (kGraphSteps steps) and the launch configuration it was captured with
+    cudaGraphExec_t step_graph = nullptr;
+    std::vector<unsigned char> step_graph_key;
+    int64_t graph_replays = 0;   // graph launches of the last recursion
 };
 
 namespace gbn {

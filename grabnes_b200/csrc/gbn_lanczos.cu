@@ -682,6 +682,49 @@ int lanczos_start_from_sets(gbn_ctx* c, const int32_t* d_set, const double* d_dr
     return GBN_OK;
 }
 
+// The captured graph of kGraphSteps recursion steps, rebuilt when the launch configuration changes.
+// Capturing launches nothing; the launch counter is corrected for the captured kernels.
+template <typename Step>
+static int ensure_step_graph(gbn_ctx* c, const StepLaunch& L, const StepParams& p, int64_t total, int ublk,
+                             int ugrid, Step& launch_step, int32_t k0)
+{
+    std::vector<unsigned char> key(sizeof(StepParams) + sizeof(StepLaunch) + 4 * sizeof(int64_t));
+    StepParams q;
+    memcpy(&q, &p, sizeof q);   // bytewise, padding included
+    q.x_cur = q.x_prev = nullptr;
+    const int64_t extra[4] = {total, ublk, ugrid, ((int64_t)c->prec << 32) | (int64_t)c->nrhs};
+    memcpy(key.data(), &q, sizeof q);
+    memcpy(key.data() + sizeof q, &L, sizeof L);
+    memcpy(key.data() + sizeof q + sizeof L, extra, sizeof extra);
+    const void* vp[3] = {c->vec[0].p, c->vec[1].p, c->vec[2].p};
+    key.insert(key.end(), (const unsigned char*)vp, (const unsigned char*)vp + sizeof vp);
+    if (c->step_graph && key == c->step_graph_key) return GBN_OK;
+    if (c->step_graph) {
+        cudaGraphExecDestroy(c->step_graph);
+        c->step_graph = nullptr;
+    }
+    const int64_t before = c->launches;
+    GBN_CK(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = GBN_OK;
+    for (int32_t k = k0; k < k0 + kGraphSteps && rc == GBN_OK; ++k) rc = launch_step(k);
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+    c->launches = before;
+    if (rc) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    if (e != cudaSuccess) return cuda_fail(c, e, "cudaStreamEndCapture");
+    const cudaError_t e2 = cudaGraphInstantiate(&c->step_graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e2 != cudaSuccess) {
+        c->step_graph = nullptr;
+        return cuda_fail(c, e2, "cudaGraphInstantiate");
+    }
+    c->step_graph_key = key;
+    return GBN_OK;
+}
+
 int lanczos_run(gbn_ctx* c, int32_t nmax)
 {
     const int R = c->nrhs;
@@ -689,10 +732,12 @@ int lanczos_run(gbn_ctx* c, int32_t nmax)
     k_init_scalars<<<1, 64, 0, c->stream>>>(c->scal.as<double>(), c->counter.as<unsigned int>(), R);
     GBN_CK_LAUNCH(c);
     StepLaunch L;
+    memset(&L, 0, sizeof L);   // the graph key compares these structures bytewise, padding included
     const int rc = step_launch(c, R, &L);
     if (rc) return rc;
     c->last_staged = L.staged;
     StepParams p;
+    memset(&p, 0, sizeof p);
     p.slice_ptr = c->ell.slice_ptr.as<int64_t>();
     p.mat = c->ell.mat.as<unsigned char>();
     p.entry_bytes = c->ell.entry_bytes;
@@ -719,9 +764,9 @@ int lanczos_run(gbn_ctx* c, int32_t nmax)
     if (!c->kev[0]) {
         for (int i = 0; i < 3 * kTimedSteps; ++i) GBN_CK(c, cudaEventCreate(&c->kev[i]));
     }
-    GBN_CK(c, cudaEventRecord(c->ev0, c->stream));
-    for (int32_t k = 0; k < nmax; ++k) {
-        // step k (0-based): x_prev in vec[1 + k%2], x_cur written to vec[1 + (k+1)%2]
+    // step k (0-based): x_prev in vec[1 + k%2], x_cur written to vec[1 + (k+1)%2]; the step index of the
+    // a_n, b_n outputs lives on the device (counter[1]), so a run of an even number of steps replays as is
+    auto launch_step = [&](int32_t k) -> int {
         void* xprev = c->vec[1 + (k & 1)].p;
         void* xcur = c->vec[1 + ((k + 1) & 1)].p;
         if (k < nsample) GBN_CK(c, cudaEventRecord(c->kev[3 * k], c->stream));
@@ -738,6 +783,31 @@ int lanczos_run(gbn_ctx* c, int32_t nmax)
         L.fn<<<L.grid, L.block, L.smem, c->stream>>>(p);
         GBN_CK_LAUNCH(c);
         if (k < nsample) GBN_CK(c, cudaEventRecord(c->kev[3 * k + 2], c->stream));
+        return GBN_OK;
+    };
+    c->graph_replays = 0;
+    GBN_CK(c, cudaEventRecord(c->ev0, c->stream));
+    int32_t k = 0;
+    for (; k < nsample; ++k) {
+        const int rc2 = launch_step(k);
+        if (rc2) return rc2;
+    }
+    // The remaining steps replay a captured graph of kGraphSteps steps (launch overhead is what limits
+    // small cells), unless the caller is capturing this stream into a graph of its own.
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    GBN_CK(c, cudaStreamIsCapturing(c->stream, &cap));
+    if (cap == cudaStreamCaptureStatusNone && nmax - k >= 2 * kGraphSteps) {
+        const int rc2 = ensure_step_graph(c, L, p, total, ublk, ugrid, launch_step, k);
+        if (rc2) return rc2;
+        for (; nmax - k >= kGraphSteps; k += kGraphSteps) {
+            GBN_CK(c, cudaGraphLaunch(c->step_graph, c->stream));
+            c->launches += 2 * kGraphSteps;
+            ++c->graph_replays;
+        }
+    }
+    for (; k < nmax; ++k) {
+        const int rc2 = launch_step(k);
+        if (rc2) return rc2;
     }
     GBN_CK(c, cudaEventRecord(c->ev1, c->stream));
     GBN_CK(c, cudaEventSynchronize(c->ev1));
