@@ -99,7 +99,7 @@ EXPORTS = ["gbn_cell_atoms", "gbn_build_cell", "gbn_cart_roundtrip", "gbn_rng_un
            "gbn_peierls", "gbn_get_hamiltonian", "gbn_load_hamiltonian", "gbn_lanczos", "gbn_lanczos_phases",
            "gbn_stage_phases", "gbn_run_staged", "gbn_cf_dos", "gbn_cheb_evolve", "gbn_kubo_evol", "gbn_set_neighd", "gbn_lanczos_noalloc",
            "gbn_cheb_interval", "gbn_cheb_coef", "gbn_dos_gradient", "gbn_lanczos_sites", "gbn_lanczos_sets",
-           "gbn_pdos_atoms", "gbn_pdos_sets"]
+           "gbn_pdos_atoms", "gbn_pdos_sets", "gbn_lanczos_fields"]
 
 
 def _declare(L):
@@ -130,6 +130,8 @@ def _declare(L):
     L.gbn_lanczos.argtypes = [vp, i32, i32, _p(np.complex128), _opt(np.int32), i32, _p(np.float64), _p(np.float64)]
     L.gbn_lanczos_phases.argtypes = [vp, i32, i32, _p(np.float64), _opt(np.int32), i32, _p(np.float64),
                                      _p(np.float64)]
+    L.gbn_lanczos_fields.argtypes = [vp, i32, i32, _p(np.int32), i32, _p(np.float64), _opt(np.int32), i32,
+                                     _p(np.float64), _p(np.float64)]
     L.gbn_lanczos_sites.argtypes = [vp, i32, i32, _p(np.int64), _opt(np.int32), i32, _p(np.float64), _p(np.float64)]
     L.gbn_lanczos_sets.argtypes = [vp, i32, i32, _p(np.int32), _p(np.float64), _p(np.float64), _opt(np.int32), i32,
                                    _p(np.float64), _p(np.float64)]
@@ -286,6 +288,22 @@ class Context:
         b = np.zeros((nrhs, nmax))
         self._ck(self._L.gbn_lanczos_phases(self._h, precision, nrhs, uu.reshape(-1), ns, nmax, a.reshape(-1),
                                             b.reshape(-1)))
+        return a, b
+
+    def lanczos_fields(self, m, u, nsteps, precision=GBN_MIXED):
+        """Random-phase recursions of many fields in one batch from the field-free assembled Hamiltonian:
+        m[nfields] flux quanta, u[nfields, nvec, N] draws, nsteps int or [nfields, nvec];
+        returns a, b [nfields, nvec, nmax]."""
+        mm = _c(m, np.int32)
+        uu = np.ascontiguousarray(u, np.float64)
+        nf, nv = uu.shape[0], uu.shape[1]
+        assert len(mm) == nf
+        ns = np.broadcast_to(np.asarray(nsteps, np.int32), (nf, nv)).copy()
+        nmax = int(ns.max())
+        a = np.zeros((nf, nv, nmax))
+        b = np.zeros((nf, nv, nmax))
+        self._ck(self._L.gbn_lanczos_fields(self._h, precision, nf, mm, nv, uu.reshape(-1), ns.reshape(-1), nmax,
+                                            a.reshape(-1), b.reshape(-1)))
         return a, b
 
     def lanczos_sites(self, sites, nsteps, precision=GBN_FP64):

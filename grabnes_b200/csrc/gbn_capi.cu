@@ -37,10 +37,10 @@ static int tile_width(int nrhs)
 // vectors of right-hand sides r0 .. r0 + cnt - 1 into the tile (after lanczos_prepare).
 template <typename Start>
 static int run_tiles(gbn_ctx* c, int prec, int nrhs, Start&& start, const int32_t* nsteps, int32_t nmax, double* a,
-                     double* b)
+                     double* b, bool field = false)
 {
     const int T = tile_width(nrhs);
-    int rc = lanczos_prepare(c, prec, T);
+    int rc = lanczos_prepare(c, prec, T, field);
     if (rc) return rc;
     double step_ms = 0.0, spmm_sum = 0.0, upd_sum = 0.0;
     int64_t launches = 0;
@@ -494,6 +494,77 @@ int gbn_lanczos_sets(gbn_ctx* c, int32_t precision, int32_t nsets, const int32_t
     return GBN_OK;
 }
 
+int gbn_lanczos_fields(gbn_ctx* c, int32_t precision, int32_t nfields, const int32_t* m, int32_t nvec, const double* u,
+                       const int32_t* nsteps, int32_t nmax, double* a, double* b)
+{
+    if (!c) return GBN_ERR_ARG;
+    if (nfields < 1 || nvec < 1 || !m) return fail(c, GBN_ERR_ARG, "nfields and nvec must be positive, m not NULL");
+    const int64_t nr64 = (int64_t)nfields * nvec;
+    if (nr64 > (int64_t)1 << 30) return fail(c, GBN_ERR_ARG, "too many right-hand sides");
+    const int nrhs = (int)nr64;
+    int rc = check_solver_args(c, precision, nrhs, u, nsteps, nmax, a, b);
+    if (rc) return rc;
+    if (c->has_field)
+        return fail(c, GBN_ERR_STATE, "the hoppings already carry a field: assemble again without gbn_peierls");
+    if (c->ham_complex)
+        return fail(c, GBN_ERR_STATE, "batched fields need a Hamiltonian assembled on the device (gbn_assemble)");
+    cudaSetDevice(c->device);
+    rc = peierls_turns(c);
+    if (rc) return rc;
+    // the RPT right-hand sides of a thread share one field: RPT divides the vectors per field
+    const int T = tile_width(nrhs);
+    const int saved_rpt = c->tune_rpt;
+    int rpt, tpr;
+    split_rhs(precision, T, saved_rpt, &rpt, &tpr);
+    while (nvec % rpt) rpt >>= 1;
+    // run order: within a field its vectors by decreasing length, in chunks of RPT; chunks by decreasing
+    // length, so that a tile's vectors end close together (a tile runs to its longest vector)
+    auto len = [&](int r) { return nsteps ? nsteps[r] : nmax; };
+    std::vector<std::pair<int32_t, int32_t>> chunks;   // (length of the chunk's first vector, first slot)
+    std::vector<int32_t> sorted((size_t)nrhs);
+    for (int f = 0; f < nfields; ++f) {
+        int32_t* v = sorted.data() + (size_t)f * nvec;
+        for (int k = 0; k < nvec; ++k) v[k] = f * nvec + k;
+        std::stable_sort(v, v + nvec, [&](int32_t x, int32_t y) { return len(x) > len(y); });
+        for (int k = 0; k < nvec; k += rpt) chunks.push_back({len(v[k]), f * nvec + k});
+    }
+    std::stable_sort(chunks.begin(), chunks.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
+    std::vector<int32_t> order, ns_run, fm_run;
+    for (const auto& ch : chunks)
+        for (int k = 0; k < rpt; ++k) {
+            const int32_t r = sorted[(size_t)ch.second + k];
+            order.push_back(r);
+            ns_run.push_back(len(r));
+            fm_run.push_back(m[r / nvec]);
+        }
+    const int64_t n = c->n;
+    GBN_CK(c, c->upload.ensure(sizeof(double) * (size_t)n * T));
+    GBN_CK(c, c->field_m.ensure(sizeof(int32_t) * (size_t)T));
+    std::vector<double> ar((size_t)nrhs * nmax), br((size_t)nrhs * nmax);
+    std::vector<int32_t> fm((size_t)T);
+    c->tune_rpt = rpt;
+    rc = run_tiles(
+        c, precision, nrhs,
+        [&](int r0, int cnt) -> int {
+            for (int r = 0; r < cnt; ++r)
+                GBN_CK(c, cudaMemcpyAsync(c->upload.as<double>() + (size_t)r * n, u + (size_t)order[(size_t)(r0 + r)] * n,
+                                          sizeof(double) * (size_t)n, cudaMemcpyHostToDevice, c->stream));
+            for (int r = 0; r < T; ++r) fm[(size_t)r] = fm_run[(size_t)(r0 + (r < cnt ? r : 0))];
+            GBN_CK(c, cudaMemcpyAsync(c->field_m.p, fm.data(), sizeof(int32_t) * (size_t)T, cudaMemcpyHostToDevice,
+                                      c->stream));
+            return lanczos_start_from_phases(c, c->upload.as<double>(), cnt);
+        },
+        ns_run.data(), nmax, ar.data(), br.data(), true);
+    c->tune_rpt = saved_rpt;
+    c->staged = false;
+    if (rc) return rc;
+    for (int r = 0; r < nrhs; ++r) {
+        memcpy(a + (size_t)order[(size_t)r] * nmax, ar.data() + (size_t)r * nmax, sizeof(double) * nmax);
+        memcpy(b + (size_t)order[(size_t)r] * nmax, br.data() + (size_t)r * nmax, sizeof(double) * nmax);
+    }
+    return GBN_OK;
+}
+
 int gbn_stage_phases(gbn_ctx* c, int32_t precision, int32_t nrhs, const double* u)
 {
     if (!c) return GBN_ERR_ARG;
@@ -521,7 +592,7 @@ int gbn_run_staged(gbn_ctx* c, int32_t nmax, double* a, double* b)
     if (nmax < 1) return fail(c, GBN_ERR_ARG, "nmax must be at least 1");
     cudaSetDevice(c->device);
     int rc = GBN_OK;
-    if (!c->ell.valid) {   // the layout was invalidated (new tuning or Hamiltonian) since staging
+    if (!c->ell.valid || c->ell.field) {   // the layout was invalidated (new tuning or Hamiltonian) since staging
         rc = lanczos_prepare(c, c->prec, c->nrhs);
         if (rc) return rc;
     }

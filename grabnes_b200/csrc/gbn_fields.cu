@@ -1,0 +1,39 @@
+// Sparse-product kernels of the field-batched layout: one field-free matrix serves right-hand sides of
+// many perpendicular fields.  Each stored entry holds the field-free hopping and its Peierls phase per
+// flux quantum (HamPeierlsPeriodicGauge, lanczosKuboCode/Src/ham.F90:12834-12882, is linear in the
+// number of flux quanta m), and the threads of a right-hand side of m quanta rotate the entry by
+// exp(2 pi i frac(m tau)) as they use it.  One matrix stream then feeds every field of a tile instead
+// of one assembled matrix per field.
+#include "gbn_step.cuh"
+
+namespace gbn {
+
+template <typename VT, int G>
+static StepFn pick_field_g(int rpt, int tpr)
+{
+#define GBN_CASE(RP, TP) \
+    if (rpt == RP && tpr == TP) return k_spmm_step<VT, false, G, RP, TP, true>;
+    GBN_CASE(1, 1) GBN_CASE(1, 2) GBN_CASE(1, 4) GBN_CASE(1, 8) GBN_CASE(1, 16) GBN_CASE(1, 32)
+    GBN_CASE(2, 1) GBN_CASE(2, 2) GBN_CASE(2, 4) GBN_CASE(2, 8) GBN_CASE(2, 16)
+    if constexpr (sizeof(VT) == 4) {
+        GBN_CASE(4, 1) GBN_CASE(4, 2) GBN_CASE(4, 4) GBN_CASE(4, 8)
+    }
+#undef GBN_CASE
+    return nullptr;
+}
+
+StepFn field_step_kernel(int prec, int G, int rpt, int tpr)
+{
+    if (prec == GBN_MIXED) {
+        if (G == 1) return pick_field_g<float, 1>(rpt, tpr);
+        if (G == 2) return pick_field_g<float, 2>(rpt, tpr);
+        if (G == 4) return pick_field_g<float, 4>(rpt, tpr);
+    } else {
+        if (G == 1) return pick_field_g<double, 1>(rpt, tpr);
+        if (G == 2) return pick_field_g<double, 2>(rpt, tpr);
+        if (G == 4) return pick_field_g<double, 4>(rpt, tpr);
+    }
+    return nullptr;
+}
+
+}  // namespace gbn

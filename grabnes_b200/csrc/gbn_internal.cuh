@@ -65,6 +65,7 @@ struct Ell {
     int dval_dir = 0;        // NeighD component of dval (1 = x, 2 = y; 0 = not built)
     int64_t max_record = 0;  // bytes of the largest slice record
     int64_t cap_record = 0;  // staging buffer size: 99.5 % of the records fit (larger ones are read in place)
+    bool field = false;      // field-batched values: field-free hopping and Peierls phase per flux quantum
     bool valid = false;
 };
 
@@ -110,6 +111,9 @@ struct gbn_ctx {
     gbn::DevBuf rat_hop;   // positions used for the Peierls phases
     bool have_ham = false;
     bool ham_complex = false;
+    bool has_field = false;   // gbn_peierls has been applied to the assembled hoppings
+    gbn::DevBuf ptau;         // uint64 [n*max_neigh]: Peierls phase per flux quantum, fraction of a turn * 2^64
+    gbn::DevBuf field_m;      // int32 [R]: flux quanta of each right-hand side of a field-batched tile
 
     // row permutation used by the solver: perm[new] = reference index, iperm[reference] = new
     gbn::DevBuf perm, iperm;
@@ -170,11 +174,12 @@ int cuda_fail(gbn_ctx* c, cudaError_t e, const char* what);
 // layout / permutation (gbn_layout.cu)
 int build_identity_perm(gbn_ctx* c);
 int build_spatial_perm(gbn_ctx* c);
-int build_ell(gbn_ctx* c, int prec, int G, int gpw);
+// field: the field-batched values (FieldVal: field-free hopping and c->ptau), for gbn_lanczos_fields
+int build_ell(gbn_ctx* c, int prec, int G, int gpw, bool field = false);
 int auto_group(const gbn_ctx* c);
 
 // recursion (gbn_lanczos.cu)
-int lanczos_prepare(gbn_ctx* c, int prec, int nrhs);
+int lanczos_prepare(gbn_ctx* c, int prec, int nrhs, bool field = false);
 int lanczos_start_from_phases(gbn_ctx* c, const double* d_u, int nrhs_real);
 int lanczos_start_from_psi(gbn_ctx* c, const double* d_psi, int nrhs_real);
 int lanczos_start_from_sites(gbn_ctx* c, const int64_t* d_site, int nrhs_real);
@@ -192,6 +197,7 @@ int cf_dos(gbn_ctx* c, int32_t nrhs, const double* d_a, const double* d_b, const
 int neigh_search(gbn_ctx* c, double cut2intra, double cut2inter, int32_t second_layer);
 int assemble(gbn_ctx* c, const gbn_model* m, const double* d_rat_on, const double* d_rat_hop, const double* d_uniform);
 int peierls(gbn_ctx* c, double flux);
+int peierls_turns(gbn_ctx* c);   // c->ptau from the positions, images and cell of the assembled model
 
 // gradient of a DOS loss (gbn_adjoint.cu)
 int dos_gradient(gbn_ctx* c, const gbn_model* m, double g0, const double* u_host, int32_t K, int32_t C, double eta,

@@ -23,28 +23,9 @@
 #include <math.h>
 #include <string.h>
 
-#include "gbn_spmm.cuh"
+#include "gbn_step.cuh"
 
 namespace gbn {
-
-struct StepParams {
-    const int64_t* slice_ptr;
-    const unsigned char* mat;  // slice records (column indices, then G values per union column)
-    int64_t entry_bytes;       // 4 + G * value bytes
-    int64_t cap_record;        // bytes of a staging buffer (larger records are read in place)
-    int32_t prefetch;          // staged kernel: prefetch the gather rows of a slice (1 L2, 2 L1)
-    const void* h0;
-    const void* x_cur;   // x_k   [npad][R] (gathered)
-    const void* x_prev;  // x_{k-1}
-    void* v_out;         // v_{k+1}
-    double* scal;        // [R][2] a_{k-1}, b_{k-1}
-    double* partials;    // [gridDim][R][4]
-    unsigned int* counter;  // [0] block counter, [1] step index, [2] error flag
-    double* a_out;       // [R][nmax]
-    double* b_out;
-    int64_t nslices;
-    int32_t nmax;
-};
 
 // ---------------------------------------------------------------------------- update kernel
 // x_k = (v_k - a x_{k-1}) * (1/b) for all rows and right-hand sides (streaming).  The grid stride and
@@ -68,163 +49,6 @@ __global__ void __launch_bounds__(256) k_update(const typename V2<VT>::t* __rest
 }
 
 // ---------------------------------------------------------------------------- sparse product
-struct SliceSums {
-    double s1, s2, s3, s4;
-};
-
-// Reduction of the four sums over the block, then by the last block over all blocks; writes a_k, b_k.
-// Needs at least 4 R threads per block.
-template <int RPT, int TPR>
-__device__ __forceinline__ void reduce_and_finalize(const StepParams& p, SliceSums* acc_s)
-{
-    constexpr int R = RPT * TPR;
-    const int lane = threadIdx.x & 31;
-    const int sub = lane / TPR;
-    const int q = lane % TPR;
-#pragma unroll
-    for (int t = 0; t < RPT; ++t) {
-#pragma unroll
-        for (int off = TPR; off < 32; off <<= 1) {
-            acc_s[t].s1 += __shfl_xor_sync(0xffffffffu, acc_s[t].s1, off);
-            acc_s[t].s2 += __shfl_xor_sync(0xffffffffu, acc_s[t].s2, off);
-            acc_s[t].s3 += __shfl_xor_sync(0xffffffffu, acc_s[t].s3, off);
-            acc_s[t].s4 += __shfl_xor_sync(0xffffffffu, acc_s[t].s4, off);
-        }
-    }
-    __shared__ double red[8][R][4];
-    const int wib = threadIdx.x >> 5;
-    if (sub == 0) {
-#pragma unroll
-        for (int t = 0; t < RPT; ++t) {
-            const int r = q * RPT + t;
-            red[wib][r][0] = acc_s[t].s1; red[wib][r][1] = acc_s[t].s2;
-            red[wib][r][2] = acc_s[t].s3; red[wib][r][3] = acc_s[t].s4;
-        }
-    }
-    __syncthreads();
-    if (threadIdx.x < R * 4) {
-        const int r = threadIdx.x >> 2, k = threadIdx.x & 3;
-        double a = 0.0;
-        for (int wI = 0; wI < (int)(blockDim.x >> 5); ++wI) a += red[wI][r][k];
-        p.partials[((int64_t)blockIdx.x * R + r) * 4 + k] = a;
-    }
-    // the last block to finish reduces all blocks in a fixed order
-    __shared__ bool last;
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) last = (atomicAdd(p.counter, 1u) == gridDim.x - 1);
-    __syncthreads();
-    if (!last) return;
-    __threadfence();
-    __shared__ double tot[R][4];
-    if (threadIdx.x < R * 4) {
-        const int r = threadIdx.x >> 2, k = threadIdx.x & 3;
-        double a = 0.0;
-        for (unsigned int bI = 0; bI < gridDim.x; ++bI) a += __ldcg(&p.partials[((int64_t)bI * R + r) * 4 + k]);
-        tot[r][k] = a;
-    }
-    __syncthreads();
-    if (threadIdx.x < R) {
-        const int r = threadIdx.x;
-        const unsigned int step = p.counter[1];
-        const double a = tot[r][0];
-        const double b2 = tot[r][1] - 2.0 * a * tot[r][2] + a * a * tot[r][3];
-        const double b = sqrt(fabs(b2));
-        if (!(b > 0.0) || !isfinite(a) || !isfinite(b)) atomicOr(&p.counter[2], 1u);
-        if ((int)step < p.nmax) {
-            p.a_out[(int64_t)r * p.nmax + step] = a;
-            p.b_out[(int64_t)r * p.nmax + step] = b;
-        }
-        p.scal[2 * r] = a;
-        p.scal[2 * r + 1] = b;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        p.counter[0] = 0u;
-        p.counter[1] = p.counter[1] + 1u;
-    }
-}
-
-// One slice of the grouped sliced ELL: GPW = 32/TPR groups; the TPR threads of a group each hold RPT
-// right-hand sides of all G rows of the group.  Per union column a thread reads the column index and
-// the G values (same address for the group's threads) and gathers RPT vector elements of that column
-// once for all G rows.  The epilogue per row adds the on-site term and is FP64 from there:
-// v_{k+1} = y - b_{k-1} x_{k-1} rounded once, and the four dot-product terms.  cp/vp point at the
-// thread's group in the slice record, in global memory (streamed) or in shared memory (SMEM).
-template <typename VT, bool CPLX, int G, int RPT, int TPR, bool SMEM>
-__device__ __forceinline__ void group_slice(const StepParams& p, int64_t s, int w, const int32_t* __restrict__ cp,
-                                            const typename Hop<VT, CPLX>::t* __restrict__ vp, const double* cb,
-                                            SliceSums* acc_s)
-{
-    using C2 = typename V2<VT>::t;
-    constexpr int GPW = 32 / TPR;
-    constexpr int R = RPT * TPR;
-    const int lane = threadIdx.x & 31;
-    const int sub = lane / TPR;
-    const int q = lane % TPR;
-    const C2* __restrict__ xc = static_cast<const C2*>(p.x_cur);
-    const C2* __restrict__ xp = static_cast<const C2*>(p.x_prev);
-    C2* __restrict__ vout = static_cast<C2*>(p.v_out);
-    const VT* __restrict__ h0 = static_cast<const VT*>(p.h0);
-    const int64_t row0 = (s * GPW + sub) * G;
-    C2 acc[G][RPT];
-    group_columns<VT, CPLX, G, RPT, TPR, SMEM>(xc, w, cp, vp, acc);
-    // epilogue per row: the on-site term (own x_k row, loaded here so that it holds no registers during
-    // the column loop), then v_{k+1} and the dot-product terms in FP64
-#pragma unroll
-    for (int g = 0; g < G; ++g) {
-        C2 xo[RPT], xm[RPT], vn[RPT];
-        VecIO<VT, RPT>::load(xc + (row0 + g) * R + q * RPT, xo);
-        VecIO<VT, RPT>::load(xp + (row0 + g) * R + q * RPT, xm);
-        const VT d = h0[row0 + g];
-#pragma unroll
-        for (int t = 0; t < RPT; ++t) {
-            acc[g][t].x = fma(d, xo[t].x, acc[g][t].x);
-            acc[g][t].y = fma(d, xo[t].y, acc[g][t].y);
-            vn[t].x = (VT)((double)acc[g][t].x - cb[t] * (double)xm[t].x);
-            vn[t].y = (VT)((double)acc[g][t].y - cb[t] * (double)xm[t].y);
-            const double xr = xo[t].x, xi = xo[t].y, yr = acc[g][t].x, yi = acc[g][t].y;
-            const double vr = vn[t].x, vi = vn[t].y;
-            acc_s[t].s1 += xr * yr + xi * yi;
-            acc_s[t].s2 += vr * vr + vi * vi;
-            acc_s[t].s3 += xr * vr + xi * vi;
-            acc_s[t].s4 += xr * xr + xi * xi;
-        }
-        VecIO<VT, RPT>::store(vout + (row0 + g) * R + q * RPT, vn);
-    }
-}
-
-// Matrix records read from global memory.  Every block owns a contiguous range of slices (a compact
-// region of the row order); its warps take neighbouring slices, so the rows they gather overlap in L1.
-template <typename VT, bool CPLX, int G, int RPT, int TPR>
-__global__ void __launch_bounds__(256) k_spmm_step(StepParams p)
-{
-    using HT = typename Hop<VT, CPLX>::t;
-    constexpr int GPW = 32 / TPR;
-    const int q = (threadIdx.x & 31) % TPR;
-    const int sub = (threadIdx.x & 31) / TPR;
-    double cb[RPT];
-    SliceSums acc_s[RPT];
-#pragma unroll
-    for (int t = 0; t < RPT; ++t) {
-        cb[t] = p.scal[2 * (q * RPT + t) + 1];
-        acc_s[t] = SliceSums{0.0, 0.0, 0.0, 0.0};
-    }
-    const int nwb = (int)(blockDim.x >> 5);
-    const int64_t per = (p.nslices + gridDim.x - 1) / gridDim.x;
-    const int64_t s0 = (int64_t)blockIdx.x * per;
-    const int64_t s1e = (s0 + per < p.nslices) ? s0 + per : p.nslices;
-    for (int64_t s = s0 + (threadIdx.x >> 5); s < s1e; s += nwb) {
-        const int64_t base = p.slice_ptr[s];
-        const int w = (int)((p.slice_ptr[s + 1] - base) / GPW);
-        const unsigned char* rec = p.mat + base * p.entry_bytes;
-        group_slice<VT, CPLX, G, RPT, TPR, false>(p, s, w, reinterpret_cast<const int32_t*>(rec) + sub,
-                                                  reinterpret_cast<const HT*>(rec + (size_t)w * GPW * 4) + sub * G,
-                                                  cb, acc_s);
-    }
-    reduce_and_finalize<RPT, TPR>(p, acc_s);
-}
-
 // ---- bulk asynchronous copies (cp.async.bulk, the TMA engine) into shared memory, mbarrier completion
 __device__ __forceinline__ uint32_t smem_u32(const void* ptr) { return (uint32_t)__cvta_generic_to_shared(ptr); }
 
@@ -513,7 +337,6 @@ void split_rhs(int prec, int R, int want, int* rpt, int* tpr)
     *tpr = R / r;
 }
 
-using StepFn = void (*)(StepParams);
 
 template <typename VT, bool CPLX, int G>
 static StepFn pick_g(int rpt, int tpr, bool staged)
@@ -562,9 +385,15 @@ static int step_launch(gbn_ctx* c, int R, StepLaunch* L)
     const Ell& E = c->ell;
     const size_t per_warp = 2 * (size_t)E.cap_record;
     const size_t min_warps = (size_t)((4 * R + 31) / 32);
-    const bool staged = c->tune_staged != 0 && per_warp > 0 && 128 + min_warps * per_warp <= kStagedSmemBudget;
+    const bool staged = !E.field && c->tune_staged != 0 && per_warp > 0 && 128 + min_warps * per_warp <= kStagedSmemBudget;
     L->staged = staged;
-    L->fn = step_kernel(c->prec, E.cplx, E.G, R, c->tune_rpt, staged);
+    if (E.field) {
+        int rpt, tpr;
+        split_rhs(c->prec, R, c->tune_rpt, &rpt, &tpr);
+        L->fn = field_step_kernel(c->prec, E.G, rpt, tpr);
+    } else {
+        L->fn = step_kernel(c->prec, E.cplx, E.G, R, c->tune_rpt, staged);
+    }
     if (!L->fn) return fail(c, GBN_ERR_ARG, "no recursion kernel for this tile width");
     L->block = 256;
     L->smem = 0;
@@ -583,7 +412,7 @@ static int step_launch(gbn_ctx* c, int R, StepLaunch* L)
     return GBN_OK;
 }
 
-int lanczos_prepare(gbn_ctx* c, int prec, int nrhs)
+int lanczos_prepare(gbn_ctx* c, int prec, int nrhs, bool field)
 {
     if (nrhs != 1 && nrhs != 2 && nrhs != 4 && nrhs != 8 && nrhs != 16 && nrhs != 32)
         return fail(c, GBN_ERR_ARG, "internal: tile width must be 1, 2, 4, 8, 16 or 32");
@@ -591,8 +420,8 @@ int lanczos_prepare(gbn_ctx* c, int prec, int nrhs)
     split_rhs(prec, nrhs, c->tune_rpt, &rpt, &tpr);
     const int gpw = 32 / tpr;
     const int G = c->tune_group > 0 ? c->tune_group : auto_group(c);
-    if (!c->ell.valid || c->ell.prec != prec || c->ell.gpw != gpw || c->ell.G != G) {
-        const int rc = build_ell(c, prec, G, gpw);
+    if (!c->ell.valid || c->ell.prec != prec || c->ell.gpw != gpw || c->ell.G != G || c->ell.field != field) {
+        const int rc = build_ell(c, prec, G, gpw, field);
         if (rc) return rc;
     }
     c->prec = prec;
@@ -752,6 +581,7 @@ int lanczos_run(gbn_ctx* c, int32_t nmax)
     p.b_out = c->ab.as<double>() + (size_t)R * nmax;
     p.nslices = c->ell.nslices;
     p.nmax = nmax;
+    p.field_m = c->field_m.as<int32_t>();
     const int64_t total = c->ell.npad * R;
     const int ublk = 256;   // a multiple of R (k_update keeps one right-hand side per thread)
     const int ugrid = c->num_sms * 8;

@@ -12,12 +12,14 @@
 #include <thrust/scan.h>
 #include <thrust/sequence.h>
 #include <thrust/sort.h>
+#include <thrust/transform.h>
 #include <thrust/unique.h>
 
 #include <algorithm>
 #include <vector>
 
 #include "gbn_internal.cuh"
+#include "gbn_spmm.cuh"
 
 namespace gbn {
 
@@ -212,6 +214,16 @@ template <> __device__ __forceinline__ float neg_hop<float>(double2 h) { return 
 template <> __device__ __forceinline__ double neg_hop<double>(double2 h) { return -h.x; }
 template <> __device__ __forceinline__ float2 neg_hop<float2>(double2 h) { return make_float2((float)(-h.x), (float)(-h.y)); }
 template <> __device__ __forceinline__ double2 neg_hop<double2>(double2 h) { return make_double2(-h.x, -h.y); }
+// field-batched value of one entry: the negated field-free hopping (real) and its phase per flux quantum
+template <typename HV> __device__ __forceinline__ HV field_val(double2 h, uint64_t tau);
+template <> __device__ __forceinline__ FieldVal<float> field_val<FieldVal<float>>(double2 h, uint64_t tau)
+{
+    return FieldVal<float>{(float)(-h.x), (uint32_t)((tau + 0x80000000ull) >> 32)};
+}
+template <> __device__ __forceinline__ FieldVal<double> field_val<FieldVal<double>>(double2 h, uint64_t tau)
+{
+    return FieldVal<double>{-h.x, tau};
+}
 __device__ __forceinline__ void add_to(float& a, float b) { a += b; }
 __device__ __forceinline__ void add_to(double& a, double b) { a += b; }
 __device__ __forceinline__ void add_to(float2& a, float2 b) { a.x += b.x; a.y += b.y; }
@@ -220,12 +232,13 @@ __device__ __forceinline__ void add_to(double2& a, double2 b) { a.x += b.x; a.y 
 // One thread per group (solver order): union columns, padding columns, values (the records must be
 // zeroed), on-site terms.  An entry that repeats a column of its row (two periodic images of one atom)
 // is added to the same value.
-template <typename HV, typename DV>
+// FIELD: values FieldVal from the field-free hoppings and tau (each column at most once per row).
+template <typename HV, typename DV, bool FIELD = false>
 __global__ void k_fill_groups(const int32_t* nneigh, const int32_t* nlist, const double2* hopp, const double* h0,
                               const int32_t* rperm, const int32_t* riperm, const int32_t* gorder, const int32_t* ucount,
                               const int64_t* ustart, const uint64_t* ukeys, int64_t n, int32_t max_neigh, int G,
                               int gpw, int64_t ngroups, int64_t nslices, const int64_t* slice_ptr, unsigned char* mat,
-                              DV* h0p)
+                              DV* h0p, const uint64_t* tau = nullptr)
 {
     const int64_t ng = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (ng >= nslices * gpw) return;
@@ -263,9 +276,21 @@ __global__ void k_fill_groups(const int32_t* nneigh, const int32_t* nlist, const
                 if ((uint32_t)ul[mid] < rc) lo = mid + 1;
                 else hi = mid;
             }
-            add_to(val[(lo * gpw + j) * G + rr], neg_hop<HV>(hopp[p * max_neigh + e]));
+            if constexpr (FIELD) val[(lo * gpw + j) * G + rr] = field_val<HV>(hopp[p * max_neigh + e], tau[p * max_neigh + e]);
+            else add_to(val[(lo * gpw + j) * G + rr], neg_hop<HV>(hopp[p * max_neigh + e]));
         }
     }
+}
+
+// (row, column) keys of all entries in the reference order, to find rows that hold two periodic images
+// of one neighbour (the field-batched layout cannot merge them: their phases differ)
+__global__ void k_row_keys(const int32_t* nneigh, const int32_t* nlist, int64_t n, int32_t max_neigh,
+                           const int64_t* off, uint64_t* keys)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    for (int e = 0; e < nneigh[i]; ++e)
+        keys[off[i] + e] = ((uint64_t)i << 32) | (uint32_t)(nlist[i * max_neigh + e] - 1);
 }
 
 // bytes of the largest slice record
@@ -284,7 +309,7 @@ int auto_group(const gbn_ctx* c)
     return per_row >= 8.0 ? 2 : 1;
 }
 
-int build_ell(gbn_ctx* c, int prec, int G, int gpw)
+int build_ell(gbn_ctx* c, int prec, int G, int gpw, bool field)
 {
     if (!c->have_ham) return fail(c, GBN_ERR_STATE, "no Hamiltonian loaded");
     if (G != 1 && G != 2 && G != 4) return fail(c, GBN_ERR_ARG, "rows per group must be 1, 2 or 4");
@@ -299,6 +324,9 @@ int build_ell(gbn_ctx* c, int prec, int G, int gpw)
     E.gpw = gpw;
     E.prec = prec;
     E.cplx = c->ham_complex;
+    E.field = field;
+    if (field && (c->ham_complex || !c->ptau.p))
+        return fail(c, GBN_ERR_STATE, "batched fields need the field-free assembled Hamiltonian and its phases");
     const int64_t n = c->n;
     E.ngroups = (n + G - 1) / G;
     E.nslices = (E.ngroups + gpw - 1) / gpw;
@@ -320,6 +348,24 @@ int build_ell(gbn_ctx* c, int prec, int G, int gpw)
     GBN_CK(c, cudaMemcpyAsync(&nnz, off.as<int64_t>() + n, sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream));
     GBN_CK(c, cudaStreamSynchronize(c->stream));
     GBN_CK(c, keys.ensure(sizeof(uint64_t) * (size_t)(nnz > 0 ? nnz : 1)));
+    if (field && nnz > 0) {   // every (row, column) at most once
+        DevBuf roff;
+        GBN_CK(c, roff.ensure(sizeof(int64_t) * (n + 1)));
+        GBN_CK(c, cudaMemsetAsync(roff.as<int64_t>() + n, 0, sizeof(int64_t), c->stream));
+        thrust::device_ptr<const int32_t> np(nn);
+        thrust::device_ptr<int64_t> rp(roff.as<int64_t>());
+        thrust::transform(pol, np, np + n, rp, [] __device__(int32_t v) { return (int64_t)v; });
+        thrust::exclusive_scan(pol, rp, rp + n + 1, rp);
+        k_row_keys<<<grn, 256, 0, c->stream>>>(nn, nl, n, c->max_neigh, roff.as<int64_t>(), keys.as<uint64_t>());
+        GBN_CK_LAUNCH(c);
+        thrust::device_ptr<uint64_t> kq(keys.as<uint64_t>());
+        thrust::sort(pol, kq, kq + nnz);
+        const int64_t nuniq = thrust::unique(pol, kq, kq + nnz) - kq;
+        c->launches += 6;
+        if (nuniq != nnz)
+            return fail(c, GBN_ERR_ARG, "a row holds two periodic images of one neighbour: the cell is too small for "
+                                        "batched fields (use gbn_peierls per field)");
+    }
     k_group_keys<<<grn, 256, 0, c->stream>>>(nn, nl, c->perm.as<int32_t>(), n, c->max_neigh, G, off.as<int64_t>(),
                                              keys.as<uint64_t>());
     GBN_CK_LAUNCH(c);
@@ -367,7 +413,8 @@ int build_ell(gbn_ctx* c, int prec, int G, int gpw)
     GBN_CK(c, cudaStreamSynchronize(c->stream));
 
     size_t vsz;
-    if (prec == GBN_MIXED) vsz = E.cplx ? sizeof(float2) : sizeof(float);
+    if (field) vsz = prec == GBN_MIXED ? sizeof(FieldVal<float>) : sizeof(FieldVal<double>);
+    else if (prec == GBN_MIXED) vsz = E.cplx ? sizeof(float2) : sizeof(float);
     else vsz = E.cplx ? sizeof(double2) : sizeof(double);
     const size_t eb = sizeof(int32_t) + vsz * G;
     const size_t ne = (size_t)(E.nnz_stored > 0 ? E.nnz_stored : 1);
@@ -382,7 +429,18 @@ int build_ell(gbn_ctx* c, int prec, int G, int gpw)
                                                       gorder.as<int32_t>(), ucount.as<int32_t>(), ustart.as<int64_t>(), \
                                                       keys.as<uint64_t>(), n, c->max_neigh, G, gpw, E.ngroups,         \
                                                       E.nslices, sp, E.mat.as<unsigned char>(), E.h0.as<DV>())
-    if (prec == GBN_MIXED) {
+    if (field) {
+        if (prec == GBN_MIXED)
+            k_fill_groups<FieldVal<float>, float, true><<<grg, 128, 0, c->stream>>>(
+                nn, nl, hp, h0, E.rperm.as<int32_t>(), E.riperm.as<int32_t>(), gorder.as<int32_t>(), ucount.as<int32_t>(),
+                ustart.as<int64_t>(), keys.as<uint64_t>(), n, c->max_neigh, G, gpw, E.ngroups, E.nslices, sp,
+                E.mat.as<unsigned char>(), E.h0.as<float>(), c->ptau.as<uint64_t>());
+        else
+            k_fill_groups<FieldVal<double>, double, true><<<grg, 128, 0, c->stream>>>(
+                nn, nl, hp, h0, E.rperm.as<int32_t>(), E.riperm.as<int32_t>(), gorder.as<int32_t>(), ucount.as<int32_t>(),
+                ustart.as<int64_t>(), keys.as<uint64_t>(), n, c->max_neigh, G, gpw, E.ngroups, E.nslices, sp,
+                E.mat.as<unsigned char>(), E.h0.as<double>(), c->ptau.as<uint64_t>());
+    } else if (prec == GBN_MIXED) {
         if (E.cplx) GBN_FILL(float2, float);
         else GBN_FILL(float, float);
     } else {

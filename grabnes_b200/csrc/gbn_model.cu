@@ -219,6 +219,52 @@ __global__ void k_peierls(int64_t n, const double* rat, double u0, double u1, do
     }
 }
 
+// The phase of k_peierls per flux quantum as a fraction of a turn, in 64-bit fixed point: for m quanta
+// the phase is m * pi [(r_i x r_j + (r_i + r_j) x T) / A + n1 n2] (flux = m pi 1e20 / A), i.e. m turns
+// times (r_i x r_j + (r_i + r_j) x T) / (2 A) + n1 n2 / 2, taken modulo one turn.
+__global__ void k_peierls_turns(int64_t n, const double* rat, double u0, double u1, double u3, double u4,
+                                double area, int32_t max_neigh, const int32_t* nneigh, const int32_t* nlist,
+                                const int32_t* ncell, uint64_t* tau)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double rix = rat[3 * i], riy = rat[3 * i + 1];
+    for (int j = 0; j < nneigh[i]; ++j) {
+        const int64_t e = i * max_neigh + j;
+        const int64_t jj = nlist[e] - 1;
+        const double rjx = rat[3 * jj], rjy = rat[3 * jj + 1];
+        const int n1 = ncell[3 * e], n2 = ncell[3 * e + 1];
+        const double v1x = rix + rjx, v1y = riy + rjy;
+        const double v2x = (double)n1 * u0 + (double)n2 * u3, v2y = (double)n1 * u1 + (double)n2 * u4;
+        const double c3 = v1x * v2y - v1y * v2x;
+        const double r3 = rix * rjy - riy * rjx;
+        double t = (r3 + c3) / (2.0 * area);
+        t -= floor(t);
+        if (n1 != 0 && n2 != 0 && (((long long)n1 * (long long)n2) & 1LL)) t += 0.5;
+        if (t >= 1.0) t -= 1.0;
+        // t * 2^64 in [0, 2^64): the high and the low 32 bits separately (exact for t's 53 bits)
+        const double hi = floor(t * 4294967296.0);
+        const double lo = (t * 4294967296.0 - hi) * 4294967296.0;
+        uint64_t q = ((uint64_t)hi << 32) + (uint64_t)llrint(lo);
+        tau[e] = q;
+    }
+}
+
+int peierls_turns(gbn_ctx* c)
+{
+    if (!c->rat_hop.p || !c->ncell.p) return fail(c, GBN_ERR_STATE, "batched fields need the device geometry and neighbour search");
+    const double* u = c->ucell;
+    const double area = fabs(u[0] * u[4] - u[1] * u[3]);
+    GBN_CK(c, c->ptau.ensure(sizeof(uint64_t) * (size_t)c->n * c->max_neigh));
+    GBN_CK(c, cudaMemsetAsync(c->ptau.p, 0, sizeof(uint64_t) * (size_t)c->n * c->max_neigh, c->stream));
+    const unsigned grd = (unsigned)((c->n + 127) / 128);
+    k_peierls_turns<<<grd, 128, 0, c->stream>>>(c->n, c->rat_hop.as<double>(), u[0], u[1], u[3], u[4], area,
+                                                c->max_neigh, c->nneigh.as<int32_t>(), c->nlist.as<int32_t>(),
+                                                c->ncell.as<int32_t>(), c->ptau.as<uint64_t>());
+    GBN_CK_LAUNCH(c);
+    return GBN_OK;
+}
+
 int assemble(gbn_ctx* c, const gbn_model* m, const double* d_rat_on, const double* d_rat_hop, const double* d_uniform)
 {
     const int64_t n = c->n;
@@ -234,6 +280,7 @@ int assemble(gbn_ctx* c, const gbn_model* m, const double* d_rat_on, const doubl
     GBN_CK_LAUNCH(c);
     c->have_ham = true;
     c->ham_complex = false;
+    c->has_field = false;
     c->ell.valid = false;
     return GBN_OK;
 }
@@ -253,6 +300,7 @@ int peierls(gbn_ctx* c, double flux)
     GBN_CK_LAUNCH(c);
     GBN_CK(c, cudaStreamSynchronize(c->stream));
     c->ham_complex = true;
+    c->has_field = true;
     c->ell.valid = false;
     return GBN_OK;
 }

@@ -83,6 +83,36 @@ template <typename VT> struct Hop<VT, true> {
     }
 };
 
+// Values of the field-batched layout: the field-free (negated) hopping h and the Peierls phase per flux
+// quantum t as a fixed-point fraction of a turn (2^-32 turn resolution in FP32, 2^-64 in FP64).  For m
+// flux quanta the entry is h * exp(2 pi i frac(m t)); the product m t wraps exactly in integer arithmetic.
+template <typename VT> struct FieldVal;
+template <> struct FieldVal<float> { float h; uint32_t t; };
+template <> struct FieldVal<double> { double h; uint64_t t; };
+
+// h exp(i 2 pi u / 2^32): the top 16 bits of the turn fraction u by sincospif (exact argument), the low
+// bits by the second-order expansion of exp(i pi s_lo), |pi s_lo| < 1e-4 (error below 2e-13)
+__device__ __forceinline__ float2 field_rotate(FieldVal<float> v, uint32_t m)
+{
+    const uint32_t u = v.t * m;
+    const float s_hi = (float)(int32_t)(u & 0xffff0000u) * 4.656612873077393e-10f;   // 2^-31
+    const float s_lo = (float)(u & 0xffffu) * 4.656612873077393e-10f;
+    float sn, cs;
+    sincospif(s_hi, &sn, &cs);
+    const float e = 3.14159265358979f * s_lo;
+    const float er = fmaf(-0.5f * e, e, 1.0f);   // cos(e)
+    const float ei = e;                          // sin(e)
+    const float c2 = cs * er - sn * ei, s2 = sn * er + cs * ei;
+    return make_float2(v.h * c2, v.h * s2);
+}
+__device__ __forceinline__ double2 field_rotate(FieldVal<double> v, uint64_t m)
+{
+    const uint64_t u = v.t * m;
+    double sn, cs;
+    sincospi((double)(int64_t)u * 1.0842021724855044e-19, &sn, &cs);   // 2^-63
+    return make_double2(v.h * cs, v.h * sn);
+}
+
 // G consecutive values of one union column (G * sizeof(HT) = 4..64 bytes, naturally aligned), read
 // with the widest loads: from global memory once and evicted first (the matrix is streamed every
 // step), or from shared memory
@@ -117,14 +147,23 @@ __device__ __forceinline__ void load_group_vals(const HT* p, HT (&h)[G])
 // index and the G values (same address for the group's threads) and gathers RPT vector elements of that
 // column once for all G rows.  cp/vp point at the thread's group in the slice record, in global memory
 // (streamed, evict-first) or in shared memory (SMEM); w is the slice width (a multiple of 4).
-template <typename VT, bool CPLX, int G, int RPT, int TPR, bool SMEM>
+// FIELD: the values are FieldVal<VT> and every thread rotates them by its right-hand sides' field mf
+// (mf flux quanta, the same for the thread's RPT right-hand sides) before the complex products.
+template <typename VT, bool CPLX, bool FIELD> struct StoredVal { using t = typename Hop<VT, CPLX>::t; };
+template <typename VT, bool CPLX> struct StoredVal<VT, CPLX, true> { using t = FieldVal<VT>; };
+template <typename VT> struct FieldMult;
+template <> struct FieldMult<float> { using t = uint32_t; };
+template <> struct FieldMult<double> { using t = uint64_t; };
+
+template <typename VT, bool CPLX, int G, int RPT, int TPR, bool SMEM, bool FIELD = false>
 __device__ __forceinline__ void group_columns(const typename V2<VT>::t* __restrict__ x, int w,
                                               const int32_t* __restrict__ cp,
-                                              const typename Hop<VT, CPLX>::t* __restrict__ vp,
-                                              typename V2<VT>::t (&acc)[G][RPT])
+                                              const typename StoredVal<VT, CPLX, FIELD>::t* __restrict__ vp,
+                                              typename V2<VT>::t (&acc)[G][RPT],
+                                              typename FieldMult<VT>::t mf = 0)
 {
     using C2 = typename V2<VT>::t;
-    using HT = typename Hop<VT, CPLX>::t;
+    using HT = typename StoredVal<VT, CPLX, FIELD>::t;
     constexpr int GPW = 32 / TPR;
     constexpr int R = RPT * TPR;
     constexpr int U = kColUnroll;
@@ -146,12 +185,23 @@ __device__ __forceinline__ void group_columns(const typename V2<VT>::t* __restri
         }
 #pragma unroll
         for (int u = 0; u < U; ++u) VecIO<VT, RPT>::load(xq + (size_t)(uint32_t)c[u] * R, xg[u]);
+        if constexpr (FIELD) {
 #pragma unroll
-        for (int u = 0; u < U; ++u)
+            for (int u = 0; u < U; ++u)
 #pragma unroll
-            for (int g = 0; g < G; ++g)
+                for (int g = 0; g < G; ++g) {
+                    const C2 hr = field_rotate(h[u][g], mf);
 #pragma unroll
-                for (int t = 0; t < RPT; ++t) Hop<VT, CPLX>::madd(acc[g][t], h[u][g], xg[u][t]);
+                    for (int t = 0; t < RPT; ++t) Hop<VT, true>::madd(acc[g][t], hr, xg[u][t]);
+                }
+        } else {
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+#pragma unroll
+                for (int g = 0; g < G; ++g)
+#pragma unroll
+                    for (int t = 0; t < RPT; ++t) Hop<VT, CPLX>::madd(acc[g][t], h[u][g], xg[u][t]);
+        }
         cp += U * GPW;
         vp += U * GPW * G;
     }

@@ -1,0 +1,200 @@
+// The per-step pieces of the recursion's sparse product shared by its kernels (gbn_lanczos.cu: matrix
+// records from global or shared memory; gbn_fields.cu: many fields from one field-free matrix): the
+// launch parameters, the slice loop body with its FP64 epilogue, and the fixed-order reduction of the
+// four dot products that writes a_k, b_k.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include "gbn_spmm.cuh"
+
+namespace gbn {
+
+struct StepParams {
+    const int64_t* slice_ptr;
+    const unsigned char* mat;  // slice records (column indices, then G values per union column)
+    int64_t entry_bytes;       // 4 + G * value bytes
+    int64_t cap_record;        // bytes of a staging buffer (larger records are read in place)
+    int32_t prefetch;          // staged kernel: prefetch the gather rows of a slice (1 L2, 2 L1)
+    const void* h0;
+    const void* x_cur;   // x_k   [npad][R] (gathered)
+    const void* x_prev;  // x_{k-1}
+    void* v_out;         // v_{k+1}
+    double* scal;        // [R][2] a_{k-1}, b_{k-1}
+    double* partials;    // [gridDim][R][4]
+    unsigned int* counter;  // [0] block counter, [1] step index, [2] error flag
+    double* a_out;       // [R][nmax]
+    double* b_out;
+    int64_t nslices;
+    int32_t nmax;
+    const int32_t* field_m;  // field-batched layout: flux quanta of each right-hand side [R] (else unused)
+};
+
+using StepFn = void (*)(StepParams);
+// the sparse-product kernel of the field-batched layout (gbn_fields.cu)
+StepFn field_step_kernel(int prec, int G, int rpt, int tpr);
+
+struct SliceSums {
+    double s1, s2, s3, s4;
+};
+
+// Reduction of the four sums over the block, then by the last block over all blocks; writes a_k, b_k.
+// Needs at least 4 R threads per block.
+template <int RPT, int TPR>
+__device__ __forceinline__ void reduce_and_finalize(const StepParams& p, SliceSums* acc_s)
+{
+    constexpr int R = RPT * TPR;
+    const int lane = threadIdx.x & 31;
+    const int sub = lane / TPR;
+    const int q = lane % TPR;
+#pragma unroll
+    for (int t = 0; t < RPT; ++t) {
+#pragma unroll
+        for (int off = TPR; off < 32; off <<= 1) {
+            acc_s[t].s1 += __shfl_xor_sync(0xffffffffu, acc_s[t].s1, off);
+            acc_s[t].s2 += __shfl_xor_sync(0xffffffffu, acc_s[t].s2, off);
+            acc_s[t].s3 += __shfl_xor_sync(0xffffffffu, acc_s[t].s3, off);
+            acc_s[t].s4 += __shfl_xor_sync(0xffffffffu, acc_s[t].s4, off);
+        }
+    }
+    __shared__ double red[8][R][4];
+    const int wib = threadIdx.x >> 5;
+    if (sub == 0) {
+#pragma unroll
+        for (int t = 0; t < RPT; ++t) {
+            const int r = q * RPT + t;
+            red[wib][r][0] = acc_s[t].s1; red[wib][r][1] = acc_s[t].s2;
+            red[wib][r][2] = acc_s[t].s3; red[wib][r][3] = acc_s[t].s4;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < R * 4) {
+        const int r = threadIdx.x >> 2, k = threadIdx.x & 3;
+        double a = 0.0;
+        for (int wI = 0; wI < (int)(blockDim.x >> 5); ++wI) a += red[wI][r][k];
+        p.partials[((int64_t)blockIdx.x * R + r) * 4 + k] = a;
+    }
+    // the last block to finish reduces all blocks in a fixed order
+    __shared__ bool last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = (atomicAdd(p.counter, 1u) == gridDim.x - 1);
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    __shared__ double tot[R][4];
+    if (threadIdx.x < R * 4) {
+        const int r = threadIdx.x >> 2, k = threadIdx.x & 3;
+        double a = 0.0;
+        for (unsigned int bI = 0; bI < gridDim.x; ++bI) a += __ldcg(&p.partials[((int64_t)bI * R + r) * 4 + k]);
+        tot[r][k] = a;
+    }
+    __syncthreads();
+    if (threadIdx.x < R) {
+        const int r = threadIdx.x;
+        const unsigned int step = p.counter[1];
+        const double a = tot[r][0];
+        const double b2 = tot[r][1] - 2.0 * a * tot[r][2] + a * a * tot[r][3];
+        const double b = sqrt(fabs(b2));
+        if (!(b > 0.0) || !isfinite(a) || !isfinite(b)) atomicOr(&p.counter[2], 1u);
+        if ((int)step < p.nmax) {
+            p.a_out[(int64_t)r * p.nmax + step] = a;
+            p.b_out[(int64_t)r * p.nmax + step] = b;
+        }
+        p.scal[2 * r] = a;
+        p.scal[2 * r + 1] = b;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        p.counter[0] = 0u;
+        p.counter[1] = p.counter[1] + 1u;
+    }
+}
+
+// One slice of the grouped sliced ELL: GPW = 32/TPR groups; the TPR threads of a group each hold RPT
+// right-hand sides of all G rows of the group.  Per union column a thread reads the column index and
+// the G values (same address for the group's threads) and gathers RPT vector elements of that column
+// once for all G rows.  The epilogue per row adds the on-site term and is FP64 from there:
+// v_{k+1} = y - b_{k-1} x_{k-1} rounded once, and the four dot-product terms.  cp/vp point at the
+// thread's group in the slice record, in global memory (streamed) or in shared memory (SMEM).
+// FIELD: field-batched values (FieldVal), the thread's field is that of its first right-hand side.
+template <typename VT, bool CPLX, int G, int RPT, int TPR, bool SMEM, bool FIELD = false>
+__device__ __forceinline__ void group_slice(const StepParams& p, int64_t s, int w, const int32_t* __restrict__ cp,
+                                            const typename StoredVal<VT, CPLX, FIELD>::t* __restrict__ vp,
+                                            const double* cb, SliceSums* acc_s)
+{
+    using C2 = typename V2<VT>::t;
+    constexpr int GPW = 32 / TPR;
+    constexpr int R = RPT * TPR;
+    const int lane = threadIdx.x & 31;
+    const int sub = lane / TPR;
+    const int q = lane % TPR;
+    const C2* __restrict__ xc = static_cast<const C2*>(p.x_cur);
+    const C2* __restrict__ xp = static_cast<const C2*>(p.x_prev);
+    C2* __restrict__ vout = static_cast<C2*>(p.v_out);
+    const VT* __restrict__ h0 = static_cast<const VT*>(p.h0);
+    const int64_t row0 = (s * GPW + sub) * G;
+    C2 acc[G][RPT];
+    typename FieldMult<VT>::t mf = 0;
+    if constexpr (FIELD) mf = (typename FieldMult<VT>::t)(int64_t)p.field_m[q * RPT];
+    group_columns<VT, CPLX, G, RPT, TPR, SMEM, FIELD>(xc, w, cp, vp, acc, mf);
+    // epilogue per row: the on-site term (own x_k row, loaded here so that it holds no registers during
+    // the column loop), then v_{k+1} and the dot-product terms in FP64
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+        C2 xo[RPT], xm[RPT], vn[RPT];
+        VecIO<VT, RPT>::load(xc + (row0 + g) * R + q * RPT, xo);
+        VecIO<VT, RPT>::load(xp + (row0 + g) * R + q * RPT, xm);
+        const VT d = h0[row0 + g];
+#pragma unroll
+        for (int t = 0; t < RPT; ++t) {
+            acc[g][t].x = fma(d, xo[t].x, acc[g][t].x);
+            acc[g][t].y = fma(d, xo[t].y, acc[g][t].y);
+            vn[t].x = (VT)((double)acc[g][t].x - cb[t] * (double)xm[t].x);
+            vn[t].y = (VT)((double)acc[g][t].y - cb[t] * (double)xm[t].y);
+            const double xr = xo[t].x, xi = xo[t].y, yr = acc[g][t].x, yi = acc[g][t].y;
+            const double vr = vn[t].x, vi = vn[t].y;
+            acc_s[t].s1 += xr * yr + xi * yi;
+            acc_s[t].s2 += vr * vr + vi * vi;
+            acc_s[t].s3 += xr * vr + xi * vi;
+            acc_s[t].s4 += xr * xr + xi * xi;
+        }
+        VecIO<VT, RPT>::store(vout + (row0 + g) * R + q * RPT, vn);
+    }
+}
+
+// Matrix records read from global memory.  Every block owns a contiguous range of slices (a compact
+// region of the row order); its warps take neighbouring slices, so the rows they gather overlap in L1.
+// FIELD: the field-batched layout (values FieldVal<VT>, fields p.field_m).
+template <typename VT, bool CPLX, int G, int RPT, int TPR, bool FIELD = false>
+__global__ void __launch_bounds__(256) k_spmm_step(StepParams p)
+{
+    using HT = typename StoredVal<VT, CPLX, FIELD>::t;
+    constexpr int GPW = 32 / TPR;
+    const int q = (threadIdx.x & 31) % TPR;
+    const int sub = (threadIdx.x & 31) / TPR;
+    double cb[RPT];
+    SliceSums acc_s[RPT];
+#pragma unroll
+    for (int t = 0; t < RPT; ++t) {
+        cb[t] = p.scal[2 * (q * RPT + t) + 1];
+        acc_s[t] = SliceSums{0.0, 0.0, 0.0, 0.0};
+    }
+    const int nwb = (int)(blockDim.x >> 5);
+    const int64_t per = (p.nslices + gridDim.x - 1) / gridDim.x;
+    const int64_t s0 = (int64_t)blockIdx.x * per;
+    const int64_t s1e = (s0 + per < p.nslices) ? s0 + per : p.nslices;
+    for (int64_t s = s0 + (threadIdx.x >> 5); s < s1e; s += nwb) {
+        const int64_t base = p.slice_ptr[s];
+        const int w = (int)((p.slice_ptr[s + 1] - base) / GPW);
+        const unsigned char* rec = p.mat + base * p.entry_bytes;
+        group_slice<VT, CPLX, G, RPT, TPR, false, FIELD>(p, s, w, reinterpret_cast<const int32_t*>(rec) + sub,
+                                                  reinterpret_cast<const HT*>(rec + (size_t)w * GPW * 4) + sub * G,
+                                                  cb, acc_s);
+    }
+    reduce_and_finalize<RPT, TPR>(p, acc_s);
+}
+
+}  // namespace gbn

@@ -159,6 +159,15 @@ int gbn_lanczos(gbn_ctx* ctx, int32_t precision, int32_t nrhs, const double* psi
  * u[nrhs][N]: psi_i = exp(2 pi i u_i)/sqrt(N) (KuboInitWF, kubo.F90:61-64). */
 int gbn_lanczos_phases(gbn_ctx* ctx, int32_t precision, int32_t nrhs, const double* u,
                        const int32_t* nsteps, int32_t nmax, double* a, double* b);
+/* Many perpendicular fields in one batch (the MagField sweep of magf.F90:100-146 with KuboInitWF +
+ * KuboRecursion per field): field f has m[f] flux quanta through the cell and nvec random-phase start
+ * vectors, u[f][v][N] their uniform draws as for gbn_lanczos_phases; nsteps[f][v] (or NULL = nmax) their
+ * recursion lengths; a, b: [f][v][nmax].  The hoppings must come from gbn_assemble without gbn_peierls:
+ * the entries keep the field-free hopping and the Peierls phase per flux quantum, and each field's phase
+ * is applied on the fly, so that one matrix serves all fields.  Vectors of similar length share tiles.
+ * A cell so small that a row holds two periodic images of one neighbour is rejected (GBN_ERR_ARG). */
+int gbn_lanczos_fields(gbn_ctx* ctx, int32_t precision, int32_t nfields, const int32_t* m, int32_t nvec,
+                       const double* u, const int32_t* nsteps, int32_t nmax, double* a, double* b);
 /* Local DOS of single atoms (KuboInitWFPDOS, kubo.F90:87-138): start vector r is the unit vector
  * on atom sites[r] (1-based), built on the device; all sites run as one batch of right-hand sides. */
 int gbn_lanczos_sites(gbn_ctx* ctx, int32_t precision, int32_t nsites, const int64_t* sites,

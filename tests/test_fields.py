@@ -1,0 +1,108 @@
+"""Many fields in one batch (gbn_lanczos_fields): the Peierls phase of every entry applied on the fly
+from one field-free matrix, against the oracle's per-field Hamiltonian (HamPeierlsPeriodicGauge for each
+field) and recursion."""
+import numpy as np
+import pytest
+
+import refcases as R
+from oracle import oracle as orc
+
+pytestmark = pytest.mark.gpu
+
+G = pytest.importorskip("grabnes_b200")
+
+MOIRE = dict(TypeOfSystem="Graphene", CellSize=11, SuperCell=8, LatticePercent=-1.0 / 11.0, MoirePotential=True,
+             MoireJeil=True, MoireH0AndHZ=True, MoireOffDiag=True, MoireOffDiagMidpoint=True)
+FIELDS = [0, 2, 5, -3, 16]
+NVEC = 4
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    with G.Context(0) as c:
+        yield c
+
+
+@pytest.fixture(scope="module")
+def base():
+    return R.build(MOIRE)
+
+
+def _field_free(ctx, r):
+    geo = r["geo"]
+    ctx.set_geometry(geo["rat"], geo["species"], geo["layer"], geo["ucell"])
+    ctx.neighbours(r["cut2intra"], r["cut2inter"], r["second_layer"], tables=False)
+    ctx.assemble(R.gpu_model(r["model"]), r["rat_on"], r["rat_hop"], None)
+
+
+def _draws(n):
+    return np.stack([np.stack([orc.rng_draws(1000 + 10 * f + v, n) for v in range(NVEC)]) for f in range(len(FIELDS))])
+
+
+def _close(a, b, a0, b0, tol):
+    scale = max(np.abs(a0).max(), np.abs(b0).max())
+    return np.abs(a - a0).max() <= tol * scale and np.abs(b - b0).max() <= tol * scale
+
+
+def test_fields_fp64_match_per_field_oracle(ctx, base):
+    """FP64, uneven lengths: every vector of every field within 1e-10 of the oracle's recursion on that
+    field's Hamiltonian."""
+    n = base["geo"]["n"]
+    u = _draws(n)
+    ns = np.random.default_rng(5).integers(60, 121, (len(FIELDS), NVEC)).astype(np.int32)
+    _field_free(ctx, base)
+    a, b = ctx.lanczos_fields(FIELDS, u, ns, G.GBN_FP64)
+    for f, m in enumerate(FIELDS):
+        r = R.build(dict(MOIRE, MagFieldInteger=m)) if m else base
+        for v in range(NVEC):
+            psi = np.exp(2j * np.pi * u[f, v]) / np.sqrt(n)
+            k = int(ns[f, v])
+            a0, b0 = orc.recursion(r["nb"], r["hop"], r["h0"], psi, k, 0)
+            assert _close(a[f, v, :k], b[f, v, :k], a0, b0, 1e-10), (m, v)
+
+
+def test_fields_mixed_dos(ctx, base):
+    """Mixed precision (FP32 vectors and field-free hoppings, phases from 32-bit turn fractions): the DOS
+    of each field against the FP64 oracle's, and against the per-field mixed path (gbn_peierls)."""
+    n, g0 = base["geo"]["n"], base["g0"]
+    u = _draws(n)
+    _field_free(ctx, base)
+    a, b = ctx.lanczos_fields(FIELDS, u, 120, G.GBN_MIXED)
+    eta, ne, lo, hi = 0.02 / g0, 600, -0.6 / g0, 0.6 / g0
+    for f, m in enumerate(FIELDS):
+        r = R.build(dict(MOIRE, MagFieldInteger=m)) if m else base
+        d_ref = 0.0
+        d_mix = 0.0
+        d_fld = 0.0
+        _field_free(ctx, base)
+        if m:
+            ctx.peierls(r["flux"])
+        ap, bp = ctx.lanczos_phases(u[f], 120, G.GBN_MIXED)
+        for v in range(NVEC):
+            psi = np.exp(2j * np.pi * u[f, v]) / np.sqrt(n)
+            a0, b0 = orc.recursion(r["nb"], r["hop"], r["h0"], psi, 120, 0)
+            d_ref = d_ref + orc.frac(a0, b0, eta, ne, lo, hi)[1]
+            d_fld = d_fld + orc.frac(a[f, v], b[f, v], eta, ne, lo, hi)[1]
+            d_mix = d_mix + orc.frac(ap[v], bp[v], eta, ne, lo, hi)[1]
+        err_fld = np.abs(d_fld - d_ref).sum() / np.abs(d_ref).sum()
+        err_mix = np.abs(d_mix - d_ref).sum() / np.abs(d_ref).sum()
+        assert err_fld <= 1e-6, (m, err_fld, err_mix)
+
+
+def test_fields_reject_a_field_already_applied(ctx, base):
+    _field_free(ctx, base)
+    ctx.peierls(R.build(dict(MOIRE, MagFieldInteger=2))["flux"])
+    u = _draws(base["geo"]["n"])
+    with pytest.raises(G.GbnError):
+        ctx.lanczos_fields(FIELDS, u, 20, G.GBN_FP64)
+
+
+def test_fields_reject_repeated_images():
+    """A 4x4 graphene cell with third neighbours: a row meets periodic images of one atom twice."""
+    r = R.build(dict(TypeOfSystem="Graphene", CellSize=2, NeighLevels=3))
+    n = r["geo"]["n"]
+    assert any(len(set(row[:k])) < k for row, k in zip(r["nb"]["nlist"], r["nb"]["nneigh"]))
+    with G.Context(0) as c:
+        _field_free(c, r)
+        with pytest.raises(G.GbnError):
+            c.lanczos_fields([1, 2], np.zeros((2, 1, n)), 5, G.GBN_FP64)
