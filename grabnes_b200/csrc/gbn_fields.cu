@@ -9,10 +9,10 @@
 namespace gbn {
 
 template <typename VT, int G>
-static StepFn pick_field_g(int rpt, int tpr)
+static StepFn pick_field_g(int rpt, int tpr, bool staged)
 {
 #define GBN_CASE(RP, TP) \
-    if (rpt == RP && tpr == TP) return k_spmm_step<VT, false, G, RP, TP, true>;
+    if (rpt == RP && tpr == TP) return staged ? k_spmm_staged<VT, false, G, RP, TP, true> : k_spmm_step<VT, false, G, RP, TP, true>;
     GBN_CASE(1, 1) GBN_CASE(1, 2) GBN_CASE(1, 4) GBN_CASE(1, 8) GBN_CASE(1, 16) GBN_CASE(1, 32)
     GBN_CASE(2, 1) GBN_CASE(2, 2) GBN_CASE(2, 4) GBN_CASE(2, 8) GBN_CASE(2, 16)
     if constexpr (sizeof(VT) == 4) {
@@ -22,16 +22,16 @@ static StepFn pick_field_g(int rpt, int tpr)
     return nullptr;
 }
 
-StepFn field_step_kernel(int prec, int G, int rpt, int tpr)
+StepFn field_step_kernel(int prec, int G, int rpt, int tpr, bool staged)
 {
     if (prec == GBN_MIXED) {
-        if (G == 1) return pick_field_g<float, 1>(rpt, tpr);
-        if (G == 2) return pick_field_g<float, 2>(rpt, tpr);
-        if (G == 4) return pick_field_g<float, 4>(rpt, tpr);
+        if (G == 1) return pick_field_g<float, 1>(rpt, tpr, staged);
+        if (G == 2) return pick_field_g<float, 2>(rpt, tpr, staged);
+        if (G == 4) return pick_field_g<float, 4>(rpt, tpr, staged);
     } else {
-        if (G == 1) return pick_field_g<double, 1>(rpt, tpr);
-        if (G == 2) return pick_field_g<double, 2>(rpt, tpr);
-        if (G == 4) return pick_field_g<double, 4>(rpt, tpr);
+        if (G == 1) return pick_field_g<double, 1>(rpt, tpr, staged);
+        if (G == 2) return pick_field_g<double, 2>(rpt, tpr, staged);
+        if (G == 4) return pick_field_g<double, 4>(rpt, tpr, staged);
     }
     return nullptr;
 }

@@ -49,170 +49,6 @@ __global__ void __launch_bounds__(256) k_update(const typename V2<VT>::t* __rest
 }
 
 // ---------------------------------------------------------------------------- sparse product
-// ---- bulk asynchronous copies (cp.async.bulk, the TMA engine) into shared memory, mbarrier completion
-__device__ __forceinline__ uint32_t smem_u32(const void* ptr) { return (uint32_t)__cvta_generic_to_shared(ptr); }
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes)
-{
-    uint64_t state;
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 %0, [%1], %2;"
-                 : "=l"(state) : "r"(smem_u32(bar)), "r"(bytes) : "memory");
-    (void)state;
-}
-
-// global -> shared copy of `bytes` (multiple of 16, both addresses 16-byte aligned), no multicast
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
-{
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
-                 ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar)) : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
-{
-    uint32_t done;
-    asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
-                 : "=r"(done) : "r"(smem_u32(bar)), "r"(parity) : "memory");
-    return done != 0;
-}
-
-__device__ __forceinline__ uint64_t global_ns()
-{
-    uint64_t t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-
-// bounded wait: gives up after about one second (the caller records the failure)
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity)
-{
-    if (mbar_try_wait(bar, parity)) return true;
-    const uint64_t t0 = global_ns();
-    while (!mbar_try_wait(bar, parity))
-        if (global_ns() - t0 > 1000000000ull) return false;
-    return true;
-}
-
-// Prefetch of the vector rows that the columns of a staged record will gather (x_k rows of R
-// complex values, 128-byte lines), spread over the warp's lanes.  Prefetches do not block and hold
-// no registers.
-template <typename VT, int R>
-__device__ __forceinline__ void prefetch_rows(const StepParams& p, const int32_t* cols, int ncols)
-{
-    constexpr int ROWB = R * (int)sizeof(typename V2<VT>::t);
-    const char* x = static_cast<const char*>(p.x_cur);
-    const int lane = threadIdx.x & 31;
-    for (int i = lane; i < ncols; i += 32) {
-        const char* a = x + (size_t)(uint32_t)cols[i] * ROWB;
-#pragma unroll
-        for (int off = 0; off < ROWB; off += 128) {
-            if (p.prefetch == 2) asm volatile("prefetch.global.L1 [%0];" ::"l"(a + off));
-            else asm volatile("prefetch.global.L2 [%0];" ::"l"(a + off));
-        }
-    }
-}
-
-// Matrix records staged in shared memory.  Each warp owns two record buffers and an mbarrier per
-// buffer; its lane 0 copies the record of the warp's next-but-one slice with one bulk copy while the
-// warp works on the current one, so the column indices that the gathers depend on come from shared
-// memory instead of a DRAM round trip per unrolled column batch.  Optionally the warp first
-// prefetches all the vector rows a slice will gather.  Records larger than a buffer (the largest
-// 0.5 %) are read in place.  No block-wide synchronisation in the loop; every wait is bounded (flag
-// bit 2, GBN_ERR_TIMEOUT).
-template <typename VT, bool CPLX, int G, int RPT, int TPR>
-__global__ void __launch_bounds__(256) k_spmm_staged(StepParams p)
-{
-    using HT = typename Hop<VT, CPLX>::t;
-    constexpr int GPW = 32 / TPR;
-    constexpr int R = RPT * TPR;
-    extern __shared__ __align__(128) unsigned char dyn[];
-    const int lane = threadIdx.x & 31;
-    const int wib = threadIdx.x >> 5;
-    const int q = lane % TPR;
-    const int sub = lane / TPR;
-    uint64_t* bar = reinterpret_cast<uint64_t*>(dyn) + 2 * wib;
-    unsigned char* buf = dyn + 128 + (size_t)wib * 2 * p.cap_record;
-    double cb[RPT];
-    SliceSums acc_s[RPT];
-#pragma unroll
-    for (int t = 0; t < RPT; ++t) {
-        cb[t] = p.scal[2 * (q * RPT + t) + 1];
-        acc_s[t] = SliceSums{0.0, 0.0, 0.0, 0.0};
-    }
-    const int nwb = (int)(blockDim.x >> 5);
-    const int64_t per = (p.nslices + gridDim.x - 1) / gridDim.x;
-    const int64_t s0 = (int64_t)blockIdx.x * per;
-    const int64_t s1e = (s0 + per < p.nslices) ? s0 + per : p.nslices;
-    const int64_t eb = p.entry_bytes;
-
-    auto rec_bytes = [&](int64_t s) { return (p.slice_ptr[s + 1] - p.slice_ptr[s]) * eb; };
-    auto issue = [&](int64_t s, int st) {   // lane 0 only; records above the cap are not copied
-        const int64_t bytes = rec_bytes(s);
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        const bool copy = bytes > 0 && bytes <= p.cap_record;
-        mbar_expect_tx(&bar[st], copy ? (uint32_t)bytes : 0u);
-        if (copy) bulk_g2s(buf + st * p.cap_record, p.mat + p.slice_ptr[s] * eb, (uint32_t)bytes, &bar[st]);
-    };
-
-    if (lane == 0) {
-        mbar_init(&bar[0], 1);
-        mbar_init(&bar[1], 1);
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    __syncwarp();
-    int64_t s = s0 + wib;
-    uint32_t pending = (s < s1e ? 1u : 0u) | (s + nwb < s1e ? 2u : 0u);   // bit st: a copy into buffer st
-    if (lane == 0) {
-        if (pending & 1u) issue(s, 0);
-        if (pending & 2u) issue(s + nwb, 1);
-    }
-    uint32_t phase = 0u;   // bit st: parity of buffer st's next phase
-    bool ok = true;
-    for (int it = 0; s < s1e; s += nwb, ++it) {
-        const int st = it & 1;
-        // the record of this slice (copied while the previous one was processed)
-        const bool got = mbar_wait_bounded(&bar[st], (phase >> st) & 1u);
-        if (!__all_sync(0xffffffffu, got)) {   // uniform exit of the warp if a copy never completed
-            ok = false;
-            break;
-        }
-        phase ^= 1u << st;
-        pending &= ~(1u << st);
-        const int64_t base = p.slice_ptr[s];
-        const int w = (int)((p.slice_ptr[s + 1] - base) / GPW);
-        const int64_t bytes = rec_bytes(s);
-        if (bytes <= p.cap_record) {
-            const unsigned char* rec = buf + st * p.cap_record;
-            if (p.prefetch) prefetch_rows<VT, R>(p, reinterpret_cast<const int32_t*>(rec), w * GPW);
-            group_slice<VT, CPLX, G, RPT, TPR, true>(p, s, w, reinterpret_cast<const int32_t*>(rec) + sub,
-                                                     reinterpret_cast<const HT*>(rec + (size_t)w * GPW * 4) + sub * G,
-                                                     cb, acc_s);
-        } else {
-            const unsigned char* rec = p.mat + base * eb;
-            group_slice<VT, CPLX, G, RPT, TPR, false>(p, s, w, reinterpret_cast<const int32_t*>(rec) + sub,
-                                                      reinterpret_cast<const HT*>(rec + (size_t)w * GPW * 4) + sub * G,
-                                                      cb, acc_s);
-        }
-        __syncwarp();   // every lane is done with this buffer before it is refilled
-        if (s + 2 * nwb < s1e) {
-            pending |= 1u << st;
-            if (lane == 0) issue(s + 2 * nwb, st);
-        }
-    }
-    if (!ok) {
-        if (lane == 0) atomicOr(&p.counter[2], 2u);
-        // let copies still in flight land before the block's shared memory is released
-        for (int st = 0; st < 2; ++st)
-            if ((pending >> st) & 1u) mbar_wait_bounded(&bar[st], (phase >> st) & 1u);
-        __syncwarp();
-    }
-    reduce_and_finalize<RPT, TPR>(p, acc_s);
-}
-
 // ---------------------------------------------------------------------------- start vectors
 // v <- psi (rows in the solver order), x_prev <- 0; then the first update gives x_1 = psi (a_0 = 0, b_0 = 1).
 template <typename VT>
@@ -385,12 +221,12 @@ static int step_launch(gbn_ctx* c, int R, StepLaunch* L)
     const Ell& E = c->ell;
     const size_t per_warp = 2 * (size_t)E.cap_record;
     const size_t min_warps = (size_t)((4 * R + 31) / 32);
-    const bool staged = !E.field && c->tune_staged != 0 && per_warp > 0 && 128 + min_warps * per_warp <= kStagedSmemBudget;
+    const bool staged = c->tune_staged != 0 && per_warp > 0 && 128 + min_warps * per_warp <= kStagedSmemBudget;
     L->staged = staged;
     if (E.field) {
         int rpt, tpr;
         split_rhs(c->prec, R, c->tune_rpt, &rpt, &tpr);
-        L->fn = field_step_kernel(c->prec, E.G, rpt, tpr);
+        L->fn = field_step_kernel(c->prec, E.G, rpt, tpr, staged);
     } else {
         L->fn = step_kernel(c->prec, E.cplx, E.G, R, c->tune_rpt, staged);
     }

@@ -61,6 +61,23 @@ def test_fields_fp64_match_per_field_oracle(ctx, base):
             assert _close(a[f, v, :k], b[f, v, :k], a0, b0, 1e-10), (m, v)
 
 
+@pytest.mark.parametrize("grp", [1, 2])
+def test_fields_every_matrix_path(ctx, base, grp):
+    """Records staged in shared memory or read in place, rows per group 1 or 2: FP64 recursions of the
+    batched fields agree to 1e-10 of the spectral scale."""
+    n = base["geo"]["n"]
+    u = _draws(n)
+    _field_free(ctx, base)
+    out = []
+    try:
+        for staged in (0, 1):
+            ctx.set_tuning(0, 0, grp, staged)
+            out.append(ctx.lanczos_fields(FIELDS, u, 80, G.GBN_FP64))
+    finally:
+        ctx.set_tuning()
+    assert _close(out[1][0], out[1][1], out[0][0], out[0][1], 1e-10)
+
+
 def test_fields_mixed_dos(ctx, base):
     """Mixed precision (FP32 vectors and field-free hoppings, phases from 32-bit turn fractions): the DOS
     of each field against the FP64 oracle's, and against the per-field mixed path (gbn_peierls)."""
