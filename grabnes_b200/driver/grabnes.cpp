@@ -22,6 +22,7 @@
 #include <string.h>
 #include <sys/stat.h>
 
+#include <algorithm>
 #include <cctype>
 #include <cmath>
 #include <map>
@@ -727,6 +728,37 @@ int run(const Job& j0)
     ck(gbn_rng_uniform(j.seed, n, u.data()), nullptr, "gbn_rng_uniform");
     const bool magfield = !(j.mbi == 0 && j.mbf == 0);
     std::vector<double> a((size_t)j.nrecurs), b((size_t)j.nrecurs), psi;
+    if (magfield && j.mbi != j.mbf && j.pdos.mode == 0 && j.only_dos) {
+        // a DOS-only sweep: all fields in one batch from the field-free Hamiltonian, each field's Peierls
+        // phases applied on the fly (the reference reseeds, so every field starts from the same vector)
+        std::vector<int32_t> fm;
+        for (long mb = j.mbi; mb <= j.mbf; mb += j.mstep) fm.push_back((int32_t)mb);
+        const int nf = (int)fm.size();
+        std::vector<double> uu((size_t)nf * n), aa((size_t)nf * j.nrecurs), bb((size_t)nf * j.nrecurs);
+        for (int f = 0; f < nf; ++f) std::copy(u.begin(), u.end(), uu.begin() + (size_t)f * n);
+        ck(gbn_assemble(ctx, &j.model, j.moire ? rat_on.data() : nullptr, j.moire ? rat_hop.data() : nullptr,
+                        j.model.anderson ? u.data() : nullptr),
+           ctx, "gbn_assemble");
+        ck(gbn_lanczos_fields(ctx, GBN_FP64, nf, fm.data(), 1, uu.data(), nullptr, j.nrecurs, aa.data(), bb.data()),
+           ctx, "gbn_lanczos_fields");
+        printf("grabnes: %d fields in one batch\n", nf);
+        for (int f = 0; f < nf; ++f) {
+            const double bmag = fm[(size_t)f] * kFluxQuantum / (area * 1.0e-20);
+            char folder[64];
+            snprintf(folder, sizeof folder, "m%05d_B%.4f", fm[(size_t)f], bmag);
+            if (mkdir(folder, 0755) != 0 && errno != EEXIST) die(std::string("cannot create folder ") + folder);
+            const std::string prefix = std::string("./") + folder + "/" + j.prefix;
+            printf("grabnes: field %d of %ld..%ld, %.5f T, files in %s\n", fm[(size_t)f], j.mbi, j.mbf, bmag, folder);
+            kubo_dos_files(ctx, j, prefix, aa.data() + (size_t)f * j.nrecurs, bb.data() + (size_t)f * j.nrecurs);
+            if (j.polynomials) {   // <prefix>.cn.dat only: Calculate.OnlyDOS stops before the evolution
+                a.assign(aa.begin() + (size_t)f * j.nrecurs, aa.begin() + (size_t)(f + 1) * j.nrecurs);
+                b.assign(bb.begin() + (size_t)f * j.nrecurs, bb.begin() + (size_t)(f + 1) * j.nrecurs);
+                time_evolution(ctx, j, psi, a, b, prefix, n);
+            }
+        }
+        gbn_destroy(ctx);
+        return 0;
+    }
     for (long mb = j.mbi; mb <= j.mbf; mb += (magfield ? j.mstep : 1)) {
         std::string prefix = j.prefix;
         if (magfield && j.mbi != j.mbf) {
