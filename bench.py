@@ -137,6 +137,12 @@ def run_ours(args, ws, rank, local):
 
     torch.cuda.set_device(local)
     stream = torch.cuda.Stream()
+    if args.fields_only:   # the batched-field sweep alone (profiling of its kernels)
+        out = fields_leg(G, M, local, stream, ws, args.fields_scale)
+        if rank == 0:
+            print(json.dumps(out), flush=True)
+        replicas.finish(ws)
+        return
     ctx = G.Context(local)
     ctx.set_stream(stream.cuda_stream)
     job = M.job_from_keys(dict(WORKLOAD, **{"Structure.SuperCell": args.supercell}))
@@ -283,7 +289,7 @@ FIELDS_KEYS = {"Run.TypeOfSystem": "Graphene", "Structure.CellSize": 55, "Struct
                "Moire.H0AndHZ": True, "Moire.OffDiag": True, "Moire.OffDiagMidpoint": True}
 
 
-def fields_leg(G, M, local, stream, ws):
+def fields_leg(G, M, local, stream, ws, scale=1.0):
     """Graphene on hBN, effective moire model (387,200 atoms; on-site and bond terms of the three first-shell
     harmonics, OffDiagMidpoint): 33 fields of m = 0, 2, .., 64 flux quanta (0-26 T), 8 random-phase
     vectors per field (264 right-hand sides, GNU RNG seed 11), recursion lengths uniform in [500, 3000]
@@ -301,7 +307,8 @@ def fields_leg(G, M, local, stream, ws):
     rat_hop = G.cart_roundtrip(rat_on, cell["ucell"])
     ms = np.arange(0, 65, 2, dtype=np.int32)
     nvec = 8
-    ns = np.random.default_rng(11).integers(500, 3001, (len(ms), nvec)).astype(np.int32)
+    ns = np.random.default_rng(11).integers(500, 3001, (len(ms), nvec))
+    ns = np.maximum(1, np.rint(ns * scale)).astype(np.int32)   # scale < 1: shortened lengths (profiling)
     u = G.rng_uniform(11, len(ms) * nvec * n).reshape(len(ms), nvec, n)
     area = M.cell_area(cell["ucell"])
     work = float(n) * float(ns.sum())
@@ -336,7 +343,8 @@ def fields_leg(G, M, local, stream, ws):
     launches = ctx.launches
     _, t_field = timed(per_field)
     ctx.close()
-    return {"workload": "graphene_hbn_moire_387200atoms_33fields_x8vec_500-3000steps", "atoms": n,
+    name = "graphene_hbn_moire_387200atoms_33fields_x8vec_500-3000steps" + ("" if scale == 1.0 else f"_x{scale:g}")
+    return {"workload": name, "atoms": n,
             "fields": int(len(ms)), "vectors_per_field": nvec, "useful_atom_steps": work,
             "batched_s": t_batch, "batched_atom_steps_per_s": ws * work / t_batch, "batched_loop_s": loop_s,
             "per_field_s": t_field, "per_field_atom_steps_per_s": ws * work / t_field,
@@ -413,6 +421,8 @@ def main():
     p.add_argument("--nsteps", type=int, default=NSTEPS, help="recursion steps per job (2000 = the workload)")
     p.add_argument("--value-only", action="store_true", help="time the device-resident jobs only (profiling)")
     p.add_argument("--no-fields", action="store_true", help="skip the batched-field sweep (graphene/hBN, 33 fields)")
+    p.add_argument("--fields-only", action="store_true", help="run the batched-field sweep alone")
+    p.add_argument("--fields-scale", type=float, default=1.0, help="scale of the sweep's recursion lengths (profiling)")
     p.add_argument("--tuning", default="", help="fixed kernel tuning 'rhs_per_thread,blocks_per_sm,rows_per_group,staged,prefetch' "
                                                 "instead of the autotuner")
     args = p.parse_args()
