@@ -39,6 +39,7 @@ class Model(C.Structure):
         ("d_interlayer", C.c_double), ("aCC", C.c_double), ("g_intlay", C.c_double),
         ("anderson", C.c_int32), ("anderson_w", C.c_double), ("e0_c", C.c_double),
         ("inter_cut_rho", C.c_double), ("inter_smooth_w", C.c_double),
+        ("koshino_sr", C.c_int32), ("renormalize_coupling", C.c_int32), ("coupling_factor", C.c_double),
     ]
 
 

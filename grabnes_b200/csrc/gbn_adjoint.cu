@@ -224,8 +224,11 @@ __global__ void k_ad_params(AdTables t, gbn_model m, double g0, const double* ne
             } else if (m.interlayer == 1) {
                 const double dist = sqrt(Dx * Dx + Dy * Dy + Dz * Dz);
                 const double rho = sqrt(Dx * Dx + Dy * Dy);
-                const double es = exp(-(dist - m.d_interlayer) / m.bl_delta);
-                const double ep = exp(-(dist - m.aCC) / m.bl_delta);
+                // KoshinoSR and the coupling factor scale the whole term (constants of theta)
+                const double f = (m.koshino_sr ? exp((fabs(Dz) - 3.25) / 1.34) : 1.0) *
+                                 (m.renormalize_coupling ? m.coupling_factor : 1.0);
+                const double es = exp(-(dist - m.d_interlayer) / m.bl_delta) * f;
+                const double ep = exp(-(dist - m.aCC) / m.bl_delta) * f;
                 const double vsig = m.vppsigma0 * es, vpi = m.vpppi0 * ep;
                 const double q2 = (Dz / dist) * (Dz / dist);
                 double dsw;

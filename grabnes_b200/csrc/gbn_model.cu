@@ -180,10 +180,12 @@ __global__ void k_hopping(gbn_model m, int64_t n, const double* rat, const int32
             } else if (Li == Lj + 1 || Li == Lj - 1) {
                 if (m.interlayer == 1) {
                     const double dist = sqrt(Dx * Dx + Dy * Dy + Dz * Dz);
-                    const double vsig = m.vppsigma0 * exp(-(dist - m.d_interlayer) / m.bl_delta);
-                    const double vpi = m.vpppi0 * exp(-(dist - m.aCC) / m.bl_delta);
+                    const double sr = m.koshino_sr ? exp((fabs(Dz) - 3.25) / 1.34) : 1.0;
+                    const double vsig = m.vppsigma0 * exp(-(dist - m.d_interlayer) / m.bl_delta) * sr;
+                    const double vpi = m.vpppi0 * exp(-(dist - m.aCC) / m.bl_delta) * sr;
                     const double q = Dz / dist;
                     hr = hr + (vpi * (1.0 - q * q) + vsig * (q * q)) * smooth_cut(m, sqrt(Dx * Dx + Dy * Dy));
+                    if (m.renormalize_coupling) hr = m.coupling_factor * hr;
                 } else {
                     const double d = sqrt(Dx * Dx + Dy * Dy);
                     hr = hr + m.g_intlay * exp(-d / m.d_interlayer);

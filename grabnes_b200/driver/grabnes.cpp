@@ -378,6 +378,9 @@ Job job_from_input(const Input& in)
     m.anderson = in.l("Disorder.Anderson", false) ? 1 : 0;
     m.anderson_w = in.has("Disorder.AndersonAmp") ? in.d("Disorder.AndersonAmp", 0.0) / g0 : 1.0;
     m.e0_c = in.d("TB.OnSiteC", 0.0) / g0;
+    m.koshino_sr = in.l("Interlayer.KoshinoSR", false) ? 1 : 0;
+    m.renormalize_coupling = in.l("Interlayer.RenormalizeCoupling", false) ? 1 : 0;
+    m.coupling_factor = in.d("Interlayer.CouplingFactor", 1.0);
     j.second_layer = in.l("Interlayer.AddSecondLayerInteractions", false);
     j.nrecurs = (int)in.i("Kubo.RecursionNumber", 700);
     j.eta = in.d("Kubo.Epsilon", 0.01) / g0;
@@ -514,13 +517,14 @@ void print_job(const Job& j)
            "\"moire_onsite\": %d, \"moire_offdiag\": %d, \"moire_mid\": %d, \"moire_twisted\": %d, \"eps\": %.17g, "
            "\"twist_rad\": %.17g, \"C0\": %.17g, \"Cz\": %.17g, \"Cab\": %.17g, \"interlayer\": %d, "
            "\"vpppi0\": %.17g, \"vppsigma0\": %.17g, \"bl_delta\": %.17g, \"anderson\": %d, \"anderson_w\": %.17g, "
-           "\"tksl2\": %.17g}}\n",
+           "\"tksl2\": %.17g, \"koshino_sr\": %d, \"renormalize_coupling\": %d, \"coupling_factor\": %.17g}}\n",
            j.cell.kind, j.cell.aG, j.cell.cell_size, j.cell.super_cell, j.cell.m[0], j.cell.m[1], j.cell.m[2], j.cell.m[3],
            j.cell.height, j.cell.d_interlayer, j.g0, j.cut2intra, j.cut2inter, (int)j.second_layer, (int)j.moire,
            j.nrecurs, j.eta, j.n_en, j.emin, j.emax, j.seed, j.prefix.c_str(), (int)j.only_dos, j.npol, j.nt, j.nwr,
            j.dt, j.pdos.mode, j.seed_set, m.tbnn, m.intralayer, m.moire_onsite,
            m.moire_offdiag, m.moire_mid, m.moire_twisted, m.eps, m.twist_rad, m.C0, m.Cz, m.Cab, m.interlayer,
-           m.vpppi0, m.vppsigma0, m.bl_delta, m.anderson, m.anderson_w, m.tksl[2]);
+           m.vpppi0, m.vppsigma0, m.bl_delta, m.anderson, m.anderson_w, m.tksl[2], m.koshino_sr,
+           m.renormalize_coupling, m.coupling_factor);
 }
 
 void write_pairs(const std::string& path, const std::vector<double>& x, const std::vector<double>& y, double head,

@@ -139,6 +139,9 @@ def job_from_keys(keys):
     amp = g("Disorder.AndersonAmp", None)
     m.anderson_w = 1.0 if amp is None else amp / g0
     m.e0_c = g("TB.OnSiteC", 0.0) / g0
+    m.koshino_sr = int(bool(g("Interlayer.KoshinoSR", False)))
+    m.renormalize_coupling = int(bool(g("Interlayer.RenormalizeCoupling", False)))
+    m.coupling_factor = g("Interlayer.CouplingFactor", 1.0)
     seed = g("Kubo.SeedValue", 123456)
     kubo = dict(nrecurs=g("Kubo.RecursionNumber", 700), eta=g("Kubo.Epsilon", 0.01) / g0, n_en=g("Kubo.NumberofEnergyPoints", 1000),
                 emin=g("Kubo.EnergyMin", -4.0) / g0, emax=g("Kubo.EnergyMax", 4.0) / g0, seed=seed,

@@ -67,6 +67,12 @@ typedef struct gbn_model {
      * rho the in-plane distance [Ang] and rho_c = inter_cut_rho.  0 = the reference's hard cutoff. */
     double  inter_cut_rho;
     double  inter_smooth_w;
+    /* Interlayer.KoshinoSR: both two-centre terms scaled per bond by exp((|dz| - 3.25)/1.34); and
+     * Interlayer.RenormalizeCoupling: every interlayer hopping times coupling_factor
+     * (Interlayer.CouplingFactor) (ham.F90:6247-6260, 6807-6838, 9817-9823). */
+    int32_t koshino_sr;
+    int32_t renormalize_coupling;
+    double  coupling_factor;
 } gbn_model;
 
 /* ---- host-side cell construction and random numbers (no context, no GPU needed) ------ */

@@ -96,6 +96,10 @@ typedef struct {
     double  anderson_w;        /* /g0                                              */
     int32_t seed;              /* Kubo.SeedValue                                   */
     double  e0_c;              /* TB.OnSiteC/g0                                    */
+    /* Interlayer.KoshinoSR (ham.F90:9817-9823) and RenormalizeCoupling (ham.F90:6807-6838) */
+    int32_t koshino_sr;
+    int32_t renormalize_coupling;
+    double  coupling_factor;
 } orc_model;
 
 void orc_onsite(const orc_model* m, int64_t n, const double* Rat,

@@ -40,6 +40,7 @@ class Model(C.Structure):
         ("interlayer", C.c_int32), ("vpppi0", C.c_double), ("vppsigma0", C.c_double), ("bl_delta", C.c_double),
         ("d_interlayer", C.c_double), ("aCC", C.c_double), ("g_intlay", C.c_double),
         ("anderson", C.c_int32), ("anderson_w", C.c_double), ("seed", C.c_int32), ("e0_c", C.c_double),
+        ("koshino_sr", C.c_int32), ("renormalize_coupling", C.c_int32), ("coupling_factor", C.c_double),
     ]
 
 

@@ -192,11 +192,15 @@ void orc_hopping(const orc_model* m, int64_t n, const double* Rat, const int32_t
                 }
             } else if (layer[i] == layer[jj] + 1 || layer[i] == layer[jj] - 1) {
                 if (m->interlayer == ORC_INTER_TWO_CENTRE) {
+                    /* ham.F90:9810-9830: renormalizeHoppingFactorAAp of KoshinoSR (aval 1.34, bval 3.25) */
                     const double dist = sqrt(D[0] * D[0] + D[1] * D[1] + D[2] * D[2]);
-                    const double vsig = m->vppsigma0 * exp(-(dist - m->d_interlayer) / m->bl_delta) * 1.0;
-                    const double vpi = m->vpppi0 * exp(-(dist - m->aCC) / m->bl_delta) * 1.0;
+                    const double renorm = m->koshino_sr ? exp((fabs(D[2]) - 3.25) / 1.34) : 1.0;
+                    const double vsig = m->vppsigma0 * exp(-(dist - m->d_interlayer) / m->bl_delta) * renorm;
+                    const double vpi = m->vpppi0 * exp(-(dist - m->aCC) / m->bl_delta) * renorm;
                     const double q = D[2] / dist;
                     h[0] = h[0] + (vpi * (1.0 - q * q) + vsig * (q * q));
+                    /* ham.F90:6807-6838 without Interlayer.DifferentCouplings */
+                    if (m->renormalize_coupling) h[0] = m->coupling_factor * h[0];
                 } else {
                     const double d = sqrt(D[0] * D[0] + D[1] * D[1]);
                     h[0] = h[0] + m->g_intlay * exp(-d / m->d_interlayer);

@@ -132,6 +132,9 @@ def build(keys):
     m.anderson_w = g("AndersonAmp", 1.0 * g0) / g0
     m.seed = g("SeedValue", 123456)
     m.e0_c = g("OnSiteC", 0.0) / g0
+    m.koshino_sr = int(g("KoshinoSR", False))
+    m.renormalize_coupling = int(g("RenormalizeCoupling", False))
+    m.coupling_factor = g("CouplingFactor", 1.0)
 
     rat = geo["rat"]
     rat_on = orc.roundtrip(rat, geo["ucell"]) if moire else rat

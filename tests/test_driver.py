@@ -29,6 +29,13 @@ INPUTS = {
         "TypeOfBL": "Koshino", "vpppi0": 2.7, "vppsigma0": 0.48, "BLdelta": 0.319, "InterlayerDistance": 3.35,
         "Neigh.LayerNeighbors": 100, "Neigh.LayerDistFactor": 3.2005, "TB.Hopping": 2.7, "RecursionNumber": 150,
     },
+    "example08_model": {
+        "Run.TypeOfSystem": "TwistedBilayerBasedOnMoireCell", "Structure.MoireCellParameters": (31, 30, 30, 31),
+        "Stack.TwoLayers": True, "Structure.InterlayerDistance": 3.35, "Intralayer.F2G2Model": True,
+        "TB.NeighLevels": 5, "TB.Hopping": 3.5, "TB.OnSiteC": 0.4914, "Interlayer.TypeOfBL": "Koshino",
+        "Interlayer.KoshinoSR": True, "Interlayer.RenormalizeCoupling": True, "Interlayer.CouplingFactor": 1.008,
+        "Neigh.LayerNeighbors": 400, "Neigh.LayerDistFactor": 4.0, "Kubo.RecursionNumber": 100,
+    },
     "anderson": {"Run.TypeOfSystem": "Graphene", "Structure.CellSize": 30, "Disorder.Anderson": True,
                  "Disorder.AndersonAmp": 1.0, "Kubo.SeedValue": 5, "TB.NeighLevels": 2},
 }
@@ -76,9 +83,9 @@ def test_driver_reads_input_like_the_package(tmp_path, name):
     assert math.isclose(got["emin"], job["kubo"]["emin"], rel_tol=1e-15)
     m = job["model"]
     for f in ("tbnn", "intralayer", "moire_onsite", "moire_offdiag", "moire_mid", "moire_twisted", "interlayer",
-              "anderson"):
+              "anderson", "koshino_sr", "renormalize_coupling"):
         assert got["model"][f] == getattr(m, f), f
-    for f in ("eps", "C0", "Cz", "Cab", "vpppi0", "vppsigma0", "bl_delta", "anderson_w"):
+    for f in ("eps", "C0", "Cz", "Cab", "vpppi0", "vppsigma0", "bl_delta", "anderson_w", "coupling_factor"):
         assert math.isclose(got["model"][f], getattr(m, f), rel_tol=1e-15, abs_tol=1e-300), f
     assert got["cell_size"] == job["cell"]["cell_size"] and got["super_cell"] == job["cell"]["super_cell"]
     assert tuple(got["m"]) == tuple(job["cell"]["m"])

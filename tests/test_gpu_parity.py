@@ -33,6 +33,12 @@ CASES = {
     "tbg": dict(TypeOfSystem="TwistedBilayerBasedOnMoireCell", MoireCellParameters=(31, 30, 30, 31), SuperCell=1,
                 TypeOfBL="Koshino", Hopping=2.7, LatticeParameter=2.4595, Vpppi0=2.7, Vppsigma0=0.48,
                 BLdelta=0.319, InterlayerDistance=3.35, LayerNeighbors=100, LayerDistFactor=3.2005),
+    # example 08's twisted bilayer model: F2G2 intralayer to the fifth shell, on-site 0.4914 eV, KoshinoSR
+    # two-centre interlayer to 6.25 A in plane, coupling renormalised by 1.008
+    "tbg_sr": dict(TypeOfSystem="TwistedBilayerBasedOnMoireCell", MoireCellParameters=(31, 30, 30, 31), SuperCell=1,
+                   TypeOfBL="Koshino", Hopping=3.5, OnSiteC=0.4914, NeighLevels=5, InterlayerDistance=3.35,
+                   LayerNeighbors=400, LayerDistFactor=4.0, KoshinoSR=True, RenormalizeCoupling=True,
+                   CouplingFactor=1.008),
     # Anderson disorder (config 5 model) on graphene
     "anderson": dict(TypeOfSystem="Graphene", CellSize=30, Anderson=True, AndersonAmp=1.0, SeedValue=5),
 }
