@@ -371,6 +371,22 @@ int gbn_load_hamiltonian(gbn_ctx* c, int64_t n, int32_t max_neigh, const int32_t
     return GBN_OK;
 }
 
+int gbn_set_images(gbn_ctx* c, const int32_t* ncell)
+{
+    if (!c || !ncell) return GBN_ERR_ARG;
+    if (!c->have_neigh) return fail(c, GBN_ERR_STATE, "load the neighbour list first");
+    if (!c->have_geometry) return fail(c, GBN_ERR_STATE, "the Peierls phases need the positions: gbn_set_geometry first");
+    cudaSetDevice(c->device);
+    const size_t e = (size_t)c->n * c->max_neigh;
+    GBN_CK(c, c->ncell.ensure(sizeof(int32_t) * 3 * e));
+    GBN_CK(c, cudaMemcpyAsync(c->ncell.p, ncell, sizeof(int32_t) * 3 * e, cudaMemcpyHostToDevice, c->stream));
+    GBN_CK(c, c->rat_hop.ensure(sizeof(double) * 3 * (size_t)c->n));
+    GBN_CK(c, cudaMemcpyAsync(c->rat_hop.p, c->rat.p, sizeof(double) * 3 * (size_t)c->n, cudaMemcpyDeviceToDevice,
+                              c->stream));
+    GBN_CK(c, cudaStreamSynchronize(c->stream));
+    return GBN_OK;
+}
+
 int gbn_set_neighd(gbn_ctx* c, const double* neighd)
 {
     if (!c || !neighd) return GBN_ERR_ARG;

@@ -297,6 +297,9 @@ struct Job {
     bool field_by_value = false, field_steps_by_value = false;
     double b_value = 0, b_init = 0, b_final = 0, b_step = 0;
     std::string prefix;
+    bool write_data = false;    // Output.WriteDataFiles
+    bool read_data = false;     // Output.ReadDataFiles
+    bool read_details = false;  // Neigh.ReadDetails
     gbn_pdos pdos{};        // Kubo.PDOS selection (mode 0: the DOS of the whole cell)
     int seed_set = 1235;    // Kubo.SeedSet: the stream of the layer start vectors
 };
@@ -397,6 +400,9 @@ Job job_from_input(const Input& in)
     j.nwr = (int)in.i("Kubo.WriteNumberofSteps", 10);
     j.dt = in.d("Kubo.TimeStep", 5.0);
     if (j.npol < 1 || j.nt < 0 || j.nwr < 1) die("Kubo.NumberofPolynomials and Kubo.WriteNumberofSteps must be positive");
+    j.write_data = in.l("Output.WriteDataFiles", false);
+    j.read_data = in.l("Output.ReadDataFiles", false);
+    j.read_details = in.l("Neigh.ReadDetails", false);
     // local DOS selections (CalcKubo, calc.F90:214-300): the first flag that is set picks the mode
     if (in.l("Kubo.PDOS", false)) {
         gbn_pdos& p = j.pdos;
@@ -577,6 +583,218 @@ void time_evolution(gbn_ctx* ctx, const Job& j, std::vector<double> psi, const s
     }
 }
 
+// A list-directed real of gfortran without its padding (for complex pairs).
+std::string ld_trim(double x)
+{
+    std::string t = fortran_ld(x);
+    const size_t a = t.find_first_not_of(' '), b = t.find_last_not_of(' ');
+    return a == std::string::npos ? t : t.substr(a, b - a + 1);
+}
+
+FILE* open_or_die(const std::string& path)
+{
+    FILE* f = fopen(path.c_str(), "w");
+    if (!f) die("cannot write " + path);
+    return f;
+}
+
+// Output.WriteDataFiles, neighbour part (NeighWriteDataFiles, neigh.F90:383-440): v, dx, dy, dz, pos,
+// neighCell.dat, neighD.dat in the working folder, with the reference's edit descriptors.
+void write_neigh_files(gbn_ctx* ctx, int64_t n, int32_t maxn, const std::vector<double>& rat,
+                       const std::vector<int32_t>& species)
+{
+    std::vector<int32_t> nn((size_t)n), nl((size_t)n * maxn), nc((size_t)3 * n * maxn);
+    std::vector<double> nd((size_t)3 * n * maxn);
+    ck(gbn_get_neighbours(ctx, nn.data(), nl.data(), nd.data(), nc.data()), ctx, "gbn_get_neighbours");
+    FILE* fv = open_or_die("v");
+    FILE* fx[3] = {open_or_die("dx"), open_or_die("dy"), open_or_die("dz")};
+    FILE* fp = open_or_die("pos");
+    FILE* fc = open_or_die("neighCell.dat");
+    FILE* fd = open_or_die("neighD.dat");
+    for (int64_t i = 0; i < n; ++i) {
+        const int k = nn[(size_t)i];
+        const size_t e0 = (size_t)i * maxn;
+        fprintf(fv, "%12d\n", k);
+        for (int j = 0; j < k; ++j) fprintf(fv, "%8d %s", nl[e0 + j], (j % 500 == 499 && j + 1 < k) ? "\n" : "");
+        fprintf(fv, "\n");
+        for (int c = 0; c < 3; ++c) {
+            for (int j = 0; j < k; ++j)
+                fprintf(fx[c], "%10.5f %s", nd[3 * (e0 + j) + c], (j % 500 == 499 && j + 1 < k) ? "\n" : "");
+            fprintf(fx[c], "\n");
+        }
+        const char* label = species[(size_t)i] == 3 ? "B    " : (species[(size_t)i] == 4 ? "N    " : "C    ");
+        fprintf(fp, " %s%s%s%s\n", label, fortran_ld(rat[(size_t)3 * i]).c_str(), fortran_ld(rat[(size_t)3 * i + 1]).c_str(),
+                fortran_ld(rat[(size_t)3 * i + 2]).c_str());
+        for (int j = 0; j < k; ++j) {
+            const size_t e = e0 + j;
+            fprintf(fc, "%6d %6d %6d \n", nc[3 * e], nc[3 * e + 1], nc[3 * e + 2]);
+            fprintf(fd, "%24.16E %24.16E %24.16E \n", nd[3 * e], nd[3 * e + 1], nd[3 * e + 2]);
+        }
+    }
+    for (FILE* f : {fv, fx[0], fx[1], fx[2], fp, fc, fd}) fclose(f);
+    printf("grabnes: neighbour tables written (v, dx, dy, dz, pos, neighCell.dat, neighD.dat)\n");
+}
+
+// Output.WriteDataFiles, Hamiltonian part (HamHopping and HamHopWriteTables, ham.F90:6944-7040):
+// <prefix>.s.mag (the hoppings of each atom, g0 units, the reference's sign), <prefix>.e (H0, Species,
+// layerIndex), <prefix>.pos, <prefix>.cell (ucell then the reciprocal cell, one vector per line), and the
+// empty <prefix>.HABreal / .HABimag of models without those terms.
+void write_ham_files(gbn_ctx* ctx, const std::string& prefix, int64_t n, int32_t maxn, const std::vector<double>& rat,
+                     const std::vector<int32_t>& species, const std::vector<int32_t>& layer, const double* u)
+{
+    std::vector<int32_t> nn((size_t)n);
+    ck(gbn_get_neighbours(ctx, nn.data(), nullptr, nullptr, nullptr), ctx, "gbn_get_neighbours");
+    std::vector<double> h0((size_t)n), hop((size_t)2 * n * maxn);
+    ck(gbn_get_hamiltonian(ctx, h0.data(), hop.data()), ctx, "gbn_get_hamiltonian");
+    FILE* f = open_or_die(prefix + ".s.mag");
+    for (int64_t i = 0; i < n; ++i) {
+        for (int j = 0; j < nn[(size_t)i]; ++j) {
+            const size_t e = (size_t)i * maxn + j;
+            fprintf(f, " (%s,%s)", ld_trim(hop[2 * e]).c_str(), ld_trim(hop[2 * e + 1]).c_str());
+        }
+        fprintf(f, "\n");
+    }
+    fclose(f);
+    f = open_or_die(prefix + ".e");
+    for (int64_t i = 0; i < n; ++i)
+        fprintf(f, "%s%12d%12d\n", fortran_ld(h0[(size_t)i]).c_str(), species[(size_t)i], layer[(size_t)i]);
+    fclose(f);
+    fclose(open_or_die(prefix + ".HABreal"));
+    fclose(open_or_die(prefix + ".HABimag"));
+    f = open_or_die(prefix + ".pos");
+    for (int64_t i = 0; i < n; ++i)
+        fprintf(f, "%s%s%s\n", fortran_ld(rat[(size_t)3 * i]).c_str(), fortran_ld(rat[(size_t)3 * i + 1]).c_str(),
+                fortran_ld(rat[(size_t)3 * i + 2]).c_str());
+    fclose(f);
+    // rcell(:,k) = 2 pi (ucell(:,k+1) x ucell(:,k+2)) / volume (cell.F90:400-402)
+    auto cross = [](const double* x, const double* y, double* z) {
+        z[0] = x[1] * y[2] - x[2] * y[1];
+        z[1] = x[2] * y[0] - x[0] * y[2];
+        z[2] = x[0] * y[1] - x[1] * y[0];
+    };
+    double c12[3];
+    cross(u, u + 3, c12);
+    const double vol = fabs(c12[0] * u[6] + c12[1] * u[7] + c12[2] * u[8]);
+    double rc[9];
+    cross(u + 3, u + 6, rc);
+    cross(u + 6, u, rc + 3);
+    cross(u, u + 3, rc + 6);
+    f = open_or_die(prefix + ".cell");
+    for (int v = 0; v < 3; ++v)
+        fprintf(f, "%s%s%s\n", fortran_ld(u[3 * v]).c_str(), fortran_ld(u[3 * v + 1]).c_str(), fortran_ld(u[3 * v + 2]).c_str());
+    for (int v = 0; v < 3; ++v)
+        fprintf(f, "%s%s%s\n", fortran_ld(2.0 * kPi * rc[3 * v] / vol).c_str(), fortran_ld(2.0 * kPi * rc[3 * v + 1] / vol).c_str(),
+                fortran_ld(2.0 * kPi * rc[3 * v + 2] / vol).c_str());
+    fclose(f);
+}
+
+// Output.ReadDataFiles: the neighbour list from v (NeighReadDataFiles, neigh.F90:446-522: with
+// Neigh.ReadDetails also neighCell.dat and neighD.dat, otherwise each entry's image is the one of the nine
+// in-plane images closer than aG/sqrt(3)*1.1, the last found), H0 from generate.e and the hoppings from
+// generate.s, one 're im' pair per entry (calc.F90:86-95, ham.F90:659-672).
+struct Tables {
+    int32_t maxn = 0;
+    std::vector<int32_t> nn, nl, nc;
+    std::vector<double> nd, h0, hop;
+};
+
+std::vector<double> read_numbers(const std::string& path, bool first_column_only)
+{
+    FILE* f = fopen(path.c_str(), "r");
+    if (!f) die("Output.ReadDataFiles: cannot open " + path);
+    std::vector<double> out;
+    char line[1 << 16];
+    while (fgets(line, sizeof line, f)) {
+        for (char* q = line; *q; ++q)
+            if (*q == 'd' || *q == 'D') *q = 'e';   // Fortran double-precision exponents
+        char* p = line;
+        for (;;) {
+            char* end = nullptr;
+            const double v = strtod(p, &end);
+            if (end == p) break;
+            out.push_back(v);
+            p = end;
+            if (first_column_only) break;
+        }
+    }
+    fclose(f);
+    return out;
+}
+
+Tables read_tables(const Job& j, int64_t n, const std::vector<double>& ucell, const std::vector<double>& rat)
+{
+    Tables t;
+    const std::vector<double> v = read_numbers("v", false);
+    t.nn.assign((size_t)n, 0);
+    std::vector<std::vector<int32_t>> rows((size_t)n);
+    size_t p = 0;
+    for (int64_t i = 0; i < n; ++i) {
+        if (p >= v.size()) die("Output.ReadDataFiles: v ends before atom " + std::to_string(i + 1));
+        const int k = (int)v[p++];
+        if (k < 0 || p + (size_t)k > v.size()) die("Output.ReadDataFiles: v is inconsistent at atom " + std::to_string(i + 1));
+        t.nn[(size_t)i] = k;
+        for (int q = 0; q < k; ++q) rows[(size_t)i].push_back((int32_t)v[p++]);
+        t.maxn = std::max(t.maxn, k);
+    }
+    t.maxn = std::max(t.maxn, 1);
+    const size_t E = (size_t)n * t.maxn;
+    t.nl.assign(E, 1);
+    t.nc.assign(3 * E, 0);
+    t.nd.assign(3 * E, 0.0);
+    for (int64_t i = 0; i < n; ++i)
+        for (int q = 0; q < t.nn[(size_t)i]; ++q) {
+            const int32_t m = rows[(size_t)i][(size_t)q];
+            if (m < 1 || m > n) die("Output.ReadDataFiles: neighbour index outside 1..N in v");
+            t.nl[(size_t)i * t.maxn + q] = m;
+        }
+    if (j.read_details) {
+        const std::vector<double> c = read_numbers("neighCell.dat", false), d = read_numbers("neighD.dat", false);
+        size_t q3 = 0;
+        for (int64_t i = 0; i < n; ++i)
+            for (int q = 0; q < t.nn[(size_t)i]; ++q, q3 += 3) {
+                if (q3 + 3 > c.size() || q3 + 3 > d.size()) die("Output.ReadDataFiles: neighCell.dat / neighD.dat too short");
+                for (int k = 0; k < 3; ++k) {
+                    t.nc[3 * ((size_t)i * t.maxn + q) + k] = (int32_t)c[q3 + k];
+                    t.nd[3 * ((size_t)i * t.maxn + q) + k] = d[q3 + k];
+                }
+            }
+    } else {
+        const double cut = j.cell.aG / sqrt(3.0) * 1.1;
+        for (int64_t i = 0; i < n; ++i)
+            for (int q = 0; q < t.nn[(size_t)i]; ++q) {
+                const int64_t m = t.nl[(size_t)i * t.maxn + q] - 1;
+                for (int ix = -1; ix <= 1; ++ix)
+                    for (int iy = -1; iy <= 1; ++iy) {
+                        if (i == m && ix == 0 && iy == 0) continue;
+                        double w[3], d2 = 0.0;
+                        for (int k = 0; k < 3; ++k) {
+                            w[k] = rat[(size_t)3 * i + k] - rat[(size_t)3 * m + k] - (ix * ucell[k] + iy * ucell[3 + k]);
+                            d2 += w[k] * w[k];
+                        }
+                        if (sqrt(d2) < cut) {
+                            const size_t e = (size_t)i * t.maxn + q;
+                            t.nc[3 * e] = ix; t.nc[3 * e + 1] = iy; t.nc[3 * e + 2] = 0;
+                            for (int k = 0; k < 3; ++k) t.nd[3 * e + k] = -w[k];
+                        }
+                    }
+            }
+    }
+    t.h0 = read_numbers("generate.e", true);
+    if ((int64_t)t.h0.size() < n) die("Output.ReadDataFiles: generate.e has fewer lines than atoms");
+    t.h0.resize((size_t)n);
+    const std::vector<double> s = read_numbers("generate.s", false);
+    t.hop.assign(2 * E, 0.0);
+    size_t q2 = 0;
+    for (int64_t i = 0; i < n; ++i)
+        for (int q = 0; q < t.nn[(size_t)i]; ++q, q2 += 2) {
+            if (q2 + 2 > s.size()) die("Output.ReadDataFiles: generate.s has fewer entries than the neighbour list");
+            t.hop[2 * ((size_t)i * t.maxn + q)] = s[q2];
+            t.hop[2 * ((size_t)i * t.maxn + q) + 1] = s[q2 + 1];
+        }
+    printf("grabnes: neighbour list, on-site energies and hoppings read from v, generate.e, generate.s\n");
+    return t;
+}
+
 // KuboDOS (kubo.F90:276-319) after the recursion: <prefix>.b0.dat, .a0.dat (KuboRecursion's files), the
 // continued fraction <prefix>.DOS and the coefficients <prefix>.AB.
 void kubo_dos_files(gbn_ctx* ctx, const Job& j, const std::string& prefix, const double* a, const double* b)
@@ -717,7 +935,15 @@ int run(const Job& j0)
     ck(gbn_set_geometry(ctx, n, rat.data(), species.data(), layer.data(), ucell.data()), ctx, "gbn_set_geometry");
     int32_t maxn = 0;
     int64_t total = 0;
-    ck(gbn_neighbours(ctx, j.cut2intra, j.cut2inter, j.second_layer ? 1 : 0, &maxn, &total), ctx, "gbn_neighbours");
+    Tables tab;
+    if (j.read_data) {
+        tab = read_tables(j, n, ucell, rat);
+        maxn = tab.maxn;
+        for (int32_t k : tab.nn) total += k;
+    } else {
+        ck(gbn_neighbours(ctx, j.cut2intra, j.cut2inter, j.second_layer ? 1 : 0, &maxn, &total), ctx, "gbn_neighbours");
+        if (j.write_data) write_neigh_files(ctx, n, maxn, rat, species);
+    }
     printf("grabnes: %lld neighbour entries (at most %d per atom)\n", (long long)total, maxn);
     std::vector<double> rat_on, rat_hop;
     if (j.moire) {   // the positions the reference's moire routines see after their own conversions
@@ -732,7 +958,7 @@ int run(const Job& j0)
     ck(gbn_rng_uniform(j.seed, n, u.data()), nullptr, "gbn_rng_uniform");
     const bool magfield = !(j.mbi == 0 && j.mbf == 0);
     std::vector<double> a((size_t)j.nrecurs), b((size_t)j.nrecurs), psi;
-    if (magfield && j.mbi != j.mbf && j.pdos.mode == 0 && j.only_dos) {
+    if (magfield && j.mbi != j.mbf && j.pdos.mode == 0 && j.only_dos && !j.read_data && !j.write_data) {
         // a DOS-only sweep: all fields in one batch from the field-free Hamiltonian, each field's Peierls
         // phases applied on the fly (the reference reseeds, so every field starts from the same vector)
         std::vector<int32_t> fm;
@@ -773,13 +999,21 @@ int run(const Job& j0)
             prefix = std::string("./") + folder + "/" + j.prefix;
             printf("grabnes: field %ld of %ld..%ld, %.5f T, files in %s\n", mb, j.mbi, j.mbf, bmag, folder);
         }
-        ck(gbn_assemble(ctx, &j.model, j.moire ? rat_on.data() : nullptr, j.moire ? rat_hop.data() : nullptr,
-                        j.model.anderson ? u.data() : nullptr),
-           ctx, "gbn_assemble");
+        if (j.read_data) {   // the hoppings of generate.s for every field, then its phases
+            ck(gbn_load_hamiltonian(ctx, n, tab.maxn, tab.nn.data(), tab.nl.data(), tab.hop.data(), tab.h0.data()), ctx,
+               "gbn_load_hamiltonian");
+            ck(gbn_set_images(ctx, tab.nc.data()), ctx, "gbn_set_images");
+            ck(gbn_set_neighd(ctx, tab.nd.data()), ctx, "gbn_set_neighd");
+        } else {
+            ck(gbn_assemble(ctx, &j.model, j.moire ? rat_on.data() : nullptr, j.moire ? rat_hop.data() : nullptr,
+                            j.model.anderson ? u.data() : nullptr),
+               ctx, "gbn_assemble");
+        }
         if (magfield) {
             const double bmag = mb * kFluxQuantum / (area * 1.0e-20);
             ck(gbn_peierls(ctx, bmag * kPi / kFluxQuantum), ctx, "gbn_peierls");
         }
+        if (j.write_data && !j.read_data) write_ham_files(ctx, prefix, n, maxn, rat_now, species, layer, ucell.data());
         bool any = true;
         if (j.pdos.mode == 0) {   // KuboInitWF + KuboDOS
             ck(gbn_lanczos_phases(ctx, GBN_FP64, 1, u.data(), nullptr, j.nrecurs, a.data(), b.data()), ctx,

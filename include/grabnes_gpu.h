@@ -144,6 +144,10 @@ int gbn_get_neighbours(gbn_ctx* ctx, int32_t* nneigh, int32_t* nlist, double* ne
  * the reference's fractional/Cartesian round trips); uniform holds the N Anderson draws (or NULL). */
 int gbn_assemble(gbn_ctx* ctx, const gbn_model* model, const double* rat_onsite,
                  const double* rat_hop, const double* uniform);
+/* neighCell(3,maxNeigh,N) of a neighbour list loaded with gbn_load_hamiltonian, so that gbn_peierls can
+ * act on loaded hoppings, with the positions of gbn_set_geometry (the Output.ReadDataFiles path of
+ * CalcKubo, calc.F90:86-104: hoppings read from a file, then HamPeierlsPeriodicGauge). */
+int gbn_set_images(gbn_ctx* ctx, const int32_t* ncell);
 /* HamPeierlsPeriodicGauge (ham.F90:12834-12882): multiply the assembled hoppings by the phases of
  * flux (= B pi / Phi0, in 1/Ang^2 * 1e20) including the corner term; positions from gbn_assemble. */
 int gbn_peierls(gbn_ctx* ctx, double flux);

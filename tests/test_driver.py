@@ -244,3 +244,86 @@ def test_driver_atom_pdos_and_time_evolution(tmp_path):
     ab = np.loadtxt(folder / "gr.AB_0002.dat", skiprows=1)
     assert np.abs(ab[:, 0] - az).max() <= 1e-9 * np.abs(az).max()
     assert np.abs(ab[:, 1] - bz).max() <= 1e-9 * np.abs(bz).max()
+
+
+def _parse_v(path):
+    tok = open(path).read().split()
+    out, p = [], 0
+    while p < len(tok):
+        k = int(tok[p]); p += 1
+        out.append([int(x) for x in tok[p:p + k]]); p += k
+    return out
+
+
+@pytest.mark.gpu
+def test_driver_write_data_files(tmp_path):
+    """Output.WriteDataFiles: the neighbour files (v, dx, dy, dz, pos, neighCell.dat, neighD.dat) and the
+    Hamiltonian files (<prefix>.s.mag with the field's phases, .e, .pos, .cell) against the oracle's
+    tables, read the way the reference's tools/hamiltonian/verify_tables.py reads them."""
+    import re
+    keys = dict(INPUTS["moire_sweep"], **{"Output.WriteDataFiles": True, "MagField.Integer": 2, "Kubo.RecursionNumber": 20})
+    path = str(tmp_path / "Gendata.in")
+    _write(path, keys)
+    subprocess.run([DRIVER, path], check=True, cwd=str(tmp_path), capture_output=True, text=True)
+    base = dict(TypeOfSystem="Graphene", CellSize=11, SuperCell=4, LatticePercent=-1.0 / 11.0, MoirePotential=True,
+                MoireJeil=True, MoireH0AndHZ=True, MoireOffDiag=True, MoireOffDiagMidpoint=True, MagFieldInteger=2)
+    r = R.build(base)
+    nb, geo = r["nb"], r["geo"]
+    n = geo["n"]
+    rows = _parse_v(tmp_path / "v")
+    assert [len(x) for x in rows] == list(nb["nneigh"])
+    assert all(row == list(nb["nlist"][i, :len(row)]) for i, row in enumerate(rows))
+    mask = np.arange(nb["max_neigh"])[None, :] < nb["nneigh"][:, None]
+    cells = np.loadtxt(tmp_path / "neighCell.dat", dtype=np.int64).reshape(-1, 3)
+    assert np.array_equal(cells, nb["ncell"][mask])
+    disp = np.loadtxt(tmp_path / "neighD.dat").reshape(-1, 3)
+    assert np.array_equal(disp.view(np.int64), nb["neighd"][mask].view(np.int64))   # 17 digits: bitwise
+    dx = np.concatenate([np.array(line.split(), float) for line in open(tmp_path / "dx") if line.strip()])
+    assert np.abs(dx - nb["neighd"][mask][:, 0]).max() <= 5e-6
+    pair = re.compile(r"\(\s*([-+0-9.Ee]+)\s*,\s*([-+0-9.Ee]+)\s*\)")
+    hop = [complex(float(a), float(b)) for line in open(tmp_path / "generate.s.mag") for a, b in pair.findall(line)]
+    assert np.abs(np.array(hop) - r["hop"][mask]).max() <= 1e-13
+    e = np.loadtxt(tmp_path / "generate.e")
+    assert np.abs(e[:, 0] - r["h0"]).max() <= 1e-13
+    assert np.array_equal(e[:, 1].astype(int), geo["species"]) and np.array_equal(e[:, 2].astype(int), geo["layer"])
+    pos = np.loadtxt(tmp_path / "generate.pos")
+    assert np.array_equal(pos, r["rat_hop"])
+    cell = np.loadtxt(tmp_path / "generate.cell")
+    u = geo["ucell"].reshape(3, 3)
+    assert np.array_equal(cell[:3], u)
+    assert np.abs(cell[3:] @ u.T - 2 * np.pi * np.eye(3)).max() <= 1e-12
+    labels = [line.split()[0] for line in open(tmp_path / "pos")]
+    assert labels == ["C"] * n
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("details", [True, False])
+def test_driver_read_data_files(tmp_path, details):
+    """Output.ReadDataFiles: neighbour list from v (images from neighCell.dat / neighD.dat with
+    Neigh.ReadDetails, else the nearest in-plane image), H0 from generate.e, field-free hoppings from
+    generate.s, then the Peierls phases of MagField.Integer 3: a_n, b_n against the oracle."""
+    r0 = R.build(dict(TypeOfSystem="Graphene", CellSize=40, Hopping=2.7))
+    nb = r0["nb"]
+    mask = np.arange(nb["max_neigh"])[None, :] < nb["nneigh"][:, None]
+    with open(tmp_path / "v", "w") as f:
+        for i in range(len(nb["nneigh"])):
+            f.write(f"{nb['nneigh'][i]:12d}\n" + " ".join(f"{x:8d}" for x in nb["nlist"][i, :nb["nneigh"][i]]) + "\n")
+    if details:
+        np.savetxt(tmp_path / "neighCell.dat", nb["ncell"][mask], fmt="%6d")
+        np.savetxt(tmp_path / "neighD.dat", nb["neighd"][mask], fmt="%24.16E")
+    np.savetxt(tmp_path / "generate.e", np.c_[r0["h0"], r0["geo"]["species"], r0["geo"]["layer"]], fmt="%.17g")
+    hop = r0["hop"][mask]
+    np.savetxt(tmp_path / "generate.s", np.c_[hop.real, hop.imag], fmt="%.17g")
+    keys = {"Run.Prefix": "rd", "Run.TypeOfSystem": "Graphene", "Structure.CellSize": 40, "TB.Hopping": 2.7,
+            "Output.ReadDataFiles": True, "Neigh.ReadDetails": details, "MagField.Integer": 3,
+            "Kubo.RecursionNumber": 150, "Kubo.SeedValue": 9, "Calculate.OnlyDOS": True}
+    path = str(tmp_path / "Gendata.in")
+    _write(path, keys)
+    subprocess.run([DRIVER, path], check=True, cwd=str(tmp_path), capture_output=True, text=True)
+    r = R.build(dict(TypeOfSystem="Graphene", CellSize=40, Hopping=2.7, MagFieldInteger=3))
+    n = r["geo"]["n"]
+    a0, b0 = orc.recursion(r["nb"], r["hop"], r["h0"], orc.init_wf(n, 9), 150, 0)
+    a = np.loadtxt(tmp_path / "rd.a0.dat")
+    b = np.loadtxt(tmp_path / "rd.b0.dat")
+    scale = max(np.abs(a0).max(), np.abs(b0).max())
+    assert np.abs(a - a0).max() <= 1e-10 * scale and np.abs(b - b0).max() <= 1e-10 * scale
