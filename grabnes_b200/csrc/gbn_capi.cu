@@ -371,6 +371,14 @@ int gbn_load_hamiltonian(gbn_ctx* c, int64_t n, int32_t max_neigh, const int32_t
     return GBN_OK;
 }
 
+int gbn_haldane(gbn_ctx* c, double aG, double t2, double phase, int32_t paper, uint32_t layer_mask)
+{
+    if (!c) return GBN_ERR_ARG;
+    if (!(aG > 0.0)) return fail(c, GBN_ERR_ARG, "aG must be positive");
+    cudaSetDevice(c->device);
+    return haldane(c, aG, t2, phase, paper, layer_mask);
+}
+
 int gbn_set_images(gbn_ctx* c, const int32_t* ncell)
 {
     if (!c || !ncell) return GBN_ERR_ARG;

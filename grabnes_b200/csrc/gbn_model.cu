@@ -307,4 +307,84 @@ int peierls(gbn_ctx* c, double flux)
     return GBN_OK;
 }
 
+// HamHaldaneChirality (ham.F90:13063-13100): +1 if the path i -> k -> j through a common nearest neighbour
+// turns clockwise, -1 if anticlockwise, 0 if no such neighbour exists.
+__device__ int haldane_chirality(const int32_t* layer, int32_t mn, const int32_t* nneigh, const int32_t* nlist,
+                                 const double* neighd, double aG, int64_t i, int jn)
+{
+    const double* dij = neighd + 3 * (i * mn + jn);
+    const double acc = aG / sqrt(3.0);
+    const int32_t target = nlist[i * mn + jn];
+    for (int k1 = 0; k1 < nneigh[i]; ++k1) {
+        const int64_t k = nlist[i * mn + k1] - 1;
+        if (layer[k] != layer[i]) continue;
+        const double* d1 = neighd + 3 * (i * mn + k1);
+        if (fabs(sqrt(d1[0] * d1[0] + d1[1] * d1[1]) - acc) > 0.1) continue;
+        for (int k2 = 0; k2 < nneigh[k]; ++k2) {
+            if (nlist[k * mn + k2] != target) continue;
+            const double* d2 = neighd + 3 * (k * mn + k2);
+            if (fabs(sqrt(d2[0] * d2[0] + d2[1] * d2[1]) - acc) > 0.1) continue;
+            const double ex = d1[0] + d2[0] - dij[0], ey = d1[1] + d2[1] - dij[1];
+            if (sqrt(ex * ex + ey * ey) > 0.1) continue;
+            const double cr = d1[0] * d2[1] - d1[1] * d2[0];
+            return cr < 0.0 ? 1 : -1;
+        }
+    }
+    return 0;
+}
+
+// HamHopHaldane (ham.F90:7043-7142): second-neighbour bonds (|d - aG| < 0.1 Ang, same layer, graphene
+// species) get + t2 exp(i nu phase), or with the paper orientation are multiplied by exp(i nu phase).
+__global__ void k_haldane(int64_t n, const int32_t* species, const int32_t* layer, int32_t mn, const int32_t* nneigh,
+                          const int32_t* nlist, const double* neighd, double aG, double t2, double phase, int paper,
+                          uint32_t mask, double2* hopp, unsigned long long* missing)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (mask != 0u && (layer[i] < 1 || layer[i] > 32 || !((mask >> (layer[i] - 1)) & 1u))) return;
+    for (int j = 0; j < nneigh[i]; ++j) {
+        const int64_t e = i * mn + j;
+        const int64_t jj = nlist[e] - 1;
+        if (layer[jj] != layer[i]) continue;
+        const double dx = neighd[3 * e], dy = neighd[3 * e + 1];
+        const double d = sqrt(dx * dx + dy * dy);
+        if (!((d - 0.1) < aG && (d + 0.1) > aG && species[i] <= 2)) continue;
+        const int nu = haldane_chirality(layer, mn, nneigh, nlist, neighd, aG, i, j);
+        if (nu == 0) {
+            atomicAdd(missing, 1ull);
+            continue;
+        }
+        double sn, cs;
+        sincos(nu * phase, &sn, &cs);
+        const double2 h = hopp[e];
+        hopp[e] = paper ? make_double2(h.x * cs - h.y * sn, h.x * sn + h.y * cs)
+                        : make_double2(h.x + t2 * cs, h.y + t2 * sn);
+    }
+}
+
+int haldane(gbn_ctx* c, double aG, double t2, double phase, int32_t paper, uint32_t layer_mask)
+{
+    if (!c->have_ham || !c->have_neighd || !c->have_geometry)
+        return fail(c, GBN_ERR_STATE, "the Haldane term needs the geometry, NeighD and a Hamiltonian");
+    DevBuf cnt;
+    GBN_CK(c, cnt.ensure(sizeof(unsigned long long)));
+    GBN_CK(c, cudaMemsetAsync(cnt.p, 0, sizeof(unsigned long long), c->stream));
+    const unsigned grd = (unsigned)((c->n + 127) / 128);
+    k_haldane<<<grd, 128, 0, c->stream>>>(c->n, c->species.as<int32_t>(), c->layer.as<int32_t>(), c->max_neigh,
+                                          c->nneigh.as<int32_t>(), c->nlist.as<int32_t>(), c->neighd.as<double>(), aG,
+                                          t2, phase, paper, layer_mask, c->hopp.as<double2>(),
+                                          cnt.as<unsigned long long>());
+    GBN_CK_LAUNCH(c);
+    unsigned long long missing = 0;
+    GBN_CK(c, cudaMemcpyAsync(&missing, cnt.p, sizeof missing, cudaMemcpyDeviceToHost, c->stream));
+    GBN_CK(c, cudaStreamSynchronize(c->stream));
+    c->ham_complex = true;
+    c->has_field = true;   // not a field-free Hamiltonian any more (batched fields would drop the term)
+    c->ell.valid = false;
+    if (missing)
+        return fail(c, GBN_ERR_NUMERIC, std::to_string(missing) + " second-neighbour bonds have no common nearest "
+                                        "neighbour: their chirality is undefined (not a honeycomb lattice?)");
+    return GBN_OK;
+}
+
 }  // namespace gbn

@@ -248,6 +248,11 @@ public:
             die("input key " + name + ": " + e.what());
         }
     }
+    int count(const std::string& name) const
+    {
+        std::string v;
+        return find(name, &v) ? (int)split_ws(v).size() : 0;
+    }
     long i(const std::string& name, long def, int elem = 0) const
     {
         const double v = d(name, (double)def, elem);
@@ -297,6 +302,12 @@ struct Job {
     bool field_by_value = false, field_steps_by_value = false;
     double b_value = 0, b_init = 0, b_final = 0, b_step = 0;
     std::string prefix;
+    // Haldane term (HamHopHaldane, ham.F90:7043-7142) and its phase sweep (HaldPhaseInit, magf.F90:148-211)
+    bool haldane = false, hal_paper = false, hal_opposite = false, hal_setfluxq = false;
+    int hal_mode = 0;            // 0 none, 1 Haldane.SpecifyFlux, 2 SpecifyPhase, 3 SpecifyRange
+    double hal_t2 = 0.0, hal_flux = 0.0, hal_phase = 0.0;   // t2 in g0
+    uint32_t hal_mask = 0;       // Haldane.LayerControl: bit l-1 = layer l of HaldaneLayers
+    long mphii = 0, mphif = 0, mphistep = 1;
     bool write_data = false;    // Output.WriteDataFiles
     bool read_data = false;     // Output.ReadDataFiles
     bool read_details = false;  // Neigh.ReadDetails
@@ -400,6 +411,37 @@ Job job_from_input(const Input& in)
     j.nwr = (int)in.i("Kubo.WriteNumberofSteps", 10);
     j.dt = in.d("Kubo.TimeStep", 5.0);
     if (j.npol < 1 || j.nt < 0 || j.nwr < 1) die("Kubo.NumberofPolynomials and Kubo.WriteNumberofSteps must be positive");
+    j.haldane = in.l("Haldane.NNN", false);
+    j.hal_paper = in.l("Haldane.PaperOrientation", false);
+    j.hal_opposite = in.l("Haldane.OppositePhase", false);
+    j.hal_t2 = in.d("Haldane.T2", 0.0) / g0;   // HamInputEnergyEV: eV in, g0 units
+    if (in.l("Haldane.SpecifyFlux", false)) {
+        j.hal_mode = 1;
+        j.hal_flux = in.d("Haldane.Flux", 0.0);
+        j.hal_setfluxq = in.l("Haldane.SetFluxQ", false);
+    } else if (in.l("Haldane.SpecifyPhase", false)) {
+        j.hal_mode = 2;
+        j.hal_phase = in.d("Haldane.Phase", 0.0);
+    } else if (in.l("Haldane.SpecifyRange", false)) {
+        j.hal_mode = 3;
+        j.mphii = in.i("HaldPhase.InitialInteger", 0);
+        j.mphif = in.i("HaldPhase.FinalInteger", 0);
+        if (j.mphii == j.mphif && j.mphii != 0)
+            die("Haldane.SpecifyRange: HaldPhase.InitialInteger = HaldPhase.FinalInteger divides the phase step by zero");
+        if (j.mphii > j.mphif) die("Haldane.SpecifyRange: HaldPhase.InitialInteger is above HaldPhase.FinalInteger");
+    }
+    if (j.mphii != 0 || j.mphif != 0) {
+        j.mphistep = in.i("HaldPhase.Step", 1);
+        if (j.mphistep <= 0) j.mphistep = 1;
+    }
+    if (in.l("Haldane.LayerControl", false) && in.has("HaldaneLayers")) {
+        for (int k = 0; k < in.count("HaldaneLayers") && k < 32; ++k) {
+            const long l = in.i("HaldaneLayers", -1, k);
+            if (l < 1 || l > 32) die("HaldaneLayers: layers are numbered 1..32");
+            j.hal_mask |= 1u << (l - 1);
+        }
+        if (j.hal_mask == 0) j.hal_mask = 0x80000000u;   // a list of no layer: the term is applied nowhere
+    }
     j.write_data = in.l("Output.WriteDataFiles", false);
     j.read_data = in.l("Output.ReadDataFiles", false);
     j.read_details = in.l("Neigh.ReadDetails", false);
@@ -519,7 +561,8 @@ void print_job(const Job& j)
            "\"height\": %.17g, \"d_interlayer\": %.17g, \"g0\": %.17g, \"cut2intra\": %.17g, \"cut2inter\": %.17g, "
            "\"second_layer\": %d, \"moire\": %d, \"nrecurs\": %d, \"eta\": %.17g, \"n_en\": %d, \"emin\": %.17g, "
            "\"emax\": %.17g, \"seed\": %d, \"prefix\": \"%s\", \"only_dos\": %d, \"npol\": %d, \"nt\": %d, "
-           "\"nwr\": %d, \"dt\": %.17g, \"pdos_mode\": %d, \"seed_set\": %d, \"model\": {\"tbnn\": %d, \"intralayer\": %d, "
+           "\"nwr\": %d, \"dt\": %.17g, \"pdos_mode\": %d, \"seed_set\": %d, \"haldane\": %d, \"hal_t2\": %.17g, "
+           "\"hal_mode\": %d, \"mphi\": [%ld, %ld, %ld], \"model\": {\"tbnn\": %d, \"intralayer\": %d, "
            "\"moire_onsite\": %d, \"moire_offdiag\": %d, \"moire_mid\": %d, \"moire_twisted\": %d, \"eps\": %.17g, "
            "\"twist_rad\": %.17g, \"C0\": %.17g, \"Cz\": %.17g, \"Cab\": %.17g, \"interlayer\": %d, "
            "\"vpppi0\": %.17g, \"vppsigma0\": %.17g, \"bl_delta\": %.17g, \"anderson\": %d, \"anderson_w\": %.17g, "
@@ -527,7 +570,7 @@ void print_job(const Job& j)
            j.cell.kind, j.cell.aG, j.cell.cell_size, j.cell.super_cell, j.cell.m[0], j.cell.m[1], j.cell.m[2], j.cell.m[3],
            j.cell.height, j.cell.d_interlayer, j.g0, j.cut2intra, j.cut2inter, (int)j.second_layer, (int)j.moire,
            j.nrecurs, j.eta, j.n_en, j.emin, j.emax, j.seed, j.prefix.c_str(), (int)j.only_dos, j.npol, j.nt, j.nwr,
-           j.dt, j.pdos.mode, j.seed_set, m.tbnn, m.intralayer, m.moire_onsite,
+           j.dt, j.pdos.mode, j.seed_set, (int)j.haldane, j.hal_t2, j.hal_mode, j.mphii, j.mphif, j.mphistep, m.tbnn, m.intralayer, m.moire_onsite,
            m.moire_offdiag, m.moire_mid, m.moire_twisted, m.eps, m.twist_rad, m.C0, m.Cz, m.Cab, m.interlayer,
            m.vpppi0, m.vppsigma0, m.bl_delta, m.anderson, m.anderson_w, m.tksl[2], m.koshino_sr,
            m.renormalize_coupling, m.coupling_factor);
@@ -958,7 +1001,8 @@ int run(const Job& j0)
     ck(gbn_rng_uniform(j.seed, n, u.data()), nullptr, "gbn_rng_uniform");
     const bool magfield = !(j.mbi == 0 && j.mbf == 0);
     std::vector<double> a((size_t)j.nrecurs), b((size_t)j.nrecurs), psi;
-    if (magfield && j.mbi != j.mbf && j.pdos.mode == 0 && j.only_dos && !j.read_data && !j.write_data) {
+    if (magfield && j.mbi != j.mbf && j.pdos.mode == 0 && j.only_dos && !j.read_data && !j.write_data && !j.haldane &&
+        j.mphii == j.mphif) {
         // a DOS-only sweep: all fields in one batch from the field-free Hamiltonian, each field's Peierls
         // phases applied on the fly (the reference reseeds, so every field starts from the same vector)
         std::vector<int32_t> fm;
@@ -989,7 +1033,9 @@ int run(const Job& j0)
         gbn_destroy(ctx);
         return 0;
     }
-    for (long mb = j.mbi; mb <= j.mbf; mb += (magfield ? j.mstep : 1)) {
+    const bool hsweep = j.mphii != j.mphif;   // HaldPhaseInit: a Haldane phase sweep
+    for (long mb = j.mbi; mb <= j.mbf; mb += (magfield ? j.mstep : 1))
+    for (long mphi = j.mphii; mphi <= j.mphif; mphi += j.mphistep) {
         std::string prefix = j.prefix;
         if (magfield && j.mbi != j.mbf) {
             const double bmag = mb * kFluxQuantum / (area * 1.0e-20);
@@ -999,6 +1045,20 @@ int run(const Job& j0)
             prefix = std::string("./") + folder + "/" + j.prefix;
             printf("grabnes: field %ld of %ld..%ld, %.5f T, files in %s\n", mb, j.mbi, j.mbf, bmag, folder);
         }
+        // HaldPhaseValue (magf.F90:213-250): the phase of step mphi, and its folder (named like a field's)
+        double hphase = 0.0;
+        if (j.hal_mode == 1) hphase = j.hal_setfluxq ? 2.0 * kPi * j.hal_flux / 1.0471975512 : 2.0 * kPi * j.hal_flux / kFluxQuantum;
+        else if (j.hal_mode == 2) hphase = j.hal_phase;
+        else if (j.hal_mode == 3 && hsweep) hphase = 1.0 / (double)(j.mphif - j.mphii) * (double)mphi * 2.0 * kPi;
+        if (hsweep) {
+            char folder[64];
+            snprintf(folder, sizeof folder, "m%05ld_B%.4f", mphi, hphase);
+            if (mkdir(folder, 0755) != 0 && errno != EEXIST) die(std::string("cannot create folder ") + folder);
+            prefix = std::string("./") + folder + "/" + j.prefix;
+            printf("grabnes: Haldane phase step %ld of %ld..%ld, %.6f rad, files in %s\n", mphi, j.mphii, j.mphif, hphase,
+                   folder);
+        }
+        if (j.hal_opposite) hphase = -hphase;
         if (j.read_data) {   // the hoppings of generate.s for every field, then its phases
             ck(gbn_load_hamiltonian(ctx, n, tab.maxn, tab.nn.data(), tab.nl.data(), tab.hop.data(), tab.h0.data()), ctx,
                "gbn_load_hamiltonian");
@@ -1013,6 +1073,7 @@ int run(const Job& j0)
             const double bmag = mb * kFluxQuantum / (area * 1.0e-20);
             ck(gbn_peierls(ctx, bmag * kPi / kFluxQuantum), ctx, "gbn_peierls");
         }
+        if (j.haldane) ck(gbn_haldane(ctx, j.cell.aG, j.hal_t2, hphase, j.hal_paper ? 1 : 0, j.hal_mask), ctx, "gbn_haldane");
         if (j.write_data && !j.read_data) write_ham_files(ctx, prefix, n, maxn, rat_now, species, layer, ucell.data());
         bool any = true;
         if (j.pdos.mode == 0) {   // KuboInitWF + KuboDOS
@@ -1032,7 +1093,7 @@ int run(const Job& j0)
             if (any) time_evolution(ctx, j, psi, a, b, prefix, n);
             else printf("grabnes: the PDOS selection is empty: no time evolution\n");
         }
-        if (!magfield) break;
+        if (!magfield && !hsweep) break;
     }
     gbn_destroy(ctx);
     return 0;

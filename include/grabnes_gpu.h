@@ -144,6 +144,14 @@ int gbn_get_neighbours(gbn_ctx* ctx, int32_t* nneigh, int32_t* nlist, double* ne
  * the reference's fractional/Cartesian round trips); uniform holds the N Anderson draws (or NULL). */
 int gbn_assemble(gbn_ctx* ctx, const gbn_model* model, const double* rat_onsite,
                  const double* rat_hop, const double* uniform);
+/* HamHopHaldane (ham.F90:7043-7142, chirality HamHaldaneChirality ham.F90:13063-13100), after
+ * gbn_peierls as in HamHopping: every second-neighbour bond within a layer (|d - aG| < 0.1 Ang,
+ * Species 1 or 2) gets + t2 exp(i nu phase), or, with paper != 0, is multiplied by exp(i nu phase);
+ * nu = +1 / -1 for a clockwise / anticlockwise path through the common nearest neighbour.  t2 in g0,
+ * phase in rad (Haldane.OppositePhase already applied); layer_mask bit l-1 selects layer l
+ * (Haldane.LayerControl), 0 = every layer.  Needs NeighD (gbn_neighbours or gbn_set_neighd).
+ * GBN_ERR_NUMERIC if a bond has no common nearest neighbour (the reference stops there too). */
+int gbn_haldane(gbn_ctx* ctx, double aG, double t2, double phase, int32_t paper, uint32_t layer_mask);
 /* neighCell(3,maxNeigh,N) of a neighbour list loaded with gbn_load_hamiltonian, so that gbn_peierls can
  * act on loaded hoppings, with the positions of gbn_set_geometry (the Output.ReadDataFiles path of
  * CalcKubo, calc.F90:86-104: hoppings read from a file, then HamPeierlsPeriodicGauge). */

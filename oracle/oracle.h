@@ -108,6 +108,13 @@ void orc_hopping(const orc_model* m, int64_t n, const double* Rat,
                  const int32_t* species, const int32_t* layer,
                  int32_t maxNeigh, const int32_t* Nneigh, const int32_t* NList,
                  const double* NeighD, double* hopp);
+/* HamHopHaldane (ham.F90:7043-7142) with HamHaldaneChirality (ham.F90:13063-13100), after the
+ * Peierls phases: second-neighbour bonds within a layer get + t2 exp(i nu phase) (paper: times
+ * exp(i nu phase)); layer_mask bit l-1 enables layer l (0 = every layer).  Returns the number of
+ * bonds without a common nearest neighbour (the reference stops on any). */
+int64_t orc_haldane(int64_t n, const int32_t* species, const int32_t* layer, int32_t maxNeigh,
+                    const int32_t* Nneigh, const int32_t* NList, const double* NeighD, double aG, double t2,
+                    double phase, int32_t paper, uint32_t layer_mask, double* hopp);
 void orc_peierls(int64_t n, const double* Rat, const double* ucell,
                  int32_t maxNeigh, const int32_t* Nneigh, const int32_t* NList,
                  const int32_t* neighCell, double flux, double* hopp);

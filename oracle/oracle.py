@@ -80,6 +80,9 @@ def _declare(L):
     L.orc_onsite.argtypes = [C.POINTER(Model), i64, _p(np.float64), _p(np.int32), _p(np.int32), _p(np.float64)]
     L.orc_hopping.argtypes = [C.POINTER(Model), i64, _p(np.float64), _p(np.int32), _p(np.int32), i32,
                               _p(np.int32), _p(np.int32), _p(np.float64), _p(np.complex128)]
+    L.orc_haldane.argtypes = [i64, _p(np.int32), _p(np.int32), i32, _p(np.int32), _p(np.int32), _p(np.float64), C.c_double,
+                              C.c_double, C.c_double, i32, C.c_uint32, _p(np.float64)]
+    L.orc_haldane.restype = i64
     L.orc_peierls.argtypes = [i64, _p(np.float64), _p(np.float64), i32, _p(np.int32), _p(np.int32),
                               _p(np.int32), d, _p(np.complex128)]
     L.orc_init_wf.argtypes = [i64, i32, _p(np.complex128)]
@@ -162,6 +165,17 @@ def hopping(model, rat, species, layer, nb):
                       nb["nneigh"], np.ascontiguousarray(nb["nlist"]).reshape(-1),
                       np.ascontiguousarray(nb["neighd"]).reshape(-1), hop)
     return hop.reshape(n, mx)
+
+
+def haldane(species, layer, nb, aG, t2, phase, hop, paper=False, layer_mask=0):
+    """HamHopHaldane on the hoppings (returns the new hoppings and the bonds without a chirality)."""
+    n = len(nb["nneigh"])
+    h = np.ascontiguousarray(hop, np.complex128).reshape(-1).copy()
+    miss = lib().orc_haldane(n, np.ascontiguousarray(species, np.int32), np.ascontiguousarray(layer, np.int32),
+                             nb["max_neigh"], nb["nneigh"], np.ascontiguousarray(nb["nlist"]).reshape(-1),
+                             np.ascontiguousarray(nb["neighd"]).reshape(-1), aG, t2, phase, int(paper), layer_mask,
+                             h.view(np.float64))
+    return h.reshape(n, nb["max_neigh"]), miss
 
 
 def peierls(rat, ucell, nb, flux, hop):

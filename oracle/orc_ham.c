@@ -239,3 +239,62 @@ void orc_peierls(int64_t n, const double* Rat, const double* ucell, int32_t maxN
         }
     }
 }
+
+/* HamHaldaneChirality, ham.F90:13063-13100: +1 if the path i -> k -> j through a common nearest
+ * neighbour turns clockwise, -1 if anticlockwise, 0 if there is none. */
+static int haldane_chirality(const int32_t* layer, int32_t maxNeigh, const int32_t* Nneigh, const int32_t* NList,
+                             const double* NeighD, double aG, int64_t i, int jn)
+{
+    const double* dij = NeighD + 3 * ((size_t)i * maxNeigh + jn);
+    const double acc = aG / sqrt(3.0);
+    for (int k1 = 0; k1 < Nneigh[i]; ++k1) {
+        const int64_t k = NList[(size_t)i * maxNeigh + k1] - 1;
+        if (layer[k] != layer[i]) continue;
+        const double* d1 = NeighD + 3 * ((size_t)i * maxNeigh + k1);
+        if (fabs(sqrt(d1[0] * d1[0] + d1[1] * d1[1]) - acc) > 0.1) continue;
+        for (int k2 = 0; k2 < Nneigh[k]; ++k2) {
+            if (NList[(size_t)k * maxNeigh + k2] != NList[(size_t)i * maxNeigh + jn]) continue;
+            const double* d2 = NeighD + 3 * ((size_t)k * maxNeigh + k2);
+            if (fabs(sqrt(d2[0] * d2[0] + d2[1] * d2[1]) - acc) > 0.1) continue;
+            const double ex = d1[0] + d2[0] - dij[0], ey = d1[1] + d2[1] - dij[1];
+            if (sqrt(ex * ex + ey * ey) > 0.1) continue;
+            const double cr = d1[0] * d2[1] - d1[1] * d2[0];
+            return cr < 0.0 ? 1 : -1;
+        }
+    }
+    return 0;
+}
+
+int64_t orc_haldane(int64_t n, const int32_t* species, const int32_t* layer, int32_t maxNeigh,
+                    const int32_t* Nneigh, const int32_t* NList, const double* NeighD, double aG, double t2,
+                    double phase, int32_t paper, uint32_t layer_mask, double* hopp)
+{
+    int64_t missing = 0;
+    for (int64_t i = 0; i < n; ++i) {
+        if (layer_mask != 0u && (layer[i] < 1 || layer[i] > 32 || !((layer_mask >> (layer[i] - 1)) & 1u))) continue;
+        for (int j = 0; j < Nneigh[i]; ++j) {
+            const size_t e = (size_t)i * maxNeigh + j;
+            const int64_t jj = NList[e] - 1;
+            if (layer[jj] != layer[i]) continue;
+            const double* D = NeighD + 3 * e;
+            const double d = sqrt(D[0] * D[0] + D[1] * D[1]);
+            if (!((d - 0.1) < aG && (d + 0.1) > aG && species[i] <= 2)) continue;
+            const int nu = haldane_chirality(layer, maxNeigh, Nneigh, NList, NeighD, aG, i, j);
+            if (nu == 0) {
+                ++missing;
+                continue;
+            }
+            const double c = cos(nu * phase), s = sin(nu * phase);
+            double* h = hopp + 2 * e;
+            if (paper) {
+                const double re = h[0] * c - h[1] * s, im = h[0] * s + h[1] * c;
+                h[0] = re;
+                h[1] = im;
+            } else {
+                h[0] = h[0] + t2 * c;
+                h[1] = h[1] + t2 * s;
+            }
+        }
+    }
+    return missing;
+}
