@@ -100,7 +100,7 @@ EXPORTS = ["gbn_cell_atoms", "gbn_build_cell", "gbn_cart_roundtrip", "gbn_rng_un
            "gbn_peierls", "gbn_get_hamiltonian", "gbn_load_hamiltonian", "gbn_lanczos", "gbn_lanczos_phases",
            "gbn_stage_phases", "gbn_run_staged", "gbn_cf_dos", "gbn_cheb_evolve", "gbn_kubo_evol", "gbn_set_neighd", "gbn_lanczos_noalloc",
            "gbn_cheb_interval", "gbn_cheb_coef", "gbn_dos_gradient", "gbn_lanczos_sites", "gbn_lanczos_sets",
-           "gbn_pdos_atoms", "gbn_pdos_sets", "gbn_lanczos_fields", "gbn_set_images", "gbn_haldane"]
+           "gbn_pdos_atoms", "gbn_pdos_sets", "gbn_lanczos_fields", "gbn_set_images", "gbn_haldane", "gbn_kubo_tevol"]
 
 
 def _declare(L):
@@ -150,6 +150,8 @@ def _declare(L):
     L.gbn_kubo_evol.argtypes = [vp, i32, i32, _p(np.complex128), i32, d, d, i32, _p(np.complex128),
                                 _p(np.complex128)]
     L.gbn_set_neighd.argtypes = [vp, _p(np.float64)]
+    L.gbn_kubo_tevol.argtypes = [vp, i32, i32, _p(np.complex128), i32, d, d, i32, i32, i32, i32, _p(np.complex128),
+                                 _p(np.complex128), _opt(np.float64), _opt(np.float64), _opt(np.float64)]
     L.gbn_cheb_interval.argtypes = [_p(np.float64), _p(np.float64), i32, C.POINTER(d), C.POINTER(d)]
     L.gbn_dos_gradient.argtypes = [vp, C.POINTER(Model), d, _p(np.float64), i32, i32, d, i32, d, d, _p(np.float64),
                                    C.POINTER(d), _p(np.float64), _opt(np.float64), _opt(np.float64), _opt(np.float64)]
@@ -269,6 +271,19 @@ class Context:
     def haldane(self, aG, t2, phase, paper=False, layer_mask=0):
         """HamHopHaldane on the current hoppings (after peierls): t2 in g0, phase in rad."""
         self._ck(self._L.gbn_haldane(self._h, aG, t2, phase, int(paper), layer_mask))
+
+    def kubo_tevol(self, c, ac, bc, psi, zupsi, nt, nwr, nrecurs, direction=1, precision=GBN_FP64):
+        """KuboTEvol on the device: returns (psi, zupsi, norms [nrhs, nt//nwr], a, b [nrhs, nt//nwr, nrecurs])."""
+        p = np.ascontiguousarray(np.atleast_2d(psi), np.complex128).copy()
+        z = np.ascontiguousarray(np.atleast_2d(zupsi), np.complex128).copy()
+        nrhs, nw = p.shape[0], nt // nwr
+        norms = np.zeros((nrhs, max(nw, 1)))
+        a = np.zeros((nrhs, max(nw, 1), nrecurs))
+        b = np.zeros((nrhs, max(nw, 1), nrecurs))
+        cc = _c(c, np.complex128)
+        self._ck(self._L.gbn_kubo_tevol(self._h, precision, nrhs, cc, len(cc), ac, bc, direction, nt, nwr, nrecurs,
+                                        p.reshape(-1), z.reshape(-1), norms.reshape(-1), a.reshape(-1), b.reshape(-1)))
+        return p, z, norms[:, :nw], a[:, :nw], b[:, :nw]
 
     def set_images(self, ncell):
         """neighCell of the loaded neighbour list (for peierls after load_hamiltonian)."""

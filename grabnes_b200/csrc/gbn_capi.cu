@@ -691,6 +691,21 @@ int gbn_kubo_evol(gbn_ctx* c, int32_t precision, int32_t nrhs, const double* coe
     return kubo_evol(c, precision, nrhs, coef, npol, ac, bc, dir, psi, zupsi);
 }
 
+int gbn_kubo_tevol(gbn_ctx* c, int32_t precision, int32_t nrhs, const double* coef, int32_t npol, double ac, double bc,
+                   int32_t dir, int32_t nt, int32_t nwr, int32_t nrecurs, double* psi, double* zupsi, double* norms,
+                   double* a, double* b)
+{
+    if (!c) return GBN_ERR_ARG;
+    if (!c->have_ham) return fail(c, GBN_ERR_STATE, "no Hamiltonian");
+    if (precision != GBN_FP64 && precision != GBN_MIXED) return fail(c, GBN_ERR_ARG, "bad precision");
+    if (nrhs < 1 || npol < 1 || !coef || !psi || !zupsi || !(bc > 0.0) || !isfinite(ac) || nt < 0 || nwr < 1 ||
+        nrecurs < 1)
+        return fail(c, GBN_ERR_ARG, "bad KuboTEvol arguments");
+    if (nt / nwr > 0 && (!norms || !a || !b)) return fail(c, GBN_ERR_ARG, "NULL output arrays");
+    cudaSetDevice(c->device);
+    return kubo_tevol(c, precision, nrhs, coef, npol, ac, bc, dir, nt, nwr, nrecurs, psi, zupsi, norms, a, b);
+}
+
 int gbn_dos_gradient(gbn_ctx* c, const gbn_model* model, double g0, const double* u, int32_t nrecurs, int32_t checkpoint,
                      double eta, int32_t n_en, double emin, double emax, const double* target, double* loss, double* grad,
                      double* dos, double* a, double* b)

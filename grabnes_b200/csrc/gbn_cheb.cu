@@ -151,6 +151,60 @@ static int tile_width(int nrhs)
     return t;
 }
 
+// One tile of the Chebyshev propagation z <- U z: zin (device, [cnt][n] complex128, reference order) in
+// and out; c->cheb[0] holds the accumulator, c->vec[1], c->vec[2] the recurrence.  *ms: device time of
+// the polynomial loop.
+static int cheb_tile(gbn_ctx* c, int prec, ChebFn fn, int grid, int T, int cnt, const double* c_host, int npol,
+                     double ac, double bc, double2* zin, int64_t* launches, float* ms)
+{
+    const int64_t n = c->n, npad = c->ell.npad;
+    double2* z = c->cheb[0].as<double2>();
+    const int32_t* rp = c->ell.rperm.as<int32_t>();
+    const int blk = 256;
+    const unsigned sgrid = (unsigned)((npad * T + blk - 1) / blk);
+    const unsigned fgrid = (unsigned)((n * T + blk - 1) / blk);
+    void* bufA = c->vec[1].p;   // psi_n
+    void* bufB = c->vec[2].p;   // psi_{n-1}, then psi_{n+1}
+    if (prec == GBN_MIXED)
+        k_cheb_start<float><<<sgrid, blk, 0, c->stream>>>(static_cast<float2*>(bufA), static_cast<float2*>(bufB), z,
+                                                           zin, rp, n, npad, T, cnt, c_host[0], c_host[1]);
+    else
+        k_cheb_start<double><<<sgrid, blk, 0, c->stream>>>(static_cast<double2*>(bufA), static_cast<double2*>(bufB),
+                                                            z, zin, rp, n, npad, T, cnt, c_host[0], c_host[1]);
+    GBN_CK_LAUNCH(c);
+    if (!c->ev0) {
+        GBN_CK(c, cudaEventCreate(&c->ev0));
+        GBN_CK(c, cudaEventCreate(&c->ev1));
+    }
+    GBN_CK(c, cudaEventRecord(c->ev0, c->stream));
+    ChebParams p;
+    p.slice_ptr = c->ell.slice_ptr.as<int64_t>();
+    p.mat = c->ell.mat.as<unsigned char>();
+    p.entry_bytes = c->ell.entry_bytes;
+    p.h0 = c->ell.h0.p;
+    p.z = z;
+    p.ac = ac;
+    p.nslices = c->ell.nslices;
+    for (int k = 1; k < npol; ++k) {
+        p.psi_n = bufA;
+        p.psi_out = bufB;
+        p.cr = c_host[2 * k];
+        p.ci = c_host[2 * k + 1];
+        p.alpha = (k == 1) ? 1.0 / (2.0 * bc) : 1.0 / bc;
+        p.beta = (k == 1) ? 0.0 : 1.0;
+        fn<<<grid, 256, 0, c->stream>>>(p);
+        GBN_CK_LAUNCH(c);
+        std::swap(bufA, bufB);
+        ++*launches;
+    }
+    GBN_CK(c, cudaEventRecord(c->ev1, c->stream));
+    k_cheb_finish<<<fgrid, blk, 0, c->stream>>>(z, zin, rp, n, T, cnt);
+    GBN_CK_LAUNCH(c);
+    GBN_CK(c, cudaEventSynchronize(c->ev1));
+    GBN_CK(c, cudaEventElapsedTime(ms, c->ev0, c->ev1));
+    return GBN_OK;
+}
+
 int cheb_evolve(gbn_ctx* c, int32_t prec, int32_t nrhs, const double* c_host, int32_t npol, double ac, double bc,
                 double* z_host)
 {
@@ -175,11 +229,6 @@ int cheb_evolve(gbn_ctx* c, int32_t prec, int32_t nrhs, const double* c_host, in
     GBN_CK(c, c->cheb[0].ensure(sizeof(double2) * (size_t)npad * T));
     GBN_CK(c, c->cheb[1].ensure(sizeof(double2) * (size_t)n * T));
     c->staged = false;   // the recursion's staged start vectors were laid out for another tile
-    double2* z = c->cheb[0].as<double2>();
-    const int32_t* rp = c->ell.rperm.as<int32_t>();
-    const int blk = 256;
-    const unsigned sgrid = (unsigned)((npad * T + blk - 1) / blk);
-    const unsigned fgrid = (unsigned)((n * T + blk - 1) / blk);
     int64_t launches = 0;
     float ms_total = 0.f;
     for (int r0 = 0; r0 < nrhs; r0 += T) {
@@ -187,48 +236,12 @@ int cheb_evolve(gbn_ctx* c, int32_t prec, int32_t nrhs, const double* c_host, in
         double2* zin = c->cheb[1].as<double2>();
         GBN_CK(c, cudaMemcpyAsync(zin, z_host + (size_t)2 * n * r0, sizeof(double2) * (size_t)n * cnt,
                                   cudaMemcpyHostToDevice, c->stream));
-        void* bufA = c->vec[1].p;   // psi_n
-        void* bufB = c->vec[2].p;   // psi_{n-1}, then psi_{n+1}
-        if (prec == GBN_MIXED)
-            k_cheb_start<float><<<sgrid, blk, 0, c->stream>>>(static_cast<float2*>(bufA), static_cast<float2*>(bufB), z,
-                                                               zin, rp, n, npad, T, cnt, c_host[0], c_host[1]);
-        else
-            k_cheb_start<double><<<sgrid, blk, 0, c->stream>>>(static_cast<double2*>(bufA), static_cast<double2*>(bufB),
-                                                                z, zin, rp, n, npad, T, cnt, c_host[0], c_host[1]);
-        GBN_CK_LAUNCH(c);
-        if (!c->ev0) {
-            GBN_CK(c, cudaEventCreate(&c->ev0));
-            GBN_CK(c, cudaEventCreate(&c->ev1));
-        }
-        GBN_CK(c, cudaEventRecord(c->ev0, c->stream));
-        ChebParams p;
-        p.slice_ptr = c->ell.slice_ptr.as<int64_t>();
-        p.mat = c->ell.mat.as<unsigned char>();
-        p.entry_bytes = c->ell.entry_bytes;
-        p.h0 = c->ell.h0.p;
-        p.z = z;
-        p.ac = ac;
-        p.nslices = c->ell.nslices;
-        for (int k = 1; k < npol; ++k) {
-            p.psi_n = bufA;
-            p.psi_out = bufB;
-            p.cr = c_host[2 * k];
-            p.ci = c_host[2 * k + 1];
-            p.alpha = (k == 1) ? 1.0 / (2.0 * bc) : 1.0 / bc;
-            p.beta = (k == 1) ? 0.0 : 1.0;
-            fn<<<grid, 256, 0, c->stream>>>(p);
-            GBN_CK_LAUNCH(c);
-            std::swap(bufA, bufB);
-            ++launches;
-        }
-        GBN_CK(c, cudaEventRecord(c->ev1, c->stream));
-        k_cheb_finish<<<fgrid, blk, 0, c->stream>>>(z, zin, rp, n, T, cnt);
-        GBN_CK_LAUNCH(c);
+        float ms = 0.f;
+        rc = cheb_tile(c, prec, fn, grid, T, cnt, c_host, npol, ac, bc, zin, &launches, &ms);
+        if (rc) return rc;
         GBN_CK(c, cudaMemcpyAsync(z_host + (size_t)2 * n * r0, zin, sizeof(double2) * (size_t)n * cnt,
                                   cudaMemcpyDeviceToHost, c->stream));
         GBN_CK(c, cudaStreamSynchronize(c->stream));
-        float ms = 0.f;
-        GBN_CK(c, cudaEventElapsedTime(&ms, c->ev0, c->ev1));
         ms_total += ms;
     }
     c->timing.step_ms = ms_total;
@@ -487,6 +500,86 @@ static int build_dvals(gbn_ctx* c, int dir)
     return GBN_OK;
 }
 
+// One tile of KuboEvol's dual recurrence: pin, zin (device, [cnt][n] complex128, reference order) hold psi
+// and zupsi (already propagated by U) in and psi <- U psi, zupsi <- zupsi + [U, X] psi out.
+static int dual_tile(gbn_ctx* c, int prec, DualFn fn, int grid, int T, int cnt, const double* c_host, int npol,
+                     double ac, double bc, double2* pin, double2* zin, int64_t* launches)
+{
+    const int64_t n = c->n, npad = c->ell.npad;
+    double2* pacc = c->cheb[0].as<double2>();
+    double2* zacc = c->cheb[2].as<double2>();
+    const int32_t* rp = c->ell.rperm.as<int32_t>();
+    const int blk = 256;
+    const unsigned sgrid = (unsigned)((npad * T + blk - 1) / blk);
+    const unsigned fgrid = (unsigned)((n * T + blk - 1) / blk);
+    void* pA = c->vec[1].p;
+    void* pB = c->vec[2].p;
+    void* xA = c->cheb[3].p;
+    void* xB = c->cheb[4].p;
+    if (prec == GBN_MIXED)
+        k_dual_start<float><<<sgrid, blk, 0, c->stream>>>(static_cast<float2*>(pA), static_cast<float2*>(pB),
+                                                           static_cast<float2*>(xA), static_cast<float2*>(xB), pacc,
+                                                           zacc, pin, zin, rp, n, npad, T, cnt, c_host[0], c_host[1]);
+    else
+        k_dual_start<double><<<sgrid, blk, 0, c->stream>>>(static_cast<double2*>(pA), static_cast<double2*>(pB),
+                                                            static_cast<double2*>(xA), static_cast<double2*>(xB), pacc,
+                                                            zacc, pin, zin, rp, n, npad, T, cnt, c_host[0], c_host[1]);
+    GBN_CK_LAUNCH(c);
+    DualParams p;
+    p.slice_ptr = c->ell.slice_ptr.as<int64_t>();
+    p.mat = c->ell.mat.as<unsigned char>();
+    p.dval = c->ell.dval.p;
+    p.entry_bytes = c->ell.entry_bytes;
+    p.h0 = c->ell.h0.p;
+    p.pacc = pacc;
+    p.zacc = zacc;
+    p.ac = ac;
+    p.nslices = c->ell.nslices;
+    for (int k = 1; k < npol; ++k) {
+        p.psi_n = pA;
+        p.x_n = xA;
+        p.psi_out = pB;
+        p.x_out = xB;
+        p.cr = c_host[2 * k];
+        p.ci = c_host[2 * k + 1];
+        p.alpha = (k == 1) ? 1.0 / (2.0 * bc) : 1.0 / bc;
+        p.beta = (k == 1) ? 0.0 : 1.0;
+        fn<<<grid, 256, 0, c->stream>>>(p);
+        GBN_CK_LAUNCH(c);
+        std::swap(pA, pB);
+        std::swap(xA, xB);
+        ++*launches;
+    }
+    k_cheb_finish<<<fgrid, blk, 0, c->stream>>>(pacc, pin, rp, n, T, cnt);
+    GBN_CK_LAUNCH(c);
+    k_cheb_finish<<<fgrid, blk, 0, c->stream>>>(zacc, zin, rp, n, T, cnt);
+    GBN_CK_LAUNCH(c);
+    return GBN_OK;
+}
+
+// Kernels and buffers of KuboEvol for a tile of T right-hand sides (after cheb_evolve's preparation).
+static int dual_prepare(gbn_ctx* c, int prec, int T, int dir, DualFn* fn, int* grid)
+{
+    int rpt, tpr;
+    split_rhs(prec, T, c->tune_rpt, &rpt, &tpr);
+    int rc = build_dvals(c, dir);
+    if (rc) return rc;
+    if (prec == GBN_MIXED) *fn = c->ell.cplx ? pick_dual<float, true>(c->ell.G, rpt, tpr)
+                                             : pick_dual<float, false>(c->ell.G, rpt, tpr);
+    else *fn = c->ell.cplx ? pick_dual<double, true>(c->ell.G, rpt, tpr) : pick_dual<double, false>(c->ell.G, rpt, tpr);
+    if (!*fn) return fail(c, GBN_ERR_ARG, "no KuboEvol kernel for this tile width");
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, *fn, 256, 0) != cudaSuccess || per_sm < 1) per_sm = 1;
+    *grid = c->num_sms * per_sm;
+    const int64_t npad = c->ell.npad;
+    const size_t esz = (prec == GBN_MIXED) ? sizeof(float2) : sizeof(double2);
+    GBN_CK(c, c->cheb[0].ensure(sizeof(double2) * (size_t)npad * T));   // psi accumulator (Z of U as well)
+    GBN_CK(c, c->cheb[2].ensure(sizeof(double2) * (size_t)npad * T));   // zupsi accumulator
+    GBN_CK(c, c->cheb[3].ensure(esz * (size_t)npad * T));              // X_n
+    GBN_CK(c, c->cheb[4].ensure(esz * (size_t)npad * T));              // X_{n-1}
+    return GBN_OK;
+}
+
 int kubo_evol(gbn_ctx* c, int32_t prec, int32_t nrhs, const double* c_host, int32_t npol, double ac, double bc,
               int32_t dir, double* psi_host, double* zupsi_host)
 {
@@ -496,87 +589,168 @@ int kubo_evol(gbn_ctx* c, int32_t prec, int32_t nrhs, const double* c_host, int3
     int rc = cheb_evolve(c, prec, nrhs, c_host, npol, ac, bc, zupsi_host);
     if (rc) return rc;
     const int T = tile_width(nrhs);   // the layout cheb_evolve prepared
-    int rpt, tpr;
-    split_rhs(prec, T, c->tune_rpt, &rpt, &tpr);
-    rc = build_dvals(c, dir);
-    if (rc) return rc;
     DualFn fn;
-    if (prec == GBN_MIXED) fn = c->ell.cplx ? pick_dual<float, true>(c->ell.G, rpt, tpr)
-                                            : pick_dual<float, false>(c->ell.G, rpt, tpr);
-    else fn = c->ell.cplx ? pick_dual<double, true>(c->ell.G, rpt, tpr) : pick_dual<double, false>(c->ell.G, rpt, tpr);
-    if (!fn) return fail(c, GBN_ERR_ARG, "no KuboEvol kernel for this tile width");
-    int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 256, 0) != cudaSuccess || per_sm < 1) per_sm = 1;
-    const int grid = c->num_sms * per_sm;
-    const int64_t n = c->n, npad = c->ell.npad;
-    const size_t esz = (prec == GBN_MIXED) ? sizeof(float2) : sizeof(double2);
-    GBN_CK(c, c->cheb[0].ensure(sizeof(double2) * (size_t)npad * T));   // psi accumulator
-    GBN_CK(c, c->cheb[2].ensure(sizeof(double2) * (size_t)npad * T));   // zupsi accumulator
-    GBN_CK(c, c->cheb[3].ensure(esz * (size_t)npad * T));              // X_n
-    GBN_CK(c, c->cheb[4].ensure(esz * (size_t)npad * T));              // X_{n-1}
+    int grid;
+    rc = dual_prepare(c, prec, T, dir, &fn, &grid);
+    if (rc) return rc;
+    const int64_t n = c->n;
     GBN_CK(c, c->cheb[1].ensure(sizeof(double2) * (size_t)n * T));     // psi in / out
     GBN_CK(c, c->cheb[5].ensure(sizeof(double2) * (size_t)n * T));     // zupsi in / out
-    double2* pacc = c->cheb[0].as<double2>();
-    double2* zacc = c->cheb[2].as<double2>();
     double2* pin = c->cheb[1].as<double2>();
     double2* zin = c->cheb[5].as<double2>();
-    const int32_t* rp = c->ell.rperm.as<int32_t>();
-    const int blk = 256;
-    const unsigned sgrid = (unsigned)((npad * T + blk - 1) / blk);
-    const unsigned fgrid = (unsigned)((n * T + blk - 1) / blk);
+    int64_t launches = 0;
     for (int r0 = 0; r0 < nrhs; r0 += T) {
         const int cnt = std::min(T, nrhs - r0);
         GBN_CK(c, cudaMemcpyAsync(pin, psi_host + (size_t)2 * n * r0, sizeof(double2) * (size_t)n * cnt,
                                   cudaMemcpyHostToDevice, c->stream));
         GBN_CK(c, cudaMemcpyAsync(zin, zupsi_host + (size_t)2 * n * r0, sizeof(double2) * (size_t)n * cnt,
                                   cudaMemcpyHostToDevice, c->stream));
-        void* pA = c->vec[1].p;
-        void* pB = c->vec[2].p;
-        void* xA = c->cheb[3].p;
-        void* xB = c->cheb[4].p;
-        if (prec == GBN_MIXED)
-            k_dual_start<float><<<sgrid, blk, 0, c->stream>>>(static_cast<float2*>(pA), static_cast<float2*>(pB),
-                                                               static_cast<float2*>(xA), static_cast<float2*>(xB), pacc,
-                                                               zacc, pin, zin, rp, n, npad, T, cnt, c_host[0], c_host[1]);
-        else
-            k_dual_start<double><<<sgrid, blk, 0, c->stream>>>(static_cast<double2*>(pA), static_cast<double2*>(pB),
-                                                                static_cast<double2*>(xA), static_cast<double2*>(xB), pacc,
-                                                                zacc, pin, zin, rp, n, npad, T, cnt, c_host[0], c_host[1]);
-        GBN_CK_LAUNCH(c);
-        DualParams p;
-        p.slice_ptr = c->ell.slice_ptr.as<int64_t>();
-        p.mat = c->ell.mat.as<unsigned char>();
-        p.dval = c->ell.dval.p;
-        p.entry_bytes = c->ell.entry_bytes;
-        p.h0 = c->ell.h0.p;
-        p.pacc = pacc;
-        p.zacc = zacc;
-        p.ac = ac;
-        p.nslices = c->ell.nslices;
-        for (int k = 1; k < npol; ++k) {
-            p.psi_n = pA;
-            p.x_n = xA;
-            p.psi_out = pB;
-            p.x_out = xB;
-            p.cr = c_host[2 * k];
-            p.ci = c_host[2 * k + 1];
-            p.alpha = (k == 1) ? 1.0 / (2.0 * bc) : 1.0 / bc;
-            p.beta = (k == 1) ? 0.0 : 1.0;
-            fn<<<grid, 256, 0, c->stream>>>(p);
-            GBN_CK_LAUNCH(c);
-            std::swap(pA, pB);
-            std::swap(xA, xB);
-        }
-        k_cheb_finish<<<fgrid, blk, 0, c->stream>>>(pacc, pin, rp, n, T, cnt);
-        GBN_CK_LAUNCH(c);
-        k_cheb_finish<<<fgrid, blk, 0, c->stream>>>(zacc, zin, rp, n, T, cnt);
-        GBN_CK_LAUNCH(c);
+        rc = dual_tile(c, prec, fn, grid, T, cnt, c_host, npol, ac, bc, pin, zin, &launches);
+        if (rc) return rc;
         GBN_CK(c, cudaMemcpyAsync(psi_host + (size_t)2 * n * r0, pin, sizeof(double2) * (size_t)n * cnt,
                                   cudaMemcpyDeviceToHost, c->stream));
         GBN_CK(c, cudaMemcpyAsync(zupsi_host + (size_t)2 * n * r0, zin, sizeof(double2) * (size_t)n * cnt,
                                   cudaMemcpyDeviceToHost, c->stream));
         GBN_CK(c, cudaStreamSynchronize(c->stream));
     }
+    return GBN_OK;
+}
+
+// |z_r|^2 of a [cnt][n] complex128 block: per-block partial sums (fixed order), then their sum per r
+__global__ void k_norm_parts(const double2* z, int64_t n, int cnt, int parts, double* out)
+{
+    const int r = blockIdx.x / parts, part = blockIdx.x % parts;
+    if (r >= cnt) return;
+    const int64_t per = (n + parts - 1) / parts, lo = part * per, hi = (lo + per < n) ? lo + per : n;
+    double s = 0.0;
+    for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+        const double2 v = z[(int64_t)r * n + i];
+        s += v.x * v.x + v.y * v.y;
+    }
+    __shared__ double sh[256];
+    sh[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[(int64_t)r * parts + part] = sh[0];
+}
+
+__global__ void k_norm_sum(const double* parts_in, int parts, int cnt, double* norm)
+{
+    const int r = threadIdx.x;
+    if (r >= cnt) return;
+    double s = 0.0;
+    for (int k = 0; k < parts; ++k) s += parts_in[(int64_t)r * parts + k];
+    norm[r] = s;
+}
+
+// out_r = z_r / sqrt(norm_r) (the normalised ZUPsi of KuboTEvol), in [cnt][n] layout
+__global__ void k_normalise(const double2* z, const double* norm, int64_t n, int cnt, double2* out)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n * cnt) return;
+    const int r = (int)(i / n);
+    const double s = sqrt(fabs(norm[r]));
+    out[i] = make_double2(z[i].x / s, z[i].y / s);
+}
+
+// KuboTEvol (kubo.F90:321-397) with psi and zupsi resident on the device: nt steps of KuboEvol; after every
+// nwr-th step the norm |zupsi|^2 and the recursion of zupsi / |zupsi| (nrecurs steps).  psi and zupsi
+// are read at the start and written back at the end; norms [nrhs][nt/nwr], a, b [nrhs][nt/nwr][nrecurs].
+int kubo_tevol(gbn_ctx* c, int32_t prec, int32_t nrhs, const double* c_host, int32_t npol, double ac, double bc,
+               int32_t dir, int32_t nt, int32_t nwr, int32_t nrecurs, double* psi_host, double* zupsi_host,
+               double* norms, double* a_out, double* b_out)
+{
+    if (!c->have_neighd) return fail(c, GBN_ERR_STATE, "KuboEvol needs NeighD (gbn_neighbours or gbn_set_neighd)");
+    if (dir != 1 && dir != 2) return fail(c, GBN_ERR_ARG, "dir must be 1 (x) or 2 (y)");
+    const int T = tile_width(nrhs);
+    int rc = lanczos_prepare(c, prec, T);
+    if (rc) return rc;
+    c->staged = false;
+    int rpt, tpr;
+    split_rhs(prec, T, c->tune_rpt, &rpt, &tpr);
+    ChebFn cfn;
+    if (prec == GBN_MIXED) cfn = c->ell.cplx ? pick_cheb<float, true>(c->ell.G, rpt, tpr)
+                                             : pick_cheb<float, false>(c->ell.G, rpt, tpr);
+    else cfn = c->ell.cplx ? pick_cheb<double, true>(c->ell.G, rpt, tpr) : pick_cheb<double, false>(c->ell.G, rpt, tpr);
+    if (!cfn) return fail(c, GBN_ERR_ARG, "no Chebyshev kernel for this tile width");
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cfn, 256, 0) != cudaSuccess || per_sm < 1) per_sm = 1;
+    const int cgrid = c->num_sms * per_sm;
+    DualFn dfn;
+    int dgrid;
+    rc = dual_prepare(c, prec, T, dir, &dfn, &dgrid);
+    if (rc) return rc;
+    const int64_t n = c->n;
+    const int nw = nt / nwr;
+    const int parts = 256;
+    GBN_CK(c, c->cheb[6].ensure(sizeof(double2) * (size_t)n * T));   // psi state
+    GBN_CK(c, c->cheb[7].ensure(sizeof(double2) * (size_t)n * T));   // zupsi state
+    GBN_CK(c, c->upload.ensure(sizeof(double2) * (size_t)n * T));    // normalised zupsi
+    DevBuf part_buf, norm_buf;
+    GBN_CK(c, part_buf.ensure(sizeof(double) * (size_t)T * parts));
+    GBN_CK(c, norm_buf.ensure(sizeof(double) * (size_t)T));
+    double2* pin = c->cheb[6].as<double2>();
+    double2* zin = c->cheb[7].as<double2>();
+    std::vector<double> hn((size_t)T), hab;
+    int64_t launches = 0;
+    double loop_ms = 0.0;
+    for (int r0 = 0; r0 < nrhs; r0 += T) {
+        const int cnt = std::min(T, nrhs - r0);
+        GBN_CK(c, cudaMemcpyAsync(pin, psi_host + (size_t)2 * n * r0, sizeof(double2) * (size_t)n * cnt,
+                                  cudaMemcpyHostToDevice, c->stream));
+        GBN_CK(c, cudaMemcpyAsync(zin, zupsi_host + (size_t)2 * n * r0, sizeof(double2) * (size_t)n * cnt,
+                                  cudaMemcpyHostToDevice, c->stream));
+        int w = 0;
+        for (int it = 1; it <= nt; ++it) {
+            float ms = 0.f;
+            rc = cheb_tile(c, prec, cfn, cgrid, T, cnt, c_host, npol, ac, bc, zin, &launches, &ms);   // zupsi <- U zupsi
+            if (rc) return rc;
+            rc = dual_tile(c, prec, dfn, dgrid, T, cnt, c_host, npol, ac, bc, pin, zin, &launches);
+            if (rc) return rc;
+            if (it % nwr != 0 || w >= nw) continue;
+            k_norm_parts<<<(unsigned)(cnt * parts), 256, 0, c->stream>>>(zin, n, cnt, parts, part_buf.as<double>());
+            GBN_CK_LAUNCH(c);
+            k_norm_sum<<<1, 32, 0, c->stream>>>(part_buf.as<double>(), parts, cnt, norm_buf.as<double>());
+            GBN_CK_LAUNCH(c);
+            GBN_CK(c, cudaMemcpyAsync(hn.data(), norm_buf.p, sizeof(double) * cnt, cudaMemcpyDeviceToHost, c->stream));
+            GBN_CK(c, cudaStreamSynchronize(c->stream));
+            bool all_pos = true;
+            for (int r = 0; r < cnt; ++r) all_pos = all_pos && hn[(size_t)r] > 0.0;
+            for (int r = 0; r < cnt; ++r) norms[(size_t)(r0 + r) * nw + w] = hn[(size_t)r];
+            if (all_pos) {
+                const unsigned g = (unsigned)((n * cnt + 255) / 256);
+                k_normalise<<<g, 256, 0, c->stream>>>(zin, norm_buf.as<double>(), n, cnt, c->upload.as<double2>());
+                GBN_CK_LAUNCH(c);
+                rc = lanczos_start_from_psi(c, c->upload.as<double>(), cnt);
+                if (rc) return rc;
+                rc = lanczos_run(c, nrecurs);
+                if (rc) return rc;
+                loop_ms += c->timing.step_ms;
+                hab.resize((size_t)2 * T * nrecurs);
+                GBN_CK(c, cudaMemcpyAsync(hab.data(), c->ab.p, sizeof(double) * hab.size(), cudaMemcpyDeviceToHost,
+                                          c->stream));
+                GBN_CK(c, cudaStreamSynchronize(c->stream));
+            }
+            for (int r = 0; r < cnt; ++r) {
+                double* ao = a_out + ((size_t)(r0 + r) * nw + w) * nrecurs;
+                double* bo = b_out + ((size_t)(r0 + r) * nw + w) * nrecurs;
+                for (int k = 0; k < nrecurs; ++k) {
+                    ao[k] = all_pos ? hab[(size_t)r * nrecurs + k] : NAN;
+                    bo[k] = all_pos ? hab[(size_t)T * nrecurs + (size_t)r * nrecurs + k] : NAN;
+                }
+            }
+            ++w;
+        }
+        GBN_CK(c, cudaMemcpyAsync(psi_host + (size_t)2 * n * r0, pin, sizeof(double2) * (size_t)n * cnt,
+                                  cudaMemcpyDeviceToHost, c->stream));
+        GBN_CK(c, cudaMemcpyAsync(zupsi_host + (size_t)2 * n * r0, zin, sizeof(double2) * (size_t)n * cnt,
+                                  cudaMemcpyDeviceToHost, c->stream));
+        GBN_CK(c, cudaStreamSynchronize(c->stream));
+    }
+    c->timing.step_launches = launches;
     return GBN_OK;
 }
 

@@ -210,6 +210,9 @@ int cheb_evolve(gbn_ctx* c, int32_t prec, int32_t nrhs, const double* c_host, in
                 double* z_host);
 int kubo_evol(gbn_ctx* c, int32_t prec, int32_t nrhs, const double* c_host, int32_t npol, double ac, double bc,
               int32_t dir, double* psi_host, double* zupsi_host);
+int kubo_tevol(gbn_ctx* c, int32_t prec, int32_t nrhs, const double* c_host, int32_t npol, double ac, double bc,
+               int32_t dir, int32_t nt, int32_t nwr, int32_t nrecurs, double* psi_host, double* zupsi_host,
+               double* norms, double* a_out, double* b_out);
 
 inline int grid_for(gbn_ctx* c, int blocks_per_sm) { return c->num_sms * blocks_per_sm; }
 

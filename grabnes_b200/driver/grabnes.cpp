@@ -604,24 +604,27 @@ void time_evolution(gbn_ctx* ctx, const Job& j, std::vector<double> psi, const s
     }
     write_pairs(prefix + ".cn.dat", re, ab, 0.0, false);
     if (j.only_dos) return;
-    std::vector<double> zu((size_t)2 * n, 0.0), zn((size_t)2 * n);
-    std::vector<double> az((size_t)j.nrecurs), bz((size_t)j.nrecurs), energy((size_t)j.n_en + 1), dos((size_t)j.n_en + 1);
-    for (int it = 1; it <= j.nt; ++it) {
-        ck(gbn_kubo_evol(ctx, GBN_FP64, 1, c.data(), j.npol, ac, bc, 1, psi.data(), zu.data()), ctx, "gbn_kubo_evol");
-        if (it % j.nwr != 0) continue;
-        double norm = 0.0;
-        for (int64_t i = 0; i < 2 * n; ++i) norm += zu[(size_t)i] * zu[(size_t)i];
+    // all nT steps on the device (gbn_kubo_tevol); the files of every nWr-th step from its coefficients
+    std::vector<double> zu((size_t)2 * n, 0.0);
+    const int nw = j.nt / j.nwr;
+    std::vector<double> norms((size_t)std::max(nw, 1)), az((size_t)std::max(nw, 1) * j.nrecurs),
+        bz((size_t)std::max(nw, 1) * j.nrecurs), energy((size_t)j.n_en + 1), dos((size_t)j.n_en + 1);
+    ck(gbn_kubo_tevol(ctx, GBN_FP64, 1, c.data(), j.npol, ac, bc, 1, j.nt, j.nwr, j.nrecurs, psi.data(), zu.data(),
+                      norms.data(), az.data(), bz.data()),
+       ctx, "gbn_kubo_tevol");
+    for (int w = 0; w < nw; ++w) {
+        const int it = (w + 1) * j.nwr;
+        double norm = norms[(size_t)w];
         if (!(norm > 0.0)) continue;
-        const double s = 1.0 / sqrt(norm);
-        for (int64_t i = 0; i < 2 * n; ++i) zn[(size_t)i] = zu[(size_t)i] * s;
-        ck(gbn_lanczos(ctx, GBN_FP64, 1, zn.data(), nullptr, j.nrecurs, az.data(), bz.data()), ctx, "gbn_lanczos");
-        ck(gbn_cf_dos(ctx, 1, az.data(), bz.data(), nullptr, j.nrecurs, j.eta, j.n_en, j.emin, j.emax, &norm,
+        std::vector<double> aw(az.begin() + (size_t)w * j.nrecurs, az.begin() + (size_t)(w + 1) * j.nrecurs);
+        std::vector<double> bw(bz.begin() + (size_t)w * j.nrecurs, bz.begin() + (size_t)(w + 1) * j.nrecurs);
+        ck(gbn_cf_dos(ctx, 1, aw.data(), bw.data(), nullptr, j.nrecurs, j.eta, j.n_en, j.emin, j.emax, &norm,
                       energy.data(), dos.data()),
            ctx, "gbn_cf_dos");
         char tag[32];
         snprintf(tag, sizeof tag, "%04d", it);
         write_pairs(prefix + ".Z2_" + tag + ".dat", energy, dos, 0.0, false);
-        write_pairs(prefix + ".AB_" + tag + ".dat", az, bz, norm, true);
+        write_pairs(prefix + ".AB_" + tag + ".dat", aw, bw, norm, true);
         printf("grabnes: time step %d of %d, |ZUPsi|^2 = %.10g\n", it, j.nt, norm);
     }
 }

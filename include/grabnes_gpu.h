@@ -279,6 +279,14 @@ int gbn_cheb_evolve(gbn_ctx* ctx, int32_t precision, int32_t nrhs, const double*
  * gbn_neighbours or NeighD through gbn_set_neighd.  precision as for gbn_cheb_evolve. */
 int gbn_kubo_evol(gbn_ctx* ctx, int32_t precision, int32_t nrhs, const double* c, int32_t npol, double ac,
                   double bc, int32_t dir, double* psi, double* zupsi);
+/* KuboTEvol (kubo.F90:321-397) with psi and zupsi kept on the device: nt steps of gbn_kubo_evol; after
+ * every nwr-th step, norms[r][w] = |zupsi_r|^2 and a, b [r][w][nrecurs] = the FP64-reduced recursion of
+ * zupsi_r / |zupsi_r| (w = 0 .. nt/nwr - 1; NaN where a norm is 0).  psi, zupsi [nrhs][N] complex are
+ * read at the start and hold the evolved states on return.  Host traffic: the states once each way and
+ * the coefficients, instead of both states every step. */
+int gbn_kubo_tevol(gbn_ctx* ctx, int32_t precision, int32_t nrhs, const double* c, int32_t npol, double ac,
+                   double bc, int32_t dir, int32_t nt, int32_t nwr, int32_t nrecurs, double* psi, double* zupsi,
+                   double* norms, double* a, double* b);
 /* NeighD(3,maxNeigh,N) for gbn_kubo_evol after gbn_load_hamiltonian. */
 int gbn_set_neighd(gbn_ctx* ctx, const double* neighd);
 
