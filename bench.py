@@ -137,6 +137,12 @@ def run_ours(args, ws, rank, local):
 
     torch.cuda.set_device(local)
     stream = torch.cuda.Stream()
+    if args.tevol_only:   # the time evolution alone (profiling of its kernels)
+        out = tevol_leg(G, M, local, stream, ws)
+        if rank == 0:
+            print(json.dumps(out), flush=True)
+        replicas.finish(ws)
+        return
     if args.fields_only:   # the batched-field sweep alone (profiling of its kernels)
         out = fields_leg(G, M, local, stream, ws, args.fields_scale)
         if rank == 0:
@@ -254,6 +260,10 @@ def run_ours(args, ws, rank, local):
     fields = None
     if not args.no_fields:
         fields = fields_leg(G, M, local, stream, ws)
+    # ---- Chebyshev Kubo time evolution (graphene/hBN 0.61 degrees, Anderson disorder)
+    tevol = None
+    if not args.no_tevol:
+        tevol = tevol_leg(G, M, local, stream, ws)
 
     out = {
         "metric": METRIC, "value": value, "unit": "atom-steps/s", "n_gpus": ws, "steps": args.steps,
@@ -276,7 +286,7 @@ def run_ours(args, ws, rank, local):
         "dos_error_vs_fp64": {"l1_mean_dos": dos_err, "l1_worst_vector": dos_err_per_vector,
                               "eta_ev": ETA_EV, "energies": NE + 1},
         "cpu_baseline": cpu, "clocks": clk, "gpu_launches": launches, "setup_s": setup_s,
-        "fields_batch": fields,
+        "fields_batch": fields, "kubo_time_evolution": tevol,
     }
     if rank == 0:
         print(json.dumps(out), flush=True)
@@ -351,6 +361,68 @@ def fields_leg(G, M, local, stream, ws, scale=1.0):
             "speedup_vs_per_field": t_field / t_batch, "precision": "mixed"}
 
 
+TEVOL_KEYS = {"Run.TypeOfSystem": "Graphene", "Structure.CellSize": 83, "Structure.SuperCell": 16,
+              "Moire.LatticePercent": -0.018016854251615, "Moire.Twisted": True, "Moire.TwistAngle": 0.608806541588,
+              "Moire.Potential": True, "Moire.Jeil": True, "Moire.H0AndHZ": True, "Moire.OffDiag": True,
+              "Moire.OffDiagMidpoint": True, "Disorder.Anderson": True, "Disorder.AndersonAmp": 1.0,
+              "Kubo.SeedValue": 5}
+HBAR_EV_S = 6.582119569e-16
+
+
+def tevol_leg(G, M, local, stream, ws, nt=10, npol=100, nvec=8, nrecurs=100):
+    """Chebyshev Kubo time evolution of graphene on hBN at 0.61 degrees (example 07's cell, CellSize 83,
+    SuperCell 16 = 3,527,168 atoms) with Anderson disorder W = 1 eV (seed 5): dt = 1 fs (g0 dt / hbar),
+    KuboCn with the reference's default 100 polynomials, 8 random-phase vectors, mixed precision; nt of
+    the workload's 1000 steps, one recursion of the commutator state at the end.  gbn_kubo_tevol (states
+    resident on the device) against the same steps through gbn_kubo_evol with the states on the host
+    every step.  Work unit: an atom-polynomial step of the dual recurrence (N x vectors x (npol - 1) per
+    time step); each time step also propagates zupsi by U (as many single products)."""
+    import torch
+    job = M.job_from_keys(TEVOL_KEYS)
+    ctx = G.Context(local)
+    ctx.set_stream(stream.cuda_stream)
+    cell = M.setup(ctx, job)
+    n = cell["n"]
+    g0 = job["g0"]
+    dt = 1.0e-15 * g0 / HBAR_EV_S
+    u = G.rng_uniform(5, nvec * n).reshape(nvec, n)
+    psi = np.exp(2j * np.pi * u) / np.sqrt(n)
+    a, b = ctx.lanczos_phases(u[:1], 200, G.GBN_MIXED)
+    ac, bc = G.cheb_interval(a[0], b[0])
+    c = G.cheb_coef(dt, ac, bc, npol)
+    zero = np.zeros_like(psi)
+    ctx.kubo_tevol(c, ac, bc, psi, zero, 1, 1, 10, 1, G.GBN_MIXED)   # warm-up (layout, kernels)
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        r = fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return r, dist_max(e0.elapsed_time(e1), ws) / 1e3
+
+    (p1, z1, nrm, _, _), t_dev = timed(lambda: ctx.kubo_tevol(c, ac, bc, psi, zero, nt, nt, nrecurs, 1, G.GBN_MIXED))
+
+    def host_loop():
+        p, z = psi, zero
+        for _ in range(nt):
+            p, z = ctx.kubo_evol(c, ac, bc, p, z, direction=1, precision=G.GBN_MIXED)
+        nz = np.sum(np.abs(z) ** 2, axis=1)
+        ctx.lanczos(z / np.sqrt(nz)[:, None], nrecurs, G.GBN_MIXED)
+        return nz
+
+    nz, t_host = timed(host_loop)
+    ctx.close()
+    work = float(n) * nvec * (npol - 1) * nt
+    return {"workload": "graphene_hbn_0.61deg_anderson_3527168atoms_8vec_dt1fs", "atoms": n, "vectors": nvec,
+            "npol": npol, "time_steps": nt, "dt_g0_over_hbar": dt, "atom_poly_steps": work,
+            "device_resident_s": t_dev, "device_resident_atom_poly_steps_per_s": ws * work / t_dev,
+            "host_states_s": t_host, "host_states_atom_poly_steps_per_s": ws * work / t_host,
+            "speedup_vs_host_states": t_host / t_dev,
+            "norm_rel_diff": float(np.abs(nrm[:, 0] - nz).max() / np.abs(nz).max()), "precision": "mixed"}
+
+
 def cpu_baseline(ctx, n, u0, steps):
     """The oracle port of KuboRecursion (reference data layout, complex128, three passes per step)."""
     from oracle import oracle as orc
@@ -422,6 +494,8 @@ def main():
     p.add_argument("--value-only", action="store_true", help="time the device-resident jobs only (profiling)")
     p.add_argument("--no-fields", action="store_true", help="skip the batched-field sweep (graphene/hBN, 33 fields)")
     p.add_argument("--fields-only", action="store_true", help="run the batched-field sweep alone")
+    p.add_argument("--no-tevol", action="store_true", help="skip the Chebyshev Kubo time evolution leg")
+    p.add_argument("--tevol-only", action="store_true", help="run the Chebyshev Kubo time evolution leg alone")
     p.add_argument("--fields-scale", type=float, default=1.0, help="scale of the sweep's recursion lengths (profiling)")
     p.add_argument("--tuning", default="", help="fixed kernel tuning 'rhs_per_thread,blocks_per_sm,rows_per_group,staged,prefetch' "
                                                 "instead of the autotuner")
