@@ -137,6 +137,12 @@ def run_ours(args, ws, rank, local):
 
     torch.cuda.set_device(local)
     stream = torch.cuda.Stream()
+    if args.gradient_only:
+        out = gradient_leg(G, M, local, stream, ws)
+        if rank == 0:
+            print(json.dumps(out), flush=True)
+        replicas.finish(ws)
+        return
     if args.tevol_only:   # the time evolution alone (profiling of its kernels)
         out = tevol_leg(G, M, local, stream, ws)
         if rank == 0:
@@ -264,6 +270,9 @@ def run_ours(args, ws, rank, local):
     tevol = None
     if not args.no_tevol:
         tevol = tevol_leg(G, M, local, stream, ws)
+    grad = None
+    if not args.no_gradient:
+        grad = gradient_leg(G, M, local, stream, ws)
 
     out = {
         "metric": METRIC, "value": value, "unit": "atom-steps/s", "n_gpus": ws, "steps": args.steps,
@@ -286,7 +295,7 @@ def run_ours(args, ws, rank, local):
         "dos_error_vs_fp64": {"l1_mean_dos": dos_err, "l1_worst_vector": dos_err_per_vector,
                               "eta_ev": ETA_EV, "energies": NE + 1},
         "cpu_baseline": cpu, "clocks": clk, "gpu_launches": launches, "setup_s": setup_s,
-        "fields_batch": fields, "kubo_time_evolution": tevol,
+        "fields_batch": fields, "kubo_time_evolution": tevol, "dos_gradient": grad,
     }
     if rank == 0:
         print(json.dumps(out), flush=True)
@@ -423,6 +432,50 @@ def tevol_leg(G, M, local, stream, ws, nt=10, npol=100, nvec=8, nrecurs=100):
             "norm_rel_diff": float(np.abs(nrm[:, 0] - nz).max() / np.abs(nz).max()), "precision": "mixed"}
 
 
+GRAD_KEYS = {"Run.TypeOfSystem": "TwistedBilayerBasedOnMoireCell", "Structure.MoireCellParameters": (32, 31, 31, 32),
+             "Structure.SuperCell": 9, "Interlayer.TypeOfBL": "Koshino", "Interlayer.Vpppi0": 2.7,
+             "Interlayer.Vppsigma0": 0.48, "Interlayer.BLdelta": 0.319, "Neigh.LayerNeighbors": 100,
+             "Neigh.LayerDistFactor": 3.2005, "TB.Hopping": 2.7, "Kubo.SeedValue": 3}
+
+
+def gradient_leg(G, M, local, stream, ws, nrecurs=600, checkpoint=32):
+    """Gradient of a DOS loss of twisted bilayer graphene at 1.05 degrees (cell 32 31 31 32 tiled 9 x 9 =
+    964,548 atoms, two-centre interlayer hopping with a smooth cutoff of width 0.5 Ang): L = sum_E (DOS -
+    target)^2, eta = 5 meV, 2001 energies on [-1, 1] eV, target from parameters perturbed by 2 % (seed
+    3), 600 recursion steps (FP64) with checkpoints every 32 steps.  One gbn_dos_gradient (forward sweep,
+    loss and the reverse sweep for dL/d(t, Vpp_sigma0, delta, w)) against the forward recursion alone."""
+    import torch
+    from grabnes_b200 import autograd as AD
+    ctx = G.Context(local)
+    ctx.set_stream(stream.cuda_stream)
+    job = M.job_from_keys(GRAD_KEYS)
+    theta = np.array([2.7, 0.48, 0.319, 0.5])
+    prob = AD.DosProblem(ctx, job, None, nrecurs, 0.005, 2000, -1.0, 1.0, checkpoint=checkpoint)
+    rng = np.random.default_rng(3)
+    _, _, target = prob.evaluate(theta * (1.0 + 0.02 * rng.uniform(-1, 1, 4)))
+    prob.target = target
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        r = fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return r, dist_max(e0.elapsed_time(e1), ws) / 1e3
+
+    (loss, grad, _), t_grad = timed(lambda: prob.evaluate(theta))
+    m = AD.model_with(prob.base, prob.g0, theta)
+    ctx.assemble(m, prob.rat_on, prob.rat_hop, None)
+    _, t_fwd = timed(lambda: ctx.lanczos_phases(prob.u, nrecurs, G.GBN_FP64))
+    n = prob.n
+    ctx.close()
+    return {"workload": "tbg_1.05deg_9x9_964548atoms_600steps_checkpoint32", "atoms": n, "recursion_steps": nrecurs,
+            "checkpoint": checkpoint, "gradient_s": t_grad, "forward_recursion_s": t_fwd,
+            "gradient_over_forward": t_grad / t_fwd, "loss": float(loss), "gradient": [float(x) for x in grad],
+            "precision": "fp64"}
+
+
 def cpu_baseline(ctx, n, u0, steps):
     """The oracle port of KuboRecursion (reference data layout, complex128, three passes per step)."""
     from oracle import oracle as orc
@@ -495,6 +548,8 @@ def main():
     p.add_argument("--no-fields", action="store_true", help="skip the batched-field sweep (graphene/hBN, 33 fields)")
     p.add_argument("--fields-only", action="store_true", help="run the batched-field sweep alone")
     p.add_argument("--no-tevol", action="store_true", help="skip the Chebyshev Kubo time evolution leg")
+    p.add_argument("--no-gradient", action="store_true", help="skip the DOS-gradient leg")
+    p.add_argument("--gradient-only", action="store_true", help="run the DOS-gradient leg alone")
     p.add_argument("--tevol-only", action="store_true", help="run the Chebyshev Kubo time evolution leg alone")
     p.add_argument("--fields-scale", type=float, default=1.0, help="scale of the sweep's recursion lengths (profiling)")
     p.add_argument("--tuning", default="", help="fixed kernel tuning 'rhs_per_thread,blocks_per_sm,rows_per_group,staged,prefetch' "
