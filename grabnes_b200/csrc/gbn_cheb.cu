@@ -29,7 +29,16 @@ struct ChebParams {
     double cr, ci;       // c_{n+1}
     double ac, alpha, beta;   // psi_{n+1} = (H psi_n - ac psi_n) * alpha - beta * psi_{n-1}
     int64_t nslices;
+    double cpr, cpi;     // c_n, when its term is added here (acc 2)
+    int32_t acc;         // accumulator update: 0 none (deferred), 1 z += c_{n+1} psi_{n+1}, 2 z += c_n psi_n first
 };
+
+// z += c psi with psi as stored; both the deferred and the direct terms go through this one expression
+__device__ __forceinline__ void acc_add(double2& z, double cr, double ci, double sr, double si)
+{
+    z.x += cr * sr - ci * si;
+    z.y += cr * si + ci * sr;
+}
 
 template <typename VT, bool CPLX, int G, int RPT, int TPR>
 __global__ void __launch_bounds__(256) k_cheb_step(ChebParams p)
@@ -74,12 +83,15 @@ __global__ void __launch_bounds__(256) k_cheb_step(ChebParams p)
                 const double ni = ((double)y.y - p.ac * (double)own[t].y) * p.alpha - p.beta * (double)prev[t].y;
                 nxt[t].x = (VT)nr;
                 nxt[t].y = (VT)ni;
-                // z += c_{n+1} psi_{n+1}, with psi_{n+1} as stored (what the next step gathers)
-                double2 zz = p.z[e0 + t];
-                const double sr = (double)nxt[t].x, si = (double)nxt[t].y;
-                zz.x += p.cr * sr - p.ci * si;
-                zz.y += p.cr * si + p.ci * sr;
-                p.z[e0 + t] = zz;
+                // z += c_{n+1} psi_{n+1}, with psi_{n+1} as stored (what the next step gathers); every
+                // second step also adds the deferred c_n psi_n (psi_n is this row's own, loaded above),
+                // in the same order, so the accumulator is read and written on every other step only
+                if (p.acc != 0) {
+                    double2 zz = p.z[e0 + t];
+                    if (p.acc == 2) acc_add(zz, p.cpr, p.cpi, (double)own[t].x, (double)own[t].y);
+                    acc_add(zz, p.cr, p.ci, (double)nxt[t].x, (double)nxt[t].y);
+                    p.z[e0 + t] = zz;
+                }
             }
             VecIO<VT, RPT>::store(xo + e0, nxt);
         }
@@ -151,6 +163,24 @@ static int tile_width(int nrhs)
     return t;
 }
 
+// Accumulator schedule of polynomial step k (1 .. npol-1, the step that forms psi_k): the term of an odd
+// k is deferred to step k + 1, which adds c_k psi_k (its own row) before c_{k+1} psi_{k+1}; the last step
+// adds its own term.
+template <typename P>
+static void set_acc(P& p, const double* c_host, int k, int npol)
+{
+    const bool last = k == npol - 1;
+    if (k % 2 == 1 && !last) {
+        p.acc = 0;
+    } else if (k % 2 == 0) {
+        p.acc = 2;
+        p.cpr = c_host[2 * (k - 1)];
+        p.cpi = c_host[2 * (k - 1) + 1];
+    } else {
+        p.acc = 1;
+    }
+}
+
 // One tile of the Chebyshev propagation z <- U z: zin (device, [cnt][n] complex128, reference order) in
 // and out; c->cheb[0] holds the accumulator, c->vec[1], c->vec[2] the recurrence.  *ms: device time of
 // the polynomial loop.
@@ -192,6 +222,7 @@ static int cheb_tile(gbn_ctx* c, int prec, ChebFn fn, int grid, int T, int cnt, 
         p.ci = c_host[2 * k + 1];
         p.alpha = (k == 1) ? 1.0 / (2.0 * bc) : 1.0 / bc;
         p.beta = (k == 1) ? 0.0 : 1.0;
+        set_acc(p, c_host, k, npol);
         fn<<<grid, 256, 0, c->stream>>>(p);
         GBN_CK_LAUNCH(c);
         std::swap(bufA, bufB);
@@ -319,6 +350,8 @@ struct DualParams {
     double2* zacc;       // zupsi accumulator (FP64)
     double cr, ci, ac, alpha, beta;
     int64_t nslices;
+    double cpr, cpi;     // c_n, when its terms are added here (acc 2)
+    int32_t acc;         // as in ChebParams
 };
 
 template <typename VT, bool CPLX, int G, int RPT, int TPR>
@@ -404,14 +437,17 @@ __global__ void __launch_bounds__(256) k_dual_step(DualParams p)
                 np[t].y = (VT)(((double)yp.y - p.ac * (double)ownp[t].y) * p.alpha - p.beta * (double)prevp[t].y);
                 nx[t].x = (VT)(((double)yx.x - p.ac * (double)ownx[t].x) * p.alpha - p.beta * (double)prevx[t].x);
                 nx[t].y = (VT)(((double)yx.y - p.ac * (double)ownx[t].y) * p.alpha - p.beta * (double)prevx[t].y);
-                double2 a1 = p.pacc[e0 + t], a2 = p.zacc[e0 + t];
-                const double pr = (double)np[t].x, pi = (double)np[t].y, xr = (double)nx[t].x, xi = (double)nx[t].y;
-                a1.x += p.cr * pr - p.ci * pi;
-                a1.y += p.cr * pi + p.ci * pr;
-                a2.x += p.cr * xr - p.ci * xi;
-                a2.y += p.cr * xi + p.ci * xr;
-                p.pacc[e0 + t] = a1;
-                p.zacc[e0 + t] = a2;
+                if (p.acc != 0) {   // the accumulators on every other step (see k_cheb_step)
+                    double2 a1 = p.pacc[e0 + t], a2 = p.zacc[e0 + t];
+                    if (p.acc == 2) {
+                        acc_add(a1, p.cpr, p.cpi, (double)ownp[t].x, (double)ownp[t].y);
+                        acc_add(a2, p.cpr, p.cpi, (double)ownx[t].x, (double)ownx[t].y);
+                    }
+                    acc_add(a1, p.cr, p.ci, (double)np[t].x, (double)np[t].y);
+                    acc_add(a2, p.cr, p.ci, (double)nx[t].x, (double)nx[t].y);
+                    p.pacc[e0 + t] = a1;
+                    p.zacc[e0 + t] = a2;
+                }
             }
             VecIO<VT, RPT>::store(po + e0, np);
             VecIO<VT, RPT>::store(xo + e0, nx);
@@ -544,6 +580,7 @@ static int dual_tile(gbn_ctx* c, int prec, DualFn fn, int grid, int T, int cnt, 
         p.ci = c_host[2 * k + 1];
         p.alpha = (k == 1) ? 1.0 / (2.0 * bc) : 1.0 / bc;
         p.beta = (k == 1) ? 0.0 : 1.0;
+        set_acc(p, c_host, k, npol);
         fn<<<grid, 256, 0, c->stream>>>(p);
         GBN_CK_LAUNCH(c);
         std::swap(pA, pB);
