@@ -176,7 +176,7 @@ int build_identity_perm(gbn_ctx* c);
 int build_spatial_perm(gbn_ctx* c);
 // field: the field-batched values (FieldVal: field-free hopping and c->ptau), for gbn_lanczos_fields
 int build_ell(gbn_ctx* c, int prec, int G, int gpw, bool field = false);
-int auto_group(const gbn_ctx* c);
+int auto_group(const gbn_ctx* c, int R);   // default rows per group for a tile of R vectors
 
 // recursion (gbn_lanczos.cu)
 int lanczos_prepare(gbn_ctx* c, int prec, int nrhs, bool field = false);

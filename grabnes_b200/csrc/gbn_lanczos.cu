@@ -255,7 +255,7 @@ int lanczos_prepare(gbn_ctx* c, int prec, int nrhs, bool field)
     int rpt, tpr;
     split_rhs(prec, nrhs, c->tune_rpt, &rpt, &tpr);
     const int gpw = 32 / tpr;
-    const int G = c->tune_group > 0 ? c->tune_group : auto_group(c);
+    const int G = c->tune_group > 0 ? c->tune_group : auto_group(c, nrhs);
     if (!c->ell.valid || c->ell.prec != prec || c->ell.gpw != gpw || c->ell.G != G || c->ell.field != field) {
         const int rc = build_ell(c, prec, G, gpw, field);
         if (rc) return rc;

@@ -301,12 +301,15 @@ __global__ void k_max_record(const int64_t* slice_ptr, int64_t nslices, int64_t 
     if (s < nslices) atomicMax(out, (unsigned long long)((slice_ptr[s + 1] - slice_ptr[s]) * entry_bytes));
 }
 
-// Mean entries per row decide the default group size: the union of a group's columns pays off when
-// neighbouring rows share many columns (bilayers with tens of interlayer neighbours).
-int auto_group(const gbn_ctx* c)
+// Default rows per group from the mean entries per row and the tile width R (measured with the autotuner
+// on B200: graphene-like rows of about 3 entries gather too little per slice with one or two vectors, and
+// groups of 4 rows share their union columns; bilayers with tens of interlayer entries share columns
+// between pairs of rows once several vectors amortise the union's padding).
+int auto_group(const gbn_ctx* c, int R)
 {
     const double per_row = c->n > 0 ? (double)c->total / (double)c->n : 0.0;
-    return per_row >= 8.0 ? 2 : 1;
+    if (per_row < 8.0) return R <= 2 ? 4 : (R <= 4 ? 2 : 1);
+    return R == 1 ? 1 : 2;
 }
 
 int build_ell(gbn_ctx* c, int prec, int G, int gpw, bool field)
