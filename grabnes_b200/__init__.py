@@ -100,7 +100,7 @@ EXPORTS = ["gbn_cell_atoms", "gbn_build_cell", "gbn_cart_roundtrip", "gbn_rng_un
            "gbn_peierls", "gbn_get_hamiltonian", "gbn_load_hamiltonian", "gbn_lanczos", "gbn_lanczos_phases",
            "gbn_stage_phases", "gbn_run_staged", "gbn_cf_dos", "gbn_cheb_evolve", "gbn_kubo_evol", "gbn_set_neighd", "gbn_lanczos_noalloc",
            "gbn_cheb_interval", "gbn_cheb_coef", "gbn_dos_gradient", "gbn_lanczos_sites", "gbn_lanczos_sets",
-           "gbn_pdos_atoms", "gbn_pdos_sets", "gbn_lanczos_fields", "gbn_set_images", "gbn_haldane", "gbn_kubo_tevol"]
+           "gbn_pdos_atoms", "gbn_pdos_sets", "gbn_lanczos_fields", "gbn_set_images", "gbn_haldane", "gbn_kubo_tevol", "gbn_check_hamiltonian"]
 
 
 def _declare(L):
@@ -128,6 +128,7 @@ def _declare(L):
     L.gbn_peierls.argtypes = [vp, d]
     L.gbn_set_images.argtypes = [vp, _p(np.int32)]
     L.gbn_haldane.argtypes = [vp, d, d, d, i32, C.c_uint32]
+    L.gbn_check_hamiltonian.argtypes = [vp, _p(np.int64), C.POINTER(d)]
     L.gbn_get_hamiltonian.argtypes = [vp, _opt(np.float64), _opt(np.complex128)]
     L.gbn_load_hamiltonian.argtypes = [vp, i64, i32, _p(np.int32), _p(np.int32), _p(np.complex128), _p(np.float64)]
     L.gbn_lanczos.argtypes = [vp, i32, i32, _p(np.complex128), _opt(np.int32), i32, _p(np.float64), _p(np.float64)]
@@ -267,6 +268,13 @@ class Context:
         self._ck(self._L.gbn_load_hamiltonian(self._h, n, mx, _c(nneigh, np.int32), _c(nlist, np.int32),
                                               _c(hopp, np.complex128), _c(h0, np.float64)))
         self.n, self.max_neigh = n, mx
+
+    def check_hamiltonian(self):
+        """(non-finite hoppings, non-finite on-site, first atom, entries without reverse, pairs, max asymmetry)"""
+        out = np.zeros(5, np.int64)
+        mx = C.c_double()
+        self._ck(self._L.gbn_check_hamiltonian(self._h, out, C.byref(mx)))
+        return tuple(int(x) for x in out) + (mx.value,)
 
     def haldane(self, aG, t2, phase, paper=False, layer_mask=0):
         """HamHopHaldane on the current hoppings (after peierls): t2 in g0, phase in rad."""

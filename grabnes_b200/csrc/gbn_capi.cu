@@ -371,6 +371,13 @@ int gbn_load_hamiltonian(gbn_ctx* c, int64_t n, int32_t max_neigh, const int32_t
     return GBN_OK;
 }
 
+int gbn_check_hamiltonian(gbn_ctx* c, int64_t* counts, double* max_asym)
+{
+    if (!c || !counts || !max_asym) return GBN_ERR_ARG;
+    cudaSetDevice(c->device);
+    return check_hamiltonian(c, counts, max_asym);
+}
+
 int gbn_haldane(gbn_ctx* c, double aG, double t2, double phase, int32_t paper, uint32_t layer_mask)
 {
     if (!c) return GBN_ERR_ARG;

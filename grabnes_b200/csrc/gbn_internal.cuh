@@ -198,7 +198,8 @@ int neigh_search(gbn_ctx* c, double cut2intra, double cut2inter, int32_t second_
 int assemble(gbn_ctx* c, const gbn_model* m, const double* d_rat_on, const double* d_rat_hop, const double* d_uniform);
 int peierls(gbn_ctx* c, double flux);
 int peierls_turns(gbn_ctx* c);
-int haldane(gbn_ctx* c, double aG, double t2, double phase, int32_t paper, uint32_t layer_mask);   // c->ptau from the positions, images and cell of the assembled model
+int haldane(gbn_ctx* c, double aG, double t2, double phase, int32_t paper, uint32_t layer_mask);
+int check_hamiltonian(gbn_ctx* c, int64_t* out, double* max_asym);   // c->ptau from the positions, images and cell of the assembled model
 
 // gradient of a DOS loss (gbn_adjoint.cu)
 int dos_gradient(gbn_ctx* c, const gbn_model* m, double g0, const double* u_host, int32_t K, int32_t C, double eta,

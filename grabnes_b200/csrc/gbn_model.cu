@@ -10,6 +10,7 @@
 // One thread per atom, FP64; results are in the reference layout hopp(maxNeigh,N).
 #include <cuda_runtime.h>
 #include <math.h>
+#include <string.h>
 
 #include "gbn_internal.cuh"
 
@@ -384,6 +385,78 @@ int haldane(gbn_ctx* c, double aG, double t2, double phase, int32_t paper, uint3
     if (missing)
         return fail(c, GBN_ERR_NUMERIC, std::to_string(missing) + " second-neighbour bonds have no common nearest "
                                         "neighbour: their chirality is undefined (not a honeycomb lattice?)");
+    return GBN_OK;
+}
+
+// HamCheckFinite (ham.F90:4432-4477) and the pair scan of HamCheckHermiticity (ham.F90:4491-4571), one
+// thread per atom: cnt[0] non-finite hoppings, [1] non-finite on-site energies, [2] first offending
+// atom (0-based, via min), [3] entries without a reverse entry (same pair, opposite lattice translation),
+// [4] pairs compared, [5] the largest |hopp(j,i) - conj(hopp(j2,m))| as the bits of a non-negative double.
+__global__ void k_check(int64_t n, int32_t mn, const int32_t* nneigh, const int32_t* nlist, const int32_t* ncell,
+                        const double2* hopp, const double* h0, unsigned long long* cnt)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    unsigned long long nhop = 0, missing = 0, pairs = 0;
+    double mx = 0.0;
+    bool bad = !isfinite(h0[i]);
+    if (bad) atomicAdd(&cnt[1], 1ull);
+    for (int j = 0; j < nneigh[i]; ++j) {
+        const int64_t e = i * mn + j;
+        const double2 a = hopp[e];
+        if (!(isfinite(a.x) && isfinite(a.y))) {
+            ++nhop;
+            bad = true;
+        }
+        const int64_t m = nlist[e] - 1;
+        if (m < i) continue;
+        int j2 = 0;
+        for (; j2 < nneigh[m]; ++j2) {
+            const int64_t e2 = m * mn + j2;
+            if (nlist[e2] - 1 == i && ncell[3 * e2] == -ncell[3 * e] && ncell[3 * e2 + 1] == -ncell[3 * e + 1] &&
+                ncell[3 * e2 + 2] == -ncell[3 * e + 2])
+                break;
+        }
+        if (j2 >= nneigh[m]) {
+            ++missing;
+            continue;
+        }
+        if (m == i && j2 <= j) continue;
+        ++pairs;
+        const double2 b = hopp[m * mn + j2];
+        const double asym = hypot(a.x - b.x, a.y + b.y);
+        mx = asym > mx ? asym : mx;   // a NaN asymmetry is counted by the finiteness check
+    }
+    if (nhop) atomicAdd(&cnt[0], nhop);
+    if (missing) atomicAdd(&cnt[3], missing);
+    if (pairs) atomicAdd(&cnt[4], pairs);
+    if (bad) atomicMin(&cnt[2], (unsigned long long)i);
+    if (mx > 0.0) atomicMax(&cnt[5], (unsigned long long)__double_as_longlong(mx));
+}
+
+int check_hamiltonian(gbn_ctx* c, int64_t* out, double* max_asym)
+{
+    if (!c->have_ham || !c->ncell.p) return fail(c, GBN_ERR_STATE, "the checks need a Hamiltonian and the neighbour images");
+    DevBuf cnt;
+    GBN_CK(c, cnt.ensure(sizeof(unsigned long long) * 6));
+    unsigned long long init[6] = {0ull, 0ull, ~0ull, 0ull, 0ull, 0ull};
+    GBN_CK(c, cudaMemcpyAsync(cnt.p, init, sizeof init, cudaMemcpyHostToDevice, c->stream));
+    const unsigned grd = (unsigned)((c->n + 127) / 128);
+    k_check<<<grd, 128, 0, c->stream>>>(c->n, c->max_neigh, c->nneigh.as<int32_t>(), c->nlist.as<int32_t>(),
+                                        c->ncell.as<int32_t>(), c->hopp.as<double2>(), c->h0.as<double>(),
+                                        cnt.as<unsigned long long>());
+    GBN_CK_LAUNCH(c);
+    unsigned long long h[6];
+    GBN_CK(c, cudaMemcpyAsync(h, cnt.p, sizeof h, cudaMemcpyDeviceToHost, c->stream));
+    GBN_CK(c, cudaStreamSynchronize(c->stream));
+    out[0] = (int64_t)h[0];
+    out[1] = (int64_t)h[1];
+    out[2] = h[2] == ~0ull ? 0 : (int64_t)h[2] + 1;
+    out[3] = (int64_t)h[3];
+    out[4] = (int64_t)h[4];
+    double mx;
+    memcpy(&mx, &h[5], sizeof mx);
+    *max_asym = mx;
     return GBN_OK;
 }
 

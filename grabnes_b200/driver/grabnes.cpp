@@ -841,6 +841,35 @@ Tables read_tables(const Job& j, int64_t n, const std::vector<double>& ucell, co
     return t;
 }
 
+// The end of HamHopping (ham.F90:6940-6941): HamCheckFinite stops on non-finite values; HamCheckHermiticity
+// reports the largest asymmetry of the two directions of a bond for the models with position-dependent
+// bond terms (here Moire.OffDiag, and Haldane.NNN with Haldane.SpecifyPhase).
+void check_hamiltonian(gbn_ctx* ctx, const Job& j)
+{
+    int64_t cnt[5] = {0, 0, 0, 0, 0};
+    double asym = 0.0;
+    ck(gbn_check_hamiltonian(ctx, cnt, &asym), ctx, "gbn_check_hamiltonian");
+    if (cnt[0] + cnt[1] > 0)
+        die("The Hamiltonian contains non-finite values: " + std::to_string(cnt[0]) + " hopping and " +
+            std::to_string(cnt[1]) + " on-site entries (first at atom " + std::to_string(cnt[2]) + ")");
+    const bool od = j.model.moire_offdiag != 0, hphase = j.haldane && j.hal_mode == 2;
+    if (!(od || hphase)) return;
+    if (cnt[3] > 0) printf("grabnes: hopping table: %lld entries without reverse entry\n", (long long)cnt[3]);
+    const double ev = asym * j.g0;
+    if (hphase && !od) {
+        if (ev > 1.0e-9)
+            printf("grabnes: warning: the hopping table is NOT Hermitian with HaldaneNNN and HaldaneSpecifyPhase: the "
+                   "two directions of a bond differ by up to %.6g eV\n", ev);
+    } else if (od && j.model.moire_mid) {
+        printf("grabnes: hopping table with MoireOffDiagMidpoint: the two directions of a bond differ by up to %.6g eV\n",
+               ev);
+    } else {
+        printf("grabnes: warning: the hopping table is NOT Hermitian: the two directions of a bond differ by up to "
+               "%.6g eV, because MoireOffDiag is evaluated at the first atom of each bond. Set MoireOffDiagMidpoint "
+               ".true. to evaluate it at the bond midpoint (Hermitian).\n", ev);
+    }
+}
+
 // KuboDOS (kubo.F90:276-319) after the recursion: <prefix>.b0.dat, .a0.dat (KuboRecursion's files), the
 // continued fraction <prefix>.DOS and the coefficients <prefix>.AB.
 void kubo_dos_files(gbn_ctx* ctx, const Job& j, const std::string& prefix, const double* a, const double* b)
@@ -1077,6 +1106,7 @@ int run(const Job& j0)
             ck(gbn_peierls(ctx, bmag * kPi / kFluxQuantum), ctx, "gbn_peierls");
         }
         if (j.haldane) ck(gbn_haldane(ctx, j.cell.aG, j.hal_t2, hphase, j.hal_paper ? 1 : 0, j.hal_mask), ctx, "gbn_haldane");
+        if (!j.read_data) check_hamiltonian(ctx, j);
         if (j.write_data && !j.read_data) write_ham_files(ctx, prefix, n, maxn, rat_now, species, layer, ucell.data());
         bool any = true;
         if (j.pdos.mode == 0) {   // KuboInitWF + KuboDOS

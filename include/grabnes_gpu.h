@@ -144,6 +144,13 @@ int gbn_get_neighbours(gbn_ctx* ctx, int32_t* nneigh, int32_t* nlist, double* ne
  * the reference's fractional/Cartesian round trips); uniform holds the N Anderson draws (or NULL). */
 int gbn_assemble(gbn_ctx* ctx, const gbn_model* model, const double* rat_onsite,
                  const double* rat_hop, const double* uniform);
+/* HamCheckFinite (ham.F90:4432-4477) and the pair scan of HamCheckHermiticity (ham.F90:4491-4571) on the
+ * current Hamiltonian: counts[0] non-finite hoppings, [1] non-finite on-site energies, [2] the first
+ * atom with either (1-based, 0 if none), [3] entries without a reverse entry (the same pair with the
+ * opposite lattice translation), [4] pairs compared; *max_asym = max |hopp(j,i) - conj(hopp(j2,m))| in
+ * g0.  The reference stops on non-finite values and prints or warns about the asymmetry; the caller
+ * decides here.  Needs the neighbour images (gbn_neighbours, or gbn_set_images after loading). */
+int gbn_check_hamiltonian(gbn_ctx* ctx, int64_t* counts, double* max_asym);
 /* HamHopHaldane (ham.F90:7043-7142, chirality HamHaldaneChirality ham.F90:13063-13100), after
  * gbn_peierls as in HamHopping: every second-neighbour bond within a layer (|d - aG| < 0.1 Ang,
  * Species 1 or 2) gets + t2 exp(i nu phase), or, with paper != 0, is multiplied by exp(i nu phase);

@@ -115,6 +115,13 @@ void orc_hopping(const orc_model* m, int64_t n, const double* Rat,
 int64_t orc_haldane(int64_t n, const int32_t* species, const int32_t* layer, int32_t maxNeigh,
                     const int32_t* Nneigh, const int32_t* NList, const double* NeighD, double aG, double t2,
                     double phase, int32_t paper, uint32_t layer_mask, double* hopp);
+/* HamCheckFinite (ham.F90:4432-4477) and the pair scan of HamCheckHermiticity (ham.F90:4491-4571):
+ * out[0] non-finite hoppings, out[1] non-finite on-site energies, out[2] first offending atom (1-based,
+ * 0 if none), out[3] entries without a reverse entry, out[4] pairs compared; *max_asym the largest
+ * |hopp(j,i) - conj(hopp(j2,m))| (g0 units). */
+void orc_check_hamiltonian(int64_t n, int32_t maxNeigh, const int32_t* Nneigh, const int32_t* NList,
+                           const int32_t* neighCell, const double* hopp, const double* H0, int64_t* out,
+                           double* max_asym);
 void orc_peierls(int64_t n, const double* Rat, const double* ucell,
                  int32_t maxNeigh, const int32_t* Nneigh, const int32_t* NList,
                  const int32_t* neighCell, double flux, double* hopp);

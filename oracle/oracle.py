@@ -83,6 +83,8 @@ def _declare(L):
     L.orc_haldane.argtypes = [i64, _p(np.int32), _p(np.int32), i32, _p(np.int32), _p(np.int32), _p(np.float64), C.c_double,
                               C.c_double, C.c_double, i32, C.c_uint32, _p(np.float64)]
     L.orc_haldane.restype = i64
+    L.orc_check_hamiltonian.argtypes = [i64, i32, _p(np.int32), _p(np.int32), _p(np.int32), _p(np.float64),
+                                        _p(np.float64), _p(np.int64), C.POINTER(C.c_double)]
     L.orc_peierls.argtypes = [i64, _p(np.float64), _p(np.float64), i32, _p(np.int32), _p(np.int32),
                               _p(np.int32), d, _p(np.complex128)]
     L.orc_init_wf.argtypes = [i64, i32, _p(np.complex128)]
@@ -176,6 +178,18 @@ def haldane(species, layer, nb, aG, t2, phase, hop, paper=False, layer_mask=0):
                              np.ascontiguousarray(nb["neighd"]).reshape(-1), aG, t2, phase, int(paper), layer_mask,
                              h.view(np.float64))
     return h.reshape(n, nb["max_neigh"]), miss
+
+
+def check_hamiltonian(nb, hop, h0):
+    """(non-finite hoppings, non-finite on-site, first atom, entries without reverse, pairs, max asymmetry)"""
+    n = len(h0)
+    out = np.zeros(5, np.int64)
+    mx = C.c_double()
+    h = np.ascontiguousarray(hop, np.complex128).reshape(-1)
+    lib().orc_check_hamiltonian(n, nb["max_neigh"], nb["nneigh"], np.ascontiguousarray(nb["nlist"]).reshape(-1),
+                                np.ascontiguousarray(nb["ncell"]).reshape(-1), h.view(np.float64),
+                                np.ascontiguousarray(h0, np.float64), out, C.byref(mx))
+    return tuple(int(x) for x in out) + (mx.value,)
 
 
 def peierls(rat, ucell, nb, flux, hop):

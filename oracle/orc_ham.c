@@ -298,3 +298,53 @@ int64_t orc_haldane(int64_t n, const int32_t* species, const int32_t* layer, int
     }
     return missing;
 }
+
+void orc_check_hamiltonian(int64_t n, int32_t maxNeigh, const int32_t* Nneigh, const int32_t* NList,
+                           const int32_t* neighCell, const double* hopp, const double* H0, int64_t* out,
+                           double* max_asym)
+{
+    int64_t nhop = 0, nons = 0, first = 0, missing = 0, pairs = 0;
+    double mx = 0.0;
+    for (int64_t i = 0; i < n; ++i) {
+        if (!isfinite(H0[i])) {
+            ++nons;
+            if (first == 0) first = i + 1;
+        }
+        for (int j = 0; j < Nneigh[i]; ++j) {
+            const double* h = hopp + 2 * ((size_t)i * maxNeigh + j);
+            if (!(isfinite(h[0]) && isfinite(h[1]))) {
+                ++nhop;
+                if (first == 0) first = i + 1;
+            }
+        }
+    }
+    for (int64_t i = 0; i < n; ++i)
+        for (int j = 0; j < Nneigh[i]; ++j) {
+            const size_t e = (size_t)i * maxNeigh + j;
+            const int64_t m = NList[e] - 1;
+            if (m < i) continue;
+            int j2 = 0;
+            for (; j2 < Nneigh[m]; ++j2) {
+                const size_t e2 = (size_t)m * maxNeigh + j2;
+                if (NList[e2] - 1 == i && neighCell[3 * e2] == -neighCell[3 * e] &&
+                    neighCell[3 * e2 + 1] == -neighCell[3 * e + 1] && neighCell[3 * e2 + 2] == -neighCell[3 * e + 2])
+                    break;
+            }
+            if (j2 >= Nneigh[m]) {
+                ++missing;
+                continue;
+            }
+            if (m == i && j2 <= j) continue;
+            ++pairs;
+            const double* a = hopp + 2 * e;
+            const double* b = hopp + 2 * ((size_t)m * maxNeigh + j2);
+            const double asym = hypot(a[0] - b[0], a[1] + b[1]);
+            if (asym > mx) mx = asym;
+        }
+    out[0] = nhop;
+    out[1] = nons;
+    out[2] = first;
+    out[3] = missing;
+    out[4] = pairs;
+    *max_asym = mx;
+}
