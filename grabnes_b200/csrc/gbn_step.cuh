@@ -36,6 +36,19 @@ using StepFn = void (*)(StepParams);
 // the sparse-product kernel of the field-batched layout (gbn_fields.cu)
 StepFn field_step_kernel(int prec, int G, int rpt, int tpr, bool staged);
 
+// Compensated summation (Neumaier's variant of Kahan's) for the block and grid reductions of the dot
+// products: the running error term recovers the low-order bits that each addition loses.
+struct NeumaierSum {
+    double s = 0.0, c = 0.0;
+    __device__ __forceinline__ void add(double x)
+    {
+        const double t = s + x;
+        c += (fabs(s) >= fabs(x)) ? (s - t) + x : (x - t) + s;
+        s = t;
+    }
+    __device__ __forceinline__ double value() const { return s + c; }
+};
+
 struct SliceSums {
     double s1, s2, s3, s4;
 };
@@ -72,9 +85,9 @@ __device__ __forceinline__ void reduce_and_finalize(const StepParams& p, SliceSu
     __syncthreads();
     if (threadIdx.x < R * 4) {
         const int r = threadIdx.x >> 2, k = threadIdx.x & 3;
-        double a = 0.0;
-        for (int wI = 0; wI < (int)(blockDim.x >> 5); ++wI) a += red[wI][r][k];
-        p.partials[((int64_t)blockIdx.x * R + r) * 4 + k] = a;
+        NeumaierSum a;
+        for (int wI = 0; wI < (int)(blockDim.x >> 5); ++wI) a.add(red[wI][r][k]);
+        p.partials[((int64_t)blockIdx.x * R + r) * 4 + k] = a.value();
     }
     // the last block to finish reduces all blocks in a fixed order
     __shared__ bool last;
@@ -87,9 +100,9 @@ __device__ __forceinline__ void reduce_and_finalize(const StepParams& p, SliceSu
     __shared__ double tot[R][4];
     if (threadIdx.x < R * 4) {
         const int r = threadIdx.x >> 2, k = threadIdx.x & 3;
-        double a = 0.0;
-        for (unsigned int bI = 0; bI < gridDim.x; ++bI) a += __ldcg(&p.partials[((int64_t)bI * R + r) * 4 + k]);
-        tot[r][k] = a;
+        NeumaierSum a;
+        for (unsigned int bI = 0; bI < gridDim.x; ++bI) a.add(__ldcg(&p.partials[((int64_t)bI * R + r) * 4 + k]));
+        tot[r][k] = a.value();
     }
     __syncthreads();
     if (threadIdx.x < R) {
