@@ -12,7 +12,11 @@ Reported: value = atom-steps/s with the start vectors resident on the device (wh
 ranks); e2e = the same through gbn_lanczos_phases with host buffers (H2D of the draws, D2H of a, b);
 roofline of the recursion-step kernel against measured HBM bandwidth; the plain FP64 paths (batched
 and single vector) and the DOS error of the mixed path against the FP64 path; the oracle port timed
-on the host cores as CPU baseline.  --impl reference times that CPU port alone (the reference is
+on the host cores as CPU baseline.  Further legs (each can be skipped or run alone): the 33-field
+graphene/hBN sweep batched against field by field (fields_batch), the Chebyshev Kubo time evolution of
+the 3.5M-atom graphene/hBN cell with its states on the device against on the host
+(kubo_time_evolution), one DOS-loss gradient of a 964,548-atom twisted bilayer (dos_gradient), and the
+batched mixed-precision DOS of the 3.5M-atom graphene/hBN cell with its roofline (moire_dos).  --impl reference times that CPU port alone (the reference is
 Fortran + MPI and cannot be built in this image).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]

@@ -327,3 +327,25 @@ def test_driver_read_data_files(tmp_path, details):
     b = np.loadtxt(tmp_path / "rd.b0.dat")
     scale = max(np.abs(a0).max(), np.abs(b0).max())
     assert np.abs(a - a0).max() <= 1e-10 * scale and np.abs(b - b0).max() <= 1e-10 * scale
+
+
+@pytestmark_cpu
+def test_driver_reads_pdos_and_haldane_keys(tmp_path):
+    """The first PDOS flag that is set wins, PDOSMoireSuperMoire defaulting to .true. (calc.F90:214-300);
+    Haldane.T2 is read in eV; HaldPhase bounds only with Haldane.SpecifyRange (magf.F90:148-211)."""
+    path = str(tmp_path / "Gendata.in")
+    _write(path, {"Kubo.PDOS": True, "Kubo.PDOSAtomList": True, "TB.Hopping": 2.7})
+    got = _print_job(path)
+    assert got["pdos_mode"] == G.PDOS_SUPERMOIRE   # the default-true SuperMoire flag comes before AtomList
+    _write(path, {"Kubo.PDOS": True, "Kubo.PDOSMoireSuperMoire": False, "Kubo.PDOSMoireSuperMoire2": False,
+                  "Kubo.PDOSMoireSuperMoire3": False, "Kubo.PDOSAtomList": True, "Kubo.PDOSLayer": True})
+    assert _print_job(path)["pdos_mode"] == G.PDOS_LAYER
+    _write(path, {"TB.Hopping": 2.7, "Haldane.NNN": True, "Haldane.T2": 0.27, "Haldane.SpecifyRange": True,
+                  "HaldPhase.InitialInteger": 0, "HaldPhase.FinalInteger": 6, "HaldPhase.Step": 3})
+    got = _print_job(path)
+    assert got["haldane"] == 1 and got["hal_mode"] == 3 and got["mphi"] == [0, 6, 3]
+    assert math.isclose(got["hal_t2"], 0.1, rel_tol=1e-15)
+    _write(path, {"Haldane.NNN": True, "Haldane.SpecifyPhase": True, "Haldane.Phase": 1.0,
+                  "HaldPhase.InitialInteger": 0, "HaldPhase.FinalInteger": 6})
+    got = _print_job(path)
+    assert got["hal_mode"] == 2 and got["mphi"][:2] == [0, 0]   # no sweep without SpecifyRange
