@@ -31,14 +31,31 @@ namespace {
 
 constexpr int kAdThreads = 256;
 
+// The adjoint's copy of the Hamiltonian: the reference tables (row i, slot j at i * mn + j, complex
+// hoppings) transposed to slot-major order, entry (i, j) at j * n + i with the real hopping and the
+// 0-based column, so that the threads of a warp (consecutive rows) read consecutive words.
 struct AdTables {
     int64_t n;
     int32_t mn;
     const int32_t* nneigh;
-    const int32_t* nlist;
-    const double2* hopp;
+    const int32_t* col;
+    const double* hop;
     const double* h0;
 };
+
+__global__ void k_ad_tables(int64_t n, int32_t mn, const int32_t* __restrict__ nneigh,
+                            const int32_t* __restrict__ nlist, const double2* __restrict__ hopp,
+                            int32_t* __restrict__ col, double* __restrict__ hop)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int nn = nneigh[i];
+    for (int j = 0; j < mn; ++j) {
+        const int64_t src = i * mn + j, dst = (int64_t)j * n + i;
+        col[dst] = j < nn ? nlist[src] - 1 : (int32_t)i;
+        hop[dst] = j < nn ? hopp[src].x : 0.0;
+    }
+}
 
 // y = H x, one row per thread
 __global__ void k_ad_apply(AdTables t, const double2* __restrict__ x, double2* __restrict__ y)
@@ -47,12 +64,13 @@ __global__ void k_ad_apply(AdTables t, const double2* __restrict__ x, double2* _
     if (i >= t.n) return;
     const double2 xi = x[i];
     double cr = t.h0[i] * xi.x, ci = t.h0[i] * xi.y;
-    const int64_t base = i * t.mn;
-    for (int j = 0; j < t.nneigh[i]; ++j) {
-        const double2 h = t.hopp[base + j];
-        const double2 xj = x[t.nlist[base + j] - 1];
-        cr -= h.x * xj.x - h.y * xj.y;
-        ci -= h.x * xj.y + h.y * xj.x;
+    const int nn = t.nneigh[i];
+    for (int j = 0; j < nn; ++j) {
+        const int64_t e = (int64_t)j * t.n + i;
+        const double h = t.hop[e];
+        const double2 xj = x[t.col[e]];
+        cr -= h * xj.x;
+        ci -= h * xj.y;
     }
     y[i] = make_double2(cr, ci);
 }
@@ -76,25 +94,44 @@ __device__ __forceinline__ void block_partials(double (&v)[NQ], double* partials
     }
 }
 
-// sum of the block partials in block order; op decides what becomes of the totals (one thread)
+// sum of the block partials in a fixed order; op decides what becomes of the totals
 enum : int { kSetA = 0, kSetB = 1, kSetS1 = 2, kRevDots = 3 };
 
-__global__ void k_ad_finish(const double* partials, int nblocks, int nq, int op, int k, double* a, double* b,
-                            double* abar, double* bbar, double* scal)
+constexpr int kFinThreads = 256;
+
+__global__ void __launch_bounds__(kFinThreads) k_ad_finish(const double* partials, int nblocks, int nq, int op,
+                                                           int k, double* a, double* b, double* abar, double* bbar,
+                                                           double* scal)
 {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    // thread t sums the partials of blocks t, t + 256, ... in block order, then a fixed tree
+    __shared__ double sh[3][kFinThreads];
     double s[3] = {0.0, 0.0, 0.0};
-    for (int blk = 0; blk < nblocks; ++blk)
-        for (int q = 0; q < nq; ++q) s[q] += partials[(int64_t)blk * nq + q];
+    for (int blk = threadIdx.x; blk < nblocks; blk += kFinThreads) {
+        const double* p = partials + (int64_t)blk * nq;
+        s[0] += p[0];
+        if (nq > 1) s[1] += p[1];
+        if (nq > 2) s[2] += p[2];
+    }
+#pragma unroll
+    for (int q = 0; q < 3; ++q) sh[q][threadIdx.x] = s[q];
+    __syncthreads();
+    for (int w = kFinThreads / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w)
+#pragma unroll
+            for (int q = 0; q < 3; ++q) sh[q][threadIdx.x] += sh[q][threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x != 0) return;
+    const double s0 = sh[0][0], s1 = sh[1][0];
     if (op == kSetA) {
-        a[k] = s[0];
+        a[k] = s0;
     } else if (op == kSetB) {
-        b[k] = sqrt(fabs(s[0]));
+        b[k] = sqrt(fabs(s0));
     } else if (op == kSetS1) {
-        scal[0] = s[0];   // Re qbar_{k+1}^+ q_{k+1}
-    } else {              // kRevDots: s[0] = Re q_k^+ rbar, s[1] = Re q_{k-1}^+ rbar
-        scal[1] = abar[k] - s[0];   // total abar_k
-        if (k > 0) bbar[k - 1] -= s[1];
+        scal[0] = s0;   // Re qbar_{k+1}^+ q_{k+1}
+    } else {            // kRevDots: s0 = Re q_k^+ rbar, s1 = Re q_{k-1}^+ rbar
+        scal[1] = abar[k] - s0;   // total abar_k
+        if (k > 0) bbar[k - 1] -= s1;
     }
 }
 
@@ -175,14 +212,14 @@ __global__ void k_ad_back(AdTables t, const double2* __restrict__ ubar, const do
     const double ak = a[k], bk = b[k], bp = k > 0 ? b[k - 1] : 0.0, ab = scal[1];
     const double2 ui = ubar[i];
     double hr = t.h0[i] * ui.x, hi = t.h0[i] * ui.y;
-    const int64_t base = i * t.mn;
-    for (int j = 0; j < t.nneigh[i]; ++j) {
-        const int64_t e = base + j;
-        const int64_t jj = t.nlist[e] - 1;
-        const double2 h = t.hopp[e];
+    const int nn = t.nneigh[i];
+    for (int j = 0; j < nn; ++j) {
+        const int64_t e = (int64_t)j * t.n + i;
+        const int32_t jj = t.col[e];
+        const double h = t.hop[e];
         const double2 uj = ubar[jj];
-        hr -= h.x * uj.x - h.y * uj.y;
-        hi -= h.x * uj.y + h.y * uj.x;
+        hr -= h * uj.x;
+        hi -= h * uj.y;
         const double2 qj = qk[jj];
         hbar[e] += ui.x * qj.x + ui.y * qj.y;
     }
@@ -211,13 +248,13 @@ __global__ void k_ad_params(AdTables t, gbn_model m, double g0, const double* ne
 {
     double v[4] = {0.0, 0.0, 0.0, 0.0};
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < t.n; i += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t base = i * t.mn;
-        for (int j = 0; j < t.nneigh[i]; ++j) {
-            const int64_t e = base + j;
+        const int nn = t.nneigh[i];
+        for (int j = 0; j < nn; ++j) {
+            const int64_t e = (int64_t)j * t.n + i, r = i * t.mn + j;   // slot-major; reference order
             const double hb = hbar[e];
             if (hb == 0.0) continue;
-            const int64_t jj = t.nlist[e] - 1;
-            const double Dx = neighd[3 * e], Dy = neighd[3 * e + 1], Dz = neighd[3 * e + 2];
+            const int32_t jj = t.col[e];
+            const double Dx = neighd[3 * r], Dy = neighd[3 * r + 1], Dz = neighd[3 * r + 2];
             if (layer[i] == layer[jj]) {
                 const double d = sqrt(Dx * Dx + Dy * Dy);
                 if (d < 1.7) v[0] -= hb / g0;   // nearest neighbours: hopp = t / g0
@@ -324,8 +361,6 @@ int dos_gradient(gbn_ctx* c, const gbn_model* m, double g0, const double* u_host
         return fail(c, GBN_ERR_ARG, "bad gradient arguments");
     if (C < 1 || C > K) C = K;
     const int64_t n = c->n;
-    AdTables t{n, c->max_neigh, c->nneigh.as<int32_t>(), c->nlist.as<int32_t>(), c->hopp.as<double2>(),
-               c->h0.as<double>()};
     const int nseg = (K + C - 1) / C;
     const size_t vb = sizeof(double2) * (size_t)n;
     // device memory: checkpoints (q_{c-1}, q_c) per segment, a segment of C + 2 vectors, 5 work vectors,
@@ -343,6 +378,10 @@ int dos_gradient(gbn_ctx* c, const gbn_model* m, double g0, const double* u_host
     GBN_CK(c, abr.ensure(sizeof(double) * K));
     GBN_CK(c, bbr.ensure(sizeof(double) * K));
     GBN_CK(c, ud.ensure(sizeof(double) * (size_t)n));
+    DevBuf tcol, thop;
+    GBN_CK(c, tcol.ensure(sizeof(int32_t) * (size_t)n * c->max_neigh));
+    GBN_CK(c, thop.ensure(sizeof(double) * (size_t)n * c->max_neigh));
+    AdTables t{n, c->max_neigh, c->nneigh.as<int32_t>(), tcol.as<int32_t>(), thop.as<double>(), c->h0.as<double>()};
     double2* CK = ck.as<double2>();
     double2* W = work.as<double2>();
     double* A = ab.as<double>();
@@ -354,17 +393,20 @@ int dos_gradient(gbn_ctx* c, const gbn_model* m, double g0, const double* u_host
 
     // forward pass with checkpoints: q_k in W[0], q_{k-1} in W[1], u/r in W[2], q_{k+1} in W[3]
     double2 *qk = W, *qm = W + n, *ur = W + 2 * n, *qn = W + 3 * n;
+    k_ad_tables<<<rows_grid, kAdThreads, 0, st>>>(n, c->max_neigh, c->nneigh.as<int32_t>(), c->nlist.as<int32_t>(),
+                                                  c->hopp.as<double2>(), tcol.as<int32_t>(), thop.as<double>());
     k_ad_start<<<rows_grid, kAdThreads, 0, st>>>(n, ud.as<double>(), qk, qm);
     GBN_CK_LAUNCH(c);
+    c->launches += 2;
     auto fwd_step = [&](double2* q, double2* qmm, double2* u, double2* qnext, int k) -> int {
         k_ad_apply<<<rows_grid, kAdThreads, 0, st>>>(t, q, u);
         k_ad_dot_au<<<blocks, kAdThreads, 0, st>>>(n, q, u, P);
-        k_ad_finish<<<1, 32, 0, st>>>(P, blocks, 1, kSetA, k, A, B, nullptr, nullptr, nullptr);
+        k_ad_finish<<<1, kFinThreads, 0, st>>>(P, blocks, 1, kSetA, k, A, B, nullptr, nullptr, nullptr);
         k_ad_residual<<<blocks, kAdThreads, 0, st>>>(n, u, q, qmm, A, B, k, P);
-        k_ad_finish<<<1, 32, 0, st>>>(P, blocks, 1, kSetB, k, A, B, nullptr, nullptr, nullptr);
+        k_ad_finish<<<1, kFinThreads, 0, st>>>(P, blocks, 1, kSetB, k, A, B, nullptr, nullptr, nullptr);
         k_ad_scale<<<blocks, kAdThreads, 0, st>>>(n, u, qnext, B, k);
         GBN_CK_LAUNCH(c);
-        c->launches += 5;
+        c->launches += 6;
         return GBN_OK;
     };
     for (int k = 0; k < K; ++k) {
@@ -426,9 +468,9 @@ int dos_gradient(gbn_ctx* c, const gbn_model* m, double g0, const double* u_host
             const double2* q0 = S + (size_t)(j + 1) * n;
             const double2* qkm = (k > 0) ? S + (size_t)j * n : nullptr;
             k_ad_dot<<<blocks, kAdThreads, 0, st>>>(n, qa, qk1, P);
-            k_ad_finish<<<1, 32, 0, st>>>(P, blocks, 1, kSetS1, k, nullptr, nullptr, AB, BB, SC);
+            k_ad_finish<<<1, kFinThreads, 0, st>>>(P, blocks, 1, kSetS1, k, nullptr, nullptr, AB, BB, SC);
             k_ad_rbar<<<blocks, kAdThreads, 0, st>>>(n, qa, qk1, q0, qkm, rb, B, BB, SC, k, P);
-            k_ad_finish<<<1, 32, 0, st>>>(P, blocks, 2, kRevDots, k, nullptr, nullptr, AB, BB, SC);
+            k_ad_finish<<<1, kFinThreads, 0, st>>>(P, blocks, 2, kRevDots, k, nullptr, nullptr, AB, BB, SC);
             k_ad_ubar<<<blocks, kAdThreads, 0, st>>>(n, rb, q0, ub, SC);
             // qbar_k into tmpv, the partial qbar_{k-1} into qa (no longer needed)
             k_ad_back<<<rows_grid, kAdThreads, 0, st>>>(t, ub, rb, qb, qk1, q0, qkm, tmpv, qa, A, B, SC, k,
@@ -446,6 +488,7 @@ int dos_gradient(gbn_ctx* c, const gbn_model* m, double g0, const double* u_host
     k_ad_params<<<pblocks, kAdThreads, 0, st>>>(t, *m, g0, c->neighd.as<double>(), c->layer.as<int32_t>(),
                                                 hbar.as<double>(), P);
     GBN_CK_LAUNCH(c);
+    c->launches += 1;
     std::vector<double> hp((size_t)pblocks * 4);
     GBN_CK(c, cudaMemcpyAsync(hp.data(), P, sizeof(double) * hp.size(), cudaMemcpyDeviceToHost, st));
     GBN_CK(c, cudaStreamSynchronize(st));
