@@ -198,7 +198,7 @@ class Context:
     def set_stream(self, stream_handle):
         self._ck(self._L.gbn_set_stream(self._h, C.c_void_p(stream_handle)))
 
-    def set_tuning(self, rhs_per_thread=0, blocks_per_sm=0, rows_per_group=0, staged=-1, prefetch=0):
+    def set_tuning(self, rhs_per_thread=0, blocks_per_sm=0, rows_per_group=0, staged=-1, prefetch=-1):
         self._ck(self._L.gbn_set_tuning(self._h, rhs_per_thread, blocks_per_sm, rows_per_group, staged, prefetch))
 
     @property

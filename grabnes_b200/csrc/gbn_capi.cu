@@ -196,7 +196,7 @@ int gbn_set_tuning(gbn_ctx* c, int32_t rhs_per_thread, int32_t blocks_per_sm, in
     if (!c) return GBN_ERR_ARG;
     if (rhs_per_thread < 0 || rhs_per_thread > 4 || blocks_per_sm < 0 || blocks_per_sm > 32 ||
         (rows_per_group != 0 && rows_per_group != 1 && rows_per_group != 2 && rows_per_group != 4) || staged < -1 ||
-        staged > 1 || prefetch < 0 || prefetch > 2)
+        staged > 1 || prefetch < -1 || prefetch > 4)
         return fail(c, GBN_ERR_ARG, "tuning values out of range");
     c->tune_rpt = rhs_per_thread;
     c->tune_blocks_per_sm = blocks_per_sm;

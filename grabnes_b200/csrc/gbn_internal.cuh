@@ -141,7 +141,8 @@ struct gbn_ctx {
     int tune_blocks_per_sm = 0;  // cap on resident blocks per SM
     int tune_group = 0;          // rows per group of the matrix layout (1, 2, 4)
     int tune_staged = -1;        // matrix records staged in shared memory by bulk copies (-1 auto, 0 no, 1 yes)
-    int tune_prefetch = 0;       // staged kernel: prefetch the gather rows of a slice (0 no, 1 to L2, 2 to L1)
+    int tune_prefetch = -1;      // staged kernel: prefetch the gather rows of a slice (0 no, 1 to L2, 2 to L1)
+                                 // or the rows of its epilogue (3 to L1, 4 to L2; -1 = 4)
     bool last_staged = false;    // the last recursion used the staged kernel
 
     // Chebyshev work vectors

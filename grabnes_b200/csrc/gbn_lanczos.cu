@@ -407,7 +407,7 @@ int lanczos_run(gbn_ctx* c, int32_t nmax)
     p.mat = c->ell.mat.as<unsigned char>();
     p.entry_bytes = c->ell.entry_bytes;
     p.cap_record = c->ell.cap_record;
-    p.prefetch = c->tune_prefetch;
+    p.prefetch = c->tune_prefetch < 0 ? 4 : c->tune_prefetch;   // default: the epilogue rows into L2
     p.h0 = c->ell.h0.p;
     p.v_out = c->vec[0].p;
     p.scal = c->scal.as<double>();

@@ -17,7 +17,8 @@ struct StepParams {
     const unsigned char* mat;  // slice records (column indices, then G values per union column)
     int64_t entry_bytes;       // 4 + G * value bytes
     int64_t cap_record;        // bytes of a staging buffer (larger records are read in place)
-    int32_t prefetch;          // staged kernel: prefetch the gather rows of a slice (1 L2, 2 L1)
+    int32_t prefetch;          // staged kernel: prefetch the gather rows of a slice (1 L2, 2 L1) or
+                               // the rows of its epilogue (3 L1, 4 L2)
     const void* h0;
     const void* x_cur;   // x_k   [npad][R] (gathered)
     const void* x_prev;  // x_{k-1}
@@ -277,6 +278,32 @@ __device__ __forceinline__ void prefetch_rows(const StepParams& p, const int32_t
     }
 }
 
+// Prefetch of the rows a slice's epilogue reads (its own rows of x_k and x_{k-1}, contiguous in the
+// row order, and their on-site values), issued before the column loop so that the epilogue's loads
+// find them in L1 (mode 3) or L2 (mode 4) instead of waiting a DRAM round trip.
+template <typename VT, int R, int G, int GPW>
+__device__ __forceinline__ void prefetch_epilogue(const StepParams& p, int64_t s)
+{
+    constexpr int BLK = GPW * G * R * (int)sizeof(typename V2<VT>::t);   // bytes of one slice's rows
+    const int lane = threadIdx.x & 31;
+    const size_t off = (size_t)s * BLK;
+    const char* a = static_cast<const char*>(p.x_prev) + off;
+    const char* b = static_cast<const char*>(p.x_cur) + off;
+    for (int i = lane * 128; i < BLK; i += 32 * 128) {
+        if (p.prefetch == 3) {
+            asm volatile("prefetch.global.L1 [%0];" ::"l"(a + i));
+            asm volatile("prefetch.global.L1 [%0];" ::"l"(b + i));
+        } else {
+            asm volatile("prefetch.global.L2 [%0];" ::"l"(a + i));
+            asm volatile("prefetch.global.L2 [%0];" ::"l"(b + i));
+        }
+    }
+    if (lane == 31) {
+        const char* h = static_cast<const char*>(p.h0) + (size_t)s * GPW * G * sizeof(VT);
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(h));
+    }
+}
+
 // Matrix records staged in shared memory.  Each warp owns two record buffers and an mbarrier per
 // buffer; its lane 0 copies the record of the warp's next-but-one slice with one bulk copy while the
 // warp works on the current one, so the column indices that the gathers depend on come from shared
@@ -347,9 +374,11 @@ __global__ void __launch_bounds__(256) k_spmm_staged(StepParams p)
         const int64_t base = p.slice_ptr[s];
         const int w = (int)((p.slice_ptr[s + 1] - base) / GPW);
         const int64_t bytes = rec_bytes(s);
+        if (p.prefetch >= 3) prefetch_epilogue<VT, R, G, GPW>(p, s);
         if (bytes <= p.cap_record) {
             const unsigned char* rec = buf + st * p.cap_record;
-            if (p.prefetch) prefetch_rows<VT, R>(p, reinterpret_cast<const int32_t*>(rec), w * GPW);
+            if (p.prefetch == 1 || p.prefetch == 2)
+                prefetch_rows<VT, R>(p, reinterpret_cast<const int32_t*>(rec), w * GPW);
             group_slice<VT, CPLX, G, RPT, TPR, true, FIELD>(p, s, w, reinterpret_cast<const int32_t*>(rec) + sub,
                                                      reinterpret_cast<const HT*>(rec + (size_t)w * GPW * 4) + sub * G,
                                                      cb, acc_s);

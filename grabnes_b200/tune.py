@@ -3,16 +3,16 @@
 Candidates: rows per group of the matrix layout (1 = plain sliced ELL; 2, 4 = neighbouring rows share
 one gather per union column), right-hand sides per thread (the width of each thread's vector loads,
 and with it the groups a warp processes per slice), the matrix path (slice records staged in shared
-memory by per-warp bulk copies, or read from global memory), the prefetch of the gather rows (staged
-path only) and a cap on resident blocks per SM.  Each candidate runs a short recursion on the
-caller's own Hamiltonian and start vectors; the one with the smallest device time per step (update +
-sparse product, CUDA events) is kept on the context.
+memory by per-warp bulk copies, or read from global memory), a prefetch (staged path only) of the
+gather rows of each slice or of the rows its epilogue reads, and a cap on resident blocks per SM.
+Each candidate runs a short recursion on the caller's own Hamiltonian and start vectors; the one with
+the smallest device time per step (update + sparse product, CUDA events) is kept on the context.
 """
 import itertools
 
 
 def autotune(ctx, u, precision, nsteps=12, rhs_per_thread=(1, 2, 4), blocks_per_sm=(0,),
-             rows_per_group=(1, 2, 4), staged=(0, 1), prefetch=(0, 1)):
+             rows_per_group=(1, 2, 4), staged=(0, 1), prefetch=(0, 1, 4)):
     results = []
     cands = [c for c in itertools.product(rows_per_group, staged, prefetch, rhs_per_thread, blocks_per_sm)
              if c[1] == 1 or c[2] == 0]   # the prefetch belongs to the staged path

@@ -113,7 +113,8 @@ int         gbn_set_stream(gbn_ctx* ctx, void* cuda_stream);
  * entries per row), the matrix path of the sparse product (1 = each warp stages its next slice
  * records in shared memory with bulk asynchronous copies, 0 = records read from global memory,
  * -1 = staged when two records per warp fit in shared memory) and, for the staged path, a prefetch of
- * the vector rows each slice gathers (0 = none, 1 = into L2, 2 = into L1).  Used by the autotuner
+ * the vector rows each slice gathers (0 = none, 1 = into L2, 2 = into L1) or of the rows its epilogue
+ * reads (3 = into L1, 4 = into L2; -1 = the default, 4).  Used by the autotuner
  * (grabnes_b200/tune.py). */
 int         gbn_set_tuning(gbn_ctx* ctx, int32_t rhs_per_thread, int32_t blocks_per_sm, int32_t rows_per_group,
                            int32_t staged, int32_t prefetch);

@@ -178,10 +178,12 @@ def test_mixed_precision_dos(ctx):
 
 @pytest.mark.parametrize("rpt", [1, 2, 4])
 def test_layout_variants_agree(ctx, rpt):
-    """Rows per group 1, 2 and 4 of the matrix layout, records staged in shared memory (with and without
-    the gather-row prefetch) or read from global memory, for every split of the right-hand sides over
-    threads: the same products summed in another order (union columns of a group instead of a row's own
-    columns), so mixed-precision a_n, b_n agree to FP32 rounding over 60 steps."""
+    """Rows per group 1, 2 and 4 of the matrix layout, records staged in shared memory (without a
+    prefetch, with the gather-row prefetch into L2 or L1, with the epilogue-row prefetch into L1 or L2)
+    or read from global memory, for every split of the right-hand sides over threads: the same products
+    summed in another order (union columns of a group instead of a row's own columns), so mixed-precision
+    a_n, b_n agree to FP32 rounding over 60 steps; a prefetch is only a hint, so every prefetch mode
+    gives exactly the results of the staged path without one."""
     r = built("tbg")
     n = r["geo"]["n"]
     ctx.load_hamiltonian(r["nb"]["nneigh"], r["nb"]["nlist"], r["hop"], r["h0"])
@@ -189,9 +191,14 @@ def test_layout_variants_agree(ctx, rpt):
     out = []
     try:
         for grp in (1, 2, 4):
-            for staged, pf in ((0, 0), (1, 0), (1, 1), (1, 2)):
+            staged_runs = []
+            for staged, pf in ((0, 0), (1, 0), (1, 1), (1, 2), (1, 3), (1, 4)):
                 ctx.set_tuning(rpt, 0, grp, staged, pf)
                 out.append(ctx.lanczos_phases(u, 60, G.GBN_MIXED))
+                if staged:
+                    staged_runs.append(out[-1])
+            for a, b in staged_runs[1:]:
+                assert np.array_equal(a, staged_runs[0][0]) and np.array_equal(b, staged_runs[0][1])
     finally:
         ctx.set_tuning()
     for k in range(1, len(out)):
