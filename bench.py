@@ -251,7 +251,10 @@ def run_ours(args, ws, rank, local):
     e2e_ms = dist_max(statistics.median(e2e_ms), ws)
     e2e_value = ws * atom_steps / (e2e_ms / 1e3)
 
-    # ---- plain FP64 paths and the DOS error of the mixed path
+    # ---- plain FP64 paths and the DOS error of the mixed path, with the library's default tuning (the
+    # autotuned values belong to the 16-vector mixed-precision tile; the default picks the rows per
+    # group for the tile width: 2 for 16 vectors, 1 for a single vector)
+    ctx.set_tuning()
     torch.cuda.synchronize()
     f0 = time.perf_counter()
     a64, b64 = ctx.lanczos_phases(u_np, nsteps, G.GBN_FP64)
