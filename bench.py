@@ -182,9 +182,13 @@ def run_ours(args, ws, rank, local):
     # vectors are staged once and every job rebuilds them on the device
     from grabnes_b200.tune import autotune
     if args.tuning:
-        rpt, bps, grp, st, pf = (int(x) for x in args.tuning.split(","))
-        ctx.set_tuning(rpt, bps, grp, st, pf)
-        best = dict(rhs_per_thread=rpt, blocks_per_sm=bps, rows_per_group=grp, staged=st, prefetch=pf, fixed=True)
+        vals = [int(x) for x in args.tuning.split(",")]
+        rpt, bps, grp, st, pf = vals[:5]
+        unroll = vals[5] if len(vals) > 5 else 0
+        best = dict(rhs_per_thread=rpt, blocks_per_sm=bps, rows_per_group=grp, staged=st, prefetch=pf,
+                    unroll=unroll, fixed=True)
+        from grabnes_b200.tune import apply
+        apply(ctx, best)
         tuning = []
     else:
         best, tuning = autotune(ctx, u, G.GBN_MIXED)
@@ -255,6 +259,7 @@ def run_ours(args, ws, rank, local):
     # autotuned values belong to the 16-vector mixed-precision tile; the default picks the rows per
     # group for the tile width: 2 for 16 vectors, 1 for a single vector)
     ctx.set_tuning()
+    ctx.set_kernel_variant()
     torch.cuda.synchronize()
     f0 = time.perf_counter()
     a64, b64 = ctx.lanczos_phases(u_np, nsteps, G.GBN_FP64)
@@ -527,6 +532,7 @@ def moire_dos_leg(G, M, local, stream, ws, nrhs=16, nsteps=2000, peak=None):
     ctx.run_staged(nsteps, a_mix, b_mix)
     ms2, _ = ctx.last_timing()
     ctx.set_tuning()
+    ctx.set_kernel_variant()
     a64, b64 = ctx.lanczos_phases(u[:1], nsteps, G.GBN_FP64)
     ms64, _ = ctx.last_timing()
     _, d_mix = ctx.cf_dos(a_mix[:1], b_mix[:1], 0.005 / g0, 1200, -0.6 / g0, 0.6 / g0)
@@ -624,8 +630,8 @@ def main():
     p.add_argument("--gradient-only", action="store_true", help="run the DOS-gradient leg alone")
     p.add_argument("--tevol-only", action="store_true", help="run the Chebyshev Kubo time evolution leg alone")
     p.add_argument("--fields-scale", type=float, default=1.0, help="scale of the sweep's recursion lengths (profiling)")
-    p.add_argument("--tuning", default="", help="fixed kernel tuning 'rhs_per_thread,blocks_per_sm,rows_per_group,staged,prefetch' "
-                                                "instead of the autotuner")
+    p.add_argument("--tuning", default="", help="fixed kernel tuning 'rhs_per_thread,blocks_per_sm,rows_per_group,staged,prefetch"
+                                                "[,unroll]' instead of the autotuner")
     args = p.parse_args()
     ws, rank, local = dist_init() if args.impl == "ours" else (int(os.environ.get("WORLD_SIZE", "1")),
                                                                  int(os.environ.get("RANK", "0")), 0)

@@ -95,7 +95,7 @@ def _opt(dtype):
     return Opt
 
 
-EXPORTS = ["gbn_cell_atoms", "gbn_build_cell", "gbn_cart_roundtrip", "gbn_rng_uniform", "gbn_create", "gbn_destroy", "gbn_last_error", "gbn_version", "gbn_set_stream", "gbn_set_tuning", "gbn_launch_count",
+EXPORTS = ["gbn_cell_atoms", "gbn_build_cell", "gbn_cart_roundtrip", "gbn_rng_uniform", "gbn_create", "gbn_destroy", "gbn_last_error", "gbn_version", "gbn_set_stream", "gbn_set_tuning", "gbn_set_kernel_variant", "gbn_launch_count",
            "gbn_last_timing", "gbn_last_kernel_timing", "gbn_set_geometry", "gbn_neighbours", "gbn_get_neighbours", "gbn_assemble",
            "gbn_peierls", "gbn_get_hamiltonian", "gbn_load_hamiltonian", "gbn_lanczos", "gbn_lanczos_phases",
            "gbn_stage_phases", "gbn_run_staged", "gbn_cf_dos", "gbn_cheb_evolve", "gbn_kubo_evol", "gbn_set_neighd", "gbn_lanczos_noalloc",
@@ -117,6 +117,7 @@ def _declare(L):
     L.gbn_version.restype = C.c_char_p
     L.gbn_set_stream.argtypes = [vp, vp]
     L.gbn_set_tuning.argtypes = [vp, i32, i32, i32, i32, i32]
+    L.gbn_set_kernel_variant.argtypes = [vp, i32, i32, i32]
     L.gbn_launch_count.argtypes = [vp]
     L.gbn_launch_count.restype = i64
     L.gbn_last_timing.argtypes = [vp, C.POINTER(d), C.POINTER(i64)]
@@ -200,6 +201,12 @@ class Context:
 
     def set_tuning(self, rhs_per_thread=0, blocks_per_sm=0, rows_per_group=0, staged=-1, prefetch=-1):
         self._ck(self._L.gbn_set_tuning(self._h, rhs_per_thread, blocks_per_sm, rows_per_group, staged, prefetch))
+
+    def set_kernel_variant(self, col_unroll=0, stage_values=-1, min_blocks=0):
+        """Columns in flight per batch of the sparse product (4, 8; 0 = default), whether staged slice
+        records carry the values (1) or only the column indices (0; -1 = default), and the resident blocks
+        per SM its registers are bounded for (1, 3; 0 = 1)."""
+        self._ck(self._L.gbn_set_kernel_variant(self._h, col_unroll, stage_values, min_blocks))
 
     @property
     def launches(self):

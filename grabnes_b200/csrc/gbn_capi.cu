@@ -196,14 +196,25 @@ int gbn_set_tuning(gbn_ctx* c, int32_t rhs_per_thread, int32_t blocks_per_sm, in
     if (!c) return GBN_ERR_ARG;
     if (rhs_per_thread < 0 || rhs_per_thread > 4 || blocks_per_sm < 0 || blocks_per_sm > 32 ||
         (rows_per_group != 0 && rows_per_group != 1 && rows_per_group != 2 && rows_per_group != 4) || staged < -1 ||
-        staged > 1 || prefetch < -1 || prefetch > 4)
+        staged > 1 || prefetch < -1 || prefetch > 7)
         return fail(c, GBN_ERR_ARG, "tuning values out of range");
     c->tune_rpt = rhs_per_thread;
     c->tune_blocks_per_sm = blocks_per_sm;
     c->tune_group = rows_per_group;
     c->tune_staged = staged;
-    c->tune_prefetch = prefetch;
-    c->ell.valid = false;
+    c->tune_prefetch = prefetch;   // a layout of other rows per group or threads per group is rebuilt when used
+    return GBN_OK;
+}
+
+int gbn_set_kernel_variant(gbn_ctx* c, int32_t col_unroll, int32_t stage_values, int32_t min_blocks)
+{
+    if (!c) return GBN_ERR_ARG;
+    if ((col_unroll != 0 && col_unroll != 4 && col_unroll != 8) || stage_values < -1 || stage_values > 1 ||
+        (min_blocks != 0 && min_blocks != 1 && min_blocks != 3))
+        return fail(c, GBN_ERR_ARG, "kernel variant out of range");
+    c->tune_unroll = col_unroll;
+    c->tune_stage_values = stage_values;
+    c->tune_min_blocks = min_blocks;
     return GBN_OK;
 }
 
@@ -623,10 +634,9 @@ int gbn_run_staged(gbn_ctx* c, int32_t nmax, double* a, double* b)
     if (nmax < 1) return fail(c, GBN_ERR_ARG, "nmax must be at least 1");
     cudaSetDevice(c->device);
     int rc = GBN_OK;
-    if (!c->ell.valid || c->ell.field) {   // the layout was invalidated (new tuning or Hamiltonian) since staging
-        rc = lanczos_prepare(c, c->prec, c->nrhs);
-        if (rc) return rc;
-    }
+    // the layout matches the current Hamiltonian and tuning (rebuilt only when either changed since staging)
+    rc = lanczos_prepare(c, c->prec, c->nrhs);
+    if (rc) return rc;
     // the start vectors are rebuilt from the staged draws so that every run starts from them
     rc = lanczos_start_from_phases(c, c->upload.as<double>(), c->nrhs);
     if (rc) return rc;

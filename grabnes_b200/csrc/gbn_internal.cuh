@@ -65,6 +65,7 @@ struct Ell {
     int dval_dir = 0;        // NeighD component of dval (1 = x, 2 = y; 0 = not built)
     int64_t max_record = 0;  // bytes of the largest slice record
     int64_t cap_record = 0;  // staging buffer size: 99.5 % of the records fit (larger ones are read in place)
+    int64_t cap_pct[4] = {0, 0, 0, 0};   // record sizes at the 99.5th, 99th, 95th and 90th percentiles
     bool field = false;      // field-batched values: field-free hopping and Peierls phase per flux quantum
     bool valid = false;
 };
@@ -125,8 +126,8 @@ struct gbn_ctx {
     int prec = -1;
     int nrhs = 0;
     gbn::DevBuf vec[4];      // v, x_prev, x_cur (ping-pong of the x pair)
-    gbn::DevBuf partials;    // double [blocks][R][4]
-    gbn::DevBuf scal;        // double [R][2]: a_{k-1}, b_{k-1}
+    gbn::DevBuf partials;    // double [blocks][R]
+    gbn::DevBuf scal;        // double [R][4]: a, norms of the current and the previous carried vector
     gbn::DevBuf counter;     // uint32 block counter + int32 step index + int32 flag
     gbn::DevBuf ab;          // double [2][R][nmax]
     gbn::DevBuf upload;      // staging of host inputs
@@ -143,6 +144,9 @@ struct gbn_ctx {
     int tune_staged = -1;        // matrix records staged in shared memory by bulk copies (-1 auto, 0 no, 1 yes)
     int tune_prefetch = -1;      // staged kernel: prefetch the gather rows of a slice (0 no, 1 to L2, 2 to L1)
                                  // or the rows of its epilogue (3 to L1, 4 to L2; -1 = 4)
+    int tune_unroll = 0;         // union columns in flight per batch of the product (4, 8; 0 = automatic)
+    int tune_stage_values = -1;  // staged records carry the values (1) or only the column indices (0); -1 auto
+    int tune_min_blocks = 0;     // product kernel compiled for 1 or 3 resident blocks per SM (0 = 1)
     bool last_staged = false;    // the last recursion used the staged kernel
 
     // Chebyshev work vectors

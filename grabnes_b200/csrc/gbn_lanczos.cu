@@ -2,23 +2,27 @@
 //
 // The reference (lanczosKuboCode/Src/kubosubs.F90:26-138) makes three passes over the vectors per
 // step: H psi with <psi, H psi>; w = H psi - a psi - b psi_prev with |w|; the scaling psi = w / b.
-// Here the carried state is the pair
-//     v_k = H x_{k-1} - b_{k-2} x_{k-2}      and     x_{k-1},
-// and a step is
-//   k_update    x_k = (v_k - a_{k-1} x_{k-1}) / b_{k-1}             stream: read v, x_{k-1}; write x_k
-//   k_spmm_*    y = H x_k (one gather of x_k per union column of a row group), v_{k+1} = y - b_{k-1} x_{k-1},
-//               and four FP64 dot products per vector
-//                  S1 = Re<x_k, y>, S2 = |v_{k+1}|^2, S3 = Re<x_k, v_{k+1}>, S4 = |x_k|^2,
-//               from which a_k = S1 and b_k^2 = |v_{k+1} - a_k x_k|^2 = S2 - 2 a_k S3 + a_k^2 S4.
-// The partial sums of the blocks are reduced in a fixed order by the last block to finish (so the
-// result does not depend on scheduling), which also writes a_k, b_k and the scalars of the next step.
+// Here the carried vectors are unnormalised: x_k = u_k / b_{k-1}, and a step is
+//   k_update    u_k = v_k - (a_{k-1} / b_{k-2}) u_{k-1}  and  b_{k-1} = |u_k|
+//               (v_k - a_{k-1} x_{k-1} is the reference's w, b_{k-1} its norm; stream: read v, u_{k-1},
+//               write u_k; one FP64 sum per vector)
+//   k_spmm_*    y = H u_k (one gather of u_k per union column of a row group),
+//               v_{k+1} = y / b_{k-1} - (b_{k-1} / b_{k-2}) u_{k-1}   (= H x_k - b_{k-1} x_{k-1})
+//               and a_k = Re<u_k, y> / b_{k-1}^2 (one FP64 sum per vector).
+// The first update takes the start vector as given (b = 1 for it, as the reference's first step uses
+// Psi unnormalised) and a run of n steps ends with one more update, which gives b_{n-1}.  Each kernel's
+// block partial sums are reduced in a fixed order by its last block to finish (so the result does not
+// depend on scheduling), which also writes a_k or b_{k-1} and the scalars of the next launch.
 //
 // Vectors of R right-hand sides are interleaved per row ([row][R] complex): TPR threads share a row
 // group, each holding RPT right-hand sides (8-32 bytes per gather).  With 16 vectors a gathered row is
 // one 128-byte line.  The product is bound by the latency of the chain column index -> gather: the
-// grouped layout (struct Ell) gathers a column once for the G rows of a group, and the staged kernel
-// brings each warp's next slice record (column indices and values) into shared memory with one bulk
-// asynchronous copy, so that only the gathers themselves wait on memory.
+// grouped layout (struct Ell) gathers a column once for the G rows of a group, the staged kernel
+// brings each warp's next slice record (column indices, and values unless they stream beside the
+// gathers) into shared memory with one bulk asynchronous copy, and U columns' gathers are in flight
+// together, so that only the gathers themselves wait on memory.
+#include <algorithm>
+
 #include <cuda_runtime.h>
 #include <math.h>
 #include <string.h>
@@ -28,29 +32,74 @@
 namespace gbn {
 
 // ---------------------------------------------------------------------------- update kernel
-// x_k = (v_k - a x_{k-1}) * (1/b) for all rows and right-hand sides (streaming).  The grid stride and
-// the block size are multiples of R, so every thread keeps one right-hand side and its 1/b.
+// u_k = v_k - (a_{k-1} / b_{k-2}) u_{k-1} for all rows and right-hand sides (streaming), and
+// b_{k-1} = |u_k| from the stored (rounded) elements.  The grid stride and the block size are multiples
+// of R, so every thread keeps one right-hand side; the block's sums are reduced per right-hand side in
+// thread order, then by the last block over the blocks in a fixed order.
 template <typename VT>
 __global__ void __launch_bounds__(256) k_update(const typename V2<VT>::t* __restrict__ v,
                                                 const typename V2<VT>::t* __restrict__ xp,
-                                                typename V2<VT>::t* __restrict__ xc, const double* __restrict__ scal,
-                                                int64_t total, int R)
+                                                typename V2<VT>::t* __restrict__ xc, double* scal, double* partials,
+                                                unsigned int* counter, double* b_out, int nmax, int64_t total, int R)
 {
     const int r = (int)(threadIdx.x & (unsigned)(R - 1));
-    const double a = scal[2 * r], ib = 1.0 / scal[2 * r + 1];
+    const double c = scal[kScal * r] / scal[kScal * r + 1];
+    using C2 = typename V2<VT>::t;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += stride) {
-        const typename V2<VT>::t vv = __ldcs(v + e), xx = __ldcs(xp + e);
-        typename V2<VT>::t o;   // FP64 arithmetic, one rounding to the storage type
-        o.x = (VT)(((double)vv.x - a * (double)xx.x) * ib);
-        o.y = (VT)(((double)vv.y - a * (double)xx.y) * ib);
+    double q = 0.0;
+    auto one = [&](C2 vv, C2 xx, int64_t e) {   // FP64 arithmetic, one rounding to the storage type
+        C2 o;
+        o.x = (VT)((double)vv.x - c * (double)xx.x);
+        o.y = (VT)((double)vv.y - c * (double)xx.y);
         xc[e] = o;
+        q += (double)o.x * (double)o.x + (double)o.y * (double)o.y;
+    };
+    // four elements per thread in flight: all eight loads are issued before the first use
+    constexpr int D = 4;
+    int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    for (; e + (D - 1) * stride < total; e += D * stride) {
+        C2 vv[D], xx[D];
+#pragma unroll
+        for (int i = 0; i < D; ++i) {
+            vv[i] = __ldcs(v + e + i * stride);
+            xx[i] = __ldcs(xp + e + i * stride);
+        }
+#pragma unroll
+        for (int i = 0; i < D; ++i) one(vv[i], xx[i], e + i * stride);
     }
+    for (; e < total; e += stride) one(__ldcs(v + e), __ldcs(xp + e), e);
+    // block: the 256 / R threads of each right-hand side, combined in a fixed tree
+    __shared__ double rs[256], rc[256];
+    rs[threadIdx.x] = q;
+    rc[threadIdx.x] = 0.0;
+    tree_fixed_sum(rs, rc, (int)blockDim.x / R, R);
+    if ((int)threadIdx.x < R) partials[(int64_t)blockIdx.x * R + threadIdx.x] = rs[threadIdx.x] + rc[threadIdx.x];
+    __shared__ bool last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    __shared__ double tot[32];
+    grid_fixed_sum(partials, (int)gridDim.x, R, rs, rc, tot);
+    if ((int)threadIdx.x < R) {
+        const double b = sqrt(tot[threadIdx.x]);
+        const unsigned int step = counter[1];   // products done so far: this is b_{step-1}
+        if (step > 0) {
+            if (!(b > 0.0) || !isfinite(b)) atomicOr(&counter[2], 1u);
+            if ((int)step <= nmax) b_out[(int64_t)threadIdx.x * nmax + step - 1] = b;
+        }
+        scal[kScal * threadIdx.x + 2] = scal[kScal * threadIdx.x + 1];
+        scal[kScal * threadIdx.x + 1] = step > 0 ? b : 1.0;   // the start vector is used as given
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) counter[0] = 0u;
 }
 
 // ---------------------------------------------------------------------------- sparse product
 // ---------------------------------------------------------------------------- start vectors
-// v <- psi (rows in the solver order), x_prev <- 0; then the first update gives x_1 = psi (a_0 = 0, b_0 = 1).
+// v <- psi (rows in the solver order), u_prev <- 0; then the first update gives u_0 = psi (a = 0, norm 1).
 template <typename VT>
 __global__ void k_start_from_phases(typename V2<VT>::t* v, typename V2<VT>::t* x, const double* u,
                                     const int32_t* perm, int64_t n, int64_t npad, int R, int nrhs_real,
@@ -151,8 +200,10 @@ __global__ void k_init_scalars(double* scal, unsigned int* counter, int R)
 {
     const int r = threadIdx.x;
     if (r < R) {
-        scal[2 * r] = 0.0;
-        scal[2 * r + 1] = 1.0;
+        scal[kScal * r] = 0.0;
+        scal[kScal * r + 1] = 1.0;
+        scal[kScal * r + 2] = 1.0;
+        scal[kScal * r + 3] = 0.0;
     }
     if (r == 0) {
         counter[0] = 0u;
@@ -174,71 +225,104 @@ void split_rhs(int prec, int R, int want, int* rpt, int* tpr)
 }
 
 
-template <typename VT, bool CPLX, int G>
-static StepFn pick_g(int rpt, int tpr, bool staged)
-{
-#define GBN_CASE(RP, TP) \
-    if (rpt == RP && tpr == TP) return staged ? k_spmm_staged<VT, CPLX, G, RP, TP> : k_spmm_step<VT, CPLX, G, RP, TP>;
-    GBN_CASE(1, 1) GBN_CASE(1, 2) GBN_CASE(1, 4) GBN_CASE(1, 8) GBN_CASE(1, 16) GBN_CASE(1, 32)
-    GBN_CASE(2, 1) GBN_CASE(2, 2) GBN_CASE(2, 4) GBN_CASE(2, 8) GBN_CASE(2, 16)
-    if constexpr (sizeof(VT) == 4) {
-        GBN_CASE(4, 1) GBN_CASE(4, 2) GBN_CASE(4, 4) GBN_CASE(4, 8)
-    }
-#undef GBN_CASE
-    return nullptr;
-}
-
-template <typename VT, bool CPLX>
-static StepFn pick(int G, int rpt, int tpr, bool staged)
-{
-    if (G == 1) return pick_g<VT, CPLX, 1>(rpt, tpr, staged);
-    if (G == 2) return pick_g<VT, CPLX, 2>(rpt, tpr, staged);
-    if (G == 4) return pick_g<VT, CPLX, 4>(rpt, tpr, staged);
-    return nullptr;
-}
-
-static StepFn step_kernel(int prec, bool cplx, int G, int R, int want_rpt, bool staged)
+static StepFn step_kernel(int prec, bool cplx, int G, int R, int want_rpt, bool staged, StepVariant v)
 {
     int rpt, tpr;
     split_rhs(prec, R, want_rpt, &rpt, &tpr);
-    if (prec == GBN_MIXED) return cplx ? pick<float, true>(G, rpt, tpr, staged) : pick<float, false>(G, rpt, tpr, staged);
-    return cplx ? pick<double, true>(G, rpt, tpr, staged) : pick<double, false>(G, rpt, tpr, staged);
+    if (prec == GBN_MIXED) return step_kernel_mixed(cplx, G, rpt, tpr, staged, v);
+    return step_kernel_fp64(cplx, G, rpt, tpr, staged, v);
 }
 
 // Launch shape of the sparse product.  Staged: warps per block such that two record buffers per warp
-// fit the shared-memory budget (the plain kernel when the block reduction's 4 R threads do not fit).
+// fit the shared-memory budget.  cap: bytes of one buffer (whole records, or their column indices).
 struct StepLaunch {
     StepFn fn = nullptr;
     int grid = 0, block = 256;
     size_t smem = 0;
+    int64_t cap = 0;
     bool staged = false;
 };
 
 constexpr size_t kStagedSmemBudget = 200 * 1024;
+// blocks per SM of the streaming update kernel
+constexpr int kUpdateBlocksPerSM = 8;
 
 static int step_launch(gbn_ctx* c, int R, StepLaunch* L)
 {
     const Ell& E = c->ell;
-    const size_t per_warp = 2 * (size_t)E.cap_record;
-    const size_t min_warps = (size_t)((4 * R + 31) / 32);
-    const bool staged = c->tune_staged != 0 && per_warp > 0 && 128 + min_warps * per_warp <= kStagedSmemBudget;
-    L->staged = staged;
-    if (E.field) {
+    if (E.nslices * E.gpw * E.G > E.npad)   // the epilogue and its prefetch address whole slices of rows
+        return fail(c, GBN_ERR_ARG, "internal: matrix slices cover more rows than the vectors hold");
+    // defaults (measured on the 4.47M-atom twisted bilayer and the 3.5M-atom graphene/hBN cell with 16
+    // vectors, and on 80k/1.1M-atom cells with one vector): 8 columns in flight in mixed precision, 4 in
+    // FP64; with 8 columns and one row per group, registers bounded for 3 blocks per SM
+    StepVariant v;
+    v.unroll = c->tune_unroll > 0 ? c->tune_unroll : (c->prec == GBN_MIXED ? 8 : 4);
+    v.stage_values = c->tune_stage_values != 0;
+    v.min_blocks = c->tune_min_blocks > 0 ? c->tune_min_blocks : (v.unroll == 8 && E.G == 1 && !E.cplx ? 3 : 1);
+    // buffer bytes of a record of percentile i: whole records, or their index part (multiples of 16)
+    auto cap_of = [&](int i) -> int64_t {
+        const int64_t rec = E.cap_pct[i];
+        return v.stage_values ? rec : (rec / E.entry_bytes * 4 + 15) / 16 * 16;
+    };
+    const bool want_staged = c->tune_staged != 0 && cap_of(0) > 0;
+    // the kernel of this variant; shapes without it take the base variant unless one was asked for
+    const bool asked = c->tune_unroll > 0 || c->tune_stage_values >= 0 || c->tune_min_blocks > 0;
+    auto pick = [&](bool staged) -> StepFn {
         int rpt, tpr;
         split_rhs(c->prec, R, c->tune_rpt, &rpt, &tpr);
-        L->fn = field_step_kernel(c->prec, E.G, rpt, tpr, staged);
-    } else {
-        L->fn = step_kernel(c->prec, E.cplx, E.G, R, c->tune_rpt, staged);
-    }
-    if (!L->fn) return fail(c, GBN_ERR_ARG, "no recursion kernel for this tile width");
+        const StepVariant base;
+        if (E.field)
+            return (v.unroll == 4 && v.stage_values && v.min_blocks == 1) || !asked
+                       ? field_step_kernel(c->prec, E.G, rpt, tpr, staged) : nullptr;
+        StepFn f = step_kernel(c->prec, E.cplx, E.G, R, c->tune_rpt, staged, v);
+        if (!f && !asked) f = step_kernel(c->prec, E.cplx, E.G, R, c->tune_rpt, staged, base);
+        return f;
+    };
+    L->fn = pick(want_staged);
+    if (!L->fn) return fail(c, GBN_ERR_ARG, "no recursion kernel for this tile width and kernel variant");
     L->block = 256;
     L->smem = 0;
-    if (staged) {
-        size_t nw = (kStagedSmemBudget - 128) / per_warp;
-        nw = nw > 8 ? 8 : nw;   // >= min_warps by the test above
-        L->block = (int)(32 * nw);
-        L->smem = 128 + nw * per_warp;
-        GBN_CK(c, cudaFuncSetAttribute(L->fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L->smem));
+    L->staged = false;
+    L->cap = 0;
+    if (want_staged) {
+        // Shared memory per block such that the blocks the registers allow (at most 3) fit on an SM with
+        // their static shared memory: 8 warps with the largest record percentile whose two buffers per
+        // warp fit (larger records are read in place), else fewer warps with the 99.5th percentile.
+        int smem_sm = 0, resv = 0, optin = 0, reg_blocks = 0;
+        GBN_CK(c, cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, c->device));
+        GBN_CK(c, cudaDeviceGetAttribute(&resv, cudaDevAttrReservedSharedMemoryPerBlock, c->device));
+        GBN_CK(c, cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device));
+        cudaFuncAttributes fa;
+        GBN_CK(c, cudaFuncGetAttributes(&fa, L->fn));
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&reg_blocks, L->fn, 256, 0) != cudaSuccess || reg_blocks < 1)
+            reg_blocks = 1;
+        int target = reg_blocks < 3 ? reg_blocks : 3;
+        if (c->tune_blocks_per_sm > 0 && c->tune_blocks_per_sm < target) target = c->tune_blocks_per_sm;
+        int64_t budget = (int64_t)smem_sm / target - (int64_t)fa.sharedSizeBytes - resv;
+        if (budget > optin - (int64_t)fa.sharedSizeBytes) budget = optin - (int64_t)fa.sharedSizeBytes;
+        int64_t cap = 0;
+        int nw = 0;
+        for (int i = 0; i < 4 && !cap; ++i)
+            if (cap_of(i) > 0 && 128 + 8 * 2 * cap_of(i) <= budget) {
+                cap = cap_of(i);
+                nw = 8;
+            }
+        if (!cap && 128 + 2 * cap_of(0) <= budget) {
+            cap = cap_of(0);
+            nw = (int)((budget - 128) / (2 * cap));
+            nw = nw > 8 ? 8 : nw;
+        }
+        if (cap) {
+            L->staged = true;
+            L->cap = cap;
+            L->block = 32 * nw;   // >= 32 threads: R <= 32 threads read the step's scalars
+            L->smem = 128 + (size_t)nw * 2 * cap;
+            GBN_CK(c, cudaFuncSetAttribute(L->fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L->smem));
+        }
+    }
+    if (want_staged && !L->staged) {   // no buffer fits: the plain kernel
+        L->fn = pick(false);
+        if (!L->fn) return fail(c, GBN_ERR_ARG, "no recursion kernel for this tile width and kernel variant");
     }
     int per_sm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, L->fn, L->block, L->smem) != cudaSuccess || per_sm < 1)
@@ -268,8 +352,9 @@ int lanczos_prepare(gbn_ctx* c, int prec, int nrhs, bool field)
     StepLaunch L;
     const int rc = step_launch(c, nrhs, &L);
     if (rc) return rc;
-    GBN_CK(c, c->partials.ensure(sizeof(double) * (size_t)L.grid * nrhs * 4));
-    GBN_CK(c, c->scal.ensure(sizeof(double) * 2 * nrhs));
+    const size_t blocks = (size_t)(L.grid > c->num_sms * kUpdateBlocksPerSM ? L.grid : c->num_sms * kUpdateBlocksPerSM);
+    GBN_CK(c, c->partials.ensure(sizeof(double) * blocks * nrhs));
+    GBN_CK(c, c->scal.ensure(sizeof(double) * kScal * nrhs));
     GBN_CK(c, c->counter.ensure(sizeof(unsigned int) * 4));
     return GBN_OK;
 }
@@ -393,6 +478,12 @@ static int ensure_step_graph(gbn_ctx* c, const StepLaunch& L, const StepParams& 
 int lanczos_run(gbn_ctx* c, int32_t nmax)
 {
     const int R = c->nrhs;
+    // the run synchronises at its end (timing, error flags), which a stream capture does not allow
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    GBN_CK(c, cudaStreamIsCapturing(c->stream, &cap));
+    if (cap != cudaStreamCaptureStatusNone)
+        return fail(c, GBN_ERR_ARG, "the recursion cannot run while its stream is being captured into a graph: "
+                                    "it waits for its own kernels to read their timing and error flags");
     GBN_CK(c, c->ab.ensure(sizeof(double) * 2 * (size_t)R * nmax));
     k_init_scalars<<<1, 64, 0, c->stream>>>(c->scal.as<double>(), c->counter.as<unsigned int>(), R);
     GBN_CK_LAUNCH(c);
@@ -406,8 +497,9 @@ int lanczos_run(gbn_ctx* c, int32_t nmax)
     p.slice_ptr = c->ell.slice_ptr.as<int64_t>();
     p.mat = c->ell.mat.as<unsigned char>();
     p.entry_bytes = c->ell.entry_bytes;
-    p.cap_record = c->ell.cap_record;
-    p.prefetch = c->tune_prefetch < 0 ? 4 : c->tune_prefetch;   // default: the epilogue rows into L2
+    p.cap_record = L.cap;
+    // default: the epilogue rows into L2, and in mixed precision the rows of u_k two sweeps ahead
+    p.prefetch = c->tune_prefetch < 0 ? (c->prec == GBN_MIXED ? 6 : 4) : c->tune_prefetch;
     p.h0 = c->ell.h0.p;
     p.v_out = c->vec[0].p;
     p.scal = c->scal.as<double>();
@@ -420,7 +512,9 @@ int lanczos_run(gbn_ctx* c, int32_t nmax)
     p.field_m = c->field_m.as<int32_t>();
     const int64_t total = c->ell.npad * R;
     const int ublk = 256;   // a multiple of R (k_update keeps one right-hand side per thread)
-    const int ugrid = c->num_sms * 8;
+    // at least 8 elements per thread, at most kUpdateBlocksPerSM blocks per SM
+    const int ugrid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)c->num_sms * kUpdateBlocksPerSM,
+                                                                   (total + ublk * 8 - 1) / (ublk * 8)));
     if (!c->ev0) {
         GBN_CK(c, cudaEventCreate(&c->ev0));
         GBN_CK(c, cudaEventCreate(&c->ev1));
@@ -432,17 +526,32 @@ int lanczos_run(gbn_ctx* c, int32_t nmax)
     }
     // step k (0-based): x_prev in vec[1 + k%2], x_cur written to vec[1 + (k+1)%2]; the step index of the
     // a_n, b_n outputs lives on the device (counter[1]), so a run of an even number of steps replays as is
+    // the update of step k: u_k from v_k and u_{k-1}, and b_{k-1}
+    auto launch_update = [&](int32_t k) -> int {
+        void* xprev = c->vec[1 + (k & 1)].p;
+        void* xcur = c->vec[1 + ((k + 1) & 1)].p;
+        double* bo = c->ab.as<double>() + (size_t)R * nmax;
+        if (c->prec == GBN_MIXED)
+            k_update<float><<<ugrid, ublk, 0, c->stream>>>(c->vec[0].as<float2>(), static_cast<const float2*>(xprev),
+                                                          static_cast<float2*>(xcur), c->scal.as<double>(),
+                                                          c->partials.as<double>(), c->counter.as<unsigned int>(), bo,
+                                                          nmax, total, R);
+        else
+            k_update<double><<<ugrid, ublk, 0, c->stream>>>(c->vec[0].as<double2>(), static_cast<const double2*>(xprev),
+                                                           static_cast<double2*>(xcur), c->scal.as<double>(),
+                                                           c->partials.as<double>(), c->counter.as<unsigned int>(), bo,
+                                                           nmax, total, R);
+        GBN_CK_LAUNCH(c);
+        return GBN_OK;
+    };
+    // step k (0-based): u_{k-1} in vec[1 + k%2], u_k written to vec[1 + (k+1)%2]; the step index of the
+    // a_n, b_n outputs lives on the device (counter[1]), so a run of an even number of steps replays as is
     auto launch_step = [&](int32_t k) -> int {
         void* xprev = c->vec[1 + (k & 1)].p;
         void* xcur = c->vec[1 + ((k + 1) & 1)].p;
         if (k < nsample) GBN_CK(c, cudaEventRecord(c->kev[3 * k], c->stream));
-        if (c->prec == GBN_MIXED)
-            k_update<float><<<ugrid, ublk, 0, c->stream>>>(c->vec[0].as<float2>(), static_cast<const float2*>(xprev),
-                                                          static_cast<float2*>(xcur), c->scal.as<double>(), total, R);
-        else
-            k_update<double><<<ugrid, ublk, 0, c->stream>>>(c->vec[0].as<double2>(), static_cast<const double2*>(xprev),
-                                                           static_cast<double2*>(xcur), c->scal.as<double>(), total, R);
-        GBN_CK_LAUNCH(c);
+        const int rcu = launch_update(k);
+        if (rcu) return rcu;
         if (k < nsample) GBN_CK(c, cudaEventRecord(c->kev[3 * k + 1], c->stream));
         p.x_cur = xcur;
         p.x_prev = xprev;
@@ -459,10 +568,8 @@ int lanczos_run(gbn_ctx* c, int32_t nmax)
         if (rc2) return rc2;
     }
     // The remaining steps replay a captured graph of kGraphSteps steps (launch overhead is what limits
-    // small cells), unless the caller is capturing this stream into a graph of its own.
-    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
-    GBN_CK(c, cudaStreamIsCapturing(c->stream, &cap));
-    if (cap == cudaStreamCaptureStatusNone && nmax - k >= 2 * kGraphSteps) {
+    // small cells).
+    if (nmax - k >= 2 * kGraphSteps) {
         const int rc2 = ensure_step_graph(c, L, p, total, ublk, ugrid, launch_step, k);
         if (rc2) return rc2;
         for (; nmax - k >= kGraphSteps; k += kGraphSteps) {
@@ -473,6 +580,10 @@ int lanczos_run(gbn_ctx* c, int32_t nmax)
     }
     for (; k < nmax; ++k) {
         const int rc2 = launch_step(k);
+        if (rc2) return rc2;
+    }
+    {   // the closing update gives b_{nmax-1}
+        const int rc2 = launch_update(nmax);
         if (rc2) return rc2;
     }
     GBN_CK(c, cudaEventRecord(c->ev1, c->stream));

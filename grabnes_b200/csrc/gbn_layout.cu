@@ -469,11 +469,16 @@ int build_ell(gbn_ctx* c, int prec, int G, int gpw, bool field)
         std::vector<int64_t> rec((size_t)E.nslices);
         for (int64_t i = 0; i < E.nslices; ++i) rec[(size_t)i] = (hsp[(size_t)i + 1] - hsp[(size_t)i]) * (int64_t)eb;
         if (!rec.empty()) {
-            const size_t k = std::min(rec.size() - 1, (size_t)((double)rec.size() * 0.995));
-            std::nth_element(rec.begin(), rec.begin() + (ptrdiff_t)k, rec.end());
-            E.cap_record = (rec[k] + 15) / 16 * 16;
+            std::sort(rec.begin(), rec.end());
+            const double pct[4] = {0.995, 0.99, 0.95, 0.90};
+            for (int i = 0; i < 4; ++i) {
+                const size_t k = std::min(rec.size() - 1, (size_t)((double)rec.size() * pct[i]));
+                E.cap_pct[i] = (rec[k] + 15) / 16 * 16;
+            }
+            E.cap_record = E.cap_pct[0];
         } else {
             E.cap_record = 0;
+            for (int i = 0; i < 4; ++i) E.cap_pct[i] = 0;
         }
     }
     E.val_size = (int)vsz;

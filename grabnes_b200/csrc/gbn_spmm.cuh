@@ -145,8 +145,10 @@ __device__ __forceinline__ void load_group_vals(const HT* p, HT (&h)[G])
 // The union-column loop of one group: GPW = 32/TPR groups per slice; the TPR threads of a group each
 // hold RPT right-hand sides of all G rows of the group.  Per union column a thread reads the column
 // index and the G values (same address for the group's threads) and gathers RPT vector elements of that
-// column once for all G rows.  cp/vp point at the thread's group in the slice record, in global memory
-// (streamed, evict-first) or in shared memory (SMEM); w is the slice width (a multiple of 4).
+// column once for all G rows.  cp/vp point at the thread's group in the slice record; the indices come
+// from shared memory (SMEM) or global memory (streamed, evict-first), the values likewise (SMEM_VAL).
+// w is the slice width (a multiple of kColUnroll).  U columns are in flight per batch: their indices,
+// gathers and values are all issued before the first product, so U gathers wait on memory together.
 // FIELD: the values are FieldVal<VT> and every thread rotates them by its right-hand sides' field mf
 // (mf flux quanta, the same for the thread's RPT right-hand sides) before the complex products.
 template <typename VT, bool CPLX, bool FIELD> struct StoredVal { using t = typename Hop<VT, CPLX>::t; };
@@ -155,7 +157,49 @@ template <typename VT> struct FieldMult;
 template <> struct FieldMult<float> { using t = uint32_t; };
 template <> struct FieldMult<double> { using t = uint64_t; };
 
-template <typename VT, bool CPLX, int G, int RPT, int TPR, bool SMEM, bool FIELD = false>
+template <typename VT, bool CPLX, int G, int RPT, int TPR, bool SMEM, bool SMEM_VAL, bool FIELD, int NB>
+__device__ __forceinline__ void column_batch(const typename V2<VT>::t* __restrict__ xq,
+                                             const int32_t* __restrict__ cp,
+                                             const typename StoredVal<VT, CPLX, FIELD>::t* __restrict__ vp,
+                                             typename V2<VT>::t (&acc)[G][RPT], typename FieldMult<VT>::t mf)
+{
+    using C2 = typename V2<VT>::t;
+    using HT = typename StoredVal<VT, CPLX, FIELD>::t;
+    constexpr int GPW = 32 / TPR;
+    constexpr int R = RPT * TPR;
+    int32_t c[NB];
+    HT h[NB][G];
+    C2 xg[NB][RPT];
+#pragma unroll
+    for (int u = 0; u < NB; ++u) {
+        if constexpr (SMEM) c[u] = cp[u * GPW];
+        else c[u] = __ldcs(cp + u * GPW);
+    }
+#pragma unroll
+    for (int u = 0; u < NB; ++u) VecIO<VT, RPT>::load(xq + (size_t)(uint32_t)c[u] * R, xg[u]);
+#pragma unroll
+    for (int u = 0; u < NB; ++u) load_group_vals<HT, G, SMEM_VAL>(vp + u * GPW * G, h[u]);
+    if constexpr (FIELD) {
+#pragma unroll
+        for (int u = 0; u < NB; ++u)
+#pragma unroll
+            for (int g = 0; g < G; ++g) {
+                const C2 hr = field_rotate(h[u][g], mf);
+#pragma unroll
+                for (int t = 0; t < RPT; ++t) Hop<VT, true>::madd(acc[g][t], hr, xg[u][t]);
+            }
+    } else {
+#pragma unroll
+        for (int u = 0; u < NB; ++u)
+#pragma unroll
+            for (int g = 0; g < G; ++g)
+#pragma unroll
+                for (int t = 0; t < RPT; ++t) Hop<VT, CPLX>::madd(acc[g][t], h[u][g], xg[u][t]);
+    }
+}
+
+template <typename VT, bool CPLX, int G, int RPT, int TPR, bool SMEM, bool FIELD = false, int U = kColUnroll,
+          bool SMEM_VAL = SMEM>
 __device__ __forceinline__ void group_columns(const typename V2<VT>::t* __restrict__ x, int w,
                                               const int32_t* __restrict__ cp,
                                               const typename StoredVal<VT, CPLX, FIELD>::t* __restrict__ vp,
@@ -163,47 +207,26 @@ __device__ __forceinline__ void group_columns(const typename V2<VT>::t* __restri
                                               typename FieldMult<VT>::t mf = 0)
 {
     using C2 = typename V2<VT>::t;
-    using HT = typename StoredVal<VT, CPLX, FIELD>::t;
     constexpr int GPW = 32 / TPR;
-    constexpr int R = RPT * TPR;
-    constexpr int U = kColUnroll;
+    static_assert(U % kColUnroll == 0, "the unroll is a multiple of the slice-width granule");
     const int q = (threadIdx.x & 31) % TPR;
     const C2* __restrict__ xq = x + q * RPT;
 #pragma unroll
     for (int g = 0; g < G; ++g)
 #pragma unroll
         for (int t = 0; t < RPT; ++t) { acc[g][t].x = 0; acc[g][t].y = 0; }
-    for (int k = 0; k < w; k += U) {
-        int32_t c[U];
-        HT h[U][G];
-        C2 xg[U][RPT];
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-            if constexpr (SMEM) c[u] = cp[u * GPW];
-            else c[u] = __ldcs(cp + u * GPW);
-            load_group_vals<HT, G, SMEM>(vp + u * GPW * G, h[u]);
-        }
-#pragma unroll
-        for (int u = 0; u < U; ++u) VecIO<VT, RPT>::load(xq + (size_t)(uint32_t)c[u] * R, xg[u]);
-        if constexpr (FIELD) {
-#pragma unroll
-            for (int u = 0; u < U; ++u)
-#pragma unroll
-                for (int g = 0; g < G; ++g) {
-                    const C2 hr = field_rotate(h[u][g], mf);
-#pragma unroll
-                    for (int t = 0; t < RPT; ++t) Hop<VT, true>::madd(acc[g][t], hr, xg[u][t]);
-                }
-        } else {
-#pragma unroll
-            for (int u = 0; u < U; ++u)
-#pragma unroll
-                for (int g = 0; g < G; ++g)
-#pragma unroll
-                    for (int t = 0; t < RPT; ++t) Hop<VT, CPLX>::madd(acc[g][t], h[u][g], xg[u][t]);
-        }
+    int k = 0;
+    for (; k + U <= w; k += U) {
+        column_batch<VT, CPLX, G, RPT, TPR, SMEM, SMEM_VAL, FIELD, U>(xq, cp, vp, acc, mf);
         cp += U * GPW;
         vp += U * GPW * G;
+    }
+    if constexpr (U > kColUnroll) {
+        for (; k < w; k += kColUnroll) {
+            column_batch<VT, CPLX, G, RPT, TPR, SMEM, SMEM_VAL, FIELD, kColUnroll>(xq, cp, vp, acc, mf);
+            cp += kColUnroll * GPW;
+            vp += kColUnroll * GPW * G;
+        }
     }
 }
 

@@ -1,7 +1,7 @@
 // The per-step pieces of the recursion's sparse product shared by its kernels (gbn_lanczos.cu: matrix
 // records from global or shared memory; gbn_fields.cu: many fields from one field-free matrix): the
 // launch parameters, the slice loop body with its FP64 epilogue, and the fixed-order reduction of the
-// four dot products that writes a_k, b_k.
+// product's one dot product per right-hand side, which writes a_k.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -12,19 +12,25 @@
 
 namespace gbn {
 
+// Scalars of the recursion per right-hand side r, scal[4 r + i]:
+//   i = 0  a of the last product;  1  norm of the current carried vector u (x = u / norm);
+//   2  norm of the previous carried vector;  3  unused.
+constexpr int kScal = 4;
+
 struct StepParams {
     const int64_t* slice_ptr;
     const unsigned char* mat;  // slice records (column indices, then G values per union column)
     int64_t entry_bytes;       // 4 + G * value bytes
     int64_t cap_record;        // bytes of a staging buffer (larger records are read in place)
     int32_t prefetch;          // staged kernel: prefetch the gather rows of a slice (1 L2, 2 L1) or
-                               // the rows of its epilogue (3 L1, 4 L2)
+                               // the rows of its epilogue (3 L1, 4 L2); 5..7: as 4, and the rows of
+                               // u_k of the warp's slice 1, 2 or 4 sweeps ahead into L2 in one bulk prefetch
     const void* h0;
-    const void* x_cur;   // x_k   [npad][R] (gathered)
-    const void* x_prev;  // x_{k-1}
-    void* v_out;         // v_{k+1}
-    double* scal;        // [R][2] a_{k-1}, b_{k-1}
-    double* partials;    // [gridDim][R][4]
+    const void* x_cur;   // u_k   [npad][R] (gathered; x_k = u_k / b_{k-1})
+    const void* x_prev;  // u_{k-1}        (x_{k-1} = u_{k-1} / b_{k-2})
+    void* v_out;         // v_{k+1} = H x_k - b_{k-1} x_{k-1}
+    double* scal;        // [R][kScal]
+    double* partials;    // [gridDim][R]
     unsigned int* counter;  // [0] block counter, [1] step index, [2] error flag
     double* a_out;       // [R][nmax]
     double* b_out;
@@ -36,6 +42,18 @@ struct StepParams {
 using StepFn = void (*)(StepParams);
 // the sparse-product kernel of the field-batched layout (gbn_fields.cu)
 StepFn field_step_kernel(int prec, int G, int rpt, int tpr, bool staged);
+
+// Variant of the product kernel: columns in flight per batch (4 or 8) and, for the staged kernel,
+// whether the staged records carry the values or only the column indices.  Real-valued layouts at the
+// widest loads per thread have every variant; other shapes use unroll 4 with whole records.
+struct StepVariant {
+    int unroll = 4;
+    bool stage_values = true;
+    int min_blocks = 1;   // staged, unroll 8: registers bounded for 3 resident blocks of 256 threads per SM
+};
+// the product kernel of the real or complex layout (gbn_step_mixed.cu, gbn_step_fp64.cu)
+StepFn step_kernel_mixed(bool cplx, int G, int rpt, int tpr, bool staged, StepVariant v);
+StepFn step_kernel_fp64(bool cplx, int G, int rpt, int tpr, bool staged, StepVariant v);
 
 // Compensated summation (Neumaier's variant of Kahan's) for the block and grid reductions of the dot
 // products: the running error term recovers the low-order bits that each addition loses.
@@ -50,14 +68,76 @@ struct NeumaierSum {
     __device__ __forceinline__ double value() const { return s + c; }
 };
 
-struct SliceSums {
-    double s1, s2, s3, s4;
-};
+// Compensated pairwise combination of per-thread sums in shared memory, in a fixed order: entry
+// j * R + r of (vs, vc) holds the sum and the error term of part j of right-hand side r (j < per); a
+// tree of TwoSum steps over j leaves the total of r in vs[r] + vc[r].  Called by every thread of the
+// block (it synchronises); per * R <= blockDim.x.
+__device__ __forceinline__ void tree_fixed_sum(double* vs, double* vc, int per, int R)
+{
+    __syncthreads();
+    int half = 1;
+    while (half < per) half <<= 1;
+    for (half >>= 1; half >= 1; half >>= 1) {
+        const int j = (int)threadIdx.x / R, r = (int)threadIdx.x % R;
+        if (j < half && j + half < per) {
+            const int a = j * R + r, b = (j + half) * R + r;
+            const double s = vs[a], x = vs[b];
+            const double t = s + x;
+            const double e = (fabs(s) >= fabs(x)) ? (s - t) + x : (x - t) + s;
+            vs[a] = t;
+            vc[a] = vc[a] + vc[b] + e;
+        }
+        __syncthreads();
+    }
+}
 
-// Reduction of the four sums over the block, then by the last block over all blocks; writes a_k, b_k.
-// Needs at least 4 R threads per block.
+// Fixed-order total of the blocks' partial sums partials[nblk][R], computed by every thread of the calling
+// (last) block: thread t takes right-hand side t % R and the blocks t / R, t / R + T / R, ... (T threads,
+// a multiple of R), eight loads in flight, with Neumaier's compensation; then the T / R per-thread totals
+// of each right-hand side are combined by tree_fixed_sum.  The assignment depends only on nblk, R and T,
+// so the result does not depend on scheduling.  vs, vc: T doubles of shared memory each; tot[r] receives
+// the totals.
+__device__ __forceinline__ void grid_fixed_sum(const double* partials, int nblk, int R, double* vs, double* vc,
+                                               double* tot)
+{
+    const int per = (int)blockDim.x / R;
+    const int r = (int)threadIdx.x % R;
+    constexpr int D = 8;
+    NeumaierSum s;
+    int j = (int)threadIdx.x / R;
+    for (; j + (D - 1) * per < nblk; j += D * per) {
+        double v[D];
+#pragma unroll
+        for (int i = 0; i < D; ++i) v[i] = __ldcg(partials + (int64_t)(j + i * per) * R + r);
+#pragma unroll
+        for (int i = 0; i < D; ++i) s.add(v[i]);
+    }
+    for (; j < nblk; j += per) s.add(__ldcg(partials + (int64_t)j * R + r));
+    vs[threadIdx.x] = s.s;
+    vc[threadIdx.x] = s.c;
+    tree_fixed_sum(vs, vc, per, R);
+    if ((int)threadIdx.x < R) tot[threadIdx.x] = vs[threadIdx.x] + vc[threadIdx.x];
+    __syncthreads();
+}
+
+// Scalars of the step for the block's right-hand sides, in shared memory: 1 / b_{k-1} (x_k = u_k / b_{k-1})
+// and b_{k-1} / b_{k-2} (the coefficient of u_{k-1} in v_{k+1}).  Read per epilogue row, so that they
+// hold no registers across the column loop.  Needs at least R threads per block.
+template <int R>
+__device__ __forceinline__ void load_step_scalars(const StepParams& p, double (&sc)[2][R])
+{
+    if (threadIdx.x < R) {
+        const double nb = p.scal[kScal * threadIdx.x + 1], nbp = p.scal[kScal * threadIdx.x + 2];
+        sc[0][threadIdx.x] = 1.0 / nb;
+        sc[1][threadIdx.x] = nb / nbp;
+    }
+    __syncthreads();
+}
+
+// Reduction of the sum Re<u_k, H u_k> over the block, then by the last block over all blocks in a fixed
+// order; writes a_k = Re<u_k, H u_k> / b_{k-1}^2 and advances the step index.
 template <int RPT, int TPR>
-__device__ __forceinline__ void reduce_and_finalize(const StepParams& p, SliceSums* acc_s)
+__device__ __forceinline__ void reduce_and_finalize(const StepParams& p, double* acc_s)
 {
     constexpr int R = RPT * TPR;
     const int lane = threadIdx.x & 31;
@@ -66,29 +146,20 @@ __device__ __forceinline__ void reduce_and_finalize(const StepParams& p, SliceSu
 #pragma unroll
     for (int t = 0; t < RPT; ++t) {
 #pragma unroll
-        for (int off = TPR; off < 32; off <<= 1) {
-            acc_s[t].s1 += __shfl_xor_sync(0xffffffffu, acc_s[t].s1, off);
-            acc_s[t].s2 += __shfl_xor_sync(0xffffffffu, acc_s[t].s2, off);
-            acc_s[t].s3 += __shfl_xor_sync(0xffffffffu, acc_s[t].s3, off);
-            acc_s[t].s4 += __shfl_xor_sync(0xffffffffu, acc_s[t].s4, off);
-        }
+        for (int off = TPR; off < 32; off <<= 1) acc_s[t] += __shfl_xor_sync(0xffffffffu, acc_s[t], off);
     }
-    __shared__ double red[8][R][4];
+    __shared__ double red[8][R];
     const int wib = threadIdx.x >> 5;
     if (sub == 0) {
 #pragma unroll
-        for (int t = 0; t < RPT; ++t) {
-            const int r = q * RPT + t;
-            red[wib][r][0] = acc_s[t].s1; red[wib][r][1] = acc_s[t].s2;
-            red[wib][r][2] = acc_s[t].s3; red[wib][r][3] = acc_s[t].s4;
-        }
+        for (int t = 0; t < RPT; ++t) red[wib][q * RPT + t] = acc_s[t];
     }
     __syncthreads();
-    if (threadIdx.x < R * 4) {
-        const int r = threadIdx.x >> 2, k = threadIdx.x & 3;
+    if (threadIdx.x < R) {
+        const int r = threadIdx.x;
         NeumaierSum a;
-        for (int wI = 0; wI < (int)(blockDim.x >> 5); ++wI) a.add(red[wI][r][k]);
-        p.partials[((int64_t)blockIdx.x * R + r) * 4 + k] = a.value();
+        for (int wI = 0; wI < (int)(blockDim.x >> 5); ++wI) a.add(red[wI][r]);
+        p.partials[(int64_t)blockIdx.x * R + r] = a.value();
     }
     // the last block to finish reduces all blocks in a fixed order
     __shared__ bool last;
@@ -98,27 +169,16 @@ __device__ __forceinline__ void reduce_and_finalize(const StepParams& p, SliceSu
     __syncthreads();
     if (!last) return;
     __threadfence();
-    __shared__ double tot[R][4];
-    if (threadIdx.x < R * 4) {
-        const int r = threadIdx.x >> 2, k = threadIdx.x & 3;
-        NeumaierSum a;
-        for (unsigned int bI = 0; bI < gridDim.x; ++bI) a.add(__ldcg(&p.partials[((int64_t)bI * R + r) * 4 + k]));
-        tot[r][k] = a.value();
-    }
-    __syncthreads();
+    __shared__ double fin_s[256], fin_c[256], tot[R];
+    grid_fixed_sum(p.partials, (int)gridDim.x, R, fin_s, fin_c, tot);
     if (threadIdx.x < R) {
         const int r = threadIdx.x;
         const unsigned int step = p.counter[1];
-        const double a = tot[r][0];
-        const double b2 = tot[r][1] - 2.0 * a * tot[r][2] + a * a * tot[r][3];
-        const double b = sqrt(fabs(b2));
-        if (!(b > 0.0) || !isfinite(a) || !isfinite(b)) atomicOr(&p.counter[2], 1u);
-        if ((int)step < p.nmax) {
-            p.a_out[(int64_t)r * p.nmax + step] = a;
-            p.b_out[(int64_t)r * p.nmax + step] = b;
-        }
-        p.scal[2 * r] = a;
-        p.scal[2 * r + 1] = b;
+        const double nb = p.scal[kScal * r + 1];
+        const double a = tot[r] / (nb * nb);
+        if (!isfinite(a)) atomicOr(&p.counter[2], 1u);
+        if ((int)step < p.nmax) p.a_out[(int64_t)r * p.nmax + step] = a;
+        p.scal[kScal * r] = a;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -130,14 +190,15 @@ __device__ __forceinline__ void reduce_and_finalize(const StepParams& p, SliceSu
 // One slice of the grouped sliced ELL: GPW = 32/TPR groups; the TPR threads of a group each hold RPT
 // right-hand sides of all G rows of the group.  Per union column a thread reads the column index and
 // the G values (same address for the group's threads) and gathers RPT vector elements of that column
-// once for all G rows.  The epilogue per row adds the on-site term and is FP64 from there:
-// v_{k+1} = y - b_{k-1} x_{k-1} rounded once, and the four dot-product terms.  cp/vp point at the
-// thread's group in the slice record, in global memory (streamed) or in shared memory (SMEM).
+// once for all G rows: y = H u_k.  The epilogue per row adds the on-site term and is FP64 from there:
+// v_{k+1} = y / b_{k-1} - (b_{k-1} / b_{k-2}) u_{k-1} rounded once, and the term of Re<u_k, y>.  cp/vp
+// point at the thread's group in the slice record; the indices come from shared memory (SMEM) or global
+// memory (streamed), the values likewise (SMEM_VAL).  U columns are in flight per batch.
 // FIELD: field-batched values (FieldVal), the thread's field is that of its first right-hand side.
-template <typename VT, bool CPLX, int G, int RPT, int TPR, bool SMEM, bool FIELD = false>
+template <typename VT, bool CPLX, int G, int RPT, int TPR, bool SMEM, bool FIELD, int U, bool SMEM_VAL>
 __device__ __forceinline__ void group_slice(const StepParams& p, int64_t s, int w, const int32_t* __restrict__ cp,
                                             const typename StoredVal<VT, CPLX, FIELD>::t* __restrict__ vp,
-                                            const double* cb, SliceSums* acc_s)
+                                            const double (&sc)[2][RPT * TPR], double* acc_s)
 {
     using C2 = typename V2<VT>::t;
     constexpr int GPW = 32 / TPR;
@@ -153,9 +214,9 @@ __device__ __forceinline__ void group_slice(const StepParams& p, int64_t s, int 
     C2 acc[G][RPT];
     typename FieldMult<VT>::t mf = 0;
     if constexpr (FIELD) mf = (typename FieldMult<VT>::t)(int64_t)p.field_m[q * RPT];
-    group_columns<VT, CPLX, G, RPT, TPR, SMEM, FIELD>(xc, w, cp, vp, acc, mf);
-    // epilogue per row: the on-site term (own x_k row, loaded here so that it holds no registers during
-    // the column loop), then v_{k+1} and the dot-product terms in FP64
+    group_columns<VT, CPLX, G, RPT, TPR, SMEM, FIELD, U, SMEM_VAL>(xc, w, cp, vp, acc, mf);
+    // epilogue per row: the on-site term (own u_k row, loaded here so that it holds no registers during
+    // the column loop), then v_{k+1} and the dot-product term in FP64
 #pragma unroll
     for (int g = 0; g < G; ++g) {
         C2 xo[RPT], xm[RPT], vn[RPT];
@@ -166,14 +227,11 @@ __device__ __forceinline__ void group_slice(const StepParams& p, int64_t s, int 
         for (int t = 0; t < RPT; ++t) {
             acc[g][t].x = fma(d, xo[t].x, acc[g][t].x);
             acc[g][t].y = fma(d, xo[t].y, acc[g][t].y);
-            vn[t].x = (VT)((double)acc[g][t].x - cb[t] * (double)xm[t].x);
-            vn[t].y = (VT)((double)acc[g][t].y - cb[t] * (double)xm[t].y);
-            const double xr = xo[t].x, xi = xo[t].y, yr = acc[g][t].x, yi = acc[g][t].y;
-            const double vr = vn[t].x, vi = vn[t].y;
-            acc_s[t].s1 += xr * yr + xi * yi;
-            acc_s[t].s2 += vr * vr + vi * vi;
-            acc_s[t].s3 += xr * vr + xi * vi;
-            acc_s[t].s4 += xr * xr + xi * xi;
+            const double ib = sc[0][q * RPT + t], rb = sc[1][q * RPT + t];
+            const double yr = acc[g][t].x, yi = acc[g][t].y;
+            vn[t].x = (VT)(yr * ib - rb * (double)xm[t].x);
+            vn[t].y = (VT)(yi * ib - rb * (double)xm[t].y);
+            acc_s[t] += (double)xo[t].x * yr + (double)xo[t].y * yi;
         }
         VecIO<VT, RPT>::store(vout + (row0 + g) * R + q * RPT, vn);
     }
@@ -182,20 +240,18 @@ __device__ __forceinline__ void group_slice(const StepParams& p, int64_t s, int 
 // Matrix records read from global memory.  Every block owns a contiguous range of slices (a compact
 // region of the row order); its warps take neighbouring slices, so the rows they gather overlap in L1.
 // FIELD: the field-batched layout (values FieldVal<VT>, fields p.field_m).
-template <typename VT, bool CPLX, int G, int RPT, int TPR, bool FIELD = false>
+template <typename VT, bool CPLX, int G, int RPT, int TPR, bool FIELD = false, int U = kColUnroll>
 __global__ void __launch_bounds__(256) k_spmm_step(StepParams p)
 {
     using HT = typename StoredVal<VT, CPLX, FIELD>::t;
     constexpr int GPW = 32 / TPR;
-    const int q = (threadIdx.x & 31) % TPR;
+    constexpr int R = RPT * TPR;
     const int sub = (threadIdx.x & 31) / TPR;
-    double cb[RPT];
-    SliceSums acc_s[RPT];
+    __shared__ double sc[2][R];
+    load_step_scalars<R>(p, sc);
+    double acc_s[RPT];
 #pragma unroll
-    for (int t = 0; t < RPT; ++t) {
-        cb[t] = p.scal[2 * (q * RPT + t) + 1];
-        acc_s[t] = SliceSums{0.0, 0.0, 0.0, 0.0};
-    }
+    for (int t = 0; t < RPT; ++t) acc_s[t] = 0.0;
     const int nwb = (int)(blockDim.x >> 5);
     const int64_t per = (p.nslices + gridDim.x - 1) / gridDim.x;
     const int64_t s0 = (int64_t)blockIdx.x * per;
@@ -204,9 +260,9 @@ __global__ void __launch_bounds__(256) k_spmm_step(StepParams p)
         const int64_t base = p.slice_ptr[s];
         const int w = (int)((p.slice_ptr[s + 1] - base) / GPW);
         const unsigned char* rec = p.mat + base * p.entry_bytes;
-        group_slice<VT, CPLX, G, RPT, TPR, false, FIELD>(p, s, w, reinterpret_cast<const int32_t*>(rec) + sub,
-                                                  reinterpret_cast<const HT*>(rec + (size_t)w * GPW * 4) + sub * G,
-                                                  cb, acc_s);
+        group_slice<VT, CPLX, G, RPT, TPR, false, FIELD, U, false>(
+            p, s, w, reinterpret_cast<const int32_t*>(rec) + sub,
+            reinterpret_cast<const HT*>(rec + (size_t)w * GPW * 4) + sub * G, sc, acc_s);
     }
     reduce_and_finalize<RPT, TPR>(p, acc_s);
 }
@@ -304,16 +360,36 @@ __device__ __forceinline__ void prefetch_epilogue(const StepParams& p, int64_t s
     }
 }
 
+// Bulk prefetch of `bytes` contiguous bytes into L2 (one instruction; address and size multiples of 16).
+__device__ __forceinline__ void bulk_prefetch_l2(const void* a, uint32_t bytes)
+{
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"(bytes) : "memory");
+}
+
+// The rows of u_k that slice s owns (contiguous in the row order; most of its neighbours' gathers of
+// them come later in the block's sweep), prefetched into L2 by lane 0 of the warp.  s < nslices, so the
+// range lies inside the vector (nslices * GPW * G <= npad rows).
+template <typename VT, int R, int G, int GPW>
+__device__ __forceinline__ void prefetch_ahead(const StepParams& p, int64_t s)
+{
+    constexpr int BLK = GPW * G * R * (int)sizeof(typename V2<VT>::t);   // multiple of 16 (R * 8 * GPW * G)
+    if ((threadIdx.x & 31) == 0 && s < p.nslices)
+        bulk_prefetch_l2(static_cast<const char*>(p.x_cur) + (size_t)s * BLK, (uint32_t)BLK);
+}
+
 // Matrix records staged in shared memory.  Each warp owns two record buffers and an mbarrier per
 // buffer; its lane 0 copies the record of the warp's next-but-one slice with one bulk copy while the
 // warp works on the current one, so the column indices that the gathers depend on come from shared
-// memory instead of a DRAM round trip per unrolled column batch.  Optionally the warp first
-// prefetches all the vector rows a slice will gather.  Records larger than a buffer (the largest
-// 0.5 %) are read in place.  No block-wide synchronisation in the loop; every wait is bounded (flag
-// bit 2, GBN_ERR_TIMEOUT).
+// memory instead of a DRAM round trip per unrolled column batch.  SV: the whole record (indices and
+// values) is staged; otherwise only its column indices, and the values stream from global memory beside
+// the gathers (their loads do not gate any address), which leaves more of the SM's memory to L1.
+// Optionally the warp first prefetches all the vector rows a slice will gather.  Records larger than a
+// buffer (the largest 0.5 %) are read in place.  No block-wide synchronisation in the loop; every wait
+// is bounded (flag bit 2, GBN_ERR_TIMEOUT).
 // FIELD: the field-batched layout (values FieldVal<VT>, fields p.field_m).
-template <typename VT, bool CPLX, int G, int RPT, int TPR, bool FIELD = false>
-__global__ void __launch_bounds__(256) k_spmm_staged(StepParams p)
+template <typename VT, bool CPLX, int G, int RPT, int TPR, bool FIELD = false, int U = kColUnroll, bool SV = true,
+          int MINB = 1>
+__global__ void __launch_bounds__(256, MINB) k_spmm_staged(StepParams p)
 {
     using HT = typename StoredVal<VT, CPLX, FIELD>::t;
     constexpr int GPW = 32 / TPR;
@@ -321,30 +397,35 @@ __global__ void __launch_bounds__(256) k_spmm_staged(StepParams p)
     extern __shared__ __align__(128) unsigned char dyn[];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
-    const int q = lane % TPR;
     const int sub = lane / TPR;
     uint64_t* bar = reinterpret_cast<uint64_t*>(dyn) + 2 * wib;
-    unsigned char* buf = dyn + 128 + (size_t)wib * 2 * p.cap_record;
-    double cb[RPT];
-    SliceSums acc_s[RPT];
+    const int64_t cap = p.cap_record;   // bytes of one buffer: whole records (SV) or their index part
+    unsigned char* buf = dyn + 128 + (size_t)wib * 2 * cap;
+    __shared__ double sc[2][R];
+    load_step_scalars<R>(p, sc);
+    double acc_s[RPT];
 #pragma unroll
-    for (int t = 0; t < RPT; ++t) {
-        cb[t] = p.scal[2 * (q * RPT + t) + 1];
-        acc_s[t] = SliceSums{0.0, 0.0, 0.0, 0.0};
-    }
+    for (int t = 0; t < RPT; ++t) acc_s[t] = 0.0;
     const int nwb = (int)(blockDim.x >> 5);
     const int64_t per = (p.nslices + gridDim.x - 1) / gridDim.x;
     const int64_t s0 = (int64_t)blockIdx.x * per;
     const int64_t s1e = (s0 + per < p.nslices) ? s0 + per : p.nslices;
     const int64_t eb = p.entry_bytes;
 
-    auto rec_bytes = [&](int64_t s) { return (p.slice_ptr[s + 1] - p.slice_ptr[s]) * eb; };
-    auto issue = [&](int64_t s, int st) {   // lane 0 only; records above the cap are not copied
-        const int64_t bytes = rec_bytes(s);
+    // bytes copied for slice s: the record, or its column indices (the first 4 w GPW bytes)
+    auto copy_bytes = [&](int64_t s) { return (p.slice_ptr[s + 1] - p.slice_ptr[s]) * (SV ? eb : 4); };
+    // lane 0 only.  Records above the cap are not copied but prefetched into L2 whole, and so is the
+    // value part of a record whose indices alone are staged, so that the loads read in place hit L2.
+    auto issue = [&](int64_t s, int st) {
+        const int64_t nent = p.slice_ptr[s + 1] - p.slice_ptr[s];
+        const int64_t bytes = nent * (SV ? eb : 4);
+        const unsigned char* src = p.mat + p.slice_ptr[s] * eb;
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        const bool copy = bytes > 0 && bytes <= p.cap_record;
+        const bool copy = bytes > 0 && bytes <= cap;
         mbar_expect_tx(&bar[st], copy ? (uint32_t)bytes : 0u);
-        if (copy) bulk_g2s(buf + st * p.cap_record, p.mat + p.slice_ptr[s] * eb, (uint32_t)bytes, &bar[st]);
+        if (copy) bulk_g2s(buf + st * cap, src, (uint32_t)bytes, &bar[st]);
+        if (nent > 0 && !copy) bulk_prefetch_l2(src, (uint32_t)(nent * eb));
+        else if (nent > 0 && !SV) bulk_prefetch_l2(src + nent * 4, (uint32_t)(nent * (eb - 4)));
     };
 
     if (lane == 0) {
@@ -373,20 +454,20 @@ __global__ void __launch_bounds__(256) k_spmm_staged(StepParams p)
         pending &= ~(1u << st);
         const int64_t base = p.slice_ptr[s];
         const int w = (int)((p.slice_ptr[s + 1] - base) / GPW);
-        const int64_t bytes = rec_bytes(s);
+        const unsigned char* grec = p.mat + base * eb;
         if (p.prefetch >= 3) prefetch_epilogue<VT, R, G, GPW>(p, s);
-        if (bytes <= p.cap_record) {
-            const unsigned char* rec = buf + st * p.cap_record;
+        if (p.prefetch >= 5) prefetch_ahead<VT, R, G, GPW>(p, s + (int64_t)(p.prefetch == 5 ? 1 : p.prefetch == 6 ? 2 : 4) * nwb);
+        if (copy_bytes(s) <= cap) {
+            const unsigned char* rec = buf + st * cap;
             if (p.prefetch == 1 || p.prefetch == 2)
                 prefetch_rows<VT, R>(p, reinterpret_cast<const int32_t*>(rec), w * GPW);
-            group_slice<VT, CPLX, G, RPT, TPR, true, FIELD>(p, s, w, reinterpret_cast<const int32_t*>(rec) + sub,
-                                                     reinterpret_cast<const HT*>(rec + (size_t)w * GPW * 4) + sub * G,
-                                                     cb, acc_s);
+            const HT* vp = reinterpret_cast<const HT*>((SV ? rec : grec) + (size_t)w * GPW * 4) + sub * G;
+            group_slice<VT, CPLX, G, RPT, TPR, true, FIELD, U, SV>(p, s, w, reinterpret_cast<const int32_t*>(rec) + sub,
+                                                                  vp, sc, acc_s);
         } else {
-            const unsigned char* rec = p.mat + base * eb;
-            group_slice<VT, CPLX, G, RPT, TPR, false, FIELD>(p, s, w, reinterpret_cast<const int32_t*>(rec) + sub,
-                                                      reinterpret_cast<const HT*>(rec + (size_t)w * GPW * 4) + sub * G,
-                                                      cb, acc_s);
+            group_slice<VT, CPLX, G, RPT, TPR, false, FIELD, U, false>(
+                p, s, w, reinterpret_cast<const int32_t*>(grec) + sub,
+                reinterpret_cast<const HT*>(grec + (size_t)w * GPW * 4) + sub * G, sc, acc_s);
         }
         __syncwarp();   // every lane is done with this buffer before it is refilled
         if (s + 2 * nwb < s1e) {
@@ -402,6 +483,55 @@ __global__ void __launch_bounds__(256) k_spmm_staged(StepParams p)
         __syncwarp();
     }
     reduce_and_finalize<RPT, TPR>(p, acc_s);
+}
+
+// ---------------------------------------------------------------------------- kernel selection
+template <typename VT, bool CPLX, int G, int RP, int TP>
+StepFn step_variant(bool staged, StepVariant v)
+{
+    constexpr int kWide = sizeof(VT) == 4 ? 4 : 2;   // right-hand sides of a 32-byte load
+    constexpr bool kAll = !CPLX && (RP == kWide || TP == 1);
+    if constexpr (kAll) {
+        if (!staged) {
+            if (v.min_blocks != 1) return nullptr;
+            return v.unroll == 8 ? k_spmm_step<VT, CPLX, G, RP, TP, false, 8> : k_spmm_step<VT, CPLX, G, RP, TP>;
+        }
+        if (v.unroll == 8 && v.min_blocks == 3)
+            return v.stage_values ? k_spmm_staged<VT, CPLX, G, RP, TP, false, 8, true, 3>
+                                  : k_spmm_staged<VT, CPLX, G, RP, TP, false, 8, false, 3>;
+        if (v.min_blocks != 1) return nullptr;
+        if (v.unroll == 8)
+            return v.stage_values ? k_spmm_staged<VT, CPLX, G, RP, TP, false, 8, true>
+                                  : k_spmm_staged<VT, CPLX, G, RP, TP, false, 8, false>;
+        return v.stage_values ? k_spmm_staged<VT, CPLX, G, RP, TP, false, 4, true>
+                              : k_spmm_staged<VT, CPLX, G, RP, TP, false, 4, false>;
+    } else {
+        if (v.unroll != 4 || !v.stage_values || v.min_blocks != 1) return nullptr;
+        return staged ? k_spmm_staged<VT, CPLX, G, RP, TP> : k_spmm_step<VT, CPLX, G, RP, TP>;
+    }
+}
+
+template <typename VT, bool CPLX, int G>
+StepFn step_pick_g(int rpt, int tpr, bool staged, StepVariant v)
+{
+#define GBN_CASE(RP, TP) \
+    if (rpt == RP && tpr == TP) return step_variant<VT, CPLX, G, RP, TP>(staged, v);
+    GBN_CASE(1, 1) GBN_CASE(1, 2) GBN_CASE(1, 4) GBN_CASE(1, 8) GBN_CASE(1, 16) GBN_CASE(1, 32)
+    GBN_CASE(2, 1) GBN_CASE(2, 2) GBN_CASE(2, 4) GBN_CASE(2, 8) GBN_CASE(2, 16)
+    if constexpr (sizeof(VT) == 4) {
+        GBN_CASE(4, 1) GBN_CASE(4, 2) GBN_CASE(4, 4) GBN_CASE(4, 8)
+    }
+#undef GBN_CASE
+    return nullptr;
+}
+
+template <typename VT, bool CPLX>
+StepFn step_pick(int G, int rpt, int tpr, bool staged, StepVariant v)
+{
+    if (G == 1) return step_pick_g<VT, CPLX, 1>(rpt, tpr, staged, v);
+    if (G == 2) return step_pick_g<VT, CPLX, 2>(rpt, tpr, staged, v);
+    if (G == 4) return step_pick_g<VT, CPLX, 4>(rpt, tpr, staged, v);
+    return nullptr;
 }
 
 }  // namespace gbn

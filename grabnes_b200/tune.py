@@ -3,34 +3,67 @@
 Candidates: rows per group of the matrix layout (1 = plain sliced ELL; 2, 4 = neighbouring rows share
 one gather per union column), right-hand sides per thread (the width of each thread's vector loads,
 and with it the groups a warp processes per slice), the matrix path (slice records staged in shared
-memory by per-warp bulk copies, or read from global memory), a prefetch (staged path only) of the
-gather rows of each slice or of the rows its epilogue reads, and a cap on resident blocks per SM.
-Each candidate runs a short recursion on the caller's own Hamiltonian and start vectors; the one with
-the smallest device time per step (update + sparse product, CUDA events) is kept on the context.
+memory by per-warp bulk copies, or read from global memory), the union columns whose gathers are in
+flight together (4 or 8), a prefetch (staged path only) of the gather rows of each slice, of the rows
+its epilogue reads, or of those and the rows of u_k one or more sweeps ahead, and a cap on resident
+blocks per SM.  The search runs in two stages on the caller's own Hamiltonian and start vectors:
+the layout and path (rows per group, right-hand sides per thread, staged or not) at the default
+variant, then the variant (unroll, prefetch) of the best layout.  Each candidate runs a short
+recursion; the one with the smallest device time per step (update + sparse product, CUDA events) is
+kept on the context.
 """
 import itertools
 
 
-def autotune(ctx, u, precision, nsteps=12, rhs_per_thread=(1, 2, 4), blocks_per_sm=(0,),
-             rows_per_group=(1, 2, 4), staged=(0, 1), prefetch=(0, 1, 4)):
-    results = []
-    cands = [c for c in itertools.product(rows_per_group, staged, prefetch, rhs_per_thread, blocks_per_sm)
-             if c[1] == 1 or c[2] == 0]   # the prefetch belongs to the staged path
-    for grp, st, pf, rpt, bps in cands:
-        try:
-            ctx.set_tuning(rpt, bps, grp, st, pf)
-            ctx.stage_phases(u, precision)
-            ctx.run_staged(nsteps)
-            ctx.run_staged(nsteps)
-        except Exception as exc:   # a candidate the library refuses is skipped
-            results.append(dict(rows_per_group=grp, staged=st, prefetch=pf, rhs_per_thread=rpt, blocks_per_sm=bps,
-                                error=str(exc)))
-            continue
-        spmm, upd = ctx.kernel_timing()
-        results.append(dict(rows_per_group=grp, staged=st, prefetch=pf, rhs_per_thread=rpt, blocks_per_sm=bps,
-                            spmm_ms=spmm, update_ms=upd, step_ms=spmm + upd))
-    ok = [r for r in results if "step_ms" in r]
-    best = min(ok, key=lambda r: r["step_ms"])
+def _time(ctx, u, precision, nsteps, cand):
+    grp, st, pf, rpt, bps, unroll, sv, mb = cand
+    try:
+        ctx.set_tuning(rpt, bps, grp, st, pf)
+        ctx.set_kernel_variant(unroll, sv, mb)
+        ctx.stage_phases(u, precision)
+        ctx.run_staged(nsteps)
+        ctx.run_staged(nsteps)
+    except Exception as exc:   # a candidate the library refuses is skipped
+        return dict(rows_per_group=grp, staged=st, prefetch=pf, rhs_per_thread=rpt, blocks_per_sm=bps,
+                    unroll=unroll, stage_values=sv, min_blocks=mb, error=str(exc))
+    spmm, upd = ctx.kernel_timing()
+    return dict(rows_per_group=grp, staged=st, prefetch=pf, rhs_per_thread=rpt, blocks_per_sm=bps, unroll=unroll,
+                stage_values=sv, min_blocks=mb, spmm_ms=spmm, update_ms=upd, step_ms=spmm + upd)
+
+
+def _key(r):
+    return (r["rows_per_group"], r["staged"], r["prefetch"], r["rhs_per_thread"], r["blocks_per_sm"], r["unroll"],
+            r["stage_values"], r["min_blocks"])
+
+
+def apply(ctx, best):
+    """Set a tuning dictionary (as returned by autotune) on the context."""
     ctx.set_tuning(best["rhs_per_thread"], best["blocks_per_sm"], best["rows_per_group"], best["staged"],
                    best["prefetch"])
+    ctx.set_kernel_variant(best.get("unroll", 0), best.get("stage_values", -1), best.get("min_blocks", 0))
+
+
+def autotune(ctx, u, precision, nsteps=12, rhs_per_thread=(1, 2, 4), blocks_per_sm=(0,),
+             rows_per_group=(1, 2, 4), staged=(0, 1), prefetch=(0, 4, 6, 7), unroll=(4, 8)):
+    results = []
+    # stage 1: layout and matrix path at the library's default variant (-1/0: chosen by the library)
+    for grp, st, rpt, bps in itertools.product(rows_per_group, staged, rhs_per_thread, blocks_per_sm):
+        results.append(_time(ctx, u, precision, nsteps, (grp, st, -1, rpt, bps, 0, -1, 0)))
+    ok = [r for r in results if "step_ms" in r]
+    best = min(ok, key=lambda r: r["step_ms"])
+    # stage 2: unroll, prefetch, staged values or indices only, and the register bound of the best layout
+    seen = {_key(r) for r in results}
+    pfs = prefetch if best["staged"] == 1 else (0,)
+    svs = (1, 0) if best["staged"] == 1 else (1,)
+    for pf, un, sv, mb in itertools.product(pfs, unroll, svs, (1, 3)):
+        if mb == 3 and (un != 8 or best["staged"] != 1):
+            continue
+        cand = (best["rows_per_group"], best["staged"], pf, best["rhs_per_thread"], best["blocks_per_sm"], un, sv, mb)
+        if cand in seen:
+            continue
+        seen.add(cand)
+        results.append(_time(ctx, u, precision, nsteps, cand))
+    ok = [r for r in results if "step_ms" in r]
+    best = min(ok, key=lambda r: r["step_ms"])
+    apply(ctx, best)
     return best, results

@@ -114,10 +114,18 @@ int         gbn_set_stream(gbn_ctx* ctx, void* cuda_stream);
  * records in shared memory with bulk asynchronous copies, 0 = records read from global memory,
  * -1 = staged when two records per warp fit in shared memory) and, for the staged path, a prefetch of
  * the vector rows each slice gathers (0 = none, 1 = into L2, 2 = into L1) or of the rows its epilogue
- * reads (3 = into L1, 4 = into L2; -1 = the default, 4).  Used by the autotuner
+ * reads (3 = into L1, 4 = into L2; 5, 6, 7 = as 4, and one bulk prefetch into L2 of the rows of the
+ * warp's slice 1, 2 or 4 sweeps ahead; -1 = the default, 4).  Used by the autotuner
  * (grabnes_b200/tune.py). */
 int         gbn_set_tuning(gbn_ctx* ctx, int32_t rhs_per_thread, int32_t blocks_per_sm, int32_t rows_per_group,
                            int32_t staged, int32_t prefetch);
+/* Variant of the recursion's sparse-product kernel: union columns whose gathers are in flight together
+ * per batch (4 or 8; 0 = the default), for the staged path whether the staged slice records carry the
+ * values (1) or only the column indices, with the values prefetched into L2 and streamed beside the
+ * gathers (0; -1 = the default), and the resident blocks per SM the kernel's registers are bounded for
+ * (1 or 3, 3 only with unroll 8 on the staged path; 0 = 1).  No counterpart in the reference.  Used by
+ * the autotuner (grabnes_b200/tune.py). */
+int         gbn_set_kernel_variant(gbn_ctx* ctx, int32_t col_unroll, int32_t stage_values, int32_t min_blocks);
 /* Kernels launched by this context since creation (for launch accounting). */
 int64_t     gbn_launch_count(const gbn_ctx* ctx);
 /* Device time of the recursion loop of the last gbn_lanczos* / gbn_run_staged call and its number of

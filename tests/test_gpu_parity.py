@@ -179,8 +179,8 @@ def test_mixed_precision_dos(ctx):
 @pytest.mark.parametrize("rpt", [1, 2, 4])
 def test_layout_variants_agree(ctx, rpt):
     """Rows per group 1, 2 and 4 of the matrix layout, records staged in shared memory (without a
-    prefetch, with the gather-row prefetch into L2 or L1, with the epilogue-row prefetch into L1 or L2)
-    or read from global memory, for every split of the right-hand sides over threads: the same products
+    prefetch, with the gather-row prefetch into L2 or L1, with the epilogue-row prefetch into L1 or L2,
+    with that and the bulk L2 prefetch of u_k rows 1, 2 or 4 sweeps ahead) or read from global memory, for every split of the right-hand sides over threads: the same products
     summed in another order (union columns of a group instead of a row's own columns), so mixed-precision
     a_n, b_n agree to FP32 rounding over 60 steps; a prefetch is only a hint, so every prefetch mode
     gives exactly the results of the staged path without one."""
@@ -192,7 +192,7 @@ def test_layout_variants_agree(ctx, rpt):
     try:
         for grp in (1, 2, 4):
             staged_runs = []
-            for staged, pf in ((0, 0), (1, 0), (1, 1), (1, 2), (1, 3), (1, 4)):
+            for staged, pf in ((0, 0), (1, 0), (1, 1), (1, 2), (1, 3), (1, 4), (1, 5), (1, 6), (1, 7)):
                 ctx.set_tuning(rpt, 0, grp, staged, pf)
                 out.append(ctx.lanczos_phases(u, 60, G.GBN_MIXED))
                 if staged:
@@ -203,6 +203,36 @@ def test_layout_variants_agree(ctx, rpt):
         ctx.set_tuning()
     for k in range(1, len(out)):
         assert _rel(out[0][0], out[k][0]) <= 1e-6 and _rel(out[0][1], out[k][1]) <= 1e-6
+
+
+@pytest.mark.parametrize("prec", [G.GBN_MIXED, G.GBN_FP64])
+@pytest.mark.parametrize("grp", [1, 2, 4])
+def test_kernel_variants_agree(ctx, grp, prec):
+    """The product's variants (4 or 8 union columns in flight, staged records with values or with the
+    column indices only, registers bounded for 1 or 3 blocks per SM) add each row's products in the same
+    order; only the grid, and with it the split of the dot products over blocks, follows the occupancy of
+    the variant.  So a_n, b_n agree to the rounding of the sums: 1e-6 relative in mixed precision, 1e-10
+    in FP64, and FP64 matches the oracle (1e-10)."""
+    r = built("tbg")
+    n = r["geo"]["n"]
+    ctx.load_hamiltonian(r["nb"]["nneigh"], r["nb"]["nlist"], r["hop"], r["h0"])
+    u = np.stack([orc.rng_draws(31 + k, n) for k in range(16)])
+    runs = []
+    try:
+        ctx.set_tuning(0, 0, grp, 1, 4)
+        for un, sv, mb in ((4, 1, 1), (8, 1, 1), (4, 0, 1), (8, 0, 1), (8, 1, 3), (8, 0, 3)):
+            ctx.set_kernel_variant(un, sv, mb)
+            runs.append(ctx.lanczos_phases(u, 200, prec))
+    finally:
+        ctx.set_tuning()
+        ctx.set_kernel_variant()
+    tol = 1e-6 if prec == G.GBN_MIXED else 1e-10
+    for a, b in runs[1:]:
+        assert _rel(a, runs[0][0]) <= tol and _rel(b, runs[0][1]) <= tol
+    if prec == G.GBN_FP64:
+        psi = np.exp(2j * np.pi * u[0]) / np.sqrt(n)
+        a0, b0 = orc.recursion(r["nb"], r["hop"], r["h0"], psi, 200, 0)
+        assert _rel(runs[0][0][0], a0) <= 1e-10 and _rel(runs[0][1][0], b0) <= 1e-10
 
 
 @pytest.mark.parametrize("grp", [1, 2, 4])
