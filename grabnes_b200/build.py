@@ -68,7 +68,7 @@ def build(verbose=False, jobs=8):
 def build_driver(verbose=False):
     """The `grabnes Gendata.in` executable (host C++ over the C ABI), next to the library."""
     src = os.path.join(DRIVER_DIR, "grabnes.cpp")
-    deps = [src, LIB] + glob.glob(os.path.join(HERE, "..", "include", "*.h"))
+    deps = [src, LIB] + glob.glob(os.path.join(HERE, "..", "include", "*.h")) + glob.glob(os.path.join(DRIVER_DIR, "*.inc"))
     if os.path.exists(DRIVER) and os.path.getmtime(DRIVER) >= max(os.path.getmtime(d) for d in deps):
         return DRIVER
     cxx = shutil.which("g++") or "g++"

@@ -35,9 +35,21 @@
 namespace {
 
 const double kPi = 3.14159265358979323846;
-const double kFluxQuantum = 6.62606896e-34 / 1.602176565e-19;   // h/e (constants.f90)
-const double kShellRadius[9] = {1.0, 1.7320508075688772, 2.0, 2.6457513110645906, 3.0,
-                                3.4641016151377544, 3.6055512754639891, 4.0, 4.3588989435406740};
+// the shell radii and constants shared with grabnes_b200/model.py (gendata_keys.inc)
+#define GBN_ALIAS(present, former)
+#define GBN_SHELL_RADIUS(r) r,
+#define GBN_CONST(name, value)
+const double kShellRadius[] = {
+#include "gendata_keys.inc"
+};
+#undef GBN_SHELL_RADIUS
+#undef GBN_CONST
+#define GBN_SHELL_RADIUS(r)
+#define GBN_CONST(name, value) const double k##name = value;
+#include "gendata_keys.inc"
+#undef GBN_CONST
+#define GBN_CONST(name, value)
+const double kFluxQuantum = kHPLANCK / kQE;   // h/e
 
 [[noreturn]] void die(const std::string& msg)
 {
@@ -54,29 +66,10 @@ std::string norm_key(const std::string& k)
 }
 
 // former (section-less) names of the keys read here (lanczosKuboCode/Src/MIO/input_aliases.inc)
+#undef GBN_ALIAS
+#define GBN_ALIAS(present, former) {present, former},
 const char* kAliases[][2] = {
-    {"Run.TypeOfSystem", "TypeOfSystem"}, {"Run.Prefix", "Prefix"},
-    {"Structure.LatticeParameter", "LatticeParameter"}, {"Structure.CellSize", "CellSize"},
-    {"Structure.SuperCell", "SuperCell"}, {"Structure.MoireCellParameters", "MoireCellParameters"},
-    {"Structure.CellHeight", "CellHeight"}, {"Structure.InterlayerDistance", "InterlayerDistance"},
-    {"Interlayer.TypeOfBL", "TypeOfBL"}, {"Interlayer.Vpppi0", "vpppi0"}, {"Interlayer.Vppsigma0", "vppsigma0"},
-    {"Interlayer.BLdelta", "BLdelta"}, {"Interlayer.AddSecondLayerInteractions", "addSecondLayerInteractions"},
-    {"Intralayer.KoshinoIntralayer", "KoshinoIntralayer"}, {"Moire.Potential", "MoirePotential"},
-    {"Moire.Jeil", "MoireJeil"}, {"Moire.OnlyH0", "MoireOnlyH0"}, {"Moire.OnlyHZ", "MoireOnlyHZ"},
-    {"Moire.NoH0AndHZ", "MoireNoH0AndHZ"}, {"Moire.H0AndHZ", "MoireH0AndHZ"}, {"Moire.PreFactor", "MoirePreFactor"},
-    {"Moire.PotC0", "MoirePotC0"}, {"Moire.PotCz", "MoirePotCz"}, {"Moire.PotCab", "MoirePotCab"},
-    {"Moire.PotPhi0", "MoirePotPhi0"}, {"Moire.PotPhiz", "MoirePotPhiz"}, {"Moire.PotPhiab", "MoirePotPhiab"},
-    {"Moire.LatticePercent", "Latticepercent"}, {"Moire.Twisted", "MoireTwisted"},
-    {"Moire.TwistAngle", "MoireTwistAngle"}, {"Moire.OffDiag", "MoireOffDiag"},
-    {"Moire.OffDiagMidpoint", "MoireOffDiagMidpoint"}, {"Moire.LayerShift1", "MoireLayerShift1"},
-    {"Moire.FirstMoireMassFactor", "MoireFirstMoireMassFactor"},
-    {"Moire.SecondMoireMassFactor", "MoireSecondMoireMassFactor"}, {"Disorder.Anderson", "Anderson"},
-    {"Disorder.AndersonAmp", "AndersonAmp"}, {"Kubo.RecursionNumber", "RecursionNumber"},
-    {"Kubo.Epsilon", "Epsilon"}, {"Kubo.NumberofEnergyPoints", "NumberofEnergyPoints"},
-    {"Kubo.EnergyMin", "EnergyMin"}, {"Kubo.EnergyMax", "EnergyMax"}, {"Kubo.SeedValue", "seedValue"},
-    {"Kubo.SetSeed", "setSeed"}, {"Kubo.NumberofPolynomials", "NumberofPolynomials"},
-    {"Kubo.TimeStep", "TimeStep"}, {"Kubo.NumberofTimeSteps", "NumberofTimeSteps"},
-    {"Kubo.WriteNumberofSteps", "WriteNumberofSteps"}, {"MagField.Value", "MagField"},
+#include "gendata_keys.inc"
 };
 
 // ---------------------------------------------------------------------------- values

@@ -16,36 +16,26 @@ import math
 
 from . import CELL_GRAPHENE, CELL_TBG_MOIRE, Model
 
-SHELL_RADIUS = [1.0, 1.7320508075688772, 2.0, 2.6457513110645906, 3.0,
-                3.4641016151377544, 3.6055512754639891, 4.0, 4.3588989435406740]
-FLUXQ = 6.62606896e-34 / 1.602176565e-19   # h/e of constants.f90
+def _shared_table():
+    """The key aliases, shell radii and constants shared with the drop-in driver
+    (grabnes_b200/driver/gendata_keys.inc, the one list of them)."""
+    import os
+    import re
+    text = open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "driver", "gendata_keys.inc")).read()
+    text = re.sub(r"//[^\n]*", "", text)
+    aliases = dict(re.findall(r'GBN_ALIAS\("([^"]+)",\s*"([^"]+)"\)', text))
+    radii = [float(x) for x in re.findall(r"GBN_SHELL_RADIUS\(([^)]+)\)", text)]
+    consts = {k: float(v) for k, v in re.findall(r"GBN_CONST\((\w+),\s*([^)]+)\)", text)}
+    return aliases, radii, consts
+
+
+_ALIASES, SHELL_RADIUS, _CONSTS = _shared_table()
+FLUXQ = _CONSTS["HPLANCK"] / _CONSTS["QE"]   # h/e of constants.f90
 F2G2_SINGLE_LAYER = {2: -0.2354, 3: 0.1877, 4: 0.0, 5: -0.0633, 6: 0.0, 7: 0.0}   # ham.F90:8331-8350 [eV]
 
 
 # former (section-less) names of the keys read here: lanczosKuboCode/Src/MIO/input_aliases.inc
-FORMER = {
-    "Run.TypeOfSystem": "TypeOfSystem", "Structure.LatticeParameter": "LatticeParameter",
-    "Structure.CellSize": "CellSize", "Structure.SuperCell": "SuperCell",
-    "Structure.MoireCellParameters": "MoireCellParameters", "Structure.CellHeight": "CellHeight",
-    "Structure.InterlayerDistance": "InterlayerDistance", "Interlayer.TypeOfBL": "TypeOfBL",
-    "Interlayer.Vpppi0": "vpppi0", "Interlayer.Vppsigma0": "vppsigma0", "Interlayer.BLdelta": "BLdelta",
-    "Interlayer.AddSecondLayerInteractions": "addSecondLayerInteractions",
-    "Intralayer.KoshinoIntralayer": "KoshinoIntralayer", "Moire.Potential": "MoirePotential",
-    "Moire.Jeil": "MoireJeil", "Moire.OnlyH0": "MoireOnlyH0", "Moire.OnlyHZ": "MoireOnlyHZ",
-    "Moire.NoH0AndHZ": "MoireNoH0AndHZ", "Moire.H0AndHZ": "MoireH0AndHZ", "Moire.PreFactor": "MoirePreFactor",
-    "Moire.PotC0": "MoirePotC0", "Moire.PotCz": "MoirePotCz", "Moire.PotCab": "MoirePotCab",
-    "Moire.PotPhi0": "MoirePotPhi0", "Moire.PotPhiz": "MoirePotPhiz", "Moire.PotPhiab": "MoirePotPhiab",
-    "Moire.LatticePercent": "Latticepercent", "Moire.Twisted": "MoireTwisted", "Moire.TwistAngle": "MoireTwistAngle",
-    "Moire.OffDiag": "MoireOffDiag", "Moire.OffDiagMidpoint": "MoireOffDiagMidpoint",
-    "Moire.LayerShift1": "MoireLayerShift1", "Moire.FirstMoireMassFactor": "MoireFirstMoireMassFactor",
-    "Moire.SecondMoireMassFactor": "MoireSecondMoireMassFactor", "Disorder.Anderson": "Anderson",
-    "Disorder.AndersonAmp": "AndersonAmp", "Kubo.RecursionNumber": "RecursionNumber", "Kubo.Epsilon": "Epsilon",
-    "Kubo.NumberofEnergyPoints": "NumberofEnergyPoints", "Kubo.EnergyMin": "EnergyMin",
-    "Kubo.EnergyMax": "EnergyMax", "Kubo.SeedValue": "seedValue", "Kubo.SetSeed": "setSeed",
-    "Kubo.NumberofPolynomials": "NumberofPolynomials", "Kubo.TimeStep": "TimeStep",
-    "Kubo.NumberofTimeSteps": "NumberofTimeSteps", "Kubo.WriteNumberofSteps": "WriteNumberofSteps",
-    "Run.Prefix": "Prefix",
-}
+FORMER = dict(_ALIASES)
 
 
 def _norm(k):

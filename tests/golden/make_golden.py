@@ -1,8 +1,8 @@
 """Extract the golden fixtures used by the parity tests from the reference checkout.
 
-Run in a container that has the reference at REFERENCE (default /root/reference):
+Run with the path of a checkout of the reference:
 
-    python tests/golden/make_golden.py [REFERENCE]
+    python tests/golden/make_golden.py REFERENCE_CHECKOUT
 
 It writes, next to this script:
   model_survey_fingerprints.json  Hamiltonian fingerprints of the reference's model survey
@@ -49,4 +49,6 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py REFERENCE_CHECKOUT")
+    main(sys.argv[1])
