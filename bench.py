@@ -116,19 +116,36 @@ def barrier(ws):
     replicas.barrier(ws)
 
 
-PROFILE = os.path.join(ROOT, "profiles", "k_spmm_staged_tbg.md")
+PROFILES = os.path.join(ROOT, "profiles")
 
 
-def traffic_from_profile():
-    """DRAM bytes per sparse-product launch at the bench workload, from the committed ncu summary (a
-    capture of the same kernel on the 10 x 10 tiling, scaled by the rows processed)."""
+def kernel_key(best):
+    """Name of the sparse-product kernel a tuning selects, as the ncu summaries in profiles/ label their
+    captures: rows per group, columns in flight, staged values or indices, register bound, prefetch."""
+    staged = best.get("staged", -1) != 0
+    unroll = best.get("unroll", 0) or 8              # library defaults in mixed precision
+    sv = 0 if best.get("stage_values", -1) == 0 else 1
+    g = best.get("rows_per_group", 0) or 2           # default rows per group for 16 vectors of ~33 entries
+    mb = best.get("min_blocks", 0) or (3 if (unroll == 8 and g == 1 and staged) else 1)
+    pf = best.get("prefetch", -1)
+    pf = 6 if pf < 0 else pf
+    if not staged:
+        return f"k_spmm_step<float, real, G={g}, U={unroll}>"
+    return f"k_spmm_staged<float, real, G={g}, U={unroll}, SV={sv}, MINB={mb}, prefetch={pf}>"
+
+
+def traffic_from_profile(key):
+    """DRAM bytes per sparse-product launch at the bench workload for the kernel `key`, from the committed
+    ncu summaries (captures of the same kernel on the 10 x 10 tiling, scaled by the rows processed); None
+    when no summary covers that kernel."""
+    import glob
     import re
-    try:
-        with open(PROFILE) as f:
-            m = re.search(r"dram_bytes_per_launch_bench_workload\s*=\s*([0-9.eE+]+)", f.read())
-        return float(m.group(1)) if m else None
-    except OSError:
-        return None
+    for path in sorted(glob.glob(os.path.join(PROFILES, "*.md"))):
+        with open(path) as f:
+            for m in re.finditer(r"dram_bytes_per_launch_bench_workload\[(.+?)\]\s*=\s*([0-9.eE+]+)", f.read()):
+                if m.group(1).strip() == key:
+                    return float(m.group(2)), os.path.relpath(path, ROOT)
+    return None, None
 
 
 # ------------------------------------------------------------------------------------------- ours
@@ -142,7 +159,7 @@ def run_ours(args, ws, rank, local):
     torch.cuda.set_device(local)
     stream = torch.cuda.Stream()
     if args.moire_dos_only:
-        out = moire_dos_leg(G, M, local, stream, ws, peak=peaks()[0])
+        out = moire_dos_leg(G, M, local, stream, ws, nsteps=args.moire_steps, peak=peaks()[0], tuning=args.tuning)
         if rank == 0:
             print(json.dumps(out), flush=True)
         replicas.finish(ws)
@@ -182,12 +199,8 @@ def run_ours(args, ws, rank, local):
     # vectors are staged once and every job rebuilds them on the device
     from grabnes_b200.tune import autotune
     if args.tuning:
-        vals = [int(x) for x in args.tuning.split(",")]
-        rpt, bps, grp, st, pf = vals[:5]
-        unroll = vals[5] if len(vals) > 5 else 0
-        best = dict(rhs_per_thread=rpt, blocks_per_sm=bps, rows_per_group=grp, staged=st, prefetch=pf,
-                    unroll=unroll, fixed=True)
         from grabnes_b200.tune import apply
+        best = fixed_tuning(args.tuning)
         apply(ctx, best)
         tuning = []
     else:
@@ -235,9 +248,8 @@ def run_ours(args, ws, rank, local):
     b_alg = nnz * (4 + 4) + n * 4 + NRHS * n * 3 * 8
     achieved = b_alg / (spmm_ms / 1e3) / 1e9
     peak, peak_kind = peaks()
-    traffic = traffic_from_profile()
-    kname = "k_spmm_{}<float, real, G={}>".format("staged" if best.get("staged", -1) != 0 else "step",
-                                                  best.get("rows_per_group", 0))
+    kname = kernel_key(best)
+    traffic, traffic_src = traffic_from_profile(kname)
 
     # ---- end to end through the C ABI with host buffers (pinned)
     u_pin = torch.from_numpy(u.copy()).pin_memory()
@@ -274,11 +286,17 @@ def run_ours(args, ws, rank, local):
     dm, d6 = d_mix.mean(axis=0), d_64.mean(axis=0)
     dos_err = float(np.abs(dm - d6).sum() / np.abs(d6).sum())
     dos_err_per_vector = float(max(np.abs(d_mix[r] - d_64[r]).sum() / np.abs(d_64[r]).sum() for r in range(NRHS)))
+    # the DOS of vector 0 against the FP64 oracle (the reference's three-pass recursion restated in C) on
+    # the same Hamiltonian, the whole 2000 steps (rank 0, N=1; about a minute on the host cores)
+    oracle_err = None
+    if rank == 0 and ws == 1 and not args.no_cpu and not args.no_oracle_dos:
+        oracle_err = oracle_dos_error(ctx, n, u[0], nsteps, a_mix[0], b_mix[0], a64[0], b64[0], g0)
 
     # ---- CPU baseline: the oracle's OpenMP port of KuboRecursion on the host cores (rank 0, N=1)
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         cpu = cpu_baseline(ctx, n, u[0], args.cpu_steps)
+    _HOST_TABLES.clear()
 
     # ---- the field sweep of the graphene/hBN moire model: all fields in one batch against field by field
     fields = None
@@ -305,7 +323,8 @@ def run_ours(args, ws, rank, local):
         "e2e": {"value": e2e_value, "unit": "atom-steps/s", "h2d_bytes_per_step": int(u.nbytes),
                 "d2h_bytes_per_step": int(a_mix.nbytes + b_mix.nbytes)},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "peak_source": peak_kind, "traffic": traffic, "algorithmic_bytes_per_launch": b_alg,
+                     "peak_source": peak_kind, "traffic": traffic, "traffic_source": traffic_src,
+                     "algorithmic_bytes_per_launch": b_alg,
                      "kernel": kname, "avg_launch_ms": spmm_ms, "update_kernel_ms": update_ms,
                      "step_ms": kern_ms / kern_launches,
                      "step_achieved": b_alg / (kern_ms / kern_launches / 1e3) / 1e9},
@@ -315,6 +334,7 @@ def run_ours(args, ws, rank, local):
                  "batched_wall_s": fp64_batched_s, "single_wall_s": fp64_single_s},
         "dos_error_vs_fp64": {"l1_mean_dos": dos_err, "l1_worst_vector": dos_err_per_vector,
                               "eta_ev": ETA_EV, "energies": NE + 1},
+        "dos_error_vs_oracle": oracle_err,
         "cpu_baseline": cpu, "clocks": clk, "gpu_launches": launches, "setup_s": setup_s,
         "fields_batch": fields, "kubo_time_evolution": tevol, "dos_gradient": grad,
         "moire_dos": mdos,
@@ -506,7 +526,18 @@ def gradient_leg(G, M, local, stream, ws, nrecurs=600, checkpoint=32):
 MOIRE_DOS_KEYS = {k: v for k, v in TEVOL_KEYS.items() if not k.startswith("Disorder.")}
 
 
-def moire_dos_leg(G, M, local, stream, ws, nrhs=16, nsteps=2000, peak=None):
+def fixed_tuning(spec):
+    """A tuning dictionary from 'rhs_per_thread,blocks_per_sm,rows_per_group,staged,prefetch[,unroll
+    [,stage_values[,min_blocks]]]'."""
+    vals = [int(x) for x in spec.split(",")]
+    names = ["rhs_per_thread", "blocks_per_sm", "rows_per_group", "staged", "prefetch", "unroll", "stage_values",
+             "min_blocks"]
+    best = dict(unroll=0, stage_values=-1, min_blocks=0, fixed=True)
+    best.update(zip(names, vals))
+    return best
+
+
+def moire_dos_leg(G, M, local, stream, ws, nrhs=16, nsteps=2000, peak=None, tuning=""):
     """Batched mixed-precision Lanczos DOS of graphene on hBN at 0.61 degrees (example 07's cell, CellSize
     83, SuperCell 16 = 3,527,168 atoms, effective moire model with the midpoint bond term): 16 random-
     phase vectors (GNU RNG seed 123456 + k), 2000 steps, autotuned kernels, start vectors resident;
@@ -520,7 +551,12 @@ def moire_dos_leg(G, M, local, stream, ws, nrhs=16, nsteps=2000, peak=None):
     cell = M.setup(ctx, job)
     n, nnz, g0 = cell["n"], ctx.neighbours_total, job["g0"]
     u = np.stack([G.rng_uniform(123456 + k, n) for k in range(nrhs)])
-    best, _ = autotune(ctx, u, G.GBN_MIXED)
+    if tuning:
+        from grabnes_b200.tune import apply
+        best = fixed_tuning(tuning)
+        apply(ctx, best)
+    else:
+        best, _ = autotune(ctx, u, G.GBN_MIXED)
     ctx.stage_phases(u, G.GBN_MIXED)
     ctx.run_staged(200)
     torch.cuda.synchronize()
@@ -552,11 +588,45 @@ def moire_dos_leg(G, M, local, stream, ws, nrhs=16, nsteps=2000, peak=None):
             "dos_error_vs_fp64_vector0": float(np.abs(d_mix[0] - d_64[0]).sum() / np.abs(d_64[0]).sum())}
 
 
+_HOST_TABLES = {}
+
+
+def host_tables(ctx):
+    """The context's neighbour tables and Hamiltonian in the reference layout, copied to the host once."""
+    if id(ctx) not in _HOST_TABLES:
+        tabs = ctx.tables()
+        h0, hop = ctx.hamiltonian()
+        _HOST_TABLES.clear()
+        _HOST_TABLES[id(ctx)] = (tabs, h0, hop)
+    return _HOST_TABLES[id(ctx)]
+
+
+def oracle_dos_error(ctx, n, u0, nsteps, a_mix, b_mix, a64, b64, g0):
+    """Normalised L1 error of the DOS of one start vector, mixed precision and FP64 on the device, against
+    the oracle's FP64 recursion of the same vector on the same Hamiltonian (reference layout, complex128)."""
+    from oracle import oracle as orc
+    tabs, h0, hop = host_tables(ctx)
+    psi = np.exp(2j * np.pi * u0) / np.sqrt(n)
+    t0 = time.perf_counter()
+    a0, b0 = orc.recursion(tabs, hop, h0, psi, nsteps, cpu_count())
+    dt = time.perf_counter() - t0
+    args = (ETA_EV / g0, NE, EMIN_EV / g0, EMAX_EV / g0)
+    _, d0 = orc.frac(a0, b0, *args)
+    _, dm = ctx.cf_dos(a_mix[None, :], b_mix[None, :], *args)
+    _, d6 = ctx.cf_dos(a64[None, :], b64[None, :], *args)
+    l1 = lambda d: float(np.abs(d[0] - d0).sum() / np.abs(d0).sum())
+    k = min(200, nsteps)
+    return {"vector": 0, "recursion_steps": nsteps, "eta_ev": ETA_EV, "energies": NE + 1,
+            "l1_mixed": l1(dm), "l1_fp64": l1(d6),
+            "ab_rel_fp64_first200": float(max(np.abs(a64[:k] - a0[:k]).max(), np.abs(b64[:k] - b0[:k]).max())
+                                          / np.abs(b0[:k]).max()),
+            "oracle_s": dt, "oracle_cores": cpu_count()}
+
+
 def cpu_baseline(ctx, n, u0, steps):
     """The oracle port of KuboRecursion (reference data layout, complex128, three passes per step)."""
     from oracle import oracle as orc
-    tabs = ctx.tables()
-    h0, hop = ctx.hamiltonian()
+    tabs, h0, hop = host_tables(ctx)
     psi = np.exp(2j * np.pi * u0) / np.sqrt(n)
     cores = cpu_count()
     orc.recursion(tabs, hop, h0, psi, 1, cores)   # first touch
@@ -602,7 +672,12 @@ def run_reference(args, ws, rank):
     out = {"metric": METRIC, "value": value, "unit": "atom-steps/s", "n_gpus": ws, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": per * 1e3, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "c128", "data": "synthetic (reference model)", "impl": "reference",
-           "config": {"workload": WORKLOAD_NAME, "atoms": n, "sample_steps": steps, "vectors": 1},
+           "config": {"workload": WORKLOAD_NAME, "atoms": n, "sample_steps": steps, "vectors": 1,
+                      "same_config": False,
+                      "extrapolation": f"the workload is {NRHS} vectors x {NSTEPS} steps; each bench step times 1 "
+                                       f"vector x {steps} steps of the same Hamiltonian, and the rate is per "
+                                       f"atom-step, which the CPU recursion's cost is linear in (each step is "
+                                       f"three passes over the same arrays)"},
            "cpu_baseline": {"value": value, "unit": "atom-steps/s", "cores": cores, "kind": "port",
                             "sample": f"1 vector x {steps} recursion steps of the full {n}-atom Hamiltonian per bench "
                                       f"step (complex128, reference layout; setup {setup_s:.0f} s untimed)"},
@@ -618,6 +693,7 @@ def main():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--cpu-steps", type=int, default=300, help="recursion steps of the CPU sample")
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--no-oracle-dos", action="store_true", help="skip the oracle DOS check of vector 0")
     p.add_argument("--supercell", type=int, default=20, help="moire cells per side (20 = the workload)")
     p.add_argument("--nsteps", type=int, default=NSTEPS, help="recursion steps per job (2000 = the workload)")
     p.add_argument("--value-only", action="store_true", help="time the device-resident jobs only (profiling)")
@@ -631,7 +707,8 @@ def main():
     p.add_argument("--tevol-only", action="store_true", help="run the Chebyshev Kubo time evolution leg alone")
     p.add_argument("--fields-scale", type=float, default=1.0, help="scale of the sweep's recursion lengths (profiling)")
     p.add_argument("--tuning", default="", help="fixed kernel tuning 'rhs_per_thread,blocks_per_sm,rows_per_group,staged,prefetch"
-                                                "[,unroll]' instead of the autotuner")
+                                                "[,unroll[,stage_values[,min_blocks]]]' instead of the autotuner")
+    p.add_argument("--moire-steps", type=int, default=2000, help="recursion steps of the graphene/hBN DOS leg")
     args = p.parse_args()
     ws, rank, local = dist_init() if args.impl == "ours" else (int(os.environ.get("WORLD_SIZE", "1")),
                                                                  int(os.environ.get("RANK", "0")), 0)

@@ -16,6 +16,7 @@ LIB_PATH = os.path.join(HERE, "libgrabnes_gpu.so")
 
 GBN_FP64, GBN_MIXED = 0, 1
 ERRORS = {-1: "argument", -2: "cuda", -3: "state", -4: "numeric", -5: "alloc", -6: "timeout", -7: "limit"}
+GBN_ERR_ARG, GBN_ERR_CUDA, GBN_ERR_STATE, GBN_ERR_NUMERIC, GBN_ERR_ALLOC, GBN_ERR_TIMEOUT = -1, -2, -3, -4, -5, -6
 GBN_ERR_LIMIT = -7
 NOALLOC_MAX_ATOMS = 1048576   # GBN_NOALLOC_MAX_ATOMS
 

@@ -11,7 +11,7 @@
 //
 // The array is a static __device__ object: every GPU that loads this library holds its
 // kNaScratchBytes (about 48 MiB) until the process exits.  In host code its name is only a host-side
-// stand-in, so the host asks the runtime for its device address once per device
+// stand-in, so the host asks the runtime for its device address once per device and context
 // (cudaGetSymbolAddress, in na_scratch_on_current_device) and passes that address to the kernels.
 //
 // The recursion is the same three passes per step as the reference's KuboRecursion
@@ -19,6 +19,7 @@
 //   a_n = Re <psi_n|H|psi_n>,  r = H psi_n - a_n psi_n - b_{n-1} psi_{n-1},  b_n = |r|,  psi_{n+1} = r / b_n
 // with H psi = H0 psi - sum_j hopp(j) psi(NList(j)).  Sums are reduced in a fixed order (per-block
 // partials, the last block adds them), so two calls on the same inputs give the same bits.
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
@@ -163,18 +164,54 @@ __global__ void k_na_shift(int64_t n, NaScratch s, const double* b, int it)
 constexpr int kNaMaxDevices = 64;
 std::mutex g_na_mutex;
 unsigned char* g_na_ptr[kNaMaxDevices];
+unsigned long long g_na_ctx_id[kNaMaxDevices];   // unique id of the context the address belongs to
 
-// Device address of g_na_scratch on the current device, looked up on the first call for that device.
+// Driver entry points reached through the runtime (no link to the driver library): the current context
+// and its unique id, which CUDA never reuses, so that an address looked up before a device reset (which
+// destroys the context and unloads this module from it) is not used afterwards.
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
+
+bool current_context_id(unsigned long long* id)
+{
+    static CtxGetCurrentFn get_current = nullptr;
+    static CtxGetIdFn get_id = nullptr;
+    static bool looked = false;
+    if (!looked) {
+        looked = true;
+        cudaDriverEntryPointQueryResult q1, q2;
+        void* f1 = nullptr;
+        void* f2 = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f1, cudaEnableDefault, &q1) == cudaSuccess &&
+            q1 == cudaDriverEntryPointSuccess &&
+            cudaGetDriverEntryPoint("cuCtxGetId", &f2, cudaEnableDefault, &q2) == cudaSuccess &&
+            q2 == cudaDriverEntryPointSuccess) {
+            get_current = reinterpret_cast<CtxGetCurrentFn>(f1);
+            get_id = reinterpret_cast<CtxGetIdFn>(f2);
+        }
+    }
+    CUcontext ctx = nullptr;
+    return get_current && get_id && get_current(&ctx) == CUDA_SUCCESS && ctx && get_id(ctx, id) == CUDA_SUCCESS;
+}
+
+// Device address of g_na_scratch on the current device.  It is looked up (cudaGetSymbolAddress, which
+// may load this library's module into the context) on the first call for a device, and again when that
+// device's context is a new one (after a reset); otherwise the cached address is used.  A caller that
+// cannot tell the context's identity (driver entry points unavailable) gets a lookup on every call.
 int na_scratch_on_current_device(unsigned char** out)
 {
     int dev = -1;
     if (cudaGetDevice(&dev) != cudaSuccess) return GBN_ERR_CUDA;
     if (dev < 0 || dev >= kNaMaxDevices) return GBN_ERR_ARG;
+    if (cudaSetDevice(dev) != cudaSuccess) return GBN_ERR_CUDA;   // makes the device's context current
+    unsigned long long id = 0;
+    const bool have_id = current_context_id(&id);
     std::lock_guard<std::mutex> lock(g_na_mutex);
-    if (!g_na_ptr[dev]) {
+    if (!g_na_ptr[dev] || !have_id || g_na_ctx_id[dev] != id) {
         void* p = nullptr;
         if (cudaGetSymbolAddress(&p, g_na_scratch) != cudaSuccess || !p) return GBN_ERR_CUDA;
         g_na_ptr[dev] = static_cast<unsigned char*>(p);
+        g_na_ctx_id[dev] = have_id ? id : 0ull;
     }
     *out = g_na_ptr[dev];
     return GBN_OK;

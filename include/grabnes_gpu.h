@@ -335,8 +335,9 @@ int gbn_dos_gradient(gbn_ctx* ctx, const gbn_model* model, double g0, const doub
  * of the current device, in the layouts of gbn_load_hamiltonian: nneigh(N), nlist(maxNeigh,N)
  * (1-based), hopp(maxNeigh,N) complex, h0(N), psi(N) complex (normalised by the caller; hopp and psi
  * 16-byte aligned); a, b: nrecurs doubles each, written by the call.
- * The first call on a device looks up the array's device address (cudaGetSymbolAddress); make that
- * first call before any stream capture on that device.  All calls on a device share the array, so
+ * The first call on a device, and the first after that device's context was reset, looks up the
+ * array's device address (cudaGetSymbolAddress); make that call before any stream capture on that
+ * device.  All calls on a device share the array, so
  * calls that overlap on the GPU (other host threads, other streams) race: serialise them.
  * Returns GBN_ERR_LIMIT when n > GBN_NOALLOC_MAX_ATOMS, GBN_ERR_ARG for other bad arguments
  * (including Nneigh/NList entries out of range, found on the device), GBN_ERR_NUMERIC for a b_n that

@@ -60,6 +60,21 @@ def test_noalloc_recursion_matches_context_recursion():
         a_np, b_np = a.cpu().numpy(), b.cpu().numpy()
         assert _rel(a_np, a_ref[0]) <= 1e-10 and _rel(b_np, b_ref[0]) <= 1e-10
 
+    # one NList entry out of range: the kernel skips that access and reports it (GBN_ERR_ARG); the flag
+    # lives in the shared array, so the next good call must find it cleared and repeat the good result
+    bad = np.ascontiguousarray(nb["nlist"], np.int32).reshape(-1).copy()
+    bad[5] = n + 7
+    nlist_bad = torch.from_numpy(bad).to(dev)
+    rc = L.gbn_lanczos_noalloc(n, mn, nneigh.data_ptr(), nlist_bad.data_ptr(), hopp.data_ptr(), h0.data_ptr(),
+                               d_psi.data_ptr(), NSTEPS, a.data_ptr(), b.data_ptr(), stream.cuda_stream)
+    assert rc == G.GBN_ERR_ARG
+    a2 = torch.full((NSTEPS,), float("nan"), dtype=torch.float64, device=dev)
+    b2 = torch.full((NSTEPS,), float("nan"), dtype=torch.float64, device=dev)
+    rc = L.gbn_lanczos_noalloc(n, mn, nneigh.data_ptr(), nlist.data_ptr(), hopp.data_ptr(), h0.data_ptr(),
+                               d_psi.data_ptr(), NSTEPS, a2.data_ptr(), b2.data_ptr(), stream.cuda_stream)
+    assert rc == 0, G.ERRORS.get(rc, rc)
+    assert np.array_equal(a2.cpu().numpy(), a_np) and np.array_equal(b2.cpu().numpy(), b_np)
+
     # beyond the stated maximum: rejected on the host before anything is launched
     rc = L.gbn_lanczos_noalloc(G.NOALLOC_MAX_ATOMS + 1, mn, nneigh.data_ptr(), nlist.data_ptr(), hopp.data_ptr(),
                                h0.data_ptr(), d_psi.data_ptr(), NSTEPS, a.data_ptr(), b.data_ptr(), stream.cuda_stream)
