@@ -134,15 +134,18 @@ def kernel_key(best):
     return f"k_spmm_staged<float, real, G={g}, U={unroll}, SV={sv}, MINB={mb}, prefetch={pf}>"
 
 
-def traffic_from_profile(key):
-    """DRAM bytes per sparse-product launch at the bench workload for the kernel `key`, from the committed
-    ncu summaries (captures of the same kernel on the 10 x 10 tiling, scaled by the rows processed); None
-    when no summary covers that kernel."""
+def traffic_from_profile(key, workload="bench_workload"):
+    """DRAM bytes per sparse-product launch of the kernel `key` on a workload ("bench_workload": the TBG
+    job, from captures of the same kernel on the 10 x 10 tiling scaled by the rows processed;
+    "moire_dos": the 3.5M-atom graphene/hBN job, captured at full size), from the lines
+    `dram_bytes_per_launch_<workload>[<key>] = <bytes>` of the committed ncu summaries; None when no
+    summary covers that kernel."""
     import glob
     import re
+    pat = re.compile(r"dram_bytes_per_launch_" + workload + r"\[(.+?)\]\s*=\s*([0-9.eE+]+)")
     for path in sorted(glob.glob(os.path.join(PROFILES, "*.md"))):
         with open(path) as f:
-            for m in re.finditer(r"dram_bytes_per_launch_bench_workload\[(.+?)\]\s*=\s*([0-9.eE+]+)", f.read()):
+            for m in pat.finditer(f.read()):
                 if m.group(1).strip() == key:
                     return float(m.group(2)), os.path.relpath(path, ROOT)
     return None, None
@@ -327,7 +330,8 @@ def run_ours(args, ws, rank, local):
                      "algorithmic_bytes_per_launch": b_alg,
                      "kernel": kname, "avg_launch_ms": spmm_ms, "update_kernel_ms": update_ms,
                      "step_ms": kern_ms / kern_launches,
-                     "step_achieved": b_alg / (kern_ms / kern_launches / 1e3) / 1e9},
+                     "step_achieved": b_alg / (kern_ms / kern_launches / 1e3) / 1e9,
+                     "step_frac": b_alg / (kern_ms / kern_launches / 1e3) / 1e9 / peak},
         "tuning": best,
         "fp64": {"batched_atom_steps_per_s": atom_steps / (fp64_batched_kernel_ms / 1e3),
                  "single_vector_atom_steps_per_s": float(n) * nsteps / (fp64_single_kernel_ms / 1e3),
@@ -577,13 +581,17 @@ def moire_dos_leg(G, M, local, stream, ws, nrhs=16, nsteps=2000, peak=None, tuni
     b_alg = nnz * (4 + 4) + n * 4 + nrhs * n * 3 * 8
     ach = b_alg / (spmm_ms / 1e3) / 1e9
     step = min(ms, ms2) / nsteps
+    kname = kernel_key(best)
+    traffic, traffic_src = traffic_from_profile(kname, "moire_dos")
     return {"workload": "graphene_hbn_0.61deg_3527168atoms_16vec_2000steps", "atoms": n, "entries": nnz,
             "vectors": nrhs, "recursion_steps": nsteps, "tuning": best,
             "batched_mixed_atom_steps_per_s": ws * n * nrhs / (step / 1e3),
             "fp64_single_vector_atom_steps_per_s": ws * n / (ms64 / nsteps / 1e3),
             "step_ms": step, "spmm_ms": spmm_ms, "update_ms": upd_ms,
             "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
-                         "frac": (ach / peak) if peak else None, "algorithmic_bytes_per_launch": b_alg},
+                         "frac": (ach / peak) if peak else None, "algorithmic_bytes_per_launch": b_alg,
+                         "kernel": kname, "traffic": traffic, "traffic_source": traffic_src},
+            "step_frac": (b_alg / (step / 1e3) / 1e9 / peak) if peak else None,
             "step_achieved_gbs": b_alg / (step / 1e3) / 1e9,
             "dos_error_vs_fp64_vector0": float(np.abs(d_mix[0] - d_64[0]).sum() / np.abs(d_64[0]).sum())}
 
