@@ -100,7 +100,7 @@ EXPORTS = ["gbn_cell_atoms", "gbn_build_cell", "gbn_cart_roundtrip", "gbn_rng_un
            "gbn_last_timing", "gbn_last_kernel_timing", "gbn_set_geometry", "gbn_neighbours", "gbn_get_neighbours", "gbn_assemble",
            "gbn_peierls", "gbn_get_hamiltonian", "gbn_load_hamiltonian", "gbn_lanczos", "gbn_lanczos_phases",
            "gbn_stage_phases", "gbn_run_staged", "gbn_cf_dos", "gbn_cheb_evolve", "gbn_kubo_evol", "gbn_set_neighd", "gbn_lanczos_noalloc",
-           "gbn_cheb_interval", "gbn_cheb_coef", "gbn_dos_gradient", "gbn_lanczos_sites", "gbn_lanczos_sets",
+           "gbn_cheb_interval", "gbn_cheb_coef", "gbn_dos_gradient", "gbn_dos_gradient_prec", "gbn_lanczos_sites", "gbn_lanczos_sets",
            "gbn_pdos_atoms", "gbn_pdos_sets", "gbn_lanczos_fields", "gbn_set_images", "gbn_haldane", "gbn_kubo_tevol", "gbn_check_hamiltonian"]
 
 
@@ -158,6 +158,9 @@ def _declare(L):
     L.gbn_cheb_interval.argtypes = [_p(np.float64), _p(np.float64), i32, C.POINTER(d), C.POINTER(d)]
     L.gbn_dos_gradient.argtypes = [vp, C.POINTER(Model), d, _p(np.float64), i32, i32, d, i32, d, d, _p(np.float64),
                                    C.POINTER(d), _p(np.float64), _opt(np.float64), _opt(np.float64), _opt(np.float64)]
+    L.gbn_dos_gradient_prec.argtypes = [vp, i32, C.POINTER(Model), d, _p(np.float64), i32, i32, d, i32, d, d,
+                                        _p(np.float64), C.POINTER(d), _p(np.float64), _opt(np.float64),
+                                        _opt(np.float64), _opt(np.float64)]
     L.gbn_cheb_coef.argtypes = [d, d, d, i32, _p(np.complex128)]
     # device pointers (ints from tensor.data_ptr()), no context
     L.gbn_lanczos_noalloc.argtypes = [i64, i32, vp, vp, vp, vp, vp, i32, vp, vp, vp]
@@ -392,15 +395,18 @@ class Context:
         return e, dos
 
     # ---------------------------------------------------------------- gradient
-    def dos_gradient(self, model, g0, u, nrecurs, eta, n_en, emin, emax, target, checkpoint=32):
-        """Loss, dL/d(t, Vpp_sigma0, delta, w) and the DOS of the assembled Hamiltonian (see gbn_dos_gradient)."""
+    def dos_gradient(self, model, g0, u, nrecurs, eta, n_en, emin, emax, target, checkpoint=32,
+                     precision=GBN_FP64):
+        """Loss, dL/d(t, Vpp_sigma0, delta, w) and the DOS of the assembled Hamiltonian (see gbn_dos_gradient;
+        precision GBN_MIXED: the FP32-vector variant, gbn_dos_gradient_prec)."""
         loss = C.c_double()
         grad = np.zeros(4)
         dos = np.zeros(n_en + 1)
         a = np.zeros(nrecurs)
         b = np.zeros(nrecurs)
-        self._ck(self._L.gbn_dos_gradient(self._h, C.byref(model), g0, _c(u, np.float64), nrecurs, checkpoint, eta,
-                                          n_en, emin, emax, _c(target, np.float64), C.byref(loss), grad, dos, a, b))
+        self._ck(self._L.gbn_dos_gradient_prec(self._h, precision, C.byref(model), g0, _c(u, np.float64), nrecurs,
+                                               checkpoint, eta, n_en, emin, emax, _c(target, np.float64),
+                                               C.byref(loss), grad, dos, a, b))
         return loss.value, grad, dos, a, b
 
     # ---------------------------------------------------------------- Chebyshev

@@ -15,7 +15,7 @@ import math
 
 import numpy as np
 
-from . import Model, build_cell, cart_roundtrip, rng_uniform
+from . import GBN_FP64, Model, build_cell, cart_roundtrip, rng_uniform
 
 PARAMS = ("t", "vppsigma0", "delta", "w")
 
@@ -34,7 +34,8 @@ def model_with(base, g0, theta):
 class DosProblem:
     """The fixed part of a DOS-fitting problem: geometry, neighbour tables, start vector and target."""
 
-    def __init__(self, ctx, job, target, nrecurs, eta_ev, n_en, emin_ev, emax_ev, checkpoint=32, cut_rho=None):
+    def __init__(self, ctx, job, target, nrecurs, eta_ev, n_en, emin_ev, emax_ev, checkpoint=32, cut_rho=None,
+                 precision=None):
         self.ctx, self.job = ctx, job
         self.g0 = job["g0"]
         cell = build_cell(**job["cell"])
@@ -51,6 +52,8 @@ class DosProblem:
         self.target = np.ascontiguousarray(target, np.float64) if target is not None else np.zeros(n_en + 1)
         self.nrecurs, self.n_en, self.checkpoint = nrecurs, n_en, checkpoint
         self.eta, self.emin, self.emax = eta_ev / self.g0, emin_ev / self.g0, emax_ev / self.g0
+        # GBN_FP64 (default) or GBN_MIXED: the FP32-vector variant of the recursion and its adjoint
+        self.precision = GBN_FP64 if precision is None else precision
 
     def evaluate(self, theta):
         """(loss, gradient [4], DOS [n_en + 1]) at theta."""
@@ -58,7 +61,8 @@ class DosProblem:
         uni = self.u if m.anderson else None
         self.ctx.assemble(m, self.rat_on, self.rat_hop, uni)
         loss, grad, dos, _, _ = self.ctx.dos_gradient(m, self.g0, self.u, self.nrecurs, self.eta, self.n_en,
-                                                      self.emin, self.emax, self.target, self.checkpoint)
+                                                      self.emin, self.emax, self.target, self.checkpoint,
+                                                      self.precision)
         return loss, grad, dos
 
 

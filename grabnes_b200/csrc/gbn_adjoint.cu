@@ -16,6 +16,8 @@
 //     qbar_{k-1} += -b_{k-1} rbar;   Hbar_ij += Re conj(ubar_i) q_{k,j}
 // and dL/dtheta = sum over entries of Hbar_ij dH_ij/dtheta, dH = -d(hopp), from the entries' geometry.
 // Vectors are in the reference atom order; the sums are block partials reduced in a fixed order.
+// Two variants: FP64 vectors and hoppings, or complex64 vectors and FP32 hoppings with the same FP64
+// arithmetic, sums, scalars, continued fraction and Hbar accumulation (each stored vector rounded once).
 #include <cuda_runtime.h>
 #include <math.h>
 
@@ -31,21 +33,31 @@ namespace {
 
 constexpr int kAdThreads = 256;
 
+// Vector storage: complex128 (FP64 variant) or complex64 (FP32 variant).  Every kernel loads into FP64,
+// computes in FP64 and rounds once when it stores; sums, scalars and Hbar stay FP64 in both variants.
+__device__ __forceinline__ double2 ldv(const double2& v) { return v; }
+__device__ __forceinline__ double2 ldv(const float2& v) { return make_double2(v.x, v.y); }
+template <typename V> __device__ __forceinline__ V stv(double x, double y);
+template <> __device__ __forceinline__ double2 stv<double2>(double x, double y) { return make_double2(x, y); }
+template <> __device__ __forceinline__ float2 stv<float2>(double x, double y) { return make_float2((float)x, (float)y); }
+
 // The adjoint's copy of the Hamiltonian: the reference tables (row i, slot j at i * mn + j, complex
-// hoppings) transposed to slot-major order, entry (i, j) at j * n + i with the real hopping and the
-// 0-based column, so that the threads of a warp (consecutive rows) read consecutive words.
+// hoppings) transposed to slot-major order, entry (i, j) at j * n + i with the real hopping (HT: double or
+// float) and the 0-based column, so that the threads of a warp (consecutive rows) read consecutive words.
+template <typename HT>
 struct AdTables {
     int64_t n;
     int32_t mn;
     const int32_t* nneigh;
     const int32_t* col;
-    const double* hop;
+    const HT* hop;
     const double* h0;
 };
 
+template <typename HT>
 __global__ void k_ad_tables(int64_t n, int32_t mn, const int32_t* __restrict__ nneigh,
                             const int32_t* __restrict__ nlist, const double2* __restrict__ hopp,
-                            int32_t* __restrict__ col, double* __restrict__ hop)
+                            int32_t* __restrict__ col, HT* __restrict__ hop)
 {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -53,26 +65,27 @@ __global__ void k_ad_tables(int64_t n, int32_t mn, const int32_t* __restrict__ n
     for (int j = 0; j < mn; ++j) {
         const int64_t src = i * mn + j, dst = (int64_t)j * n + i;
         col[dst] = j < nn ? nlist[src] - 1 : (int32_t)i;
-        hop[dst] = j < nn ? hopp[src].x : 0.0;
+        hop[dst] = (HT)(j < nn ? hopp[src].x : 0.0);
     }
 }
 
 // y = H x, one row per thread
-__global__ void k_ad_apply(AdTables t, const double2* __restrict__ x, double2* __restrict__ y)
+template <typename V, typename HT>
+__global__ void k_ad_apply(AdTables<HT> t, const V* __restrict__ x, V* __restrict__ y)
 {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= t.n) return;
-    const double2 xi = x[i];
+    const double2 xi = ldv(x[i]);
     double cr = t.h0[i] * xi.x, ci = t.h0[i] * xi.y;
     const int nn = t.nneigh[i];
     for (int j = 0; j < nn; ++j) {
         const int64_t e = (int64_t)j * t.n + i;
-        const double h = t.hop[e];
-        const double2 xj = x[t.col[e]];
+        const double h = (double)t.hop[e];
+        const double2 xj = ldv(x[t.col[e]]);
         cr -= h * xj.x;
         ci -= h * xj.y;
     }
-    y[i] = make_double2(cr, ci);
+    y[i] = stv<V>(cr, ci);
 }
 
 // fixed-order reduction: partial sums of up to 3 quantities per block
@@ -136,98 +149,120 @@ __global__ void __launch_bounds__(kFinThreads) k_ad_finish(const double* partial
 }
 
 // forward: a_k = Re q^+ u (partials)
-__global__ void k_ad_dot_au(int64_t n, const double2* q, const double2* u, double* partials)
+template <typename V>
+__global__ void k_ad_dot_au(int64_t n, const V* q, const V* u, double* partials)
 {
     double v[1] = {0.0};
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        v[0] += q[i].x * u[i].x + q[i].y * u[i].y;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double2 qi = ldv(q[i]), ui = ldv(u[i]);
+        v[0] += qi.x * ui.x + qi.y * ui.y;
+    }
     block_partials<1>(v, partials);
 }
 
-// forward: r = u - a_k q - b_{k-1} qm (into u) and |r|^2 partials
-__global__ void k_ad_residual(int64_t n, double2* u, const double2* q, const double2* qm, const double* a,
-                              const double* b, int k, double* partials)
+// forward: r = u - a_k q - b_{k-1} qm (into u) and |r|^2 partials (of the stored r)
+template <typename V>
+__global__ void k_ad_residual(int64_t n, V* u, const V* q, const V* qm, const double* a, const double* b, int k,
+                              double* partials)
 {
     const double ak = a[k], bp = k > 0 ? b[k - 1] : 0.0;
     double v[1] = {0.0};
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        const double2 r = make_double2((u[i].x - ak * q[i].x) - bp * qm[i].x, (u[i].y - ak * q[i].y) - bp * qm[i].y);
+        const double2 ui = ldv(u[i]), qi = ldv(q[i]), qmi = ldv(qm[i]);
+        const V r = stv<V>((ui.x - ak * qi.x) - bp * qmi.x, (ui.y - ak * qi.y) - bp * qmi.y);
         u[i] = r;
-        v[0] += r.x * r.x + r.y * r.y;
+        const double2 rd = ldv(r);
+        v[0] += rd.x * rd.x + rd.y * rd.y;
     }
     block_partials<1>(v, partials);
 }
 
 // forward: q_{k+1} = r / b_k
-__global__ void k_ad_scale(int64_t n, const double2* r, double2* qn, const double* b, int k)
+template <typename V>
+__global__ void k_ad_scale(int64_t n, const V* r, V* qn, const double* b, int k)
 {
     const double bk = b[k];
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        qn[i] = make_double2(r[i].x / bk, r[i].y / bk);
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double2 ri = ldv(r[i]);
+        qn[i] = stv<V>(ri.x / bk, ri.y / bk);
+    }
 }
 
 // reverse: Re qbar_{k+1}^+ q_{k+1}
-__global__ void k_ad_dot(int64_t n, const double2* x, const double2* y, double* partials)
+template <typename V>
+__global__ void k_ad_dot(int64_t n, const V* x, const V* y, double* partials)
 {
     double v[1] = {0.0};
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        v[0] += x[i].x * y[i].x + x[i].y * y[i].y;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double2 xi = ldv(x[i]), yi = ldv(y[i]);
+        v[0] += xi.x * yi.x + xi.y * yi.y;
+    }
     block_partials<1>(v, partials);
 }
 
 // reverse: rbar = qa / b_k + beta q_{k+1}, beta = bbar_k - s1 / b_k; dots with q_k and q_{k-1}
-__global__ void k_ad_rbar(int64_t n, const double2* qa, const double2* qk1, const double2* qk, const double2* qkm,
-                          double2* rbar, const double* b, const double* bbar, const double* scal, int k,
-                          double* partials)
+template <typename V>
+__global__ void k_ad_rbar(int64_t n, const V* qa, const V* qk1, const V* qk, const V* qkm, V* rbar,
+                          const double* b, const double* bbar, const double* scal, int k, double* partials)
 {
     const double bk = b[k];
     const double beta = bbar[k] - scal[0] / bk;
     double v[2] = {0.0, 0.0};
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        const double2 r = make_double2(qa[i].x / bk + beta * qk1[i].x, qa[i].y / bk + beta * qk1[i].y);
-        rbar[i] = r;
-        v[0] += qk[i].x * r.x + qk[i].y * r.y;
-        if (qkm) v[1] += qkm[i].x * r.x + qkm[i].y * r.y;
+        const double2 qai = ldv(qa[i]), q1 = ldv(qk1[i]), q0 = ldv(qk[i]);
+        const V rs = stv<V>(qai.x / bk + beta * q1.x, qai.y / bk + beta * q1.y);
+        rbar[i] = rs;
+        const double2 r = ldv(rs);
+        v[0] += q0.x * r.x + q0.y * r.y;
+        if (qkm) {
+            const double2 qmi = ldv(qkm[i]);
+            v[1] += qmi.x * r.x + qmi.y * r.y;
+        }
     }
     block_partials<2>(v, partials);
 }
 
 // reverse: ubar = rbar + abar_k q_k
-__global__ void k_ad_ubar(int64_t n, const double2* rbar, const double2* qk, double2* ubar, const double* scal)
+template <typename V>
+__global__ void k_ad_ubar(int64_t n, const V* rbar, const V* qk, V* ubar, const double* scal)
 {
     const double ab = scal[1];
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        ubar[i] = make_double2(rbar[i].x + ab * qk[i].x, rbar[i].y + ab * qk[i].y);
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double2 r = ldv(rbar[i]), q = ldv(qk[i]);
+        ubar[i] = stv<V>(r.x + ab * q.x, r.y + ab * q.y);
+    }
 }
 
 // reverse: qbar_k = qb - a_k rbar + abar_k u_k + H ubar (into out); qbar_{k-1} partial = -b_{k-1} rbar
-// (into qnext); Hbar_ij += Re conj(ubar_i) q_{k,j}
-__global__ void k_ad_back(AdTables t, const double2* __restrict__ ubar, const double2* __restrict__ rbar,
-                          const double2* __restrict__ qb, const double2* __restrict__ qk1, const double2* __restrict__ qk,
-                          const double2* __restrict__ qkm, double2* __restrict__ out, double2* __restrict__ qnext,
+// (into qnext); Hbar_ij += Re conj(ubar_i) q_{k,j} (FP64)
+template <typename V, typename HT>
+__global__ void k_ad_back(AdTables<HT> t, const V* __restrict__ ubar, const V* __restrict__ rbar,
+                          const V* __restrict__ qb, const V* __restrict__ qk1, const V* __restrict__ qk,
+                          const V* __restrict__ qkm, V* __restrict__ out, V* __restrict__ qnext,
                           const double* a, const double* b, const double* scal, int k, double* __restrict__ hbar)
 {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= t.n) return;
     const double ak = a[k], bk = b[k], bp = k > 0 ? b[k - 1] : 0.0, ab = scal[1];
-    const double2 ui = ubar[i];
+    const double2 ui = ldv(ubar[i]);
     double hr = t.h0[i] * ui.x, hi = t.h0[i] * ui.y;
     const int nn = t.nneigh[i];
     for (int j = 0; j < nn; ++j) {
         const int64_t e = (int64_t)j * t.n + i;
         const int32_t jj = t.col[e];
-        const double h = t.hop[e];
-        const double2 uj = ubar[jj];
+        const double h = (double)t.hop[e];
+        const double2 uj = ldv(ubar[jj]);
         hr -= h * uj.x;
         hi -= h * uj.y;
-        const double2 qj = qk[jj];
+        const double2 qj = ldv(qk[jj]);
         hbar[e] += ui.x * qj.x + ui.y * qj.y;
     }
-    const double2 r = rbar[i], q1 = qk1[i], q0 = qk[i];
-    const double2 qm = qkm ? qkm[i] : make_double2(0.0, 0.0);
+    const double2 r = ldv(rbar[i]), q1 = ldv(qk1[i]), q0 = ldv(qk[i]);
+    const double2 qm = qkm ? ldv(qkm[i]) : make_double2(0.0, 0.0);
+    const double2 qbi = ldv(qb[i]);
     const double2 uk = make_double2(bk * q1.x + ak * q0.x + bp * qm.x, bk * q1.y + ak * q0.y + bp * qm.y);
-    out[i] = make_double2(qb[i].x - ak * r.x + ab * uk.x + hr, qb[i].y - ak * r.y + ab * uk.y + hi);
-    qnext[i] = make_double2(-bp * r.x, -bp * r.y);
+    out[i] = stv<V>(qbi.x - ak * r.x + ab * uk.x + hr, qbi.y - ak * r.y + ab * uk.y + hi);
+    qnext[i] = stv<V>(-bp * r.x, -bp * r.y);
 }
 
 __device__ __forceinline__ double smooth_cut_w(double rho, double rc, double w, double* ds_dw)
@@ -243,7 +278,8 @@ __device__ __forceinline__ double smooth_cut_w(double rho, double rc, double w, 
 }
 
 // dL/dtheta = sum_e Hbar_e * (-d hopp_e / d theta), per-block partials of the four derivatives
-__global__ void k_ad_params(AdTables t, gbn_model m, double g0, const double* neighd, const int32_t* layer,
+template <typename HT>
+__global__ void k_ad_params(AdTables<HT> t, gbn_model m, double g0, const double* neighd, const int32_t* layer,
                             const double* hbar, double* partials)
 {
     double v[4] = {0.0, 0.0, 0.0, 0.0};
@@ -292,15 +328,16 @@ __global__ void k_ad_params(AdTables t, gbn_model m, double g0, const double* ne
     }
 }
 
-__global__ void k_ad_start(int64_t n, const double* u, double2* q0, double2* qm)
+template <typename V>
+__global__ void k_ad_start(int64_t n, const double* u, V* q0, V* qm)
 {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double s, c;
     sincos(6.283185307179586 * u[i], &s, &c);
     const double isn = 1.0 / sqrt((double)n);
-    q0[i] = make_double2(c * isn, s * isn);
-    qm[i] = make_double2(0.0, 0.0);
+    q0[i] = stv<V>(c * isn, s * isn);
+    qm[i] = stv<V>(0.0, 0.0);
 }
 
 // DOS of the continued fraction (KuboFrac), the loss and its adjoints abar, bbar (host, FP64)
@@ -350,7 +387,8 @@ double cf_loss_adjoint(const std::vector<double>& a, const std::vector<double>& 
 
 }  // namespace
 
-int dos_gradient(gbn_ctx* c, const gbn_model* m, double g0, const double* u_host, int32_t K, int32_t C, double eta,
+template <typename V, typename HT>
+static int dos_gradient_t(gbn_ctx* c, const gbn_model* m, double g0, const double* u_host, int32_t K, int32_t C, double eta,
                  int32_t n_en, double emin, double emax, const double* target, double* loss_out, double* grad,
                  double* dos, double* a_out, double* b_out)
 {
@@ -362,7 +400,7 @@ int dos_gradient(gbn_ctx* c, const gbn_model* m, double g0, const double* u_host
     if (C < 1 || C > K) C = K;
     const int64_t n = c->n;
     const int nseg = (K + C - 1) / C;
-    const size_t vb = sizeof(double2) * (size_t)n;
+    const size_t vb = sizeof(V) * (size_t)n;
     // device memory: checkpoints (q_{c-1}, q_c) per segment, a segment of C + 2 vectors, 5 work vectors,
     // Hbar per entry, scalars and partial sums
     DevBuf ck, seg, work, hbar, scal, parts, ab, bb, abr, bbr, ud;
@@ -380,10 +418,10 @@ int dos_gradient(gbn_ctx* c, const gbn_model* m, double g0, const double* u_host
     GBN_CK(c, ud.ensure(sizeof(double) * (size_t)n));
     DevBuf tcol, thop;
     GBN_CK(c, tcol.ensure(sizeof(int32_t) * (size_t)n * c->max_neigh));
-    GBN_CK(c, thop.ensure(sizeof(double) * (size_t)n * c->max_neigh));
-    AdTables t{n, c->max_neigh, c->nneigh.as<int32_t>(), tcol.as<int32_t>(), thop.as<double>(), c->h0.as<double>()};
-    double2* CK = ck.as<double2>();
-    double2* W = work.as<double2>();
+    GBN_CK(c, thop.ensure(sizeof(HT) * (size_t)n * c->max_neigh));
+    AdTables<HT> t{n, c->max_neigh, c->nneigh.as<int32_t>(), tcol.as<int32_t>(), thop.as<HT>(), c->h0.as<double>()};
+    V* CK = ck.as<V>();
+    V* W = work.as<V>();
     double* A = ab.as<double>();
     double* B = bb.as<double>();
     double* P = parts.as<double>();
@@ -392,13 +430,13 @@ int dos_gradient(gbn_ctx* c, const gbn_model* m, double g0, const double* u_host
     GBN_CK(c, cudaMemcpyAsync(ud.p, u_host, sizeof(double) * n, cudaMemcpyHostToDevice, st));
 
     // forward pass with checkpoints: q_k in W[0], q_{k-1} in W[1], u/r in W[2], q_{k+1} in W[3]
-    double2 *qk = W, *qm = W + n, *ur = W + 2 * n, *qn = W + 3 * n;
+    V *qk = W, *qm = W + n, *ur = W + 2 * n, *qn = W + 3 * n;
     k_ad_tables<<<rows_grid, kAdThreads, 0, st>>>(n, c->max_neigh, c->nneigh.as<int32_t>(), c->nlist.as<int32_t>(),
-                                                  c->hopp.as<double2>(), tcol.as<int32_t>(), thop.as<double>());
+                                                  c->hopp.as<double2>(), tcol.as<int32_t>(), thop.as<HT>());
     k_ad_start<<<rows_grid, kAdThreads, 0, st>>>(n, ud.as<double>(), qk, qm);
     GBN_CK_LAUNCH(c);
     c->launches += 2;
-    auto fwd_step = [&](double2* q, double2* qmm, double2* u, double2* qnext, int k) -> int {
+    auto fwd_step = [&](V* q, V* qmm, V* u, V* qnext, int k) -> int {
         k_ad_apply<<<rows_grid, kAdThreads, 0, st>>>(t, q, u);
         k_ad_dot_au<<<blocks, kAdThreads, 0, st>>>(n, q, u, P);
         k_ad_finish<<<1, kFinThreads, 0, st>>>(P, blocks, 1, kSetA, k, A, B, nullptr, nullptr, nullptr);
@@ -417,7 +455,7 @@ int dos_gradient(gbn_ctx* c, const gbn_model* m, double g0, const double* u_host
         }
         int rc = fwd_step(qk, qm, ur, qn, k);
         if (rc) return rc;
-        double2* tmp = qm;
+        V* tmp = qm;
         qm = qk;
         qk = qn;
         qn = tmp;
@@ -440,8 +478,8 @@ int dos_gradient(gbn_ctx* c, const gbn_model* m, double g0, const double* u_host
     GBN_CK(c, cudaMemcpyAsync(bbr.p, bbar.data(), sizeof(double) * K, cudaMemcpyHostToDevice, st));
 
     // reverse sweep by segments: seg[j] = q_{c-1+j}, j = 0 .. len+1 (q_{c-1} .. q_{c+len})
-    double2* S = seg.as<double2>();
-    double2 *qa = W, *qb = W + n, *rb = W + 2 * n, *ub = W + 3 * n, *tmpv = W + 4 * n;
+    V* S = seg.as<V>();
+    V *qa = W, *qb = W + n, *rb = W + 2 * n, *ub = W + 3 * n, *tmpv = W + 4 * n;
     GBN_CK(c, cudaMemsetAsync(qa, 0, vb, st));   // qbar_K = 0
     GBN_CK(c, cudaMemsetAsync(qb, 0, vb, st));   // qbar_{K-1} (partial) = 0
     GBN_CK(c, cudaMemsetAsync(hbar.p, 0, sizeof(double) * (size_t)n * c->max_neigh, st));
@@ -455,7 +493,7 @@ int dos_gradient(gbn_ctx* c, const gbn_model* m, double g0, const double* u_host
         GBN_CK(c, cudaMemcpyAsync(S + n, CK + (size_t)(2 * sI + 1) * n, vb, cudaMemcpyDeviceToDevice, st));
         for (int j = 0; j < len; ++j) {   // recompute q_{c0+1} .. q_{c0+len} with the stored a, b
             const int k = c0 + j;
-            double2 *q = S + (size_t)(j + 1) * n, *qmm = S + (size_t)j * n, *qnext = S + (size_t)(j + 2) * n;
+            V *q = S + (size_t)(j + 1) * n, *qmm = S + (size_t)j * n, *qnext = S + (size_t)(j + 2) * n;
             k_ad_apply<<<rows_grid, kAdThreads, 0, st>>>(t, q, tmpv);
             k_ad_residual<<<blocks, kAdThreads, 0, st>>>(n, tmpv, q, qmm, A, B, k, P);
             k_ad_scale<<<blocks, kAdThreads, 0, st>>>(n, tmpv, qnext, B, k);
@@ -464,9 +502,9 @@ int dos_gradient(gbn_ctx* c, const gbn_model* m, double g0, const double* u_host
         }
         for (int j = len - 1; j >= 0; --j) {
             const int k = c0 + j;
-            const double2* qk1 = S + (size_t)(j + 2) * n;
-            const double2* q0 = S + (size_t)(j + 1) * n;
-            const double2* qkm = (k > 0) ? S + (size_t)j * n : nullptr;
+            const V* qk1 = S + (size_t)(j + 2) * n;
+            const V* q0 = S + (size_t)(j + 1) * n;
+            const V* qkm = (k > 0) ? S + (size_t)j * n : nullptr;
             k_ad_dot<<<blocks, kAdThreads, 0, st>>>(n, qa, qk1, P);
             k_ad_finish<<<1, kFinThreads, 0, st>>>(P, blocks, 1, kSetS1, k, nullptr, nullptr, AB, BB, SC);
             k_ad_rbar<<<blocks, kAdThreads, 0, st>>>(n, qa, qk1, q0, qkm, rb, B, BB, SC, k, P);
@@ -477,7 +515,7 @@ int dos_gradient(gbn_ctx* c, const gbn_model* m, double g0, const double* u_host
                                                        hbar.as<double>());
             GBN_CK_LAUNCH(c);
             c->launches += 6;
-            double2* old_qa = qa;
+            V* old_qa = qa;
             qa = tmpv;   // qbar_k (complete)
             tmpv = qb;   // free
             qb = old_qa; // qbar_{k-1} (partial)
@@ -498,6 +536,19 @@ int dos_gradient(gbn_ctx* c, const gbn_model* m, double g0, const double* u_host
         grad[q] = s;
     }
     return GBN_OK;
+}
+
+int dos_gradient(gbn_ctx* c, int32_t prec, const gbn_model* m, double g0, const double* u_host, int32_t K, int32_t C,
+                 double eta, int32_t n_en, double emin, double emax, const double* target, double* loss_out,
+                 double* grad, double* dos, double* a_out, double* b_out)
+{
+    if (prec == GBN_FP64)
+        return dos_gradient_t<double2, double>(c, m, g0, u_host, K, C, eta, n_en, emin, emax, target, loss_out, grad,
+                                               dos, a_out, b_out);
+    if (prec == GBN_MIXED)
+        return dos_gradient_t<float2, float>(c, m, g0, u_host, K, C, eta, n_en, emin, emax, target, loss_out, grad,
+                                             dos, a_out, b_out);
+    return fail(c, GBN_ERR_ARG, "bad precision");
 }
 
 }  // namespace gbn

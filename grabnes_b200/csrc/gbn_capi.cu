@@ -729,7 +729,18 @@ int gbn_dos_gradient(gbn_ctx* c, const gbn_model* model, double g0, const double
 {
     if (!c) return GBN_ERR_ARG;
     cudaSetDevice(c->device);
-    return dos_gradient(c, model, g0, u, nrecurs, checkpoint, eta, n_en, emin, emax, target, loss, grad, dos, a, b);
+    return dos_gradient(c, GBN_FP64, model, g0, u, nrecurs, checkpoint, eta, n_en, emin, emax, target, loss, grad,
+                        dos, a, b);
+}
+
+int gbn_dos_gradient_prec(gbn_ctx* c, int32_t precision, const gbn_model* model, double g0, const double* u,
+                          int32_t nrecurs, int32_t checkpoint, double eta, int32_t n_en, double emin, double emax,
+                          const double* target, double* loss, double* grad, double* dos, double* a, double* b)
+{
+    if (!c) return GBN_ERR_ARG;
+    cudaSetDevice(c->device);
+    return dos_gradient(c, precision, model, g0, u, nrecurs, checkpoint, eta, n_en, emin, emax, target, loss, grad,
+                        dos, a, b);
 }
 
 }  // extern "C"

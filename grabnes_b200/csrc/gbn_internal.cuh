@@ -207,9 +207,9 @@ int haldane(gbn_ctx* c, double aG, double t2, double phase, int32_t paper, uint3
 int check_hamiltonian(gbn_ctx* c, int64_t* out, double* max_asym);   // c->ptau from the positions, images and cell of the assembled model
 
 // gradient of a DOS loss (gbn_adjoint.cu)
-int dos_gradient(gbn_ctx* c, const gbn_model* m, double g0, const double* u_host, int32_t K, int32_t C, double eta,
-                 int32_t n_en, double emin, double emax, const double* target, double* loss_out, double* grad,
-                 double* dos, double* a_out, double* b_out);
+int dos_gradient(gbn_ctx* c, int32_t prec, const gbn_model* m, double g0, const double* u_host, int32_t K, int32_t C,
+                 double eta, int32_t n_en, double emin, double emax, const double* target, double* loss_out,
+                 double* grad, double* dos, double* a_out, double* b_out);
 
 // Chebyshev (gbn_cheb.cu)
 int cheb_evolve(gbn_ctx* c, int32_t prec, int32_t nrhs, const double* c_host, int32_t npol, double ac, double bc,

@@ -319,6 +319,13 @@ int gbn_set_neighd(gbn_ctx* ctx, const double* neighd);
 int gbn_dos_gradient(gbn_ctx* ctx, const gbn_model* model, double g0, const double* u, int32_t nrecurs,
                      int32_t checkpoint, double eta, int32_t n_en, double emin, double emax, const double* target,
                      double* loss, double* grad, double* dos, double* a, double* b);
+/* The same with a precision: GBN_FP64 (= gbn_dos_gradient) or GBN_MIXED, the FP32 variant: complex64
+ * recursion and adjoint vectors (checkpoints included) and FP32 hoppings, with FP64 arithmetic in every
+ * kernel, FP64 dot products, scalars, continued fraction and dL/dH accumulation.  No counterpart in
+ * the reference. */
+int gbn_dos_gradient_prec(gbn_ctx* ctx, int32_t precision, const gbn_model* model, double g0, const double* u,
+                          int32_t nrecurs, int32_t checkpoint, double eta, int32_t n_en, double emin, double emax,
+                          const double* target, double* loss, double* grad, double* dos, double* a, double* b);
 
 /* ---- recursion without device allocation ------------------------------------------------------ */
 /* No counterpart in the reference: an addition for hosts that cannot allocate device memory.

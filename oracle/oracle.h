@@ -100,6 +100,11 @@ typedef struct {
     int32_t koshino_sr;
     int32_t renormalize_coupling;
     double  coupling_factor;
+    /* Smooth interlayer cutoff of the differentiable model (no counterpart in the reference, whose cutoff
+     * is hard, neigh.F90:269-276): the two-centre term times s(rho) of the in-plane distance rho,
+     * s = 1 up to rho_c - w, (1 + cos(pi (rho - rho_c + w) / w)) / 2 up to rho_c, 0 beyond; w = 0: none. */
+    double  inter_smooth_w;
+    double  inter_cut_rho;
 } orc_model;
 
 void orc_onsite(const orc_model* m, int64_t n, const double* Rat,

@@ -41,6 +41,7 @@ class Model(C.Structure):
         ("d_interlayer", C.c_double), ("aCC", C.c_double), ("g_intlay", C.c_double),
         ("anderson", C.c_int32), ("anderson_w", C.c_double), ("seed", C.c_int32), ("e0_c", C.c_double),
         ("koshino_sr", C.c_int32), ("renormalize_coupling", C.c_int32), ("coupling_factor", C.c_double),
+        ("inter_smooth_w", C.c_double), ("inter_cut_rho", C.c_double),
     ]
 
 
@@ -253,3 +254,16 @@ def evol(nb, hop, h0, c, ac, bc, psi, zupsi, direction=1):
                    np.ascontiguousarray(nb["neighd"]).reshape(-1), np.ascontiguousarray(hop, np.complex128).reshape(-1),
                    np.ascontiguousarray(h0), np.ascontiguousarray(c, np.complex128), len(c), ac, bc, direction, p, z)
     return p, z
+
+
+def dos_loss(model, rat_hop, species, layer, nb, h0, u, nrecurs, eta, n_en, emin, emax, target, nthreads=0):
+    """L = sum_E (DOS(E) - target(E))^2 of the DOS-fitting problem, all in the oracle: hoppings of `model`
+    (orc_hopping, with the smooth interlayer cutoff), the FP64 three-pass recursion (KuboRecursion) of the
+    random-phase state exp(2 pi i u) / sqrt(N), and the continued fraction (KuboFrac).  Returns (L, DOS)."""
+    hop = hopping(model, rat_hop, species, layer, nb)
+    n = len(species)
+    psi = np.exp(2j * np.pi * np.asarray(u, np.float64)) / np.sqrt(n)
+    a, b = recursion(nb, hop, h0, psi, nrecurs, nthreads)
+    _, dos = frac(a, b, eta, n_en, emin, emax)
+    t = np.asarray(target, np.float64)
+    return float(((dos - t) ** 2).sum()), dos

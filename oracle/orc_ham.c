@@ -198,7 +198,14 @@ void orc_hopping(const orc_model* m, int64_t n, const double* Rat, const int32_t
                     const double vsig = m->vppsigma0 * exp(-(dist - m->d_interlayer) / m->bl_delta) * renorm;
                     const double vpi = m->vpppi0 * exp(-(dist - m->aCC) / m->bl_delta) * renorm;
                     const double q = D[2] / dist;
-                    h[0] = h[0] + (vpi * (1.0 - q * q) + vsig * (q * q));
+                    double sc = 1.0;   /* smooth cutoff of the differentiable model (1 without one) */
+                    if (m->inter_smooth_w > 0.0) {
+                        const double rho = sqrt(D[0] * D[0] + D[1] * D[1]);
+                        const double r0 = m->inter_cut_rho - m->inter_smooth_w;
+                        if (rho >= m->inter_cut_rho) sc = 0.0;
+                        else if (rho > r0) sc = 0.5 * (1.0 + cos(ORC_PI * (rho - r0) / m->inter_smooth_w));
+                    }
+                    h[0] = h[0] + (vpi * (1.0 - q * q) + vsig * (q * q)) * sc;
                     /* ham.F90:6807-6838 without Interlayer.DifferentCouplings */
                     if (m->renormalize_coupling) h[0] = m->coupling_factor * h[0];
                 } else {
