@@ -424,14 +424,17 @@ TEVOL_KEYS = {"Run.TypeOfSystem": "Graphene", "Structure.CellSize": 83, "Structu
 HBAR_EV_S = 6.582119569e-16
 
 
-def tevol_leg(G, M, local, stream, ws, nt=10, npol=100, nvec=8, nrecurs=100):
+def tevol_leg(G, M, local, stream, ws, nt=10, npol=100, nvec=8, nrecurs=100, nt_msd=100, nwr_msd=10):
     """Chebyshev Kubo time evolution of graphene on hBN at 0.61 degrees (example 07's cell, CellSize 83,
     SuperCell 16 = 3,527,168 atoms) with Anderson disorder W = 1 eV (seed 5): dt = 1 fs (g0 dt / hbar),
-    KuboCn with the reference's default 100 polynomials, 8 random-phase vectors, mixed precision; nt of
-    the workload's 1000 steps, one recursion of the commutator state at the end.  gbn_kubo_tevol (states
-    resident on the device) against the same steps through gbn_kubo_evol with the states on the host
-    every step.  Work unit: an atom-polynomial step of the dual recurrence (N x vectors x (npol - 1) per
-    time step); each time step also propagates zupsi by U (as many single products)."""
+    KuboCn with the reference's default 100 polynomials, 8 random-phase vectors, mixed precision.
+    (1) nt_msd = 100 of the workload's 1000 steps with the states on the device (gbn_kubo_tevol), the
+    recursion of the commutator state every nwr_msd steps, and the mean-square displacement and
+    diffusivity of the 8 vectors (gbn_kubo_msd); the whole workload is 10 x these steps (each step is the
+    same work), which the line states.  (2) nt = 10 steps through gbn_kubo_tevol against the same steps
+    through gbn_kubo_evol with the states on the host every step.  Work unit: an atom-polynomial step of
+    the dual recurrence (N x vectors x (npol - 1) per time step); each time step also propagates zupsi by
+    U (as many single products)."""
     import torch
     job = M.job_from_keys(TEVOL_KEYS)
     ctx = G.Context(local)
@@ -457,6 +460,10 @@ def tevol_leg(G, M, local, stream, ws, nt=10, npol=100, nvec=8, nrecurs=100):
         torch.cuda.synchronize()
         return r, dist_max(e0.elapsed_time(e1), ws) / 1e3
 
+    (_, _, nrm_m, _, _), t_msd = timed(lambda: ctx.kubo_tevol(c, ac, bc, psi, zero, nt_msd, nwr_msd, nrecurs, 1,
+                                                             G.GBN_MIXED))
+    dt_fs = dt * HBAR_EV_S / g0 * 1e15
+    t_fs, msd, d_ratio, d_slope = G.kubo_msd(nrm_m, nwr_msd, dt_fs)
     (p1, z1, nrm, _, _), t_dev = timed(lambda: ctx.kubo_tevol(c, ac, bc, psi, zero, nt, nt, nrecurs, 1, G.GBN_MIXED))
 
     def host_loop():
@@ -470,7 +477,17 @@ def tevol_leg(G, M, local, stream, ws, nt=10, npol=100, nvec=8, nrecurs=100):
     nz, t_host = timed(host_loop)
     ctx.close()
     work = float(n) * nvec * (npol - 1) * nt
+    work_m = float(n) * nvec * (npol - 1) * nt_msd
+    msd_out = {"time_steps": nt_msd, "write_every": nwr_msd, "device_resident_s": t_msd,
+               "atom_poly_steps_per_s": ws * work_m / t_msd,
+               "extrapolated_1000_steps_s": t_msd * 1000.0 / nt_msd,
+               "extrapolation": "the workload's 1000 time steps are 10 x these 100 (each step the same work)",
+               "t_fs": [float(x) for x in t_fs], "msd_ang2": [float(x) for x in msd],
+               "msd_over_t_ang2_per_fs": [float(x) for x in d_ratio],
+               "dmsd_dt_ang2_per_fs": [float(x) for x in d_slope],
+               "accumulation": "FP64 (norms reduced in FP64, complex64 vectors, FP64 accumulators)"}
     return {"workload": "graphene_hbn_0.61deg_anderson_3527168atoms_8vec_dt1fs", "atoms": n, "vectors": nvec,
+            "msd_diffusivity": msd_out,
             "npol": npol, "time_steps": nt, "dt_g0_over_hbar": dt, "atom_poly_steps": work,
             "device_resident_s": t_dev, "device_resident_atom_poly_steps_per_s": ws * work / t_dev,
             "host_states_s": t_host, "host_states_atom_poly_steps_per_s": ws * work / t_host,

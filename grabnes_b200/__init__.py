@@ -101,7 +101,7 @@ EXPORTS = ["gbn_cell_atoms", "gbn_build_cell", "gbn_cart_roundtrip", "gbn_rng_un
            "gbn_peierls", "gbn_get_hamiltonian", "gbn_load_hamiltonian", "gbn_lanczos", "gbn_lanczos_phases",
            "gbn_stage_phases", "gbn_run_staged", "gbn_cf_dos", "gbn_cheb_evolve", "gbn_kubo_evol", "gbn_set_neighd", "gbn_lanczos_noalloc",
            "gbn_cheb_interval", "gbn_cheb_coef", "gbn_dos_gradient", "gbn_dos_gradient_prec", "gbn_lanczos_sites", "gbn_lanczos_sets",
-           "gbn_pdos_atoms", "gbn_pdos_sets", "gbn_lanczos_fields", "gbn_set_images", "gbn_haldane", "gbn_kubo_tevol", "gbn_check_hamiltonian"]
+           "gbn_pdos_atoms", "gbn_pdos_sets", "gbn_lanczos_fields", "gbn_set_images", "gbn_haldane", "gbn_kubo_tevol", "gbn_check_hamiltonian", "gbn_kubo_msd"]
 
 
 def _declare(L):
@@ -118,7 +118,7 @@ def _declare(L):
     L.gbn_version.restype = C.c_char_p
     L.gbn_set_stream.argtypes = [vp, vp]
     L.gbn_set_tuning.argtypes = [vp, i32, i32, i32, i32, i32]
-    L.gbn_set_kernel_variant.argtypes = [vp, i32, i32, i32]
+    L.gbn_set_kernel_variant.argtypes = [vp, i32, i32, i32, i32]
     L.gbn_launch_count.argtypes = [vp]
     L.gbn_launch_count.restype = i64
     L.gbn_last_timing.argtypes = [vp, C.POINTER(d), C.POINTER(i64)]
@@ -162,6 +162,8 @@ def _declare(L):
                                         _p(np.float64), C.POINTER(d), _p(np.float64), _opt(np.float64),
                                         _opt(np.float64), _opt(np.float64)]
     L.gbn_cheb_coef.argtypes = [d, d, d, i32, _p(np.complex128)]
+    L.gbn_kubo_msd.argtypes = [i32, i32, i32, d, _p(np.float64), _p(np.float64), _p(np.float64), _opt(np.float64),
+                               _opt(np.float64)]
     # device pointers (ints from tensor.data_ptr()), no context
     L.gbn_lanczos_noalloc.argtypes = [i64, i32, vp, vp, vp, vp, vp, i32, vp, vp, vp]
 
@@ -206,11 +208,12 @@ class Context:
     def set_tuning(self, rhs_per_thread=0, blocks_per_sm=0, rows_per_group=0, staged=-1, prefetch=-1):
         self._ck(self._L.gbn_set_tuning(self._h, rhs_per_thread, blocks_per_sm, rows_per_group, staged, prefetch))
 
-    def set_kernel_variant(self, col_unroll=0, stage_values=-1, min_blocks=0):
+    def set_kernel_variant(self, col_unroll=0, stage_values=-1, min_blocks=0, field_table=-1):
         """Columns in flight per batch of the sparse product (4, 8; 0 = default), whether staged slice
-        records carry the values (1) or only the column indices (0; -1 = default), and the resident blocks
-        per SM its registers are bounded for (1, 3; 0 = 1)."""
-        self._ck(self._L.gbn_set_kernel_variant(self._h, col_unroll, stage_values, min_blocks))
+        records carry the values (1) or only the column indices (0; -1 = default), the resident blocks per
+        SM its registers are bounded for (1, 3; 0 = 1), and for batched fields the per-tile rotation table
+        (1) or rotations on the fly (0, -1 = default)."""
+        self._ck(self._L.gbn_set_kernel_variant(self._h, col_unroll, stage_values, min_blocks, field_table))
 
     @property
     def launches(self):
@@ -513,3 +516,15 @@ def rng_uniform(seed, n):
 
 def version():
     return lib().gbn_version().decode()
+
+
+def kubo_msd(norms, nwr, dt_fs):
+    """Mean-square displacement and diffusivity from the norms [nrhs][nw] of Context.kubo_tevol (see
+    gbn_kubo_msd): (t [fs], MSD [Ang^2], MSD / t, d MSD / dt [Ang^2 / fs])."""
+    nr = np.ascontiguousarray(np.atleast_2d(norms), np.float64)
+    nrhs, nw = nr.shape
+    t, msd, dr, ds = (np.zeros(nw) for _ in range(4))
+    rc = lib().gbn_kubo_msd(nrhs, nw, nwr, dt_fs, nr.reshape(-1), t, msd, dr, ds)
+    if rc:
+        raise GbnError(rc, "bad arguments")
+    return t, msd, dr, ds

@@ -206,15 +206,17 @@ int gbn_set_tuning(gbn_ctx* c, int32_t rhs_per_thread, int32_t blocks_per_sm, in
     return GBN_OK;
 }
 
-int gbn_set_kernel_variant(gbn_ctx* c, int32_t col_unroll, int32_t stage_values, int32_t min_blocks)
+int gbn_set_kernel_variant(gbn_ctx* c, int32_t col_unroll, int32_t stage_values, int32_t min_blocks,
+                           int32_t field_table)
 {
     if (!c) return GBN_ERR_ARG;
     if ((col_unroll != 0 && col_unroll != 4 && col_unroll != 8) || stage_values < -1 || stage_values > 1 ||
-        (min_blocks != 0 && min_blocks != 1 && min_blocks != 3))
+        (min_blocks != 0 && min_blocks != 1 && min_blocks != 3) || field_table < -1 || field_table > 1)
         return fail(c, GBN_ERR_ARG, "kernel variant out of range");
     c->tune_unroll = col_unroll;
     c->tune_stage_values = stage_values;
     c->tune_min_blocks = min_blocks;
+    c->tune_field_table = field_table;
     return GBN_OK;
 }
 
@@ -581,10 +583,11 @@ int gbn_lanczos_fields(gbn_ctx* c, int32_t precision, int32_t nfields, const int
         }
     const int64_t n = c->n;
     GBN_CK(c, c->upload.ensure(sizeof(double) * (size_t)n * T));
-    GBN_CK(c, c->field_m.ensure(sizeof(int32_t) * (size_t)T));
     std::vector<double> ar((size_t)nrhs * nmax), br((size_t)nrhs * nmax);
-    std::vector<int32_t> fm((size_t)T);
     c->tune_rpt = rpt;
+    split_rhs(precision, T, rpt, &rpt, &tpr);   // the split the tile's kernel uses
+    GBN_CK(c, c->field_m.ensure(sizeof(int32_t) * (size_t)(T + tpr)));
+    std::vector<int32_t> fm((size_t)(T + tpr));
     rc = run_tiles(
         c, precision, nrhs,
         [&](int r0, int cnt) -> int {
@@ -592,8 +595,15 @@ int gbn_lanczos_fields(gbn_ctx* c, int32_t precision, int32_t nfields, const int
                 GBN_CK(c, cudaMemcpyAsync(c->upload.as<double>() + (size_t)r * n, u + (size_t)order[(size_t)(r0 + r)] * n,
                                           sizeof(double) * (size_t)n, cudaMemcpyHostToDevice, c->stream));
             for (int r = 0; r < T; ++r) fm[(size_t)r] = fm_run[(size_t)(r0 + (r < cnt ? r : 0))];
-            GBN_CK(c, cudaMemcpyAsync(c->field_m.p, fm.data(), sizeof(int32_t) * (size_t)T, cudaMemcpyHostToDevice,
+            // the flux quanta of each thread slot of a row group (the slot's RPT right-hand sides share one
+            // field) follow those of the right-hand sides: fm[T + q] = fm[q RPT]
+            for (int q = 0; q < tpr; ++q) fm[(size_t)T + q] = fm[(size_t)q * rpt];
+            GBN_CK(c, cudaMemcpyAsync(c->field_m.p, fm.data(), sizeof(int32_t) * fm.size(), cudaMemcpyHostToDevice,
                                       c->stream));
+            if (c->tune_field_table == 1) {   // the tile's rotations, once for all its steps
+                const int rc2 = build_field_table(c, tpr, c->field_m.as<int32_t>() + T);
+                if (rc2) return rc2;
+            }
             return lanczos_start_from_phases(c, c->upload.as<double>(), cnt);
         },
         ns_run.data(), nmax, ar.data(), br.data(), true);

@@ -119,4 +119,32 @@ int gbn_cheb_coef(double dt, double ac, double bc, int32_t npol, double* c)
     return GBN_OK;
 }
 
+// Spread and diffusivity of the time evolution (no counterpart in the reference, which writes only the
+// norms, kubo.F90:376-385).  The norm |ZUPsi_r|^2 = <psi_r| [X, U(t)]^+ [X, U(t)] |psi_r> of KuboTEvol is
+// the spread <(X(t) - X(0))^2> of the start vector psi_r; for random-phase vectors it estimates the
+// trace over the states per atom, so the mean over the vectors is the mean-square displacement
+// MSD(t) = <Delta X^2>(t) [Ang^2].  The diffusivity is written both ways: D(t) = MSD(t) / t and
+// D'(t) = d MSD / dt, the latter by central differences between write steps (MSD(0) = 0 at the start,
+// one-sided at the last step).  Sums in FP64, vectors in order.
+int gbn_kubo_msd(int32_t nrhs, int32_t nw, int32_t nwr, double dt_fs, const double* norms, double* t_fs,
+                 double* msd, double* d_ratio, double* d_slope)
+{
+    if (nrhs < 1 || nw < 1 || nwr < 1 || !(dt_fs > 0.0) || !norms || !t_fs || !msd) return GBN_ERR_ARG;
+    for (int w = 0; w < nw; ++w) {
+        double s = 0.0;
+        for (int r = 0; r < nrhs; ++r) s += norms[(size_t)r * nw + w];
+        msd[w] = s / nrhs;
+        t_fs[w] = (double)(w + 1) * nwr * dt_fs;
+        if (d_ratio) d_ratio[w] = msd[w] / t_fs[w];
+    }
+    if (d_slope) {
+        for (int w = 0; w < nw; ++w) {
+            const double t0 = w > 0 ? t_fs[w - 1] : 0.0, m0 = w > 0 ? msd[w - 1] : 0.0;
+            if (w + 1 < nw) d_slope[w] = (msd[w + 1] - m0) / (t_fs[w + 1] - t0);
+            else d_slope[w] = (msd[w] - m0) / (t_fs[w] - t0);
+        }
+    }
+    return GBN_OK;
+}
+
 }  // extern "C"

@@ -3,7 +3,8 @@
 // flux quantum (HamPeierlsPeriodicGauge, lanczosKuboCode/Src/ham.F90:12834-12882, is linear in the
 // number of flux quanta m), and the threads of a right-hand side of m quanta rotate the entry by
 // exp(2 pi i frac(m tau)) as they use it.  One matrix stream then feeds every field of a tile instead
-// of one assembled matrix per field.
+// of one assembled matrix per field.  The tile-table kernels read the same records with the rotations
+// done once per tile (build_field_table): complex values per thread slot.
 #include "gbn_step.cuh"
 
 namespace gbn {
@@ -19,6 +20,36 @@ static StepFn pick_field_g(int rpt, int tpr, bool staged)
         GBN_CASE(4, 1) GBN_CASE(4, 2) GBN_CASE(4, 4) GBN_CASE(4, 8)
     }
 #undef GBN_CASE
+    return nullptr;
+}
+
+template <typename VT, int G>
+static StepFn pick_table_g(int rpt, int tpr, bool staged)
+{
+#define GBN_CASE(RP, TP)                                                                                        \
+    if (rpt == RP && tpr == TP)                                                                                 \
+        return staged ? k_spmm_staged<VT, true, G, RP, TP, false, kColUnroll, true, 1, true>                     \
+                      : k_spmm_step<VT, true, G, RP, TP, false, kColUnroll, true>;
+    GBN_CASE(1, 1) GBN_CASE(1, 2) GBN_CASE(1, 4) GBN_CASE(1, 8) GBN_CASE(1, 16) GBN_CASE(1, 32)
+    GBN_CASE(2, 1) GBN_CASE(2, 2) GBN_CASE(2, 4) GBN_CASE(2, 8) GBN_CASE(2, 16)
+    if constexpr (sizeof(VT) == 4) {
+        GBN_CASE(4, 1) GBN_CASE(4, 2) GBN_CASE(4, 4) GBN_CASE(4, 8)
+    }
+#undef GBN_CASE
+    return nullptr;
+}
+
+StepFn field_table_kernel(int prec, int G, int rpt, int tpr, bool staged)
+{
+    if (prec == GBN_MIXED) {
+        if (G == 1) return pick_table_g<float, 1>(rpt, tpr, staged);
+        if (G == 2) return pick_table_g<float, 2>(rpt, tpr, staged);
+        if (G == 4) return pick_table_g<float, 4>(rpt, tpr, staged);
+    } else {
+        if (G == 1) return pick_table_g<double, 1>(rpt, tpr, staged);
+        if (G == 2) return pick_table_g<double, 2>(rpt, tpr, staged);
+        if (G == 4) return pick_table_g<double, 4>(rpt, tpr, staged);
+    }
     return nullptr;
 }
 

@@ -67,6 +67,13 @@ struct Ell {
     int64_t cap_record = 0;  // staging buffer size: 99.5 % of the records fit (larger ones are read in place)
     int64_t cap_pct[4] = {0, 0, 0, 0};   // record sizes at the 99.5th, 99th, 95th and 90th percentiles
     bool field = false;      // field-batched values: field-free hopping and Peierls phase per flux quantum
+    // Field-batched tile table: the records with each value rotated for the fields of the tile's thread
+    // slots (slot q of a row group = its q-th thread's right-hand sides): int32 col[w][gpw] then complex
+    // val[w][gpw][slots][G] (slot q rotated by the field of slot q).  Rebuilt for every tile.
+    DevBuf ftab;
+    int ftab_slots = 0;
+    int ftab_entry_bytes = 0;   // 4 + slots * G * complex bytes
+    bool ftab_valid = false;
     bool valid = false;
 };
 
@@ -147,6 +154,7 @@ struct gbn_ctx {
     int tune_unroll = 0;         // union columns in flight per batch of the product (4, 8; 0 = automatic)
     int tune_stage_values = -1;  // staged records carry the values (1) or only the column indices (0); -1 auto
     int tune_min_blocks = 0;     // product kernel compiled for 1 or 3 resident blocks per SM (0 = 1)
+    int tune_field_table = -1;   // batched fields: rotations tabulated per tile (1) or on the fly (0, -1 default)
     bool last_staged = false;    // the last recursion used the staged kernel
 
     // Chebyshev work vectors
@@ -182,6 +190,8 @@ int build_spatial_perm(gbn_ctx* c);
 // field: the field-batched values (FieldVal: field-free hopping and c->ptau), for gbn_lanczos_fields
 int build_ell(gbn_ctx* c, int prec, int G, int gpw, bool field = false);
 int auto_group(const gbn_ctx* c, int R);   // default rows per group for a tile of R vectors
+// the tile table of the field-batched layout for the flux quanta of each thread slot (d_slot_m [slots])
+int build_field_table(gbn_ctx* c, int slots, const int32_t* d_slot_m);
 
 // recursion (gbn_lanczos.cu)
 int lanczos_prepare(gbn_ctx* c, int prec, int nrhs, bool field = false);

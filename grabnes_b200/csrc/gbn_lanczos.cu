@@ -241,6 +241,8 @@ struct StepLaunch {
     size_t smem = 0;
     int64_t cap = 0;
     bool staged = false;
+    const unsigned char* mat = nullptr;   // the records the kernel reads (the layout's, or its tile table)
+    int64_t entry_bytes = 0;
 };
 
 constexpr size_t kStagedSmemBudget = 200 * 1024;
@@ -259,10 +261,16 @@ static int step_launch(gbn_ctx* c, int R, StepLaunch* L)
     v.unroll = c->tune_unroll > 0 ? c->tune_unroll : (c->prec == GBN_MIXED ? 8 : 4);
     v.stage_values = c->tune_stage_values != 0;
     v.min_blocks = c->tune_min_blocks > 0 ? c->tune_min_blocks : (v.unroll == 8 && E.G == 1 && !E.cplx ? 3 : 1);
+    // batched fields rotate on the fly unless the tile table is asked for (measured slower on example 06's
+    // sweep: 0.175 against 0.108 ms per product, the table's complex values per thread slot triple the
+    // records' bytes)
+    const bool use_table = E.field && c->tune_field_table == 1 && E.ftab_valid;
+    L->mat = use_table ? E.ftab.as<unsigned char>() : E.mat.as<unsigned char>();
+    L->entry_bytes = use_table ? E.ftab_entry_bytes : E.entry_bytes;
     // buffer bytes of a record of percentile i: whole records, or their index part (multiples of 16)
     auto cap_of = [&](int i) -> int64_t {
-        const int64_t rec = E.cap_pct[i];
-        return v.stage_values ? rec : (rec / E.entry_bytes * 4 + 15) / 16 * 16;
+        const int64_t nent = E.cap_pct[i] / E.entry_bytes;
+        return ((v.stage_values ? nent * L->entry_bytes : nent * 4) + 15) / 16 * 16;
     };
     const bool want_staged = c->tune_staged != 0 && cap_of(0) > 0;
     // the kernel of this variant; shapes without it take the base variant unless one was asked for
@@ -271,9 +279,12 @@ static int step_launch(gbn_ctx* c, int R, StepLaunch* L)
         int rpt, tpr;
         split_rhs(c->prec, R, c->tune_rpt, &rpt, &tpr);
         const StepVariant base;
-        if (E.field)
-            return (v.unroll == 4 && v.stage_values && v.min_blocks == 1) || !asked
-                       ? field_step_kernel(c->prec, E.G, rpt, tpr, staged) : nullptr;
+        if (E.field) {
+            if (!((v.unroll == 4 && v.stage_values && v.min_blocks == 1) || !asked)) return nullptr;
+            if (use_table)
+                return E.ftab_slots == tpr ? field_table_kernel(c->prec, E.G, rpt, tpr, staged) : nullptr;
+            return field_step_kernel(c->prec, E.G, rpt, tpr, staged);
+        }
         StepFn f = step_kernel(c->prec, E.cplx, E.G, R, c->tune_rpt, staged, v);
         if (!f && !asked) f = step_kernel(c->prec, E.cplx, E.G, R, c->tune_rpt, staged, base);
         return f;
@@ -492,11 +503,14 @@ int lanczos_run(gbn_ctx* c, int32_t nmax)
     const int rc = step_launch(c, R, &L);
     if (rc) return rc;
     c->last_staged = L.staged;
+    // the block partials of this launch shape (it may differ from the one the buffers were sized for)
+    GBN_CK(c, c->partials.ensure(sizeof(double) * (size_t)R *
+                                 (size_t)std::max(L.grid, c->num_sms * kUpdateBlocksPerSM)));
     StepParams p;
     memset(&p, 0, sizeof p);
     p.slice_ptr = c->ell.slice_ptr.as<int64_t>();
-    p.mat = c->ell.mat.as<unsigned char>();
-    p.entry_bytes = c->ell.entry_bytes;
+    p.mat = L.mat;
+    p.entry_bytes = L.entry_bytes;
     p.cap_record = L.cap;
     // default: the epilogue rows into L2, and in mixed precision the rows of u_k two sweeps ahead
     p.prefetch = c->tune_prefetch < 0 ? (c->prec == GBN_MIXED ? 6 : 4) : c->tune_prefetch;

@@ -312,6 +312,72 @@ int auto_group(const gbn_ctx* c, int R)
     return R == 1 ? 1 : 2;
 }
 
+// ---------------------------------------------------------------------------- field tile table
+// One warp per slice: the column indices are copied, and every FieldVal (h, tau) becomes, for each slot q,
+// h exp(2 pi i frac(m_q tau)) with m_q the slot's flux quanta, stored at [entry][slot][G] so that the TPR
+// threads of a row group read their slots' values from one contiguous piece: the turn fraction m_q tau wraps exactly in
+// integer arithmetic and its angle is evaluated by sincospi in FP64, then rounded once to the storage type.
+template <typename VT>
+__global__ void k_field_table(const int64_t* __restrict__ slice_ptr, int64_t nslices, int gpw, int G, int slots,
+                              const unsigned char* __restrict__ mat, int64_t eb, unsigned char* __restrict__ tab,
+                              int64_t teb, const int32_t* __restrict__ slot_m)
+{
+    using C2 = typename V2<VT>::t;
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t s = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); s < nslices; s += warps) {
+        const int64_t base = slice_ptr[s], nent = slice_ptr[s + 1] - base;
+        const int32_t* ci = reinterpret_cast<const int32_t*>(mat + base * eb);
+        const FieldVal<VT>* vi = reinterpret_cast<const FieldVal<VT>*>(mat + base * eb + nent * 4);
+        int32_t* co = reinterpret_cast<int32_t*>(tab + base * teb);
+        C2* vo = reinterpret_cast<C2*>(tab + base * teb + nent * 4);
+        for (int64_t k = lane; k < nent; k += 32) co[k] = ci[k];
+        const int64_t nval = nent * G;
+        for (int64_t k = lane; k < nval; k += 32) {   // value k = (entry, g): out at (entry, slot q, g)
+            const FieldVal<VT> v = vi[k];
+            const int64_t ent = k / G, g = k % G;
+            for (int q = 0; q < slots; ++q) {
+                double sn, cs;
+                if constexpr (sizeof(VT) == 4) {
+                    const uint32_t u = v.t * (uint32_t)(int64_t)slot_m[q];
+                    sincospi((double)(int32_t)u * 4.656612873077393e-10, &sn, &cs);   // 2^-31
+                } else {
+                    const uint64_t u = v.t * (uint64_t)(int64_t)slot_m[q];
+                    sincospi((double)(int64_t)u * 1.0842021724855044e-19, &sn, &cs);   // 2^-63
+                }
+                C2 o;
+                o.x = (VT)((double)v.h * cs);
+                o.y = (VT)((double)v.h * sn);
+                vo[(ent * slots + q) * G + g] = o;
+            }
+        }
+    }
+}
+
+int build_field_table(gbn_ctx* c, int slots, const int32_t* d_slot_m)
+{
+    Ell& E = c->ell;
+    if (!E.valid || !E.field) return fail(c, GBN_ERR_STATE, "internal: no field-batched layout for a tile table");
+    const int csz = E.prec == GBN_MIXED ? (int)sizeof(float2) : (int)sizeof(double2);
+    const int64_t teb = 4 + (int64_t)slots * E.G * csz;
+    GBN_CK(c, E.ftab.ensure((size_t)(E.nnz_stored * teb)));
+    const int blk = 256;
+    const int64_t grid = std::min<int64_t>((E.nslices + (blk / 32) - 1) / (blk / 32), (int64_t)c->num_sms * 16);
+    if (E.prec == GBN_MIXED)
+        k_field_table<float><<<(unsigned)std::max<int64_t>(grid, 1), blk, 0, c->stream>>>(
+            E.slice_ptr.as<int64_t>(), E.nslices, E.gpw, E.G, slots, E.mat.as<unsigned char>(), E.entry_bytes,
+            E.ftab.as<unsigned char>(), teb, d_slot_m);
+    else
+        k_field_table<double><<<(unsigned)std::max<int64_t>(grid, 1), blk, 0, c->stream>>>(
+            E.slice_ptr.as<int64_t>(), E.nslices, E.gpw, E.G, slots, E.mat.as<unsigned char>(), E.entry_bytes,
+            E.ftab.as<unsigned char>(), teb, d_slot_m);
+    GBN_CK_LAUNCH(c);
+    E.ftab_slots = slots;
+    E.ftab_entry_bytes = (int)teb;
+    E.ftab_valid = true;
+    return GBN_OK;
+}
+
 int build_ell(gbn_ctx* c, int prec, int G, int gpw, bool field)
 {
     if (!c->have_ham) return fail(c, GBN_ERR_STATE, "no Hamiltonian loaded");
@@ -322,6 +388,7 @@ int build_ell(gbn_ctx* c, int prec, int G, int gpw, bool field)
     }
     Ell& E = c->ell;
     E.valid = false;
+    E.ftab_valid = false;
     E.dval_dir = 0;
     E.G = G;
     E.gpw = gpw;

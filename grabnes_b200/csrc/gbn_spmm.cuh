@@ -157,7 +157,7 @@ template <typename VT> struct FieldMult;
 template <> struct FieldMult<float> { using t = uint32_t; };
 template <> struct FieldMult<double> { using t = uint64_t; };
 
-template <typename VT, bool CPLX, int G, int RPT, int TPR, bool SMEM, bool SMEM_VAL, bool FIELD, int NB>
+template <typename VT, bool CPLX, int G, int RPT, int TPR, bool SMEM, bool SMEM_VAL, bool FIELD, int NB, int VS = 1>
 __device__ __forceinline__ void column_batch(const typename V2<VT>::t* __restrict__ xq,
                                              const int32_t* __restrict__ cp,
                                              const typename StoredVal<VT, CPLX, FIELD>::t* __restrict__ vp,
@@ -178,7 +178,7 @@ __device__ __forceinline__ void column_batch(const typename V2<VT>::t* __restric
 #pragma unroll
     for (int u = 0; u < NB; ++u) VecIO<VT, RPT>::load(xq + (size_t)(uint32_t)c[u] * R, xg[u]);
 #pragma unroll
-    for (int u = 0; u < NB; ++u) load_group_vals<HT, G, SMEM_VAL>(vp + u * GPW * G, h[u]);
+    for (int u = 0; u < NB; ++u) load_group_vals<HT, G, SMEM_VAL>(vp + u * GPW * G * VS, h[u]);
     if constexpr (FIELD) {
 #pragma unroll
         for (int u = 0; u < NB; ++u)
@@ -198,8 +198,10 @@ __device__ __forceinline__ void column_batch(const typename V2<VT>::t* __restric
     }
 }
 
+// VS: value blocks per union column and group (the field tile table holds one per thread slot, VS = TPR,
+// interleaved [column][group][slot][G]); the caller's vp includes the thread's own slot.
 template <typename VT, bool CPLX, int G, int RPT, int TPR, bool SMEM, bool FIELD = false, int U = kColUnroll,
-          bool SMEM_VAL = SMEM>
+          bool SMEM_VAL = SMEM, int VS = 1>
 __device__ __forceinline__ void group_columns(const typename V2<VT>::t* __restrict__ x, int w,
                                               const int32_t* __restrict__ cp,
                                               const typename StoredVal<VT, CPLX, FIELD>::t* __restrict__ vp,
@@ -217,15 +219,15 @@ __device__ __forceinline__ void group_columns(const typename V2<VT>::t* __restri
         for (int t = 0; t < RPT; ++t) { acc[g][t].x = 0; acc[g][t].y = 0; }
     int k = 0;
     for (; k + U <= w; k += U) {
-        column_batch<VT, CPLX, G, RPT, TPR, SMEM, SMEM_VAL, FIELD, U>(xq, cp, vp, acc, mf);
+        column_batch<VT, CPLX, G, RPT, TPR, SMEM, SMEM_VAL, FIELD, U, VS>(xq, cp, vp, acc, mf);
         cp += U * GPW;
-        vp += U * GPW * G;
+        vp += U * GPW * G * VS;
     }
     if constexpr (U > kColUnroll) {
         for (; k < w; k += kColUnroll) {
-            column_batch<VT, CPLX, G, RPT, TPR, SMEM, SMEM_VAL, FIELD, kColUnroll>(xq, cp, vp, acc, mf);
+            column_batch<VT, CPLX, G, RPT, TPR, SMEM, SMEM_VAL, FIELD, kColUnroll, VS>(xq, cp, vp, acc, mf);
             cp += kColUnroll * GPW;
-            vp += kColUnroll * GPW * G;
+            vp += kColUnroll * GPW * G * VS;
         }
     }
 }

@@ -40,8 +40,10 @@ struct StepParams {
 };
 
 using StepFn = void (*)(StepParams);
-// the sparse-product kernel of the field-batched layout (gbn_fields.cu)
+// the sparse-product kernel of the field-batched layout (gbn_fields.cu): rotations on the fly, or the
+// tile table (complex values per thread slot)
 StepFn field_step_kernel(int prec, int G, int rpt, int tpr, bool staged);
+StepFn field_table_kernel(int prec, int G, int rpt, int tpr, bool staged);
 
 // Variant of the product kernel: columns in flight per batch (4 or 8) and, for the staged kernel,
 // whether the staged records carry the values or only the column indices.  Real-valued layouts at the
@@ -195,7 +197,7 @@ __device__ __forceinline__ void reduce_and_finalize(const StepParams& p, double*
 // point at the thread's group in the slice record; the indices come from shared memory (SMEM) or global
 // memory (streamed), the values likewise (SMEM_VAL).  U columns are in flight per batch.
 // FIELD: field-batched values (FieldVal), the thread's field is that of its first right-hand side.
-template <typename VT, bool CPLX, int G, int RPT, int TPR, bool SMEM, bool FIELD, int U, bool SMEM_VAL>
+template <typename VT, bool CPLX, int G, int RPT, int TPR, bool SMEM, bool FIELD, int U, bool SMEM_VAL, int VS = 1>
 __device__ __forceinline__ void group_slice(const StepParams& p, int64_t s, int w, const int32_t* __restrict__ cp,
                                             const typename StoredVal<VT, CPLX, FIELD>::t* __restrict__ vp,
                                             const double (&sc)[2][RPT * TPR], double* acc_s)
@@ -214,7 +216,7 @@ __device__ __forceinline__ void group_slice(const StepParams& p, int64_t s, int 
     C2 acc[G][RPT];
     typename FieldMult<VT>::t mf = 0;
     if constexpr (FIELD) mf = (typename FieldMult<VT>::t)(int64_t)p.field_m[q * RPT];
-    group_columns<VT, CPLX, G, RPT, TPR, SMEM, FIELD, U, SMEM_VAL>(xc, w, cp, vp, acc, mf);
+    group_columns<VT, CPLX, G, RPT, TPR, SMEM, FIELD, U, SMEM_VAL, VS>(xc, w, cp, vp, acc, mf);
     // epilogue per row: the on-site term (own u_k row, loaded here so that it holds no registers during
     // the column loop), then v_{k+1} and the dot-product term in FP64
 #pragma unroll
@@ -240,13 +242,15 @@ __device__ __forceinline__ void group_slice(const StepParams& p, int64_t s, int 
 // Matrix records read from global memory.  Every block owns a contiguous range of slices (a compact
 // region of the row order); its warps take neighbouring slices, so the rows they gather overlap in L1.
 // FIELD: the field-batched layout (values FieldVal<VT>, fields p.field_m).
-template <typename VT, bool CPLX, int G, int RPT, int TPR, bool FIELD = false, int U = kColUnroll>
+// SLOT: the field-batched tile table (complex values, one block per thread slot; thread q reads block q).
+template <typename VT, bool CPLX, int G, int RPT, int TPR, bool FIELD = false, int U = kColUnroll, bool SLOT = false>
 __global__ void __launch_bounds__(256) k_spmm_step(StepParams p)
 {
     using HT = typename StoredVal<VT, CPLX, FIELD>::t;
     constexpr int GPW = 32 / TPR;
     constexpr int R = RPT * TPR;
     const int sub = (threadIdx.x & 31) / TPR;
+    const int q = (threadIdx.x & 31) % TPR;
     __shared__ double sc[2][R];
     load_step_scalars<R>(p, sc);
     double acc_s[RPT];
@@ -260,9 +264,11 @@ __global__ void __launch_bounds__(256) k_spmm_step(StepParams p)
         const int64_t base = p.slice_ptr[s];
         const int w = (int)((p.slice_ptr[s + 1] - base) / GPW);
         const unsigned char* rec = p.mat + base * p.entry_bytes;
-        group_slice<VT, CPLX, G, RPT, TPR, false, FIELD, U, false>(
+        constexpr int VS = SLOT ? TPR : 1;   // tile table: [column][group][slot][G]
+        const int voff = SLOT ? (sub * TPR + q) * G : sub * G;
+        group_slice<VT, CPLX, G, RPT, TPR, false, FIELD, U, false, VS>(
             p, s, w, reinterpret_cast<const int32_t*>(rec) + sub,
-            reinterpret_cast<const HT*>(rec + (size_t)w * GPW * 4) + sub * G, sc, acc_s);
+            reinterpret_cast<const HT*>(rec + (size_t)w * GPW * 4) + voff, sc, acc_s);
     }
     reduce_and_finalize<RPT, TPR>(p, acc_s);
 }
@@ -388,7 +394,7 @@ __device__ __forceinline__ void prefetch_ahead(const StepParams& p, int64_t s)
 // is bounded (flag bit 2, GBN_ERR_TIMEOUT).
 // FIELD: the field-batched layout (values FieldVal<VT>, fields p.field_m).
 template <typename VT, bool CPLX, int G, int RPT, int TPR, bool FIELD = false, int U = kColUnroll, bool SV = true,
-          int MINB = 1>
+          int MINB = 1, bool SLOT = false>
 __global__ void __launch_bounds__(256, MINB) k_spmm_staged(StepParams p)
 {
     using HT = typename StoredVal<VT, CPLX, FIELD>::t;
@@ -398,6 +404,7 @@ __global__ void __launch_bounds__(256, MINB) k_spmm_staged(StepParams p)
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
     const int sub = lane / TPR;
+    const int q = lane % TPR;
     uint64_t* bar = reinterpret_cast<uint64_t*>(dyn) + 2 * wib;
     const int64_t cap = p.cap_record;   // bytes of one buffer: whole records (SV) or their index part
     unsigned char* buf = dyn + 128 + (size_t)wib * 2 * cap;
@@ -457,17 +464,19 @@ __global__ void __launch_bounds__(256, MINB) k_spmm_staged(StepParams p)
         const unsigned char* grec = p.mat + base * eb;
         if (p.prefetch >= 3) prefetch_epilogue<VT, R, G, GPW>(p, s);
         if (p.prefetch >= 5) prefetch_ahead<VT, R, G, GPW>(p, s + (int64_t)(p.prefetch == 5 ? 1 : p.prefetch == 6 ? 2 : 4) * nwb);
+        constexpr int VS = SLOT ? TPR : 1;   // tile table: [column][group][slot][G], the thread's own slot
+        const int voff = SLOT ? (sub * TPR + q) * G : sub * G;
         if (copy_bytes(s) <= cap) {
             const unsigned char* rec = buf + st * cap;
             if (p.prefetch == 1 || p.prefetch == 2)
                 prefetch_rows<VT, R>(p, reinterpret_cast<const int32_t*>(rec), w * GPW);
-            const HT* vp = reinterpret_cast<const HT*>((SV ? rec : grec) + (size_t)w * GPW * 4) + sub * G;
-            group_slice<VT, CPLX, G, RPT, TPR, true, FIELD, U, SV>(p, s, w, reinterpret_cast<const int32_t*>(rec) + sub,
-                                                                  vp, sc, acc_s);
+            const HT* vp = reinterpret_cast<const HT*>((SV ? rec : grec) + (size_t)w * GPW * 4) + voff;
+            group_slice<VT, CPLX, G, RPT, TPR, true, FIELD, U, SV, VS>(
+                p, s, w, reinterpret_cast<const int32_t*>(rec) + sub, vp, sc, acc_s);
         } else {
-            group_slice<VT, CPLX, G, RPT, TPR, false, FIELD, U, false>(
+            group_slice<VT, CPLX, G, RPT, TPR, false, FIELD, U, false, VS>(
                 p, s, w, reinterpret_cast<const int32_t*>(grec) + sub,
-                reinterpret_cast<const HT*>(grec + (size_t)w * GPW * 4) + sub * G, sc, acc_s);
+                reinterpret_cast<const HT*>(grec + (size_t)w * GPW * 4) + voff, sc, acc_s);
         }
         __syncwarp();   // every lane is done with this buffer before it is refilled
         if (s + 2 * nwb < s1e) {

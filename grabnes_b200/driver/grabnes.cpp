@@ -291,6 +291,7 @@ struct Job {
     bool only_dos = false, polynomials = false;
     int npol = 100, nt = 500, nwr = 10;
     double dt = 5.0;   // units of hbar / g0
+    int tevol_vectors = 1;   // random-phase vectors of the time evolution (Kubo.TEvolVectors)
     long mbi = 0, mbf = 0, mstep = 1;
     bool field_by_value = false, field_steps_by_value = false;
     double b_value = 0, b_init = 0, b_final = 0, b_step = 0;
@@ -403,6 +404,8 @@ Job job_from_input(const Input& in)
     j.nt = (int)in.i("Kubo.NumberofTimeSteps", 500);
     j.nwr = (int)in.i("Kubo.WriteNumberofSteps", 10);
     j.dt = in.d("Kubo.TimeStep", 5.0);
+    j.tevol_vectors = (int)in.i("Kubo.TEvolVectors", 1);   // no counterpart in the reference (one vector)
+    if (j.tevol_vectors < 1 || j.tevol_vectors > 32) die("Kubo.TEvolVectors must be in 1..32");
     if (j.npol < 1 || j.nt < 0 || j.nwr < 1) die("Kubo.NumberofPolynomials and Kubo.WriteNumberofSteps must be positive");
     j.haldane = in.l("Haldane.NNN", false);
     j.hal_paper = in.l("Haldane.PaperOrientation", false);
@@ -597,14 +600,46 @@ void time_evolution(gbn_ctx* ctx, const Job& j, std::vector<double> psi, const s
     }
     write_pairs(prefix + ".cn.dat", re, ab, 0.0, false);
     if (j.only_dos) return;
-    // all nT steps on the device (gbn_kubo_tevol); the files of every nWr-th step from its coefficients
-    std::vector<double> zu((size_t)2 * n, 0.0);
+    // all nT steps on the device (gbn_kubo_tevol); the files of every nWr-th step from its coefficients.
+    // Vector 0 is the reference's start vector; Kubo.TEvolVectors > 1 adds random-phase vectors from the
+    // continuation of the same seeded stream (vector r: draws r N .. (r + 1) N - 1), batched in one call.
+    const int R = j.tevol_vectors;
+    if ((int64_t)psi.size() != 2 * n) die("time evolution without a start vector");
+    psi.resize((size_t)2 * n * R);
+    if (R > 1) {
+        std::vector<double> u((size_t)n * R);
+        ck(gbn_rng_uniform(j.seed, n * R, u.data()), nullptr, "gbn_rng_uniform");
+        const double isn = 1.0 / sqrt((double)n);
+        for (int r = 1; r < R; ++r)
+            for (int64_t i = 0; i < n; ++i) {
+                const double ph = 2.0 * kPi * u[(size_t)r * n + i];
+                psi[(size_t)2 * ((size_t)r * n + i)] = cos(ph) * isn;
+                psi[(size_t)2 * ((size_t)r * n + i) + 1] = sin(ph) * isn;
+            }
+    }
+    std::vector<double> zu((size_t)2 * n * R, 0.0);
     const int nw = j.nt / j.nwr;
-    std::vector<double> norms((size_t)std::max(nw, 1)), az((size_t)std::max(nw, 1) * j.nrecurs),
-        bz((size_t)std::max(nw, 1) * j.nrecurs), energy((size_t)j.n_en + 1), dos((size_t)j.n_en + 1);
-    ck(gbn_kubo_tevol(ctx, GBN_FP64, 1, c.data(), j.npol, ac, bc, 1, j.nt, j.nwr, j.nrecurs, psi.data(), zu.data(),
+    const int nw1 = std::max(nw, 1);
+    std::vector<double> norms((size_t)R * nw1), az((size_t)R * nw1 * j.nrecurs), bz((size_t)R * nw1 * j.nrecurs),
+        energy((size_t)j.n_en + 1), dos((size_t)j.n_en + 1);
+    ck(gbn_kubo_tevol(ctx, GBN_FP64, R, c.data(), j.npol, ac, bc, 1, j.nt, j.nwr, j.nrecurs, psi.data(), zu.data(),
                       norms.data(), az.data(), bz.data()),
        ctx, "gbn_kubo_tevol");
+    if (nw > 0) {   // <prefix>.MSD.dat: spread and diffusivity, the mean over the vectors
+        std::vector<double> nr((size_t)R * nw), t((size_t)nw), msd((size_t)nw), dr((size_t)nw), ds((size_t)nw);
+        for (int r = 0; r < R; ++r)
+            for (int w = 0; w < nw; ++w) nr[(size_t)r * nw + w] = norms[(size_t)r * nw1 + w];
+        const double dt_fs = j.dt * (kHPLANCK / (2.0 * kPi)) / kQE / j.g0 * 1e15;
+        ck(gbn_kubo_msd(R, nw, j.nwr, dt_fs, nr.data(), t.data(), msd.data(), dr.data(), ds.data()), nullptr,
+           "gbn_kubo_msd");
+        FILE* f = fopen((prefix + ".MSD.dat").c_str(), "w");
+        if (!f) die("cannot write " + prefix + ".MSD.dat");
+        fprintf(f, "# %d vector(s), direction x: t [fs], MSD = <(X(t) - X(0))^2> [Ang^2], MSD / t [Ang^2/fs], "
+                   "d MSD / dt [Ang^2/fs]\n", R);
+        for (int w = 0; w < nw; ++w)
+            fprintf(f, "%.16e %.16e %.16e %.16e\n", t[(size_t)w], msd[(size_t)w], dr[(size_t)w], ds[(size_t)w]);
+        fclose(f);
+    }
     for (int w = 0; w < nw; ++w) {
         const int it = (w + 1) * j.nwr;
         double norm = norms[(size_t)w];

@@ -19,7 +19,7 @@ def _time(ctx, u, precision, nsteps, cand):
     grp, st, pf, rpt, bps, unroll, sv, mb = cand
     try:
         ctx.set_tuning(rpt, bps, grp, st, pf)
-        ctx.set_kernel_variant(unroll, sv, mb)
+        ctx.set_kernel_variant(unroll, sv, mb, -1)
         ctx.stage_phases(u, precision)
         ctx.run_staged(nsteps)
         ctx.run_staged(nsteps)
@@ -40,7 +40,7 @@ def apply(ctx, best):
     """Set a tuning dictionary (as returned by autotune) on the context."""
     ctx.set_tuning(best["rhs_per_thread"], best["blocks_per_sm"], best["rows_per_group"], best["staged"],
                    best["prefetch"])
-    ctx.set_kernel_variant(best.get("unroll", 0), best.get("stage_values", -1), best.get("min_blocks", 0))
+    ctx.set_kernel_variant(best.get("unroll", 0), best.get("stage_values", -1), best.get("min_blocks", 0), -1)
 
 
 def autotune(ctx, u, precision, nsteps=12, rhs_per_thread=(1, 2, 4), blocks_per_sm=(0,),

@@ -123,9 +123,12 @@ int         gbn_set_tuning(gbn_ctx* ctx, int32_t rhs_per_thread, int32_t blocks_
  * per batch (4 or 8; 0 = the default), for the staged path whether the staged slice records carry the
  * values (1) or only the column indices, with the values prefetched into L2 and streamed beside the
  * gathers (0; -1 = the default), and the resident blocks per SM the kernel's registers are bounded for
- * (1 or 3, 3 only with unroll 8 on the staged path; 0 = 1).  No counterpart in the reference.  Used by
- * the autotuner (grabnes_b200/tune.py). */
-int         gbn_set_kernel_variant(gbn_ctx* ctx, int32_t col_unroll, int32_t stage_values, int32_t min_blocks);
+ * (1 or 3, 3 only with unroll 8 on the staged path; 0 = 1); for gbn_lanczos_fields, whether each tile's
+ * Peierls rotations are tabulated once before its steps (1) or done on the fly by every thread at every
+ * step (0, -1 = the default).  No counterpart in the reference.  Used by the autotuner
+ * (grabnes_b200/tune.py). */
+int         gbn_set_kernel_variant(gbn_ctx* ctx, int32_t col_unroll, int32_t stage_values, int32_t min_blocks,
+                                   int32_t field_table);
 /* Kernels launched by this context since creation (for launch accounting). */
 int64_t     gbn_launch_count(const gbn_ctx* ctx);
 /* Device time of the recursion loop of the last gbn_lanczos* / gbn_run_staged call and its number of
@@ -303,6 +306,16 @@ int gbn_kubo_evol(gbn_ctx* ctx, int32_t precision, int32_t nrhs, const double* c
 int gbn_kubo_tevol(gbn_ctx* ctx, int32_t precision, int32_t nrhs, const double* c, int32_t npol, double ac,
                    double bc, int32_t dir, int32_t nt, int32_t nwr, int32_t nrecurs, double* psi, double* zupsi,
                    double* norms, double* a, double* b);
+/* Mean-square displacement and diffusivity from the norms of gbn_kubo_tevol (no counterpart in the
+ * reference, which writes only the norms |ZUPsi|^2 of KuboTEvol, kubo.F90:376-385, in its .Z2_ files).
+ * norms [nrhs][nw] as gbn_kubo_tevol returns them, for write steps every nwr time steps of dt_fs
+ * femtoseconds (dt_fs = Kubo.TimeStep * hbar / g0).  Out [nw]: t_fs = (w + 1) nwr dt_fs; msd = the mean
+ * over the vectors of |ZUPsi_r|^2, the spread <(X(t) - X(0))^2> [Ang^2] along the evolution's
+ * direction; d_ratio = msd / t and d_slope = d msd / dt (central differences between write steps, from
+ * msd = 0 at t = 0; one-sided at the last step) [Ang^2 / fs = 0.1 cm^2 / s]; d_ratio, d_slope may be
+ * NULL.  Host arithmetic in FP64 (no device, no context). */
+int gbn_kubo_msd(int32_t nrhs, int32_t nw, int32_t nwr, double dt_fs, const double* norms, double* t_fs,
+                 double* msd, double* d_ratio, double* d_slope);
 /* NeighD(3,maxNeigh,N) for gbn_kubo_evol after gbn_load_hamiltonian. */
 int gbn_set_neighd(gbn_ctx* ctx, const double* neighd);
 

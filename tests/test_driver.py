@@ -171,6 +171,48 @@ def test_driver_time_evolution_against_oracle(tmp_path):
 
 
 @pytest.mark.gpu
+def test_driver_msd_against_oracle(tmp_path):
+    """Kubo.TEvolVectors 3 on disordered graphene: the reference's files from vector 0, and
+    <prefix>.MSD.dat, the spread <(X(t) - X(0))^2> averaged over the three vectors (|ZUPsi_r|^2 of
+    KuboTEvol, kubo.F90:376-385) with its diffusivity, against the oracle's KuboEvol loop of the same
+    vectors (vector r: draws r N .. (r + 1) N - 1 of the seeded stream): 1e-9 relative."""
+    keys = {"Run.Prefix": "msd", "Run.TypeOfSystem": "Graphene", "Structure.CellSize": 50, "TB.Hopping": 2.7,
+            "Disorder.Anderson": True, "Disorder.AndersonAmp": 1.0, "Kubo.RecursionNumber": 60,
+            "Kubo.NumberofEnergyPoints": 100, "Kubo.Epsilon": 0.05, "Kubo.EnergyMin": -8.0,
+            "Kubo.EnergyMax": 8.0, "Kubo.SeedValue": 5, "Kubo.NumberofPolynomials": 40, "Kubo.TimeStep": 2.0,
+            "Kubo.NumberofTimeSteps": 6, "Kubo.WriteNumberofSteps": 2, "Kubo.TEvolVectors": 3}
+    path = str(tmp_path / "Gendata.in")
+    _write(path, keys)
+    subprocess.run([DRIVER, path], check=True, cwd=str(tmp_path), capture_output=True, text=True)
+    r = R.build(dict(TypeOfSystem="Graphene", CellSize=50, Hopping=2.7, Anderson=True, AndersonAmp=1.0, SeedValue=5))
+    n, g0 = r["geo"]["n"], r["g0"]
+    u = orc.rng_draws(5, 3 * n).reshape(3, n)
+    psis = [np.exp(2j * np.pi * u[k]) / np.sqrt(n) for k in range(3)]
+    a, b = orc.recursion(r["nb"], r["hop"], r["h0"], psis[0], 60, 0)
+    ac, bc = orc.interval(a, b)
+    c = orc.cheb_coef(2.0, ac, bc, 40)
+    norms = np.zeros((3, 3))
+    for k in range(3):
+        psi, zu = psis[k], np.zeros(n, np.complex128)
+        for it in range(1, 7):
+            psi, zu = orc.evol(r["nb"], r["hop"], r["h0"], c, ac, bc, psi, zu, 1)
+            if it % 2 == 0:
+                norms[k, it // 2 - 1] = float(np.vdot(zu, zu).real)
+    msd = norms.mean(axis=0)
+    dt_fs = 2.0 * (6.62606896e-34 / (2 * np.pi)) / 1.602176565e-19 / g0 * 1e15
+    t = dt_fs * 2 * np.arange(1, 4)
+    slope = np.array([(msd[1] - 0.0) / (t[1] - 0.0), (msd[2] - msd[0]) / (t[2] - t[0]), (msd[2] - msd[1]) / (t[2] - t[1])])
+    got = np.loadtxt(tmp_path / "msd.MSD.dat")
+    assert got.shape == (3, 4)
+    assert np.abs(got[:, 0] - t).max() <= 1e-12 * t.max()
+    assert np.abs(got[:, 1] - msd).max() <= 1e-9 * msd.max()
+    assert np.abs(got[:, 2] - msd / t).max() <= 1e-9 * (msd / t).max()
+    assert np.abs(got[:, 3] - slope).max() <= 1e-9 * np.abs(slope).max()
+    with open(tmp_path / "msd.AB_0002.dat") as f:   # the reference's file, from vector 0
+        assert abs(float(f.readline()) - norms[0, 0]) <= 1e-9 * norms[0, 0]
+
+
+@pytest.mark.gpu
 def test_driver_layer_pdos_against_oracle(tmp_path):
     """Kubo.PDOSLayer: one folder per layer with the reference's files, from random phases on the layer's
     atoms (Kubo.SeedSet stream), against the oracle's recursion and continued fraction."""

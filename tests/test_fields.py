@@ -1,5 +1,6 @@
-"""Many fields in one batch (gbn_lanczos_fields): the Peierls phase of every entry applied on the fly
-from one field-free matrix, against the oracle's per-field Hamiltonian (HamPeierlsPeriodicGauge for each
+"""Many fields in one batch (gbn_lanczos_fields): the Peierls phase of every entry applied from one
+field-free matrix -- on the fly by every thread (the default), or through a table of each tile's
+rotations built before its steps -- against the oracle's per-field Hamiltonian (HamPeierlsPeriodicGauge for each
 field) and recursion."""
 import numpy as np
 import pytest
@@ -63,19 +64,39 @@ def test_fields_fp64_match_per_field_oracle(ctx, base):
 
 @pytest.mark.parametrize("grp", [1, 2])
 def test_fields_every_matrix_path(ctx, base, grp):
-    """Records staged in shared memory or read in place, rows per group 1 or 2: FP64 recursions of the
-    batched fields agree to 1e-10 of the spectral scale."""
+    """Records staged in shared memory or read in place, rows per group 1 or 2, the rotations from the
+    tile table or on the fly: FP64 recursions of the batched fields agree to 1e-10 of the spectral scale."""
     n = base["geo"]["n"]
     u = _draws(n)
     _field_free(ctx, base)
     out = []
     try:
         for staged in (0, 1):
-            ctx.set_tuning(0, 0, grp, staged)
-            out.append(ctx.lanczos_fields(FIELDS, u, 80, G.GBN_FP64))
+            for table in (1, 0):
+                ctx.set_tuning(0, 0, grp, staged)
+                ctx.set_kernel_variant(0, -1, 0, table)
+                out.append(ctx.lanczos_fields(FIELDS, u, 80, G.GBN_FP64))
     finally:
         ctx.set_tuning()
-    assert _close(out[1][0], out[1][1], out[0][0], out[0][1], 1e-10)
+        ctx.set_kernel_variant()
+    for k in range(1, len(out)):
+        assert _close(out[k][0], out[k][1], out[0][0], out[0][1], 1e-10), k
+
+
+def test_fields_mixed_table_against_on_the_fly(ctx, base):
+    """Mixed precision: the tile table's rotations (FP64 sincospi of the 32-bit turn fraction, rounded once)
+    against the on-the-fly rotation (split-angle FP32, error below 2e-13): a_n, b_n within FP32 rounding."""
+    n = base["geo"]["n"]
+    u = _draws(n)
+    _field_free(ctx, base)
+    try:
+        ctx.set_kernel_variant(0, -1, 0, 1)
+        a1, b1 = ctx.lanczos_fields(FIELDS, u, 100, G.GBN_MIXED)
+        ctx.set_kernel_variant(0, -1, 0, 0)
+        a0, b0 = ctx.lanczos_fields(FIELDS, u, 100, G.GBN_MIXED)
+    finally:
+        ctx.set_kernel_variant()
+    assert _close(a1, b1, a0, b0, 1e-5)
 
 
 def test_fields_mixed_dos(ctx, base):
