@@ -550,8 +550,54 @@ void ck(int rc, gbn_ctx* ctx, const char* what)
     if (rc != GBN_OK) die(std::string(what) + ": " + (ctx ? gbn_last_error(ctx) : "error " + std::to_string(rc)));
 }
 
+// Sweep sharding over processes, one per GPU (grabnes_b200/launch.py starts them): GRABNES_RANK and
+// GRABNES_NRANKS.  Unit u of a sweep -- the u-th (field, Haldane phase) pair in the reference's loop
+// order (calc.F90:82-114), or the u-th field of a batched DOS-only sweep, the same order -- runs on rank
+// u % NRANKS and writes its own folder; a job without a sweep is one unit.  No data crosses ranks.
+struct Shard {
+    int rank = 0, nranks = 1;
+    bool mine(long u) const { return u % nranks == rank; }
+};
+
+Shard shard_from_env()
+{
+    Shard s;
+    const char* r = getenv("GRABNES_RANK");
+    const char* n = getenv("GRABNES_NRANKS");
+    if (n) s.nranks = atoi(n);
+    if (r) s.rank = atoi(r);
+    if (s.nranks < 1 || s.rank < 0 || s.rank >= s.nranks) die("GRABNES_RANK must be in 0 .. GRABNES_NRANKS - 1");
+    return s;
+}
+
+// The (field, phase) units of the sweep in loop order (integer fields, before MagField.*B is resolved).
+std::vector<std::pair<long, long>> sweep_units(const Job& j)
+{
+    std::vector<std::pair<long, long>> u;
+    const bool magfield = !(j.mbi == 0 && j.mbf == 0), hsweep = j.mphii != j.mphif;
+    for (long mb = j.mbi; mb <= j.mbf; mb += (magfield ? j.mstep : 1)) {
+        for (long mphi = j.mphii; mphi <= j.mphif; mphi += j.mphistep) {
+            u.push_back({mb, mphi});
+            if (!magfield && !hsweep) return u;
+        }
+    }
+    return u;
+}
+
 void print_job(const Job& j)
 {
+    {   // the units of this rank (GRABNES_RANK / GRABNES_NRANKS), on a line of their own before the job
+        const Shard sh = shard_from_env();
+        const auto units = sweep_units(j);
+        printf("{\"rank\": %d, \"nranks\": %d, \"units\": [", sh.rank, sh.nranks);
+        bool first = true;
+        for (size_t k = 0; k < units.size(); ++k)
+            if (sh.mine((long)k)) {
+                printf("%s[%ld, %ld]", first ? "" : ", ", units[k].first, units[k].second);
+                first = false;
+            }
+        printf("]}\n");
+    }
     const gbn_model& m = j.model;
     printf("{\"kind\": %d, \"aG\": %.17g, \"cell_size\": %d, \"super_cell\": %d, \"m\": [%d, %d, %d, %d], "
            "\"height\": %.17g, \"d_interlayer\": %.17g, \"g0\": %.17g, \"cut2intra\": %.17g, \"cut2inter\": %.17g, "
@@ -1032,6 +1078,15 @@ int run(const Job& j0)
     const double area = cell_area(ucell.data());
     resolve_fields(j, area);
     printf("grabnes: %lld atoms, cell area %.6f Ang^2, g0 = %.6f eV\n", (long long)n, area, j.g0);
+    const Shard shard = shard_from_env();
+    if (shard.nranks > 1) {
+        const auto units = sweep_units(j);
+        long mine = 0;
+        for (size_t k = 0; k < units.size(); ++k) mine += shard.mine((long)k) ? 1 : 0;
+        printf("grabnes: rank %d of %d, %ld of the %zu units of this job\n", shard.rank, shard.nranks, mine,
+               units.size());
+        if (mine == 0) return 0;
+    }
     gbn_ctx* ctx = nullptr;
     const char* dev = getenv("GRABNES_DEVICE");
     ck(gbn_create(&ctx, dev ? atoi(dev) : 0), nullptr, "gbn_create (no CUDA device?)");
@@ -1066,8 +1121,15 @@ int run(const Job& j0)
         // a DOS-only sweep: all fields in one batch from the field-free Hamiltonian, each field's Peierls
         // phases applied on the fly (the reference reseeds, so every field starts from the same vector)
         std::vector<int32_t> fm;
-        for (long mb = j.mbi; mb <= j.mbf; mb += j.mstep) fm.push_back((int32_t)mb);
+        long unit = 0;
+        for (long mb = j.mbi; mb <= j.mbf; mb += j.mstep)
+            if (shard.mine(unit++)) fm.push_back((int32_t)mb);
         const int nf = (int)fm.size();
+        if (nf == 0) {
+            printf("grabnes: rank %d of %d has no field of this sweep\n", shard.rank, shard.nranks);
+            gbn_destroy(ctx);
+            return 0;
+        }
         std::vector<double> uu((size_t)nf * n), aa((size_t)nf * j.nrecurs), bb((size_t)nf * j.nrecurs);
         for (int f = 0; f < nf; ++f) std::copy(u.begin(), u.end(), uu.begin() + (size_t)f * n);
         ck(gbn_assemble(ctx, &j.model, j.moire ? rat_on.data() : nullptr, j.moire ? rat_hop.data() : nullptr,
@@ -1094,8 +1156,13 @@ int run(const Job& j0)
         return 0;
     }
     const bool hsweep = j.mphii != j.mphif;   // HaldPhaseInit: a Haldane phase sweep
+    long unit = -1;
     for (long mb = j.mbi; mb <= j.mbf; mb += (magfield ? j.mstep : 1))
     for (long mphi = j.mphii; mphi <= j.mphif; mphi += j.mphistep) {
+        if (!shard.mine(++unit)) {   // another rank's unit
+            if (!magfield && !hsweep) break;
+            continue;
+        }
         std::string prefix = j.prefix;
         if (magfield && j.mbi != j.mbf) {
             const double bmag = mb * kFluxQuantum / (area * 1.0e-20);

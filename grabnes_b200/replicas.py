@@ -34,6 +34,12 @@ def init(backend="nccl", timeout_s=300):
     return ws, rank, local
 
 
+def shard_units(n_units, rank, ws):
+    """The units of a sweep that rank runs: unit u on rank u % ws (the drop-in driver's rule for its
+    (field, Haldane phase) units, GRABNES_RANK / GRABNES_NRANKS)."""
+    return [u for u in range(n_units) if u % ws == rank]
+
+
 def seed_of(base, rank):
     """Seed of a rank's random-phase vectors: disjoint streams per rank (the reference seeds by SeedValue)."""
     return base + SEED_STRIDE * rank

@@ -59,9 +59,11 @@ def _write(path, keys, extra=""):
         f.write(extra)
 
 
-def _print_job(path):
-    out = subprocess.run([DRIVER, "--print-job", path], check=True, capture_output=True, text=True).stdout
-    return json.loads(out)
+def _print_job(path, env=None):
+    """The job the driver reads (its last line) and, with env, the sweep units of that rank (its first)."""
+    out = subprocess.run([DRIVER, "--print-job", path], check=True, capture_output=True, text=True,
+                         env=env).stdout.strip().splitlines()
+    return json.loads(out[-1]) if env is None else (json.loads(out[-1]), json.loads(out[0]))
 
 
 pytestmark_cpu = pytest.mark.skipif(not os.path.exists(DRIVER), reason="driver not built")
@@ -89,6 +91,27 @@ def test_driver_reads_input_like_the_package(tmp_path, name):
         assert math.isclose(got["model"][f], getattr(m, f), rel_tol=1e-15, abs_tol=1e-300), f
     assert got["cell_size"] == job["cell"]["cell_size"] and got["super_cell"] == job["cell"]["super_cell"]
     assert tuple(got["m"]) == tuple(job["cell"]["m"])
+
+
+@pytestmark_cpu
+@pytest.mark.parametrize("nranks", [1, 2, 3])
+def test_driver_sweep_shards(tmp_path, nranks):
+    """GRABNES_RANK / GRABNES_NRANKS: every (field, Haldane phase) unit of a sweep runs on exactly one rank,
+    unit u on rank u % NRANKS, in the reference's loop order (fields outer, phases inner)."""
+    from grabnes_b200 import replicas
+    path = str(tmp_path / "Gendata.in")
+    _write(path, {"Run.TypeOfSystem": "Graphene", "Structure.CellSize": 10}, "MagField.InitialInteger 0\n"
+           "MagField.FinalInteger 8\nMagField.IntegerStep 2\nHaldane.NNN .true.\nHaldane.SpecifyRange .true.\n"
+           "HaldPhase.InitialInteger 0\nHaldPhase.FinalInteger 2\n")
+    everything = [[mb, ph] for mb in range(0, 9, 2) for ph in range(0, 3)]
+    got = []
+    for rank in range(nranks):
+        env = dict(os.environ, GRABNES_RANK=str(rank), GRABNES_NRANKS=str(nranks))
+        _, units = _print_job(path, env)
+        assert units["rank"] == rank and units["nranks"] == nranks
+        assert units["units"] == [everything[k] for k in replicas.shard_units(len(everything), rank, nranks)]
+        got += units["units"]
+    assert sorted(got) == sorted(everything)
 
 
 @pytestmark_cpu
@@ -129,6 +152,39 @@ def test_driver_field_sweep_against_oracle(tmp_path):
         assert np.abs(dos[:, 1] - d0).sum() <= 1e-6 * np.abs(d0).sum()   # normalised L1, the DOS bar
         ab = np.loadtxt(tmp_path / folder / "generate.AB", skiprows=1)
         assert np.array_equal(ab[:, 0], a) and np.array_equal(ab[:, 1], b)
+
+
+@pytest.mark.gpu
+def test_launcher_two_ranks_match_one_process(tmp_path):
+    """The three-field sweep through grabnes_b200.launch with two ranks (both on this GPU: each is its own
+    process and CUDA context, and no kernel of one waits on the other) against one driver process: the
+    same folders, a_n and b_n within 1e-10 of their scale and the DOS within 1e-6 (normalised L1) -- the
+    ranks batch different sets of fields, so their tiles differ."""
+    import sys
+    keys = dict(INPUTS["moire_sweep"])
+    sweep = "MagField.InitialInteger 0\nMagField.FinalInteger 4\nMagField.IntegerStep 2\n"
+    one, two = tmp_path / "one", tmp_path / "two"
+    one.mkdir()
+    two.mkdir()
+    for d in (one, two):
+        _write(str(d / "Gendata.in"), keys, sweep)
+    subprocess.run([DRIVER, "Gendata.in"], check=True, cwd=str(one), capture_output=True, text=True)
+    env = dict(os.environ, PYTHONPATH=os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    p = subprocess.run([sys.executable, "-m", "grabnes_b200.launch", "--gpus", "2", "Gendata.in"], cwd=str(two),
+                       env=env, capture_output=True, text=True, timeout=600)
+    assert p.returncode == 0, p.stdout + p.stderr
+    f1 = sorted(d for d in os.listdir(one) if d.startswith("m0"))
+    f2 = sorted(d for d in os.listdir(two) if d.startswith("m0"))
+    assert f1 == f2 and len(f1) == 3
+    for folder in f1:
+        for name in ("generate.a0.dat", "generate.b0.dat"):
+            x, y = np.loadtxt(one / folder / name), np.loadtxt(two / folder / name)
+            assert np.abs(x - y).max() <= 1e-10 * np.abs(x).max()
+        d1, d2 = np.loadtxt(one / folder / "generate.DOS"), np.loadtxt(two / folder / "generate.DOS")
+        assert np.array_equal(d1[:, 0], d2[:, 0])
+        assert np.abs(d1[:, 1] - d2[:, 1]).sum() <= 1e-6 * np.abs(d1[:, 1]).sum()
+    logs = [(two / f"grabnes.rank{r}.log").read_text() for r in range(2)]
+    assert "rank 0 of 2" in logs[0] and "rank 1 of 2" in logs[1]
 
 
 @pytest.mark.gpu

@@ -79,3 +79,60 @@ def test_seeds_are_disjoint_per_rank():
     from grabnes_b200 import replicas
     seeds = {replicas.seed_of(SEED, k) for k in range(8)}
     assert len(seeds) == 8
+
+
+# ---------------------------------------------------------------------------- sharded driver sweeps
+FAKE_DRIVER = """#!{python}
+# Stands in for the driver on a machine without a GPU: the real driver's --print-job gives this rank's
+# units (GRABNES_RANK / GRABNES_NRANKS, its sharding rule), and every unit writes its own folder.
+import json, os, subprocess, sys
+out = subprocess.run([{real!r}, "--print-job", sys.argv[1]], capture_output=True, text=True, check=True)
+units = json.loads(out.stdout.splitlines()[0])["units"]
+for mb, ph in units:
+    d = "m%05d_p%d" % (mb, ph)
+    os.makedirs(d, exist_ok=True)
+    with open(os.path.join(d, "unit.txt"), "w") as f:
+        f.write("%d %d\\n" % (mb, ph))
+"""
+
+
+def _launch(workdir, ws, driver):
+    import subprocess
+    import sys
+    with open(os.path.join(workdir, "Gendata.in"), "w") as f:
+        f.write("Run.TypeOfSystem Graphene\nStructure.CellSize 10\nMagField.InitialInteger 0\n"
+                "MagField.FinalInteger 12\nMagField.IntegerStep 2\n")
+    env = dict(os.environ, PYTHONPATH=ROOT)
+    return subprocess.run([sys.executable, "-m", "grabnes_b200.launch", "--gpus", str(ws), "--driver", driver,
+                           "Gendata.in"], cwd=workdir, env=env, capture_output=True, text=True, timeout=300)
+
+
+def test_launcher_splits_a_sweep_over_two_gloo_ranks(tmp_path):
+    """grabnes_b200.launch with two ranks (gloo on CPU): every field of a 7-field sweep is run by exactly
+    one rank (the driver's own sharding rule, read from its --print-job), the folders of the two ranks
+    together are those of a single-rank run, and rank 0 records both ranks' exit status."""
+    import json
+    real = os.path.join(ROOT, "grabnes_b200", "grabnes")
+    if not os.path.exists(real):
+        pytest.skip("driver not built")
+    import sys
+    fake = tmp_path / "fake_driver.py"
+    fake.write_text(FAKE_DRIVER.format(python=sys.executable, real=real))
+    fake.chmod(0o755)
+    runs = {}
+    for ws in (1, 2):
+        wd = tmp_path / f"ws{ws}"
+        wd.mkdir()
+        p = _launch(str(wd), ws, str(fake))
+        assert p.returncode == 0, p.stdout + p.stderr
+        runs[ws] = {d: (wd / d / "unit.txt").read_text() for d in sorted(os.listdir(wd)) if d.startswith("m0")}
+        st = json.loads((wd / "grabnes.shards.json").read_text())
+        assert st["ranks"] == ws and [s["rc"] for s in st["statuses"]] == [0] * ws
+    assert len(runs[1]) == 7 and runs[2] == runs[1]
+
+
+def test_shard_units_cover_each_unit_once():
+    from grabnes_b200 import replicas
+    for ws in (1, 2, 3, 5):
+        got = sorted(u for r in range(ws) for u in replicas.shard_units(11, r, ws))
+        assert got == list(range(11))
