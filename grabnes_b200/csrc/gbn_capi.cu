@@ -211,7 +211,7 @@ int gbn_set_kernel_variant(gbn_ctx* c, int32_t col_unroll, int32_t stage_values,
 {
     if (!c) return GBN_ERR_ARG;
     if ((col_unroll != 0 && col_unroll != 4 && col_unroll != 8) || stage_values < -1 || stage_values > 1 ||
-        (min_blocks != 0 && min_blocks != 1 && min_blocks != 3) || field_table < -1 || field_table > 1)
+        (min_blocks < 0 || min_blocks > 3) || field_table < -1 || field_table > 1)
         return fail(c, GBN_ERR_ARG, "kernel variant out of range");
     c->tune_unroll = col_unroll;
     c->tune_stage_values = stage_values;

@@ -51,7 +51,7 @@ StepFn field_table_kernel(int prec, int G, int rpt, int tpr, bool staged);
 struct StepVariant {
     int unroll = 4;
     bool stage_values = true;
-    int min_blocks = 1;   // staged, unroll 8: registers bounded for 3 resident blocks of 256 threads per SM
+    int min_blocks = 1;   // staged, unroll 8: registers bounded for 2 (whole records) or 3 resident blocks per SM
 };
 // the product kernel of the real or complex layout (gbn_step_mixed.cu, gbn_step_fp64.cu)
 StepFn step_kernel_mixed(bool cplx, int G, int rpt, int tpr, bool staged, StepVariant v);
@@ -508,6 +508,7 @@ StepFn step_variant(bool staged, StepVariant v)
         if (v.unroll == 8 && v.min_blocks == 3)
             return v.stage_values ? k_spmm_staged<VT, CPLX, G, RP, TP, false, 8, true, 3>
                                   : k_spmm_staged<VT, CPLX, G, RP, TP, false, 8, false, 3>;
+        if (v.unroll == 8 && v.min_blocks == 2 && v.stage_values) return k_spmm_staged<VT, CPLX, G, RP, TP, false, 8, true, 2>;
         if (v.min_blocks != 1) return nullptr;
         if (v.unroll == 8)
             return v.stage_values ? k_spmm_staged<VT, CPLX, G, RP, TP, false, 8, true>

@@ -8,7 +8,8 @@ flight together (4 or 8), a prefetch (staged path only) of the gather rows of ea
 its epilogue reads, or of those and the rows of u_k one or more sweeps ahead, and a cap on resident
 blocks per SM.  The search runs in two stages on the caller's own Hamiltonian and start vectors:
 the layout and path (rows per group, right-hand sides per thread, staged or not) at the default
-variant, then the variant (unroll, prefetch) of the best layout.  Each candidate runs a short
+variant, then, for the best layout of each rows-per-group value, the variant (unroll, prefetch, staged
+values or indices, the register bound for 1, 2 or 3 blocks per SM).  Each candidate runs a short
 recursion; the one with the smallest device time per step (update + sparse product, CUDA events) is
 kept on the context.
 """
@@ -44,25 +45,34 @@ def apply(ctx, best):
 
 
 def autotune(ctx, u, precision, nsteps=12, rhs_per_thread=(1, 2, 4), blocks_per_sm=(0,),
-             rows_per_group=(1, 2, 4), staged=(0, 1), prefetch=(0, 4, 6, 7), unroll=(4, 8)):
+             rows_per_group=(1, 2, 4), staged=(0, 1), prefetch=(0, 4, 6), unroll=(4, 8)):
     results = []
     # stage 1: layout and matrix path at the library's default variant (-1/0: chosen by the library)
     for grp, st, rpt, bps in itertools.product(rows_per_group, staged, rhs_per_thread, blocks_per_sm):
         results.append(_time(ctx, u, precision, nsteps, (grp, st, -1, rpt, bps, 0, -1, 0)))
     ok = [r for r in results if "step_ms" in r]
-    best = min(ok, key=lambda r: r["step_ms"])
-    # stage 2: unroll, prefetch, staged values or indices only, and the register bound of the best layout
+    # stage 2: for the best layout of every rows-per-group value, the unroll, prefetch, staged values or
+    # indices only, and the register bound (1, 2 or 3 blocks per SM): the best variant differs between
+    # layouts, so the layouts' defaults do not rank them
     seen = {_key(r) for r in results}
-    pfs = prefetch if best["staged"] == 1 else (0,)
-    svs = (1, 0) if best["staged"] == 1 else (1,)
-    for pf, un, sv, mb in itertools.product(pfs, unroll, svs, (1, 3)):
-        if mb == 3 and (un != 8 or best["staged"] != 1):
+    for grp in rows_per_group:
+        mine = [r for r in ok if r["rows_per_group"] == grp]
+        if not mine:
             continue
-        cand = (best["rows_per_group"], best["staged"], pf, best["rhs_per_thread"], best["blocks_per_sm"], un, sv, mb)
-        if cand in seen:
-            continue
-        seen.add(cand)
-        results.append(_time(ctx, u, precision, nsteps, cand))
+        lay = min(mine, key=lambda r: r["step_ms"])
+        pfs = prefetch if lay["staged"] == 1 else (0,)
+        for pf, un, sv, mb in itertools.product(pfs, unroll, (1, 0), (1, 2, 3)):
+            if lay["staged"] != 1 and (sv == 0 or mb != 1):
+                continue
+            if mb > 1 and un != 8:
+                continue
+            if mb == 2 and sv == 0:
+                continue
+            cand = (grp, lay["staged"], pf, lay["rhs_per_thread"], lay["blocks_per_sm"], un, sv, mb)
+            if cand in seen:
+                continue
+            seen.add(cand)
+            results.append(_time(ctx, u, precision, nsteps, cand))
     ok = [r for r in results if "step_ms" in r]
     best = min(ok, key=lambda r: r["step_ms"])
     apply(ctx, best)

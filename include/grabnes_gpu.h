@@ -123,7 +123,7 @@ int         gbn_set_tuning(gbn_ctx* ctx, int32_t rhs_per_thread, int32_t blocks_
  * per batch (4 or 8; 0 = the default), for the staged path whether the staged slice records carry the
  * values (1) or only the column indices, with the values prefetched into L2 and streamed beside the
  * gathers (0; -1 = the default), and the resident blocks per SM the kernel's registers are bounded for
- * (1 or 3, 3 only with unroll 8 on the staged path; 0 = 1); for gbn_lanczos_fields, whether each tile's
+ * (1, 2 or 3; 2 and 3 only with unroll 8 on the staged path, 2 only with whole records staged; 0 = 1); for gbn_lanczos_fields, whether each tile's
  * Peierls rotations are tabulated once before its steps (1) or done on the fly by every thread at every
  * step (0, -1 = the default).  No counterpart in the reference.  Used by the autotuner
  * (grabnes_b200/tune.py). */
