@@ -74,6 +74,14 @@ struct Ell {
     int ftab_slots = 0;
     int ftab_entry_bytes = 0;   // 4 + slots * G * complex bytes
     bool ftab_valid = false;
+    // Tiles of consecutive slices for the tile-local product: tile t holds slices
+    // [tile_slice[t], tile_slice[t+1]) and gathers only the rows halo[halo_ptr[t] .. halo_ptr[t+1]) (at most
+    // tile_hmax, in order of first use); tmat is mat with every column index replaced by its position in
+    // the tile's halo list, so that a tile's gathers read a copy of those rows in shared memory.
+    DevBuf tile_slice, halo_ptr, halo, tmat;
+    int64_t ntiles = 0;
+    int tile_hmax = 0;
+    bool tiles_valid = false;
     bool valid = false;
 };
 
@@ -154,6 +162,7 @@ struct gbn_ctx {
     int tune_unroll = 0;         // union columns in flight per batch of the product (4, 8; 0 = automatic)
     int tune_stage_values = -1;  // staged records carry the values (1) or only the column indices (0); -1 auto
     int tune_min_blocks = 0;     // product kernel compiled for 1 or 3 resident blocks per SM (0 = 1)
+    int tune_tiled = -1;         // tile-local product (halo rows in shared memory): 1 yes, 0 no, -1 default (no)
     int tune_field_table = -1;   // batched fields: rotations tabulated per tile (1) or on the fly (0, -1 default)
     bool last_staged = false;    // the last recursion used the staged kernel
 
@@ -192,6 +201,8 @@ int build_ell(gbn_ctx* c, int prec, int G, int gpw, bool field = false);
 int auto_group(const gbn_ctx* c, int R);   // default rows per group for a tile of R vectors
 // the tile table of the field-batched layout for the flux quanta of each thread slot (d_slot_m [slots])
 int build_field_table(gbn_ctx* c, int slots, const int32_t* d_slot_m);
+// tiles of the layout whose halos have at most hmax rows (host pass over the records)
+int build_tiles(gbn_ctx* c, int hmax);
 
 // recursion (gbn_lanczos.cu)
 int lanczos_prepare(gbn_ctx* c, int prec, int nrhs, bool field = false);

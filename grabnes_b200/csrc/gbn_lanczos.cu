@@ -243,11 +243,67 @@ struct StepLaunch {
     bool staged = false;
     const unsigned char* mat = nullptr;   // the records the kernel reads (the layout's, or its tile table)
     int64_t entry_bytes = 0;
+    bool tiled = false;                   // the tile-local product (halo rows in shared memory)
+    int32_t pitch = 0, halo_off = 0;
 };
 
 constexpr size_t kStagedSmemBudget = 200 * 1024;
 // blocks per SM of the streaming update kernel
 constexpr int kUpdateBlocksPerSM = 8;
+
+// The tile-local product (k_spmm_tiled), mixed precision and real values: 8 warps, two staging buffers
+// per warp of the largest record percentile that leaves a halo buffer of at least 256 rows, with the
+// blocks the registers allow (at most 2) per SM; the tiles are rebuilt when their halo limit changes.
+// Returns false (and leaves L untouched) when the shape has no such kernel or nothing fits.
+static int tiled_launch(gbn_ctx* c, int R, StepLaunch* L, bool* done)
+{
+    *done = false;
+    Ell& E = c->ell;
+    if (E.field || E.cplx || c->prec != GBN_MIXED) return GBN_OK;
+    int rpt, tpr;
+    split_rhs(c->prec, R, c->tune_rpt, &rpt, &tpr);
+    StepFn fn = tiled_kernel_mixed(E.G, rpt, tpr, c->tune_min_blocks == 2 ? 2 : 1);
+    if (!fn) return GBN_OK;
+    int smem_sm = 0, resv = 0, optin = 0, reg_blocks = 0;
+    GBN_CK(c, cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, c->device));
+    GBN_CK(c, cudaDeviceGetAttribute(&resv, cudaDevAttrReservedSharedMemoryPerBlock, c->device));
+    GBN_CK(c, cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device));
+    cudaFuncAttributes fa;
+    GBN_CK(c, cudaFuncGetAttributes(&fa, fn));
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&reg_blocks, fn, 256, 0) != cudaSuccess || reg_blocks < 1)
+        reg_blocks = 1;
+    const int target = reg_blocks < 2 ? reg_blocks : 2;
+    int64_t budget = (int64_t)smem_sm / target - (int64_t)fa.sharedSizeBytes - resv;
+    if (budget > optin - (int64_t)fa.sharedSizeBytes) budget = optin - (int64_t)fa.sharedSizeBytes;
+    const int pitch = R * (int)sizeof(float2) + 16;
+    constexpr int kMinHalo = 256;
+    for (int i = 0; i < 4; ++i) {
+        const int64_t cap = E.cap_pct[i];
+        if (cap <= 0) continue;
+        const int64_t stage = 128 + 8 * 2 * cap;
+        const int64_t hmax = (budget - stage) / pitch;
+        if (hmax < kMinHalo) continue;
+        const int hm = (int)std::min<int64_t>(hmax, 4096);
+        if (!E.tiles_valid || E.tile_hmax != hm) {
+            const int rc = build_tiles(c, hm);
+            if (rc) return rc;
+        }
+        L->fn = fn;
+        L->tiled = true;
+        L->staged = true;
+        L->cap = cap;
+        L->pitch = pitch;
+        L->halo_off = (int32_t)stage;
+        L->block = 256;
+        L->smem = (size_t)stage + (size_t)hm * pitch;
+        L->mat = E.tmat.as<unsigned char>();
+        L->entry_bytes = E.entry_bytes;
+        GBN_CK(c, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L->smem));
+        *done = true;
+        return GBN_OK;
+    }
+    return GBN_OK;
+}
 
 static int step_launch(gbn_ctx* c, int R, StepLaunch* L)
 {
@@ -334,6 +390,11 @@ static int step_launch(gbn_ctx* c, int R, StepLaunch* L)
     if (want_staged && !L->staged) {   // no buffer fits: the plain kernel
         L->fn = pick(false);
         if (!L->fn) return fail(c, GBN_ERR_ARG, "no recursion kernel for this tile width and kernel variant");
+    }
+    if (c->tune_tiled == 1) {   // the tile-local product where the shape has one
+        bool done = false;
+        const int rc = tiled_launch(c, R, L, &done);
+        if (rc) return rc;
     }
     int per_sm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, L->fn, L->block, L->smem) != cudaSuccess || per_sm < 1)
@@ -524,6 +585,14 @@ int lanczos_run(gbn_ctx* c, int32_t nmax)
     p.nslices = c->ell.nslices;
     p.nmax = nmax;
     p.field_m = c->field_m.as<int32_t>();
+    if (L.tiled) {
+        p.tile_slice = c->ell.tile_slice.as<int64_t>();
+        p.halo_ptr = c->ell.halo_ptr.as<int64_t>();
+        p.halo = c->ell.halo.as<int32_t>();
+        p.ntiles = c->ell.ntiles;
+        p.pitch = L.pitch;
+        p.halo_off = L.halo_off;
+    }
     const int64_t total = c->ell.npad * R;
     const int ublk = 256;   // a multiple of R (k_update keeps one right-hand side per thread)
     // at least 8 elements per thread, at most kUpdateBlocksPerSM blocks per SM

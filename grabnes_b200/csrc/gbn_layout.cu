@@ -378,6 +378,77 @@ int build_field_table(gbn_ctx* c, int slots, const int32_t* d_slot_m)
     return GBN_OK;
 }
 
+// ---------------------------------------------------------------------------- tiles
+// Greedy tiling of the slices in row order: a tile takes slices while the distinct rows its records gather
+// (padding columns included) stay within hmax; a slice that alone exceeds hmax makes the layout untileable
+// at that hmax.  The halo rows are numbered in order of first use and every column index of the tile's
+// records is replaced by that number (tmat).  Host work O(entries), once per layout and hmax.
+int build_tiles(gbn_ctx* c, int hmax)
+{
+    Ell& E = c->ell;
+    if (!E.valid || E.field) return fail(c, GBN_ERR_STATE, "internal: tiles need a valid layout without fields");
+    if (hmax < 1) return fail(c, GBN_ERR_ARG, "internal: tile halo limit must be positive");
+    const int64_t ns = E.nslices, eb = E.entry_bytes;
+    std::vector<int64_t> sp((size_t)ns + 1);
+    GBN_CK(c, cudaMemcpyAsync(sp.data(), E.slice_ptr.p, sizeof(int64_t) * sp.size(), cudaMemcpyDeviceToHost, c->stream));
+    const size_t mbytes = (size_t)(E.nnz_stored * eb);
+    std::vector<unsigned char> m(mbytes ? mbytes : 1);
+    if (mbytes) GBN_CK(c, cudaMemcpyAsync(m.data(), E.mat.p, mbytes, cudaMemcpyDeviceToHost, c->stream));
+    GBN_CK(c, cudaStreamSynchronize(c->stream));
+    std::vector<int32_t> stamp((size_t)E.npad, -1), seen((size_t)E.npad, -1), local((size_t)E.npad, 0);
+    std::vector<int64_t> tslice{0}, hptr{0};
+    std::vector<int32_t> halo;
+    int32_t t = 0, h = 0;
+    for (int64_t s = 0; s < ns; ++s) {
+        int32_t* col = reinterpret_cast<int32_t*>(m.data() + sp[(size_t)s] * eb);
+        const int64_t nent = sp[(size_t)s + 1] - sp[(size_t)s];
+        int32_t fresh = 0, distinct = 0;   // rows of this slice not yet in the tile's halo; all its rows
+        for (int64_t k = 0; k < nent; ++k) {
+            const int32_t cc = col[k];
+            if (seen[(size_t)cc] != (int32_t)s) {
+                seen[(size_t)cc] = (int32_t)s;
+                ++distinct;
+                if (stamp[(size_t)cc] != t) ++fresh;
+            }
+        }
+        if (distinct > hmax) return fail(c, GBN_ERR_ARG, "internal: a slice gathers more rows than a tile holds");
+        if (h + fresh > hmax) {   // close the tile before this slice
+            tslice.push_back(s);
+            hptr.push_back((int64_t)halo.size());
+            ++t;
+            h = 0;
+        }
+        for (int64_t k = 0; k < nent; ++k) {
+            const int32_t cc = col[k];
+            if (stamp[(size_t)cc] != t) {
+                stamp[(size_t)cc] = t;
+                local[(size_t)cc] = h++;
+                halo.push_back(cc);
+            }
+            col[k] = local[(size_t)cc];
+        }
+    }
+    tslice.push_back(ns);
+    hptr.push_back((int64_t)halo.size());
+    E.ntiles = (int64_t)tslice.size() - 1;
+    GBN_CK(c, E.tile_slice.ensure(sizeof(int64_t) * tslice.size()));
+    GBN_CK(c, E.halo_ptr.ensure(sizeof(int64_t) * hptr.size()));
+    GBN_CK(c, E.halo.ensure(sizeof(int32_t) * (halo.size() ? halo.size() : 1)));
+    GBN_CK(c, E.tmat.ensure(m.size()));
+    GBN_CK(c, cudaMemcpyAsync(E.tile_slice.p, tslice.data(), sizeof(int64_t) * tslice.size(), cudaMemcpyHostToDevice,
+                              c->stream));
+    GBN_CK(c, cudaMemcpyAsync(E.halo_ptr.p, hptr.data(), sizeof(int64_t) * hptr.size(), cudaMemcpyHostToDevice,
+                              c->stream));
+    if (!halo.empty())
+        GBN_CK(c, cudaMemcpyAsync(E.halo.p, halo.data(), sizeof(int32_t) * halo.size(), cudaMemcpyHostToDevice,
+                                  c->stream));
+    GBN_CK(c, cudaMemcpyAsync(E.tmat.p, m.data(), m.size(), cudaMemcpyHostToDevice, c->stream));
+    GBN_CK(c, cudaStreamSynchronize(c->stream));   // the host buffers go out of scope
+    E.tile_hmax = hmax;
+    E.tiles_valid = true;
+    return GBN_OK;
+}
+
 int build_ell(gbn_ctx* c, int prec, int G, int gpw, bool field)
 {
     if (!c->have_ham) return fail(c, GBN_ERR_STATE, "no Hamiltonian loaded");
@@ -389,6 +460,7 @@ int build_ell(gbn_ctx* c, int prec, int G, int gpw, bool field)
     Ell& E = c->ell;
     E.valid = false;
     E.ftab_valid = false;
+    E.tiles_valid = false;
     E.dval_dir = 0;
     E.G = G;
     E.gpw = gpw;

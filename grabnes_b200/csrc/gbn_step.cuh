@@ -37,6 +37,13 @@ struct StepParams {
     int64_t nslices;
     int32_t nmax;
     const int32_t* field_m;  // field-batched layout: flux quanta of each right-hand side [R] (else unused)
+    // tile-local product (k_spmm_tiled): tiles of slices, their halo rows, the halo buffer in shared memory
+    const int64_t* tile_slice;  // [ntiles + 1]
+    const int64_t* halo_ptr;    // [ntiles + 1]
+    const int32_t* halo;        // rows of u_k each tile gathers
+    int64_t ntiles;
+    int32_t pitch;              // bytes per halo row in shared memory (the row, padded by 16 bytes)
+    int32_t halo_off;           // byte offset of the halo buffer in dynamic shared memory
 };
 
 using StepFn = void (*)(StepParams);
@@ -56,6 +63,8 @@ struct StepVariant {
 // the product kernel of the real or complex layout (gbn_step_mixed.cu, gbn_step_fp64.cu)
 StepFn step_kernel_mixed(bool cplx, int G, int rpt, int tpr, bool staged, StepVariant v);
 StepFn step_kernel_fp64(bool cplx, int G, int rpt, int tpr, bool staged, StepVariant v);
+// the tile-local product (mixed precision, real values; gbn_step_mixed.cu), nullptr for other shapes
+StepFn tiled_kernel_mixed(int G, int rpt, int tpr, int min_blocks);
 
 // Compensated summation (Neumaier's variant of Kahan's) for the block and grid reductions of the dot
 // products: the running error term recovers the low-order bits that each addition loses.
@@ -492,6 +501,247 @@ __global__ void __launch_bounds__(256, MINB) k_spmm_staged(StepParams p)
         __syncwarp();
     }
     reduce_and_finalize<RPT, TPR>(p, acc_s);
+}
+
+// ---------------------------------------------------------------------------- tile-local product
+// A vector row (RPT right-hand sides of one thread) from the halo buffer in shared memory.
+template <typename VT, int RPT> struct SmemRow;
+template <> struct SmemRow<float, 4> {
+    static __device__ __forceinline__ void load(const unsigned char* p, float2 o[4]) {
+        const float4 a = *reinterpret_cast<const float4*>(p), b = *reinterpret_cast<const float4*>(p + 16);
+        o[0] = make_float2(a.x, a.y); o[1] = make_float2(a.z, a.w); o[2] = make_float2(b.x, b.y); o[3] = make_float2(b.z, b.w);
+    }
+};
+template <> struct SmemRow<float, 2> {
+    static __device__ __forceinline__ void load(const unsigned char* p, float2 o[2]) {
+        const float4 a = *reinterpret_cast<const float4*>(p);
+        o[0] = make_float2(a.x, a.y); o[1] = make_float2(a.z, a.w);
+    }
+};
+template <> struct SmemRow<float, 1> {
+    static __device__ __forceinline__ void load(const unsigned char* p, float2 o[1]) { o[0] = *reinterpret_cast<const float2*>(p); }
+};
+
+// One batch of NB union columns of the tile-local product: the indices (tile-local) and values from the
+// staged record (SMEM) or the record in global memory, the rows from the halo buffer.
+template <typename VT, int G, int RPT, int TPR, bool SMEM, int NB>
+__device__ __forceinline__ void tile_batch(const unsigned char* __restrict__ xs, int pitch,
+                                           const int32_t* __restrict__ cp, const VT* __restrict__ vp,
+                                           typename V2<VT>::t (&acc)[G][RPT])
+{
+    using C2 = typename V2<VT>::t;
+    constexpr int GPW = 32 / TPR;
+    int32_t c[NB];
+    VT h[NB][G];
+    C2 xg[NB][RPT];
+#pragma unroll
+    for (int u = 0; u < NB; ++u) {
+        if constexpr (SMEM) c[u] = cp[u * GPW];
+        else c[u] = __ldcs(cp + u * GPW);
+    }
+#pragma unroll
+    for (int u = 0; u < NB; ++u) SmemRow<VT, RPT>::load(xs + (size_t)(uint32_t)c[u] * pitch, xg[u]);
+#pragma unroll
+    for (int u = 0; u < NB; ++u) load_group_vals<VT, G, SMEM>(vp + u * GPW * G, h[u]);
+#pragma unroll
+    for (int u = 0; u < NB; ++u)
+#pragma unroll
+        for (int g = 0; g < G; ++g)
+#pragma unroll
+            for (int t = 0; t < RPT; ++t) Hop<VT, false>::madd(acc[g][t], h[u][g], xg[u][t]);
+}
+
+// One slice of the tile-local product: the union-column loop over the halo buffer, then the same FP64
+// epilogue as group_slice (own rows of u_k and u_{k-1} from global memory).
+template <typename VT, int G, int RPT, int TPR, bool SMEM, int U>
+__device__ __forceinline__ void tile_slice_step(const StepParams& p, int64_t s, int w, const unsigned char* xbuf,
+                                           const int32_t* __restrict__ cp, const VT* __restrict__ vp,
+                                           const double (&sc)[2][RPT * TPR], double* acc_s)
+{
+    using C2 = typename V2<VT>::t;
+    constexpr int GPW = 32 / TPR;
+    constexpr int R = RPT * TPR;
+    const int lane = threadIdx.x & 31;
+    const int sub = lane / TPR;
+    const int q = lane % TPR;
+    const C2* __restrict__ xc = static_cast<const C2*>(p.x_cur);
+    const C2* __restrict__ xp = static_cast<const C2*>(p.x_prev);
+    C2* __restrict__ vout = static_cast<C2*>(p.v_out);
+    const VT* __restrict__ h0 = static_cast<const VT*>(p.h0);
+    const int64_t row0 = (s * GPW + sub) * G;
+    const unsigned char* xs = xbuf + q * RPT * (int)sizeof(C2);
+    C2 acc[G][RPT];
+#pragma unroll
+    for (int g = 0; g < G; ++g)
+#pragma unroll
+        for (int t = 0; t < RPT; ++t) { acc[g][t].x = 0; acc[g][t].y = 0; }
+    int k = 0;
+    for (; k + U <= w; k += U) {
+        tile_batch<VT, G, RPT, TPR, SMEM, U>(xs, p.pitch, cp, vp, acc);
+        cp += U * GPW;
+        vp += U * GPW * G;
+    }
+    if constexpr (U > kColUnroll) {
+        for (; k < w; k += kColUnroll) {
+            tile_batch<VT, G, RPT, TPR, SMEM, kColUnroll>(xs, p.pitch, cp, vp, acc);
+            cp += kColUnroll * GPW;
+            vp += kColUnroll * GPW * G;
+        }
+    }
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+        C2 xo[RPT], xm[RPT], vn[RPT];
+        VecIO<VT, RPT>::load(xc + (row0 + g) * R + q * RPT, xo);
+        VecIO<VT, RPT>::load(xp + (row0 + g) * R + q * RPT, xm);
+        const VT d = h0[row0 + g];
+#pragma unroll
+        for (int t = 0; t < RPT; ++t) {
+            acc[g][t].x = fma(d, xo[t].x, acc[g][t].x);
+            acc[g][t].y = fma(d, xo[t].y, acc[g][t].y);
+            const double ib = sc[0][q * RPT + t], rb = sc[1][q * RPT + t];
+            const double yr = acc[g][t].x, yi = acc[g][t].y;
+            vn[t].x = (VT)(yr * ib - rb * (double)xm[t].x);
+            vn[t].y = (VT)(yi * ib - rb * (double)xm[t].y);
+            acc_s[t] += (double)xo[t].x * yr + (double)xo[t].y * yi;
+        }
+        VecIO<VT, RPT>::store(vout + (row0 + g) * R + q * RPT, vn);
+    }
+}
+
+__device__ __forceinline__ void cp_async16(void* dst, const void* src)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+
+// The tile-local product.  Every block owns a contiguous range of tiles.  Per tile: the warps' first two
+// slice records are copied into their staging buffers (bulk copies, as in k_spmm_staged), the block copies
+// the tile's halo rows of u_k into shared memory (cp.async, 16 bytes per thread and request, rows padded
+// to `pitch` so that the rows of one gather batch spread over the banks), and the warps then run the
+// tile's slices with every gather read from shared memory: a gather batch waits a shared-memory latency
+// instead of the slowest of its rows' L1 misses.  Waits are bounded as in k_spmm_staged; a warp that gives
+// up marks the block, which stops at the next tile boundary (every thread still reaches every barrier).
+// Measured slower than k_spmm_staged on both bench cells (4.47M-atom twisted bilayer: 1.60 against 1.19 ms;
+// 3.5M-atom graphene/hBN: 0.58 against 0.30 ms): a halo that fits beside the staging buffers holds tiles
+// of a few hundred rows, so each warp runs two or three slices between the block's barriers and the fill
+// of every tile stalls the block.  It is an opt-in variant (gbn_set_kernel_variant), not a default.
+template <typename VT, int G, int RPT, int TPR, int U, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_spmm_tiled(StepParams p)
+{
+    using C2 = typename V2<VT>::t;
+    constexpr int GPW = 32 / TPR;
+    constexpr int R = RPT * TPR;
+    constexpr int ROWB = R * (int)sizeof(C2);
+    constexpr int CH = ROWB / 16;
+    static_assert(ROWB % 16 == 0, "halo rows are copied in 16-byte pieces");
+    extern __shared__ __align__(128) unsigned char dyn[];
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    const int sub = lane / TPR;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(dyn) + 2 * wib;
+    const int64_t cap = p.cap_record;
+    unsigned char* buf = dyn + 128 + (size_t)wib * 2 * cap;
+    unsigned char* xbuf = dyn + p.halo_off;
+    __shared__ double sc[2][R];
+    __shared__ int bad;
+    if (threadIdx.x == 0) bad = 0;
+    load_step_scalars<R>(p, sc);   // synchronises the block
+    double acc_s[RPT];
+#pragma unroll
+    for (int t = 0; t < RPT; ++t) acc_s[t] = 0.0;
+    const int nwb = (int)(blockDim.x >> 5);
+    const int64_t per = (p.ntiles + gridDim.x - 1) / gridDim.x;
+    const int64_t t0 = (int64_t)blockIdx.x * per;
+    const int64_t t1 = (t0 + per < p.ntiles) ? t0 + per : p.ntiles;
+    const int64_t eb = p.entry_bytes;
+    const unsigned char* x = static_cast<const unsigned char*>(p.x_cur);
+
+    auto copy_bytes = [&](int64_t s) { return (p.slice_ptr[s + 1] - p.slice_ptr[s]) * eb; };
+    auto issue = [&](int64_t s, int st) {   // lane 0 only; records above the cap are read in place
+        const int64_t bytes = copy_bytes(s);
+        const unsigned char* src = p.mat + p.slice_ptr[s] * eb;
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        const bool copy = bytes > 0 && bytes <= cap;
+        mbar_expect_tx(&bar[st], copy ? (uint32_t)bytes : 0u);
+        if (copy) bulk_g2s(buf + st * cap, src, (uint32_t)bytes, &bar[st]);
+        else if (bytes > 0) bulk_prefetch_l2(src, (uint32_t)bytes);
+    };
+    if (lane == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncwarp();
+    uint32_t phase = 0u, pending = 0u;
+    for (int64_t t = t0; t < t1; ++t) {
+        const int64_t sb = p.tile_slice[t], se = p.tile_slice[t + 1];
+        int64_t s = sb + wib;
+        if (!bad) {
+            pending = (s < se ? 1u : 0u) | (s + nwb < se ? 2u : 0u);
+            if (lane == 0) {
+                if (pending & 1u) issue(s, 0);
+                if (pending & 2u) issue(s + nwb, 1);
+            }
+        }
+        // the tile's halo rows into shared memory
+        const int64_t hb = p.halo_ptr[t];
+        const int hn = (int)(p.halo_ptr[t + 1] - hb);
+        for (int i = threadIdx.x; i < hn * CH; i += blockDim.x) {
+            const int r = i / CH, ch = i - r * CH;
+            cp_async16(xbuf + (size_t)r * p.pitch + ch * 16, x + (size_t)(uint32_t)p.halo[hb + r] * ROWB + ch * 16);
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+        asm volatile("cp.async.wait_group 0;" ::: "memory");
+        __syncthreads();
+        for (int it = 0; s < se && !bad; s += nwb, ++it) {
+            const int st = it & 1;
+            const bool got = mbar_wait_bounded(&bar[st], (phase >> st) & 1u);
+            if (!__all_sync(0xffffffffu, got)) {
+                if (lane == 0) atomicOr(&bad, 1);
+                break;
+            }
+            phase ^= 1u << st;
+            pending &= ~(1u << st);
+            const int64_t base = p.slice_ptr[s];
+            const int w = (int)((p.slice_ptr[s + 1] - base) / GPW);
+            if (p.prefetch >= 3) prefetch_epilogue<VT, R, G, GPW>(p, s);
+            if (copy_bytes(s) <= cap) {
+                const unsigned char* rec = buf + st * cap;
+                tile_slice_step<VT, G, RPT, TPR, true, U>(p, s, w, xbuf, reinterpret_cast<const int32_t*>(rec) + sub,
+                                                     reinterpret_cast<const VT*>(rec + (size_t)w * GPW * 4) + sub * G,
+                                                     sc, acc_s);
+            } else {
+                const unsigned char* rec = p.mat + base * eb;
+                tile_slice_step<VT, G, RPT, TPR, false, U>(p, s, w, xbuf, reinterpret_cast<const int32_t*>(rec) + sub,
+                                                      reinterpret_cast<const VT*>(rec + (size_t)w * GPW * 4) + sub * G,
+                                                      sc, acc_s);
+            }
+            __syncwarp();   // every lane is done with this buffer before it is refilled
+            if (s + 2 * nwb < se) {
+                pending |= 1u << st;
+                if (lane == 0) issue(s + 2 * nwb, st);
+            }
+        }
+        __syncthreads();   // the halo buffer is reused by the next tile
+        if (bad) break;
+    }
+    if (bad) {
+        if (lane == 0) atomicOr(&p.counter[2], 2u);
+        for (int st = 0; st < 2; ++st)   // let copies still in flight land before shared memory is released
+            if ((pending >> st) & 1u) mbar_wait_bounded(&bar[st], (phase >> st) & 1u);
+        __syncwarp();
+    }
+    reduce_and_finalize<RPT, TPR>(p, acc_s);
+}
+
+template <typename VT, int G>
+StepFn tiled_pick_g(int rpt, int tpr, int min_blocks)
+{
+    if constexpr (sizeof(VT) == 4) {
+        if (rpt == 4 && tpr == 4) return min_blocks == 2 ? k_spmm_tiled<VT, G, 4, 4, 8, 2> : k_spmm_tiled<VT, G, 4, 4, 8, 1>;
+        if (rpt == 4 && tpr == 2) return min_blocks == 2 ? k_spmm_tiled<VT, G, 4, 2, 8, 2> : k_spmm_tiled<VT, G, 4, 2, 8, 1>;
+        if (rpt == 4 && tpr == 8) return min_blocks == 2 ? k_spmm_tiled<VT, G, 4, 8, 8, 2> : k_spmm_tiled<VT, G, 4, 8, 8, 1>;
+    }
+    return nullptr;
 }
 
 // ---------------------------------------------------------------------------- kernel selection

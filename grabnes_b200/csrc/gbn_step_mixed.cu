@@ -11,4 +11,12 @@ StepFn step_kernel_mixed(bool cplx, int G, int rpt, int tpr, bool staged, StepVa
     return cplx ? step_pick<float, true>(G, rpt, tpr, staged, v) : step_pick<float, false>(G, rpt, tpr, staged, v);
 }
 
+StepFn tiled_kernel_mixed(int G, int rpt, int tpr, int min_blocks)
+{
+    if (G == 1) return tiled_pick_g<float, 1>(rpt, tpr, min_blocks);
+    if (G == 2) return tiled_pick_g<float, 2>(rpt, tpr, min_blocks);
+    if (G == 4) return tiled_pick_g<float, 4>(rpt, tpr, min_blocks);
+    return nullptr;
+}
+
 }  // namespace gbn

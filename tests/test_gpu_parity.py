@@ -209,7 +209,8 @@ def test_layout_variants_agree(ctx, rpt):
 @pytest.mark.parametrize("grp", [1, 2, 4])
 def test_kernel_variants_agree(ctx, grp, prec):
     """The product's variants (4 or 8 union columns in flight, staged records with values or with the
-    column indices only, registers bounded for 1, 2 or 3 blocks per SM) add each row's products in the same
+    column indices only, registers bounded for 1, 2 or 3 blocks per SM, and in mixed precision the
+    tile-local product that gathers from a shared-memory copy of each tile's rows) add each row's products in the same
     order; only the grid, and with it the split of the dot products over blocks, follows the occupancy of
     the variant.  So a_n, b_n agree to the rounding of the sums: 1e-6 relative in mixed precision, 1e-10
     in FP64, and FP64 matches the oracle (1e-10)."""
@@ -220,8 +221,9 @@ def test_kernel_variants_agree(ctx, grp, prec):
     runs = []
     try:
         ctx.set_tuning(0, 0, grp, 1, 4)
-        for un, sv, mb in ((4, 1, 1), (8, 1, 1), (4, 0, 1), (8, 0, 1), (8, 1, 2), (8, 1, 3), (8, 0, 3)):
-            ctx.set_kernel_variant(un, sv, mb)
+        for un, sv, mb, tl in ((4, 1, 1, 0), (8, 1, 1, 0), (4, 0, 1, 0), (8, 0, 1, 0), (8, 1, 2, 0), (8, 1, 3, 0),
+                               (8, 0, 3, 0), (8, 1, 1, 1), (8, 1, 2, 1)):
+            ctx.set_kernel_variant(un, sv, mb, -1, tl)
             runs.append(ctx.lanczos_phases(u, 200, prec))
     finally:
         ctx.set_tuning()
