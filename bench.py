@@ -129,9 +129,10 @@ def kernel_key(best):
     mb = best.get("min_blocks", 0) or (3 if (unroll == 8 and g == 1 and staged) else 1)
     pf = best.get("prefetch", -1)
     pf = 6 if pf < 0 else pf
+    rpt = best.get("rhs_per_thread", 0) or 4         # right-hand sides per thread (16 vectors: 4 threads a row)
     if not staged:
-        return f"k_spmm_step<float, real, G={g}, U={unroll}>"
-    return f"k_spmm_staged<float, real, G={g}, U={unroll}, SV={sv}, MINB={mb}, prefetch={pf}>"
+        return f"k_spmm_step<float, real, G={g}, RPT={rpt}, U={unroll}>"
+    return f"k_spmm_staged<float, real, G={g}, RPT={rpt}, U={unroll}, SV={sv}, MINB={mb}, prefetch={pf}>"
 
 
 def traffic_from_profile(key, workload="bench_workload"):
@@ -208,6 +209,8 @@ def run_ours(args, ws, rank, local):
         tuning = []
     else:
         best, tuning = autotune(ctx, u, G.GBN_MIXED)
+        best = dict(best, candidates_top5=sorted((r for r in tuning if "step_ms" in r),
+                                                  key=lambda r: r["step_ms"])[:5])
     ctx.stage_phases(u, G.GBN_MIXED)
     for _ in range(args.warmup):
         ctx.run_staged(nsteps)
@@ -577,7 +580,9 @@ def moire_dos_leg(G, M, local, stream, ws, nrhs=16, nsteps=2000, peak=None, tuni
         best = fixed_tuning(tuning)
         apply(ctx, best)
     else:
-        best, _ = autotune(ctx, u, G.GBN_MIXED)
+        best, cands = autotune(ctx, u, G.GBN_MIXED)
+        best = dict(best, candidates_top5=sorted((r for r in cands if "step_ms" in r),
+                                                  key=lambda r: r["step_ms"])[:5])
     ctx.stage_phases(u, G.GBN_MIXED)
     ctx.run_staged(200)
     torch.cuda.synchronize()

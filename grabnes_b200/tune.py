@@ -9,7 +9,8 @@ its epilogue reads, or of those and the rows of u_k one or more sweeps ahead, an
 blocks per SM.  The search runs in two stages on the caller's own Hamiltonian and start vectors:
 the layout and path (rows per group, right-hand sides per thread, staged or not) at the default
 variant, then, for the best layout of each rows-per-group value, the variant (unroll, prefetch, staged
-values or indices, the register bound for 1, 2 or 3 blocks per SM).  Each candidate runs a short
+values or indices, the register bound for 1, 2 or 3 blocks per SM), and the same for its staged layout at
+the widest vector loads.  Each candidate runs a short
 recursion; the one with the smallest device time per step (update + sparse product, CUDA events) is
 kept on the context.
 """
@@ -55,11 +56,18 @@ def autotune(ctx, u, precision, nsteps=12, rhs_per_thread=(1, 2, 4), blocks_per_
     # indices only, and the register bound (1, 2 or 3 blocks per SM): the best variant differs between
     # layouts, so the layouts' defaults do not rank them
     seen = {_key(r) for r in results}
+    layouts = []
     for grp in rows_per_group:
         mine = [r for r in ok if r["rows_per_group"] == grp]
         if not mine:
             continue
-        lay = min(mine, key=lambda r: r["step_ms"])
+        layouts.append(min(mine, key=lambda r: r["step_ms"]))
+        # and the staged layout at the widest loads (the variants often reorder the splits)
+        wide = [r for r in mine if r["staged"] == 1 and r["rhs_per_thread"] == max(rhs_per_thread)]
+        if wide and wide[0] is not layouts[-1]:
+            layouts.append(wide[0])
+    for lay in layouts:
+        grp = lay["rows_per_group"]
         pfs = prefetch if lay["staged"] == 1 else (0,)
         for pf, un, sv, mb in itertools.product(pfs, unroll, (1, 0), (1, 2, 3)):
             if lay["staged"] != 1 and (sv == 0 or mb != 1):
