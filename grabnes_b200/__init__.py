@@ -41,6 +41,8 @@ class Model(C.Structure):
         ("anderson", C.c_int32), ("anderson_w", C.c_double), ("e0_c", C.c_double),
         ("inter_cut_rho", C.c_double), ("inter_smooth_w", C.c_double),
         ("koshino_sr", C.c_int32), ("renormalize_coupling", C.c_int32), ("coupling_factor", C.c_double),
+        ("second_moire", C.c_int32), ("eps_factor", C.c_double), ("twisted2", C.c_int32), ("twist2_rad", C.c_double),
+        ("rotate_first", C.c_int32), ("shift2", C.c_double), ("shift2_x", C.c_double), ("shift2_y", C.c_double),
     ]
 
 
@@ -101,7 +103,8 @@ EXPORTS = ["gbn_cell_atoms", "gbn_build_cell", "gbn_cart_roundtrip", "gbn_rng_un
            "gbn_peierls", "gbn_get_hamiltonian", "gbn_load_hamiltonian", "gbn_lanczos", "gbn_lanczos_phases",
            "gbn_stage_phases", "gbn_run_staged", "gbn_cf_dos", "gbn_cheb_evolve", "gbn_kubo_evol", "gbn_set_neighd", "gbn_lanczos_noalloc",
            "gbn_cheb_interval", "gbn_cheb_coef", "gbn_dos_gradient", "gbn_dos_gradient_prec", "gbn_lanczos_sites", "gbn_lanczos_sets",
-           "gbn_pdos_atoms", "gbn_pdos_sets", "gbn_lanczos_fields", "gbn_set_images", "gbn_haldane", "gbn_kubo_tevol", "gbn_check_hamiltonian", "gbn_kubo_msd"]
+           "gbn_pdos_atoms", "gbn_pdos_sets", "gbn_lanczos_fields", "gbn_set_images", "gbn_haldane", "gbn_kubo_tevol", "gbn_check_hamiltonian", "gbn_kubo_msd",
+           "gbn_get_onsite_layers"]
 
 
 def _declare(L):
@@ -132,6 +135,7 @@ def _declare(L):
     L.gbn_haldane.argtypes = [vp, d, d, d, i32, C.c_uint32]
     L.gbn_check_hamiltonian.argtypes = [vp, _p(np.int64), C.POINTER(d)]
     L.gbn_get_hamiltonian.argtypes = [vp, _opt(np.float64), _opt(np.complex128)]
+    L.gbn_get_onsite_layers.argtypes = [vp, _opt(np.float64), _opt(np.float64)]
     L.gbn_load_hamiltonian.argtypes = [vp, i64, i32, _p(np.int32), _p(np.int32), _p(np.complex128), _p(np.float64)]
     L.gbn_lanczos.argtypes = [vp, i32, i32, _p(np.complex128), _opt(np.int32), i32, _p(np.float64), _p(np.float64)]
     L.gbn_lanczos_phases.argtypes = [vp, i32, i32, _p(np.float64), _opt(np.int32), i32, _p(np.float64),
@@ -275,6 +279,14 @@ class Context:
         hop = np.zeros(self.n * self.max_neigh, np.complex128)
         self._ck(self._L.gbn_get_hamiltonian(self._h, h0, hop))
         return h0, hop.reshape(self.n, -1)
+
+    def onsite_layers(self):
+        """(H0Bottom, H0Top) of the assembled model: the on-site energies after the first moire's terms
+        (0 without the moire branch) and H0 - H0Bottom with the second moire (0 without it)."""
+        bottom = np.zeros(self.n, np.float64)
+        top = np.zeros(self.n, np.float64)
+        self._ck(self._L.gbn_get_onsite_layers(self._h, bottom, top))
+        return bottom, top
 
     def load_hamiltonian(self, nneigh, nlist, hopp, h0):
         n = len(h0)

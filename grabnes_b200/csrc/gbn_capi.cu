@@ -148,7 +148,8 @@ int gbn_destroy(gbn_ctx* c)
     if (c->stream) cudaStreamSynchronize(c->stream);
     DevBuf* bufs[] = {&c->rat, &c->species, &c->layer, &c->nneigh, &c->nlist, &c->neighd, &c->ncell, &c->h0,
                       &c->hopp, &c->rat_hop, &c->perm, &c->iperm, &c->ell.slice_ptr, &c->ell.mat,
-                      &c->ell.h0, &c->ell.rperm, &c->ell.riperm, &c->ell.dval, &c->partials, &c->scal, &c->counter, &c->ab, &c->upload};
+                      &c->ell.h0, &c->ell.rperm, &c->ell.riperm, &c->ell.dval, &c->partials, &c->scal, &c->counter, &c->ab, &c->upload,
+                      &c->h0_bottom};
     for (DevBuf* b : bufs) b->release();
     for (auto& v : c->vec) v.release();
     for (auto& v : c->cheb) v.release();
@@ -291,6 +292,10 @@ int gbn_assemble(gbn_ctx* c, const gbn_model* m, const double* rat_on, const dou
     if (!c->have_neigh || !c->have_neighd) return fail(c, GBN_ERR_STATE, "no neighbour tables: call gbn_neighbours first");
     if (m->tbnn < 1 || m->tbnn > 8) return fail(c, GBN_ERR_ARG, "tbnn must be in 1..8");
     if (m->anderson && !uniform) return fail(c, GBN_ERR_ARG, "Anderson disorder needs the uniform draws");
+    if (m->second_moire && !m->rotate_first &&
+        ((m->twisted2 && m->moire_onsite && m->eps == 0.0) ||
+         (m->moire_offdiag && (m->eps == 0.0 || m->eps_factor == 0.0))))
+        return fail(c, GBN_ERR_ARG, "the second moire without SecondMoireRotateFirst divides by the lattice mismatch");
     cudaSetDevice(c->device);
     DevBuf ron, uni;
     const double* d_on = c->rat.as<double>();
@@ -339,6 +344,33 @@ int gbn_get_hamiltonian(gbn_ctx* c, double* h0, double* hopp)
     return GBN_OK;
 }
 
+int gbn_get_onsite_layers(gbn_ctx* c, double* bottom, double* top)
+{
+    if (!c) return GBN_ERR_ARG;
+    if (!c->have_ham) return fail(c, GBN_ERR_STATE, "no Hamiltonian");
+    cudaSetDevice(c->device);
+    const size_t n = (size_t)c->n;
+    if (bottom) {
+        if (c->have_bottom)
+            GBN_CK(c, cudaMemcpyAsync(bottom, c->h0_bottom.p, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
+        else
+            memset(bottom, 0, sizeof(double) * n);
+    }
+    if (top) {
+        if (c->have_top) {
+            std::vector<double> b(n);
+            GBN_CK(c, cudaMemcpyAsync(top, c->h0.p, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
+            GBN_CK(c, cudaMemcpyAsync(b.data(), c->h0_bottom.p, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
+            GBN_CK(c, cudaStreamSynchronize(c->stream));
+            for (size_t i = 0; i < n; ++i) top[i] = top[i] - b[i];   // H0Top = H0 - H0Bottom (ham.F90:3639)
+        } else {
+            memset(top, 0, sizeof(double) * n);
+        }
+    }
+    GBN_CK(c, cudaStreamSynchronize(c->stream));
+    return GBN_OK;
+}
+
 int gbn_load_hamiltonian(gbn_ctx* c, int64_t n, int32_t max_neigh, const int32_t* nneigh, const int32_t* nlist,
                          const double* hopp, const double* h0)
 {
@@ -380,6 +412,7 @@ int gbn_load_hamiltonian(gbn_ctx* c, int64_t n, int32_t max_neigh, const int32_t
     c->have_neigh = true;
     c->have_neighd = same_atoms && c->have_neighd;
     c->have_ham = true;
+    c->have_bottom = c->have_top = false;
     c->ham_complex = cplx;
     c->ell.valid = false;
     return GBN_OK;

@@ -125,6 +125,9 @@ struct gbn_ctx {
     // Hamiltonian (reference layout, FP64)
     gbn::DevBuf h0, hopp;  // double[n], double2[n*max_neigh]
     gbn::DevBuf rat_hop;   // positions used for the Peierls phases
+    gbn::DevBuf h0_bottom; // double[n]: H0 after the first moire's terms (moire branch only)
+    bool have_bottom = false;   // the assembled model ran the moire branch (h0_bottom is set)
+    bool have_top = false;      // ... and the second moire (H0Top = H0 - H0Bottom)
     bool have_ham = false;
     bool ham_complex = false;
     bool has_field = false;   // gbn_peierls has been applied to the assembled hoppings

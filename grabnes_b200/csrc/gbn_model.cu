@@ -65,50 +65,128 @@ __device__ void d_moire_disp(const gbn_model& m, double x, double y, double* dx,
     }
 }
 
+// Displacement of the second moire before its shift and flip (HamOnSiteSecondMoireTerms, ham.F90:3573-3590)
+__device__ void d_second_moire_disp(const gbn_model& m, double x, double y, double* dx, double* dy)
+{
+    const double e = m.eps * m.eps_factor;
+    if (m.twisted2) {
+        double st, ct;
+        sincos(m.twist2_rad, &st, &ct);
+        const double ys = m.rotate_first ? y : y - m.shift2 / m.eps;
+        *dx = x * ((1.0 + e) * ct - 1.0) - ys * (1.0 + e) * st;
+        *dy = ys * ((1.0 + e) * ct - 1.0) + x * (1.0 + e) * st;
+    } else {
+        *dx = x * e;
+        *dy = y * e;
+    }
+}
+
+__device__ __forceinline__ void d_moire_terms(const gbn_model& m, double dx, double dy, double* hz, double* hd)
+{
+    *hz = 0.0;
+    *hd = 0.0;
+    if (m.moire_onsite == 2) *hd = d_diago(dx, dy, m.C0, m.Phi0, m.aG);
+    else if (m.moire_onsite == 3) *hz = d_diago(dx, dy, m.Cz, m.Phiz, m.aG);
+    else if (m.moire_onsite == 1) {
+        *hz = d_diago(dx, dy, m.Cz, m.Phiz, m.aG);
+        *hd = d_diago(dx, dy, m.C0, m.Phi0, m.aG);
+    }
+}
+
+// HamOnSite in its order: the carbon site energy (:947), Anderson disorder (:1237-1248), the first moire's
+// terms (HamOnSiteMoireEffective, :3437-3544), H0Bottom = H0 (:2703, into h0b when given), then the second
+// moire's terms on every atom (HamOnSiteSecondMoireTerms, :3546-3642).
 __global__ void k_onsite(gbn_model m, int64_t n, const double* rat, const int32_t* species, const int32_t* layer,
-                         const double* uniform, double* h0)
+                         const double* uniform, double* h0, double* h0b)
 {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double h = m.e0_c;
+    if (m.anderson) h = h + (uniform[i] - 0.5) * m.anderson_w;
+    const double sgn = (species[i] % 2 == 1) ? -1.0 : 1.0;
     if (m.moire_onsite != 0) {
-        double dx, dy;
+        double dx, dy, hz, hd;
         d_moire_disp(m, rat[3 * i], rat[3 * i + 1], &dx, &dy);
         dy = dy + m.shift1;
         const int L = layer[i];
         if ((L == 1 && m.sign1 < 0.0) || (L == 2 && m.sign2 < 0.0)) { dx = -dx; dy = -dy; }
-        double hz = 0.0, hd = 0.0;
-        if (m.moire_onsite == 2) hd = d_diago(dx, dy, m.C0, m.Phi0, m.aG);
-        else if (m.moire_onsite == 3) hz = d_diago(dx, dy, m.Cz, m.Phiz, m.aG);
-        else if (m.moire_onsite == 1) {
-            hz = d_diago(dx, dy, m.Cz, m.Phiz, m.aG);
-            hd = d_diago(dx, dy, m.C0, m.Phi0, m.aG);
-        }
-        const double sgn = (species[i] % 2 == 1) ? -1.0 : 1.0;
+        d_moire_terms(m, dx, dy, &hz, &hd);
         if (L == 1) h = h + (sgn * hz * m.sign1 + hd);
         else if (L == 2) h = h + (sgn * hz * m.sign2 + hd);
+        if (h0b) h0b[i] = h;
+        if (m.second_moire) {
+            d_second_moire_disp(m, rat[3 * i], rat[3 * i + 1], &dx, &dy);
+            if (m.rotate_first) {
+                dy = dy + m.shift2_y;
+                dx = dx + m.shift2_x;
+            }
+            if (m.sign2 < 0.0) { dx = -dx; dy = -dy; }
+            d_moire_terms(m, dx, dy, &hz, &hd);
+            h = h + (sgn * hz * m.sign2 + hd);
+        }
+    } else if (h0b) {
+        h0b[i] = 0.0;
     }
-    if (m.anderson) h = h + (uniform[i] - 0.5) * m.anderson_w;
     h0[i] = h;
+}
+
+// del(1..3) of the second moire's bond term of atom i (HamHopSecondMoire, ham.F90:7772-7833): the
+// displacement is rotated by TwistAngle2 whether or not Twisted2 is set, flipped before the shift, and Im of
+// the amplitude changes sign with the mass factor.
+__device__ void d_second_moire_deltas(const gbn_model& m, double x, double y, int spec, double del[3])
+{
+    const double e = m.eps * m.eps_factor;
+    double st, ct, dx, dy;
+    sincos(m.twist2_rad, &st, &ct);
+    if (m.rotate_first) {
+        dx = x * ((1.0 + e) * ct - 1.0) - y * (1.0 + e) * st;
+        dy = y * ((1.0 + e) * ct - 1.0) + x * (1.0 + e) * st;
+    } else {
+        const double ys = y - m.shift2 / m.eps / m.eps_factor;
+        dx = x * ((1.0 + e) * ct - 1.0) - ys * (1.0 + m.eps) * st;
+        dy = ys * ((1.0 + m.eps) * ct - 1.0) + x * (1.0 + m.eps / m.eps_factor) * st;
+    }
+    if (m.sign2 < 0.0) { dx = -dx; dy = -dy; }
+    if (m.rotate_first) {
+        dx = dx + m.shift2_x;
+        dy = dy + m.shift2_y;
+    }
+    double re, im;
+    d_offdiago(dx, dy, m.Cab, m.Phiab, m.aG, &re, &im);
+    if (m.sign2 < 0.0) im = -im;
+    if (spec == 1 || spec == 2) d_bond_deltas(spec, re, im, del);
+}
+
+// MoireBondDeltaMidpoint (ham.F90:4822-4883): the bond term of one bond from the moire displacement at its
+// midpoint.  First moire: eps, its twist, shift1 before the flip; second moire: eps * eps_factor, TwistAngle2,
+// shift2 after the flip, Im flipped and del(2), del(3) swapped with the mass factor's sign.
+__device__ double d_mid_delta(double rix, double riy, double bx, double by, int spec, double epsM, double thM,
+                              double pre_y, bool flip, double post_x, double post_y, bool flip_imag, bool swap23,
+                              double Cab, double Phi, double aG)
+{
+    if (spec != 1 && spec != 2) return 0.0;
+    const double rm0 = rix + 0.5 * bx, rm1 = riy + 0.5 * by;
+    double st, ct;
+    sincos(thM, &st, &ct);
+    double ddx = rm0 * ((1.0 + epsM) * ct - 1.0) - rm1 * (1.0 + epsM) * st;
+    double ddy = rm1 * ((1.0 + epsM) * ct - 1.0) + rm0 * (1.0 + epsM) * st;
+    ddy = ddy + pre_y;
+    if (flip) { ddx = -ddx; ddy = -ddy; }
+    ddx = ddx + post_x;
+    ddy = ddy + post_y;
+    double re, im, del[3];
+    d_offdiago(ddx, ddy, Cab, Phi, aG, &re, &im);
+    if (flip_imag) im = -im;
+    d_bond_deltas(spec, re, im, del);
+    if (fabs(bx) < aG / 4.0) return del[0];
+    if (bx < 0.0) return swap23 ? del[1] : del[2];
+    return swap23 ? del[2] : del[1];
 }
 
 __device__ double d_moire_mid_delta(const gbn_model& m, double rix, double riy, double bx, double by, int spec, bool flip)
 {
-    if (spec != 1 && spec != 2) return 0.0;
-    const double rm0 = rix + 0.5 * bx, rm1 = riy + 0.5 * by;
     const double th = m.moire_twisted ? m.twist_rad : 0.0;
-    double st, ct;
-    sincos(th, &st, &ct);
-    double ddx = rm0 * ((1.0 + m.eps) * ct - 1.0) - rm1 * (1.0 + m.eps) * st;
-    double ddy = rm1 * ((1.0 + m.eps) * ct - 1.0) + rm0 * (1.0 + m.eps) * st;
-    ddy = ddy + m.shift1;
-    if (flip) { ddx = -ddx; ddy = -ddy; }
-    double re, im, del[3];
-    d_offdiago(ddx, ddy, m.Cab, m.Phiab, m.aG, &re, &im);
-    d_bond_deltas(spec, re, im, del);
-    if (fabs(bx) < m.aG / 4.0) return del[0];
-    if (bx < 0.0) return del[2];
-    return del[1];
+    return d_mid_delta(rix, riy, bx, by, spec, m.eps, th, m.shift1, flip, 0.0, 0.0, false, false, m.Cab, m.Phiab, m.aG);
 }
 
 __device__ double d_f2g2_shell(const gbn_model& m, double dist)
@@ -154,6 +232,13 @@ __global__ void k_hopping(gbn_model m, int64_t n, const double* rat, const int32
         d_offdiago(dx, dy, m.Cab, m.Phiab, m.aG, &re, &im);
         if (si == 1 || si == 2) d_bond_deltas(si, re, im, del);
     }
+    // the second moire's bond term (HamHopSecondMoire, ham.F90:7745-7880), a pass of its own in the
+    // reference after every other term and before the Peierls phases: subtracted here from the same
+    // entry, with its own delta carried over between the bonds of the atom as there
+    const bool second = m.second_moire && m.moire_offdiag;
+    double delta2 = 0.0;
+    double del2[3] = {0.0, 0.0, 0.0};
+    if (second) d_second_moire_deltas(m, rix, riy, si, del2);
     const int k = nneigh[i];
     for (int j = 0; j < max_neigh; ++j) {
         const int64_t e = i * max_neigh + j;
@@ -175,6 +260,18 @@ __global__ void k_hopping(gbn_model m, int64_t n, const double* rat, const int32
                         if (m.intralayer == 1) hr = hr + d_f2g2_shell(m, d);
                         if (d > 1.5) delta = 0.0;
                         hr = hr + (m.gn_cc[lv] - delta);
+                        if (second) {
+                            if (fabs(Dx) < 0.01) delta2 = del2[0];
+                            else if (Dx < -0.02) delta2 = (m.sign2 < 0.0) ? del2[1] : del2[2];
+                            else if (Dx > 0.02) delta2 = (m.sign2 < 0.0) ? del2[2] : del2[1];
+                            if (m.moire_mid) {
+                                const bool neg = m.sign2 < 0.0;
+                                delta2 = d_mid_delta(rix, riy, Dx, Dy, si, m.eps * m.eps_factor, m.twist2_rad, 0.0, neg,
+                                                     m.shift2_x, m.shift2_y, neg, neg, m.Cab, m.Phiab, m.aG);
+                            }
+                            if (d > 1.7) delta2 = 0.0;
+                            hr = hr - delta2;
+                        }
                         break;
                     }
                 }
@@ -274,8 +371,14 @@ int assemble(gbn_ctx* c, const gbn_model* m, const double* d_rat_on, const doubl
     GBN_CK(c, c->h0.ensure(sizeof(double) * n));
     GBN_CK(c, c->hopp.ensure(sizeof(double2) * (size_t)n * c->max_neigh));
     const unsigned grd = (unsigned)((n + 127) / 128);
+    // H0Bottom is kept only for the moire branch (elsewhere it is 0 and nothing is stored)
+    double* h0b = nullptr;
+    if (m->moire_onsite != 0) {
+        GBN_CK(c, c->h0_bottom.ensure(sizeof(double) * n));
+        h0b = c->h0_bottom.as<double>();
+    }
     k_onsite<<<grd, 128, 0, c->stream>>>(*m, n, d_rat_on, c->species.as<int32_t>(), c->layer.as<int32_t>(), d_uniform,
-                                         c->h0.as<double>());
+                                         c->h0.as<double>(), h0b);
     GBN_CK_LAUNCH(c);
     k_hopping<<<grd, 128, 0, c->stream>>>(*m, n, d_rat_hop, c->species.as<int32_t>(), c->layer.as<int32_t>(),
                                           c->max_neigh, c->nneigh.as<int32_t>(), c->nlist.as<int32_t>(),
@@ -285,6 +388,8 @@ int assemble(gbn_ctx* c, const gbn_model* m, const double* d_rat_on, const doubl
     c->ham_complex = false;
     c->has_field = false;
     c->ell.valid = false;
+    c->have_bottom = h0b != nullptr;
+    c->have_top = h0b != nullptr && m->second_moire != 0;
     return GBN_OK;
 }
 

@@ -376,6 +376,21 @@ Job job_from_input(const Input& in)
     m.shift1 = in.d("Moire.LayerShift1", 0.0);
     m.sign1 = in.d("Moire.FirstMoireMassFactor", 1.0);
     m.sign2 = in.d("Moire.SecondMoireMassFactor", 1.0);
+    // Moire.AddSecondMoire (ham.F90:2652-2704 on-site, 5859-5888 and 7745-7880 bonds)
+    m.second_moire = in.l("Moire.AddSecondMoire", false) ? 1 : 0;
+    if (m.second_moire && in.l("Structure.BasedOnMoireCellParameters", false))
+        die("Moire.AddSecondMoire with Structure.BasedOnMoireCellParameters: the reference's second moire then "
+            "reads a lattice mismatch it never sets");
+    m.eps_factor = in.d("Moire.LatticePercentFactor", 1.0);
+    m.twisted2 = in.l("Moire.Twisted2", false) ? 1 : 0;
+    m.twist2_rad = in.d("Moire.TwistAngle2", 0.0) * kPi / 180.0;
+    m.rotate_first = in.l("Moire.SecondMoireRotateFirst", true) ? 1 : 0;
+    m.shift2 = in.d("Moire.LayerShift2", 0.0);
+    {
+        const double phi2m = atan((1.0 + m.eps) * sin(m.twist2_rad) / ((1.0 + m.eps) * cos(m.twist2_rad) - 1.0));
+        m.shift2_x = m.shift2 * cos(phi2m);
+        m.shift2_y = m.shift2 * sin(phi2m);
+    }
     if (bl == "Koshino" || bl == "HTC") m.interlayer = 1;
     m.vpppi0 = in.d("Interlayer.Vpppi0", koshino_intra ? 2.7 : 3.5) / g0;
     m.vppsigma0 = -in.d("Interlayer.Vppsigma0", 0.48) / g0;
@@ -608,14 +623,17 @@ void print_job(const Job& j)
            "\"moire_onsite\": %d, \"moire_offdiag\": %d, \"moire_mid\": %d, \"moire_twisted\": %d, \"eps\": %.17g, "
            "\"twist_rad\": %.17g, \"C0\": %.17g, \"Cz\": %.17g, \"Cab\": %.17g, \"interlayer\": %d, "
            "\"vpppi0\": %.17g, \"vppsigma0\": %.17g, \"bl_delta\": %.17g, \"anderson\": %d, \"anderson_w\": %.17g, "
-           "\"tksl2\": %.17g, \"koshino_sr\": %d, \"renormalize_coupling\": %d, \"coupling_factor\": %.17g}}\n",
+           "\"tksl2\": %.17g, \"koshino_sr\": %d, \"renormalize_coupling\": %d, \"coupling_factor\": %.17g, "
+           "\"second_moire\": %d, \"eps_factor\": %.17g, \"twisted2\": %d, \"twist2_rad\": %.17g, "
+           "\"rotate_first\": %d, \"shift2_x\": %.17g, \"shift2_y\": %.17g, \"sign2\": %.17g}}\n",
            j.cell.kind, j.cell.aG, j.cell.cell_size, j.cell.super_cell, j.cell.m[0], j.cell.m[1], j.cell.m[2], j.cell.m[3],
            j.cell.height, j.cell.d_interlayer, j.g0, j.cut2intra, j.cut2inter, (int)j.second_layer, (int)j.moire,
            j.nrecurs, j.eta, j.n_en, j.emin, j.emax, j.seed, j.prefix.c_str(), (int)j.only_dos, j.npol, j.nt, j.nwr,
            j.dt, j.pdos.mode, j.seed_set, (int)j.haldane, j.hal_t2, j.hal_mode, j.mphii, j.mphif, j.mphistep, m.tbnn, m.intralayer, m.moire_onsite,
            m.moire_offdiag, m.moire_mid, m.moire_twisted, m.eps, m.twist_rad, m.C0, m.Cz, m.Cab, m.interlayer,
            m.vpppi0, m.vppsigma0, m.bl_delta, m.anderson, m.anderson_w, m.tksl[2], m.koshino_sr,
-           m.renormalize_coupling, m.coupling_factor);
+           m.renormalize_coupling, m.coupling_factor, m.second_moire, m.eps_factor, m.twisted2, m.twist2_rad,
+           m.rotate_first, m.shift2_x, m.shift2_y, m.sign2);
 }
 
 void write_pairs(const std::string& path, const std::vector<double>& x, const std::vector<double>& y, double head,
@@ -758,9 +776,11 @@ void write_neigh_files(gbn_ctx* ctx, int64_t n, int32_t maxn, const std::vector<
 // Output.WriteDataFiles, Hamiltonian part (HamHopping and HamHopWriteTables, ham.F90:6944-7040):
 // <prefix>.s.mag (the hoppings of each atom, g0 units, the reference's sign), <prefix>.e (H0, Species,
 // layerIndex), <prefix>.pos, <prefix>.cell (ucell then the reciprocal cell, one vector per line), and the
-// empty <prefix>.HABreal / .HABimag of models without those terms.
+// empty <prefix>.HABreal / .HABimag of models without those terms, <prefix>.bottom.e and (second moire)
+// <prefix>.top.e.
 void write_ham_files(gbn_ctx* ctx, const std::string& prefix, int64_t n, int32_t maxn, const std::vector<double>& rat,
-                     const std::vector<int32_t>& species, const std::vector<int32_t>& layer, const double* u)
+                     const std::vector<int32_t>& species, const std::vector<int32_t>& layer, const double* u,
+                     bool second_moire)
 {
     std::vector<int32_t> nn((size_t)n);
     ck(gbn_get_neighbours(ctx, nn.data(), nullptr, nullptr, nullptr), ctx, "gbn_get_neighbours");
@@ -806,6 +826,18 @@ void write_ham_files(gbn_ctx* ctx, const std::string& prefix, int64_t n, int32_t
         fprintf(f, "%s%s%s\n", fortran_ld(2.0 * kPi * rc[3 * v] / vol).c_str(), fortran_ld(2.0 * kPi * rc[3 * v + 1] / vol).c_str(),
                 fortran_ld(2.0 * kPi * rc[3 * v + 2] / vol).c_str());
     fclose(f);
+    // <prefix>.bottom.e (always) and <prefix>.top.e (Moire.AddSecondMoire): H0Bottom / H0Top and Species,
+    // ham.F90:7020-7034
+    std::vector<double> bottom((size_t)n), top((size_t)n);
+    ck(gbn_get_onsite_layers(ctx, bottom.data(), top.data()), ctx, "gbn_get_onsite_layers");
+    f = open_or_die(prefix + ".bottom.e");
+    for (int64_t i = 0; i < n; ++i) fprintf(f, "%s%12d\n", fortran_ld(bottom[(size_t)i]).c_str(), species[(size_t)i]);
+    fclose(f);
+    if (second_moire) {
+        f = open_or_die(prefix + ".top.e");
+        for (int64_t i = 0; i < n; ++i) fprintf(f, "%s%12d\n", fortran_ld(top[(size_t)i]).c_str(), species[(size_t)i]);
+        fclose(f);
+    }
 }
 
 // Output.ReadDataFiles: the neighbour list from v (NeighReadDataFiles, neigh.F90:446-522: with
@@ -1202,7 +1234,8 @@ int run(const Job& j0)
         }
         if (j.haldane) ck(gbn_haldane(ctx, j.cell.aG, j.hal_t2, hphase, j.hal_paper ? 1 : 0, j.hal_mask), ctx, "gbn_haldane");
         if (!j.read_data) check_hamiltonian(ctx, j);
-        if (j.write_data && !j.read_data) write_ham_files(ctx, prefix, n, maxn, rat_now, species, layer, ucell.data());
+        if (j.write_data && !j.read_data) write_ham_files(ctx, prefix, n, maxn, rat_now, species, layer, ucell.data(),
+                                                        j.model.second_moire != 0);
         bool any = true;
         if (j.pdos.mode == 0) {   // KuboInitWF + KuboDOS
             ck(gbn_lanczos_phases(ctx, GBN_FP64, 1, u.data(), nullptr, j.nrecurs, a.data(), b.data()), ctx,

@@ -117,6 +117,20 @@ def job_from_keys(keys):
     m.shift1 = g("Moire.LayerShift1", 0.0)
     m.sign1 = g("Moire.FirstMoireMassFactor", 1.0)
     m.sign2 = g("Moire.SecondMoireMassFactor", 1.0)
+    # Moire.AddSecondMoire (ham.F90:2652-2704 on-site, 5859-5888 and 7745-7880 bonds)
+    m.second_moire = int(bool(g("Moire.AddSecondMoire", False)))
+    if m.second_moire:
+        if g("Structure.BasedOnMoireCellParameters", False):
+            raise ValueError("Moire.AddSecondMoire with Structure.BasedOnMoireCellParameters: the reference's "
+                             "second moire then reads a lattice mismatch it never sets")
+    m.eps_factor = g("Moire.LatticePercentFactor", 1.0)
+    m.twisted2 = int(bool(g("Moire.Twisted2", False)))
+    m.twist2_rad = g("Moire.TwistAngle2", 0.0) * math.pi / 180.0
+    m.rotate_first = int(bool(g("Moire.SecondMoireRotateFirst", True)))
+    m.shift2 = g("Moire.LayerShift2", 0.0)
+    phi2m = math.atan((1.0 + m.eps) * math.sin(m.twist2_rad) / ((1.0 + m.eps) * math.cos(m.twist2_rad) - 1.0))
+    m.shift2_x = m.shift2 * math.cos(phi2m)
+    m.shift2_y = m.shift2 * math.sin(phi2m)
     if bl in ("Koshino", "HTC"):
         m.interlayer = 1
     m.vpppi0 = g("Interlayer.Vpppi0", 2.7 if koshino_intra else 3.5) / g0

@@ -73,6 +73,18 @@ typedef struct gbn_model {
     int32_t koshino_sr;
     int32_t renormalize_coupling;
     double  coupling_factor;
+    /* Moire.AddSecondMoire: a second moire pattern on the same graphene (HamOnSiteSecondMoireTerms,
+     * ham.F90:3546-3642, and, with moire_offdiag, HamHopSecondMoire, ham.F90:7745-7880): lattice mismatch
+     * eps * eps_factor (Moire.LatticePercentFactor), Moire.Twisted2 / TwistAngle2 [rad], Moire.LayerShift2
+     * [Ang] with its components along phi2M = atan((1+eps) sin t2 / ((1+eps) cos t2 - 1)),
+     * Moire.SecondMoireRotateFirst; its mass term scaled by sign2 (Moire.SecondMoireMassFactor). */
+    int32_t second_moire;
+    double  eps_factor;
+    int32_t twisted2;
+    double  twist2_rad;
+    int32_t rotate_first;
+    double  shift2;
+    double  shift2_x, shift2_y;
 } gbn_model;
 
 /* ---- host-side cell construction and random numbers (no context, no GPU needed) ------ */
@@ -181,6 +193,12 @@ int gbn_set_images(gbn_ctx* ctx, const int32_t* ncell);
 int gbn_peierls(gbn_ctx* ctx, double flux);
 /* Copy H0(N) and hopp(maxNeigh,N) (complex) of the current Hamiltonian out (either may be NULL). */
 int gbn_get_hamiltonian(gbn_ctx* ctx, double* h0, double* hopp);
+/* H0Bottom and H0Top of HamOnSite (ham.F90:44-45, 2703, 3639), written by HamHopWriteTables to
+ * <prefix>.bottom.e and <prefix>.top.e (ham.F90:7020-7034): bottom = the on-site energies after the first
+ * moire's terms when the assembled model ran the moire branch (moire_onsite != 0), else 0; top = H0 - H0Bottom
+ * when it also ran the second moire (second_moire), else 0.  g0 units, reference atom order; either
+ * pointer may be NULL.  Replaces the H0Bottom / H0Top arrays of the ham module. */
+int gbn_get_onsite_layers(gbn_ctx* ctx, double* bottom, double* top);
 /* Minimal drop-in for a Fortran host: the arrays KuboRecursion receives
  * (lanczosKuboCode/Src/kubosubs.F90:26-43: H0, hopp, NList2 and the module's Nneigh, nAt). */
 int gbn_load_hamiltonian(gbn_ctx* ctx, int64_t n, int32_t max_neigh, const int32_t* nneigh,

@@ -105,10 +105,23 @@ typedef struct {
      * s = 1 up to rho_c - w, (1 + cos(pi (rho - rho_c + w) / w)) / 2 up to rho_c, 0 beyond; w = 0: none. */
     double  inter_smooth_w;
     double  inter_cut_rho;
+    /* Moire.AddSecondMoire (HamOnSiteSecondMoireTerms, ham.F90:3546-3642; HamHopSecondMoire,
+     * ham.F90:7745-7880, with Moire.OffDiag): a second moire pattern on the same graphene */
+    int32_t second_moire;
+    double  eps_factor;        /* Moire.LatticePercentFactor                       */
+    int32_t twisted2;          /* Moire.Twisted2                                   */
+    double  twist2_rad;        /* Moire.TwistAngle2 [rad]                          */
+    int32_t rotate_first;      /* Moire.SecondMoireRotateFirst                     */
+    double  shift2;            /* Moire.LayerShift2 [Ang]                          */
+    double  shift2_x, shift2_y; /* shift2 (cos, sin) phi2M, ham.F90:2688-2690      */
 } orc_model;
 
 void orc_onsite(const orc_model* m, int64_t n, const double* Rat,
                 const int32_t* species, const int32_t* layer, double* H0);
+/* orc_onsite, and H0Bottom (ham.F90:2703): the on-site energies after the first moire's terms when the
+ * moire branch runs, else 0.  H0Top = H0 - H0Bottom when the second moire runs (ham.F90:3639), else 0. */
+void orc_onsite_layers(const orc_model* m, int64_t n, const double* Rat, const int32_t* species,
+                       const int32_t* layer, double* H0, double* H0Bottom);
 void orc_hopping(const orc_model* m, int64_t n, const double* Rat,
                  const int32_t* species, const int32_t* layer,
                  int32_t maxNeigh, const int32_t* Nneigh, const int32_t* NList,

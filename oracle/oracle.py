@@ -42,6 +42,8 @@ class Model(C.Structure):
         ("anderson", C.c_int32), ("anderson_w", C.c_double), ("seed", C.c_int32), ("e0_c", C.c_double),
         ("koshino_sr", C.c_int32), ("renormalize_coupling", C.c_int32), ("coupling_factor", C.c_double),
         ("inter_smooth_w", C.c_double), ("inter_cut_rho", C.c_double),
+        ("second_moire", C.c_int32), ("eps_factor", C.c_double), ("twisted2", C.c_int32), ("twist2_rad", C.c_double),
+        ("rotate_first", C.c_int32), ("shift2", C.c_double), ("shift2_x", C.c_double), ("shift2_y", C.c_double),
     ]
 
 
@@ -79,6 +81,8 @@ def _declare(L):
     L.orc_nbr_copy.argtypes = [C.c_void_p, _p(np.int32), _p(np.int32), _p(np.float64), _p(np.int32)]
     L.orc_nbr_free.argtypes = [C.c_void_p]
     L.orc_onsite.argtypes = [C.POINTER(Model), i64, _p(np.float64), _p(np.int32), _p(np.int32), _p(np.float64)]
+    L.orc_onsite_layers.argtypes = [C.POINTER(Model), i64, _p(np.float64), _p(np.int32), _p(np.int32), _p(np.float64),
+                                    _p(np.float64)]
     L.orc_hopping.argtypes = [C.POINTER(Model), i64, _p(np.float64), _p(np.int32), _p(np.int32), i32,
                               _p(np.int32), _p(np.int32), _p(np.float64), _p(np.complex128)]
     L.orc_haldane.argtypes = [i64, _p(np.int32), _p(np.int32), i32, _p(np.int32), _p(np.int32), _p(np.float64), C.c_double,
@@ -158,6 +162,17 @@ def onsite(model, rat, species, layer):
     h0 = np.zeros(n, np.float64)
     lib().orc_onsite(C.byref(model), n, np.ascontiguousarray(rat, np.float64).reshape(-1), species, layer, h0)
     return h0
+
+
+def onsite_layers(model, rat, species, layer):
+    """(H0, H0Bottom, H0Top) of HamOnSite (ham.F90:2703, 3639): H0Bottom is H0 after the first moire's
+    terms when the moire branch runs (0 otherwise), H0Top = H0 - H0Bottom when the second moire runs."""
+    n = len(species)
+    h0, bottom = np.zeros(n, np.float64), np.zeros(n, np.float64)
+    lib().orc_onsite_layers(C.byref(model), n, np.ascontiguousarray(rat, np.float64).reshape(-1), species, layer,
+                            h0, bottom)
+    top = h0 - bottom if model.second_moire else np.zeros(n, np.float64)
+    return h0, bottom, top
 
 
 def hopping(model, rat, species, layer, nb):

@@ -63,37 +63,49 @@ static void moire_disp(const orc_model* m, double x, double y, int integer_one, 
     }
 }
 
-void orc_onsite(const orc_model* m, int64_t n, const double* Rat, const int32_t* species,
-                const int32_t* layer, double* H0)
+/* Displacement of the second moire before its shift and flip (HamOnSiteSecondMoireTerms, ham.F90:3573-3590;
+ * the Structure.BasedOnMoireCellParameters branch is not restated: it reads eps2, which is never set) */
+static void second_moire_disp(const orc_model* m, double x, double y, double* dx, double* dy)
 {
-    /* ham.F90:846-850 and HamOnSiteSpeciesEnergies :3703-4014 (carbon) */
-    for (int64_t i = 0; i < n; ++i) H0[i] = m->e0_c;
-    /* HamOnSiteMoireEffective, ham.F90:3437-3544 */
-    if (m->moire_onsite != ORC_ONSITE_NONE) {
-        for (int64_t i = 0; i < n; ++i) {
-            double dx, dy;
-            moire_disp(m, Rat[3 * i], Rat[3 * i + 1], 1, &dx, &dy);
-            dy = dy + m->shift1;
-            if ((layer[i] == 1 && m->sign1 < 0.0) || (layer[i] == 2 && m->sign2 < 0.0)) {
-                dx = -dx;
-                dy = -dy;
-            }
-            double Hz = 0.0, Hd = 0.0;
-            switch (m->moire_onsite) {
-            case ORC_ONSITE_ONLY_H0: Hz = 0.0; Hd = diago(dx, dy, m->C0, m->Phi0, m->aG); break;
-            case ORC_ONSITE_ONLY_HZ: Hz = diago(dx, dy, m->Cz, m->Phiz, m->aG); Hd = 0.0; break;
-            case ORC_ONSITE_NO_H0_AND_HZ: Hz = 0.0; Hd = 0.0; break;
-            case ORC_ONSITE_H0_AND_HZ:
-                Hz = diago(dx, dy, m->Cz, m->Phiz, m->aG);
-                Hd = diago(dx, dy, m->C0, m->Phi0, m->aG);
-                break;
-            }
-            const double sgn = (species[i] % 2 == 1) ? -1.0 : 1.0; /* (-1)**Species */
-            if (layer[i] == 1) H0[i] = H0[i] + (sgn * Hz * m->sign1 + Hd);
-            else if (layer[i] == 2) H0[i] = H0[i] + (sgn * Hz * m->sign2 + Hd);
+    const double e = m->eps * m->eps_factor;
+    const double t = m->twist2_rad;
+    if (m->twisted2) {
+        if (m->rotate_first) {
+            *dx = x * ((1.0 + e) * cos(t) - 1.0) - y * (1.0 + e) * sin(t);
+            *dy = y * ((1.0 + e) * cos(t) - 1.0) + x * (1.0 + e) * sin(t);
+        } else {
+            const double ys = y - m->shift2 / m->eps;
+            *dx = x * ((1.0 + e) * cos(t) - 1.0) - ys * (1.0 + e) * sin(t);
+            *dy = ys * ((1.0 + e) * cos(t) - 1.0) + x * (1.0 + e) * sin(t);
         }
+    } else {
+        *dx = x * e;
+        *dy = y * e;
     }
-    /* Anderson disorder, ham.F90:1237-1248, seeded by RandSeedFromInput (random.F90:31-52) */
+}
+
+static void moire_terms(const orc_model* m, double dx, double dy, double* Hz, double* Hd)
+{
+    *Hz = 0.0;
+    *Hd = 0.0;
+    switch (m->moire_onsite) {
+    case ORC_ONSITE_ONLY_H0: *Hd = diago(dx, dy, m->C0, m->Phi0, m->aG); break;
+    case ORC_ONSITE_ONLY_HZ: *Hz = diago(dx, dy, m->Cz, m->Phiz, m->aG); break;
+    case ORC_ONSITE_NO_H0_AND_HZ: break;
+    case ORC_ONSITE_H0_AND_HZ:
+        *Hz = diago(dx, dy, m->Cz, m->Phiz, m->aG);
+        *Hd = diago(dx, dy, m->C0, m->Phi0, m->aG);
+        break;
+    }
+}
+
+void orc_onsite_layers(const orc_model* m, int64_t n, const double* Rat, const int32_t* species,
+                       const int32_t* layer, double* H0, double* H0Bottom)
+{
+    /* ham.F90:846-850 and HamOnSiteSpeciesEnergies :3703-4014 (carbon), called at :947 */
+    for (int64_t i = 0; i < n; ++i) H0[i] = m->e0_c;
+    /* Anderson disorder, ham.F90:1237-1248 (before the moire terms), seeded by RandSeedFromInput
+     * (random.F90:31-52) */
     if (m->anderson) {
         orc_rng r;
         orc_rng_put(&r, m->seed);
@@ -102,29 +114,83 @@ void orc_onsite(const orc_model* m, int64_t n, const double* Rat, const int32_t*
             H0[i] = H0[i] + (rnd - 0.5) * m->anderson_w;
         }
     }
+    if (H0Bottom)
+        for (int64_t i = 0; i < n; ++i) H0Bottom[i] = 0.0;
+    if (m->moire_onsite == ORC_ONSITE_NONE) return;
+    /* HamOnSiteMoireEffective, ham.F90:3437-3544 */
+    for (int64_t i = 0; i < n; ++i) {
+        double dx, dy, Hz, Hd;
+        moire_disp(m, Rat[3 * i], Rat[3 * i + 1], 1, &dx, &dy);
+        dy = dy + m->shift1;
+        if ((layer[i] == 1 && m->sign1 < 0.0) || (layer[i] == 2 && m->sign2 < 0.0)) {
+            dx = -dx;
+            dy = -dy;
+        }
+        moire_terms(m, dx, dy, &Hz, &Hd);
+        const double sgn = (species[i] % 2 == 1) ? -1.0 : 1.0; /* (-1)**Species */
+        if (layer[i] == 1) H0[i] = H0[i] + (sgn * Hz * m->sign1 + Hd);
+        else if (layer[i] == 2) H0[i] = H0[i] + (sgn * Hz * m->sign2 + Hd);
+    }
+    /* H0Bottom = H0, ham.F90:2703 */
+    if (H0Bottom)
+        for (int64_t i = 0; i < n; ++i) H0Bottom[i] = H0[i];
+    if (!m->second_moire) return;
+    /* HamOnSiteSecondMoireTerms, ham.F90:3546-3642: every atom, whatever its layer */
+    for (int64_t i = 0; i < n; ++i) {
+        double dx, dy, Hz, Hd;
+        second_moire_disp(m, Rat[3 * i], Rat[3 * i + 1], &dx, &dy);
+        if (m->rotate_first) {
+            dy = dy + m->shift2_y;
+            dx = dx + m->shift2_x;
+        }
+        if (m->sign2 < 0.0) {
+            dx = -dx;
+            dy = -dy;
+        }
+        moire_terms(m, dx, dy, &Hz, &Hd);
+        const double sgn = (species[i] % 2 == 1) ? -1.0 : 1.0;
+        H0[i] = H0[i] + (sgn * Hz * m->sign2 + Hd);
+    }
 }
 
-/* MoireBondDeltaMidpoint, ham.F90:4822-4883 (first moire: no post shift, no flips of Im) */
-static double moire_mid_delta(const orc_model* m, const double* ri, const double* bond, int spec, int flip)
+void orc_onsite(const orc_model* m, int64_t n, const double* Rat, const int32_t* species,
+                const int32_t* layer, double* H0)
+{
+    orc_onsite_layers(m, n, Rat, species, layer, H0, NULL);
+}
+
+/* MoireBondDeltaMidpoint, ham.F90:4822-4883: the bond term of one bond from the moire displacement at the
+ * bond's midpoint.  First moire: its own mismatch and twist, shift1 before the flip, no post shift, no flip
+ * of Im, no swap; second moire (ham.F90:7866-7869): eps * eps_factor, TwistAngle2, the flip, shift2 after
+ * it, and the flip of Im and the swap of del(2) and del(3) with the mass factor's sign. */
+static double mid_delta(const double* ri, const double* bond, int spec, double epsM, double thM, double pre_y,
+                        int flip, double post_x, double post_y, int flip_imag, int swap23, double Cab, double Phi,
+                        double aG)
 {
     if (spec != 1 && spec != 2) return 0.0;
     const double rm0 = ri[0] + 0.5 * bond[0], rm1 = ri[1] + 0.5 * bond[1];
-    const double th = m->moire_twisted ? m->twist_rad : 0.0;
-    double ddx = rm0 * ((1.0 + m->eps) * cos(th) - 1.0) - rm1 * (1.0 + m->eps) * sin(th);
-    double ddy = rm1 * ((1.0 + m->eps) * cos(th) - 1.0) + rm0 * (1.0 + m->eps) * sin(th);
-    ddy = ddy + m->shift1;
+    double ddx = rm0 * ((1.0 + epsM) * cos(thM) - 1.0) - rm1 * (1.0 + epsM) * sin(thM);
+    double ddy = rm1 * ((1.0 + epsM) * cos(thM) - 1.0) + rm0 * (1.0 + epsM) * sin(thM);
+    ddy = ddy + pre_y;
     if (flip) {
         ddx = -ddx;
         ddy = -ddy;
     }
-    ddx = ddx + 0.0;
-    ddy = ddy + 0.0;
+    ddx = ddx + post_x;
+    ddy = ddy + post_y;
     double re, im, del[3];
-    offdiago(ddx, ddy, m->Cab, m->Phiab, m->aG, &re, &im);
+    offdiago(ddx, ddy, Cab, Phi, aG, &re, &im);
+    if (flip_imag) im = -im;
     bond_deltas(spec, re, im, del);
-    if (fabs(bond[0]) < m->aG / 4.0) return del[0];
-    if (bond[0] < 0.0) return del[2];
-    return del[1];
+    if (fabs(bond[0]) < aG / 4.0) return del[0];
+    if (bond[0] < 0.0) return swap23 ? del[1] : del[2];
+    return swap23 ? del[2] : del[1];
+}
+
+static double moire_mid_delta(const orc_model* m, const double* ri, const double* bond, int spec, int flip)
+{
+    const double th = m->moire_twisted ? m->twist_rad : 0.0;
+    return mid_delta(ri, bond, spec, m->eps, th, m->shift1, flip, 0.0, 0.0, 0, 0, m->Cab, m->Phiab, m->aG);
 }
 
 /* F2G2 single-layer shell terms of HamHopIntralayerGraphene, ham.F90:10660-10925 (twoLayers/oneLayer). */
@@ -146,6 +212,68 @@ static double f2g2_shell(const orc_model* m, double dist)
  * intralayer HamHopIntralayerDefault (:10177-10194) or HamHopIntralayerGraphene
  * (:10616-10931); interlayer HamHopInterlayerTwoCenter (:9620-9838) with
  * interlayerTwoCenter (:4094-4110), or the gIntLay term (:6837-6840). */
+/* HamHopSecondMoire, ham.F90:7745-7880: a second pass over the bonds of each layer, after every other
+ * term, that subtracts the second moire's bond term from the first-shell bonds.  Its displacement is
+ * always rotated by Moire.TwistAngle2 (Moire.Twisted2 is not read here), flipped before the shift
+ * (the on-site term shifts first), and Im of the bond amplitude changes sign with the mass factor.
+ * delta carries over between the bonds of one atom, as in the reference (bonds with 0.01 <= |dx| <= 0.02
+ * keep the previous one).  The reference leaves del unset for species other than 1 and 2; the library's
+ * cells have only those two, and 0 stands there.  With Moire.OffDiagMidpoint the term of each bond comes
+ * from its midpoint (MoireBondDeltaMidpoint with the second moire's arguments, ham.F90:7866-7869). */
+static void second_moire_bonds(const orc_model* m, int64_t n, const double* Rat, const int32_t* species,
+                               const int32_t* layer, int32_t maxNeigh, const int32_t* Nneigh,
+                               const int32_t* NList, const double* NeighD, double* hopp)
+{
+    for (int64_t i = 0; i < n; ++i) {
+        double delta = 0.0;
+        double del[3] = {0.0, 0.0, 0.0};
+        const double x = Rat[3 * i], y = Rat[3 * i + 1], t = m->twist2_rad, e = m->eps * m->eps_factor;
+        double dx, dy;
+        if (m->rotate_first) {
+            dx = x * ((1.0 + e) * cos(t) - 1.0) - y * (1.0 + e) * sin(t);
+            dy = y * ((1.0 + e) * cos(t) - 1.0) + x * (1.0 + e) * sin(t);
+        } else {
+            const double ys = y - m->shift2 / m->eps / m->eps_factor;
+            dx = x * ((1.0 + e) * cos(t) - 1.0) - ys * (1.0 + m->eps) * sin(t);
+            dy = ys * ((1.0 + m->eps) * cos(t) - 1.0) + x * (1.0 + m->eps / m->eps_factor) * sin(t);
+        }
+        if (m->sign2 < 0.0) {
+            dx = -dx;
+            dy = -dy;
+        }
+        if (m->rotate_first) {
+            dx = dx + m->shift2_x;
+            dy = dy + m->shift2_y;
+        }
+        double re, im;
+        offdiago(dx, dy, m->Cab, m->Phiab, m->aG, &re, &im);
+        if (m->sign2 < 0.0) im = -im;
+        if (species[i] == 1 || species[i] == 2) bond_deltas(species[i], re, im, del);   /* ham.F90:7817-7833 */
+        for (int32_t j = 0; j < Nneigh[i]; ++j) {
+            const size_t e2 = (size_t)i * maxNeigh + j;
+            const int64_t jj = NList[e2] - 1;
+            if (layer[i] != layer[jj]) continue;
+            const double* D = NeighD + 3 * e2;
+            const double d = sqrt(D[0] * D[0] + D[1] * D[1]);
+            for (int lv = 0; lv < m->tbnn; ++lv) {
+                if (d < m->nradii[lv]) {
+                    if (fabs(D[0]) < 0.01) delta = del[0];
+                    else if (D[0] < -0.02) delta = (m->sign2 < 0.0) ? del[1] : del[2];
+                    else if (D[0] > 0.02) delta = (m->sign2 < 0.0) ? del[2] : del[1];
+                    if (m->moire_mid) {
+                        const int neg = m->sign2 < 0.0;
+                        delta = mid_delta(Rat + 3 * i, D, species[i], m->eps * m->eps_factor, m->twist2_rad, 0.0, neg,
+                                          m->shift2_x, m->shift2_y, neg, neg, m->Cab, m->Phiab, m->aG);
+                    }
+                    if (d > 1.7) delta = 0.0;
+                    hopp[2 * e2] = hopp[2 * e2] - 1.0 * delta;
+                    break;
+                }
+            }
+        }
+    }
+}
+
 void orc_hopping(const orc_model* m, int64_t n, const double* Rat, const int32_t* species,
                  const int32_t* layer, int32_t maxNeigh, const int32_t* Nneigh, const int32_t* NList,
                  const double* NeighD, double* hopp)
@@ -215,6 +343,8 @@ void orc_hopping(const orc_model* m, int64_t n, const double* Rat, const int32_t
             }
         }
     }
+    if (m->second_moire && m->moire_offdiag) second_moire_bonds(m, n, Rat, species, layer, maxNeigh, Nneigh, NList,
+                                                                NeighD, hopp);
 }
 
 /* HamPeierlsPeriodicGauge, ham.F90:12834-12882 (with the corner term). */

@@ -21,7 +21,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CASES = ["graphene", "graphene+NeighLevels1", "graphene+NeighLevels2", "graphene+NeighLevels3",
          "graphene+MagField1", "eff", "eff+MoireOffDiag", "eff+MoireOffDiagMidpoint", "eff+MoireTwisted",
-         "tbg", "tbg+MagField1"]
+         "eff+MoireAddSecondMoire", "eff+MoireAddSecondMoire+Midpoint", "eff+MoireAddSecondMoire+Twisted2",
+         "eff+MoireSecondMoireRotateFirst_off", "tbg", "tbg+MagField1"]
 
 
 def main(ref):

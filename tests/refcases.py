@@ -48,6 +48,12 @@ CASES = {
     "eff+MoireOffDiag": ("eff", {"MoireOffDiag": True, "MoireTwistAngle": 0.5}),
     "eff+MoireOffDiagMidpoint": ("eff", {"MoireOffDiag": True, "MoireOffDiagMidpoint": True}),
     "eff+MoireTwisted": ("eff", {"MoireTwisted": True, "MoireTwistAngle": 0.5}),
+    "eff+MoireAddSecondMoire": ("eff", {"MoireAddSecondMoire": True, "MoireOffDiag": True}),
+    "eff+MoireAddSecondMoire+Midpoint": ("eff", {"MoireAddSecondMoire": True, "MoireOffDiag": True,
+                                                 "MoireOffDiagMidpoint": True}),
+    "eff+MoireAddSecondMoire+Twisted2": ("eff", {"MoireAddSecondMoire": True, "MoireTwisted2": True,
+                                                 "MoireTwistAngle2": 0.5}),
+    "eff+MoireSecondMoireRotateFirst_off": ("eff", {"MoireAddSecondMoire": True, "MoireSecondMoireRotateFirst": False}),
     "tbg": ("tbg", {}),
     "tbg+MagField1": ("tbg", {"MagFieldInteger": 1}),
 }
@@ -117,8 +123,19 @@ def build(keys):
     m.twist_rad = g("MoireTwistAngle", 0.0) * math.pi / 180.0
     m.moire_offdiag = int(g("MoireOffDiag", False))
     m.moire_mid = int(g("MoireOffDiagMidpoint", False) and m.moire_offdiag)
-    m.shift1 = 0.0
-    m.sign1 = m.sign2 = 1.0
+    m.shift1 = g("MoireLayerShift1", 0.0)
+    m.sign1 = g("MoireFirstMoireMassFactor", 1.0)
+    m.sign2 = g("MoireSecondMoireMassFactor", 1.0)
+    # Moire.AddSecondMoire (ham.F90:2652-2704, 5859-5888)
+    m.second_moire = int(g("MoireAddSecondMoire", False))
+    m.eps_factor = g("LatticepercentFactor", 1.0)
+    m.twisted2 = int(g("MoireTwisted2", False))
+    m.twist2_rad = g("MoireTwistAngle2", 0.0) * math.pi / 180.0
+    m.rotate_first = int(g("MoireSecondMoireRotateFirst", True))
+    m.shift2 = g("MoireLayerShift2", 0.0)
+    phi2m = math.atan((1.0 + m.eps) * math.sin(m.twist2_rad) / ((1.0 + m.eps) * math.cos(m.twist2_rad) - 1.0))
+    m.shift2_x = m.shift2 * math.cos(phi2m)
+    m.shift2_y = m.shift2 * math.sin(phi2m)
     if bl in ("Koshino", "HTC"):
         m.interlayer = orc.INTER_TWO_CENTRE
     vpppi0 = g("Vpppi0", 2.7 if koshino_intra else 3.5)
@@ -139,7 +156,7 @@ def build(keys):
     rat = geo["rat"]
     rat_on = orc.roundtrip(rat, geo["ucell"]) if moire else rat
     rat_hop = orc.roundtrip(rat_on, geo["ucell"]) if moire else rat
-    h0 = orc.onsite(m, rat_on, geo["species"], geo["layer"])
+    h0, h0_bottom, h0_top = orc.onsite_layers(m, rat_on, geo["species"], geo["layer"])
     hop = orc.hopping(m, rat_hop, geo["species"], geo["layer"], nb)
     area = orc.cell_area(geo["ucell"])
     mb = g("MagFieldInteger", 0)
@@ -150,7 +167,8 @@ def build(keys):
     flux = 0.0
     if mb != 0:
         flux = mb * FLUXQ / (area * 1.0e-20) * math.pi / FLUXQ
-    return dict(geo=geo, nb=nb, h0=h0, hop=hop, g0=g0, model=m, area=area, rat_on=rat_on, rat_hop=rat_hop,
+    return dict(geo=geo, nb=nb, h0=h0, h0_bottom=h0_bottom, h0_top=h0_top, hop=hop, g0=g0, model=m, area=area,
+                rat_on=rat_on, rat_hop=rat_hop,
                 cut2intra=cut2intra, cut2inter=cut2inter, flux=flux, second_layer=g("AddSecondLayerInteractions", False))
 
 

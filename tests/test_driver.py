@@ -38,6 +38,13 @@ INPUTS = {
     },
     "anderson": {"Run.TypeOfSystem": "Graphene", "Structure.CellSize": 30, "Disorder.Anderson": True,
                  "Disorder.AndersonAmp": 1.0, "Kubo.SeedValue": 5, "TB.NeighLevels": 2},
+    "second_moire_former_names": {
+        "TypeOfSystem": "Graphene", "CellSize": 11, "SuperCell": 2, "Latticepercent": -1.0 / 11.0,
+        "MoirePotential": True, "MoireJeil": True, "MoireH0AndHZ": True, "MoireOffDiag": True,
+        "MoireAddSecondMoire": True, "LatticepercentFactor": 1.3, "MoireTwisted2": True, "MoireTwistAngle2": 0.7,
+        "MoireLayerShift2": 0.9, "MoireSecondMoireRotateFirst": False, "MoireSecondMoireMassFactor": -1.0,
+        "RecursionNumber": 50,
+    },
 }
 
 
@@ -85,9 +92,10 @@ def test_driver_reads_input_like_the_package(tmp_path, name):
     assert math.isclose(got["emin"], job["kubo"]["emin"], rel_tol=1e-15)
     m = job["model"]
     for f in ("tbnn", "intralayer", "moire_onsite", "moire_offdiag", "moire_mid", "moire_twisted", "interlayer",
-              "anderson", "koshino_sr", "renormalize_coupling"):
+              "anderson", "koshino_sr", "renormalize_coupling", "second_moire", "twisted2", "rotate_first"):
         assert got["model"][f] == getattr(m, f), f
-    for f in ("eps", "C0", "Cz", "Cab", "vpppi0", "vppsigma0", "bl_delta", "anderson_w", "coupling_factor"):
+    for f in ("eps", "C0", "Cz", "Cab", "vpppi0", "vppsigma0", "bl_delta", "anderson_w", "coupling_factor",
+              "eps_factor", "twist2_rad", "shift2_x", "shift2_y", "sign2"):
         assert math.isclose(got["model"][f], getattr(m, f), rel_tol=1e-15, abs_tol=1e-300), f
     assert got["cell_size"] == job["cell"]["cell_size"] and got["super_cell"] == job["cell"]["super_cell"]
     assert tuple(got["m"]) == tuple(job["cell"]["m"])
@@ -392,6 +400,41 @@ def test_driver_write_data_files(tmp_path):
     assert np.abs(cell[3:] @ u.T - 2 * np.pi * np.eye(3)).max() <= 1e-12
     labels = [line.split()[0] for line in open(tmp_path / "pos")]
     assert labels == ["C"] * n
+    bottom = np.loadtxt(tmp_path / "generate.bottom.e")
+    assert np.abs(bottom[:, 0] - r["h0_bottom"]).max() <= 1e-13
+    assert np.array_equal(bottom[:, 1].astype(int), geo["species"])
+    assert not (tmp_path / "generate.top.e").exists()
+
+
+@pytest.mark.gpu
+def test_driver_second_moire_files(tmp_path):
+    """Moire.AddSecondMoire with Output.WriteDataFiles: <prefix>.e, .bottom.e (H0 after the first moire) and
+    .top.e (the second moire's term, H0 - H0Bottom), ham.F90:7020-7034, and the hoppings with the second
+    moire's bond terms, against the oracle."""
+    import re
+    keys = dict(INPUTS["moire_sweep"], **{"Output.WriteDataFiles": True, "Kubo.RecursionNumber": 20,
+                                          "Moire.AddSecondMoire": True, "Moire.Twisted2": True,
+                                          "Moire.TwistAngle2": 0.7, "Moire.LatticePercentFactor": 1.3,
+                                          "Moire.LayerShift2": 0.9, "Moire.SecondMoireMassFactor": -1.0})
+    path = str(tmp_path / "Gendata.in")
+    _write(path, keys)
+    subprocess.run([DRIVER, path], check=True, cwd=str(tmp_path), capture_output=True, text=True)
+    r = R.build(dict(TypeOfSystem="Graphene", CellSize=11, SuperCell=4, LatticePercent=-1.0 / 11.0,
+                     MoirePotential=True, MoireJeil=True, MoireH0AndHZ=True, MoireOffDiag=True,
+                     MoireOffDiagMidpoint=True, MoireAddSecondMoire=True, MoireTwisted2=True, MoireTwistAngle2=0.7,
+                     LatticepercentFactor=1.3, MoireLayerShift2=0.9, MoireSecondMoireMassFactor=-1.0))
+    nb, geo = r["nb"], r["geo"]
+    mask = np.arange(nb["max_neigh"])[None, :] < nb["nneigh"][:, None]
+    pair = re.compile(r"\(\s*([-+0-9.Ee]+)\s*,\s*([-+0-9.Ee]+)\s*\)")
+    hop = [complex(float(a), float(b)) for line in open(tmp_path / "generate.s.mag") for a, b in pair.findall(line)]
+    assert np.abs(np.array(hop) - r["hop"][mask]).max() <= 1e-13
+    e = np.loadtxt(tmp_path / "generate.e")
+    assert np.abs(e[:, 0] - r["h0"]).max() <= 1e-13
+    bottom = np.loadtxt(tmp_path / "generate.bottom.e")
+    top = np.loadtxt(tmp_path / "generate.top.e")
+    assert np.abs(bottom[:, 0] - r["h0_bottom"]).max() <= 1e-13
+    assert np.abs(top[:, 0] - r["h0_top"]).max() <= 1e-13 and np.abs(top[:, 0]).max() > 1e-4
+    assert np.array_equal(top[:, 1].astype(int), geo["species"])
 
 
 @pytest.mark.gpu

@@ -41,6 +41,18 @@ CASES = {
                    CouplingFactor=1.008),
     # Anderson disorder (config 5 model) on graphene
     "anderson": dict(TypeOfSystem="Graphene", CellSize=30, Anderson=True, AndersonAmp=1.0, SeedValue=5),
+    # a second moire on the same graphene (Moire.AddSecondMoire): twisted, scaled mismatch, shifted, mass factor
+    # < 0 (flip, Im flip, del(2)/del(3) swap), bond terms at the midpoints, with Anderson disorder (added before
+    # the moire terms)
+    "moire_second": dict(TypeOfSystem="Graphene", CellSize=11, SuperCell=4, LatticePercent=-1.0 / 11.0,
+                         MoireAddSecondMoire=True, MoireTwisted2=True, MoireTwistAngle2=0.7, LatticepercentFactor=1.3,
+                         MoireLayerShift2=0.9, MoireSecondMoireMassFactor=-1.0, Anderson=True, AndersonAmp=0.2,
+                         SeedValue=9, **MOIRE),
+    # the same without SecondMoireRotateFirst (shift inside the rotation), per-atom bond terms
+    "moire_second_norot": dict(TypeOfSystem="Graphene", CellSize=11, SuperCell=4, LatticePercent=-1.0 / 11.0,
+                               MoirePotential=True, MoireJeil=True, MoireH0AndHZ=True, MoireOffDiag=True,
+                               MoireAddSecondMoire=True, MoireTwisted2=True, MoireTwistAngle2=-0.4,
+                               LatticepercentFactor=0.8, MoireLayerShift2=0.5, MoireSecondMoireRotateFirst=False),
 }
 
 _built = {}
@@ -89,6 +101,21 @@ def test_hamiltonian_assembly(ctx, name):
     h0, hop = ctx.hamiltonian()
     assert np.abs(h0 - r["h0"]).max() <= 1e-13
     assert np.abs(hop - r["hop"]).max() <= 1e-13
+
+
+@pytest.mark.parametrize("name", ["graphene", "moire_field", "moire_second", "moire_second_norot"])
+def test_onsite_bottom_and_top(ctx, name):
+    """gbn_get_onsite_layers: H0Bottom (after the first moire's terms) and H0Top (the second moire's) against
+    the oracle to 1e-13 g0; both 0 where the model has no moire branch, H0Top 0 without the second moire."""
+    r = built(name)
+    gpu_pipeline(ctx, r)
+    bottom, top = ctx.onsite_layers()
+    assert np.abs(bottom - r["h0_bottom"]).max() <= 1e-13
+    assert np.abs(top - r["h0_top"]).max() <= 1e-13
+    if name == "graphene":
+        assert not bottom.any() and not top.any()
+    if name.startswith("moire_second"):
+        assert np.abs(top).max() > 1e-4
 
 
 def _rel(x, y):

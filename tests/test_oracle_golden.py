@@ -68,3 +68,21 @@ def test_example07_twist_0p61():
                 MoireH0AndHZ=True, MoireOffDiag=True, MoireOffDiagMidpoint=True)
     e, d = _dos(keys, 1201, -0.6, 0.6, 0.005)
     assert np.abs(d - ref[:, 2]).max() < 1e-5
+
+
+@pytest.mark.parametrize("case", ["graphene", "eff", "eff+MoireAddSecondMoire", "eff+MoireAddSecondMoire+Twisted2"])
+def test_onsite_bottom_and_top(case):
+    """H0Bottom and H0Top of HamOnSite (ham.F90:2703, 3639): 0 without the moire branch; with it, H0Bottom is
+    the on-site energy after the first moire (the same model without the second moire gives it as H0), and
+    H0Top = H0 - H0Bottom is the second moire's term, 0 without one."""
+    r = R.build(R.case_keys(case))
+    h0, bottom, top = r["h0"], r["h0_bottom"], r["h0_top"]
+    if case == "graphene":
+        assert not bottom.any() and not top.any()
+        return
+    first = R.build(R.case_keys("eff"))["h0"]
+    assert np.array_equal(bottom, first)
+    if r["model"].second_moire:
+        assert np.array_equal(top, h0 - bottom) and np.abs(top).max() > 0.0
+    else:
+        assert np.array_equal(bottom, h0) and not top.any()
