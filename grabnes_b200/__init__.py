@@ -43,13 +43,17 @@ class Model(C.Structure):
         ("koshino_sr", C.c_int32), ("renormalize_coupling", C.c_int32), ("coupling_factor", C.c_double),
         ("second_moire", C.c_int32), ("eps_factor", C.c_double), ("twisted2", C.c_int32), ("twist2_rad", C.c_double),
         ("rotate_first", C.c_int32), ("shift2", C.c_double), ("shift2_x", C.c_double), ("shift2_y", C.c_double),
+        ("encapsulated", C.c_int32), ("bl_bottom_rad", C.c_double), ("bl_top_rad", C.c_double),
+        ("tau", C.c_double * 4), ("deact_upper", C.c_int32), ("deact_uppers", C.c_int32), ("bernal", C.c_int32),
+        ("tbl", C.c_double * 7),
     ]
 
 
 class Cell(C.Structure):
     """gbn_cell of include/grabnes_gpu.h"""
     _fields_ = [("kind", C.c_int32), ("cell_size", C.c_int32), ("super_cell", C.c_int32), ("m", C.c_int32 * 4),
-                ("aG", C.c_double), ("height", C.c_double), ("d_interlayer", C.c_double)]
+                ("aG", C.c_double), ("height", C.c_double), ("d_interlayer", C.c_double), ("add_shift", C.c_int32),
+                ("shift_factor", C.c_double)]
 
 
 CELL_GRAPHENE, CELL_TBG_MOIRE = 0, 1
@@ -490,9 +494,12 @@ def pdos_sets(p, species, layer, cap=4096):
     return so, sl[:k], ss[:k], asm[:k]
 
 
-def build_cell(kind, aG=2.46, cell_size=50, super_cell=1, m=(0, 0, 0, 0), height=40.0, d_interlayer=3.35):
-    """Atoms of a Graphene or TwistedBilayerBasedOnMoireCell cell, in the reference's order."""
-    p = Cell(kind, cell_size, super_cell, (C.c_int32 * 4)(*m), aG, height, d_interlayer)
+def build_cell(kind, aG=2.46, cell_size=50, super_cell=1, m=(0, 0, 0, 0), height=40.0, d_interlayer=3.35,
+               add_shift=0, shift_factor=0.0):
+    """Atoms of a Graphene or moire bilayer cell (TwistedBilayerBasedOnMoireCell,
+    MoireEncapsulatedBilayerBasedOnMoireCell), in the reference's order; add_shift 1 / 2 offsets the second
+    layer by the Bernal / bridge offset plus shift_factor [Ang] along a1+a2."""
+    p = Cell(kind, cell_size, super_cell, (C.c_int32 * 4)(*m), aG, height, d_interlayer, add_shift, shift_factor)
     n = C.c_int64()
     rc = lib().gbn_cell_atoms(C.byref(p), C.byref(n))
     if rc:

@@ -149,7 +149,7 @@ int gbn_destroy(gbn_ctx* c)
     DevBuf* bufs[] = {&c->rat, &c->species, &c->layer, &c->nneigh, &c->nlist, &c->neighd, &c->ncell, &c->h0,
                       &c->hopp, &c->rat_hop, &c->perm, &c->iperm, &c->ell.slice_ptr, &c->ell.mat,
                       &c->ell.h0, &c->ell.rperm, &c->ell.riperm, &c->ell.dval, &c->partials, &c->scal, &c->counter, &c->ab, &c->upload,
-                      &c->h0_bottom};
+                      &c->h0_bottom, &c->dimer};
     for (DevBuf* b : bufs) b->release();
     for (auto& v : c->vec) v.release();
     for (auto& v : c->cheb) v.release();
@@ -292,6 +292,10 @@ int gbn_assemble(gbn_ctx* c, const gbn_model* m, const double* rat_on, const dou
     if (!c->have_neigh || !c->have_neighd) return fail(c, GBN_ERR_STATE, "no neighbour tables: call gbn_neighbours first");
     if (m->tbnn < 1 || m->tbnn > 8) return fail(c, GBN_ERR_ARG, "tbnn must be in 1..8");
     if (m->anderson && !uniform) return fail(c, GBN_ERR_ARG, "Anderson disorder needs the uniform draws");
+    if (m->encapsulated && m->bernal != 1 && m->bernal != 2)
+        return fail(c, GBN_ERR_ARG, "the encapsulated bilayer needs bernal 1 (vertical pairs) or 2 (bilayer F2G2 set)");
+    if (m->encapsulated && !m->rotate_first && m->eps == 0.0 && (m->moire_onsite || m->moire_offdiag))
+        return fail(c, GBN_ERR_ARG, "the top layer's shift without rotate-first divides by the lattice mismatch");
     if (m->second_moire && !m->rotate_first &&
         ((m->twisted2 && m->moire_onsite && m->eps == 0.0) ||
          (m->moire_offdiag && (m->eps == 0.0 || m->eps_factor == 0.0))))

@@ -75,7 +75,7 @@ void moire_order(const int32_t m[4], int out[4], double* phi)
 }
 
 // one honeycomb layer of the supercell spanned by (mm0, mm1): fractional coordinates X[k][3]
-void honeycomb_layer(int mm0, int mm1, double angle_deg, double dz, double* X)
+void honeycomb_layer(int mm0, int mm1, double angle_deg, double dz, double yshift, double* X)
 {
     const int64_t ncell = (int64_t)mm0 * mm0 + (int64_t)mm0 * mm1 + (int64_t)mm1 * mm1;
     const double a = angle_deg * kPi / 180.0;
@@ -110,8 +110,8 @@ void honeycomb_layer(int mm0, int mm1, double angle_deg, double dz, double* X)
             f1 = (x[0] * R[1][1] - x[1] * R[0][1]) / dc;
             f2 = (x[1] * R[0][0] - x[0] * R[1][0]) / dc;
         }
-        x[0] = fmod(f1, 1.0);
-        x[1] = fmod(f2, 1.0);
+        x[0] = fmod(f1, 1.0) + yshift;
+        x[1] = fmod(f2, 1.0) + yshift;
         x[2] = 0.5 + dz;
         if (x[0] < 0.0) x[0] = fmod(x[0] + 1.0, 1.0);
         if (x[1] < 0.0) x[1] = fmod(x[1] + 1.0, 1.0);
@@ -213,7 +213,7 @@ int gbn_build_cell(const gbn_cell* p, double* ucell, double* rat, int32_t* speci
         ucell[3] = aG / 2.0 * dk;
         ucell[4] = sqrt(3.0) * aG / 2.0 * dk;
         ucell[8] = h;
-        honeycomb_layer(k, 0, 0.0, 0.0, rat);
+        honeycomb_layer(k, 0, 0.0, 0.0, 0.0, rat);
         for (int64_t i = 0; i < n; ++i) {
             species[i] = (int32_t)((i % 2) + 1);
             layer[i] = 1;
@@ -234,8 +234,15 @@ int gbn_build_cell(const gbn_cell* p, double* ucell, double* rat, int32_t* speci
     const int s = p->super_cell;
     const double g = p->d_interlayer / (2.0 * h);
     const int64_t nc = 2 * ((int64_t)o[0] * s * o[0] * s + (int64_t)o[0] * s * o[1] * s + (int64_t)o[1] * s * o[1] * s);
-    honeycomb_layer(o[0] * s, o[1] * s, 0.0, g, rat);
-    honeycomb_layer(o[2] * s, o[3] * s, -phi * 180.0 / kPi, -g, rat + 3 * nc);
+    // the second layer's offset (atoms.F90:352-366), from the indices after the swap and the super cell
+    double yshift = 0.0;
+    if (p->add_shift == 1 || p->add_shift == 2) {
+        const int a = o[0] * s, b = o[1] * s;
+        const double frac = p->shift_factor / (sqrt(3.0) * aG * sqrt((double)(a * a + a * b + b * b)));
+        yshift = (p->add_shift == 1) ? (aG / 3.0) / ((double)a * aG) + frac : (aG / 3.0 / 2.0) / ((double)a * aG) + frac;
+    }
+    honeycomb_layer(o[0] * s, o[1] * s, 0.0, g, 0.0, rat);
+    honeycomb_layer(o[2] * s, o[3] * s, -phi * 180.0 / kPi, -g, yshift, rat + 3 * nc);
     for (int64_t i = 0; i < n; ++i) species[i] = (int32_t)((i % 2) + 1);
     frac_to_cart(n, ucell, rat);
     for (int64_t i = 0; i < n; ++i) layer[i] = (rat[3 * i + 2] < 20.0) ? 1 : 2;

@@ -128,6 +128,8 @@ struct gbn_ctx {
     gbn::DevBuf h0_bottom; // double[n]: H0 after the first moire's terms (moire branch only)
     bool have_bottom = false;   // the assembled model ran the moire branch (h0_bottom is set)
     bool have_top = false;      // ... and the second moire (H0Top = H0 - H0Bottom)
+    gbn::DevBuf dimer;          // int8 [n] dimer sites of the Bernal interlayer branch, then a 64-bit count
+    int bernal_used = 0;        // the encapsulated bilayer's interlayer branch of the last assembly (0: none)
     bool have_ham = false;
     bool ham_complex = false;
     bool has_field = false;   // gbn_peierls has been applied to the assembled hoppings

@@ -81,6 +81,34 @@ __device__ void d_second_moire_disp(const gbn_model& m, double x, double y, doub
     }
 }
 
+// Displacement of the encapsulated bilayer's moire at (x, y) of layer L (HamOnSiteMoireEffectiveBilayer,
+// ham.F90:3318-3376, and the bond terms' copy, :12564-12585): layer 1 from the bottom hBN angle plus
+// (tauX1, tauY1); the other layer from the top angle plus (tauX2, tauY2), or, without rotate_first, with
+// tauY2 / eps taken off y before the rotation.
+__device__ void d_bilayer_disp(const gbn_model& m, int L, double x, double y, double* dx, double* dy)
+{
+    const double e1 = 1.0 + m.eps;
+    double st, ct;
+    sincos(L == 1 ? m.bl_bottom_rad : m.bl_top_rad, &st, &ct);
+    const double A = e1 * ct - 1.0, B = e1 * st;
+    if (L == 1 || m.rotate_first) {
+        *dx = A * x - (B * y);
+        *dy = A * y + (B * x);
+        *dx = *dx + (L == 1 ? m.tau[0] : m.tau[2]);
+        *dy = *dy + (L == 1 ? m.tau[1] : m.tau[3]);
+    } else {
+        const double ys = y - m.tau[3] / m.eps;
+        *dx = A * x - (B * ys);
+        *dy = A * ys + (B * x);
+    }
+}
+
+// Moire.BLDeactivateUpperLayer / TDBLDeactivateUpperLayers: no moire term on layer 2 / above layer 1
+__device__ __forceinline__ bool d_deactivated(const gbn_model& m, int L)
+{
+    return (L == 2 && m.deact_upper) || (L != 1 && m.deact_uppers);
+}
+
 __device__ __forceinline__ void d_moire_terms(const gbn_model& m, double dx, double dy, double* hz, double* hd)
 {
     *hz = 0.0;
@@ -104,15 +132,22 @@ __global__ void k_onsite(gbn_model m, int64_t n, const double* rat, const int32_
     double h = m.e0_c;
     if (m.anderson) h = h + (uniform[i] - 0.5) * m.anderson_w;
     const double sgn = (species[i] % 2 == 1) ? -1.0 : 1.0;
-    if (m.moire_onsite != 0) {
+    if (m.moire_onsite != 0 && m.encapsulated) {
+        // HamOnSiteMoireEffectiveBilayer (ham.F90:3303-3434): no mass factors, H0Bottom not set
+        double dx, dy, hz = 0.0, hd = 0.0;
+        const int L = layer[i];
+        d_bilayer_disp(m, L, rat[3 * i], rat[3 * i + 1], &dx, &dy);
+        if (L == 1 || !d_deactivated(m, L)) d_moire_terms(m, dx, dy, &hz, &hd);
+        h = h + sgn * hz + hd;
+    } else if (m.moire_onsite != 0) {
         double dx, dy, hz, hd;
         d_moire_disp(m, rat[3 * i], rat[3 * i + 1], &dx, &dy);
         dy = dy + m.shift1;
         const int L = layer[i];
         if ((L == 1 && m.sign1 < 0.0) || (L == 2 && m.sign2 < 0.0)) { dx = -dx; dy = -dy; }
         d_moire_terms(m, dx, dy, &hz, &hd);
-        if (L == 1) h = h + (sgn * hz * m.sign1 + hd);
-        else if (L == 2) h = h + (sgn * hz * m.sign2 + hd);
+        if (L == 1) h = h + sgn * hz * m.sign1 + hd;
+        else if (L == 2) h = h + sgn * hz * m.sign2 + hd;
         if (h0b) h0b[i] = h;
         if (m.second_moire) {
             d_second_moire_disp(m, rat[3 * i], rat[3 * i + 1], &dx, &dy);
@@ -122,7 +157,7 @@ __global__ void k_onsite(gbn_model m, int64_t n, const double* rat, const int32_
             }
             if (m.sign2 < 0.0) { dx = -dx; dy = -dy; }
             d_moire_terms(m, dx, dy, &hz, &hd);
-            h = h + (sgn * hz * m.sign2 + hd);
+            h = h + sgn * hz * m.sign2 + hd;
         }
     } else if (h0b) {
         h0b[i] = 0.0;
@@ -213,9 +248,28 @@ __device__ __forceinline__ double smooth_cut(const gbn_model& m, double rho)
     return 0.5 * (1.0 + cospi((rho - r0) / w));
 }
 
+// Dimer sites of the Bernal interlayer branch (ham.F90:6475-6484): an atom with a neighbour of an adjacent
+// layer within 0.2 A in plane; count gets their number.
+__global__ void k_dimer(int64_t n, const int32_t* layer, int32_t max_neigh, const int32_t* nneigh,
+                        const int32_t* nlist, const double* neighd, int8_t* dimer, unsigned long long* count)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int8_t d = 0;
+    for (int j = 0; j < nneigh[i]; ++j) {
+        const int64_t e = i * max_neigh + j;
+        const int Lj = layer[nlist[e] - 1];
+        if (layer[i] != Lj + 1 && layer[i] != Lj - 1) continue;
+        const double Dx = neighd[3 * e], Dy = neighd[3 * e + 1];
+        if (sqrt(Dx * Dx + Dy * Dy) < 0.2) d = 1;
+    }
+    dimer[i] = d;
+    if (d) atomicAdd(count, 1ULL);
+}
+
 __global__ void k_hopping(gbn_model m, int64_t n, const double* rat, const int32_t* species, const int32_t* layer,
                           int32_t max_neigh, const int32_t* nneigh, const int32_t* nlist, const double* neighd,
-                          double2* hopp)
+                          int bernal, const int8_t* dimer, double2* hopp)
 {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -225,11 +279,12 @@ __global__ void k_hopping(gbn_model m, int64_t n, const double* rat, const int32
     const bool flip = (Li == 1 && m.sign1 < 0.0) || (Li == 2 && m.sign2 < 0.0);
     const double rix = rat[3 * i], riy = rat[3 * i + 1];
     if (m.moire_offdiag) {
-        double dx, dy, re, im;
-        d_moire_disp(m, rix, riy, &dx, &dy);
+        double dx, dy, re = 0.0, im = 0.0;
+        if (m.encapsulated) d_bilayer_disp(m, Li, rix, riy, &dx, &dy);
+        else d_moire_disp(m, rix, riy, &dx, &dy);
         dy = dy + m.shift1;
         if (flip) { dx = -dx; dy = -dy; }
-        d_offdiago(dx, dy, m.Cab, m.Phiab, m.aG, &re, &im);
+        if (!d_deactivated(m, Li)) d_offdiago(dx, dy, m.Cab, m.Phiab, m.aG, &re, &im);
         if (si == 1 || si == 2) d_bond_deltas(si, re, im, del);
     }
     // the second moire's bond term (HamHopSecondMoire, ham.F90:7745-7880), a pass of its own in the
@@ -276,7 +331,20 @@ __global__ void k_hopping(gbn_model m, int64_t n, const double* rat, const int32
                     }
                 }
             } else if (Li == Lj + 1 || Li == Lj - 1) {
-                if (m.interlayer == 1) {
+                if (m.encapsulated) {
+                    // the encapsulated bilayer's interlayer branch (ham.F90:6721-6745)
+                    if (bernal == 2) {   // HamHopInterlayerBernalF2G2 (ham.F90:12800-12827)
+                        const bool mixed = dimer[i] != dimer[jj];
+                        const double dxy = sqrt(Dx * Dx + Dy * Dy), aCC = m.aCC, aG = m.aG;
+                        if (dxy < 0.2) hr = hr + m.tbl[4];
+                        else if (dxy > aCC * 0.9 && dxy < aCC * 1.1) hr = hr + (mixed ? m.tbl[0] : m.tbl[2]);
+                        else if (dxy > aG * 0.9 && dxy < aG * 1.1) hr = hr + m.tbl[5];
+                        else if (dxy > aCC * 2.0 * 0.9 && dxy < aCC * 2.0 * 1.1) hr = hr + (mixed ? m.tbl[1] : m.tbl[3]);
+                        else if (dxy > (aCC * 3.0) * 0.9 && dxy < (aCC * 3.0) * 1.1 && !mixed) hr = hr + m.tbl[6];
+                    } else if (fabs(Dx) < 0.01 && fabs(Dy) < 0.01) {
+                        hr = hr - m.tbl[2];
+                    }
+                } else if (m.interlayer == 1) {
                     const double dist = sqrt(Dx * Dx + Dy * Dy + Dz * Dz);
                     const double sr = m.koshino_sr ? exp((fabs(Dz) - 3.25) / 1.34) : 1.0;
                     const double vsig = m.vppsigma0 * exp(-(dist - m.d_interlayer) / m.bl_delta) * sr;
@@ -373,16 +441,36 @@ int assemble(gbn_ctx* c, const gbn_model* m, const double* d_rat_on, const doubl
     const unsigned grd = (unsigned)((n + 127) / 128);
     // H0Bottom is kept only for the moire branch (elsewhere it is 0 and nothing is stored)
     double* h0b = nullptr;
-    if (m->moire_onsite != 0) {
+    if (m->moire_onsite != 0 && !m->encapsulated) {
         GBN_CK(c, c->h0_bottom.ensure(sizeof(double) * n));
         h0b = c->h0_bottom.as<double>();
     }
     k_onsite<<<grd, 128, 0, c->stream>>>(*m, n, d_rat_on, c->species.as<int32_t>(), c->layer.as<int32_t>(), d_uniform,
                                          c->h0.as<double>(), h0b);
     GBN_CK_LAUNCH(c);
+    // the Bernal interlayer set needs an AB-stacked cell: half of the atoms dimer sites (to 10 %), else the
+    // vertical pairs only, as the reference decides (ham.F90:6473-6495)
+    int bernal = m->encapsulated ? m->bernal : 0;
+    const int8_t* dimer = nullptr;
+    if (bernal == 2) {
+        GBN_CK(c, c->dimer.ensure((size_t)n + sizeof(unsigned long long) + 8));
+        int8_t* dm = c->dimer.as<int8_t>();
+        unsigned long long* cnt = reinterpret_cast<unsigned long long*>(dm + ((n + 7) / 8) * 8);
+        GBN_CK(c, cudaMemsetAsync(cnt, 0, sizeof(unsigned long long), c->stream));
+        k_dimer<<<grd, 128, 0, c->stream>>>(n, c->layer.as<int32_t>(), c->max_neigh, c->nneigh.as<int32_t>(),
+                                            c->nlist.as<int32_t>(), c->neighd.as<double>(), dm, cnt);
+        GBN_CK_LAUNCH(c);
+        unsigned long long h_cnt = 0;
+        GBN_CK(c, cudaMemcpyAsync(&h_cnt, cnt, sizeof h_cnt, cudaMemcpyDeviceToHost, c->stream));
+        GBN_CK(c, cudaStreamSynchronize(c->stream));
+        const long long diff = 2LL * (long long)h_cnt - (long long)n;
+        if ((diff < 0 ? -diff : diff) > (long long)(n / 10)) bernal = 1;
+        dimer = dm;
+    }
+    c->bernal_used = bernal;
     k_hopping<<<grd, 128, 0, c->stream>>>(*m, n, d_rat_hop, c->species.as<int32_t>(), c->layer.as<int32_t>(),
                                           c->max_neigh, c->nneigh.as<int32_t>(), c->nlist.as<int32_t>(),
-                                          c->neighd.as<double>(), c->hopp.as<double2>());
+                                          c->neighd.as<double>(), bernal, dimer, c->hopp.as<double2>());
     GBN_CK_LAUNCH(c);
     c->have_ham = true;
     c->ham_complex = false;

@@ -307,6 +307,9 @@ struct Job {
     bool read_details = false;  // Neigh.ReadDetails
     gbn_pdos pdos{};        // Kubo.PDOS selection (mode 0: the DOS of the whole cell)
     int seed_set = 1235;    // Kubo.SeedSet: the stream of the layer start vectors
+    // moireBLShift.Calc: 0 off (the shifts stay 0), 1 Moire.BLShiftDefinedValues, 2 Moire.BLShiftRange
+    int bl_mode = 0, bl_steps = 0;
+    double bl_val[4] = {0, 0, 0, 0}, bl_min[4] = {0, 0, 0, 0}, bl_max[4] = {0, 0, 0, 0};
 };
 
 Job job_from_input(const Input& in)
@@ -314,9 +317,17 @@ Job job_from_input(const Input& in)
     Job j;
     const double aG = in.d("Structure.LatticeParameter", 2.46);
     const std::string system = in.s("Run.TypeOfSystem", "Graphene");
+    const bool encapsulated = lower(system) == "moireencapsulatedbilayerbasedonmoirecell";
     if (lower(system) == "graphene") j.cell.kind = GBN_CELL_GRAPHENE;
-    else if (lower(system) == "twistedbilayerbasedonmoirecell") j.cell.kind = GBN_CELL_TBG_MOIRE;
+    else if (lower(system) == "twistedbilayerbasedonmoirecell" || encapsulated) j.cell.kind = GBN_CELL_TBG_MOIRE;
     else die("Run.TypeOfSystem " + system + " is not on the recursion path of this program");
+    // Structure.TwistedBLAddShift (atoms.F90:352-366)
+    if (in.l("Structure.TwistedBLAddShift", false)) {
+        if (in.l("Structure.BernalShift", false)) j.cell.add_shift = 1;
+        else if (in.l("Structure.BridgeShift", false)) j.cell.add_shift = 2;
+        else die("TwistedBLAddShift needs BernalShift or BridgeShift to say which shift is added");
+        j.cell.shift_factor = in.d("Structure.BilayerShiftFactor", 0.0);
+    }
     if (!in.l("Kubo.Calc", true)) die("this program runs the recursion (Kubo.Calc .true.) only");
     if (in.l("Diag.Calc", false)) die("exact diagonalisation (Diag.Calc) is not part of this program");
     j.cell.aG = aG;
@@ -390,6 +401,52 @@ Job job_from_input(const Input& in)
         const double phi2m = atan((1.0 + m.eps) * sin(m.twist2_rad) / ((1.0 + m.eps) * cos(m.twist2_rad) - 1.0));
         m.shift2_x = m.shift2 * cos(phi2m);
         m.shift2_y = m.shift2 * sin(phi2m);
+    }
+    // MoireEncapsulatedBilayerBasedOnMoireCell (ham.F90:2607-2640, 5729-5780, 6455-6500)
+    m.encapsulated = encapsulated ? 1 : 0;
+    m.bl_bottom_rad = in.d("Moire.BilayerBottomAngle", 0.0) * kPi / 180.0;
+    m.bl_top_rad = in.d("Moire.BilayerTopAngle", 0.0) * kPi / 180.0;
+    m.deact_upper = in.l("Moire.BLDeactivateUpperLayer", false) ? 1 : 0;
+    m.deact_uppers = in.l("Moire.TDBLDeactivateUpperLayers", false) ? 1 : 0;
+    if (encapsulated) {
+        const bool f2g2 = in.l("Intralayer.F2G2Model", true) && !in.l("Intralayer.RemoveF2G2Flag", false);
+        const bool one = in.l("Interlayer.BilayerOneParameter", false);
+        if (in.l("Intralayer.BilayerThreeParameters", false) || !(f2g2 || one))
+            die("encapsulated bilayer: BilayerThreeParameters, or neither F2G2Model nor BilayerOneParameter, is not "
+                "on the recursion path of this program");
+        if (one) {
+            m.bernal = 1;
+            m.tbl[2] = -in.d("Intralayer.BilayertAB1", 0.361) / g0;
+        } else {
+            m.bernal = in.l("Interlayer.LegacyBernalTAB1", false) ? 1 : 2;
+            static const char* keys[7] = {"Intralayer.BilayertAA1", "Intralayer.BilayertAA3", "Intralayer.BilayertAB1",
+                                          "Intralayer.BilayertAB3", "Intralayer.BilayertBA0", "Intralayer.BilayertBA2",
+                                          "Intralayer.BilayertBA5"};
+            static const double dflt[7] = {0.09244, -0.02299, 0.1391, -0.07211, 0.331, -0.01016, 0.0001};
+            for (int k = 0; k < 7; ++k) m.tbl[k] = -in.d(keys[k], dflt[k]) / g0;
+        }
+    }
+    // moireBLShift.Calc (calc.F90:40-60, moireBLShift.F90): the rigid layer shifts tau of each calculation
+    if (in.l("moireBLShift.Calc", false)) {
+        if (in.l("Moire.BLShiftDefinedValues", false)) {
+            j.bl_mode = 1;
+            j.bl_val[0] = in.d("Moire.BilayerBottomXShift", 0.0);
+            j.bl_val[1] = in.d("Moire.BilayerBottomYShift", 0.0);
+            j.bl_val[2] = in.d("Moire.BilayerTopXShift", 0.0);
+            j.bl_val[3] = in.d("Moire.BilayerTopYShift", 0.0);
+        } else if (in.l("Moire.BLShiftRange", false)) {
+            j.bl_mode = 2;
+            j.bl_steps = (int)in.i("Moire.BLShiftRangeSteps", 10);
+            if (j.bl_steps < 1) die("Moire.BLShiftRangeSteps must be at least 1");
+            static const char* lo[4] = {"Moire.BilayerBottomXMin", "Moire.BilayerBottomYMin", "Moire.BilayerTopXMin",
+                                        "Moire.BilayerTopYMin"};
+            static const char* hi[4] = {"Moire.BilayerBottomXMax", "Moire.BilayerBottomYMax", "Moire.BilayerTopXMax",
+                                        "Moire.BilayerTopYMax"};
+            for (int k = 0; k < 4; ++k) {
+                j.bl_min[k] = in.d(lo[k], 0.0);
+                j.bl_max[k] = in.d(hi[k], 0.0);
+            }
+        }
     }
     if (bl == "Koshino" || bl == "HTC") m.interlayer = 1;
     m.vpppi0 = in.d("Interlayer.Vpppi0", koshino_intra ? 2.7 : 3.5) / g0;
@@ -585,10 +642,46 @@ Shard shard_from_env()
     return s;
 }
 
-// The (field, phase) units of the sweep in loop order (integer fields, before MagField.*B is resolved).
+// moireBLShiftValue (moireBLShift.F90:57-110): the layer shifts (tauX1, tauY1, tauX2, tauY2) of each
+// calculation of a moireBLShift.Calc sweep, tau = min + mS (max - min) / steps for mS = 0 .. steps, and for a
+// range its folder X1_<tauX1>_Y1_<tauY1>_X2_<tauX2>_Y2_<tauY2> (the f0.4 values).  Without a range: one
+// calculation, with the defined values or 0, in the run's own prefix.
+struct ShiftUnit {
+    double tau[4] = {0, 0, 0, 0};
+    std::string folder;
+};
+
+std::vector<ShiftUnit> shift_units(const Job& j)
+{
+    std::vector<ShiftUnit> out;
+    if (j.bl_mode == 2) {
+        for (int mS = 0; mS <= j.bl_steps; ++mS) {
+            ShiftUnit u;
+            for (int k = 0; k < 4; ++k)
+                u.tau[k] = j.bl_min[k] + (double)mS * (j.bl_max[k] - j.bl_min[k]) / (double)j.bl_steps;
+            char f[192];
+            snprintf(f, sizeof f, "X1_%.4f_Y1_%.4f_X2_%.4f_Y2_%.4f", u.tau[0], u.tau[1], u.tau[2], u.tau[3]);
+            u.folder = f;
+            out.push_back(u);
+        }
+    } else {
+        ShiftUnit u;
+        if (j.bl_mode == 1)
+            for (int k = 0; k < 4; ++k) u.tau[k] = j.bl_val[k];
+        out.push_back(u);
+    }
+    return out;
+}
+
+// The (field, phase) units of the sweep in loop order (integer fields, before MagField.*B is resolved); for
+// a layer-shift range, its shifts (mS, 0).
 std::vector<std::pair<long, long>> sweep_units(const Job& j)
 {
     std::vector<std::pair<long, long>> u;
+    if (j.bl_mode == 2) {
+        for (long mS = 0; mS <= j.bl_steps; ++mS) u.push_back({mS, 0});
+        return u;
+    }
     const bool magfield = !(j.mbi == 0 && j.mbf == 0), hsweep = j.mphii != j.mphif;
     for (long mb = j.mbi; mb <= j.mbf; mb += (magfield ? j.mstep : 1)) {
         for (long mphi = j.mphii; mphi <= j.mphif; mphi += j.mphistep) {
@@ -625,7 +718,10 @@ void print_job(const Job& j)
            "\"vpppi0\": %.17g, \"vppsigma0\": %.17g, \"bl_delta\": %.17g, \"anderson\": %d, \"anderson_w\": %.17g, "
            "\"tksl2\": %.17g, \"koshino_sr\": %d, \"renormalize_coupling\": %d, \"coupling_factor\": %.17g, "
            "\"second_moire\": %d, \"eps_factor\": %.17g, \"twisted2\": %d, \"twist2_rad\": %.17g, "
-           "\"rotate_first\": %d, \"shift2_x\": %.17g, \"shift2_y\": %.17g, \"sign2\": %.17g}}\n",
+           "\"rotate_first\": %d, \"shift2_x\": %.17g, \"shift2_y\": %.17g, \"sign2\": %.17g, "
+           "\"encapsulated\": %d, \"bl_bottom_rad\": %.17g, \"bl_top_rad\": %.17g, \"deact_upper\": %d, "
+           "\"deact_uppers\": %d, \"bernal\": %d, \"tbl\": [%.17g, %.17g, %.17g, %.17g, %.17g, %.17g, %.17g]}, "
+           "\"add_shift\": %d, \"shift_factor\": %.17g, \"bl_mode\": %d, \"bl_steps\": %d}\n",
            j.cell.kind, j.cell.aG, j.cell.cell_size, j.cell.super_cell, j.cell.m[0], j.cell.m[1], j.cell.m[2], j.cell.m[3],
            j.cell.height, j.cell.d_interlayer, j.g0, j.cut2intra, j.cut2inter, (int)j.second_layer, (int)j.moire,
            j.nrecurs, j.eta, j.n_en, j.emin, j.emax, j.seed, j.prefix.c_str(), (int)j.only_dos, j.npol, j.nt, j.nwr,
@@ -633,7 +729,9 @@ void print_job(const Job& j)
            m.moire_offdiag, m.moire_mid, m.moire_twisted, m.eps, m.twist_rad, m.C0, m.Cz, m.Cab, m.interlayer,
            m.vpppi0, m.vppsigma0, m.bl_delta, m.anderson, m.anderson_w, m.tksl[2], m.koshino_sr,
            m.renormalize_coupling, m.coupling_factor, m.second_moire, m.eps_factor, m.twisted2, m.twist2_rad,
-           m.rotate_first, m.shift2_x, m.shift2_y, m.sign2);
+           m.rotate_first, m.shift2_x, m.shift2_y, m.sign2, m.encapsulated, m.bl_bottom_rad, m.bl_top_rad,
+           m.deact_upper, m.deact_uppers, m.bernal, m.tbl[0], m.tbl[1], m.tbl[2], m.tbl[3], m.tbl[4], m.tbl[5],
+           m.tbl[6], j.cell.add_shift, j.cell.shift_factor, j.bl_mode, j.bl_steps);
 }
 
 void write_pairs(const std::string& path, const std::vector<double>& x, const std::vector<double>& y, double head,
@@ -1147,8 +1245,16 @@ int run(const Job& j0)
     std::vector<double> u((size_t)n);
     ck(gbn_rng_uniform(j.seed, n, u.data()), nullptr, "gbn_rng_uniform");
     const bool magfield = !(j.mbi == 0 && j.mbf == 0);
+    const std::vector<ShiftUnit> shifts = shift_units(j);
+    const bool shift_sweep = shifts.size() > 1;
+    // the reference names the folder of every field (or Haldane phase) after the field alone, so that a
+    // layer-shift range combined with a field or phase sweep writes all shifts into the same folders
+    if (shift_sweep && ((magfield && j.mbi != j.mbf) || j.mphii != j.mphif))
+        die("a moireBLShift range combined with a field or Haldane phase sweep writes every shift into the same "
+            "folders; run the shifts and the fields as separate jobs");
+    for (int k = 0; k < 4; ++k) j.model.tau[k] = shifts[0].tau[k];
     std::vector<double> a((size_t)j.nrecurs), b((size_t)j.nrecurs), psi;
-    if (magfield && j.mbi != j.mbf && j.pdos.mode == 0 && j.only_dos && !j.read_data && !j.write_data && !j.haldane &&
+    if (!shift_sweep && magfield && j.mbi != j.mbf && j.pdos.mode == 0 && j.only_dos && !j.read_data && !j.write_data && !j.haldane &&
         j.mphii == j.mphif) {
         // a DOS-only sweep: all fields in one batch from the field-free Hamiltonian, each field's Peierls
         // phases applied on the fly (the reference reseeds, so every field starts from the same vector)
@@ -1189,13 +1295,22 @@ int run(const Job& j0)
     }
     const bool hsweep = j.mphii != j.mphif;   // HaldPhaseInit: a Haldane phase sweep
     long unit = -1;
+    for (size_t sh = 0; sh < shifts.size(); ++sh) {   // moireBLShift.Calc: HamOnSite and HamHopping per shift
+    std::string base = j.prefix;
+    if (shift_sweep) {
+        if (!shard.mine((long)sh)) continue;   // another rank's shift
+        for (int k = 0; k < 4; ++k) j.model.tau[k] = shifts[sh].tau[k];
+        printf("grabnes: layer shift %zu of 0..%zu (tauX1 %.4f tauY1 %.4f tauX2 %.4f tauY2 %.4f)\n", sh,
+               shifts.size() - 1, shifts[sh].tau[0], shifts[sh].tau[1], shifts[sh].tau[2], shifts[sh].tau[3]);
+        base = make_folder(shifts[sh].folder, j.prefix);
+    }
     for (long mb = j.mbi; mb <= j.mbf; mb += (magfield ? j.mstep : 1))
     for (long mphi = j.mphii; mphi <= j.mphif; mphi += j.mphistep) {
-        if (!shard.mine(++unit)) {   // another rank's unit
+        if (!shift_sweep && !shard.mine(++unit)) {   // another rank's unit
             if (!magfield && !hsweep) break;
             continue;
         }
-        std::string prefix = j.prefix;
+        std::string prefix = base;
         if (magfield && j.mbi != j.mbf) {
             const double bmag = mb * kFluxQuantum / (area * 1.0e-20);
             char folder[64];
@@ -1255,6 +1370,7 @@ int run(const Job& j0)
             else printf("grabnes: the PDOS selection is empty: no time evolution\n");
         }
         if (!magfield && !hsweep) break;
+    }
     }
     gbn_destroy(ctx);
     return 0;

@@ -65,12 +65,23 @@ def job_from_keys(keys):
     g = k.get
     aG = g("Structure.LatticeParameter", 2.46)
     system = g("Run.TypeOfSystem", "Graphene")
-    kind = {"graphene": CELL_GRAPHENE, "twistedbilayerbasedonmoirecell": CELL_TBG_MOIRE}.get(system.lower())
+    kind = {"graphene": CELL_GRAPHENE, "twistedbilayerbasedonmoirecell": CELL_TBG_MOIRE,
+            "moireencapsulatedbilayerbasedonmoirecell": CELL_TBG_MOIRE}.get(system.lower())
     if kind is None:
         raise ValueError(f"Run.TypeOfSystem {system} is not on the recursion path of this library")
+    encapsulated = system.lower() == "moireencapsulatedbilayerbasedonmoirecell"
+    add_shift, shift_factor = 0, 0.0
+    if g("Structure.TwistedBLAddShift", False):   # atoms.F90:352-366
+        if g("Structure.BernalShift", False):
+            add_shift = 1
+        elif g("Structure.BridgeShift", False):
+            add_shift = 2
+        else:
+            raise ValueError("TwistedBLAddShift needs BernalShift or BridgeShift to say which shift is added")
+        shift_factor = g("Structure.BilayerShiftFactor", 0.0)
     cell = dict(kind=kind, aG=aG, cell_size=g("Structure.CellSize", 50), super_cell=g("Structure.SuperCell", 1),
                 m=tuple(g("Structure.MoireCellParameters", (0, 0, 0, 0))), height=g("Structure.CellHeight", 40.0),
-                d_interlayer=g("Structure.InterlayerDistance", 3.35))
+                d_interlayer=g("Structure.InterlayerDistance", 3.35), add_shift=add_shift, shift_factor=shift_factor)
     g0 = g("TB.Hopping", -3.72 * aG + 12.14)
     tbnn = g("TB.NeighLevels", 1)
     if not 1 <= tbnn <= 8:
@@ -131,6 +142,28 @@ def job_from_keys(keys):
     phi2m = math.atan((1.0 + m.eps) * math.sin(m.twist2_rad) / ((1.0 + m.eps) * math.cos(m.twist2_rad) - 1.0))
     m.shift2_x = m.shift2 * math.cos(phi2m)
     m.shift2_y = m.shift2 * math.sin(phi2m)
+    # MoireEncapsulatedBilayerBasedOnMoireCell (ham.F90:2607-2640, 5729-5780, 6455-6500)
+    m.encapsulated = int(encapsulated)
+    m.bl_bottom_rad = g("Moire.BilayerBottomAngle", 0.0) * math.pi / 180.0
+    m.bl_top_rad = g("Moire.BilayerTopAngle", 0.0) * math.pi / 180.0
+    m.deact_upper = int(bool(g("Moire.BLDeactivateUpperLayer", False)))
+    m.deact_uppers = int(bool(g("Moire.TDBLDeactivateUpperLayers", False)))
+    if encapsulated:
+        f2g2 = g("Intralayer.F2G2Model", True) and not g("Intralayer.RemoveF2G2Flag", False)
+        one = g("Interlayer.BilayerOneParameter", False)
+        if g("Intralayer.BilayerThreeParameters", False) or not (f2g2 or one):
+            raise ValueError("encapsulated bilayer: BilayerThreeParameters, or neither F2G2Model nor "
+                             "BilayerOneParameter, is not on the recursion path of this library")
+        if one:
+            m.bernal = 1
+            m.tbl[2] = -g("Intralayer.BilayertAB1", 0.361) / g0
+        else:
+            m.bernal = 1 if g("Interlayer.LegacyBernalTAB1", False) else 2
+            for t, (key, dflt) in enumerate(BERNAL_F2G2):
+                m.tbl[t] = -g(key, dflt) / g0
+    shifts = blshift_units(k)
+    for i in range(4):
+        m.tau[i] = shifts[0][0][i]
     if bl in ("Koshino", "HTC"):
         m.interlayer = 1
     m.vpppi0 = g("Interlayer.Vpppi0", 2.7 if koshino_intra else 3.5) / g0
@@ -153,6 +186,39 @@ def job_from_keys(keys):
                 nwr=g("Kubo.WriteNumberofSteps", 10))
     return dict(cell=cell, g0=g0, cut2intra=cut2intra, cut2inter=cut2inter,
                 second_layer=bool(g("Interlayer.AddSecondLayerInteractions", False)), model=m, moire=moire, kubo=kubo)
+
+
+# the bilayer F2G2 interlayer set (ham.F90:5756-5779): tAA1, tAA2 (key BilayertAA3), tAB1, tAB2 (key
+# BilayertAB3), tBA0, tBA2, tBA5 [eV]
+BERNAL_F2G2 = (("Intralayer.BilayertAA1", 0.09244), ("Intralayer.BilayertAA3", -0.02299),
+               ("Intralayer.BilayertAB1", 0.1391), ("Intralayer.BilayertAB3", -0.07211),
+               ("Intralayer.BilayertBA0", 0.331), ("Intralayer.BilayertBA2", -0.01016),
+               ("Intralayer.BilayertBA5", 0.0001))
+
+
+def blshift_units(keys):
+    """The layer shifts (tauX1, tauY1, tauX2, tauY2) [Ang] of each calculation of a moireBLShift.Calc sweep
+    (calc.F90:40-60, moireBLShift.F90:17-110) with its folder name, or None for the run's own prefix:
+    Moire.BLShiftRange gives tau = min + mS (max - min) / steps for mS = 0 .. Moire.BLShiftRangeSteps, in
+    folders X1_<tauX1>_Y1_<tauY1>_X2_<tauX2>_Y2_<tauY2>; Moire.BLShiftDefinedValues one calculation with
+    the Moire.Bilayer{Bottom,Top}{X,Y}Shift values; otherwise one calculation with no shift."""
+    k = keys if isinstance(keys, Keys) else Keys(keys)
+    g = k.get
+    if not g("moireBLShift.Calc", False):
+        return [((0.0, 0.0, 0.0, 0.0), None)]
+    names = ("Moire.BilayerBottomX", "Moire.BilayerBottomY", "Moire.BilayerTopX", "Moire.BilayerTopY")
+    if g("Moire.BLShiftDefinedValues", False):
+        return [(tuple(g(n + "Shift", 0.0) for n in names), None)]
+    if not g("Moire.BLShiftRange", False):
+        return [((0.0, 0.0, 0.0, 0.0), None)]
+    steps = g("Moire.BLShiftRangeSteps", 10)
+    if steps < 1:
+        raise ValueError("Moire.BLShiftRangeSteps must be at least 1")
+    out = []
+    for ms in range(steps + 1):
+        tau = tuple(g(n + "Min", 0.0) + ms * (g(n + "Max", 0.0) - g(n + "Min", 0.0)) / steps for n in names)
+        out.append((tau, "X1_%.4f_Y1_%.4f_X2_%.4f_Y2_%.4f" % tau))
+    return out
 
 
 def flux_of(m_quanta, area):

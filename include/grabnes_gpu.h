@@ -85,11 +85,28 @@ typedef struct gbn_model {
     int32_t rotate_first;
     double  shift2;
     double  shift2_x, shift2_y;
+    /* Run.TypeOfSystem MoireEncapsulatedBilayerBasedOnMoireCell: the effective moire on-site model of the
+     * encapsulated bilayer (HamOnSiteMoireEffectiveBilayer, ham.F90:3303-3434) and its bond displacement
+     * (ham.F90:12561-12590): bottom / top hBN angles (Moire.BilayerBottomAngle, TopAngle) [rad] and the rigid
+     * layer shifts tauX1, tauY1, tauX2, tauY2 of moireBLShift [Ang]; the top layer's displacement takes the
+     * rotation first with rotate_first.  deact_upper / deact_uppers: Moire.BLDeactivateUpperLayer /
+     * TDBLDeactivateUpperLayers (no moire term on layer 2 / above layer 1; the bond terms of every system).
+     * bernal: its interlayer branch (ham.F90:6455-6500, 6721-6745): 1 the vertical pairs only (-tAB1),
+     * 2 the bilayer F2G2 set of HamHopInterlayerBernalF2G2 (ham.F90:12800-12827) on an AB-stacked cell (dimer
+     * sites found from the structure; a cell that is not AB stacked falls back to 1 as in the reference).
+     * tbl: tAA1, tAA2, tAB1, tAB2, tBA0, tBA2, tBA5 as the reference stores them (-t/g0). */
+    int32_t encapsulated;
+    double  bl_bottom_rad, bl_top_rad;
+    double  tau[4];
+    int32_t deact_upper, deact_uppers;
+    int32_t bernal;
+    double  tbl[7];
 } gbn_model;
 
 /* ---- host-side cell construction and random numbers (no context, no GPU needed) ------ */
 #define GBN_CELL_GRAPHENE 0  /* Run.TypeOfSystem Graphene                       */
-#define GBN_CELL_TBG_MOIRE 1 /* Run.TypeOfSystem TwistedBilayerBasedOnMoireCell */
+#define GBN_CELL_TBG_MOIRE 1 /* Run.TypeOfSystem TwistedBilayerBasedOnMoireCell, and the same cell of
+                                MoireEncapsulatedBilayerBasedOnMoireCell (atoms.F90:455-512) */
 typedef struct gbn_cell {
     int32_t kind;         /* GBN_CELL_*                                   */
     int32_t cell_size;    /* Structure.CellSize (graphene)                */
@@ -98,6 +115,11 @@ typedef struct gbn_cell {
     double  aG;           /* Structure.LatticeParameter [Ang]             */
     double  height;       /* Structure.CellHeight [Ang]                   */
     double  d_interlayer; /* Structure.InterlayerDistance [Ang]           */
+    /* Structure.TwistedBLAddShift (atoms.F90:352-366): the moire cell's second layer offset by 1 the
+     * Bernal (Structure.BernalShift) or 2 the bridge (Structure.BridgeShift) offset, plus
+     * Structure.BilayerShiftFactor [Ang] along a1+a2 (AtomsShiftFrac, atoms.F90:1490-1504); 0: none */
+    int32_t add_shift;
+    double  shift_factor;
 } gbn_cell;
 /* Number of atoms of the cell (CellGet/AtomsPos, lanczosKuboCode/Src/cell.F90:108-140, 207-240). */
 int gbn_cell_atoms(const gbn_cell* cell, int64_t* n);

@@ -42,6 +42,11 @@ typedef struct {
     double  aG;            /* Structure.LatticeParameter [Ang]            */
     double  height;        /* Structure.CellHeight [Ang]                  */
     double  d_interlayer;  /* Structure.InterlayerDistance [Ang]          */
+    /* Structure.TwistedBLAddShift of the moire cell's second layer (atoms.F90:352-366): 0 none, 1 the
+     * Bernal offset (Structure.BernalShift), 2 the bridge offset (Structure.BridgeShift); plus
+     * Structure.BilayerShiftFactor [Ang] along a1+a2 (AtomsShiftFrac, atoms.F90:1490-1504) */
+    int32_t add_shift;
+    double  shift_factor;
 } orc_geom_params;
 
 int64_t orc_geom_natoms(const orc_geom_params* p);
@@ -114,6 +119,15 @@ typedef struct {
     int32_t rotate_first;      /* Moire.SecondMoireRotateFirst                     */
     double  shift2;            /* Moire.LayerShift2 [Ang]                          */
     double  shift2_x, shift2_y; /* shift2 (cos, sin) phi2M, ham.F90:2688-2690      */
+    /* MoireEncapsulatedBilayerBasedOnMoireCell: HamOnSiteMoireEffectiveBilayer (ham.F90:3303-3434), its bond
+     * displacement (ham.F90:12561-12590) and its interlayer branch (ham.F90:6455-6500, 6721-6745, 12800-12827) */
+    int32_t encapsulated;
+    double  bl_bottom_rad, bl_top_rad; /* Moire.BilayerBottomAngle / TopAngle [rad]       */
+    double  tau[4];            /* tauX1, tauY1, tauX2, tauY2 (moireBLShift) [Ang]      */
+    int32_t deact_upper;       /* Moire.BLDeactivateUpperLayer                     */
+    int32_t deact_uppers;      /* Moire.TDBLDeactivateUpperLayers                  */
+    int32_t bernal;            /* 1 vertical pairs (-tAB1), 2 bilayer F2G2 set      */
+    double  tbl[7];            /* tAA1 tAA2 tAB1 tAB2 tBA0 tBA2 tBA5 (-t/g0)          */
 } orc_model;
 
 void orc_onsite(const orc_model* m, int64_t n, const double* Rat,
@@ -122,6 +136,8 @@ void orc_onsite(const orc_model* m, int64_t n, const double* Rat,
  * moire branch runs, else 0.  H0Top = H0 - H0Bottom when the second moire runs (ham.F90:3639), else 0. */
 void orc_onsite_layers(const orc_model* m, int64_t n, const double* Rat, const int32_t* species,
                        const int32_t* layer, double* H0, double* H0Bottom);
+int64_t orc_bernal_dimers(int64_t n, const int32_t* layer, int32_t maxNeigh, const int32_t* Nneigh,
+                          const int32_t* NList, const double* NeighD, int8_t* dimer);
 void orc_hopping(const orc_model* m, int64_t n, const double* Rat,
                  const int32_t* species, const int32_t* layer,
                  int32_t maxNeigh, const int32_t* Nneigh, const int32_t* NList,

@@ -26,7 +26,7 @@ ONSITE_NONE, ONSITE_H0_AND_HZ, ONSITE_ONLY_H0, ONSITE_ONLY_HZ, ONSITE_NO_H0_AND_
 class GeomParams(C.Structure):
     _fields_ = [("kind", C.c_int32), ("cell_size", C.c_int32), ("super_cell", C.c_int32),
                 ("m", C.c_int32 * 4), ("aG", C.c_double), ("height", C.c_double),
-                ("d_interlayer", C.c_double)]
+                ("d_interlayer", C.c_double), ("add_shift", C.c_int32), ("shift_factor", C.c_double)]
 
 
 class Model(C.Structure):
@@ -44,6 +44,9 @@ class Model(C.Structure):
         ("inter_smooth_w", C.c_double), ("inter_cut_rho", C.c_double),
         ("second_moire", C.c_int32), ("eps_factor", C.c_double), ("twisted2", C.c_int32), ("twist2_rad", C.c_double),
         ("rotate_first", C.c_int32), ("shift2", C.c_double), ("shift2_x", C.c_double), ("shift2_y", C.c_double),
+        ("encapsulated", C.c_int32), ("bl_bottom_rad", C.c_double), ("bl_top_rad", C.c_double),
+        ("tau", C.c_double * 4), ("deact_upper", C.c_int32), ("deact_uppers", C.c_int32), ("bernal", C.c_int32),
+        ("tbl", C.c_double * 7),
     ]
 
 
@@ -115,8 +118,9 @@ def rng_draws(seed, n):
     return out
 
 
-def geometry(kind, aG=2.46, cell_size=50, super_cell=1, m=(0, 0, 0, 0), height=40.0, d_interlayer=3.35):
-    p = GeomParams(kind, cell_size, super_cell, (C.c_int32 * 4)(*m), aG, height, d_interlayer)
+def geometry(kind, aG=2.46, cell_size=50, super_cell=1, m=(0, 0, 0, 0), height=40.0, d_interlayer=3.35,
+             add_shift=0, shift_factor=0.0):
+    p = GeomParams(kind, cell_size, super_cell, (C.c_int32 * 4)(*m), aG, height, d_interlayer, add_shift, shift_factor)
     n = lib().orc_geom_natoms(C.byref(p))
     ucell = np.zeros(9, np.float64)
     rat = np.zeros(3 * n, np.float64)

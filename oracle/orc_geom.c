@@ -242,8 +242,16 @@ int orc_geom_build(const orc_geom_params* p, double* ucell, double* Rat, int32_t
     const double g = p->d_interlayer / (2.0 * h);
     const int64_t natc = 2 * ((int64_t)nn[0] * nn[0] + (int64_t)nn[0] * nn[1] + (int64_t)nn[1] * nn[1]);
     const int64_t natb = 2 * ((int64_t)nn[2] * nn[2] + (int64_t)nn[2] * nn[3] + (int64_t)nn[3] * nn[3]);
+    /* atoms.F90:352-366: the second layer's offset, from the indices after the swap and the super cell */
+    double yshift = 0.0;
+    if (p->add_shift == 1 || p->add_shift == 2) {
+        const double frac = p->shift_factor /
+                            (sqrt(3.0) * aG * sqrt((double)(nn[0] * nn[0] + nn[0] * nn[1] + nn[1] * nn[1])));
+        yshift = (p->add_shift == 1) ? (aG / 3.0) / ((double)nn[0] * aG) + frac
+                                     : (aG / 3.0 / 2.0) / ((double)nn[0] * aG) + frac;
+    }
     atoms_construct(nn[0], nn[1], 0.0, g, 0.0, Rat);
-    atoms_construct(nn[2], nn[3], -phi * 180.0 / ORC_PI, -g, 0.0, Rat + 3 * natc);
+    atoms_construct(nn[2], nn[3], -phi * 180.0 / ORC_PI, -g, yshift, Rat + 3 * natc);
     const int64_t nat = natc + natb;
     for (int64_t i = 0; i < nat; ++i) species[i] = (int32_t)(((i + 2) % 2) + 1);
     set_cart(nat, ucell, Rat);

@@ -84,6 +84,38 @@ static void second_moire_disp(const orc_model* m, double x, double y, double* dx
     }
 }
 
+/* Displacement of the encapsulated bilayer's moire at atom (x, y) of layer L (HamOnSiteMoireEffectiveBilayer,
+ * ham.F90:3318-3376, and the same lines of the bond terms, :12564-12585): layer 1 from the bottom hBN angle
+ * plus (tauX1, tauY1), the other layer from the top angle with (tauX2, tauY2) added after the rotation, or,
+ * without rotate_first, tauY2 / eps taken off y before it. */
+static void bilayer_disp(const orc_model* m, int L, double x, double y, double* dx, double* dy)
+{
+    const double e1 = 1.0 + m->eps;
+    if (L == 1) {
+        const double a = m->bl_bottom_rad;
+        *dx = (e1 * cos(a) - 1.0) * x - (e1 * sin(a) * y);
+        *dy = (e1 * cos(a) - 1.0) * y + (e1 * sin(a) * x);
+        *dx = *dx + m->tau[0];
+        *dy = *dy + m->tau[1];
+    } else if (m->rotate_first) {
+        const double a = m->bl_top_rad;
+        *dx = (e1 * cos(a) - 1.0) * x - (e1 * sin(a) * y);
+        *dy = (e1 * cos(a) - 1.0) * y + (e1 * sin(a) * x);
+        *dx = *dx + m->tau[2];
+        *dy = *dy + m->tau[3];
+    } else {
+        const double a = m->bl_top_rad, ys = y - m->tau[3] / m->eps;
+        *dx = (e1 * cos(a) - 1.0) * x - (e1 * sin(a) * ys);
+        *dy = (e1 * cos(a) - 1.0) * ys + (e1 * sin(a) * x);
+    }
+}
+
+/* Moire.BLDeactivateUpperLayer / TDBLDeactivateUpperLayers: no moire term on layer 2 / above layer 1 */
+static int deactivated(const orc_model* m, int L)
+{
+    return (L == 2 && m->deact_upper) || (L != 1 && m->deact_uppers);
+}
+
 static void moire_terms(const orc_model* m, double dx, double dy, double* Hz, double* Hd)
 {
     *Hz = 0.0;
@@ -117,6 +149,17 @@ void orc_onsite_layers(const orc_model* m, int64_t n, const double* Rat, const i
     if (H0Bottom)
         for (int64_t i = 0; i < n; ++i) H0Bottom[i] = 0.0;
     if (m->moire_onsite == ORC_ONSITE_NONE) return;
+    if (m->encapsulated) {
+        /* HamOnSiteMoireEffectiveBilayer, ham.F90:3303-3434 (H0Bottom stays 0 on this branch) */
+        for (int64_t i = 0; i < n; ++i) {
+            double dx, dy, Hz = 0.0, Hd = 0.0;
+            bilayer_disp(m, layer[i], Rat[3 * i], Rat[3 * i + 1], &dx, &dy);
+            if (layer[i] == 1 || !deactivated(m, layer[i])) moire_terms(m, dx, dy, &Hz, &Hd);
+            const double sgn = (species[i] % 2 == 1) ? -1.0 : 1.0;
+            H0[i] = H0[i] + sgn * Hz + Hd;   /* (H0 + (-1)**S Hz) + H0jj, left to right */
+        }
+        return;
+    }
     /* HamOnSiteMoireEffective, ham.F90:3437-3544 */
     for (int64_t i = 0; i < n; ++i) {
         double dx, dy, Hz, Hd;
@@ -128,8 +171,8 @@ void orc_onsite_layers(const orc_model* m, int64_t n, const double* Rat, const i
         }
         moire_terms(m, dx, dy, &Hz, &Hd);
         const double sgn = (species[i] % 2 == 1) ? -1.0 : 1.0; /* (-1)**Species */
-        if (layer[i] == 1) H0[i] = H0[i] + (sgn * Hz * m->sign1 + Hd);
-        else if (layer[i] == 2) H0[i] = H0[i] + (sgn * Hz * m->sign2 + Hd);
+        if (layer[i] == 1) H0[i] = H0[i] + sgn * Hz * m->sign1 + Hd;
+        else if (layer[i] == 2) H0[i] = H0[i] + sgn * Hz * m->sign2 + Hd;
     }
     /* H0Bottom = H0, ham.F90:2703 */
     if (H0Bottom)
@@ -149,7 +192,7 @@ void orc_onsite_layers(const orc_model* m, int64_t n, const double* Rat, const i
         }
         moire_terms(m, dx, dy, &Hz, &Hd);
         const double sgn = (species[i] % 2 == 1) ? -1.0 : 1.0;
-        H0[i] = H0[i] + (sgn * Hz * m->sign2 + Hd);
+        H0[i] = H0[i] + sgn * Hz * m->sign2 + Hd;
     }
 }
 
@@ -279,18 +322,30 @@ void orc_hopping(const orc_model* m, int64_t n, const double* Rat, const int32_t
                  const double* NeighD, double* hopp)
 {
     memset(hopp, 0, sizeof(double) * 2 * (size_t)n * maxNeigh);
+    int bernal = 0;
+    int8_t* dimer = NULL;
+    if (m->encapsulated) {
+        bernal = m->bernal;
+        if (bernal == 2) {
+            dimer = (int8_t*)calloc((size_t)n, 1);
+            if (!dimer) return;
+            const int64_t cnt = orc_bernal_dimers(n, layer, maxNeigh, Nneigh, NList, NeighD, dimer);
+            if (llabs(2 * cnt - n) > n / 10) bernal = 1; /* not AB stacked: the former coupling, ham.F90:6488-6495 */
+        }
+    }
     for (int64_t i = 0; i < n; ++i) {
         double delta = 0.0;
         double del[3] = {0.0, 0.0, 0.0};
-        if (m->moire_offdiag) { /* HamHopBondTermsMoire, ham.F90:12542-12680 (single-layer branch) */
-            double dx, dy, re, im;
-            moire_disp(m, Rat[3 * i], Rat[3 * i + 1], 0, &dx, &dy);
+        if (m->moire_offdiag) { /* HamHopBondTermsMoire, ham.F90:12542-12680 */
+            double dx, dy, re = 0.0, im = 0.0;
+            if (m->encapsulated) bilayer_disp(m, layer[i], Rat[3 * i], Rat[3 * i + 1], &dx, &dy);
+            else moire_disp(m, Rat[3 * i], Rat[3 * i + 1], 0, &dx, &dy);
             dy = dy + m->shift1;
             if ((layer[i] == 1 && m->sign1 < 0.0) || (layer[i] == 2 && m->sign2 < 0.0)) {
                 dx = -dx;
                 dy = -dy;
             }
-            offdiago(dx, dy, m->Cab, m->Phiab, m->aG, &re, &im);
+            if (!deactivated(m, layer[i])) offdiago(dx, dy, m->Cab, m->Phiab, m->aG, &re, &im);
             if (species[i] == 1 || species[i] == 2) bond_deltas(species[i], re, im, del);
         }
         const int flip = (layer[i] == 1 && m->sign1 < 0.0) || (layer[i] == 2 && m->sign2 < 0.0);
@@ -319,7 +374,21 @@ void orc_hopping(const orc_model* m, int64_t n, const double* Rat, const int32_t
                     }
                 }
             } else if (layer[i] == layer[jj] + 1 || layer[i] == layer[jj] - 1) {
-                if (m->interlayer == ORC_INTER_TWO_CENTRE) {
+                if (m->encapsulated) {
+                    /* the encapsulated bilayer's interlayer branch, ham.F90:6721-6745 */
+                    if (bernal == 2) { /* HamHopInterlayerBernalF2G2, ham.F90:12800-12827 */
+                        const int mixed = dimer[i] != dimer[jj];
+                        const double dxy = sqrt(D[0] * D[0] + D[1] * D[1]), aCC = m->aCC, aG = m->aG;
+                        const double* t = m->tbl; /* tAA1 tAA2 tAB1 tAB2 tBA0 tBA2 tBA5 */
+                        if (dxy < 0.2) h[0] = h[0] + t[4];
+                        else if (dxy > aCC * 0.9 && dxy < aCC * 1.1) h[0] = h[0] + (mixed ? t[0] : t[2]);
+                        else if (dxy > aG * 0.9 && dxy < aG * 1.1) h[0] = h[0] + t[5];
+                        else if (dxy > aCC * 2.0 * 0.9 && dxy < aCC * 2.0 * 1.1) h[0] = h[0] + (mixed ? t[1] : t[3]);
+                        else if (dxy > (aCC * 3.0) * 0.9 && dxy < (aCC * 3.0) * 1.1 && !mixed) h[0] = h[0] + t[6];
+                    } else if (fabs(D[0]) < 0.01 && fabs(D[1]) < 0.01) {
+                        h[0] = h[0] - m->tbl[2];
+                    }
+                } else if (m->interlayer == ORC_INTER_TWO_CENTRE) {
                     /* ham.F90:9810-9830: renormalizeHoppingFactorAAp of KoshinoSR (aval 1.34, bval 3.25) */
                     const double dist = sqrt(D[0] * D[0] + D[1] * D[1] + D[2] * D[2]);
                     const double renorm = m->koshino_sr ? exp((fabs(D[2]) - 3.25) / 1.34) : 1.0;
@@ -343,8 +412,29 @@ void orc_hopping(const orc_model* m, int64_t n, const double* Rat, const int32_t
             }
         }
     }
+    free(dimer);
     if (m->second_moire && m->moire_offdiag) second_moire_bonds(m, n, Rat, species, layer, maxNeigh, Nneigh, NList,
                                                                 NeighD, hopp);
+}
+
+/* Dimer sites of the Bernal interlayer branch, ham.F90:6475-6484: an atom with a neighbour of an adjacent
+ * layer within 0.2 A in plane.  Returns their number. */
+int64_t orc_bernal_dimers(int64_t n, const int32_t* layer, int32_t maxNeigh, const int32_t* Nneigh,
+                          const int32_t* NList, const double* NeighD, int8_t* dimer)
+{
+    int64_t cnt = 0;
+    for (int64_t i = 0; i < n; ++i) {
+        dimer[i] = 0;
+        for (int32_t j = 0; j < Nneigh[i]; ++j) {
+            const size_t e = (size_t)i * maxNeigh + j;
+            const int64_t jj = NList[e] - 1;
+            if (layer[i] != layer[jj] + 1 && layer[i] != layer[jj] - 1) continue;
+            const double* D = NeighD + 3 * e;
+            if (sqrt(D[0] * D[0] + D[1] * D[1]) < 0.2) dimer[i] = 1;
+        }
+        cnt += dimer[i];
+    }
+    return cnt;
 }
 
 /* HamPeierlsPeriodicGauge, ham.F90:12834-12882 (with the corner term). */

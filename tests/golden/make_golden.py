@@ -22,7 +22,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CASES = ["graphene", "graphene+NeighLevels1", "graphene+NeighLevels2", "graphene+NeighLevels3",
          "graphene+MagField1", "eff", "eff+MoireOffDiag", "eff+MoireOffDiagMidpoint", "eff+MoireTwisted",
          "eff+MoireAddSecondMoire", "eff+MoireAddSecondMoire+Midpoint", "eff+MoireAddSecondMoire+Twisted2",
-         "eff+MoireSecondMoireRotateFirst_off", "tbg", "tbg+MagField1"]
+         "eff+MoireSecondMoireRotateFirst_off", "tbg", "tbg+MagField1", "sys_MoireEncapsulatedBilayerMC",
+         "sys_MoireEncapsulatedBilayerMC+MoirePotential", "sys_MoireEncapsulatedBilayerMC+MoireOffDiag"]
 
 
 def main(ref):

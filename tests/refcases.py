@@ -37,6 +37,7 @@ BASES = {
     "graphene": dict(TypeOfSystem="Graphene", CellSize=6, **COMMON),
     "tbg": dict(TypeOfSystem="TwistedBilayerBasedOnMoireCell", **BILAYER, **COMMON),
     "eff": dict(EFFECTIVE, **COMMON),
+    "encmc": dict(TypeOfSystem="MoireEncapsulatedBilayerBasedOnMoireCell", **BILAYER, **COMMON),
 }
 CASES = {
     "graphene": ("graphene", {}),
@@ -55,6 +56,11 @@ CASES = {
                                                  "MoireTwistAngle2": 0.5}),
     "eff+MoireSecondMoireRotateFirst_off": ("eff", {"MoireAddSecondMoire": True, "MoireSecondMoireRotateFirst": False}),
     "tbg": ("tbg", {}),
+    "sys_MoireEncapsulatedBilayerMC": ("encmc", {}),
+    "sys_MoireEncapsulatedBilayerMC+MoirePotential": ("encmc", {"MoirePotential": True, "MoireJeil": True,
+                                                                "MoireH0AndHZ": True}),
+    "sys_MoireEncapsulatedBilayerMC+MoireOffDiag": ("encmc", {"MoirePotential": True, "MoireJeil": True,
+                                                              "MoireH0AndHZ": True, "MoireOffDiag": True}),
     "tbg+MagField1": ("tbg", {"MagFieldInteger": 1}),
 }
 
@@ -70,10 +76,19 @@ def build(keys):
     """Geometry, neighbours, on-site energies and hoppings (complex, g0 units) for input keys."""
     g = lambda k, d: keys.get(k, d)
     aG = g("LatticeParameter", 2.46)
-    kind = {"Graphene": orc.GRAPHENE, "TwistedBilayerBasedOnMoireCell": orc.TBG_MOIRE_CELL}[g("TypeOfSystem", "Graphene")]
+    system = g("TypeOfSystem", "Graphene")
+    kind = {"Graphene": orc.GRAPHENE, "TwistedBilayerBasedOnMoireCell": orc.TBG_MOIRE_CELL,
+            "MoireEncapsulatedBilayerBasedOnMoireCell": orc.TBG_MOIRE_CELL}[system]
+    encapsulated = system == "MoireEncapsulatedBilayerBasedOnMoireCell"
+    add_shift = 0
+    if g("TwistedBLAddShift", False):
+        add_shift = 1 if g("BernalShift", False) else 2 if g("BridgeShift", False) else None
+        if add_shift is None:
+            raise ValueError("TwistedBLAddShift needs BernalShift or BridgeShift")
     geo = orc.geometry(kind, aG=aG, cell_size=g("CellSize", 50), super_cell=g("SuperCell", 1),
                        m=g("MoireCellParameters", (0, 0, 0, 0)), height=g("CellHeight", 40.0),
-                       d_interlayer=g("InterlayerDistance", 3.35))
+                       d_interlayer=g("InterlayerDistance", 3.35), add_shift=add_shift,
+                       shift_factor=g("BilayerShiftFactor", 0.0))
     g0 = g("Hopping", -3.72 * aG + 12.14)
     tbnn = g("NeighLevels", 1)
     acc = aG / math.sqrt(3.0)
@@ -136,6 +151,30 @@ def build(keys):
     phi2m = math.atan((1.0 + m.eps) * math.sin(m.twist2_rad) / ((1.0 + m.eps) * math.cos(m.twist2_rad) - 1.0))
     m.shift2_x = m.shift2 * math.cos(phi2m)
     m.shift2_y = m.shift2 * math.sin(phi2m)
+    # MoireEncapsulatedBilayerBasedOnMoireCell (ham.F90:2607-2640, 5729-5780, 6455-6500)
+    m.encapsulated = int(encapsulated)
+    m.bl_bottom_rad = g("MoireBilayerBottomAngle", 0.0) * math.pi / 180.0
+    m.bl_top_rad = g("MoireBilayerTopAngle", 0.0) * math.pi / 180.0
+    for k, key in enumerate(("MoireBilayerBottomXShift", "MoireBilayerBottomYShift", "MoireBilayerTopXShift",
+                              "MoireBilayerTopYShift")):
+        m.tau[k] = g(key, 0.0)
+    m.deact_upper = int(g("MoireBLDeactivateUpperLayer", False))
+    m.deact_uppers = int(g("MoiretDBLDeactivateUpperLayers", False))
+    f2g2 = g("F2G2Model", True) and not g("RemoveF2G2Flag", False)
+    one, three = g("BilayerOneParameter", False), g("BilayerThreeParameters", False)
+    if encapsulated:
+        if three or not (f2g2 or one):
+            raise ValueError("encapsulated bilayer: BilayerThreeParameters, or neither F2G2Model nor "
+                             "BilayerOneParameter, is not on this path")
+        if one:
+            m.bernal, m.tbl[2] = 1, -g("BilayertAB1", 0.361) / g0
+        else:
+            m.bernal = 1 if g("LegacyBernalTAB1", False) else 2
+            for k, (key, dflt) in enumerate((("BilayertAA1", 0.09244), ("BilayertAA3", -0.02299),
+                                             ("BilayertAB1", 0.1391), ("BilayertAB3", -0.07211),
+                                             ("BilayertBA0", 0.331), ("BilayertBA2", -0.01016),
+                                             ("BilayertBA5", 0.0001))):
+                m.tbl[k] = -g(key, dflt) / g0
     if bl in ("Koshino", "HTC"):
         m.interlayer = orc.INTER_TWO_CENTRE
     vpppi0 = g("Vpppi0", 2.7 if koshino_intra else 3.5)

@@ -38,6 +38,25 @@ INPUTS = {
     },
     "anderson": {"Run.TypeOfSystem": "Graphene", "Structure.CellSize": 30, "Disorder.Anderson": True,
                  "Disorder.AndersonAmp": 1.0, "Kubo.SeedValue": 5, "TB.NeighLevels": 2},
+    "encapsulated_bilayer_former_names": {
+        "TypeOfSystem": "MoireEncapsulatedBilayerBasedOnMoireCell", "MoireCellParameters": (6, 0, 6, 0),
+        "twistedBLAddShift": True, "BernalShift": True, "BilayerShiftFactor": 0.2, "MoirePotential": True,
+        "MoireJeil": True, "MoireH0AndHZ": True, "MoireOffDiag": True, "MoireBilayerBottomAngle": 0.3,
+        "MoireBilayerTopAngle": -0.7, "MoireBLDeactivateUpperLayer": True, "BilayertBA0": 0.35, "TypeOfBL": "Koshino",
+        "moireBLShift.Calc": True, "moireBLShiftDefinedValues": True, "MoireBilayerTopXShift": 0.4, "RecursionNumber": 30,
+    },
+    "encapsulated_shift_sweep": {
+        "Run.Prefix": "generate", "Run.TypeOfSystem": "MoireEncapsulatedBilayerBasedOnMoireCell",
+        "Structure.MoireCellParameters": (6, 0, 6, 0), "Structure.SuperCell": 4, "Structure.TwistedBLAddShift": True,
+        "Structure.BernalShift": True, "Structure.InterlayerDistance": 3.34, "Interlayer.TypeOfBL": "Koshino",
+        "TB.NeighLevels": 5, "Neigh.LayerNeighbors": 100, "Neigh.LayerDistFactor": 3.2, "Moire.Potential": True,
+        "Moire.Jeil": True, "Moire.H0AndHZ": True, "Moire.OffDiag": True, "Moire.LatticePercent": -0.0166,
+        "Moire.BilayerBottomAngle": 0.4, "Moire.BilayerTopAngle": -0.9, "moireBLShift.Calc": True,
+        "Moire.BLShiftRange": True, "Moire.BLShiftRangeSteps": 2, "Moire.BilayerBottomXMax": 0.6,
+        "Moire.BilayerTopYMin": -0.3, "Moire.BilayerTopYMax": 0.9, "Kubo.RecursionNumber": 100,
+        "Kubo.Epsilon": 0.01, "Kubo.EnergyMin": -1.0, "Kubo.EnergyMax": 1.0, "Kubo.SeedValue": 11,
+        "Calculate.OnlyDOS": True,
+    },
     "second_moire_former_names": {
         "TypeOfSystem": "Graphene", "CellSize": 11, "SuperCell": 2, "Latticepercent": -1.0 / 11.0,
         "MoirePotential": True, "MoireJeil": True, "MoireH0AndHZ": True, "MoireOffDiag": True,
@@ -95,8 +114,12 @@ def test_driver_reads_input_like_the_package(tmp_path, name):
               "anderson", "koshino_sr", "renormalize_coupling", "second_moire", "twisted2", "rotate_first"):
         assert got["model"][f] == getattr(m, f), f
     for f in ("eps", "C0", "Cz", "Cab", "vpppi0", "vppsigma0", "bl_delta", "anderson_w", "coupling_factor",
-              "eps_factor", "twist2_rad", "shift2_x", "shift2_y", "sign2"):
+              "eps_factor", "twist2_rad", "shift2_x", "shift2_y", "sign2", "bl_bottom_rad", "bl_top_rad"):
         assert math.isclose(got["model"][f], getattr(m, f), rel_tol=1e-15, abs_tol=1e-300), f
+    for f in ("encapsulated", "deact_upper", "deact_uppers", "bernal"):
+        assert got["model"][f] == getattr(m, f), f
+    assert got["model"]["tbl"] == list(m.tbl)
+    assert got["add_shift"] == job["cell"]["add_shift"] and got["shift_factor"] == job["cell"]["shift_factor"]
     assert got["cell_size"] == job["cell"]["cell_size"] and got["super_cell"] == job["cell"]["super_cell"]
     assert tuple(got["m"]) == tuple(job["cell"]["m"])
 
@@ -490,3 +513,61 @@ def test_driver_reads_pdos_and_haldane_keys(tmp_path):
                   "HaldPhase.InitialInteger": 0, "HaldPhase.FinalInteger": 6})
     got = _print_job(path)
     assert got["hal_mode"] == 2 and got["mphi"][:2] == [0, 0]   # no sweep without SpecifyRange
+
+
+@pytest.mark.gpu
+def test_driver_layer_shift_sweep(tmp_path):
+    """moireBLShift.Calc with Moire.BLShiftRange (calc.F90:40-60, moireBLShift.F90): the encapsulated AB
+    bilayer at three layer shifts, one folder X1_.._Y1_.._X2_.._Y2_.. per shift; a_n, b_n and the DOS of each
+    against the oracle's Hamiltonian with those shifts.  The same sweep through grabnes_b200.launch with two
+    ranks (each its own process; no kernel waits on another) writes the same folders with the same numbers."""
+    import sys
+    keys = dict(INPUTS["encapsulated_shift_sweep"])
+    one, two = tmp_path / "one", tmp_path / "two"
+    one.mkdir()
+    two.mkdir()
+    for d in (one, two):
+        _write(str(d / "Gendata.in"), keys)
+    subprocess.run([DRIVER, "Gendata.in"], check=True, cwd=str(one), capture_output=True, text=True)
+    units = M.blshift_units(keys)
+    folders = sorted(d for d in os.listdir(one) if d.startswith("X1_"))
+    assert folders == sorted(f for _, f in units)
+    base = dict(TypeOfSystem="MoireEncapsulatedBilayerBasedOnMoireCell", MoireCellParameters=(6, 0, 6, 0),
+                SuperCell=4, TwistedBLAddShift=True, BernalShift=True, InterlayerDistance=3.34, TypeOfBL="Koshino",
+                NeighLevels=5, LayerNeighbors=100, LayerDistFactor=3.2, MoirePotential=True, MoireJeil=True,
+                MoireH0AndHZ=True, MoireOffDiag=True, LatticePercent=-0.0166, MoireBilayerBottomAngle=0.4,
+                MoireBilayerTopAngle=-0.9)
+    for tau, folder in units:
+        r = R.build(dict(base, MoireBilayerBottomXShift=tau[0], MoireBilayerBottomYShift=tau[1],
+                         MoireBilayerTopXShift=tau[2], MoireBilayerTopYShift=tau[3]))
+        n, g0 = r["geo"]["n"], r["g0"]
+        a0, b0 = orc.recursion(r["nb"], r["hop"], r["h0"], orc.init_wf(n, 11), 100, 0)
+        a = np.loadtxt(one / folder / "generate.a0.dat")
+        b = np.loadtxt(one / folder / "generate.b0.dat")
+        assert np.abs(a - a0).max() <= 1e-10 * np.abs(a0).max() and np.abs(b - b0).max() <= 1e-10 * np.abs(b0).max()
+        _, d0 = orc.frac(a0, b0, 0.01 / g0, 1000, -1.0 / g0, 1.0 / g0)
+        dos = np.loadtxt(one / folder / "generate.DOS")
+        assert np.abs(dos[:, 1] - d0).sum() <= 1e-6 * np.abs(d0).sum()
+    env = dict(os.environ, PYTHONPATH=os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    p = subprocess.run([sys.executable, "-m", "grabnes_b200.launch", "--gpus", "2", "Gendata.in"], cwd=str(two),
+                       env=env, capture_output=True, text=True, timeout=600)
+    assert p.returncode == 0, p.stdout + p.stderr
+    assert sorted(d for d in os.listdir(two) if d.startswith("X1_")) == folders
+    for folder in folders:
+        for name in ("generate.a0.dat", "generate.b0.dat"):
+            x, y = np.loadtxt(one / folder / name), np.loadtxt(two / folder / name)
+            assert np.abs(x - y).max() <= 1e-10 * np.abs(y).max()
+
+
+@pytestmark_cpu
+def test_driver_layer_shift_units(tmp_path):
+    """The driver's shift units (its --print-job units line with GRABNES_RANK / NRANKS) follow the
+    package's blshift_units: three shifts, on ranks 0, 1, 0."""
+    keys = dict(INPUTS["encapsulated_shift_sweep"])
+    path = str(tmp_path / "Gendata.in")
+    _write(path, keys)
+    assert len(M.blshift_units(keys)) == 3
+    for rank in (0, 1):
+        env = dict(os.environ, GRABNES_RANK=str(rank), GRABNES_NRANKS="2")
+        _, units = _print_job(path, env)
+        assert units["units"] == [[u, 0] for u in range(3) if u % 2 == rank]

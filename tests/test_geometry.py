@@ -22,6 +22,11 @@ CELLS = {
     "example06_55x8": dict(kind=0, aG=2.46, cell_size=55, super_cell=8),
     "tbg_31_30_30_31_x2": dict(kind=1, aG=2.4595, super_cell=2, m=(31, 30, 30, 31), d_interlayer=3.35),
     "example07_83x16": dict(kind=0, aG=2.46, cell_size=83, super_cell=16),
+    # the moire cell with its second layer offset (Structure.TwistedBLAddShift, atoms.F90:352-366): an AB
+    # (Bernal) bilayer, and a twisted cell with the bridge offset plus 0.3 A along a1+a2
+    "ab_bilayer_6060_x4_bernal": dict(kind=1, aG=2.46, super_cell=4, m=(6, 0, 6, 0), d_interlayer=3.34, add_shift=1),
+    "tbg_3223_x3_bridge": dict(kind=1, aG=2.46, super_cell=3, m=(3, 2, 2, 3), d_interlayer=3.34, add_shift=2,
+                               shift_factor=0.3),
 }
 
 

@@ -48,6 +48,24 @@ CASES = {
                          MoireAddSecondMoire=True, MoireTwisted2=True, MoireTwistAngle2=0.7, LatticepercentFactor=1.3,
                          MoireLayerShift2=0.9, MoireSecondMoireMassFactor=-1.0, Anderson=True, AndersonAmp=0.2,
                          SeedValue=9, **MOIRE),
+    # the encapsulated bilayer (MoireEncapsulatedBilayerBasedOnMoireCell) on an AB cell: Bernal offset, the
+    # bilayer F2G2 interlayer set on the dimer sites found from the structure, the bilayer moire on-site model
+    # with bottom / top angles and layer shifts, its bond terms, Anderson disorder
+    "enc_bernal": dict(TypeOfSystem="MoireEncapsulatedBilayerBasedOnMoireCell", MoireCellParameters=(6, 0, 6, 0),
+                       SuperCell=4, TwistedBLAddShift=True, BernalShift=True, InterlayerDistance=3.34,
+                       TypeOfBL="Koshino", NeighLevels=5, LayerNeighbors=100, LayerDistFactor=3.2,
+                       MoirePotential=True, MoireJeil=True, MoireH0AndHZ=True, MoireOffDiag=True,
+                       LatticePercent=-0.0166, MoireBilayerBottomAngle=0.4, MoireBilayerTopAngle=-0.9,
+                       MoireBilayerBottomXShift=0.3, MoireBilayerBottomYShift=-0.2, MoireBilayerTopXShift=0.5,
+                       MoireBilayerTopYShift=0.7, Anderson=True, AndersonAmp=0.1, SeedValue=4),
+    # a twisted encapsulated cell (the vertical pairs only, as the reference falls back to), the top shift
+    # inside the rotation, no moire term on layer 2, bond terms at the midpoints
+    "enc_twisted": dict(TypeOfSystem="MoireEncapsulatedBilayerBasedOnMoireCell", MoireCellParameters=(3, 2, 2, 3),
+                        SuperCell=6, InterlayerDistance=3.34, TypeOfBL="Koshino", NeighLevels=5, LayerNeighbors=100,
+                        LayerDistFactor=3.2, MoirePotential=True, MoireJeil=True, MoireOnlyHZ=True, MoireOffDiag=True,
+                        MoireOffDiagMidpoint=True, LatticePercent=-0.018, MoireBilayerTopAngle=1.1,
+                        MoireBilayerTopYShift=0.6, MoireBilayerBottomXShift=-0.4, MoireSecondMoireRotateFirst=False,
+                        MoireBLDeactivateUpperLayer=True, Anderson=True, AndersonAmp=0.1, SeedValue=6),
     # the same without SecondMoireRotateFirst (shift inside the rotation), per-atom bond terms
     "moire_second_norot": dict(TypeOfSystem="Graphene", CellSize=11, SuperCell=4, LatticePercent=-1.0 / 11.0,
                                MoirePotential=True, MoireJeil=True, MoireH0AndHZ=True, MoireOffDiag=True,
@@ -116,6 +134,23 @@ def test_onsite_bottom_and_top(ctx, name):
         assert not bottom.any() and not top.any()
     if name.startswith("moire_second"):
         assert np.abs(top).max() > 1e-4
+
+
+def test_encapsulated_interlayer_branch(ctx):
+    """The AB cell takes the bilayer F2G2 set (its dimer coupling tBA0 appears, on the vertical pairs), the
+    twisted cell the vertical pairs only (-tAB1), as the reference decides from the dimer sites."""
+    for name, value in (("enc_bernal", lambda m: m.tbl[4]), ("enc_twisted", lambda m: -m.tbl[2])):
+        r = built(name)
+        gpu_pipeline(ctx, r)
+        _, hop = ctx.hamiltonian()
+        geo, nb = r["geo"], r["nb"]
+        lay = geo["layer"]
+        n = geo["n"]
+        inter = [(i, j) for i in range(n) for j in range(nb["nneigh"][i]) if lay[nb["nlist"][i, j] - 1] != lay[i]]
+        vals = {hop[i, j].real for i, j in inter}
+        assert value(r["model"]) in vals, name
+        if name == "enc_twisted":
+            assert vals <= {0.0, -r["model"].tbl[2]}
 
 
 def _rel(x, y):
