@@ -132,7 +132,8 @@ def kernel_key(best):
     rpt = best.get("rhs_per_thread", 0) or 4         # right-hand sides per thread (16 vectors: 4 threads a row)
     if not staged:
         return f"k_spmm_step<float, real, G={g}, RPT={rpt}, U={unroll}>"
-    return f"k_spmm_staged<float, real, G={g}, RPT={rpt}, U={unroll}, SV={sv}, MINB={mb}, prefetch={pf}>"
+    fused = ", FUSED" if best.get("fused", -1) == 1 else ""   # the update folded into the product
+    return f"k_spmm_staged<float, real, G={g}, RPT={rpt}, U={unroll}, SV={sv}, MINB={mb}, prefetch={pf}{fused}>"
 
 
 def traffic_from_profile(key, workload="bench_workload"):
@@ -552,11 +553,11 @@ MOIRE_DOS_KEYS = {k: v for k, v in TEVOL_KEYS.items() if not k.startswith("Disor
 
 def fixed_tuning(spec):
     """A tuning dictionary from 'rhs_per_thread,blocks_per_sm,rows_per_group,staged,prefetch[,unroll
-    [,stage_values[,min_blocks]]]'."""
+    [,stage_values[,min_blocks[,fused]]]]'."""
     vals = [int(x) for x in spec.split(",")]
     names = ["rhs_per_thread", "blocks_per_sm", "rows_per_group", "staged", "prefetch", "unroll", "stage_values",
-             "min_blocks"]
-    best = dict(unroll=0, stage_values=-1, min_blocks=0, fixed=True)
+             "min_blocks", "fused"]
+    best = dict(unroll=0, stage_values=-1, min_blocks=0, fused=-1, fixed=True)
     best.update(zip(names, vals))
     return best
 

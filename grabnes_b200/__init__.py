@@ -125,7 +125,7 @@ def _declare(L):
     L.gbn_version.restype = C.c_char_p
     L.gbn_set_stream.argtypes = [vp, vp]
     L.gbn_set_tuning.argtypes = [vp, i32, i32, i32, i32, i32]
-    L.gbn_set_kernel_variant.argtypes = [vp, i32, i32, i32, i32, i32]
+    L.gbn_set_kernel_variant.argtypes = [vp, i32, i32, i32, i32, i32, i32]
     L.gbn_launch_count.argtypes = [vp]
     L.gbn_launch_count.restype = i64
     L.gbn_last_timing.argtypes = [vp, C.POINTER(d), C.POINTER(i64)]
@@ -216,12 +216,14 @@ class Context:
     def set_tuning(self, rhs_per_thread=0, blocks_per_sm=0, rows_per_group=0, staged=-1, prefetch=-1):
         self._ck(self._L.gbn_set_tuning(self._h, rhs_per_thread, blocks_per_sm, rows_per_group, staged, prefetch))
 
-    def set_kernel_variant(self, col_unroll=0, stage_values=-1, min_blocks=0, field_table=-1, tiled=-1):
+    def set_kernel_variant(self, col_unroll=0, stage_values=-1, min_blocks=0, field_table=-1, tiled=-1, fused=-1):
         """Columns in flight per batch of the sparse product (4, 8; 0 = default), whether staged slice
         records carry the values (1) or only the column indices (0; -1 = default), the resident blocks per
-        SM its registers are bounded for (1, 3; 0 = 1), and for batched fields the per-tile rotation table
-        (1) or rotations on the fly (0, -1 = default), and the tile-local product (1; 0, -1 = default: no)."""
-        self._ck(self._L.gbn_set_kernel_variant(self._h, col_unroll, stage_values, min_blocks, field_table, tiled))
+        SM its registers are bounded for (1, 2, 3; 0 = 1), and for batched fields the per-tile rotation table
+        (1) or rotations on the fly (0, -1 = default), the tile-local product (1; 0, -1 = default: no), and
+        the fused step, the update folded into the product (1; 0, -1 = default: no)."""
+        self._ck(self._L.gbn_set_kernel_variant(self._h, col_unroll, stage_values, min_blocks, field_table, tiled,
+                                                fused))
 
     @property
     def launches(self):

@@ -208,12 +208,14 @@ int gbn_set_tuning(gbn_ctx* c, int32_t rhs_per_thread, int32_t blocks_per_sm, in
 }
 
 int gbn_set_kernel_variant(gbn_ctx* c, int32_t col_unroll, int32_t stage_values, int32_t min_blocks,
-                           int32_t field_table, int32_t tiled)
+                           int32_t field_table, int32_t tiled, int32_t fused)
 {
     if (!c) return GBN_ERR_ARG;
     if ((col_unroll != 0 && col_unroll != 4 && col_unroll != 8) || stage_values < -1 || stage_values > 1 ||
-        (min_blocks < 0 || min_blocks > 3) || field_table < -1 || field_table > 1 || tiled < -1 || tiled > 1)
+        (min_blocks < 0 || min_blocks > 3) || field_table < -1 || field_table > 1 || tiled < -1 || tiled > 1 ||
+        fused < -1 || fused > 1)
         return fail(c, GBN_ERR_ARG, "kernel variant out of range");
+    c->tune_fused = fused;
     c->tune_tiled = tiled;
     c->tune_unroll = col_unroll;
     c->tune_stage_values = stage_values;

@@ -168,6 +168,7 @@ struct gbn_ctx {
     int tune_stage_values = -1;  // staged records carry the values (1) or only the column indices (0); -1 auto
     int tune_min_blocks = 0;     // product kernel compiled for 1 or 3 resident blocks per SM (0 = 1)
     int tune_tiled = -1;         // tile-local product (halo rows in shared memory): 1 yes, 0 no, -1 default (no)
+    int tune_fused = -1;         // the update folded into the product: 1 yes, 0 no, -1 default (no)
     int tune_field_table = -1;   // batched fields: rotations tabulated per tile (1) or on the fly (0, -1 default)
     bool last_staged = false;    // the last recursion used the staged kernel
 

@@ -244,6 +244,7 @@ struct StepLaunch {
     const unsigned char* mat = nullptr;   // the records the kernel reads (the layout's, or its tile table)
     int64_t entry_bytes = 0;
     bool tiled = false;                   // the tile-local product (halo rows in shared memory)
+    bool fused = false;                   // the update folded into the product (no update launches)
     int32_t pitch = 0, halo_off = 0;
 };
 
@@ -317,6 +318,8 @@ static int step_launch(gbn_ctx* c, int R, StepLaunch* L)
     v.unroll = c->tune_unroll > 0 ? c->tune_unroll : (c->prec == GBN_MIXED ? 8 : 4);
     v.stage_values = c->tune_stage_values != 0;
     v.min_blocks = c->tune_min_blocks > 0 ? c->tune_min_blocks : (v.unroll == 8 && E.G == 1 && !E.cplx ? 3 : 1);
+    // the update folded into the product, where asked for (real FP32 layouts; see k_spmm_staged)
+    v.fused = c->tune_fused == 1 && !E.field;
     // batched fields rotate on the fly unless the tile table is asked for (measured slower on example 06's
     // sweep: 0.175 against 0.108 ms per product, the table's complex values per thread slot triple the
     // records' bytes)
@@ -330,7 +333,7 @@ static int step_launch(gbn_ctx* c, int R, StepLaunch* L)
     };
     const bool want_staged = c->tune_staged != 0 && cap_of(0) > 0;
     // the kernel of this variant; shapes without it take the base variant unless one was asked for
-    const bool asked = c->tune_unroll > 0 || c->tune_stage_values >= 0 || c->tune_min_blocks > 0;
+    const bool asked = c->tune_unroll > 0 || c->tune_stage_values >= 0 || c->tune_min_blocks > 0 || v.fused;
     auto pick = [&](bool staged) -> StepFn {
         int rpt, tpr;
         split_rhs(c->prec, R, c->tune_rpt, &rpt, &tpr);
@@ -347,6 +350,7 @@ static int step_launch(gbn_ctx* c, int R, StepLaunch* L)
     };
     L->fn = pick(want_staged);
     if (!L->fn) return fail(c, GBN_ERR_ARG, "no recursion kernel for this tile width and kernel variant");
+    L->fused = v.fused;
     L->block = 256;
     L->smem = 0;
     L->staged = false;
@@ -391,7 +395,7 @@ static int step_launch(gbn_ctx* c, int R, StepLaunch* L)
         L->fn = pick(false);
         if (!L->fn) return fail(c, GBN_ERR_ARG, "no recursion kernel for this tile width and kernel variant");
     }
-    if (c->tune_tiled == 1) {   // the tile-local product where the shape has one
+    if (c->tune_tiled == 1 && !L->fused) {   // the tile-local product where the shape has one
         bool done = false;
         const int rc = tiled_launch(c, R, L, &done);
         if (rc) return rc;
@@ -424,8 +428,9 @@ int lanczos_prepare(gbn_ctx* c, int prec, int nrhs, bool field)
     StepLaunch L;
     const int rc = step_launch(c, nrhs, &L);
     if (rc) return rc;
+    if (L.fused) GBN_CK(c, c->vec[3].ensure(vbytes));   // the fused step keeps v_k and v_{k+1}
     const size_t blocks = (size_t)(L.grid > c->num_sms * kUpdateBlocksPerSM ? L.grid : c->num_sms * kUpdateBlocksPerSM);
-    GBN_CK(c, c->partials.ensure(sizeof(double) * blocks * nrhs));
+    GBN_CK(c, c->partials.ensure(sizeof(double) * blocks * nrhs * (L.fused ? 3 : 1)));
     GBN_CK(c, c->scal.ensure(sizeof(double) * kScal * nrhs));
     GBN_CK(c, c->counter.ensure(sizeof(unsigned int) * 4));
     return GBN_OK;
@@ -514,11 +519,12 @@ static int ensure_step_graph(gbn_ctx* c, const StepLaunch& L, const StepParams& 
     StepParams q;
     memcpy(&q, &p, sizeof q);   // bytewise, padding included
     q.x_cur = q.x_prev = nullptr;
+    q.v_out = q.u_out = nullptr;   // per step; the buffers they rotate over are in the key below
     const int64_t extra[4] = {total, ublk, ugrid, ((int64_t)c->prec << 32) | (int64_t)c->nrhs};
     memcpy(key.data(), &q, sizeof q);
     memcpy(key.data() + sizeof q, &L, sizeof L);
     memcpy(key.data() + sizeof q + sizeof L, extra, sizeof extra);
-    const void* vp[3] = {c->vec[0].p, c->vec[1].p, c->vec[2].p};
+    const void* vp[4] = {c->vec[0].p, c->vec[1].p, c->vec[2].p, c->vec[3].p};
     key.insert(key.end(), (const unsigned char*)vp, (const unsigned char*)vp + sizeof vp);
     if (c->step_graph && key == c->step_graph_key) return GBN_OK;
     if (c->step_graph) {
@@ -565,8 +571,9 @@ int lanczos_run(gbn_ctx* c, int32_t nmax)
     if (rc) return rc;
     c->last_staged = L.staged;
     // the block partials of this launch shape (it may differ from the one the buffers were sized for)
-    GBN_CK(c, c->partials.ensure(sizeof(double) * (size_t)R *
+    GBN_CK(c, c->partials.ensure(sizeof(double) * (size_t)R * (L.fused ? 3 : 1) *
                                  (size_t)std::max(L.grid, c->num_sms * kUpdateBlocksPerSM)));
+    if (L.fused) GBN_CK(c, c->vec[3].ensure((size_t)c->ell.npad * R * sizeof(float2)));
     StepParams p;
     memset(&p, 0, sizeof p);
     p.slice_ptr = c->ell.slice_ptr.as<int64_t>();
@@ -632,6 +639,20 @@ int lanczos_run(gbn_ctx* c, int32_t nmax)
     auto launch_step = [&](int32_t k) -> int {
         void* xprev = c->vec[1 + (k & 1)].p;
         void* xcur = c->vec[1 + ((k + 1) & 1)].p;
+        if (L.fused) {   // v_k in vec[0] / vec[3] by parity, u_{k-1} in vec[1 + k%2]; u_k, v_{k+1} written
+            p.x_cur = (k & 1) ? c->vec[3].p : c->vec[0].p;
+            p.v_out = (k & 1) ? c->vec[0].p : c->vec[3].p;
+            p.x_prev = xprev;
+            p.u_out = xcur;
+            if (k < nsample) {
+                GBN_CK(c, cudaEventRecord(c->kev[3 * k], c->stream));
+                GBN_CK(c, cudaEventRecord(c->kev[3 * k + 1], c->stream));
+            }
+            L.fn<<<L.grid, L.block, L.smem, c->stream>>>(p);
+            GBN_CK_LAUNCH(c);
+            if (k < nsample) GBN_CK(c, cudaEventRecord(c->kev[3 * k + 2], c->stream));
+            return GBN_OK;
+        }
         if (k < nsample) GBN_CK(c, cudaEventRecord(c->kev[3 * k], c->stream));
         const int rcu = launch_update(k);
         if (rcu) return rcu;
@@ -657,7 +678,7 @@ int lanczos_run(gbn_ctx* c, int32_t nmax)
         if (rc2) return rc2;
         for (; nmax - k >= kGraphSteps; k += kGraphSteps) {
             GBN_CK(c, cudaGraphLaunch(c->step_graph, c->stream));
-            c->launches += 2 * kGraphSteps;
+            c->launches += (L.fused ? 1 : 2) * kGraphSteps;
             ++c->graph_replays;
         }
     }
@@ -665,7 +686,7 @@ int lanczos_run(gbn_ctx* c, int32_t nmax)
         const int rc2 = launch_step(k);
         if (rc2) return rc2;
     }
-    {   // the closing update gives b_{nmax-1}
+    if (!L.fused) {   // the closing update gives b_{nmax-1} (the fused step's finish already did)
         const int rc2 = launch_update(nmax);
         if (rc2) return rc2;
     }

@@ -157,11 +157,17 @@ template <typename VT> struct FieldMult;
 template <> struct FieldMult<float> { using t = uint32_t; };
 template <> struct FieldMult<double> { using t = uint64_t; };
 
-template <typename VT, bool CPLX, int G, int RPT, int TPR, bool SMEM, bool SMEM_VAL, bool FIELD, int NB, int VS = 1>
+// FUSED (real FP32 layouts): the gathered vector is formed from two stored ones, x = v + (-alpha) u, by one
+// packed FMA per element from the same two loads wherever the column is gathered (xq: v, xu: u, al: the
+// thread's -alpha pairs), so every row sees the same rounded x.
+template <typename VT, bool CPLX, int G, int RPT, int TPR, bool SMEM, bool SMEM_VAL, bool FIELD, int NB, int VS = 1,
+          bool FUSED = false>
 __device__ __forceinline__ void column_batch(const typename V2<VT>::t* __restrict__ xq,
                                              const int32_t* __restrict__ cp,
                                              const typename StoredVal<VT, CPLX, FIELD>::t* __restrict__ vp,
-                                             typename V2<VT>::t (&acc)[G][RPT], typename FieldMult<VT>::t mf)
+                                             typename V2<VT>::t (&acc)[G][RPT], typename FieldMult<VT>::t mf,
+                                             const typename V2<VT>::t* __restrict__ xu = nullptr,
+                                             const typename V2<VT>::t* al = nullptr)
 {
     using C2 = typename V2<VT>::t;
     using HT = typename StoredVal<VT, CPLX, FIELD>::t;
@@ -177,6 +183,16 @@ __device__ __forceinline__ void column_batch(const typename V2<VT>::t* __restric
     }
 #pragma unroll
     for (int u = 0; u < NB; ++u) VecIO<VT, RPT>::load(xq + (size_t)(uint32_t)c[u] * R, xg[u]);
+    if constexpr (FUSED) {
+        static_assert(sizeof(VT) == 4 && !CPLX && !FIELD, "the fused gather is for real FP32 layouts");
+        C2 xh[NB][RPT];
+#pragma unroll
+        for (int u = 0; u < NB; ++u) VecIO<VT, RPT>::load(xu + (size_t)(uint32_t)c[u] * R, xh[u]);
+#pragma unroll
+        for (int u = 0; u < NB; ++u)
+#pragma unroll
+            for (int t = 0; t < RPT; ++t) xg[u][t] = __ffma2_rn(al[t], xh[u][t], xg[u][t]);
+    }
 #pragma unroll
     for (int u = 0; u < NB; ++u) load_group_vals<HT, G, SMEM_VAL>(vp + u * GPW * G * VS, h[u]);
     if constexpr (FIELD) {
@@ -201,31 +217,35 @@ __device__ __forceinline__ void column_batch(const typename V2<VT>::t* __restric
 // VS: value blocks per union column and group (the field tile table holds one per thread slot, VS = TPR,
 // interleaved [column][group][slot][G]); the caller's vp includes the thread's own slot.
 template <typename VT, bool CPLX, int G, int RPT, int TPR, bool SMEM, bool FIELD = false, int U = kColUnroll,
-          bool SMEM_VAL = SMEM, int VS = 1>
+          bool SMEM_VAL = SMEM, int VS = 1, bool FUSED = false>
 __device__ __forceinline__ void group_columns(const typename V2<VT>::t* __restrict__ x, int w,
                                               const int32_t* __restrict__ cp,
                                               const typename StoredVal<VT, CPLX, FIELD>::t* __restrict__ vp,
                                               typename V2<VT>::t (&acc)[G][RPT],
-                                              typename FieldMult<VT>::t mf = 0)
+                                              typename FieldMult<VT>::t mf = 0,
+                                              const typename V2<VT>::t* __restrict__ xu = nullptr,
+                                              const typename V2<VT>::t* al = nullptr)
 {
     using C2 = typename V2<VT>::t;
     constexpr int GPW = 32 / TPR;
     static_assert(U % kColUnroll == 0, "the unroll is a multiple of the slice-width granule");
     const int q = (threadIdx.x & 31) % TPR;
     const C2* __restrict__ xq = x + q * RPT;
+    const C2* __restrict__ xuq = FUSED ? xu + q * RPT : nullptr;
 #pragma unroll
     for (int g = 0; g < G; ++g)
 #pragma unroll
         for (int t = 0; t < RPT; ++t) { acc[g][t].x = 0; acc[g][t].y = 0; }
     int k = 0;
     for (; k + U <= w; k += U) {
-        column_batch<VT, CPLX, G, RPT, TPR, SMEM, SMEM_VAL, FIELD, U, VS>(xq, cp, vp, acc, mf);
+        column_batch<VT, CPLX, G, RPT, TPR, SMEM, SMEM_VAL, FIELD, U, VS, FUSED>(xq, cp, vp, acc, mf, xuq, al);
         cp += U * GPW;
         vp += U * GPW * G * VS;
     }
     if constexpr (U > kColUnroll) {
         for (; k < w; k += kColUnroll) {
-            column_batch<VT, CPLX, G, RPT, TPR, SMEM, SMEM_VAL, FIELD, kColUnroll, VS>(xq, cp, vp, acc, mf);
+            column_batch<VT, CPLX, G, RPT, TPR, SMEM, SMEM_VAL, FIELD, kColUnroll, VS, FUSED>(xq, cp, vp, acc, mf,
+                                                                                              xuq, al);
             cp += kColUnroll * GPW;
             vp += kColUnroll * GPW * G * VS;
         }

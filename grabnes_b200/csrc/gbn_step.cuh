@@ -14,7 +14,7 @@ namespace gbn {
 
 // Scalars of the recursion per right-hand side r, scal[4 r + i]:
 //   i = 0  a of the last product;  1  norm of the current carried vector u (x = u / norm);
-//   2  norm of the previous carried vector;  3  unused.
+//   2  norm of the previous carried vector;  3  the fused step's alpha (u_k = v_k - alpha u_{k-1}).
 constexpr int kScal = 4;
 
 struct StepParams {
@@ -29,6 +29,7 @@ struct StepParams {
     const void* x_cur;   // u_k   [npad][R] (gathered; x_k = u_k / b_{k-1})
     const void* x_prev;  // u_{k-1}        (x_{k-1} = u_{k-1} / b_{k-2})
     void* v_out;         // v_{k+1} = H x_k - b_{k-1} x_{k-1}
+    void* u_out;         // fused step: u_k, formed from v_k (x_cur) and u_{k-1} (x_prev) while gathering
     double* scal;        // [R][kScal]
     double* partials;    // [gridDim][R]
     unsigned int* counter;  // [0] block counter, [1] step index, [2] error flag
@@ -59,6 +60,7 @@ struct StepVariant {
     int unroll = 4;
     bool stage_values = true;
     int min_blocks = 1;   // staged, unroll 8: registers bounded for 2 (whole records) or 3 resident blocks per SM
+    bool fused = false;   // the update folded into the product (staged, real FP32, 4 right-hand sides per thread)
 };
 // the product kernel of the real or complex layout (gbn_step_mixed.cu, gbn_step_fp64.cu)
 StepFn step_kernel_mixed(bool cplx, int G, int rpt, int tpr, bool staged, StepVariant v);
@@ -134,43 +136,51 @@ __device__ __forceinline__ void grid_fixed_sum(const double* partials, int nblk,
 // Scalars of the step for the block's right-hand sides, in shared memory: 1 / b_{k-1} (x_k = u_k / b_{k-1})
 // and b_{k-1} / b_{k-2} (the coefficient of u_{k-1} in v_{k+1}).  Read per epilogue row, so that they
 // hold no registers across the column loop.  Needs at least R threads per block.
-template <int R>
-__device__ __forceinline__ void load_step_scalars(const StepParams& p, double (&sc)[2][R])
+template <int R, int NSC = 2>
+__device__ __forceinline__ void load_step_scalars(const StepParams& p, double (&sc)[NSC][R])
 {
     if (threadIdx.x < R) {
         const double nb = p.scal[kScal * threadIdx.x + 1], nbp = p.scal[kScal * threadIdx.x + 2];
         sc[0][threadIdx.x] = 1.0 / nb;
         sc[1][threadIdx.x] = nb / nbp;
+        if constexpr (NSC > 2) sc[2][threadIdx.x] = p.scal[kScal * threadIdx.x + 3];   // alpha (fused)
     }
     __syncthreads();
 }
 
 // Reduction of the sum Re<u_k, H u_k> over the block, then by the last block over all blocks in a fixed
 // order; writes a_k = Re<u_k, H u_k> / b_{k-1}^2 and advances the step index.
-template <int RPT, int TPR>
+// FUSED: three sums per right-hand side, S_a = Re<u_k, H u_k>, S_vv = |v_{k+1}|^2 and S_vu = Re<v_{k+1}, u_k>
+// (acc_s[s * RPT + t], block partials in planes [s][block][R]).  With alpha = a_k / b_{k-1} rounded to FP32 (the
+// value the next step forms u_{k+1} = v_{k+1} - alpha u_k with), b_k^2 = |u_{k+1}|^2 = S_vv - 2 alpha S_vu +
+// alpha^2 b_{k-1}^2; the finish writes a_k and b_k and shifts the norms, as the update kernel does otherwise.
+template <int RPT, int TPR, bool FUSED = false>
 __device__ __forceinline__ void reduce_and_finalize(const StepParams& p, double* acc_s)
 {
     constexpr int R = RPT * TPR;
+    constexpr int NS = FUSED ? 3 : 1;
     const int lane = threadIdx.x & 31;
     const int sub = lane / TPR;
     const int q = lane % TPR;
 #pragma unroll
-    for (int t = 0; t < RPT; ++t) {
+    for (int t = 0; t < NS * RPT; ++t) {
 #pragma unroll
         for (int off = TPR; off < 32; off <<= 1) acc_s[t] += __shfl_xor_sync(0xffffffffu, acc_s[t], off);
     }
-    __shared__ double red[8][R];
+    __shared__ double red[NS][8][R];
     const int wib = threadIdx.x >> 5;
     if (sub == 0) {
 #pragma unroll
-        for (int t = 0; t < RPT; ++t) red[wib][q * RPT + t] = acc_s[t];
+        for (int k = 0; k < NS; ++k)
+#pragma unroll
+            for (int t = 0; t < RPT; ++t) red[k][wib][q * RPT + t] = acc_s[k * RPT + t];
     }
     __syncthreads();
-    if (threadIdx.x < R) {
-        const int r = threadIdx.x;
+    if ((int)threadIdx.x < NS * R) {
+        const int k = (int)threadIdx.x / R, r = (int)threadIdx.x % R;
         NeumaierSum a;
-        for (int wI = 0; wI < (int)(blockDim.x >> 5); ++wI) a.add(red[wI][r]);
-        p.partials[(int64_t)blockIdx.x * R + r] = a.value();
+        for (int wI = 0; wI < (int)(blockDim.x >> 5); ++wI) a.add(red[k][wI][r]);
+        p.partials[((int64_t)k * gridDim.x + blockIdx.x) * R + r] = a.value();
     }
     // the last block to finish reduces all blocks in a fixed order
     __shared__ bool last;
@@ -180,16 +190,28 @@ __device__ __forceinline__ void reduce_and_finalize(const StepParams& p, double*
     __syncthreads();
     if (!last) return;
     __threadfence();
-    __shared__ double fin_s[256], fin_c[256], tot[R];
-    grid_fixed_sum(p.partials, (int)gridDim.x, R, fin_s, fin_c, tot);
+    __shared__ double fin_s[256], fin_c[256], tot[NS][R];
+#pragma unroll
+    for (int k = 0; k < NS; ++k)
+        grid_fixed_sum(p.partials + (int64_t)k * gridDim.x * R, (int)gridDim.x, R, fin_s, fin_c, tot[k]);
     if (threadIdx.x < R) {
         const int r = threadIdx.x;
         const unsigned int step = p.counter[1];
         const double nb = p.scal[kScal * r + 1];
-        const double a = tot[r] / (nb * nb);
+        const double a = tot[0][r] / (nb * nb);
         if (!isfinite(a)) atomicOr(&p.counter[2], 1u);
         if ((int)step < p.nmax) p.a_out[(int64_t)r * p.nmax + step] = a;
         p.scal[kScal * r] = a;
+        if constexpr (FUSED) {
+            const double al = (double)(float)(a / nb);
+            const double b2 = tot[1][r] - 2.0 * al * tot[2][r] + al * al * (nb * nb);
+            const double b = sqrt(b2);
+            if (!(b > 0.0) || !isfinite(b)) atomicOr(&p.counter[2], 1u);
+            if ((int)step < p.nmax) p.b_out[(int64_t)r * p.nmax + step] = b;
+            p.scal[kScal * r + 2] = nb;
+            p.scal[kScal * r + 1] = b;
+            p.scal[kScal * r + 3] = al;
+        }
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -206,11 +228,62 @@ __device__ __forceinline__ void reduce_and_finalize(const StepParams& p, double*
 // point at the thread's group in the slice record; the indices come from shared memory (SMEM) or global
 // memory (streamed), the values likewise (SMEM_VAL).  U columns are in flight per batch.
 // FIELD: field-batched values (FieldVal), the thread's field is that of its first right-hand side.
-template <typename VT, bool CPLX, int G, int RPT, int TPR, bool SMEM, bool FIELD, int U, bool SMEM_VAL, int VS = 1>
+// FUSED: x_cur holds v_k and x_prev u_{k-1}; the gathers and the own rows use u_k = v_k - alpha u_{k-1} (one
+// packed FP32 FMA, the same everywhere), u_k is written to u_out, and the three sums of reduce_and_finalize
+// are accumulated (acc_s[3 RPT]).
+template <typename VT, bool CPLX, int G, int RPT, int TPR, bool SMEM, bool FIELD, int U, bool SMEM_VAL, int VS = 1,
+          bool FUSED = false, int NSC = 2>
 __device__ __forceinline__ void group_slice(const StepParams& p, int64_t s, int w, const int32_t* __restrict__ cp,
                                             const typename StoredVal<VT, CPLX, FIELD>::t* __restrict__ vp,
-                                            const double (&sc)[2][RPT * TPR], double* acc_s)
+                                            const double (&sc)[NSC][RPT * TPR], double* acc_s)
 {
+    if constexpr (FUSED) {
+        using C2 = typename V2<VT>::t;
+        constexpr int GPW = 32 / TPR;
+        constexpr int R = RPT * TPR;
+        const int lane = threadIdx.x & 31;
+        const int sub = lane / TPR;
+        const int q = lane % TPR;
+        const C2* __restrict__ xv = static_cast<const C2*>(p.x_cur);
+        const C2* __restrict__ xp = static_cast<const C2*>(p.x_prev);
+        C2* __restrict__ vout = static_cast<C2*>(p.v_out);
+        C2* __restrict__ uout = static_cast<C2*>(p.u_out);
+        const VT* __restrict__ h0 = static_cast<const VT*>(p.h0);
+        const int64_t row0 = (s * GPW + sub) * G;
+        C2 al[RPT];
+#pragma unroll
+        for (int t = 0; t < RPT; ++t) {
+            const VT a = (VT)(-sc[NSC - 1][q * RPT + t]);
+            al[t].x = a;
+            al[t].y = a;
+        }
+        C2 acc[G][RPT];
+        group_columns<VT, CPLX, G, RPT, TPR, SMEM, FIELD, U, SMEM_VAL, VS, true>(xv, w, cp, vp, acc, 0, xp, al);
+#pragma unroll
+        for (int g = 0; g < G; ++g) {
+            C2 xo[RPT], xm[RPT], vn[RPT];
+            VecIO<VT, RPT>::load(xv + (row0 + g) * R + q * RPT, xo);
+            VecIO<VT, RPT>::load(xp + (row0 + g) * R + q * RPT, xm);
+            const VT d = h0[row0 + g];
+#pragma unroll
+            for (int t = 0; t < RPT; ++t) {
+                xo[t] = __ffma2_rn(al[t], xm[t], xo[t]);   // u_k, as the gathers form it
+                acc[g][t].x = fma(d, xo[t].x, acc[g][t].x);
+                acc[g][t].y = fma(d, xo[t].y, acc[g][t].y);
+                const double ib = sc[0][q * RPT + t], rb = sc[1][q * RPT + t];
+                const double yr = acc[g][t].x, yi = acc[g][t].y;
+                vn[t].x = (VT)(yr * ib - rb * (double)xm[t].x);
+                vn[t].y = (VT)(yi * ib - rb * (double)xm[t].y);
+                const double ur = xo[t].x, ui = xo[t].y, vr = vn[t].x, vi = vn[t].y;
+                acc_s[t] += ur * yr + ui * yi;
+                acc_s[RPT + t] += vr * vr + vi * vi;
+                acc_s[2 * RPT + t] += vr * ur + vi * ui;
+            }
+            VecIO<VT, RPT>::store(vout + (row0 + g) * R + q * RPT, vn);
+            VecIO<VT, RPT>::store(uout + (row0 + g) * R + q * RPT, xo);
+        }
+        return;
+    }
     using C2 = typename V2<VT>::t;
     constexpr int GPW = 32 / TPR;
     constexpr int R = RPT * TPR;
@@ -403,7 +476,7 @@ __device__ __forceinline__ void prefetch_ahead(const StepParams& p, int64_t s)
 // is bounded (flag bit 2, GBN_ERR_TIMEOUT).
 // FIELD: the field-batched layout (values FieldVal<VT>, fields p.field_m).
 template <typename VT, bool CPLX, int G, int RPT, int TPR, bool FIELD = false, int U = kColUnroll, bool SV = true,
-          int MINB = 1, bool SLOT = false>
+          int MINB = 1, bool SLOT = false, bool FUSED = false>
 __global__ void __launch_bounds__(256, MINB) k_spmm_staged(StepParams p)
 {
     using HT = typename StoredVal<VT, CPLX, FIELD>::t;
@@ -417,11 +490,13 @@ __global__ void __launch_bounds__(256, MINB) k_spmm_staged(StepParams p)
     uint64_t* bar = reinterpret_cast<uint64_t*>(dyn) + 2 * wib;
     const int64_t cap = p.cap_record;   // bytes of one buffer: whole records (SV) or their index part
     unsigned char* buf = dyn + 128 + (size_t)wib * 2 * cap;
-    __shared__ double sc[2][R];
-    load_step_scalars<R>(p, sc);
-    double acc_s[RPT];
+    constexpr int NSC = FUSED ? 3 : 2;
+    constexpr int NS = FUSED ? 3 : 1;
+    __shared__ double sc[NSC][R];
+    load_step_scalars<R, NSC>(p, sc);
+    double acc_s[NS * RPT];
 #pragma unroll
-    for (int t = 0; t < RPT; ++t) acc_s[t] = 0.0;
+    for (int t = 0; t < NS * RPT; ++t) acc_s[t] = 0.0;
     const int nwb = (int)(blockDim.x >> 5);
     const int64_t per = (p.nslices + gridDim.x - 1) / gridDim.x;
     const int64_t s0 = (int64_t)blockIdx.x * per;
@@ -480,10 +555,10 @@ __global__ void __launch_bounds__(256, MINB) k_spmm_staged(StepParams p)
             if (p.prefetch == 1 || p.prefetch == 2)
                 prefetch_rows<VT, R>(p, reinterpret_cast<const int32_t*>(rec), w * GPW);
             const HT* vp = reinterpret_cast<const HT*>((SV ? rec : grec) + (size_t)w * GPW * 4) + voff;
-            group_slice<VT, CPLX, G, RPT, TPR, true, FIELD, U, SV, VS>(
+            group_slice<VT, CPLX, G, RPT, TPR, true, FIELD, U, SV, VS, FUSED, NSC>(
                 p, s, w, reinterpret_cast<const int32_t*>(rec) + sub, vp, sc, acc_s);
         } else {
-            group_slice<VT, CPLX, G, RPT, TPR, false, FIELD, U, false, VS>(
+            group_slice<VT, CPLX, G, RPT, TPR, false, FIELD, U, false, VS, FUSED, NSC>(
                 p, s, w, reinterpret_cast<const int32_t*>(grec) + sub,
                 reinterpret_cast<const HT*>(grec + (size_t)w * GPW * 4) + voff, sc, acc_s);
         }
@@ -500,7 +575,7 @@ __global__ void __launch_bounds__(256, MINB) k_spmm_staged(StepParams p)
             if ((pending >> st) & 1u) mbar_wait_bounded(&bar[st], (phase >> st) & 1u);
         __syncwarp();
     }
-    reduce_and_finalize<RPT, TPR>(p, acc_s);
+    reduce_and_finalize<RPT, TPR, FUSED>(p, acc_s);
 }
 
 // ---------------------------------------------------------------------------- tile-local product
@@ -750,6 +825,14 @@ StepFn step_variant(bool staged, StepVariant v)
 {
     constexpr int kWide = sizeof(VT) == 4 ? 4 : 2;   // right-hand sides of a 32-byte load
     constexpr bool kAll = !CPLX && (RP == kWide || TP == 1);
+    if (v.fused) {   // staged, real FP32, the widest loads, unroll 8, whole records
+        if constexpr (sizeof(VT) == 4 && !CPLX && RP == 4 && TP >= 2) {
+            if (!staged || v.unroll != 8 || !v.stage_values) return nullptr;
+            if (v.min_blocks == 2) return k_spmm_staged<VT, CPLX, G, RP, TP, false, 8, true, 2, false, true>;
+            if (v.min_blocks == 1) return k_spmm_staged<VT, CPLX, G, RP, TP, false, 8, true, 1, false, true>;
+        }
+        return nullptr;
+    }
     if constexpr (kAll) {
         if (!staged) {
             if (v.min_blocks != 1) return nullptr;

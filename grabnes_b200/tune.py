@@ -6,43 +6,44 @@ and with it the groups a warp processes per slice), the matrix path (slice recor
 memory by per-warp bulk copies, or read from global memory), the union columns whose gathers are in
 flight together (4 or 8), a prefetch (staged path only) of the gather rows of each slice, of the rows
 its epilogue reads, or of those and the rows of u_k one or more sweeps ahead, and a cap on resident
-blocks per SM.  The search runs in two stages on the caller's own Hamiltonian and start vectors:
-the layout and path (rows per group, right-hand sides per thread, staged or not) at the default
+blocks per SM, and the fused step (the update folded into the product, one launch per step; real FP32
+layouts at the widest loads).  The search runs in two stages on the caller's own Hamiltonian and start
+vectors: the layout and path (rows per group, right-hand sides per thread, staged or not) at the default
 variant, then, for the best layout of each rows-per-group value, the variant (unroll, prefetch, staged
-values or indices, the register bound for 1, 2 or 3 blocks per SM), and the same for its staged layout at
-the widest vector loads.  Each candidate runs a short
-recursion; the one with the smallest device time per step (update + sparse product, CUDA events) is
-kept on the context.
+values or indices, the register bound for 1, 2 or 3 blocks per SM, fused or two launches), and the same
+for its staged layout at the widest vector loads.  Each candidate runs a short recursion; the one with
+the smallest device time per step (update + sparse product, CUDA events) is kept on the context.
 """
 import itertools
 
 
 def _time(ctx, u, precision, nsteps, cand):
-    grp, st, pf, rpt, bps, unroll, sv, mb = cand
+    grp, st, pf, rpt, bps, unroll, sv, mb, fu = cand
+    what = dict(rows_per_group=grp, staged=st, prefetch=pf, rhs_per_thread=rpt, blocks_per_sm=bps, unroll=unroll,
+                stage_values=sv, min_blocks=mb, fused=fu)
     try:
         ctx.set_tuning(rpt, bps, grp, st, pf)
-        ctx.set_kernel_variant(unroll, sv, mb, -1)
+        ctx.set_kernel_variant(unroll, sv, mb, -1, -1, fu)
         ctx.stage_phases(u, precision)
         ctx.run_staged(nsteps)
         ctx.run_staged(nsteps)
     except Exception as exc:   # a candidate the library refuses is skipped
-        return dict(rows_per_group=grp, staged=st, prefetch=pf, rhs_per_thread=rpt, blocks_per_sm=bps,
-                    unroll=unroll, stage_values=sv, min_blocks=mb, error=str(exc))
+        return dict(what, error=str(exc))
     spmm, upd = ctx.kernel_timing()
-    return dict(rows_per_group=grp, staged=st, prefetch=pf, rhs_per_thread=rpt, blocks_per_sm=bps, unroll=unroll,
-                stage_values=sv, min_blocks=mb, spmm_ms=spmm, update_ms=upd, step_ms=spmm + upd)
+    return dict(what, spmm_ms=spmm, update_ms=upd, step_ms=spmm + upd)
 
 
 def _key(r):
     return (r["rows_per_group"], r["staged"], r["prefetch"], r["rhs_per_thread"], r["blocks_per_sm"], r["unroll"],
-            r["stage_values"], r["min_blocks"])
+            r["stage_values"], r["min_blocks"], r.get("fused", -1))
 
 
 def apply(ctx, best):
     """Set a tuning dictionary (as returned by autotune) on the context."""
     ctx.set_tuning(best["rhs_per_thread"], best["blocks_per_sm"], best["rows_per_group"], best["staged"],
                    best["prefetch"])
-    ctx.set_kernel_variant(best.get("unroll", 0), best.get("stage_values", -1), best.get("min_blocks", 0), -1)
+    ctx.set_kernel_variant(best.get("unroll", 0), best.get("stage_values", -1), best.get("min_blocks", 0), -1, -1,
+                           best.get("fused", -1))
 
 
 def autotune(ctx, u, precision, nsteps=12, rhs_per_thread=(1, 2, 4), blocks_per_sm=(0,),
@@ -50,7 +51,7 @@ def autotune(ctx, u, precision, nsteps=12, rhs_per_thread=(1, 2, 4), blocks_per_
     results = []
     # stage 1: layout and matrix path at the library's default variant (-1/0: chosen by the library)
     for grp, st, rpt, bps in itertools.product(rows_per_group, staged, rhs_per_thread, blocks_per_sm):
-        results.append(_time(ctx, u, precision, nsteps, (grp, st, -1, rpt, bps, 0, -1, 0)))
+        results.append(_time(ctx, u, precision, nsteps, (grp, st, -1, rpt, bps, 0, -1, 0, -1)))
     ok = [r for r in results if "step_ms" in r]
     # stage 2: for the best layout of every rows-per-group value, the unroll, prefetch, staged values or
     # indices only, and the register bound (1, 2 or 3 blocks per SM): the best variant differs between
@@ -76,11 +77,20 @@ def autotune(ctx, u, precision, nsteps=12, rhs_per_thread=(1, 2, 4), blocks_per_
                 continue
             if mb == 2 and sv == 0:
                 continue
-            cand = (grp, lay["staged"], pf, lay["rhs_per_thread"], lay["blocks_per_sm"], un, sv, mb)
+            cand = (grp, lay["staged"], pf, lay["rhs_per_thread"], lay["blocks_per_sm"], un, sv, mb, -1)
             if cand in seen:
                 continue
             seen.add(cand)
             results.append(_time(ctx, u, precision, nsteps, cand))
+        # the fused step: staged whole records, unroll 8, registers for one or two blocks per SM (the library
+        # refuses shapes without it)
+        if lay["staged"] == 1 and grp <= 2:
+            for pf, mb in itertools.product(pfs, (1, 2)):
+                cand = (grp, 1, pf, lay["rhs_per_thread"], lay["blocks_per_sm"], 8, 1, mb, 1)
+                if cand in seen:
+                    continue
+                seen.add(cand)
+                results.append(_time(ctx, u, precision, nsteps, cand))
     ok = [r for r in results if "step_ms" in r]
     best = min(ok, key=lambda r: r["step_ms"])
     apply(ctx, best)

@@ -160,10 +160,13 @@ int         gbn_set_tuning(gbn_ctx* ctx, int32_t rhs_per_thread, int32_t blocks_
  * (1, 2 or 3; 2 and 3 only with unroll 8 on the staged path, 2 only with whole records staged; 0 = 1); for gbn_lanczos_fields, whether each tile's
  * Peierls rotations are tabulated once before its steps (1) or done on the fly by every thread at every
  * step (0, -1 = the default); and the tile-local product (1: mixed precision, real hoppings; each tile of
- * slices copies the rows it gathers into shared memory first; 0, -1 = the default: no).  No counterpart in
- * the reference.  Used by the autotuner (grabnes_b200/tune.py). */
+ * slices copies the rows it gathers into shared memory first; 0, -1 = the default: no); and the fused step
+ * (1: mixed precision, real hoppings, staged records, 4 right-hand sides per thread, unroll 8; the update
+ * folded into the product: every gathered column forms u_k = v_k - alpha u_{k-1} from two stored vectors,
+ * and b_k comes from three sums of the previous product, so a step is one launch; 0, -1 = the default: no).
+ * No counterpart in the reference.  Used by the autotuner (grabnes_b200/tune.py). */
 int         gbn_set_kernel_variant(gbn_ctx* ctx, int32_t col_unroll, int32_t stage_values, int32_t min_blocks,
-                                   int32_t field_table, int32_t tiled);
+                                   int32_t field_table, int32_t tiled, int32_t fused);
 /* Kernels launched by this context since creation (for launch accounting). */
 int64_t     gbn_launch_count(const gbn_ctx* ctx);
 /* Device time of the recursion loop of the last gbn_lanczos* / gbn_run_staged call and its number of

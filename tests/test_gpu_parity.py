@@ -299,6 +299,47 @@ def test_kernel_variants_agree(ctx, grp, prec):
         assert _rel(runs[0][0][0], a0) <= 1e-10 and _rel(runs[0][1][0], b0) <= 1e-10
 
 
+@pytest.mark.parametrize("name", ["tbg", "moire_twist", "graphene"])
+@pytest.mark.parametrize("grp,mb", [(1, 2), (2, 2), (2, 1), (4, 1)])
+def test_fused_step(ctx, name, grp, mb):
+    """The fused step (the update folded into the product: each gathered column forms u_k = v_k - alpha
+    u_{k-1} in FP32 with an FP32 alpha, b_k from |v_{k+1}|^2, Re<v_{k+1}, u_k> and b_{k-1}) in mixed
+    precision, 137 steps (eager steps, graph replays and a remainder), against the oracle's FP64 recursion:
+    a_n, b_n of vector 0 within three times the two-launch mixed path's own deviation (the two round u_k
+    differently, so they part in the last bits and drift apart like any two mixed runs), and the DOS
+    within the mixed path's bar, 1e-6 normalised L1; one launch per step instead of two."""
+    r = built(name)
+    n = r["geo"]["n"]
+    ctx.load_hamiltonian(r["nb"]["nneigh"], r["nb"]["nlist"], r["hop"], r["h0"])
+    u = np.stack([orc.rng_draws(41 + k, n) for k in range(16)])
+    nsteps = 137
+    try:
+        ctx.set_tuning(4, 0, grp, 1, 6)
+        ctx.set_kernel_variant(8, 1, mb, -1, -1, 0)
+        l0 = ctx.launches
+        a2, b2 = ctx.lanczos_phases(u, nsteps, G.GBN_MIXED)
+        two = ctx.launches - l0
+        ctx.set_kernel_variant(8, 1, mb, -1, -1, 1)
+        l0 = ctx.launches
+        a1, b1 = ctx.lanczos_phases(u, nsteps, G.GBN_MIXED)
+        one = ctx.launches - l0
+    finally:
+        ctx.set_tuning()
+        ctx.set_kernel_variant()
+    assert two - one >= nsteps   # the update launches are gone
+    psi = np.exp(2j * np.pi * u[0]) / np.sqrt(n)
+    a0, b0 = orc.recursion(r["nb"], r["hop"], r["h0"], psi, nsteps, 0)
+    e2 = max(_rel(a2[0], a0), _rel(b2[0], b0))
+    e1 = max(_rel(a1[0], a0), _rel(b1[0], b0))
+    print(name, grp, mb, "deviation from FP64: two-launch", e2, "fused", e1)
+    assert e1 <= 3.0 * e2 + 1e-7
+    g0 = r["g0"]
+    args = (0.01 / g0, 800, -1.0 / g0, 1.0 / g0)
+    _, d0 = orc.frac(a0, b0, *args)
+    _, d1 = ctx.cf_dos(a1[:1], b1[:1], *args)
+    assert np.abs(d1[0] - d0).sum() <= 1e-6 * np.abs(d0).sum()
+
+
 @pytest.mark.parametrize("grp", [1, 2, 4])
 def test_fp64_every_layout(ctx, grp):
     """FP64 recursion through each matrix layout and matrix path against the oracle (1e-10 relative,
