@@ -211,7 +211,8 @@ def run_ours(args, ws, rank, local):
     else:
         best, tuning = autotune(ctx, u, G.GBN_MIXED)
         best = dict(best, candidates_top5=sorted((r for r in tuning if "step_ms" in r),
-                                                  key=lambda r: r["step_ms"])[:5])
+                                                  key=lambda r: r["step_ms"])[:5],
+                    best_of_each_step_form=best_of_each_form(tuning))
     ctx.stage_phases(u, G.GBN_MIXED)
     for _ in range(args.warmup):
         ctx.run_staged(nsteps)
@@ -551,6 +552,16 @@ def gradient_leg(G, M, local, stream, ws, nrecurs=600, checkpoint=32):
 MOIRE_DOS_KEYS = {k: v for k, v in TEVOL_KEYS.items() if not k.startswith("Disorder.")}
 
 
+def best_of_each_form(cands):
+    """The autotuner's fastest candidate of each step form: two launches (product + update) and fused."""
+    out = {}
+    for form, sel in (("two_launches", lambda r: r.get("fused", -1) != 1), ("fused", lambda r: r.get("fused", -1) == 1)):
+        ok = [r for r in cands if "step_ms" in r and sel(r)]
+        if ok:
+            out[form] = min(ok, key=lambda r: r["step_ms"])
+    return out
+
+
 def fixed_tuning(spec):
     """A tuning dictionary from 'rhs_per_thread,blocks_per_sm,rows_per_group,staged,prefetch[,unroll
     [,stage_values[,min_blocks[,fused]]]]'."""
@@ -583,7 +594,8 @@ def moire_dos_leg(G, M, local, stream, ws, nrhs=16, nsteps=2000, peak=None, tuni
     else:
         best, cands = autotune(ctx, u, G.GBN_MIXED)
         best = dict(best, candidates_top5=sorted((r for r in cands if "step_ms" in r),
-                                                  key=lambda r: r["step_ms"])[:5])
+                                                  key=lambda r: r["step_ms"])[:5],
+                    best_of_each_step_form=best_of_each_form(cands))
     ctx.stage_phases(u, G.GBN_MIXED)
     ctx.run_staged(200)
     torch.cuda.synchronize()
