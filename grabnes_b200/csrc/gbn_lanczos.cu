@@ -1,4 +1,4 @@
-// Batched Lanczos recursion on the B200: two launches per recursion step.
+// Batched Lanczos recursion on the B200: two launches per recursion step, or one with the fused step.
 //
 // The reference (lanczosKuboCode/Src/kubosubs.F90:26-138) makes three passes over the vectors per
 // step: H psi with <psi, H psi>; w = H psi - a psi - b psi_prev with |w|; the scaling psi = w / b.
@@ -21,6 +21,12 @@
 // brings each warp's next slice record (column indices, and values unless they stream beside the
 // gathers) into shared memory with one bulk asynchronous copy, and U columns' gathers are in flight
 // together, so that only the gathers themselves wait on memory.
+//
+// The fused step (kernel variant fused = 1; real FP32 layouts) folds k_update into the product: product k
+// gathers v_k and u_{k-1} at every union column and forms u_k = v_k - alpha u_{k-1} (alpha = a_{k-1} / b_{k-2}
+// rounded to FP32) with one packed FMA wherever the column is gathered, writes u_k and v_{k+1}, and sums
+// Re<u_k, H u_k>, |v_{k+1}|^2 and Re<v_{k+1}, u_k>; its last block derives a_k and b_k (reduce_and_finalize).
+// v then alternates between vec[0] and vec[3], u between vec[1] and vec[2], and no closing pass is needed.
 #include <algorithm>
 
 #include <cuda_runtime.h>

@@ -170,7 +170,8 @@ int         gbn_set_kernel_variant(gbn_ctx* ctx, int32_t col_unroll, int32_t sta
 /* Kernels launched by this context since creation (for launch accounting). */
 int64_t     gbn_launch_count(const gbn_ctx* ctx);
 /* Device time of the recursion loop of the last gbn_lanczos* / gbn_run_staged call and its number of
- * recursion steps (each step launches one update and one sparse-product kernel). */
+ * recursion steps (each step launches one update and one sparse-product kernel, or one kernel with the
+ * fused step of gbn_set_kernel_variant). */
 int         gbn_last_timing(const gbn_ctx* ctx, double* step_ms_total, int64_t* step_launches);
 /* Average per-launch device time of the sparse-product and the update kernels over the first (up to 64)
  * steps of the last call, measured with CUDA events on the context's stream. */
