@@ -408,9 +408,23 @@ def fields_leg(G, M, local, stream, ws, scale=1.0):
 
     ctx.assemble(job["model"], rat_on, rat_hop, None)
     ctx.lanczos_fields(ms[:2], u[:2, :1], 60, G.GBN_MIXED)   # warm-up (layout, kernels)
+    # the step form of the sweep, chosen on one tile of four fields x 8 vectors, 200 steps: two launches
+    # (product + update) or the fused step with registers for one or two blocks per SM
+    forms = {}
+    for name, variant in (("two_launches", (0, -1, 0, 0, -1, 0)), ("fused_1_block", (0, -1, 1, 0, -1, 1)),
+                          ("fused_2_blocks", (0, -1, 2, 0, -1, 1))):
+        try:
+            ctx.set_kernel_variant(*variant)
+            ctx.lanczos_fields(ms[:4], u[:4], 200, G.GBN_MIXED)
+            forms[name] = (ctx.last_timing()[0], variant)
+        except Exception:
+            pass
+    form = min(forms, key=lambda k: forms[k][0])
+    ctx.set_kernel_variant(*forms[form][1])
     (a, _), t_batch = timed(batched)
     loop_s = ctx.last_timing()[0] / 1e3
     launches = ctx.launches
+    ctx.set_kernel_variant()
     _, t_field = timed(per_field)
     ctx.close()
     name = "graphene_hbn_moire_387200atoms_33fields_x8vec_500-3000steps" + ("" if scale == 1.0 else f"_x{scale:g}")
@@ -418,7 +432,8 @@ def fields_leg(G, M, local, stream, ws, scale=1.0):
             "fields": int(len(ms)), "vectors_per_field": nvec, "useful_atom_steps": work,
             "batched_s": t_batch, "batched_atom_steps_per_s": ws * work / t_batch, "batched_loop_s": loop_s,
             "per_field_s": t_field, "per_field_atom_steps_per_s": ws * work / t_field,
-            "speedup_vs_per_field": t_field / t_batch, "precision": "mixed"}
+            "speedup_vs_per_field": t_field / t_batch, "precision": "mixed", "step_form": form,
+            "step_form_probe_ms": {k: v[0] for k, v in forms.items()}}
 
 
 TEVOL_KEYS = {"Run.TypeOfSystem": "Graphene", "Structure.CellSize": 83, "Structure.SuperCell": 16,

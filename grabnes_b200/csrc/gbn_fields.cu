@@ -53,6 +53,30 @@ StepFn field_table_kernel(int prec, int G, int rpt, int tpr, bool staged)
     return nullptr;
 }
 
+// the fused field product: registers for one block per SM, or bounded for two (min_blocks 2)
+template <int G, int MINB>
+static StepFn pick_field_fused_g(int tpr)
+{
+    if (tpr == 2) return k_spmm_staged<float, false, G, 4, 2, true, kColUnroll, true, MINB, false, true>;
+    if (tpr == 4) return k_spmm_staged<float, false, G, 4, 4, true, kColUnroll, true, MINB, false, true>;
+    if (tpr == 8) return k_spmm_staged<float, false, G, 4, 8, true, kColUnroll, true, MINB, false, true>;
+    return nullptr;
+}
+
+StepFn field_fused_kernel(int prec, int G, int rpt, int tpr, int min_blocks)
+{
+    if (prec != GBN_MIXED || rpt != 4) return nullptr;
+    if (min_blocks == 2) {
+        if (G == 1) return pick_field_fused_g<1, 2>(tpr);
+        if (G == 2) return pick_field_fused_g<2, 2>(tpr);
+        return nullptr;
+    }
+    if (G == 1) return pick_field_fused_g<1, 1>(tpr);
+    if (G == 2) return pick_field_fused_g<2, 1>(tpr);
+    if (G == 4) return pick_field_fused_g<4, 1>(tpr);
+    return nullptr;
+}
+
 StepFn field_step_kernel(int prec, int G, int rpt, int tpr, bool staged)
 {
     if (prec == GBN_MIXED) {

@@ -325,7 +325,7 @@ static int step_launch(gbn_ctx* c, int R, StepLaunch* L)
     v.stage_values = c->tune_stage_values != 0;
     v.min_blocks = c->tune_min_blocks > 0 ? c->tune_min_blocks : (v.unroll == 8 && E.G == 1 && !E.cplx ? 3 : 1);
     // the update folded into the product, where asked for (real FP32 layouts; see k_spmm_staged)
-    v.fused = c->tune_fused == 1 && !E.field;
+    v.fused = c->tune_fused == 1;
     // batched fields rotate on the fly unless the tile table is asked for (measured slower on example 06's
     // sweep: 0.175 against 0.108 ms per product, the table's complex values per thread slot triple the
     // records' bytes)
@@ -345,6 +345,9 @@ static int step_launch(gbn_ctx* c, int R, StepLaunch* L)
         split_rhs(c->prec, R, c->tune_rpt, &rpt, &tpr);
         const StepVariant base;
         if (E.field) {
+            if (v.fused)   // the fused step of the field layout: whole records staged, 4 columns in flight
+                return (staged && !use_table && !(c->tune_unroll > 0 && c->tune_unroll != 4))
+                           ? field_fused_kernel(c->prec, E.G, rpt, tpr, c->tune_min_blocks == 2 ? 2 : 1) : nullptr;
             if (!((v.unroll == 4 && v.stage_values && v.min_blocks == 1) || !asked)) return nullptr;
             if (use_table)
                 return E.ftab_slots == tpr ? field_table_kernel(c->prec, E.G, rpt, tpr, staged) : nullptr;

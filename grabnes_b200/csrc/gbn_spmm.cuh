@@ -157,7 +157,8 @@ template <typename VT> struct FieldMult;
 template <> struct FieldMult<float> { using t = uint32_t; };
 template <> struct FieldMult<double> { using t = uint64_t; };
 
-// FUSED (real FP32 layouts): the gathered vector is formed from two stored ones, x = v + (-alpha) u, by one
+// FUSED (FP32 layouts of real or field-batched values): the gathered vector is formed from two stored ones,
+// x = v + (-alpha) u, by one
 // packed FMA per element from the same two loads wherever the column is gathered (xq: v, xu: u, al: the
 // thread's -alpha pairs), so every row sees the same rounded x.
 template <typename VT, bool CPLX, int G, int RPT, int TPR, bool SMEM, bool SMEM_VAL, bool FIELD, int NB, int VS = 1,
@@ -184,7 +185,7 @@ __device__ __forceinline__ void column_batch(const typename V2<VT>::t* __restric
 #pragma unroll
     for (int u = 0; u < NB; ++u) VecIO<VT, RPT>::load(xq + (size_t)(uint32_t)c[u] * R, xg[u]);
     if constexpr (FUSED) {
-        static_assert(sizeof(VT) == 4 && !CPLX && !FIELD, "the fused gather is for real FP32 layouts");
+        static_assert(sizeof(VT) == 4 && !CPLX, "the fused gather is for FP32 layouts of real or field values");
         C2 xh[NB][RPT];
 #pragma unroll
         for (int u = 0; u < NB; ++u) VecIO<VT, RPT>::load(xu + (size_t)(uint32_t)c[u] * R, xh[u]);

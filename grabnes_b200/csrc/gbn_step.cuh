@@ -51,6 +51,9 @@ using StepFn = void (*)(StepParams);
 // the sparse-product kernel of the field-batched layout (gbn_fields.cu): rotations on the fly, or the
 // tile table (complex values per thread slot)
 StepFn field_step_kernel(int prec, int G, int rpt, int tpr, bool staged);
+// the field-batched product with the update folded in (mixed precision, staged, 4 right-hand sides per
+// thread), nullptr for other shapes
+StepFn field_fused_kernel(int prec, int G, int rpt, int tpr, int min_blocks);
 StepFn field_table_kernel(int prec, int G, int rpt, int tpr, bool staged);
 
 // Variant of the product kernel: columns in flight per batch (4 or 8) and, for the staged kernel,
@@ -258,7 +261,9 @@ __device__ __forceinline__ void group_slice(const StepParams& p, int64_t s, int 
             al[t].y = a;
         }
         C2 acc[G][RPT];
-        group_columns<VT, CPLX, G, RPT, TPR, SMEM, FIELD, U, SMEM_VAL, VS, true>(xv, w, cp, vp, acc, 0, xp, al);
+        typename FieldMult<VT>::t mf = 0;
+        if constexpr (FIELD) mf = (typename FieldMult<VT>::t)(int64_t)p.field_m[q * RPT];
+        group_columns<VT, CPLX, G, RPT, TPR, SMEM, FIELD, U, SMEM_VAL, VS, true>(xv, w, cp, vp, acc, mf, xp, al);
 #pragma unroll
         for (int g = 0; g < G; ++g) {
             C2 xo[RPT], xm[RPT], vn[RPT];

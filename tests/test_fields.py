@@ -127,6 +127,40 @@ def test_fields_mixed_dos(ctx, base):
         assert err_fld <= 1e-6, (m, err_fld, err_mix)
 
 
+@pytest.mark.parametrize("mb", [1, 2])
+def test_fields_fused_step(ctx, base, mb):
+    """The fused step on the field-batched layout (gathers of v_k and u_{k-1} rotated per field, u_k formed
+    in the gather, one launch per step): the DOS of each field within 1e-6 (normalised L1) of the FP64
+    oracle's on that field's Hamiltonian, and at least one launch per step fewer than the two-launch step."""
+    n, g0 = base["geo"]["n"], base["g0"]
+    u = _draws(n)
+    _field_free(ctx, base)
+    try:
+        ctx.set_kernel_variant(0, -1, 0, 0, -1, 0)
+        l0 = ctx.launches
+        ctx.lanczos_fields(FIELDS, u, 120, G.GBN_MIXED)
+        two = ctx.launches - l0
+        ctx.set_kernel_variant(0, -1, mb, 0, -1, 1)
+        l0 = ctx.launches
+        a, b = ctx.lanczos_fields(FIELDS, u, 120, G.GBN_MIXED)
+        one = ctx.launches - l0
+    finally:
+        ctx.set_kernel_variant()
+    assert two - one >= 120
+    eta, ne, lo, hi = 0.02 / g0, 600, -0.6 / g0, 0.6 / g0
+    for f, m in enumerate(FIELDS):
+        r = R.build(dict(MOIRE, MagFieldInteger=m)) if m else base
+        d_ref = 0.0
+        d_fld = 0.0
+        for v in range(NVEC):
+            psi = np.exp(2j * np.pi * u[f, v]) / np.sqrt(n)
+            a0, b0 = orc.recursion(r["nb"], r["hop"], r["h0"], psi, 120, 0)
+            d_ref = d_ref + orc.frac(a0, b0, eta, ne, lo, hi)[1]
+            d_fld = d_fld + orc.frac(a[f, v], b[f, v], eta, ne, lo, hi)[1]
+        err = np.abs(d_fld - d_ref).sum() / np.abs(d_ref).sum()
+        assert err <= 1e-6, (m, err)
+
+
 def test_fields_reject_a_field_already_applied(ctx, base):
     _field_free(ctx, base)
     ctx.peierls(R.build(dict(MOIRE, MagFieldInteger=2))["flux"])
