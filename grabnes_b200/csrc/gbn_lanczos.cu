@@ -324,8 +324,15 @@ static int step_launch(gbn_ctx* c, int R, StepLaunch* L)
     v.unroll = c->tune_unroll > 0 ? c->tune_unroll : (c->prec == GBN_MIXED ? 8 : 4);
     v.stage_values = c->tune_stage_values != 0;
     v.min_blocks = c->tune_min_blocks > 0 ? c->tune_min_blocks : (v.unroll == 8 && E.G == 1 && !E.cplx ? 3 : 1);
-    // the update folded into the product, where asked for (real FP32 layouts; see k_spmm_staged)
-    v.fused = c->tune_fused == 1;
+    // the update folded into the product (FP32 layouts; see k_spmm_staged), its registers bounded for two
+    // blocks per SM unless another bound is asked for.  By default in mixed precision where rows hold at
+    // most 8 entries on average: one launch per step there was 3-24 % faster on graphene and graphene/hBN
+    // cells of 15k-3.5M atoms with 8-32 vectors, and the doubled gathers made it slower on the twisted
+    // bilayer's 33 entries per row (504 against 387 us per step, 1.1M atoms, 16 vectors)
+    const bool fused_default = c->tune_fused < 0 && c->prec == GBN_MIXED && c->n > 0 && c->total <= 8 * c->n;
+    const StepVariant v_two = v;
+    v.fused = c->tune_fused == 1 || fused_default;
+    if (v.fused && c->tune_min_blocks <= 0) v.min_blocks = 2;
     // batched fields rotate on the fly unless the tile table is asked for (measured slower on example 06's
     // sweep: 0.175 against 0.108 ms per product, the table's complex values per thread slot triple the
     // records' bytes)
@@ -339,7 +346,7 @@ static int step_launch(gbn_ctx* c, int R, StepLaunch* L)
     };
     const bool want_staged = c->tune_staged != 0 && cap_of(0) > 0;
     // the kernel of this variant; shapes without it take the base variant unless one was asked for
-    const bool asked = c->tune_unroll > 0 || c->tune_stage_values >= 0 || c->tune_min_blocks > 0 || v.fused;
+    const bool asked = c->tune_unroll > 0 || c->tune_stage_values >= 0 || c->tune_min_blocks > 0 || c->tune_fused == 1;
     auto pick = [&](bool staged) -> StepFn {
         int rpt, tpr;
         split_rhs(c->prec, R, c->tune_rpt, &rpt, &tpr);
@@ -347,17 +354,22 @@ static int step_launch(gbn_ctx* c, int R, StepLaunch* L)
         if (E.field) {
             if (v.fused)   // the fused step of the field layout: whole records staged, 4 columns in flight
                 return (staged && !use_table && !(c->tune_unroll > 0 && c->tune_unroll != 4))
-                           ? field_fused_kernel(c->prec, E.G, rpt, tpr, c->tune_min_blocks == 2 ? 2 : 1) : nullptr;
+                           ? field_fused_kernel(c->prec, E.G, rpt, tpr, v.min_blocks == 2 ? 2 : 1) : nullptr;
             if (!((v.unroll == 4 && v.stage_values && v.min_blocks == 1) || !asked)) return nullptr;
             if (use_table)
                 return E.ftab_slots == tpr ? field_table_kernel(c->prec, E.G, rpt, tpr, staged) : nullptr;
             return field_step_kernel(c->prec, E.G, rpt, tpr, staged);
         }
         StepFn f = step_kernel(c->prec, E.cplx, E.G, R, c->tune_rpt, staged, v);
+        if (!f && v.fused && fused_default) return nullptr;   // the caller takes the two-launch step
         if (!f && !asked) f = step_kernel(c->prec, E.cplx, E.G, R, c->tune_rpt, staged, base);
         return f;
     };
     L->fn = pick(want_staged);
+    if (!L->fn && fused_default) {   // no fused kernel for this shape: the two-launch step
+        v = v_two;
+        L->fn = pick(want_staged);
+    }
     if (!L->fn) return fail(c, GBN_ERR_ARG, "no recursion kernel for this tile width and kernel variant");
     L->fused = v.fused;
     L->block = 256;
@@ -401,6 +413,10 @@ static int step_launch(gbn_ctx* c, int R, StepLaunch* L)
         }
     }
     if (want_staged && !L->staged) {   // no buffer fits: the plain kernel
+        if (fused_default && v.fused) {   // the fused step is staged only
+            v = v_two;
+            L->fused = false;
+        }
         L->fn = pick(false);
         if (!L->fn) return fail(c, GBN_ERR_ARG, "no recursion kernel for this tile width and kernel variant");
     }

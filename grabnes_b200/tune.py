@@ -35,7 +35,7 @@ def _time(ctx, u, precision, nsteps, cand):
 
 def _key(r):
     return (r["rows_per_group"], r["staged"], r["prefetch"], r["rhs_per_thread"], r["blocks_per_sm"], r["unroll"],
-            r["stage_values"], r["min_blocks"], r.get("fused", -1))
+            r["stage_values"], r["min_blocks"], r.get("fused", 0))
 
 
 def apply(ctx, best):
@@ -51,7 +51,7 @@ def autotune(ctx, u, precision, nsteps=12, rhs_per_thread=(1, 2, 4), blocks_per_
     results = []
     # stage 1: layout and matrix path at the library's default variant (-1/0: chosen by the library)
     for grp, st, rpt, bps in itertools.product(rows_per_group, staged, rhs_per_thread, blocks_per_sm):
-        results.append(_time(ctx, u, precision, nsteps, (grp, st, -1, rpt, bps, 0, -1, 0, -1)))
+        results.append(_time(ctx, u, precision, nsteps, (grp, st, -1, rpt, bps, 0, -1, 0, 0)))
     ok = [r for r in results if "step_ms" in r]
     # stage 2: for the best layout of every rows-per-group value, the unroll, prefetch, staged values or
     # indices only, and the register bound (1, 2 or 3 blocks per SM): the best variant differs between
@@ -77,7 +77,7 @@ def autotune(ctx, u, precision, nsteps=12, rhs_per_thread=(1, 2, 4), blocks_per_
                 continue
             if mb == 2 and sv == 0:
                 continue
-            cand = (grp, lay["staged"], pf, lay["rhs_per_thread"], lay["blocks_per_sm"], un, sv, mb, -1)
+            cand = (grp, lay["staged"], pf, lay["rhs_per_thread"], lay["blocks_per_sm"], un, sv, mb, 0)
             if cand in seen:
                 continue
             seen.add(cand)
