@@ -336,7 +336,9 @@ def run_ours(args, ws, rank, local):
                      "kernel": kname, "avg_launch_ms": spmm_ms, "update_kernel_ms": update_ms,
                      "step_ms": kern_ms / kern_launches,
                      "step_achieved": b_alg / (kern_ms / kern_launches / 1e3) / 1e9,
-                     "step_frac": b_alg / (kern_ms / kern_launches / 1e3) / 1e9 / peak},
+                     "step_frac": b_alg / (kern_ms / kern_launches / 1e3) / 1e9 / peak,
+                     # the DRAM bytes the kernel actually moves (ncu) over its live launch time
+                     "traffic_frac": (traffic / (spmm_ms / 1e3) / 1e9 / peak) if traffic else None},
         "tuning": best,
         "fp64": {"batched_atom_steps_per_s": atom_steps / (fp64_batched_kernel_ms / 1e3),
                  "single_vector_atom_steps_per_s": float(n) * nsteps / (fp64_single_kernel_ms / 1e3),
@@ -640,7 +642,11 @@ def moire_dos_leg(G, M, local, stream, ws, nrhs=16, nsteps=2000, peak=None, tuni
             "step_ms": step, "spmm_ms": spmm_ms, "update_ms": upd_ms,
             "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
                          "frac": (ach / peak) if peak else None, "algorithmic_bytes_per_launch": b_alg,
-                         "kernel": kname, "traffic": traffic, "traffic_source": traffic_src},
+                         "kernel": kname, "traffic": traffic, "traffic_source": traffic_src,
+                         # the DRAM bytes the kernel actually moves (ncu) over its live launch time; the
+                         # fused step's kernel is the whole step and moves 32 of every 24 algorithmic bytes
+                         "traffic_frac": (traffic / (spmm_ms / 1e3) / 1e9 / peak) if (traffic and peak) else None,
+                         "kernel_is_whole_step": best.get("fused", -1) == 1},
             "step_frac": (b_alg / (step / 1e3) / 1e9 / peak) if peak else None,
             "step_achieved_gbs": b_alg / (step / 1e3) / 1e9,
             "dos_error_vs_fp64_vector0": float(np.abs(d_mix[0] - d_64[0]).sum() / np.abs(d_64[0]).sum())}
