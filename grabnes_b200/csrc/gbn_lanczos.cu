@@ -598,7 +598,8 @@ int lanczos_run(gbn_ctx* c, int32_t nmax)
     // the block partials of this launch shape (it may differ from the one the buffers were sized for)
     GBN_CK(c, c->partials.ensure(sizeof(double) * (size_t)R * (L.fused ? 3 : 1) *
                                  (size_t)std::max(L.grid, c->num_sms * kUpdateBlocksPerSM)));
-    if (L.fused) GBN_CK(c, c->vec[3].ensure((size_t)c->ell.npad * R * sizeof(float2)));
+    if (L.fused)
+        GBN_CK(c, c->vec[3].ensure((size_t)c->ell.npad * R * (c->prec == GBN_MIXED ? sizeof(float2) : sizeof(double2))));
     StepParams p;
     memset(&p, 0, sizeof p);
     p.slice_ptr = c->ell.slice_ptr.as<int64_t>();
