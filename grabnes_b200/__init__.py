@@ -221,8 +221,8 @@ class Context:
         records carry the values (1) or only the column indices (0; -1 = default), the resident blocks per
         SM its registers are bounded for (1, 2, 3; 0 = 1), and for batched fields the per-tile rotation table
         (1) or rotations on the fly (0, -1 = default), the tile-local product (1; 0, -1 = default: no), and
-        the fused step, the update folded into the product (1; 0 two launches; -1 = default: fused in mixed
-        precision on cells of at most 8 entries per row)."""
+        the fused step, the update folded into the product (1; 0 two launches; -1 = default: fused on cells
+        of at most 8 entries per row)."""
         self._ck(self._L.gbn_set_kernel_variant(self._h, col_unroll, stage_values, min_blocks, field_table, tiled,
                                                 fused))
 

@@ -324,12 +324,12 @@ static int step_launch(gbn_ctx* c, int R, StepLaunch* L)
     v.unroll = c->tune_unroll > 0 ? c->tune_unroll : (c->prec == GBN_MIXED ? 8 : 4);
     v.stage_values = c->tune_stage_values != 0;
     v.min_blocks = c->tune_min_blocks > 0 ? c->tune_min_blocks : (v.unroll == 8 && E.G == 1 && !E.cplx ? 3 : 1);
-    // the update folded into the product (FP32 layouts; see k_spmm_staged), its registers bounded for two
-    // blocks per SM unless another bound is asked for.  By default in mixed precision where rows hold at
-    // most 8 entries on average: one launch per step there was 3-24 % faster on graphene and graphene/hBN
-    // cells of 15k-3.5M atoms with 8-32 vectors, and the doubled gathers made it slower on the twisted
-    // bilayer's 33 entries per row (504 against 387 us per step, 1.1M atoms, 16 vectors)
-    const bool fused_default = c->tune_fused < 0 && c->prec == GBN_MIXED && c->n > 0 && c->total <= 8 * c->n;
+    // the update folded into the product (see k_spmm_staged), its registers bounded for two blocks per SM
+    // unless another bound is asked for.  By default where rows hold at most 8 entries on average: one launch
+    // per step there was 3-24 % faster in mixed precision and 10-95 % faster in FP64 on graphene and
+    // graphene/hBN cells of 15k-3.5M atoms with 8-32 vectors, and the doubled gathers made it slower on the
+    // twisted bilayer's 33 entries per row (mixed: 504 against 387 us per step, 1.1M atoms, 16 vectors)
+    const bool fused_default = c->tune_fused < 0 && c->n > 0 && c->total <= 8 * c->n;
     const StepVariant v_two = v;
     v.fused = c->tune_fused == 1 || fused_default;
     if (v.fused && c->tune_min_blocks <= 0) v.min_blocks = 2;

@@ -157,7 +157,14 @@ template <typename VT> struct FieldMult;
 template <> struct FieldMult<float> { using t = uint32_t; };
 template <> struct FieldMult<double> { using t = uint64_t; };
 
-// FUSED (FP32 layouts of real or field-batched values): the gathered vector is formed from two stored ones,
+// x = v + a u per element, the same instruction wherever it is formed (packed FP32 FMA, or two FP64 FMAs)
+__device__ __forceinline__ float2 fused_form(float2 a, float2 u, float2 v) { return __ffma2_rn(a, u, v); }
+__device__ __forceinline__ double2 fused_form(double2 a, double2 u, double2 v)
+{
+    return make_double2(fma(a.x, u.x, v.x), fma(a.y, u.y, v.y));
+}
+
+// FUSED (real or field-batched values): the gathered vector is formed from two stored ones,
 // x = v + (-alpha) u, by one
 // packed FMA per element from the same two loads wherever the column is gathered (xq: v, xu: u, al: the
 // thread's -alpha pairs), so every row sees the same rounded x.
@@ -185,14 +192,14 @@ __device__ __forceinline__ void column_batch(const typename V2<VT>::t* __restric
 #pragma unroll
     for (int u = 0; u < NB; ++u) VecIO<VT, RPT>::load(xq + (size_t)(uint32_t)c[u] * R, xg[u]);
     if constexpr (FUSED) {
-        static_assert(sizeof(VT) == 4 && !CPLX, "the fused gather is for FP32 layouts of real or field values");
+        static_assert(!CPLX, "the fused gather is for layouts of real or field-batched values");
         C2 xh[NB][RPT];
 #pragma unroll
         for (int u = 0; u < NB; ++u) VecIO<VT, RPT>::load(xu + (size_t)(uint32_t)c[u] * R, xh[u]);
 #pragma unroll
         for (int u = 0; u < NB; ++u)
 #pragma unroll
-            for (int t = 0; t < RPT; ++t) xg[u][t] = __ffma2_rn(al[t], xh[u][t], xg[u][t]);
+            for (int t = 0; t < RPT; ++t) xg[u][t] = fused_form(al[t], xh[u][t], xg[u][t]);
     }
 #pragma unroll
     for (int u = 0; u < NB; ++u) load_group_vals<HT, G, SMEM_VAL>(vp + u * GPW * G * VS, h[u]);

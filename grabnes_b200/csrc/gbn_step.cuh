@@ -154,10 +154,11 @@ __device__ __forceinline__ void load_step_scalars(const StepParams& p, double (&
 // Reduction of the sum Re<u_k, H u_k> over the block, then by the last block over all blocks in a fixed
 // order; writes a_k = Re<u_k, H u_k> / b_{k-1}^2 and advances the step index.
 // FUSED: three sums per right-hand side, S_a = Re<u_k, H u_k>, S_vv = |v_{k+1}|^2 and S_vu = Re<v_{k+1}, u_k>
-// (acc_s[s * RPT + t], block partials in planes [s][block][R]).  With alpha = a_k / b_{k-1} rounded to FP32 (the
-// value the next step forms u_{k+1} = v_{k+1} - alpha u_k with), b_k^2 = |u_{k+1}|^2 = S_vv - 2 alpha S_vu +
-// alpha^2 b_{k-1}^2; the finish writes a_k and b_k and shifts the norms, as the update kernel does otherwise.
-template <int RPT, int TPR, bool FUSED = false>
+// (acc_s[s * RPT + t], block partials in planes [s][block][R]).  With alpha = a_k / b_{k-1} (rounded to FP32
+// for FP32 vectors, AL32: the value the next step forms u_{k+1} = v_{k+1} - alpha u_k with), b_k^2 =
+// |u_{k+1}|^2 = S_vv - 2 alpha S_vu + alpha^2 b_{k-1}^2; the finish writes a_k and b_k and shifts the norms, as
+// the update kernel does otherwise.
+template <int RPT, int TPR, bool FUSED = false, bool AL32 = true>
 __device__ __forceinline__ void reduce_and_finalize(const StepParams& p, double* acc_s)
 {
     constexpr int R = RPT * TPR;
@@ -206,7 +207,7 @@ __device__ __forceinline__ void reduce_and_finalize(const StepParams& p, double*
         if ((int)step < p.nmax) p.a_out[(int64_t)r * p.nmax + step] = a;
         p.scal[kScal * r] = a;
         if constexpr (FUSED) {
-            const double al = (double)(float)(a / nb);
+            const double al = AL32 ? (double)(float)(a / nb) : a / nb;
             const double b2 = tot[1][r] - 2.0 * al * tot[2][r] + al * al * (nb * nb);
             const double b = sqrt(b2);
             if (!(b > 0.0) || !isfinite(b)) atomicOr(&p.counter[2], 1u);
@@ -272,7 +273,7 @@ __device__ __forceinline__ void group_slice(const StepParams& p, int64_t s, int 
             const VT d = h0[row0 + g];
 #pragma unroll
             for (int t = 0; t < RPT; ++t) {
-                xo[t] = __ffma2_rn(al[t], xm[t], xo[t]);   // u_k, as the gathers form it
+                xo[t] = fused_form(al[t], xm[t], xo[t]);   // u_k, as the gathers form it
                 acc[g][t].x = fma(d, xo[t].x, acc[g][t].x);
                 acc[g][t].y = fma(d, xo[t].y, acc[g][t].y);
                 const double ib = sc[0][q * RPT + t], rb = sc[1][q * RPT + t];
@@ -580,7 +581,7 @@ __global__ void __launch_bounds__(256, MINB) k_spmm_staged(StepParams p)
             if ((pending >> st) & 1u) mbar_wait_bounded(&bar[st], (phase >> st) & 1u);
         __syncwarp();
     }
-    reduce_and_finalize<RPT, TPR, FUSED>(p, acc_s);
+    reduce_and_finalize<RPT, TPR, FUSED, sizeof(VT) == 4>(p, acc_s);
 }
 
 // ---------------------------------------------------------------------------- tile-local product
@@ -830,11 +831,12 @@ StepFn step_variant(bool staged, StepVariant v)
 {
     constexpr int kWide = sizeof(VT) == 4 ? 4 : 2;   // right-hand sides of a 32-byte load
     constexpr bool kAll = !CPLX && (RP == kWide || TP == 1);
-    if (v.fused) {   // staged, real FP32, the widest loads, unroll 8, whole records
-        if constexpr (sizeof(VT) == 4 && !CPLX && RP == 4 && TP >= 2) {
-            if (!staged || v.unroll != 8 || !v.stage_values) return nullptr;
-            if (v.min_blocks == 2) return k_spmm_staged<VT, CPLX, G, RP, TP, false, 8, true, 2, false, true>;
-            if (v.min_blocks == 1) return k_spmm_staged<VT, CPLX, G, RP, TP, false, 8, true, 1, false, true>;
+    if (v.fused) {   // staged, real values, the widest loads, whole records; FP32 unroll 8, FP64 unroll 4
+        if constexpr (!CPLX && RP == kWide && TP >= 2 && (sizeof(VT) == 4 || G <= 2)) {
+            constexpr int UF = sizeof(VT) == 4 ? 8 : 4;
+            if (!staged || v.unroll != UF || !v.stage_values) return nullptr;
+            if (v.min_blocks == 2) return k_spmm_staged<VT, CPLX, G, RP, TP, false, UF, true, 2, false, true>;
+            if (v.min_blocks == 1) return k_spmm_staged<VT, CPLX, G, RP, TP, false, UF, true, 1, false, true>;
         }
         return nullptr;
     }

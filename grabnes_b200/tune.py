@@ -82,11 +82,12 @@ def autotune(ctx, u, precision, nsteps=12, rhs_per_thread=(1, 2, 4), blocks_per_
                 continue
             seen.add(cand)
             results.append(_time(ctx, u, precision, nsteps, cand))
-        # the fused step: staged whole records, unroll 8, registers for one or two blocks per SM (the library
-        # refuses shapes without it)
+        # the fused step: staged whole records, registers for one or two blocks per SM (the library refuses
+        # shapes without it)
         if lay["staged"] == 1 and grp <= 2:
+            uf = 4 if precision == 0 else 8   # the fused step's columns in flight: FP64 4, mixed 8
             for pf, mb in itertools.product(pfs, (1, 2)):
-                cand = (grp, 1, pf, lay["rhs_per_thread"], lay["blocks_per_sm"], 8, 1, mb, 1)
+                cand = (grp, 1, pf, lay["rhs_per_thread"], lay["blocks_per_sm"], uf, 1, mb, 1)
                 if cand in seen:
                     continue
                 seen.add(cand)

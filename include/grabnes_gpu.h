@@ -161,11 +161,12 @@ int         gbn_set_tuning(gbn_ctx* ctx, int32_t rhs_per_thread, int32_t blocks_
  * Peierls rotations are tabulated once before its steps (1) or done on the fly by every thread at every
  * step (0, -1 = the default); and the tile-local product (1: mixed precision, real hoppings; each tile of
  * slices copies the rows it gathers into shared memory first; 0, -1 = the default: no); and the fused step
- * (1: mixed precision, real hoppings, staged records, 4 right-hand sides per thread, unroll 8; the update
+ * (1: real hoppings or batched fields, staged records, the widest loads per thread, unroll 8 in mixed
+ * precision and 4 in FP64; the update
  * folded into the product: every gathered column forms u_k = v_k - alpha u_{k-1} from two stored vectors,
  * and b_k comes from three sums of the previous product, so a step is one launch; 0: two launches; -1 =
- * the default: fused in mixed precision where the rows hold at most 8 entries on average and the shape has
- * a fused kernel, two launches otherwise).
+ * the default: fused where the rows hold at most 8 entries on average and the shape has a fused kernel,
+ * two launches otherwise).
  * No counterpart in the reference.  Used by the autotuner (grabnes_b200/tune.py). */
 int         gbn_set_kernel_variant(gbn_ctx* ctx, int32_t col_unroll, int32_t stage_values, int32_t min_blocks,
                                    int32_t field_table, int32_t tiled, int32_t fused);

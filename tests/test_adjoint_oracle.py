@@ -1,6 +1,6 @@
 """The DOS-loss gradient of the library (gbn_dos_gradient, FP64, and its FP32-vector variant) against an
 independent FP64 reference gradient: central differences (h = 1e-6 relative; Richardson-extrapolated
-steps of 5e-4 and 1e-3 for the much smaller w derivative) of the loss computed
+steps of 2e-3 and 4e-3 for the much smaller w derivative) of the loss computed
 entirely by the oracle -- its own geometry, neighbour tables and hoppings with the smooth interlayer
 cutoff (orc_hopping), the reference's three-pass recursion (KuboRecursion, kubosubs.F90:26-138) and
 continued fraction (KuboFrac, kubosubs.F90:222-288).  Nothing of the library's assembly, recursion or
@@ -71,9 +71,11 @@ class OracleProblem:
         return m
 
     def loss(self, theta):
+        """The oracle's loss with a fixed number of OpenMP threads (8), so that its summation order, and with
+        it the last bits the central differences of w resolve, does not depend on the machine."""
         r = self.r
         return orc.dos_loss(self.model(theta), r["rat_hop"], r["geo"]["species"], r["geo"]["layer"], r["nb"], r["h0"],
-                            self.u, self.nrecurs, self.eta, self.n_en, self.emin, self.emax, self.target)
+                            self.u, self.nrecurs, self.eta, self.n_en, self.emin, self.emax, self.target, nthreads=8)
 
     def _cd(self, theta, k, h):
         tp, tm = theta.copy(), theta.copy()
@@ -81,12 +83,14 @@ class OracleProblem:
         tm[k] -= h
         return (self.loss(tp)[0] - self.loss(tm)[0]) / (2.0 * h)
 
-    def central_differences(self, theta, rel=1e-6, rel_w=5e-4):
+    def central_differences(self, theta, rel=1e-6, rel_w=2e-3):
         """Central differences with h = 1e-6 theta_k for t, Vpp_sigma0 and delta.  The w derivative is
         three to four orders of magnitude below the others, under the rounding noise that h = 1e-6 meets
         after hundreds of recursion steps (about 5e-6 absolute at 600 steps, the agreement of the large
-        components); it is differenced with h = 5e-4 w and 1e-3 w and extrapolated (Richardson), which
-        leaves a truncation error of order (h / w)^4 and the noise divided by 500."""
+        components); it is differenced with h = 2e-3 w and 4e-3 w and extrapolated (Richardson), which
+        leaves a truncation error of order (h / w)^4 and the noise divided by 2000.  At 5e-4 the noise
+        still moved the 107k-atom w difference by 1.4e-5 relative between 8 and 16 threads; at 2e-3 by
+        1.2e-6."""
         fd = np.zeros(4)
         for k in range(3):
             fd[k] = self._cd(theta, k, rel * theta[k])

@@ -299,6 +299,34 @@ def test_kernel_variants_agree(ctx, grp, prec):
         assert _rel(runs[0][0][0], a0) <= 1e-10 and _rel(runs[0][1][0], b0) <= 1e-10
 
 
+def test_fused_step_fp64(ctx):
+    """The fused step with FP64 vectors (u_k formed by FP64 FMAs, alpha unrounded): a_n, b_n against the
+    oracle within 1e-10 relative over 200 steps, as every FP64 path, and against the FP64 two-launch step;
+    layouts of one and two rows per group, 8 and 16 vectors."""
+    for name in ("moire_twist", "tbg", "graphene"):
+        r = built(name)
+        n = r["geo"]["n"]
+        ctx.load_hamiltonian(r["nb"]["nneigh"], r["nb"]["nlist"], r["hop"], r["h0"])
+        psi0 = None
+        for nv, grp in ((16, 1), (8, 2)):
+            u = np.stack([orc.rng_draws(51 + k, n) for k in range(nv)])
+            try:
+                ctx.set_tuning(2, 0, grp, 1, 4)
+                ctx.set_kernel_variant(4, 1, 0, -1, -1, 0)
+                a2, b2 = ctx.lanczos_phases(u, 200, G.GBN_FP64)
+                ctx.set_kernel_variant(4, 1, 2, -1, -1, 1)
+                a1, b1 = ctx.lanczos_phases(u, 200, G.GBN_FP64)
+            finally:
+                ctx.set_tuning()
+                ctx.set_kernel_variant()
+            assert _rel(a1, a2) <= 1e-10 and _rel(b1, b2) <= 1e-10, (name, nv, grp)
+            psi = np.exp(2j * np.pi * u[0]) / np.sqrt(n)
+            if psi0 is None or not np.array_equal(psi, psi0):
+                a0, b0 = orc.recursion(r["nb"], r["hop"], r["h0"], psi, 200, 0)
+                psi0 = psi
+            assert _rel(a1[0], a0) <= 1e-10 and _rel(b1[0], b0) <= 1e-10, (name, nv, grp)
+
+
 @pytest.mark.parametrize("name", ["tbg", "moire_twist", "graphene"])
 @pytest.mark.parametrize("grp,mb", [(1, 2), (2, 2), (2, 1), (4, 1)])
 def test_fused_step(ctx, name, grp, mb):
