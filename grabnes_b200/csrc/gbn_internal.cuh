@@ -204,7 +204,7 @@ int build_identity_perm(gbn_ctx* c);
 int build_spatial_perm(gbn_ctx* c);
 // field: the field-batched values (FieldVal: field-free hopping and c->ptau), for gbn_lanczos_fields
 int build_ell(gbn_ctx* c, int prec, int G, int gpw, bool field = false);
-int auto_group(const gbn_ctx* c, int R);   // default rows per group for a tile of R vectors
+int auto_group(const gbn_ctx* c, int R, int prec);   // default rows per group for a tile of R vectors
 // the tile table of the field-batched layout for the flux quanta of each thread slot (d_slot_m [slots])
 int build_field_table(gbn_ctx* c, int slots, const int32_t* d_slot_m);
 // tiles of the layout whose halos have at most hmax rows (host pass over the records)

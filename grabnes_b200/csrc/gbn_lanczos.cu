@@ -321,7 +321,9 @@ static int step_launch(gbn_ctx* c, int R, StepLaunch* L)
     // vectors, and on 80k/1.1M-atom cells with one vector): 8 columns in flight in mixed precision, 4 in
     // FP64; with 8 columns and one row per group, registers bounded for 3 blocks per SM
     StepVariant v;
-    v.unroll = c->tune_unroll > 0 ? c->tune_unroll : (c->prec == GBN_MIXED ? 8 : 4);
+    // FP64: 4 columns in flight, 8 for one vector on a low-degree cell (with auto_group's one row per group)
+    const bool fp64_single_low = c->prec == GBN_FP64 && R == 1 && c->n > 0 && c->total < 8 * c->n;
+    v.unroll = c->tune_unroll > 0 ? c->tune_unroll : (c->prec == GBN_MIXED || fp64_single_low ? 8 : 4);
     v.stage_values = c->tune_stage_values != 0;
     v.min_blocks = c->tune_min_blocks > 0 ? c->tune_min_blocks : (v.unroll == 8 && E.G == 1 && !E.cplx ? 3 : 1);
     // the update folded into the product (see k_spmm_staged), its registers bounded for two blocks per SM
@@ -440,7 +442,7 @@ int lanczos_prepare(gbn_ctx* c, int prec, int nrhs, bool field)
     int rpt, tpr;
     split_rhs(prec, nrhs, c->tune_rpt, &rpt, &tpr);
     const int gpw = 32 / tpr;
-    const int G = c->tune_group > 0 ? c->tune_group : auto_group(c, nrhs);
+    const int G = c->tune_group > 0 ? c->tune_group : auto_group(c, nrhs, prec);
     if (!c->ell.valid || c->ell.prec != prec || c->ell.gpw != gpw || c->ell.G != G || c->ell.field != field) {
         const int rc = build_ell(c, prec, G, gpw, field);
         if (rc) return rc;
