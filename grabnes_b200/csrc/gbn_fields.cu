@@ -53,28 +53,57 @@ StepFn field_table_kernel(int prec, int G, int rpt, int tpr, bool staged)
     return nullptr;
 }
 
-// the fused field product: registers for one block per SM, or bounded for two (min_blocks 2)
-template <int G, int MINB>
+// the fused field product at the widest loads (mixed precision 4 right-hand sides per thread, FP64 2):
+// registers for one block per SM, or bounded for two (min_blocks 2)
+template <typename VT, int G, int MINB>
 static StepFn pick_field_fused_g(int tpr)
 {
-    if (tpr == 2) return k_spmm_staged<float, false, G, 4, 2, true, kColUnroll, true, MINB, false, true>;
-    if (tpr == 4) return k_spmm_staged<float, false, G, 4, 4, true, kColUnroll, true, MINB, false, true>;
-    if (tpr == 8) return k_spmm_staged<float, false, G, 4, 8, true, kColUnroll, true, MINB, false, true>;
+    constexpr int RP = sizeof(VT) == 4 ? 4 : 2;
+    if (tpr == 2) return k_spmm_staged<VT, false, G, RP, 2, true, kColUnroll, true, MINB, false, true>;
+    if (tpr == 4) return k_spmm_staged<VT, false, G, RP, 4, true, kColUnroll, true, MINB, false, true>;
+    if (tpr == 8) return k_spmm_staged<VT, false, G, RP, 8, true, kColUnroll, true, MINB, false, true>;
+    if constexpr (sizeof(VT) == 8) {
+        if (tpr == 16) return k_spmm_staged<VT, false, G, RP, 16, true, kColUnroll, true, MINB, false, true>;
+    }
+    return nullptr;
+}
+
+// one right-hand side per thread: a sweep of one vector per field (the drop-in driver's DOS sweeps)
+template <typename VT, int G, int MINB>
+static StepFn pick_field_fused_single(int tpr)
+{
+    if (tpr == 8) return k_spmm_staged<VT, false, G, 1, 8, true, kColUnroll, true, MINB, false, true>;
+    if (tpr == 16) return k_spmm_staged<VT, false, G, 1, 16, true, kColUnroll, true, MINB, false, true>;
+    if (tpr == 32) return k_spmm_staged<VT, false, G, 1, 32, true, kColUnroll, true, MINB, false, true>;
+    return nullptr;
+}
+
+template <typename VT>
+static StepFn pick_field_fused(int G, int rpt, int tpr, int min_blocks)
+{
+    if (rpt == 1) {
+        if (G == 1) return min_blocks == 2 ? pick_field_fused_single<VT, 1, 2>(tpr) : pick_field_fused_single<VT, 1, 1>(tpr);
+        if (G == 2) return min_blocks == 2 ? pick_field_fused_single<VT, 2, 2>(tpr) : pick_field_fused_single<VT, 2, 1>(tpr);
+        return nullptr;
+    }
+    if (rpt != (sizeof(VT) == 4 ? 4 : 2)) return nullptr;
+    if (min_blocks == 2) {
+        if (G == 1) return pick_field_fused_g<VT, 1, 2>(tpr);
+        if (G == 2) return pick_field_fused_g<VT, 2, 2>(tpr);
+        return nullptr;
+    }
+    if (G == 1) return pick_field_fused_g<VT, 1, 1>(tpr);
+    if (G == 2) return pick_field_fused_g<VT, 2, 1>(tpr);
+    if constexpr (sizeof(VT) == 4) {
+        if (G == 4) return pick_field_fused_g<VT, 4, 1>(tpr);
+    }
     return nullptr;
 }
 
 StepFn field_fused_kernel(int prec, int G, int rpt, int tpr, int min_blocks)
 {
-    if (prec != GBN_MIXED || rpt != 4) return nullptr;
-    if (min_blocks == 2) {
-        if (G == 1) return pick_field_fused_g<1, 2>(tpr);
-        if (G == 2) return pick_field_fused_g<2, 2>(tpr);
-        return nullptr;
-    }
-    if (G == 1) return pick_field_fused_g<1, 1>(tpr);
-    if (G == 2) return pick_field_fused_g<2, 1>(tpr);
-    if (G == 4) return pick_field_fused_g<4, 1>(tpr);
-    return nullptr;
+    if (prec == GBN_MIXED) return pick_field_fused<float>(G, rpt, tpr, min_blocks);
+    return pick_field_fused<double>(G, rpt, tpr, min_blocks);
 }
 
 StepFn field_step_kernel(int prec, int G, int rpt, int tpr, bool staged)

@@ -51,8 +51,8 @@ using StepFn = void (*)(StepParams);
 // the sparse-product kernel of the field-batched layout (gbn_fields.cu): rotations on the fly, or the
 // tile table (complex values per thread slot)
 StepFn field_step_kernel(int prec, int G, int rpt, int tpr, bool staged);
-// the field-batched product with the update folded in (mixed precision, staged, 4 right-hand sides per
-// thread), nullptr for other shapes
+// the field-batched product with the update folded in (staged, the widest loads per thread), nullptr for
+// other shapes
 StepFn field_fused_kernel(int prec, int G, int rpt, int tpr, int min_blocks);
 StepFn field_table_kernel(int prec, int G, int rpt, int tpr, bool staged);
 

@@ -161,6 +161,53 @@ def test_fields_fused_step(ctx, base, mb):
         assert err <= 1e-6, (m, err)
 
 
+def test_fields_fused_step_fp64(ctx, base):
+    """The fused step on the field-batched layout in FP64: every field's a_n, b_n within 1e-10 of the
+    spectral scale of the oracle's recursion on that field's Hamiltonian, as the two-launch FP64 path."""
+    n = base["geo"]["n"]
+    u = _draws(n)
+    ns = np.full((len(FIELDS), NVEC), 90, np.int32)
+    _field_free(ctx, base)
+    try:
+        ctx.set_kernel_variant(0, -1, 2, 0, -1, 1)
+        a, b = ctx.lanczos_fields(FIELDS, u, ns, G.GBN_FP64)
+    finally:
+        ctx.set_kernel_variant()
+    for f, m in enumerate(FIELDS):
+        r = R.build(dict(MOIRE, MagFieldInteger=m)) if m else base
+        for v in range(NVEC):
+            psi = np.exp(2j * np.pi * u[f, v]) / np.sqrt(n)
+            a0, b0 = orc.recursion(r["nb"], r["hop"], r["h0"], psi, 90, 0)
+            assert _close(a[f, v], b[f, v], a0, b0, 1e-10), (m, v)
+
+
+@pytest.mark.parametrize("prec", [G.GBN_FP64, G.GBN_MIXED])
+def test_fields_fused_one_vector_per_field(ctx, base, prec):
+    """One vector per field (the drop-in driver's DOS-only sweeps: one right-hand side per thread) with the
+    fused step: FP64 within 1e-10 of the spectral scale of the oracle on each field's Hamiltonian; mixed
+    precision, the DOS of each field within 1e-6 of the oracle's."""
+    n, g0 = base["geo"]["n"], base["g0"]
+    fields = FIELDS * 3   # 15 fields: a tile of 16
+    u = np.stack([orc.rng_draws(2000 + f, n) for f in range(len(fields))])[:, None, :]
+    _field_free(ctx, base)
+    try:
+        ctx.set_kernel_variant(0, -1, 2, 0, -1, 1)
+        a, b = ctx.lanczos_fields(fields, u, 90, prec)
+    finally:
+        ctx.set_kernel_variant()
+    eta, ne, lo, hi = 0.02 / g0, 600, -0.6 / g0, 0.6 / g0
+    for f, m in enumerate(fields):
+        r = R.build(dict(MOIRE, MagFieldInteger=m)) if m else base
+        psi = np.exp(2j * np.pi * u[f, 0]) / np.sqrt(n)
+        a0, b0 = orc.recursion(r["nb"], r["hop"], r["h0"], psi, 90, 0)
+        if prec == G.GBN_FP64:
+            assert _close(a[f, 0], b[f, 0], a0, b0, 1e-10), m
+        else:
+            d0 = orc.frac(a0, b0, eta, ne, lo, hi)[1]
+            d1 = orc.frac(a[f, 0], b[f, 0], eta, ne, lo, hi)[1]
+            assert np.abs(d1 - d0).sum() <= 1e-6 * np.abs(d0).sum(), m
+
+
 def test_fields_reject_a_field_already_applied(ctx, base):
     _field_free(ctx, base)
     ctx.peierls(R.build(dict(MOIRE, MagFieldInteger=2))["flux"])
