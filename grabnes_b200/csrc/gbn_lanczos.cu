@@ -330,8 +330,11 @@ static int step_launch(gbn_ctx* c, int R, StepLaunch* L)
     // unless another bound is asked for.  By default where rows hold at most 8 entries on average: one launch
     // per step there was 3-24 % faster in mixed precision and 10-95 % faster in FP64 on graphene and
     // graphene/hBN cells of 15k-3.5M atoms with 8-32 vectors, and the doubled gathers made it slower on the
-    // twisted bilayer's 33 entries per row (mixed: 504 against 387 us per step, 1.1M atoms, 16 vectors)
-    const bool fused_default = c->tune_fused < 0 && c->n > 0 && c->total <= 8 * c->n;
+    // twisted bilayer's 33 entries per row (mixed: 504 against 387 us per step, 1.1M atoms, 16 vectors).
+    // One mixed vector: equal or faster (387k-atom graphene/hBN 18.5 against 23.4 us); one FP64 vector stays
+    // on two launches (3.5M-atom graphene/hBN 121 against 110 us, 1.28M-atom graphene 53 against 50)
+    const bool fp64_single = c->prec == GBN_FP64 && R == 1;
+    const bool fused_default = c->tune_fused < 0 && c->n > 0 && c->total <= 8 * c->n && !fp64_single;
     const StepVariant v_two = v;
     v.fused = c->tune_fused == 1 || fused_default;
     if (v.fused && c->tune_min_blocks <= 0) v.min_blocks = 2;

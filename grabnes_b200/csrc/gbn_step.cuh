@@ -831,9 +831,9 @@ StepFn step_variant(bool staged, StepVariant v)
 {
     constexpr int kWide = sizeof(VT) == 4 ? 4 : 2;   // right-hand sides of a 32-byte load
     constexpr bool kAll = !CPLX && (RP == kWide || TP == 1);
-    if (v.fused) {   // staged, real values, the widest loads, whole records; FP32 unroll 8, FP64 unroll 4
-        if constexpr (!CPLX && RP == kWide && TP >= 2 && (sizeof(VT) == 4 || G <= 2)) {
-            constexpr int UF = sizeof(VT) == 4 ? 8 : 4;
+    if (v.fused) {   // staged, real values, the widest loads (or one vector), whole records; FP32 unroll 8, FP64 4
+        if constexpr (!CPLX && ((RP == kWide && TP >= 2) || (RP == 1 && TP == 1)) && (sizeof(VT) == 4 || G <= 2)) {
+            constexpr int UF = (sizeof(VT) == 4 || RP == 1) ? 8 : 4;   // one FP64 vector: 8 columns too
             if (!staged || v.unroll != UF || !v.stage_values) return nullptr;
             if (v.min_blocks == 2) return k_spmm_staged<VT, CPLX, G, RP, TP, false, UF, true, 2, false, true>;
             if (v.min_blocks == 1) return k_spmm_staged<VT, CPLX, G, RP, TP, false, UF, true, 1, false, true>;

@@ -299,6 +299,37 @@ def test_kernel_variants_agree(ctx, grp, prec):
         assert _rel(runs[0][0][0], a0) <= 1e-10 and _rel(runs[0][1][0], b0) <= 1e-10
 
 
+@pytest.mark.parametrize("name", ["graphene", "moire_twist", "anderson"])
+def test_fused_step_single_vector(ctx, name):
+    """The fused step with one vector (one right-hand side per thread): FP64 a_n, b_n within 1e-10 of the
+    oracle over 200 steps; mixed precision (the default there on low-degree cells): its DOS within three
+    times the two-launch mixed path's deviation from the oracle's DOS (these cells are small, and 200
+    mixed steps part from FP64 whatever the step form)."""
+    r = built(name)
+    n, g0 = r["geo"]["n"], r["g0"]
+    ctx.load_hamiltonian(r["nb"]["nneigh"], r["nb"]["nlist"], r["hop"], r["h0"])
+    u = orc.rng_draws(61, n)[None, :]
+    psi = np.exp(2j * np.pi * u[0]) / np.sqrt(n)
+    a0, b0 = orc.recursion(r["nb"], r["hop"], r["h0"], psi, 200, 0)
+    try:
+        ctx.set_kernel_variant(8, 1, 2, -1, -1, 1)
+        a1, b1 = ctx.lanczos_phases(u, 200, G.GBN_FP64)
+        a2, b2 = ctx.lanczos_phases(u, 200, G.GBN_MIXED)
+        ctx.set_kernel_variant(8, 1, 0, -1, -1, 0)
+        a3, b3 = ctx.lanczos_phases(u, 200, G.GBN_MIXED)
+    finally:
+        ctx.set_kernel_variant()
+    assert _rel(a1[0], a0) <= 1e-10 and _rel(b1[0], b0) <= 1e-10
+    args = (0.01 / g0, 800, -1.0 / g0, 1.0 / g0)
+    _, d0 = orc.frac(a0, b0, *args)
+    _, d2 = ctx.cf_dos(a2, b2, *args)
+    _, d3 = ctx.cf_dos(a3, b3, *args)
+    e2 = np.abs(d2[0] - d0).sum() / np.abs(d0).sum()
+    e3 = np.abs(d3[0] - d0).sum() / np.abs(d0).sum()
+    print(name, "mixed DOS deviation: fused", e2, "two launches", e3)
+    assert e2 <= 3.0 * e3 + 1e-7
+
+
 def test_fused_step_fp64(ctx):
     """The fused step with FP64 vectors (u_k formed by FP64 FMAs, alpha unrounded): a_n, b_n against the
     oracle within 1e-10 relative over 200 steps, as every FP64 path, and against the FP64 two-launch step;
