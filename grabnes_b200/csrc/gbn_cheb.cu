@@ -62,8 +62,8 @@ __global__ void __launch_bounds__(256) k_cheb_step(ChebParams p)
         const int w = (int)((p.slice_ptr[s + 1] - base) / GPW);
         const unsigned char* rec = p.mat + base * p.entry_bytes;
         C2 acc[G][RPT];
-        group_columns<VT, CPLX, G, RPT, TPR, false>(xn, w, reinterpret_cast<const int32_t*>(rec) + sub,
-                                                    reinterpret_cast<const HT*>(rec + (size_t)w * GPW * 4) + sub * G,
+        group_columns<VT, CPLX, G, RPT, TPR, false>(xn, w, reinterpret_cast<const int32_t*>(rec) + sub * kColUnroll,
+                                                    reinterpret_cast<const HT*>(rec + (size_t)w * GPW * 4) + sub * kColUnroll * G,
                                                     acc);
         const int64_t row0 = (s * GPW + sub) * G;
 #pragma unroll
@@ -329,9 +329,9 @@ __global__ void k_fill_dvals(const int32_t* nneigh, const int32_t* nlist, const 
             const int64_t ent = p * max_neigh + e;
             const int32_t target = riperm[nlist[ent] - 1];
             int k = 0;
-            while (k < w && col[k * gpw + j] != target) ++k;
+            while (k < w && col[rec_slot(k, j, gpw)] != target) ++k;
             if (k == w) continue;   // cannot happen: every entry's column is in its group's union
-            acc_into(dval[((base + (int64_t)k * gpw + j) * G) + rr], scaled_neg_hop<HV>(hopp[ent], neighd[3 * ent + comp]));
+            acc_into(dval[((base + rec_slot(k, j, gpw)) * G) + rr], scaled_neg_hop<HV>(hopp[ent], neighd[3 * ent + comp]));
         }
     }
 }
@@ -379,9 +379,9 @@ __global__ void __launch_bounds__(256) k_dual_step(DualParams p)
         const int64_t base = p.slice_ptr[s];
         const int w = (int)((p.slice_ptr[s + 1] - base) / GPW);
         const unsigned char* rec = p.mat + base * p.entry_bytes;
-        const int32_t* __restrict__ cp = reinterpret_cast<const int32_t*>(rec) + sub;
-        const HT* __restrict__ vp = reinterpret_cast<const HT*>(rec + (size_t)w * GPW * 4) + sub * G;
-        const HT* __restrict__ dp = dv + (base + sub) * G;
+        const int32_t* __restrict__ cp = reinterpret_cast<const int32_t*>(rec) + sub * U;
+        const HT* __restrict__ vp = reinterpret_cast<const HT*>(rec + (size_t)w * GPW * 4) + sub * U * G;
+        const HT* __restrict__ dp = dv + (base + sub * U) * G;
         C2 ap[G][RPT], ax[G][RPT];
 #pragma unroll
         for (int g = 0; g < G; ++g)
@@ -390,13 +390,18 @@ __global__ void __launch_bounds__(256) k_dual_step(DualParams p)
                 ap[g][t].x = 0; ap[g][t].y = 0;
                 ax[g][t].x = 0; ax[g][t].y = 0;
             }
+        static_assert(U == 4, "one 16-byte load of a block's indices");
         for (int k = 0; k < w; k += U) {
+            const int4 cb = __ldcs(reinterpret_cast<const int4*>(cp));   // the group's U columns of this block
+            const int32_t cc[U] = {cb.x, cb.y, cb.z, cb.w};
+            HT hb[U * G], hdb[U * G];
+            load_group_vals<HT, U * G, false>(vp, hb);
+            load_group_vals<HT, U * G, false>(dp, hdb);
 #pragma unroll
             for (int u = 0; u < U; ++u) {
-                const int32_t c = __ldcs(cp + u * GPW);
-                HT h[G], hd[G];
-                load_group_vals<HT, G, false>(vp + u * GPW * G, h);
-                load_group_vals<HT, G, false>(dp + u * GPW * G, hd);
+                const int32_t c = cc[u];
+                const HT* h = hb + u * G;
+                const HT* hd = hdb + u * G;
                 C2 gp[RPT], gx[RPT];
                 VecIO<VT, RPT>::load(pn + (size_t)(uint32_t)c * R + q * RPT, gp);
                 VecIO<VT, RPT>::load(xn + (size_t)(uint32_t)c * R + q * RPT, gx);

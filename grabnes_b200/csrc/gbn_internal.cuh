@@ -88,6 +88,15 @@ struct Ell {
 // unroll of the union-column loop (slice widths are multiples of it)
 constexpr int kColUnroll = 4;
 
+// Entry position of union column k of group j in a slice record of gpw groups.  The record holds its
+// columns in blocks of kColUnroll; inside a block each group's kColUnroll indices are contiguous (16
+// bytes), and so are its values, so a thread reads a block's indices with one 16-byte load and a warp's
+// groups read one block from consecutive 16-byte pieces.
+__host__ __device__ __forceinline__ int64_t rec_slot(int k, int j, int gpw)
+{
+    return (int64_t)(k / kColUnroll) * kColUnroll * gpw + (int64_t)j * kColUnroll + k % kColUnroll;
+}
+
 struct Timing {
     double step_ms = 0.0;        // whole recursion loop of the last call
     int64_t step_launches = 0;   // recursion steps of the last call

@@ -257,8 +257,8 @@ __global__ void k_fill_groups(const int32_t* nneigh, const int32_t* nlist, const
         u = ucount[og];
         ul = ukeys + ustart[og];
     }
-    for (int k = 0; k < u; ++k) col[k * gpw + j] = riperm[(uint32_t)ul[k]];
-    for (int k = u; k < w; ++k) col[k * gpw + j] = (int32_t)row0;
+    for (int k = 0; k < u; ++k) col[rec_slot(k, j, gpw)] = riperm[(uint32_t)ul[k]];
+    for (int k = u; k < w; ++k) col[rec_slot(k, j, gpw)] = (int32_t)row0;
     for (int rr = 0; rr < G; ++rr) {
         const int64_t row = row0 + rr;
         if (row >= n) {
@@ -276,8 +276,8 @@ __global__ void k_fill_groups(const int32_t* nneigh, const int32_t* nlist, const
                 if ((uint32_t)ul[mid] < rc) lo = mid + 1;
                 else hi = mid;
             }
-            if constexpr (FIELD) val[(lo * gpw + j) * G + rr] = field_val<HV>(hopp[p * max_neigh + e], tau[p * max_neigh + e]);
-            else add_to(val[(lo * gpw + j) * G + rr], neg_hop<HV>(hopp[p * max_neigh + e]));
+            if constexpr (FIELD) val[rec_slot(lo, j, gpw) * G + rr] = field_val<HV>(hopp[p * max_neigh + e], tau[p * max_neigh + e]);
+            else add_to(val[rec_slot(lo, j, gpw) * G + rr], neg_hop<HV>(hopp[p * max_neigh + e]));
         }
     }
 }

@@ -142,10 +142,67 @@ __device__ __forceinline__ void load_group_vals(const HT* p, HT (&h)[G])
     }
 }
 
+// The column indices of NB union columns (whole blocks of kColUnroll, rec_slot's order) of the group whose
+// first index of the current block cp points at, from shared memory (SMEM) or streamed from global memory:
+// per block one 16-byte load (IB = 16), or one 4-byte load per column (IB = 4; a warp's groups still read
+// distinct banks), which holds no aligned register quad: the fused step at two or more rows per group keeps
+// its 128 registers without spilling only with these.
+template <int GPW, int NB, bool SMEM, int IB = 16>
+__device__ __forceinline__ void load_block_cols(const int32_t* cp, int32_t (&c)[NB])
+{
+    static_assert(kColUnroll == 4 && NB % kColUnroll == 0, "whole blocks of four columns");
+    static_assert(IB == 16 || IB == 4, "16-byte block loads or 4-byte column loads");
+#pragma unroll
+    for (int b = 0; b < NB / kColUnroll; ++b) {
+        if constexpr (IB == 16) {
+            const int4* p = reinterpret_cast<const int4*>(cp + b * kColUnroll * GPW);
+            int4 t;
+            if constexpr (SMEM) t = *p;
+            else t = __ldcs(p);
+            c[4 * b] = t.x;
+            c[4 * b + 1] = t.y;
+            c[4 * b + 2] = t.z;
+            c[4 * b + 3] = t.w;
+        } else {
+#pragma unroll
+            for (int i = 0; i < kColUnroll; ++i) {
+                if constexpr (SMEM) c[4 * b + i] = cp[b * kColUnroll * GPW + i];
+                else c[4 * b + i] = __ldcs(cp + b * kColUnroll * GPW + i);
+            }
+        }
+    }
+}
+
+// The G values of each of NB union columns in rec_slot's order.  A block's values of the group are
+// contiguous; where they make 16 bytes (one FP32 value per column) they are read with one load, which a
+// warp's groups serve from distinct banks.  Wider blocks (G > 1, FP64, field values, or VS > 1: the field
+// tile table's VS value blocks per entry) are read with one load of G values per column, which holds
+// fewer registers at once and meets no more bank conflicts.
+template <typename HT, int G, int GPW, int NB, bool SMEM, int VS>
+__device__ __forceinline__ void load_block_vals(const HT* vp, HT (&h)[NB][G])
+{
+#pragma unroll
+    for (int b = 0; b < NB / kColUnroll; ++b) {
+        if constexpr (VS == 1 && kColUnroll * G * sizeof(HT) == 16) {
+            HT hb[kColUnroll * G];
+            load_group_vals<HT, kColUnroll * G, SMEM>(vp + b * kColUnroll * GPW * G, hb);
+#pragma unroll
+            for (int i = 0; i < kColUnroll; ++i)
+#pragma unroll
+                for (int g = 0; g < G; ++g) h[kColUnroll * b + i][g] = hb[i * G + g];
+        } else {
+#pragma unroll
+            for (int i = 0; i < kColUnroll; ++i)
+                load_group_vals<HT, G, SMEM>(vp + (b * kColUnroll * GPW + i) * G * VS, h[kColUnroll * b + i]);
+        }
+    }
+}
+
 // The union-column loop of one group: GPW = 32/TPR groups per slice; the TPR threads of a group each
 // hold RPT right-hand sides of all G rows of the group.  Per union column a thread reads the column
 // index and the G values (same address for the group's threads) and gathers RPT vector elements of that
-// column once for all G rows.  cp/vp point at the thread's group in the slice record; the indices come
+// column once for all G rows.  cp/vp point at the thread's group in the slice record (its first
+// column of the current block, rec_slot's order); the indices come
 // from shared memory (SMEM) or global memory (streamed, evict-first), the values likewise (SMEM_VAL).
 // w is the slice width (a multiple of kColUnroll).  U columns are in flight per batch: their indices,
 // gathers and values are all issued before the first product, so U gathers wait on memory together.
@@ -184,11 +241,7 @@ __device__ __forceinline__ void column_batch(const typename V2<VT>::t* __restric
     int32_t c[NB];
     HT h[NB][G];
     C2 xg[NB][RPT];
-#pragma unroll
-    for (int u = 0; u < NB; ++u) {
-        if constexpr (SMEM) c[u] = cp[u * GPW];
-        else c[u] = __ldcs(cp + u * GPW);
-    }
+    load_block_cols<GPW, NB, SMEM, (FUSED && G > 1) ? 4 : 16>(cp, c);
 #pragma unroll
     for (int u = 0; u < NB; ++u) VecIO<VT, RPT>::load(xq + (size_t)(uint32_t)c[u] * R, xg[u]);
     if constexpr (FUSED) {
@@ -201,8 +254,7 @@ __device__ __forceinline__ void column_batch(const typename V2<VT>::t* __restric
 #pragma unroll
             for (int t = 0; t < RPT; ++t) xg[u][t] = fused_form(al[t], xh[u][t], xg[u][t]);
     }
-#pragma unroll
-    for (int u = 0; u < NB; ++u) load_group_vals<HT, G, SMEM_VAL>(vp + u * GPW * G * VS, h[u]);
+    load_block_vals<HT, G, GPW, NB, SMEM_VAL, VS>(vp, h);
     if constexpr (FIELD) {
 #pragma unroll
         for (int u = 0; u < NB; ++u)

@@ -353,9 +353,9 @@ __global__ void __launch_bounds__(256) k_spmm_step(StepParams p)
         const int w = (int)((p.slice_ptr[s + 1] - base) / GPW);
         const unsigned char* rec = p.mat + base * p.entry_bytes;
         constexpr int VS = SLOT ? TPR : 1;   // tile table: [column][group][slot][G]
-        const int voff = SLOT ? (sub * TPR + q) * G : sub * G;
+        const int voff = SLOT ? (sub * kColUnroll * TPR + q) * G : sub * kColUnroll * G;
         group_slice<VT, CPLX, G, RPT, TPR, false, FIELD, U, false, VS>(
-            p, s, w, reinterpret_cast<const int32_t*>(rec) + sub,
+            p, s, w, reinterpret_cast<const int32_t*>(rec) + sub * kColUnroll,
             reinterpret_cast<const HT*>(rec + (size_t)w * GPW * 4) + voff, sc, acc_s);
     }
     reduce_and_finalize<RPT, TPR>(p, acc_s);
@@ -555,17 +555,17 @@ __global__ void __launch_bounds__(256, MINB) k_spmm_staged(StepParams p)
         if (p.prefetch >= 3) prefetch_epilogue<VT, R, G, GPW>(p, s);
         if (p.prefetch >= 5) prefetch_ahead<VT, R, G, GPW>(p, s + (int64_t)(p.prefetch == 5 ? 1 : p.prefetch == 6 ? 2 : 4) * nwb);
         constexpr int VS = SLOT ? TPR : 1;   // tile table: [column][group][slot][G], the thread's own slot
-        const int voff = SLOT ? (sub * TPR + q) * G : sub * G;
+        const int voff = SLOT ? (sub * kColUnroll * TPR + q) * G : sub * kColUnroll * G;
         if (copy_bytes(s) <= cap) {
             const unsigned char* rec = buf + st * cap;
             if (p.prefetch == 1 || p.prefetch == 2)
                 prefetch_rows<VT, R>(p, reinterpret_cast<const int32_t*>(rec), w * GPW);
             const HT* vp = reinterpret_cast<const HT*>((SV ? rec : grec) + (size_t)w * GPW * 4) + voff;
             group_slice<VT, CPLX, G, RPT, TPR, true, FIELD, U, SV, VS, FUSED, NSC>(
-                p, s, w, reinterpret_cast<const int32_t*>(rec) + sub, vp, sc, acc_s);
+                p, s, w, reinterpret_cast<const int32_t*>(rec) + sub * kColUnroll, vp, sc, acc_s);
         } else {
             group_slice<VT, CPLX, G, RPT, TPR, false, FIELD, U, false, VS, FUSED, NSC>(
-                p, s, w, reinterpret_cast<const int32_t*>(grec) + sub,
+                p, s, w, reinterpret_cast<const int32_t*>(grec) + sub * kColUnroll,
                 reinterpret_cast<const HT*>(grec + (size_t)w * GPW * 4) + voff, sc, acc_s);
         }
         __syncwarp();   // every lane is done with this buffer before it is refilled
@@ -615,15 +615,10 @@ __device__ __forceinline__ void tile_batch(const unsigned char* __restrict__ xs,
     int32_t c[NB];
     VT h[NB][G];
     C2 xg[NB][RPT];
-#pragma unroll
-    for (int u = 0; u < NB; ++u) {
-        if constexpr (SMEM) c[u] = cp[u * GPW];
-        else c[u] = __ldcs(cp + u * GPW);
-    }
+    load_block_cols<GPW, NB, SMEM>(cp, c);
 #pragma unroll
     for (int u = 0; u < NB; ++u) SmemRow<VT, RPT>::load(xs + (size_t)(uint32_t)c[u] * pitch, xg[u]);
-#pragma unroll
-    for (int u = 0; u < NB; ++u) load_group_vals<VT, G, SMEM>(vp + u * GPW * G, h[u]);
+    load_block_vals<VT, G, GPW, NB, SMEM, 1>(vp, h);
 #pragma unroll
     for (int u = 0; u < NB; ++u)
 #pragma unroll
@@ -787,13 +782,15 @@ __global__ void __launch_bounds__(256, MINB) k_spmm_tiled(StepParams p)
             if (p.prefetch >= 3) prefetch_epilogue<VT, R, G, GPW>(p, s);
             if (copy_bytes(s) <= cap) {
                 const unsigned char* rec = buf + st * cap;
-                tile_slice_step<VT, G, RPT, TPR, true, U>(p, s, w, xbuf, reinterpret_cast<const int32_t*>(rec) + sub,
-                                                     reinterpret_cast<const VT*>(rec + (size_t)w * GPW * 4) + sub * G,
+                tile_slice_step<VT, G, RPT, TPR, true, U>(p, s, w, xbuf,
+                                                     reinterpret_cast<const int32_t*>(rec) + sub * kColUnroll,
+                                                     reinterpret_cast<const VT*>(rec + (size_t)w * GPW * 4) + sub * kColUnroll * G,
                                                      sc, acc_s);
             } else {
                 const unsigned char* rec = p.mat + base * eb;
-                tile_slice_step<VT, G, RPT, TPR, false, U>(p, s, w, xbuf, reinterpret_cast<const int32_t*>(rec) + sub,
-                                                      reinterpret_cast<const VT*>(rec + (size_t)w * GPW * 4) + sub * G,
+                tile_slice_step<VT, G, RPT, TPR, false, U>(p, s, w, xbuf,
+                                                      reinterpret_cast<const int32_t*>(rec) + sub * kColUnroll,
+                                                      reinterpret_cast<const VT*>(rec + (size_t)w * GPW * 4) + sub * kColUnroll * G,
                                                       sc, acc_s);
             }
             __syncwarp();   // every lane is done with this buffer before it is refilled
