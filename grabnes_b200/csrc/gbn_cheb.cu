@@ -63,7 +63,8 @@ __global__ void __launch_bounds__(256) k_cheb_step(ChebParams p)
         const unsigned char* rec = p.mat + base * p.entry_bytes;
         C2 acc[G][RPT];
         group_columns<VT, CPLX, G, RPT, TPR, false>(xn, w, reinterpret_cast<const int32_t*>(rec) + sub * kColUnroll,
-                                                    reinterpret_cast<const HT*>(rec + (size_t)w * GPW * 4) + sub * kColUnroll * G,
+                                                    reinterpret_cast<const HT*>(rec + (size_t)w * GPW * 4) +
+                                                        val_thread_off<HT, G, TPR, 1>(sub, q),
                                                     acc);
         const int64_t row0 = (s * GPW + sub) * G;
 #pragma unroll
@@ -331,7 +332,7 @@ __global__ void k_fill_dvals(const int32_t* nneigh, const int32_t* nlist, const 
             int k = 0;
             while (k < w && col[rec_slot(k, j, gpw)] != target) ++k;
             if (k == w) continue;   // cannot happen: every entry's column is in its group's union
-            acc_into(dval[((base + rec_slot(k, j, gpw)) * G) + rr], scaled_neg_hop<HV>(hopp[ent], neighd[3 * ent + comp]));
+            acc_into(dval[base * G + val_slot(k, j, gpw, G, (int)sizeof(HV)) + rr], scaled_neg_hop<HV>(hopp[ent], neighd[3 * ent + comp]));
         }
     }
 }
@@ -380,8 +381,8 @@ __global__ void __launch_bounds__(256) k_dual_step(DualParams p)
         const int w = (int)((p.slice_ptr[s + 1] - base) / GPW);
         const unsigned char* rec = p.mat + base * p.entry_bytes;
         const int32_t* __restrict__ cp = reinterpret_cast<const int32_t*>(rec) + sub * U;
-        const HT* __restrict__ vp = reinterpret_cast<const HT*>(rec + (size_t)w * GPW * 4) + sub * U * G;
-        const HT* __restrict__ dp = dv + (base + sub * U) * G;
+        const HT* __restrict__ vp = reinterpret_cast<const HT*>(rec + (size_t)w * GPW * 4) + val_thread_off<HT, G, TPR, 1>(sub, q);
+        const HT* __restrict__ dp = dv + base * G + val_thread_off<HT, G, TPR, 1>(sub, q);
         C2 ap[G][RPT], ax[G][RPT];
 #pragma unroll
         for (int g = 0; g < G; ++g)
@@ -394,14 +395,14 @@ __global__ void __launch_bounds__(256) k_dual_step(DualParams p)
         for (int k = 0; k < w; k += U) {
             const int4 cb = __ldcs(reinterpret_cast<const int4*>(cp));   // the group's U columns of this block
             const int32_t cc[U] = {cb.x, cb.y, cb.z, cb.w};
-            HT hb[U * G], hdb[U * G];
-            load_group_vals<HT, U * G, false>(vp, hb);
-            load_group_vals<HT, U * G, false>(dp, hdb);
+            HT hb[U][G], hdb[U][G];
+            load_block_vals<HT, G, GPW, U, false, 1>(vp, hb);
+            load_block_vals<HT, G, GPW, U, false, 1>(dp, hdb);
 #pragma unroll
             for (int u = 0; u < U; ++u) {
                 const int32_t c = cc[u];
-                const HT* h = hb + u * G;
-                const HT* hd = hdb + u * G;
+                const HT* h = hb[u];
+                const HT* hd = hdb[u];
                 C2 gp[RPT], gx[RPT];
                 VecIO<VT, RPT>::load(pn + (size_t)(uint32_t)c * R + q * RPT, gp);
                 VecIO<VT, RPT>::load(xn + (size_t)(uint32_t)c * R + q * RPT, gx);

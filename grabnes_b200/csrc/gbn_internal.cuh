@@ -42,7 +42,8 @@ struct DevBuf {
 // gathered vector row serves all G rows.  gpw groups form a slice (the groups one warp processes
 // together).  A slice is one contiguous record in `mat`, starting at byte slice_ptr[s] * entry_bytes
 // (entry_bytes = 4 + G * val_size; slice_ptr counts union entries, w * gpw per slice):
-//     int32 col[w][gpw]   then   value val[w][gpw][G]
+//     int32 col[w/4][gpw][4]   then   value val[w/4][gpw][4] (one FP32 value per column) or val[w][gpw][G]
+// (blocks of four union columns; in a block each group's four columns are contiguous: rec_slot, val_slot).
 // Slice widths w are multiples of 4 (records are multiples of 16 bytes and start on 16-byte
 // boundaries); padding columns point at the group's first row with zero values.  Values are stored
 // NEGATED (-hopp = +t/g0), so that (H x)_i = h0_i x_i + sum val * x.  G = 1 is the plain sliced ELL.
@@ -68,8 +69,9 @@ struct Ell {
     int64_t cap_pct[4] = {0, 0, 0, 0};   // record sizes at the 99.5th, 99th, 95th and 90th percentiles
     bool field = false;      // field-batched values: field-free hopping and Peierls phase per flux quantum
     // Field-batched tile table: the records with each value rotated for the fields of the tile's thread
-    // slots (slot q of a row group = its q-th thread's right-hand sides): int32 col[w][gpw] then complex
-    // val[w][gpw][slots][G] (slot q rotated by the field of slot q).  Rebuilt for every tile.
+    // slots (slot q of a row group = its q-th thread's right-hand sides): the record's int32 columns, then
+    // complex val[w][gpw][slots][G] in the order of the record's values (val_slot: field values are
+    // column-major; slot q rotated by the field of slot q).  Rebuilt for every tile.
     DevBuf ftab;
     int ftab_slots = 0;
     int ftab_entry_bytes = 0;   // 4 + slots * G * complex bytes
@@ -90,11 +92,22 @@ constexpr int kColUnroll = 4;
 
 // Entry position of union column k of group j in a slice record of gpw groups.  The record holds its
 // columns in blocks of kColUnroll; inside a block each group's kColUnroll indices are contiguous (16
-// bytes), and so are its values, so a thread reads a block's indices with one 16-byte load and a warp's
-// groups read one block from consecutive 16-byte pieces.
+// bytes), so a thread reads a block's indices with one 16-byte load and a warp's groups read one block
+// from consecutive 16-byte pieces.
 __host__ __device__ __forceinline__ int64_t rec_slot(int k, int j, int gpw)
 {
     return (int64_t)(k / kColUnroll) * kColUnroll * gpw + (int64_t)j * kColUnroll + k % kColUnroll;
+}
+
+// The values follow rec_slot's order only where a group's values of one column take 4 bytes (one FP32
+// value, G = 1: a block's four are one 16-byte load).  Wider values stay column-major, val[w][gpw][G]:
+// read one column at a time, the groups of a warp then touch consecutive bytes and distinct banks,
+// where rec_slot's order would put them 4 columns apart (2- to 8-way bank conflicts).
+__host__ __device__ __forceinline__ constexpr bool block_vals(int G, int val_bytes) { return G * val_bytes == 4; }
+// Position (in values) of the first of the G values of union column k of group j.
+__host__ __device__ __forceinline__ int64_t val_slot(int k, int j, int gpw, int G, int val_bytes)
+{
+    return block_vals(G, val_bytes) ? rec_slot(k, j, gpw) : ((int64_t)k * gpw + j) * G;
 }
 
 struct Timing {

@@ -276,8 +276,8 @@ __global__ void k_fill_groups(const int32_t* nneigh, const int32_t* nlist, const
                 if ((uint32_t)ul[mid] < rc) lo = mid + 1;
                 else hi = mid;
             }
-            if constexpr (FIELD) val[rec_slot(lo, j, gpw) * G + rr] = field_val<HV>(hopp[p * max_neigh + e], tau[p * max_neigh + e]);
-            else add_to(val[rec_slot(lo, j, gpw) * G + rr], neg_hop<HV>(hopp[p * max_neigh + e]));
+            if constexpr (FIELD) val[val_slot(lo, j, gpw, G, (int)sizeof(HV)) + rr] = field_val<HV>(hopp[p * max_neigh + e], tau[p * max_neigh + e]);
+            else add_to(val[val_slot(lo, j, gpw, G, (int)sizeof(HV)) + rr], neg_hop<HV>(hopp[p * max_neigh + e]));
         }
     }
 }

@@ -144,14 +144,16 @@ __device__ __forceinline__ void load_group_vals(const HT* p, HT (&h)[G])
 
 // The column indices of NB union columns (whole blocks of kColUnroll, rec_slot's order) of the group whose
 // first index of the current block cp points at, from shared memory (SMEM) or streamed from global memory:
-// per block one 16-byte load (IB = 16), or one 4-byte load per column (IB = 4; a warp's groups still read
-// distinct banks), which holds no aligned register quad: the fused step at two or more rows per group keeps
-// its 128 registers without spilling only with these.
+// per block one 16-byte load (IB = 16), two 8-byte loads (IB = 8) or one 4-byte load per column (IB = 4).
+// The narrower loads hold register pairs or single registers instead of an aligned quad; the fused step at
+// two or more rows per group keeps its 128 registers without spilling only with them.  A warp's groups
+// read distinct banks with 4-byte loads up to 8 groups, and with 8-byte loads pay 2-way conflicts at 16
+// groups (4 wavefronts per block, as many as 4-byte loads of a column-major record).
 template <int GPW, int NB, bool SMEM, int IB = 16>
 __device__ __forceinline__ void load_block_cols(const int32_t* cp, int32_t (&c)[NB])
 {
     static_assert(kColUnroll == 4 && NB % kColUnroll == 0, "whole blocks of four columns");
-    static_assert(IB == 16 || IB == 4, "16-byte block loads or 4-byte column loads");
+    static_assert(IB == 16 || IB == 8 || IB == 4, "16-, 8- or 4-byte index loads");
 #pragma unroll
     for (int b = 0; b < NB / kColUnroll; ++b) {
         if constexpr (IB == 16) {
@@ -163,6 +165,16 @@ __device__ __forceinline__ void load_block_cols(const int32_t* cp, int32_t (&c)[
             c[4 * b + 1] = t.y;
             c[4 * b + 2] = t.z;
             c[4 * b + 3] = t.w;
+        } else if constexpr (IB == 8) {
+            const int2* p = reinterpret_cast<const int2*>(cp + b * kColUnroll * GPW);
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                int2 t;
+                if constexpr (SMEM) t = p[h];
+                else t = __ldcs(p + h);
+                c[4 * b + 2 * h] = t.x;
+                c[4 * b + 2 * h + 1] = t.y;
+            }
         } else {
 #pragma unroll
             for (int i = 0; i < kColUnroll; ++i) {
@@ -173,27 +185,37 @@ __device__ __forceinline__ void load_block_cols(const int32_t* cp, int32_t (&c)[
     }
 }
 
-// The G values of each of NB union columns in rec_slot's order.  A block's values of the group are
-// contiguous; where they make 16 bytes (one FP32 value per column) they are read with one load, which a
-// warp's groups serve from distinct banks.  Wider blocks (G > 1, FP64, field values, or VS > 1: the field
-// tile table's VS value blocks per entry) are read with one load of G values per column, which holds
-// fewer registers at once and meets no more bank conflicts.
+// index-load width of the union-column loop: 16 bytes, except the fused step at two or more rows per group
+template <bool FUSED, int G, int GPW>
+constexpr int kIndexLoad = !(FUSED && G > 1) ? 16 : GPW <= 8 ? 4 : GPW <= 16 ? 8 : 16;
+
+// Offset of a thread's first value in a slice record's values (VS > 1: the field tile table, one value
+// block per thread slot q of the group).
+template <typename HT, int G, int TPR, int VS>
+__device__ __forceinline__ int val_thread_off(int sub, int q)
+{
+    if constexpr (VS == 1 && block_vals(G, (int)sizeof(HT))) return sub * kColUnroll;
+    else if constexpr (VS > 1) return (sub * TPR + q) * G;
+    else return sub * G;
+}
+
+// The G values of each of NB union columns (whole blocks, val_slot's order) from the thread's pointer
+// into the current block.  One FP32 value per column: a block's four values with one 16-byte load, which
+// a warp's groups serve from distinct banks.  Otherwise one load of G values per column, column-major.
 template <typename HT, int G, int GPW, int NB, bool SMEM, int VS>
 __device__ __forceinline__ void load_block_vals(const HT* vp, HT (&h)[NB][G])
 {
 #pragma unroll
     for (int b = 0; b < NB / kColUnroll; ++b) {
-        if constexpr (VS == 1 && kColUnroll * G * sizeof(HT) == 16) {
-            HT hb[kColUnroll * G];
-            load_group_vals<HT, kColUnroll * G, SMEM>(vp + b * kColUnroll * GPW * G, hb);
+        if constexpr (VS == 1 && block_vals(G, (int)sizeof(HT))) {
+            HT hb[kColUnroll];
+            load_group_vals<HT, kColUnroll, SMEM>(vp + b * kColUnroll * GPW, hb);
 #pragma unroll
-            for (int i = 0; i < kColUnroll; ++i)
-#pragma unroll
-                for (int g = 0; g < G; ++g) h[kColUnroll * b + i][g] = hb[i * G + g];
+            for (int i = 0; i < kColUnroll; ++i) h[kColUnroll * b + i][0] = hb[i];
         } else {
 #pragma unroll
             for (int i = 0; i < kColUnroll; ++i)
-                load_group_vals<HT, G, SMEM>(vp + (b * kColUnroll * GPW + i) * G * VS, h[kColUnroll * b + i]);
+                load_group_vals<HT, G, SMEM>(vp + (b * kColUnroll + i) * GPW * G * VS, h[kColUnroll * b + i]);
         }
     }
 }
@@ -241,7 +263,7 @@ __device__ __forceinline__ void column_batch(const typename V2<VT>::t* __restric
     int32_t c[NB];
     HT h[NB][G];
     C2 xg[NB][RPT];
-    load_block_cols<GPW, NB, SMEM, (FUSED && G > 1) ? 4 : 16>(cp, c);
+    load_block_cols<GPW, NB, SMEM, kIndexLoad<FUSED, G, GPW>>(cp, c);
 #pragma unroll
     for (int u = 0; u < NB; ++u) VecIO<VT, RPT>::load(xq + (size_t)(uint32_t)c[u] * R, xg[u]);
     if constexpr (FUSED) {

@@ -353,7 +353,7 @@ __global__ void __launch_bounds__(256) k_spmm_step(StepParams p)
         const int w = (int)((p.slice_ptr[s + 1] - base) / GPW);
         const unsigned char* rec = p.mat + base * p.entry_bytes;
         constexpr int VS = SLOT ? TPR : 1;   // tile table: [column][group][slot][G]
-        const int voff = SLOT ? (sub * kColUnroll * TPR + q) * G : sub * kColUnroll * G;
+        const int voff = val_thread_off<HT, G, TPR, VS>(sub, q);
         group_slice<VT, CPLX, G, RPT, TPR, false, FIELD, U, false, VS>(
             p, s, w, reinterpret_cast<const int32_t*>(rec) + sub * kColUnroll,
             reinterpret_cast<const HT*>(rec + (size_t)w * GPW * 4) + voff, sc, acc_s);
@@ -555,7 +555,7 @@ __global__ void __launch_bounds__(256, MINB) k_spmm_staged(StepParams p)
         if (p.prefetch >= 3) prefetch_epilogue<VT, R, G, GPW>(p, s);
         if (p.prefetch >= 5) prefetch_ahead<VT, R, G, GPW>(p, s + (int64_t)(p.prefetch == 5 ? 1 : p.prefetch == 6 ? 2 : 4) * nwb);
         constexpr int VS = SLOT ? TPR : 1;   // tile table: [column][group][slot][G], the thread's own slot
-        const int voff = SLOT ? (sub * kColUnroll * TPR + q) * G : sub * kColUnroll * G;
+        const int voff = val_thread_off<HT, G, TPR, VS>(sub, q);
         if (copy_bytes(s) <= cap) {
             const unsigned char* rec = buf + st * cap;
             if (p.prefetch == 1 || p.prefetch == 2)
@@ -784,13 +784,13 @@ __global__ void __launch_bounds__(256, MINB) k_spmm_tiled(StepParams p)
                 const unsigned char* rec = buf + st * cap;
                 tile_slice_step<VT, G, RPT, TPR, true, U>(p, s, w, xbuf,
                                                      reinterpret_cast<const int32_t*>(rec) + sub * kColUnroll,
-                                                     reinterpret_cast<const VT*>(rec + (size_t)w * GPW * 4) + sub * kColUnroll * G,
+                                                     reinterpret_cast<const VT*>(rec + (size_t)w * GPW * 4) + val_thread_off<VT, G, TPR, 1>(sub, 0),
                                                      sc, acc_s);
             } else {
                 const unsigned char* rec = p.mat + base * eb;
                 tile_slice_step<VT, G, RPT, TPR, false, U>(p, s, w, xbuf,
                                                       reinterpret_cast<const int32_t*>(rec) + sub * kColUnroll,
-                                                      reinterpret_cast<const VT*>(rec + (size_t)w * GPW * 4) + sub * kColUnroll * G,
+                                                      reinterpret_cast<const VT*>(rec + (size_t)w * GPW * 4) + val_thread_off<VT, G, TPR, 1>(sub, 0),
                                                       sc, acc_s);
             }
             __syncwarp();   // every lane is done with this buffer before it is refilled
